@@ -1,0 +1,262 @@
+"""k-binning and the power-spectrum estimators (oracle; test only).
+
+Restates:
+
+- ``mesh2.py:25-62``   ``_make_edges2``: edges = ``np.arange(0, kfun.min() * min(N) / 2, step)``
+  (float64), compared in float32 by ``jnp.digitize(right=False)``;
+- ``mesh.py:2833-2863`` ``_get_bin_attrs``: ibin, nmodes (Hermitian weights), xavg;
+- ``mesh.py:2876-2910`` ``_bincount``: per-bin sums over bins ``[1:-1]``;
+- ``mesh2.py:100-119``  ``BinMesh2SpectrumPoles.__call__`` (remove_zero, / nmodes);
+- ``mesh2.py:253-374``  ``compute_mesh2_spectrum``: global line of sight
+  (Legendre of mu = k.los/|k| with |k|(0) = 1) and first-point line of sight
+  (``4 pi * bin(conj(sum_m r2c(rho Y_lm(xhat)) Y_lm(khat)) A0)``), endpoint swap,
+  real part for even ell;
+- ``mesh2.py:508-621`` / ``mesh.py:3042-3129``  FKP normalisation and shot noise;
+- ``mesh.py:2226-2381`` ``get_mesh_attrs`` / ``next_fft_size``.
+
+``accum='f32'`` accumulates bins serially in float32 in flat mode order (the
+reference's CPU bincount order); ``accum='f64'`` accumulates the same float32
+per-mode products in float64 (the accuracy the CUDA kernels are held to).
+"""
+import math
+
+import numpy as np
+
+from .coords import Geometry, kcoords, rcoords, hermitian_weights, r2c, c2r
+from .paint import paint as paint_field
+from .ylm import get_ylm, legendre
+
+
+class Bins:
+    """``BinMesh2SpectrumPoles(mattrs, edges={'step': step}, ells)`` restated."""
+
+    def __init__(self, geom, step=None, edges=None, ells=(0, 2, 4), kmin=0., kmax=None):
+        dt = geom.dtype
+        self.geom = geom
+        self.ells = tuple(sorted((ells,) if np.ndim(ells) == 0 else ells))
+        if edges is None:
+            vec0 = geom.kfun.min()
+            vecmax = dt.type(vec0 * dt.type(np.min(geom.meshsize))) / dt.type(2.)
+            stop = float(vecmax) if kmax is None else kmax
+            edges = np.arange(kmin, stop, step)
+        self.edges = np.asarray(edges, dtype='f8')
+        self.edges_dtype = self.edges.astype(dt)
+        self.wmodes = hermitian_weights(geom)
+        knorm = self.knorm()
+        self.ibin = np.searchsorted(self.edges_dtype, knorm.ravel(), side='right').reshape(knorm.shape)
+        nb = len(self.edges) + 1
+        w = self.wmodes.ravel()
+        self.nmodes = np.bincount(self.ibin.ravel(), weights=w, minlength=nb)[1:-1]
+        ksum = np.bincount(self.ibin.ravel(), weights=(knorm.ravel().astype('f8') * w), minlength=nb)[1:-1]
+        with np.errstate(invalid='ignore', divide='ignore'):
+            self.xavg = ksum / self.nmodes
+
+    @property
+    def nbins(self):
+        return len(self.edges) - 1
+
+    def knorm(self):
+        dt = self.geom.dtype
+        kx, ky, kz = kcoords(self.geom)
+        k2 = (((dt.type(0.) + kx * kx).astype(dt) + ky * ky).astype(dt) + kz * kz).astype(dt)
+        return np.sqrt(k2).astype(dt)
+
+    def __call__(self, value, remove_zero=False, accum='f64'):
+        """Per-bin mean of ``value`` with Hermitian weights (``mesh2.py:100-119``)."""
+        value = np.array(value, copy=True)
+        if remove_zero:
+            value[0, 0, 0] = 0.
+        nb = len(self.edges) + 1
+        ib = self.ibin.ravel()
+        if accum == 'f64':
+            wv = value.ravel() * self.wmodes.ravel().astype(value.real.dtype)
+            if np.iscomplexobj(wv):
+                s = np.bincount(ib, weights=wv.real, minlength=nb) + 1j * np.bincount(ib, weights=wv.imag, minlength=nb)
+            else:
+                s = np.bincount(ib, weights=wv, minlength=nb)
+            return s[1:-1] / self.nmodes
+        dt = value.real.dtype
+        wv = (value.ravel() * self.wmodes.ravel().astype(dt))
+        if np.iscomplexobj(wv):
+            re = np.zeros(nb, dtype=dt)
+            im = np.zeros(nb, dtype=dt)
+            np.add.at(re, ib, wv.real.astype(dt))
+            np.add.at(im, ib, wv.imag.astype(dt))
+            s = re + 1j * im
+        else:
+            s = np.zeros(nb, dtype=dt)
+            np.add.at(s, ib, wv.astype(dt))
+        return s[1:-1] / self.nmodes.astype(dt)
+
+
+def _to_complex(geom, mesh):
+    return mesh if np.iscomplexobj(mesh) else r2c(geom, mesh)
+
+
+def _to_real(geom, mesh):
+    return mesh if not np.iscomplexobj(mesh) else c2r(geom, mesh)
+
+
+def compute_mesh2_spectrum(mesh, bins, los='z', accum='f64', mesh2=None):
+    """``compute_mesh2_spectrum(mesh, bin=bins, los=los)`` (``mesh2.py:253-374``).
+
+    Returns dict(ells, k, nmodes, num_raw (nells, nbins), norm).
+    """
+    geom = bins.geom
+    dt = geom.dtype
+    t = dt.type
+    ells = bins.ells
+    norm = t(np.prod(geom.meshsize.astype(dt))) / t(np.prod(geom.cellsize))
+    swap = False
+    if isinstance(los, str) and los in ('firstpoint', 'local', 'endpoint'):
+        swap = los == 'endpoint'
+        vlos = None
+    else:
+        vlos = np.zeros(3)
+        if isinstance(los, str):
+            vlos['xyz'.index(los)] = 1.
+        else:
+            vlos = np.asarray(los, dtype='f8')
+    num = []
+    if vlos is None:
+        rmesh = _to_real(geom, mesh)
+        A0 = _to_complex(geom, mesh if mesh2 is None else mesh2)
+        cross = mesh2 is not None
+        if swap and cross:
+            rmesh, A0 = _to_real(geom, mesh2), _to_complex(geom, mesh)
+        if 0 in ells:
+            if not cross:
+                A = (A0.real * A0.real + A0.imag * A0.imag).astype(dt)
+            else:
+                A = (np.conj(_to_complex(geom, rmesh)) * A0)
+            num.append(bins(A, accum=accum))
+        xvec = rcoords(geom)
+        kvec = kcoords(geom)
+        for ell in ells:
+            if ell == 0:
+                continue
+            carry = np.zeros(geom.cshape, dtype=A0.dtype)
+            for m in range(-ell, ell + 1):
+                Y = get_ylm(ell, m)
+                F = r2c(geom, (rmesh * Y(*xvec)).astype(dt))
+                carry = (carry + F * Y(*kvec)).astype(A0.dtype)
+            A = (np.conj(carry) * A0).astype(A0.dtype)
+            num.append(t(4. * np.pi) * bins(A, remove_zero=True, accum=accum))
+        if swap:
+            num = [np.conj(n) for n in num]
+    else:
+        A0 = _to_complex(geom, mesh)
+        if mesh2 is None:
+            A = (A0.real * A0.real + A0.imag * A0.imag).astype(dt)
+        else:
+            A = np.conj(A0) * _to_complex(geom, mesh2)
+        if 0 in ells:
+            num.append(bins(A, accum=accum))
+        kvec = kcoords(geom)
+        kl = [(kk * t(ll)).astype(dt) for kk, ll in zip(kvec, vlos)]
+        mu_num = (((t(0.) + kl[0]).astype(dt) + kl[1]).astype(dt) + kl[2]).astype(dt)
+        knorm = bins.knorm().copy()
+        knorm[0, 0, 0] = 1.
+        mu = (mu_num / knorm).astype(dt)
+        for ell in ells:
+            if ell == 0:
+                continue
+            num.append(t(2 * ell + 1) * bins((A * legendre(ell, mu)), remove_zero=True, accum=accum))
+    num = [np.real(n) if ell % 2 == 0 else np.imag(n) for ell, n in zip(ells, num)]
+    return dict(ells=ells, k=bins.xavg, edges=bins.edges, nmodes=bins.nmodes,
+                num_raw=np.array(num), norm=norm,
+                volume=np.prod(geom.kfun.astype('f8')) * bins.nmodes)
+
+
+# --------------------------------------------------------------------------- FKP
+
+def next_fft_size(n, primes=(2, 3, 5, 7), divisors=()):
+    """``next_fft_size`` (``mesh.py:2304-2340``)."""
+    n = int(n)
+    primes = tuple(p for p in primes if p > 1)
+    divisors = tuple(int(d) for d in divisors if d > 1)
+    D = 1
+    for d in divisors:
+        D = abs(D * d) // math.gcd(D, d)
+    m = ((n + D - 1) // D) * D
+    if not primes:
+        return m
+    while True:
+        x = m
+        for p in primes:
+            while x % p == 0:
+                x //= p
+        if x == 1:
+            return m
+        m += D
+
+
+def get_mesh_attrs(*positions, meshsize=None, boxsize=None, boxcenter=None, cellsize=None,
+                   boxpad=2., primes=None, dtype=np.float32):
+    """``get_mesh_attrs`` (``mesh.py:2271-2381``) without sharding; returns a Geometry."""
+    dt = np.dtype(dtype)
+    if cellsize is not None and meshsize is not None:
+        meshsize = np.broadcast_to(np.asarray(meshsize, 'i4'), (3,))
+        boxsize = meshsize * np.broadcast_to(np.asarray(cellsize, dt), (3,))
+    if boxsize is None or boxcenter is None:
+        pmin = np.min([np.min(p, axis=0) for p in positions if p.size], axis=0)
+        pmax = np.max([np.max(p, axis=0) for p in positions if p.size], axis=0)
+        delta = np.abs(pmax - pmin)
+        if boxcenter is None:
+            boxcenter = (dt.type(0.5) * (pmin + pmax)).astype(dt)
+        if boxsize is None:
+            boxsize = (delta.max() * dt.type(boxpad)).astype(dt)
+    boxsize = np.broadcast_to(np.asarray(boxsize, dt), (3,)).copy()
+    if meshsize is None:
+        cs = np.broadcast_to(np.asarray(cellsize, dt), (3,))
+        meshsize = np.ceil((boxsize / cs).astype(dt)).astype('i4')
+        meshsize = np.array([next_fft_size(n, primes=primes or ()) for n in meshsize])
+        boxsize = (meshsize * cs).astype(dt)
+    return Geometry(meshsize, boxsize=boxsize, boxcenter=boxcenter, dtype=dt)
+
+
+def fkp_particles(data_pos, data_w, rand_pos, rand_w, dtype=np.float32):
+    """``FKPField.particles`` (``mesh.py:2965-2971``): data - alpha * randoms."""
+    dt = np.dtype(dtype)
+    data_w = np.ones(len(data_pos), dt) if data_w is None else np.asarray(data_w, dt)
+    rand_w = np.ones(len(rand_pos), dt) if rand_w is None else np.asarray(rand_w, dt)
+    alpha = (np.sum(data_w, dtype=dt) / np.sum(rand_w, dtype=dt)).astype(dt)
+    pos = np.concatenate([np.asarray(data_pos, dt), np.asarray(rand_pos, dt)])
+    w = np.concatenate([data_w, (-alpha * rand_w).astype(dt)])
+    return pos, w, alpha
+
+
+def fkp2_shotnoise(weights):
+    """``compute_fkp2_shotnoise`` auto case (``mesh2.py:601-611``): sum of w^2."""
+    w = np.asarray(weights, dtype='f8')
+    return float(np.sum(w * w))
+
+
+def fkp2_normalization(geom, data_pos, data_w, rand_pos, rand_w, cellsize=10.):
+    """``compute_fkp2_normalization`` auto case (``mesh2.py:516-574``, ``mesh.py:3002-3118``).
+
+    alpha * sum(rho_d * rho_r) / V_cell with CIC meshes at the given cellsize.
+    """
+    dt = geom.dtype
+    data_w = np.ones(len(data_pos), dt) if data_w is None else np.asarray(data_w, dt)
+    rand_w = np.ones(len(rand_pos), dt) if rand_w is None else np.asarray(rand_w, dt)
+    alpha = np.sum(data_w.astype('f8')) / np.sum(rand_w.astype('f8'))
+    g2 = norm_geometry(geom, cellsize)
+    rd = paint_field(g2, data_pos, data_w, resampler='cic', interlacing=0, compensate=False)
+    rr = paint_field(g2, rand_pos, rand_w, resampler='cic', interlacing=0, compensate=False)
+    return float(alpha * np.sum(rd.astype('f8') * rr.astype('f8')) / np.prod(g2.cellsize.astype('f8')))
+
+
+def norm_geometry(geom, cellsize=10.):
+    """``get_halo_for_new_mattrs(mattrs, cellsize=...)`` (``mesh.py:3002-3039``), no sharding."""
+    dt = geom.dtype
+    cs = np.broadcast_to(np.asarray(cellsize, dt), (3,))
+    meshsize = np.ceil((geom.boxsize / cs).astype(dt)).astype('i4')
+    boxsize = (meshsize * cs.astype('f8')).astype(dt)
+    odd = (meshsize - geom.meshsize) % 2 != 0
+    if np.any(odd):
+        # keep an even difference with the painted mesh: one more cell on every axis
+        cell = (boxsize / meshsize.astype(dt)).astype(dt)
+        meshsize = meshsize + 1
+        boxsize = (cell * meshsize.astype(dt)).astype(dt)
+    return Geometry(meshsize, boxsize=boxsize, boxcenter=geom.boxcenter, dtype=dt, backend=geom.backend)
