@@ -1,0 +1,169 @@
+/*
+ * jaxpower_b200: C ABI of the B200 (sm_100a) mesh power-spectrum kernels.
+ *
+ * Drop-in boundary for jax-power's single-GPU power-spectrum path.  Each entry
+ * point replaces one reference function (cited below as path:line inside the
+ * adematti/jax-power project).  All calls:
+ *   - take plain device pointers and sizes, borrowed from the caller;
+ *   - are ordered on the given CUDA stream (cudaStream_t passed as void*),
+ *     with no hidden device synchronisation (except where stated);
+ *   - take caller-owned workspace sized by the matching *_workspace_size();
+ *   - return a pk_status; on error pk_last_error() describes it (thread local).
+ *
+ * Layouts: positions (n, 3) float32 row-major; weights (n,) float32 (NULL = 1);
+ * real mesh (N0, N1, N2) float32 C order; complex mesh (N0, N1, N2/2+1)
+ * interleaved complex64 (float2) C order (cuFFT R2C layout, the reference's
+ * Hermitian layout of fft_backend='jax').
+ */
+#ifndef JAXPOWER_B200_H
+#define JAXPOWER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int pk_status;
+enum {
+  PK_OK = 0,
+  PK_ERR_INVALID = 1,   /* bad argument (sizes, orders, null pointers) */
+  PK_ERR_CUDA = 2,      /* a CUDA runtime / cuFFT call failed */
+  PK_ERR_WORKSPACE = 3, /* workspace too small */
+  PK_ERR_RANGE = 4      /* input outside the supported range */
+};
+
+/* Fourier-layout semantics of the reference's two FFT backends
+ * (mesh.py:1488-1489, 1679-1719): 0 = 'jax' (rfftn, Hermitian weights
+ * 1 + (kz > 0)); 1 = 'jaxdecomp' (full complex FFT), reproduced on the
+ * Hermitian storage (interlacing phase symmetrised, Nyquist-plane weight 1). */
+enum { PK_BACKEND_JAX = 0, PK_BACKEND_JAXDECOMP = 1 };
+
+const char *pk_version(void);
+const char *pk_last_error(void);
+
+/* ------------------------------------------------------------------ paint
+ * Replaces resamplers.paint (resamplers.py:66-97) as driven by _paint
+ * (mesh.py:2673-2729): positions are normalised as
+ * (pos + boxsize/2 - boxcenter) / cellsize in float32 (mesh.py:2684), shifted
+ * by shift_s = s / interlacing (mesh.py:2679) for s in
+ * [shift_begin, shift_begin + nshifts) (nshifts <= 4) and painted with the
+ * order-`order` B-spline (1 ngp, 2 cic, 3 tsc, 4 pcs) on the periodic mesh.
+ * Writes nshifts real meshes, out[j * N0*N1*N2 + ...].  Deterministic: per-cell
+ * sums are accumulated in 64-bit fixed point, independent of particle order.
+ * cellsize[3] is boxsize / meshsize in float32 (mesh.py:1575).
+ * d_status (device int, may be NULL) is set to 1 if a position or weight is
+ * not finite or a position is more than 2^22 cells away; such particles are
+ * skipped. */
+pk_status pk_paint_workspace_size(int64_t n, const int32_t meshsize[3], int order,
+                                  int nshifts, size_t *bytes);
+pk_status pk_paint(void *stream, const float *positions, const float *weights, int64_t n,
+                   const int32_t meshsize[3], const float boxsize[3],
+                   const float boxcenter[3], const float cellsize[3], int order,
+                   int interlacing, int shift_begin, int nshifts, float *out,
+                   void *workspace, size_t workspace_bytes, int *d_status);
+
+/* Replaces resamplers.read (resamplers.py:100-125) via _read (mesh.py:2064-2110):
+ * out[p] = sum_offsets mesh[wrap(i0 + off)] * W(u), u normalised as above plus
+ * `shift`.  If grad (n, 3) is non-NULL, also writes
+ * grad[p, d] = scale * w_p * sum_offsets mesh * dW/du_d / cellsize_d
+ * (the position gradient of paint's adjoint); accumulate != 0 adds into
+ * out / grad instead of overwriting. */
+pk_status pk_read(void *stream, const float *mesh, const float *positions,
+                  const float *weights, int64_t n, const int32_t meshsize[3],
+                  const float boxsize[3], const float boxcenter[3], const float cellsize[3],
+                  int order, float shift, float scale, float *out, float *grad,
+                  int accumulate);
+
+/* ------------------------------------------------------------------- FFT
+ * cuFFT plans for the reference's r2c / c2r (mesh.py:1679-1719): batch meshes
+ * of shape meshsize, contiguous, out of place.  Both directions are
+ * unnormalised; jnp.fft.irfftn's 1 / (N0 N1 N2) is folded by the caller into
+ * the preceding pass (pk_interlace_compensate's scale) or pk_scale_real.
+ * A C2R overwrites its input.  direction: 0 = R2C, 1 = C2R. */
+typedef struct pk_fft_plan_s *pk_fft_plan;
+pk_status pk_fft_plan_create(const int32_t meshsize[3], int batch, int direction,
+                             pk_fft_plan *plan);
+pk_status pk_fft_exec(pk_fft_plan plan, void *stream, void *in, void *out);
+pk_status pk_fft_plan_destroy(pk_fft_plan plan);
+
+/* ------------------------------------------- interlacing + compensation
+ * Fused replacement of the interlacing accumulation (mesh.py:2737-2749),
+ * compensation (resamplers.py:16-26, mesh.py:2733-2751) in one pass:
+ *   out(k) = C(k) / I * sum_s in_s(k) * exp(i shift_s (kx_c + ky_c + kz_c))
+ * with circular k (mesh.py:1627-1629), C = prod_d sinc(k_d/2pi)^-comp_order
+ * (comp_order = 0: none).  for_c2r != 0 Hermitian-symmetrises the kz = 0 and
+ * kz = N/2 planes so any C2R gives numpy's irfftn of the same data.
+ * backend selects the 'jax' / 'jaxdecomp' semantics; the output is multiplied
+ * by scale.  in holds the nshifts = interlacing shifted meshes (shift s / I);
+ * in may equal out only when nshifts == 1 and for_c2r == 0. */
+pk_status pk_interlace_compensate(void *stream, const void *in, int nshifts,
+                                  const int32_t meshsize[3], int comp_order, int backend,
+                                  int for_c2r, float scale, void *out);
+
+/* Multiply a real array by scale (e.g. the C2R normalisation). */
+pk_status pk_scale_real(void *stream, float *mesh, int64_t size, float scale);
+
+/* --------------------------------------------------------------- binning
+ * Bins are the reference's BinMesh2SpectrumPoles (mesh2.py:25-119):
+ * k edges edges[0..nedges-1] (float32-rounded, as jnp.digitize compares them),
+ * bin b in [0, nedges-1) holds modes with edges[b] <= |k| < edges[b+1]; |k|
+ * from kcoords (mesh.py:1605-1636) in float32: kfun[d] * N_d * fftfreq.
+ * step > 0 declares uniform edges edges[b] = edges[0] + b*step (fast path).
+ * Accumulation: float32 per-mode values, warp-segmented float32 partials,
+ * float64 per-CTA histograms, float64 final sum in a fixed order
+ * (deterministic).  Outputs are float64. */
+pk_status pk_bin_workspace_size(const int32_t meshsize[3], int nedges, int nvalues,
+                                size_t *bytes);
+
+/* nmodes[b] = sum of Hermitian weights, ksum[b] = sum of w |k| (mesh.py:2833-2863). */
+pk_status pk_bin_modes(void *stream, const int32_t meshsize[3], const float kfun[3],
+                       const float *d_edges, int nedges, float step, int backend,
+                       double *d_nmodes, double *d_ksum, void *workspace,
+                       size_t workspace_bytes);
+
+/* BinMesh2SpectrumPoles.__call__ (mesh2.py:100-119) numerator: per-bin sum of
+ * w * value for a complex mesh; d_out[0 * nbins + b] real part,
+ * d_out[1 * nbins + b] imaginary part.  remove_zero drops the k = 0 mode. */
+pk_status pk_bin_mesh(void *stream, const void *value, const int32_t meshsize[3],
+                      const float kfun[3], const float *d_edges, int nedges, float step,
+                      int backend, int remove_zero, double *d_out, void *workspace,
+                      size_t workspace_bytes);
+
+/* Global line of sight (mesh2.py:346-374): for each requested ell,
+ * sum over the bin of w * Re/Im(A) * L_ell(mu), mu = k.los / |k| (|k|(0) = 1),
+ * A = |delta1|^2 (delta2 NULL) or conj(delta1) delta2; ell > 0 drops k = 0.
+ * Re for even ell, Im for odd.  d_out[ill * nbins + b] (raw sums; divide by
+ * nmodes and multiply by 2 ell + 1 on the host). */
+pk_status pk_bin_global(void *stream, const void *delta1, const void *delta2,
+                        const int32_t meshsize[3], const float kfun[3], const float los[3],
+                        const float *d_edges, int nedges, float step, int backend,
+                        int nells, const int32_t *ells, double *d_out, void *workspace,
+                        size_t workspace_bytes);
+
+/* First-point line of sight (mesh2.py:293-344), one batch of (ell, m) terms:
+ * d_out[ill * nbins + b] (+)= sum over the bin of w * Re/Im(conj(S_ell) A0),
+ * S_ell = sum_{m in batch} F_j(k) Y_ell,m(khat), F_j = r2c(rho Y_ell,m(xhat)).
+ * ell = 0 entries of `ells` take |A0|^2 (or conj(B0) A0 with b0 != NULL) and
+ * are only accumulated when include_ell0 != 0.  accumulate != 0 adds into d_out. */
+pk_status pk_bin_firstpoint(void *stream, const void *a0, const void *b0, const void *f,
+                            int nterms, const int32_t *term_ell, const int32_t *term_m,
+                            const int32_t meshsize[3], const float kfun[3],
+                            const float *d_edges, int nedges, float step, int backend,
+                            int nells, const int32_t *ells, int include_ell0,
+                            int accumulate, double *d_out, void *workspace,
+                            size_t workspace_bytes);
+
+/* Real-space Y_lm premultiply for the first-point estimator (mesh2.py:313-327):
+ * out[j] = rho(x) * Y_{ell_j, m_j}(xhat) at cell corners
+ * x_i = i * cellsize + (boxcenter - boxsize/2) (mesh.py:1594-1603), observer at 0. */
+pk_status pk_ylm_premultiply(void *stream, const float *rho, const int32_t meshsize[3],
+                             const float cellsize[3], const float offset[3], int nterms,
+                             const int32_t *term_ell, const int32_t *term_m, float *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JAXPOWER_B200_H */

@@ -1,0 +1,512 @@
+// Particle painting and reading (resampler scatter / gather) for sm_100a.
+//
+// Paint = resamplers.paint (resamplers.py:66-97) driven by _paint
+// (mesh.py:2673-2729) for all interlacing shifts at once.
+//
+// Design (HBM-bound, deterministic, no global float atomics):
+//   1. pk_bucket_count: per particle, normalise the position exactly as the
+//      reference (float32 IEEE ops, mesh.py:2684), find every mesh tile its
+//      stencil can reach for any shift, and count it there (int atomics);
+//      also track max|w| (for the fixed-point scale).
+//   2. exclusive scan of the tile counts (CUB).
+//   3. pk_bucket_fill: write (u, w) as a float4 into each reached tile's bucket.
+//   4. pk_paint_tiles: one CTA per tile: every shifted mesh of the tile is
+//      accumulated in shared memory as 64-bit fixed point (integer addition is
+//      associative, so the result does not depend on particle order or thread
+//      scheduling), then converted once to float32 and written with coalesced
+//      float4 stores.  Each output cell is written exactly once; the mesh is
+//      never memset.
+#include <cub/device/device_scan.cuh>
+#include <math.h>
+
+#include "common.cuh"
+
+namespace pk {
+
+constexpr int TILE0 = 8, TILE1 = 16, TILE2 = 32;
+constexpr int TILE_CELLS = TILE0 * TILE1 * TILE2;
+constexpr int MAX_SHIFTS = 4;
+constexpr int MAX_ORDER = 4;
+constexpr float MAX_CELL_COORD = 4194304.f;  // 2^22 cells
+
+struct PaintGeom {
+  Dims d;
+  float half[3], center[3], cell[3];
+  int order;
+  int nshifts;
+  float shifts[MAX_SHIFTS];
+  int reach_lo, reach_hi;  // stencil reach below / above floor(u), all shifts
+  int nt[3];               // tiles per axis
+};
+
+__device__ __forceinline__ float normalise(float p, float half, float center, float cell) {
+  // ((pos + boxsize / 2.) - boxcenter) / cellsize, mesh.py:2684, no contraction
+  return __fdiv_rn(__fsub_rn(__fadd_rn(p, half), center), cell);
+}
+
+__device__ __forceinline__ int wrapi(int i, int n) {
+  int r = i % n;
+  return r < 0 ? r + n : r;
+}
+
+// The reference's kernels (resamplers.py:57-63) in float32 without contraction.
+__device__ __forceinline__ float bspline(int order, float s) {
+  switch (order) {
+    case 1:
+      return 1.f;
+    case 2:
+      return __fsub_rn(1.f, s);
+    case 3:
+      if (s <= 0.5f) return __fsub_rn(0.75f, __fmul_rn(s, s));
+      {
+        float t = __fsub_rn(1.5f, s);
+        return __fmul_rn(0.5f, __fmul_rn(t, t));
+      }
+    default: {
+      const float sixth = 0.16666667f;  // (bool) / 6 in float32
+      if (s <= 1.f) {
+        float s2 = __fmul_rn(s, s);
+        float s3 = __fmul_rn(s, s2);
+        float p = __fadd_rn(__fsub_rn(4.f, __fmul_rn(6.f, s2)), __fmul_rn(3.f, s3));
+        return __fmul_rn(sixth, p);
+      }
+      float t = __fsub_rn(2.f, s);
+      return __fmul_rn(sixth, __fmul_rn(t, __fmul_rn(t, t)));
+    }
+  }
+}
+
+// dW/ds of the kernels above.
+__device__ __forceinline__ float bspline_deriv(int order, float s) {
+  switch (order) {
+    case 1:
+      return 0.f;
+    case 2:
+      return -1.f;
+    case 3:
+      return s <= 0.5f ? -2.f * s : -(1.5f - s);
+    default:
+      return s <= 1.f ? (-12.f * s + 9.f * s * s) / 6.f : -0.5f * (2.f - s) * (2.f - s);
+  }
+}
+
+// Base index: floor for even orders, round-half-to-even for odd (jnp.round).
+__device__ __forceinline__ int base_index(int order, float u) {
+  return (order & 1) ? (int)rintf(u) : (int)floorf(u);
+}
+
+__device__ __forceinline__ int offset_lo(int order) { return -((order - 1) / 2); }
+
+// Distinct tiles of the wrapped cell span [c - lo, c + hi] along one axis.
+__device__ __forceinline__ int span_tiles(int c, int lo, int hi, int n, int tile, int nt,
+                                          int out[3]) {
+  int count = 0;
+  for (int x = c - lo; x <= c + hi; ++x) {
+    int t = wrapi(x, n) / tile;
+    bool seen = false;
+    for (int k = 0; k < count; ++k) seen |= (out[k] == t);
+    if (!seen && count < 3) out[count++] = t;
+  }
+  (void)nt;
+  return count;
+}
+
+__device__ __forceinline__ bool load_particle(const PaintGeom &g, const float *pos,
+                                              const float *w, int64_t p, float u[3],
+                                              float *wp) {
+  const float *q = pos + 3 * p;
+  bool ok = true;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    u[d] = normalise(q[d], g.half[d], g.center[d], g.cell[d]);
+    ok &= isfinite(u[d]) && fabsf(u[d]) < MAX_CELL_COORD;
+  }
+  *wp = w ? w[p] : 1.f;
+  return ok;
+}
+
+template <bool FILL>
+__global__ void bucket_kernel(PaintGeom g, const float *__restrict__ pos,
+                              const float *__restrict__ w, int64_t n,
+                              unsigned *__restrict__ counts, const int *__restrict__ offsets,
+                              unsigned *__restrict__ cursors, float4 *__restrict__ bucket,
+                              unsigned *__restrict__ wmax_bits, int *__restrict__ status) {
+  const int tiles[3] = {TILE0, TILE1, TILE2};
+  const int ns[3] = {g.d.n0, g.d.n1, g.d.n2};
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    float u[3], wp;
+    if (!load_particle(g, pos, w, p, u, &wp) || !isfinite(wp)) {
+      if (!FILL && status) atomicExch(status, 1);
+      continue;
+    }
+    if (!FILL) atomicMax(wmax_bits, __float_as_uint(fabsf(wp)));
+    int t[3][3], nt[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      int c = (int)floorf(u[d]);
+      nt[d] = span_tiles(c, g.reach_lo, g.reach_hi, ns[d], tiles[d], g.nt[d], t[d]);
+    }
+    for (int a = 0; a < nt[0]; ++a)
+      for (int b = 0; b < nt[1]; ++b)
+        for (int c = 0; c < nt[2]; ++c) {
+          int tile = (t[0][a] * g.nt[1] + t[1][b]) * g.nt[2] + t[2][c];
+          if (!FILL) {
+            atomicAdd(counts + tile, 1u);
+          } else {
+            unsigned slot = atomicAdd(cursors + tile, 1u);
+            bucket[(int64_t)offsets[tile] + slot] = make_float4(u[0], u[1], u[2], wp);
+          }
+        }
+  }
+}
+
+// 2^e with e chosen so that n * max|w| * 2^e < 2^62: exact fixed point.
+__device__ __forceinline__ double fixed_scale(unsigned wmax_bits, int64_t n) {
+  float wmax = __uint_as_float(wmax_bits);
+  if (!(wmax > 0.f) || !isfinite(wmax)) return 1099511627776.0;  // 2^40
+  int ew;
+  frexpf(wmax, &ew);  // wmax < 2^ew
+  int en = 64 - __clzll((unsigned long long)(n > 0 ? n : 1));  // n < 2^en
+  int e = 62 - ew - en;
+  return ldexp(1.0, e);
+}
+
+__global__ void __launch_bounds__(256) paint_tiles_kernel(
+    PaintGeom g, const float4 *__restrict__ bucket, const int *__restrict__ offsets,
+    const unsigned *__restrict__ wmax_bits, int64_t n, float *__restrict__ out) {
+  extern __shared__ unsigned long long acc[];  // [nshifts][TILE_CELLS]
+  const int tile = blockIdx.x;
+  const int t2i = tile % g.nt[2];
+  const int t1i = (tile / g.nt[2]) % g.nt[1];
+  const int t0i = tile / (g.nt[2] * g.nt[1]);
+  const int lo0 = t0i * TILE0, lo1 = t1i * TILE1, lo2 = t2i * TILE2;
+  const int begin = offsets[tile], end = offsets[tile + 1];
+  const int ncell = g.nshifts * TILE_CELLS;
+  const bool empty = (begin == end);
+
+  if (!empty) {
+    for (int i = threadIdx.x; i < ncell; i += blockDim.x) acc[i] = 0ull;
+    __syncthreads();
+    const double scale = fixed_scale(*wmax_bits, n);
+    const int order = g.order;
+    const int olo = offset_lo(order);
+    for (int p = begin + threadIdx.x; p < end; p += blockDim.x) {
+      const float4 q = bucket[p];
+      const float uq[3] = {q.x, q.y, q.z};
+      for (int s = 0; s < g.nshifts; ++s) {
+        float k[3][MAX_ORDER];
+        int l[3][MAX_ORDER];
+        const int ns[3] = {g.d.n0, g.d.n1, g.d.n2};
+        const int los[3] = {lo0, lo1, lo2};
+        const int tl[3] = {TILE0, TILE1, TILE2};
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const float u = __fadd_rn(uq[d], g.shifts[s]);
+          const int i0 = base_index(order, u);
+#pragma unroll
+          for (int o = 0; o < MAX_ORDER; ++o) {
+            if (o < order) {
+              const int idx = i0 + olo + o;
+              const float sd = fabsf(__fsub_rn((float)idx, u));
+              k[d][o] = bspline(order, sd);
+              int loc = wrapi(idx, ns[d]) - los[d];
+              l[d][o] = (loc >= 0 && loc < tl[d]) ? loc : -1;
+            }
+          }
+        }
+        unsigned long long *as = acc + s * TILE_CELLS;
+        for (int a = 0; a < order; ++a) {
+          if (l[0][a] < 0) continue;
+          for (int b = 0; b < order; ++b) {
+            if (l[1][b] < 0) continue;
+            const float kab = __fmul_rn(k[0][a], k[1][b]);
+            const int rowoff = (l[0][a] * TILE1 + l[1][b]) * TILE2;
+            for (int c = 0; c < order; ++c) {
+              if (l[2][c] < 0) continue;
+              const float v = __fmul_rn(q.w, __fmul_rn(kab, k[2][c]));
+              const long long fx = __double2ll_rn((double)v * scale);
+              atomicAdd(as + rowoff + l[2][c], (unsigned long long)fx);
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+    // convert and store
+    const double inv = 1.0 / scale;
+    const bool vec = (g.d.n2 % 4) == 0;
+    for (int s = 0; s < g.nshifts; ++s) {
+      float *mesh = out + (int64_t)s * g.d.nreal();
+      const unsigned long long *as = acc + s * TILE_CELLS;
+      for (int i = threadIdx.x * 4; i < TILE_CELLS; i += blockDim.x * 4) {
+        const int c2 = i % TILE2, c1 = (i / TILE2) % TILE1, c0 = i / (TILE2 * TILE1);
+        const int x0 = lo0 + c0, x1 = lo1 + c1, x2 = lo2 + c2;
+        if (x0 >= g.d.n0 || x1 >= g.d.n1) continue;
+        const int64_t base = ((int64_t)x0 * g.d.n1 + x1) * g.d.n2 + x2;
+        float v[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          v[j] = __double2float_rn((double)(long long)as[i + j] * inv);
+        if (vec) {
+          if (x2 < g.d.n2) *reinterpret_cast<float4 *>(mesh + base) = make_float4(v[0], v[1], v[2], v[3]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (x2 + j < g.d.n2) mesh[base + j] = v[j];
+        }
+      }
+    }
+  } else {
+    const bool vec = (g.d.n2 % 4) == 0;
+    for (int s = 0; s < g.nshifts; ++s) {
+      float *mesh = out + (int64_t)s * g.d.nreal();
+      for (int i = threadIdx.x * 4; i < TILE_CELLS; i += blockDim.x * 4) {
+        const int c2 = i % TILE2, c1 = (i / TILE2) % TILE1, c0 = i / (TILE2 * TILE1);
+        const int x0 = lo0 + c0, x1 = lo1 + c1, x2 = lo2 + c2;
+        if (x0 >= g.d.n0 || x1 >= g.d.n1) continue;
+        const int64_t base = ((int64_t)x0 * g.d.n1 + x1) * g.d.n2 + x2;
+        if (vec) {
+          if (x2 < g.d.n2) *reinterpret_cast<float4 *>(mesh + base) = make_float4(0.f, 0.f, 0.f, 0.f);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (x2 + j < g.d.n2) mesh[base + j] = 0.f;
+        }
+      }
+    }
+  }
+}
+
+// Gather (resamplers.read) plus the position gradient of paint's adjoint.
+__global__ void read_kernel(PaintGeom g, const float *__restrict__ mesh,
+                            const float *__restrict__ pos, const float *__restrict__ w,
+                            int64_t n, float shift, float scale, float *__restrict__ out,
+                            float *__restrict__ grad, int accumulate) {
+  const int ns[3] = {g.d.n0, g.d.n1, g.d.n2};
+  const int order = g.order;
+  const int olo = offset_lo(order);
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    float u[3], wp;
+    load_particle(g, pos, w, p, u, &wp);
+    float k[3][MAX_ORDER], dk[3][MAX_ORDER];
+    int idx[3][MAX_ORDER];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float ud = __fadd_rn(u[d], shift);
+      const int i0 = base_index(order, ud);
+#pragma unroll
+      for (int o = 0; o < MAX_ORDER; ++o) {
+        if (o < order) {
+          const int ii = i0 + olo + o;
+          const float diff = __fsub_rn((float)ii, ud);
+          const float sd = fabsf(diff);
+          k[d][o] = bspline(order, sd);
+          // ds/du = -sign(idx - u); sign(0) = 0 as in JAX's abs derivative
+          const float sgn = diff > 0.f ? -1.f : (diff < 0.f ? 1.f : 0.f);
+          dk[d][o] = bspline_deriv(order, sd) * sgn;
+          idx[d][o] = wrapi(ii, ns[d]);
+        }
+      }
+    }
+    float acc = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f;
+    for (int a = 0; a < order; ++a)
+      for (int b = 0; b < order; ++b) {
+        const int64_t row = ((int64_t)idx[0][a] * g.d.n1 + idx[1][b]) * g.d.n2;
+        const float kab = __fmul_rn(k[0][a], k[1][b]);
+        for (int c = 0; c < order; ++c) {
+          const float m = mesh[row + idx[2][c]];
+          acc = __fadd_rn(acc, __fmul_rn(m, __fmul_rn(kab, k[2][c])));
+          if (grad) {
+            g0 += m * dk[0][a] * k[1][b] * k[2][c];
+            g1 += m * k[0][a] * dk[1][b] * k[2][c];
+            g2 += m * kab * dk[2][c];
+          }
+        }
+      }
+    if (out) out[p] = accumulate ? out[p] + scale * acc : scale * acc;
+    if (grad) {
+      const float f = scale * wp;
+      const float v0 = f * g0 / g.cell[0], v1 = f * g1 / g.cell[1], v2 = f * g2 / g.cell[2];
+      float *gp = grad + 3 * p;
+      if (accumulate) {
+        gp[0] += v0;
+        gp[1] += v1;
+        gp[2] += v2;
+      } else {
+        gp[0] = v0;
+        gp[1] = v1;
+        gp[2] = v2;
+      }
+    }
+  }
+}
+
+static bool fill_geom(const int32_t meshsize[3], const float boxsize[3], const float boxcenter[3],
+                      const float cellsize[3], int order, int nshifts, const float *shifts,
+                      PaintGeom *g) {
+  if (!make_dims(meshsize, &g->d)) return false;
+  if (order < 1 || order > MAX_ORDER) return false;
+  if (nshifts < 1 || nshifts > MAX_SHIFTS) return false;
+  for (int d = 0; d < 3; ++d) {
+    g->half[d] = boxsize[d] / 2.f;
+    g->center[d] = boxcenter[d];
+    g->cell[d] = cellsize[d];
+    if (!(cellsize[d] > 0.f)) return false;
+  }
+  g->order = order;
+  g->nshifts = nshifts;
+  bool shifted = false;
+  for (int s = 0; s < MAX_SHIFTS; ++s) {
+    g->shifts[s] = s < nshifts ? shifts[s] : 0.f;
+    shifted |= (s < nshifts && shifts[s] != 0.f);
+  }
+  const int hi = order - 1 - (order - 1) / 2;
+  g->reach_lo = (order - 1) / 2;
+  g->reach_hi = hi + (order & 1 ? 1 : 0) + (shifted ? 1 : 0);
+  const int tiles[3] = {TILE0, TILE1, TILE2};
+  for (int d = 0; d < 3; ++d) g->nt[d] = (meshsize[d] + tiles[d] - 1) / tiles[d];
+  return true;
+}
+
+static int max_copies_axis(int n, int tile, int nt, int span) {
+  if (nt <= 1) return 1;
+  int last = n - (nt - 1) * tile;
+  int c = (last >= span - 1 || last == tile) ? 2 : 3;
+  return c < nt ? c : nt;
+}
+
+struct PaintLayout {
+  int64_t ntiles;
+  int64_t max_entries;
+  size_t scan_bytes;
+  size_t total;
+};
+
+static pk_status paint_layout(int64_t n, const PaintGeom &g, PaintLayout *L) {
+  L->ntiles = (int64_t)g.nt[0] * g.nt[1] * g.nt[2];
+  const int span = g.reach_lo + g.reach_hi + 1;
+  const int tiles[3] = {TILE0, TILE1, TILE2};
+  const int ns[3] = {g.d.n0, g.d.n1, g.d.n2};
+  int64_t copies = 1;
+  for (int d = 0; d < 3; ++d) copies *= max_copies_axis(ns[d], tiles[d], g.nt[d], span);
+  L->max_entries = n * copies;
+  PK_REQUIRE(L->max_entries < (int64_t)INT32_MAX, PK_ERR_RANGE,
+             "too many particles for one paint call (%lld x %lld tile copies)", (long long)n,
+             (long long)copies);
+  L->scan_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, L->scan_bytes, (unsigned *)nullptr, (int *)nullptr,
+                                (int)(L->ntiles + 1));
+  Carver c(nullptr);
+  c.take<unsigned>(L->ntiles + 1);  // counts
+  c.take<int>(L->ntiles + 1);       // offsets
+  c.take<unsigned>(L->ntiles);      // cursors
+  c.take<unsigned>(4);              // wmax bits
+  c.take<char>(L->scan_bytes);
+  c.take<float4>(L->max_entries);
+  L->total = align_up(c.used);
+  return PK_OK;
+}
+
+}  // namespace pk
+
+using namespace pk;
+
+extern "C" pk_status pk_paint_workspace_size(int64_t n, const int32_t meshsize[3], int order,
+                                             int nshifts, size_t *bytes) {
+  PK_REQUIRE(bytes, PK_ERR_INVALID, "bytes is NULL");
+  PK_REQUIRE(n >= 0, PK_ERR_INVALID, "negative particle count");
+  float box[3] = {1.f, 1.f, 1.f}, cen[3] = {0.f, 0.f, 0.f}, cell[3] = {1.f, 1.f, 1.f};
+  // worst-case reach: any nonzero shift
+  float shifts[MAX_SHIFTS] = {0.f, 0.5f, 0.5f, 0.5f};
+  if (nshifts > MAX_SHIFTS) nshifts = MAX_SHIFTS;
+  PaintGeom g;
+  PK_REQUIRE(fill_geom(meshsize, box, cen, cell, order, nshifts, shifts, &g), PK_ERR_INVALID,
+             "invalid meshsize / order (1..4) / nshifts (1..%d)", MAX_SHIFTS);
+  PaintLayout L;
+  pk_status st = paint_layout(n, g, &L);
+  if (st) return st;
+  *bytes = L.total;
+  return PK_OK;
+}
+
+extern "C" pk_status pk_paint(void *stream, const float *positions, const float *weights,
+                              int64_t n, const int32_t meshsize[3], const float boxsize[3],
+                              const float boxcenter[3], const float cellsize[3], int order,
+                              int interlacing, int shift_begin, int nshifts, float *out,
+                              void *workspace, size_t workspace_bytes, int *d_status) {
+  PK_REQUIRE(out, PK_ERR_INVALID, "out is NULL");
+  PK_REQUIRE(n == 0 || positions, PK_ERR_INVALID, "positions is NULL");
+  PK_REQUIRE(boxsize && boxcenter && cellsize, PK_ERR_INVALID, "geometry pointer is NULL");
+  PK_REQUIRE(interlacing >= 1 && shift_begin >= 0 && shift_begin + nshifts <= interlacing,
+             PK_ERR_INVALID, "invalid interlacing %d / shift range [%d, %d)", interlacing,
+             shift_begin, shift_begin + nshifts);
+  float shifts[MAX_SHIFTS];
+  for (int s = 0; s < MAX_SHIFTS; ++s)  // arange(I) * 1. / I in float32 (mesh.py:2679)
+    shifts[s] = s < nshifts ? (float)(shift_begin + s) / (float)interlacing : 0.f;
+  PaintGeom g;
+  PK_REQUIRE(fill_geom(meshsize, boxsize, boxcenter, cellsize, order, nshifts, shifts, &g),
+             PK_ERR_INVALID, "invalid meshsize / order (1..4) / nshifts (1..%d) / cellsize",
+             MAX_SHIFTS);
+  PaintLayout L;
+  pk_status st = paint_layout(n, g, &L);
+  if (st) return st;
+  PK_REQUIRE(workspace && workspace_bytes >= L.total, PK_ERR_WORKSPACE,
+             "paint workspace too small: need %zu bytes, got %zu", L.total, workspace_bytes);
+  cudaStream_t s = (cudaStream_t)stream;
+  Carver c(workspace);
+  unsigned *counts = c.take<unsigned>(L.ntiles + 1);
+  int *offsets = c.take<int>(L.ntiles + 1);
+  unsigned *cursors = c.take<unsigned>(L.ntiles);
+  unsigned *wmax = c.take<unsigned>(4);
+  void *scan_tmp = c.take<char>(L.scan_bytes);
+  float4 *bucket = c.take<float4>(L.max_entries);
+
+  PK_CUDA(cudaMemsetAsync(counts, 0, (L.ntiles + 1) * sizeof(unsigned), s));
+  PK_CUDA(cudaMemsetAsync(cursors, 0, L.ntiles * sizeof(unsigned), s));
+  PK_CUDA(cudaMemsetAsync(wmax, 0, 4 * sizeof(unsigned), s));
+  const int threads = 256;
+  const int64_t want = (n + threads - 1) / threads;
+  const int blocks = (int)(want < 64LL * sm_count() ? (want > 0 ? want : 1) : 64LL * sm_count());
+  if (n > 0) {
+    bucket_kernel<false><<<blocks, threads, 0, s>>>(g, positions, weights, n, counts, nullptr,
+                                                    nullptr, nullptr, wmax, d_status);
+    PK_LAUNCH_CHECK();
+  }
+  size_t scan_bytes = L.scan_bytes;
+  PK_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, counts, offsets,
+                                        (int)(L.ntiles + 1), s));
+  if (n > 0) {
+    bucket_kernel<true><<<blocks, threads, 0, s>>>(g, positions, weights, n, nullptr, offsets,
+                                                   cursors, bucket, nullptr, nullptr);
+    PK_LAUNCH_CHECK();
+  }
+  const size_t smem = (size_t)nshifts * TILE_CELLS * sizeof(unsigned long long);
+  PK_CUDA(cudaFuncSetAttribute(paint_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem));
+  paint_tiles_kernel<<<(unsigned)L.ntiles, 256, smem, s>>>(g, bucket, offsets, wmax, n, out);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+extern "C" pk_status pk_read(void *stream, const float *mesh, const float *positions,
+                             const float *weights, int64_t n, const int32_t meshsize[3],
+                             const float boxsize[3], const float boxcenter[3],
+                             const float cellsize[3], int order, float shift, float scale,
+                             float *out, float *grad, int accumulate) {
+  PK_REQUIRE(mesh && (n == 0 || positions), PK_ERR_INVALID, "mesh / positions is NULL");
+  PK_REQUIRE(out || grad, PK_ERR_INVALID, "nothing to write (out and grad NULL)");
+  float shifts[MAX_SHIFTS] = {0.f, 0.f, 0.f, 0.f};
+  PaintGeom g;
+  PK_REQUIRE(fill_geom(meshsize, boxsize, boxcenter, cellsize, order, 1, shifts, &g),
+             PK_ERR_INVALID, "invalid meshsize / order / cellsize");
+  if (n == 0) return PK_OK;
+  const int threads = 256;
+  const int64_t want = (n + threads - 1) / threads;
+  const int blocks = (int)(want < 64LL * sm_count() ? want : 64LL * sm_count());
+  read_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(g, mesh, positions, weights, n,
+                                                            shift, scale, out, grad, accumulate);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}

@@ -1,0 +1,19 @@
+"""jaxpower_b200: B200-native (sm_100a) drop-in for jax-power's mesh power-spectrum path.
+
+Public API mirrors ``jaxpower`` for the single-GPU power-spectrum estimator:
+``MeshAttrs``, ``RealMeshField``, ``ComplexMeshField``, ``ParticleField``, ``FKPField``,
+``get_mesh_attrs``, ``BinMesh2SpectrumPoles``, ``compute_mesh2_spectrum``,
+``compute_fkp2_normalization``, ``compute_fkp2_shotnoise``, ``compute_box2_normalization``
+and the ``resamplers`` namespaces.  All computation runs in the CUDA library
+``libjaxpower_b200.so`` through its C ABI (``include/jaxpower_b200.h``).
+"""
+from . import resamplers
+from .mesh import (MeshAttrs, BaseMeshField, RealMeshField, ComplexMeshField, ParticleField, FKPField,
+                   get_mesh_attrs, next_fft_size, r2c, c2r, apply, read, paint)
+from .mesh2 import (BinMesh2SpectrumPoles, compute_mesh2_spectrum, compute_mesh2, compute_fkp2_normalization,
+                    compute_fkp2_shotnoise, compute_box2_normalization, compute_normalization,
+                    compute_box_normalization)
+from .types import Mesh2SpectrumPole, Mesh2SpectrumPoles
+from ._lib import load as load_library, LIBRARY_PATH
+
+__version__ = '0.1.0'

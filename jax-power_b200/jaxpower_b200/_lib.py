@@ -1,0 +1,122 @@
+"""ctypes binding of the C ABI (``include/jaxpower_b200.h``).
+
+This is the same boundary a ``jax.ffi`` / cgo / JNI caller would bind: plain
+device pointers, sizes and a CUDA stream.  The library must be built
+(``python jax-power_b200/build.py``); there is no CPU fallback — importing a
+compute entry point without the library raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY_PATH = os.path.join(_HERE, 'libjaxpower_b200.so')
+
+PK_BACKEND_JAX = 0
+PK_BACKEND_JAXDECOMP = 1
+
+c_int = ctypes.c_int
+c_int64 = ctypes.c_int64
+c_float = ctypes.c_float
+c_size_t = ctypes.c_size_t
+c_void_p = ctypes.c_void_p
+c_double_p = ctypes.POINTER(ctypes.c_double)
+c_float_p = ctypes.POINTER(ctypes.c_float)
+c_int32_p = ctypes.POINTER(ctypes.c_int32)
+
+# name -> (argtypes); every entry point returns an int status except the two strings
+SIGNATURES = {
+    'pk_paint_workspace_size': [c_int64, c_int32_p, c_int, c_int, ctypes.POINTER(c_size_t)],
+    'pk_paint': [c_void_p, c_void_p, c_void_p, c_int64, c_int32_p, c_float_p, c_float_p, c_float_p,
+                 c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_size_t, c_void_p],
+    'pk_read': [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32_p, c_float_p, c_float_p,
+                c_float_p, c_int, c_float, c_float, c_void_p, c_void_p, c_int],
+    'pk_fft_plan_create': [c_int32_p, c_int, c_int, ctypes.POINTER(c_void_p)],
+    'pk_fft_exec': [c_void_p, c_void_p, c_void_p, c_void_p],
+    'pk_fft_plan_destroy': [c_void_p],
+    'pk_interlace_compensate': [c_void_p, c_void_p, c_int, c_int32_p, c_int, c_int, c_int, c_float,
+                                c_void_p],
+    'pk_scale_real': [c_void_p, c_void_p, c_int64, c_float],
+    'pk_bin_workspace_size': [c_int32_p, c_int, c_int, ctypes.POINTER(c_size_t)],
+    'pk_bin_modes': [c_void_p, c_int32_p, c_float_p, c_void_p, c_int, c_float, c_int, c_void_p,
+                     c_void_p, c_void_p, c_size_t],
+    'pk_bin_mesh': [c_void_p, c_void_p, c_int32_p, c_float_p, c_void_p, c_int, c_float, c_int, c_int,
+                    c_void_p, c_void_p, c_size_t],
+    'pk_bin_global': [c_void_p, c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_void_p,
+                      c_int, c_float, c_int, c_int, c_int32_p, c_void_p, c_void_p, c_size_t],
+    'pk_bin_firstpoint': [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int32_p, c_int32_p,
+                          c_int32_p, c_float_p, c_void_p, c_int, c_float, c_int, c_int, c_int32_p,
+                          c_int, c_int, c_void_p, c_void_p, c_size_t],
+    'pk_ylm_premultiply': [c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_int, c_int32_p,
+                           c_int32_p, c_void_p],
+}
+
+_lib = None
+
+
+class PKError(RuntimeError):
+    """Error status returned by the CUDA library."""
+
+
+def load():
+    """Load the library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBRARY_PATH):
+        raise ImportError('jaxpower_b200 CUDA library not found at {}; build it with '
+                          '`python jax-power_b200/build.py` (there is no CPU fallback)'.format(LIBRARY_PATH))
+    lib = ctypes.CDLL(LIBRARY_PATH)
+    lib.pk_version.restype = ctypes.c_char_p
+    lib.pk_version.argtypes = []
+    lib.pk_last_error.restype = ctypes.c_char_p
+    lib.pk_last_error.argtypes = []
+    for name, argtypes in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = argtypes
+        fn.restype = c_int
+    _lib = lib
+    return lib
+
+
+def call(name, *args):
+    """Call an entry point; raise PKError with the library's message on failure.
+
+    Inside a ``tracing.Timeline`` the call is bracketed by CUDA events.
+    """
+    lib = load()
+    from .tracing import active
+    timeline = active()
+    token = timeline.start(name) if timeline is not None else None
+    status = getattr(lib, name)(*args)
+    if token is not None:
+        timeline.stop(token)
+    if status != 0:
+        msg = lib.pk_last_error().decode()
+        raise PKError('{} failed (status {}): {}'.format(name, status, msg))
+    return status
+
+
+def i32(values):
+    arr = (ctypes.c_int32 * len(values))(*[int(v) for v in values])
+    return arr
+
+
+def f32(values):
+    arr = (ctypes.c_float * len(values))(*[float(np.float32(v)) for v in values])
+    return arr
+
+
+def ptr(tensor):
+    """Device pointer of a torch tensor (None -> NULL)."""
+    if tensor is None:
+        return None
+    return ctypes.c_void_p(tensor.data_ptr())
+
+
+def stream_handle(stream=None):
+    import torch
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)

@@ -1,0 +1,353 @@
+"""Power-spectrum binning and estimators (host side of the CUDA library).
+
+Mirrors ``jaxpower/mesh2.py``:
+
+- ``BinMesh2SpectrumPoles`` (``mesh2.py:25-119``): k edges (``np.arange(0, k_Nyq, step)``
+  in float64, compared in float32), nmodes and xavg computed on the GPU by
+  ``pk_bin_modes``; the per-mode bin index is never materialised;
+- ``compute_mesh2_spectrum`` (``mesh2.py:253-374``): global line of sight through
+  ``pk_bin_global``; first-point / endpoint through ``pk_ylm_premultiply`` +
+  batched cuFFT R2C + ``pk_bin_firstpoint`` (sum over m done inside the binning
+  pass: bin is linear, so sum_m bin(.) = bin(sum_m .));
+- ``compute_fkp2_normalization`` / ``compute_fkp2_shotnoise`` /
+  ``compute_box2_normalization`` (``mesh2.py:508-621``).
+"""
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from .mesh import (MeshAttrs, BaseMeshField, RealMeshField, ComplexMeshField, ParticleField, FKPField,
+                   _r2c, _c2r, _workspace, _device, _paint, get_mesh_attrs)
+from .types import Mesh2SpectrumPole, Mesh2SpectrumPoles
+
+__all__ = ['BinMesh2SpectrumPoles', 'compute_mesh2_spectrum', 'compute_mesh2', 'compute_fkp2_normalization',
+           'compute_fkp2_shotnoise', 'compute_box2_normalization', 'compute_normalization',
+           'compute_box_normalization']
+
+
+def _format_ells(ells):
+    if np.ndim(ells) == 0:
+        ells = (ells,)
+    return tuple(sorted(int(e) for e in ells))
+
+
+def _uniform_step(edges):
+    if len(edges) < 2:
+        return 0.
+    d = np.diff(edges)
+    if np.all(d > 0) and np.max(np.abs(d - d.mean())) <= 1e-3 * d.mean():
+        return float(d.mean())
+    return 0.
+
+
+class BinMesh2SpectrumPoles:
+    """Binning operator for mesh to power spectrum (``mesh2.py:67-119``).
+
+    Parameters
+    ----------
+    mattrs : MeshAttrs or mesh field
+    edges : array, dict ('min', 'max', 'step') or None
+    ells : int or tuple
+    mode_oversampling : only 0 is supported
+    """
+
+    def __init__(self, mattrs, edges=None, ells=0, mode_oversampling=0):
+        if not isinstance(mattrs, MeshAttrs):
+            mattrs = mattrs.attrs
+        if mode_oversampling:
+            raise NotImplementedError('mode_oversampling > 0 is not supported on the GPU path')
+        self.mattrs = mattrs
+        self.ells = _format_ells(ells)
+        vec0 = np.float32(mattrs.kfun.min())
+        if edges is None:
+            edges = {}
+        if isinstance(edges, dict):
+            step = edges.get('step', None)
+            vecmax = np.float32(np.float32(vec0 * np.float32(np.min(mattrs.meshsize))) / np.float32(2.))
+            if step is None:
+                edges = self._find_unique_edges(vec0, edges.get('min', 0.), edges.get('max', np.inf))
+            else:
+                edges = np.arange(edges.get('min', 0.), edges.get('max', float(vecmax)), step)
+        edges = np.asarray(edges, dtype='f8')
+        if edges.ndim == 2:
+            edges = np.append(edges[:, 0], edges[-1, 1])
+        self._edges1d = edges
+        self.edges = np.column_stack([edges[:-1], edges[1:]])
+        self._step = _uniform_step(edges.astype('f4'))
+        self.d_edges = torch.as_tensor(edges.astype('f4'), device=_device())
+        nbins = len(edges) - 1
+        nmodes = torch.empty(nbins, dtype=torch.float64, device=_device())
+        ksum = torch.empty(nbins, dtype=torch.float64, device=_device())
+        ws = self._workspace()
+        _lib.call('pk_bin_modes', _lib.stream_handle(), _lib.i32(mattrs.meshsize), _lib.f32(mattrs.kfun),
+                  _lib.ptr(self.d_edges), len(edges), self._step, mattrs.backend_code, _lib.ptr(nmodes),
+                  _lib.ptr(ksum), _lib.ptr(ws), ws.numel())
+        self.nmodes = nmodes.cpu().numpy()
+        with np.errstate(invalid='ignore', divide='ignore'):
+            self.xavg = ksum.cpu().numpy() / self.nmodes
+
+    def _workspace(self):
+        nbytes = _lib.c_size_t()
+        _lib.call('pk_bin_workspace_size', _lib.i32(self.mattrs.meshsize), len(self._edges1d), 9,
+                  _lib.ctypes.byref(nbytes))
+        return _workspace(nbytes.value)
+
+    def _find_unique_edges(self, x0, xmin=0., xmax=np.inf):
+        """``_find_unique_edges`` (``mesh.py:2789-2811``): mid-points between unique |k|."""
+        kx, ky, kz = self.mattrs.kcoords(sparse=True)
+        x2 = ((kx * kx + ky * ky) + kz * kz).reshape(-1)
+        x2 = x2[(x2 >= xmin**2) & (x2 <= xmax**2)]
+        key = (x2.double() / (0.5 * float(x0))**2 + 0.5).to(torch.int64)
+        _, inverse = torch.unique(key, return_inverse=True)
+        first = torch.full((int(inverse.max()) + 1,), x2.numel(), dtype=torch.int64, device=x2.device)
+        first.scatter_reduce_(0, inverse, torch.arange(x2.numel(), device=x2.device), reduce='amin')
+        x = torch.sqrt(x2[first]).cpu().numpy().astype('f8')
+        tmp = (x[:-1] + x[1:]) / 2.
+        return np.concatenate([[tmp[0] - (x[1] - x[0])], tmp, [tmp[-1] + (x[-1] - x[-2])]])
+
+    @property
+    def nbins(self):
+        return len(self._edges1d) - 1
+
+    @property
+    def wmodes(self):
+        kz = self.mattrs.kcoords(sparse=True)[2]
+        n2 = int(self.mattrs.meshsize[2])
+        if self.mattrs.fft_backend == 'jax':
+            w = 1 + (kz > 0).to(torch.int32)
+        else:
+            z = torch.arange(kz.numel(), device=kz.device).reshape(kz.shape)
+            w = 2 - ((z == 0) | ((n2 % 2 == 0) & (z == n2 // 2))).to(torch.int32)
+        return w.expand(tuple(self.mattrs.meshsize[:2]) + (n2 // 2 + 1,))
+
+    def __call__(self, mesh, remove_zero=False):
+        """Per-bin mean of a complex mesh with Hermitian weights (``mesh2.py:100-119``)."""
+        value = mesh.value if isinstance(mesh, BaseMeshField) else mesh
+        if not isinstance(value, torch.Tensor):
+            value = torch.as_tensor(np.asarray(value))
+        value = value.to(device=_device(), dtype=torch.complex64).contiguous()
+        out = torch.empty(2 * self.nbins, dtype=torch.float64, device=value.device)
+        ws = self._workspace()
+        _lib.call('pk_bin_mesh', _lib.stream_handle(), _lib.ptr(value), _lib.i32(self.mattrs.meshsize),
+                  _lib.f32(self.mattrs.kfun), _lib.ptr(self.d_edges), len(self._edges1d), self._step,
+                  self.mattrs.backend_code, int(bool(remove_zero)), _lib.ptr(out), _lib.ptr(ws), ws.numel())
+        out = out.cpu().numpy()
+        return (out[:self.nbins] + 1j * out[self.nbins:]) / self.nmodes
+
+
+def _format_meshes(*meshes, fields=None):
+    if len(meshes) == 1 and isinstance(meshes[0], (tuple, list)):
+        meshes = tuple(meshes[0])
+    meshes = list(meshes)
+    assert 1 <= len(meshes) <= 2
+    if fields is None:
+        fields = [0]
+    else:
+        fields = list(fields)
+    meshes = meshes + [None] * (2 - len(meshes))
+    for mesh in meshes[len(fields):]:
+        fields.append(fields[-1] if mesh is None else fields[-1] + 1)
+    for i, (mesh, field) in enumerate(zip(meshes, fields)):
+        if mesh is None:
+            meshes[i] = meshes[fields.index(field)]
+    return meshes, tuple(fields)
+
+
+def _2c(mesh):
+    return mesh if isinstance(mesh, ComplexMeshField) else mesh.r2c()
+
+
+def _2r(mesh):
+    return mesh if isinstance(mesh, RealMeshField) else mesh.c2r()
+
+
+def _los(los):
+    if isinstance(los, str) and los in ('firstpoint', 'local', 'endpoint'):
+        return ('firstpoint' if los == 'local' else los), None, los == 'endpoint'
+    if isinstance(los, str):
+        vlos = np.zeros(3)
+        vlos['xyz'.index(los)] = 1.
+    else:
+        vlos = np.asarray(los, dtype='f8')
+    return los, vlos, False
+
+
+def _firstpoint_terms(ells):
+    return [(ell, m) for ell in ells if ell > 0 for m in range(-ell, ell + 1)]
+
+
+def _term_batch(mattrs, nterms):
+    """How many (ell, m) terms to transform at once, given free device memory."""
+    nr = int(np.prod(mattrs.meshsize))
+    nc = int(mattrs.meshsize[0]) * int(mattrs.meshsize[1]) * (int(mattrs.meshsize[2]) // 2 + 1)
+    per_term = 4 * nr + 8 * nc
+    free, _ = torch.cuda.mem_get_info()
+    return int(max(1, min(nterms, 32, (0.4 * free) // per_term)))
+
+
+def compute_mesh2_spectrum(*meshes, bin=None, los='z'):
+    """Power-spectrum multipoles from mesh(es) (``mesh2.py:253-374``)."""
+    meshes, fields = _format_meshes(*meshes)
+    mattrs = meshes[0].attrs
+    meshsize = mattrs.meshsize
+    norm_value = np.float32(np.prod(meshsize.astype('f4'))) / np.float32(np.prod(mattrs.cellsize))
+    los, vlos, swap = _los(los)
+    attrs = dict(los=vlos if vlos is not None else los)
+    ells = bin.ells
+    nbins = bin.nbins
+    ws = bin._workspace()
+    stream = _lib.stream_handle()
+    raw = torch.zeros(len(ells) * nbins, dtype=torch.float64, device=_device())
+    if vlos is None:
+        if swap:
+            meshes = meshes[::-1]
+        rmesh1 = meshes[0]
+        auto = fields[1] == fields[0]
+        A0 = _2c(rmesh1 if auto else meshes[1]).value.contiguous()
+        B0 = None if auto else _2c(rmesh1).value.contiguous()
+        terms = _firstpoint_terms(ells)
+        if not terms:
+            _lib.call('pk_bin_firstpoint', stream, _lib.ptr(A0), _lib.ptr(B0), None, 0, None, None,
+                      _lib.i32(meshsize), _lib.f32(mattrs.kfun), _lib.ptr(bin.d_edges), len(bin._edges1d),
+                      bin._step, mattrs.backend_code, len(ells), _lib.i32(ells), 1, 1, _lib.ptr(raw),
+                      _lib.ptr(ws), ws.numel())
+        if terms:
+            rho = _2r(rmesh1).value.contiguous()
+            offset = (mattrs.boxcenter - (mattrs.boxsize / np.float32(2.)).astype('f4')).astype('f4')
+            batch = _term_batch(mattrs, len(terms))
+            real = torch.empty((batch,) + tuple(int(n) for n in meshsize), dtype=torch.float32, device=rho.device)
+            for start in range(0, len(terms), batch):
+                chunk = terms[start:start + batch]
+                nt = len(chunk)
+                t_ell, t_m = [t[0] for t in chunk], [t[1] for t in chunk]
+                _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rho), _lib.i32(meshsize), _lib.f32(mattrs.cellsize),
+                          _lib.f32(offset), nt, _lib.i32(t_ell), _lib.i32(t_m), _lib.ptr(real))
+                F = _r2c(real[:nt], meshsize)
+                include_ell0 = int(start == 0 and 0 in ells)  # ell = 0 rides on the first batch
+                _lib.call('pk_bin_firstpoint', stream, _lib.ptr(A0), _lib.ptr(B0), _lib.ptr(F), nt, _lib.i32(t_ell),
+                          _lib.i32(t_m), _lib.i32(meshsize), _lib.f32(mattrs.kfun), _lib.ptr(bin.d_edges),
+                          len(bin._edges1d), bin._step, mattrs.backend_code, len(ells), _lib.i32(ells),
+                          include_ell0, 1, _lib.ptr(raw), _lib.ptr(ws), ws.numel())
+                del F
+        raw = raw.cpu().numpy().reshape(len(ells), nbins)
+        num = [raw[i] / bin.nmodes * (1. if ell == 0 else 4. * np.pi) for i, ell in enumerate(ells)]
+        if swap:  # conj: odd multipoles (imaginary parts) change sign
+            num = [-n if ell % 2 else n for ell, n in zip(ells, num)]
+    else:
+        auto = fields[1] == fields[0]
+        d1 = _2c(meshes[0]).value.contiguous()
+        d2 = None if auto else _2c(meshes[1]).value.contiguous()
+        _lib.call('pk_bin_global', stream, _lib.ptr(d1), _lib.ptr(d2), _lib.i32(meshsize), _lib.f32(mattrs.kfun),
+                  _lib.f32(vlos), _lib.ptr(bin.d_edges), len(bin._edges1d), bin._step, mattrs.backend_code,
+                  len(ells), _lib.i32(ells), _lib.ptr(raw), _lib.ptr(ws), ws.numel())
+        raw = raw.cpu().numpy().reshape(len(ells), nbins)
+        num = [raw[i] / bin.nmodes * (2 * ell + 1) for i, ell in enumerate(ells)]
+    norm = np.full(nbins, norm_value, dtype='f8')
+    poles = [Mesh2SpectrumPole(k=bin.xavg, k_edges=bin.edges, nmodes=bin.nmodes, num_raw=num[i],
+                               num_shotnoise=np.zeros(nbins), norm=norm,
+                               volume=float(np.prod(mattrs.kfun.astype('f8'))) * bin.nmodes, ell=ell, attrs=attrs)
+             for i, ell in enumerate(ells)]
+    return Mesh2SpectrumPoles(poles)
+
+
+def compute_mesh2(*meshes, bin=None, los='z'):
+    if isinstance(bin, BinMesh2SpectrumPoles):
+        return compute_mesh2_spectrum(*meshes, bin=bin, los=los)
+    raise NotImplementedError('only BinMesh2SpectrumPoles is supported')
+
+
+# ---------------------------------------------------------------------- normalisation
+
+def _norm_attrs(mattrs, cellsize):
+    """``get_halo_for_new_mattrs(mattrs, cellsize=...)`` without sharding (``mesh.py:3002-3039``)."""
+    cs = np.broadcast_to(np.asarray(cellsize, 'f4'), (3,))
+    meshsize = np.ceil((mattrs.boxsize / cs).astype('f4')).astype('i4')
+    boxsize = (meshsize * cs.astype('f8')).astype('f4')
+    if np.any((meshsize - mattrs.meshsize) % 2):
+        cell = (boxsize / meshsize.astype('f4')).astype('f4')
+        meshsize = meshsize + 1
+        boxsize = (cell * meshsize.astype('f4')).astype('f4')
+    return MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=mattrs.boxcenter, fft_backend=mattrs.fft_backend)
+
+
+def _iter_meshes(*inputs, resampler='cic', interlacing=0, compensate=False, **kwargs):
+    attrs = {k: v for k, v in kwargs.items() if v is not None}
+    for inp in inputs:
+        if isinstance(inp, RealMeshField):
+            yield inp
+            continue
+        mattrs = inp.attrs
+        if 'cellsize' in attrs:
+            mattrs = _norm_attrs(mattrs, attrs['cellsize'])
+        elif attrs:
+            mattrs = mattrs.clone(**attrs)
+        yield _paint(mattrs, inp.positions, inp._weights, resampler=resampler, interlacing=interlacing,
+                     compensate=compensate, out='real')
+
+
+def compute_normalization(*inputs, resampler='cic', start=1., **kwargs):
+    """sum(prod meshes) * cell volume^(1 - n) (``mesh.py:3092-3118``), accumulated in float64."""
+    product = None
+    cellsize = None
+    for mesh in _iter_meshes(*inputs, resampler=resampler, **kwargs):
+        v = mesh.value.double()
+        product = v if product is None else product * v
+        cellsize = mesh.attrs.cellsize
+    return float(start) * float(product.sum()) * float(np.prod(cellsize.astype('f8')))**(1 - len(inputs))
+
+
+def compute_box_normalization(*inputs):
+    mattrs = inputs[0].attrs
+    size = float(np.prod(mattrs.meshsize.astype('f8')))
+    normalization = 1.
+    for mesh in inputs:
+        normalization *= float(mesh.sum()) / size
+    return normalization * size * float(np.prod(mattrs.cellsize.astype('f8')))**(1 - len(inputs))
+
+
+def compute_box2_normalization(*inputs, bin=None):
+    meshes = _format_meshes(*inputs)[0]
+    norm = compute_box_normalization(*meshes)
+    if bin is not None:
+        return [norm] * len(bin.ells)
+    return norm
+
+
+def compute_fkp2_normalization(*fkps, bin=None, cellsize=10., split=None, fields=None, **kwargs):
+    """FKP normalisation (``mesh2.py:516-574``): alpha * sum(rho_d rho_r) / V_cell, CIC at ``cellsize``."""
+    if split is not None:
+        raise NotImplementedError('split normalisation (random subsampling) is not supported')
+    kwargs.update(cellsize=cellsize)
+    fkps, fields = _format_meshes(*fkps)
+    if fields[1] == fields[0]:
+        fkp = fkps[0]
+        alpha = float(fkp.data.sum()) / float(fkp.randoms.sum())
+        norm = alpha * compute_normalization(fkp.data, fkp.randoms, **kwargs)
+    else:
+        alpha2 = float(fkps[1].data.sum()) / float(fkps[1].randoms.sum())
+        norm = alpha2 * compute_normalization(fkps[0].data, fkps[1].randoms, **kwargs)
+        alpha2 = float(fkps[0].data.sum()) / float(fkps[0].randoms.sum())
+        norm += alpha2 * compute_normalization(fkps[1].data, fkps[0].randoms, **kwargs)
+        norm = norm / 2
+    if bin is not None:
+        return [norm] * len(bin.ells)
+    return norm
+
+
+def compute_fkp2_shotnoise(*fkps, bin=None, fields=None):
+    """FKP shot noise (``mesh2.py:577-621``): sum of w1 w2 for the same positions, else 0."""
+    fkps, fields = _format_meshes(*fkps, fields=fields)
+
+    def particles(f):
+        return f.particles if isinstance(f, FKPField) else f
+
+    if fields[1] == fields[0]:
+        p = [particles(f) for f in fkps]
+        shotnoise = float((p[0].weights.double() * p[1].weights.double()).sum())
+    else:
+        shotnoise = 0.
+    if bin is not None:
+        return [shotnoise * (ell == 0) * np.ones(bin.nbins) for ell in bin.ells]
+    return shotnoise

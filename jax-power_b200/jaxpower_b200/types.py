@@ -1,0 +1,94 @@
+"""Power-spectrum result containers (the layout of lsstypes' ``Mesh2SpectrumPole(s)``).
+
+jax-power returns lsstypes objects (``types.py:93-94``); lsstypes is an external,
+unpinned dependency.  This module keeps the fields the estimator fills
+(``mesh2.py:341-344, 371-374``) — ``k``, ``k_edges``, ``nmodes``, ``num_raw``,
+``num_shotnoise``, ``norm``, ``volume``, ``ell``, ``attrs`` — and the methods the
+reference's tests use: ``value()`` = (num_raw - num_shotnoise) / norm (the
+normalisation that reproduces the reference's golden ``value().std()``),
+``clone(norm=..., num_shotnoise=...)``, ``get(ells=...)``, ``values(name)``,
+``coords('k')``, ``ells``.  Arrays are NumPy float64 on the host.
+"""
+import numpy as np
+
+__all__ = ['Mesh2SpectrumPole', 'Mesh2SpectrumPoles']
+
+
+class Mesh2SpectrumPole:
+
+    _fields = ('k', 'k_edges', 'nmodes', 'num_raw', 'num_shotnoise', 'norm', 'volume')
+
+    def __init__(self, k, k_edges, nmodes, num_raw, num_shotnoise=None, norm=None, volume=None, ell=0,
+                 attrs=None):
+        self.k = np.asarray(k, dtype='f8')
+        self.k_edges = np.asarray(k_edges, dtype='f8')
+        self.nmodes = np.asarray(nmodes, dtype='f8')
+        self.num_raw = np.asarray(num_raw)
+        self.num_shotnoise = np.zeros_like(self.num_raw) if num_shotnoise is None else \
+            np.broadcast_to(np.asarray(num_shotnoise), self.num_raw.shape).copy()
+        self.norm = np.ones_like(self.num_raw, dtype='f8') if norm is None else \
+            np.broadcast_to(np.asarray(norm, dtype='f8'), self.num_raw.shape).copy()
+        self.volume = volume
+        self.ell = int(ell)
+        self.attrs = dict(attrs or {})
+
+    def value(self):
+        return (self.num_raw - self.num_shotnoise) / self.norm
+
+    def coords(self, name='k'):
+        return getattr(self, name)
+
+    def values(self, name='value'):
+        if name == 'value':
+            return self.value()
+        if name == 'shotnoise':
+            return self.num_shotnoise / self.norm
+        return getattr(self, name)
+
+    def clone(self, **kwargs):
+        state = {name: getattr(self, name) for name in self._fields}
+        state.update(ell=self.ell, attrs=self.attrs)
+        state.update(kwargs)
+        return self.__class__(**state)
+
+    def __repr__(self):
+        return 'Mesh2SpectrumPole(ell={}, nbins={})'.format(self.ell, self.k.size)
+
+
+class Mesh2SpectrumPoles:
+
+    def __init__(self, poles):
+        self.poles = list(poles)
+
+    @property
+    def ells(self):
+        return tuple(p.ell for p in self.poles)
+
+    def __iter__(self):
+        return iter(self.poles)
+
+    def __len__(self):
+        return len(self.poles)
+
+    def get(self, ells=None, ell=None):
+        if ells is None:
+            ells = ell
+        if ells is None:
+            return self
+        if np.ndim(ells) == 0:
+            return self.poles[self.ells.index(int(ells))]
+        return Mesh2SpectrumPoles([self.poles[self.ells.index(int(e))] for e in ells])
+
+    def value(self):
+        return np.concatenate([p.value() for p in self.poles])
+
+    def clone(self, **kwargs):
+        """Per-pole update; list values (one per ell) are dispatched, scalars broadcast."""
+        poles = []
+        for i, p in enumerate(self.poles):
+            kw = {k: (v[i] if isinstance(v, (list, tuple)) else v) for k, v in kwargs.items()}
+            poles.append(p.clone(**kw))
+        return Mesh2SpectrumPoles(poles)
+
+    def __repr__(self):
+        return 'Mesh2SpectrumPoles(ells={})'.format(self.ells)

@@ -76,13 +76,29 @@ def cell_index(u, order, shape):
     return base_index(u, order) % np.asarray(shape, dtype='i8')
 
 
-def paint_mesh(shape, u, weights, order, dtype=np.float32):
+def paint_mesh(shape, u, weights, order, dtype=np.float32, accum=None):
     """``resamplers.paint`` (``resamplers.py:66-97``) onto a zero mesh of ``shape``.
 
     ``u``: (N, 3) positions in cell units (already normalised), ``weights``: (N,).
     float32: serial ``np.add.at`` in particle order for each offset (reference order).
     float64: same kernels in float64, accumulated with ``np.bincount``.
+    ``accum='f64'`` with float32: the reference's float32 contributions ``w * ker``
+    summed in float64 and rounded once to float32 (an order-independent sum).
     """
+    if accum == 'f64' and np.dtype(dtype) == np.float32:
+        shape = tuple(int(s) for s in shape)
+        u = np.asarray(u, dtype=np.float32)
+        w = np.asarray(weights, dtype=np.float32)
+        nshape = np.asarray(shape, dtype='i8')
+        id0 = base_index(u, order)
+        acc = np.zeros(int(np.prod(shape)), dtype='f8')
+        strides = np.array([shape[1] * shape[2], shape[2], 1], dtype='i8')
+        for ishift in stencil(order):
+            idx = id0 + ishift
+            k = kernel(order, np.abs(idx.astype(np.float32) - u), np.float32)
+            val = (w * ((k[:, 0] * k[:, 1]) * k[:, 2])).astype(np.float32)
+            acc += np.bincount((idx % nshape) @ strides, weights=val.astype('f8'), minlength=acc.size)
+        return acc.astype(np.float32).reshape(shape)
     dtype = np.dtype(dtype)
     shape = tuple(int(s) for s in shape)
     u = np.asarray(u, dtype=dtype)

@@ -1,0 +1,160 @@
+"""Paint / read parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+The oracle restates ``resamplers.py:57-125`` and ``mesh.py:2673-2754`` in the
+reference's float32 operation order.  Cell assignment must be bit-exact; mesh
+values agree to float32 rounding of the (order-dependent) cell sums.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle.coords import Geometry
+from oracle import paint as opaint
+
+pytestmark = pytest.mark.gpu
+
+RESAMPLERS = {'ngp': 1, 'cic': 2, 'tsc': 3, 'pcs': 4}
+
+
+def _jp():
+    import jaxpower_b200 as jp
+    return jp
+
+
+def _catalog(n, boxsize, boxcenter, seed=0):
+    rng = np.random.default_rng(seed)
+    pos = (rng.uniform(-0.5, 0.5, (n, 3)) * np.asarray(boxsize) + np.asarray(boxcenter)).astype('f4')
+    w = rng.uniform(0.5, 1.5, n).astype('f4')
+    return pos, w
+
+
+@pytest.mark.parametrize('meshsize', [(16, 16, 16), (17, 12, 10), (4, 4, 4), (32, 40, 36)])
+@pytest.mark.parametrize('resampler', list(RESAMPLERS))
+def test_paint_shifts_match_oracle(meshsize, resampler):
+    jp = _jp()
+    from jaxpower_b200.mesh import _paint_shifts
+    boxsize, boxcenter = np.array([100., 120., 90.]), np.array([3., -5., 10.])
+    pos, w = _catalog(5000, 1.2 * boxsize, boxcenter, seed=1)  # some particles outside: periodic wrap
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=boxcenter)
+    order = RESAMPLERS[resampler]
+    interlacing = 3
+    meshes, status = _paint_shifts(attrs, torch.as_tensor(pos).cuda(), torch.as_tensor(w).cuda(), order, interlacing)
+    assert int(status.item()) == 0
+    geom = Geometry(meshsize, boxsize, boxcenter)
+    u = opaint.normalize_positions(geom, pos)
+    for s, shift in enumerate(opaint.interlacing_shifts(interlacing, np.float32)):
+        us = (u + shift).astype('f4')
+        got = meshes[s].cpu().numpy()
+        # the GPU sums the reference's float32 contributions in 64-bit fixed point (resolution
+        # n max|w| 2^-62 per contribution) and rounds once: equal to the float64-accumulated
+        # oracle up to one float32 ulp plus that resolution
+        exact = opaint.paint_mesh(geom.rshape, us, w, order, accum='f64')
+        fixed = 5000 * 1.5 * 2.**-62 * 64
+        assert np.all(np.abs(got - exact) <= np.spacing(np.abs(exact)) + fixed), s
+        # and to the reference's serial float32 order within its accumulated rounding
+        serial = opaint.paint_mesh(geom.rshape, us, w, order)
+        percell = 5000. * order**3 / np.prod(meshsize)
+        scale = np.abs(serial).max()
+        assert np.allclose(got, serial, rtol=0, atol=2e-7 * max(1., np.sqrt(percell)) * scale), s
+        assert np.isclose(got.sum(dtype='f8'), w.sum(dtype='f8'), rtol=1e-6)
+
+
+@pytest.mark.parametrize('resampler', list(RESAMPLERS))
+def test_cell_assignment_bit_exact(resampler):
+    """Dyadic positions on cell edges, half-cell ties (round half to even), box edges and
+    outside the box, small-integer weights: the mesh must be bit-identical to the oracle's
+    (float32 contributions summed exactly, rounded once), which needs every particle in
+    exactly the reference's cells."""
+    jp = _jp()
+    from jaxpower_b200.mesh import _paint_shifts
+    n = 16
+    boxsize, boxcenter = 32., 0.  # cellsize 2
+    ticks = np.arange(-40, 40) * 0.5  # multiples of a quarter cell, beyond the box on both sides
+    rng = np.random.default_rng(3)
+    pos = rng.choice(ticks, size=(4000, 3)).astype('f4')
+    pos[:8] = [[-16., -16., -16.], [16., 16., 16.], [15., -15., 1.], [-1., 1., 3.],
+               [0., 0., 0.], [31., -31., 15.5], [-16.5, 16.5, 0.5], [1.5, 2.5, 3.5]]
+    w = rng.integers(1, 4, size=4000).astype('f4')
+    attrs = jp.MeshAttrs(meshsize=n, boxsize=boxsize, boxcenter=boxcenter)
+    order = RESAMPLERS[resampler]
+    meshes, _ = _paint_shifts(attrs, torch.as_tensor(pos).cuda(), torch.as_tensor(w).cuda(), order, 2)
+    geom = Geometry(n, boxsize, boxcenter)
+    u = opaint.normalize_positions(geom, pos)
+    for s, shift in enumerate(opaint.interlacing_shifts(2, np.float32)):
+        ref = opaint.paint_mesh(geom.rshape, (u + shift).astype('f4'), w, order, accum='f64')
+        assert np.array_equal(meshes[s].cpu().numpy(), ref), s
+
+
+@pytest.mark.parametrize('resampler', ['cic', 'tsc', 'pcs'])
+@pytest.mark.parametrize('interlacing', [0, 2, 3, 5])
+@pytest.mark.parametrize('compensate', [False, True])
+@pytest.mark.parametrize('out', ['real', 'complex'])
+def test_particle_paint_pipeline(resampler, interlacing, compensate, out):
+    jp = _jp()
+    meshsize, boxsize, boxcenter = (32, 24, 20), np.array([500., 400., 300.]), np.array([0., 10., 20.])
+    pos, w = _catalog(20000, boxsize, boxcenter, seed=2)
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=boxcenter)
+    mesh = jp.ParticleField(pos, w, attrs=attrs).paint(resampler=resampler, interlacing=interlacing,
+                                                       compensate=compensate, out=out)
+    geom = Geometry(meshsize, boxsize, boxcenter)
+    ref = opaint.paint(geom, pos, w, resampler, interlacing, compensate, out)
+    got = mesh.value.cpu().numpy()
+    assert got.shape == ref.shape
+    scale = np.abs(ref).max()
+    assert np.allclose(got, ref, rtol=0, atol=2e-5 * scale), np.abs(got - ref).max() / scale
+    if out == 'real':  # mass conservation (tests/test_mesh.py:231)
+        assert np.isclose(got.sum(dtype='f8'), w.sum(dtype='f8'), rtol=1e-5)
+
+
+@pytest.mark.parametrize('backend', ['jax', 'jaxdecomp'])
+def test_paint_backends_real(backend):
+    jp = _jp()
+    meshsize, boxsize = 32, 200.
+    pos, w = _catalog(30000, [boxsize] * 3, [0.] * 3, seed=5)
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, fft_backend=backend)
+    mesh = jp.ParticleField(pos, w, attrs=attrs).paint(resampler='tsc', interlacing=3, compensate=True)
+    geom = Geometry(meshsize, boxsize, 0., backend=backend)
+    ref = opaint.paint(geom, pos, w, 'tsc', 3, True, 'real')
+    scale = np.abs(ref).max()
+    assert np.allclose(mesh.value.cpu().numpy(), ref, rtol=0, atol=2e-5 * scale)
+
+
+@pytest.mark.parametrize('resampler', list(RESAMPLERS))
+def test_read_matches_oracle(resampler):
+    jp = _jp()
+    meshsize, boxsize = (16, 20, 12), np.array([50., 60., 40.])
+    rng = np.random.default_rng(7)
+    value = rng.normal(size=meshsize).astype('f4')
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize)
+    mesh = jp.RealMeshField(torch.as_tensor(value).cuda(), attrs=attrs)
+    pos, _ = _catalog(3000, 1.1 * boxsize, [0.] * 3, seed=8)
+    got = mesh.read(pos, resampler=resampler).cpu().numpy()
+    geom = Geometry(meshsize, boxsize, 0.)
+    ref = opaint.read_mesh(value, opaint.normalize_positions(geom, pos), RESAMPLERS[resampler])
+    assert np.allclose(got, ref, rtol=1e-5, atol=1e-5)
+
+
+def test_paint_deterministic():
+    jp = _jp()
+    pos, w = _catalog(200000, [1000.] * 3, [0.] * 3, seed=11)
+    attrs = jp.MeshAttrs(meshsize=64, boxsize=1000.)
+    p = jp.ParticleField(pos, w, attrs=attrs)
+    a = p.paint(resampler='tsc', interlacing=3, compensate=True, out='complex').value
+    b = p.paint(resampler='tsc', interlacing=3, compensate=True, out='complex').value
+    assert torch.equal(a, b)
+    # particle order does not change the mesh (fixed-point accumulation)
+    perm = np.random.default_rng(0).permutation(len(pos))
+    c = jp.ParticleField(pos[perm], w[perm], attrs=attrs).paint(resampler='tsc', interlacing=3, compensate=True,
+                                                                out='complex').value
+    assert torch.equal(a, c)
+
+
+def test_paint_empty_and_status():
+    jp = _jp()
+    attrs = jp.MeshAttrs(meshsize=8, boxsize=10.)
+    mesh = jp.ParticleField(np.zeros((0, 3), 'f4'), attrs=attrs).paint(resampler='cic')
+    assert float(mesh.value.abs().sum()) == 0.
+    pos = np.array([[0., 0., 0.], [np.nan, 0., 0.], [1., 1., 1.]], dtype='f4')
+    with pytest.raises(ValueError):
+        from jaxpower_b200.mesh import _paint
+        _paint(attrs, pos, None, resampler='cic', check=True)

@@ -1,0 +1,169 @@
+"""Binning and estimator parity: CUDA path vs the CPU oracle, and the reference goldens.
+
+Bin membership (|k| in float32, jnp.digitize against float32 edges) must be
+bit-exact: nmodes and index sums per bin match exactly.  P_ell must agree with
+the oracle's float64 accumulation of the same float32 per-mode products within
+1e-5 relative, measured against max |P_0|.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle.coords import Geometry, kcoords
+from oracle import paint as opaint
+from oracle.spectrum import Bins, compute_mesh2_spectrum as ospectrum, fkp_particles, fkp2_normalization
+from tests.golden.catalogs import paint_jit_positions, uniform_particles
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), 'golden', 'reference_goldens.json')))
+RTOL = 1e-5
+# The goldens were computed with x64 on; the reference's own float32 arithmetic (x64 off,
+# its default) reproduced by the oracle misses them by up to 1.3e-5 (test_ref 'x').  The
+# GPU path is float32, so it is held to 3e-5 of the x64 golden and to 2e-6 of the
+# float32 oracle.
+GOLDEN_F32_RTOL = 3e-5
+
+
+def _jp():
+    import jaxpower_b200 as jp
+    return jp
+
+
+@pytest.mark.parametrize('meshsize,boxsize,step', [((64, 64, 64), 1000., 0.01), ((32, 24, 20), (300., 250., 200.), 0.02),
+                                                   ((33, 17, 15), 100., 0.05), ((128, 128, 128), 1000., 0.005)])
+@pytest.mark.parametrize('backend', ['jax', 'jaxdecomp'])
+def test_bin_modes_exact(meshsize, boxsize, step, backend):
+    jp = _jp()
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, fft_backend=backend)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': step}, ells=(0, 2, 4))
+    geom = Geometry(meshsize, boxsize, 0., backend=backend)
+    ob = Bins(geom, step=step, ells=(0, 2, 4))
+    assert np.array_equal(b.edges, np.column_stack([ob.edges[:-1], ob.edges[1:]]))
+    # the Hermitian emulation of the full complex grid counts the same modes
+    assert np.array_equal(b.nmodes, ob.nmodes)
+    assert np.allclose(b.xavg, ob.xavg, rtol=1e-6, equal_nan=True)
+    if backend == 'jax':
+        # identical membership: per-bin sums of a per-mode integer label (exact in float32 partials)
+        cshape = geom.cshape
+        label = (np.arange(np.prod(cshape), dtype='i8').reshape(cshape) % 4096).astype('f4')
+        got = b(torch.as_tensor(label.astype('c8')).cuda())
+        ref = ob(label, accum='f64')
+        assert np.allclose(got.real * b.nmodes, ref * ob.nmodes, rtol=1e-13, atol=0)
+
+
+def _random_field(meshsize, boxsize, seed=0, n=200000):
+    rng = np.random.default_rng(seed)
+    pos = (rng.uniform(-0.5, 0.5, (n, 3)) * np.asarray(boxsize)).astype('f4')
+    return pos
+
+
+@pytest.mark.parametrize('los', ['x', 'z', (0.2, 0.3, 0.9327379053088815)])
+@pytest.mark.parametrize('out', ['real', 'complex'])
+def test_global_los_matches_oracle(los, out):
+    jp = _jp()
+    meshsize, boxsize, step = (64, 48, 40), np.array([1000., 800., 700.]), 0.01
+    pos = _random_field(meshsize, boxsize, seed=1)
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize)
+    mesh = jp.ParticleField(pos, attrs=attrs).paint(resampler='tsc', interlacing=3, compensate=True, out=out)
+    mesh = mesh - (mesh.value.mean() if out == 'real' else 0.)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': step}, ells=(0, 1, 2, 3, 4))
+    res = jp.compute_mesh2_spectrum(mesh, bin=b, los=los)
+    geom = Geometry(meshsize, boxsize, 0.)
+    ob = Bins(geom, step=step, ells=(0, 1, 2, 3, 4))
+    ref = ospectrum(mesh.value.cpu().numpy(), ob, los=los)  # same float32 mesh, float64 accumulation
+    scale = np.abs(ref['num_raw'][0]).max()
+    for i, ell in enumerate(ob.ells):
+        got = res.get(ell).num_raw
+        assert np.allclose(got, ref['num_raw'][i], rtol=0, atol=RTOL * scale), (ell, np.abs(got - ref['num_raw'][i]).max() / scale)
+    assert np.allclose(res.get(0).norm, ref['norm'])
+
+
+@pytest.mark.parametrize('los', ['firstpoint', 'endpoint'])
+@pytest.mark.parametrize('cross', [False, True])
+def test_firstpoint_matches_oracle(los, cross):
+    jp = _jp()
+    meshsize, boxsize, boxcenter, step = 32, 600., 500., 0.02
+    rng = np.random.default_rng(4)
+    value = rng.normal(size=(meshsize,) * 3).astype('f4')
+    value2 = (value + 0.5 * rng.normal(size=(meshsize,) * 3)).astype('f4')
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=boxcenter)
+    m1 = jp.RealMeshField(torch.as_tensor(value).cuda(), attrs=attrs)
+    m2 = jp.RealMeshField(torch.as_tensor(value2).cuda(), attrs=attrs)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': step}, ells=(0, 2, 4))
+    meshes = (m1, m2) if cross else (m1,)
+    res = jp.compute_mesh2_spectrum(*meshes, bin=b, los=los)
+    geom = Geometry(meshsize, boxsize, boxcenter)
+    ob = Bins(geom, step=step, ells=(0, 2, 4))
+    ref = ospectrum(value, ob, los=los, mesh2=value2 if cross else None)
+    scale = np.abs(ref['num_raw'][0]).max()
+    for i, ell in enumerate(ob.ells):
+        got = res.get(ell).num_raw
+        assert np.allclose(got, ref['num_raw'][i], rtol=0, atol=RTOL * scale), (ell, np.abs(got - ref['num_raw'][i]).max() / scale)
+
+
+def test_paint_jit_golden_gpu():
+    """tests/test_mesh.py:211: mesh.std() of TSC / interlacing 3 / compensated paint."""
+    jp = _jp()
+    g = GOLDEN['paint_jit']
+    pos = paint_jit_positions(g['seed'], g['nparticles']).astype('f4')
+    attrs = jp.MeshAttrs(meshsize=g['meshsize'], boxsize=g['boxsize'], boxcenter=g['boxcenter'], fft_backend='jaxdecomp')
+    mesh = jp.ParticleField(pos, attrs=attrs).paint(resampler=g['resampler'], interlacing=g['interlacing'],
+                                                    compensate=g['compensate'], out='real')
+    std = float(mesh.value.double().std(unbiased=False))
+    assert np.isclose(std, g['std'], rtol=GOLDEN_F32_RTOL, atol=0.), (std, g['std'])
+
+
+def test_spectrum_ref_golden_gpu():
+    """tests/test_mesh2.py:1032-1040: value().std() for los x / firstpoint / endpoint."""
+    jp = _jp()
+    g = GOLDEN['spectrum_ref']
+    attrs = jp.MeshAttrs(meshsize=g['meshsize'], boxsize=g['boxsize'], boxcenter=g['boxcenter'], fft_backend='jaxdecomp')
+    data = jp.ParticleField(uniform_particles(g['data_seed'], g['size'], g['boxsize'], g['boxcenter']).astype('f4'), attrs=attrs)
+    randoms = jp.ParticleField(uniform_particles(g['randoms_seed'], g['randoms_size'], g['boxsize'], g['boxcenter']).astype('f4'), attrs=attrs)
+    fkp = jp.FKPField(data, randoms)
+    mesh = fkp.paint(resampler=g['resampler'], interlacing=g['interlacing'], compensate=g['compensate'])
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': g['edges_step_in_kfun'] * attrs.kfun.min()}, ells=tuple(g['ells']))
+    geom = Geometry(g['meshsize'], g['boxsize'], g['boxcenter'], backend='jaxdecomp')
+    pos, w, _ = fkp_particles(data.positions.cpu().numpy(), None, randoms.positions.cpu().numpy(), None)
+    omesh = opaint.paint(geom, pos, w, g['resampler'], g['interlacing'], g['compensate'], 'real')
+    ob = Bins(geom, step=g['edges_step_in_kfun'] * geom.kfun.min(), ells=tuple(g['ells']))
+    for los, expected in g['value_std'].items():
+        value = jp.compute_mesh2_spectrum(mesh, bin=b, los=los).value()
+        r = ospectrum(omesh, ob, los=los)
+        f32_oracle = (r['num_raw'] / r['norm']).std()
+        assert np.isclose(value.std(), expected, rtol=GOLDEN_F32_RTOL, atol=0.), (los, value.std(), expected)
+        assert np.isclose(value.std(), f32_oracle, rtol=2e-6, atol=0.), (los, value.std(), f32_oracle)
+
+
+def test_fkp_normalization_shotnoise():
+    jp = _jp()
+    boxsize, boxcenter = 1000., 500.
+    rng = np.random.default_rng(9)
+    dpos = (rng.uniform(0, 800, (20000, 3)) + 100.).astype('f4')
+    rpos = (rng.uniform(0, 800, (60000, 3)) + 100.).astype('f4')
+    dw = rng.uniform(0.5, 1., 20000).astype('f4')
+    rw = rng.uniform(0.5, 1., 60000).astype('f4')
+    attrs = jp.MeshAttrs(meshsize=64, boxsize=boxsize, boxcenter=boxcenter)
+    fkp = jp.FKPField(jp.ParticleField(dpos, dw, attrs=attrs), jp.ParticleField(rpos, rw, attrs=attrs))
+    norm = jp.compute_fkp2_normalization(fkp)
+    geom = Geometry(64, boxsize, boxcenter)
+    ref = fkp2_normalization(geom, dpos, dw, rpos, rw, cellsize=10.)
+    assert np.isclose(norm, ref, rtol=1e-5)
+    sn = jp.compute_fkp2_shotnoise(fkp)
+    _, w, _ = fkp_particles(dpos, dw, rpos, rw)
+    assert np.isclose(sn, np.sum(w.astype('f8')**2), rtol=1e-5)
+
+
+def test_spectrum_deterministic():
+    jp = _jp()
+    pos = _random_field((64,) * 3, [1000.] * 3, seed=3, n=300000)
+    attrs = jp.MeshAttrs(meshsize=64, boxsize=1000., boxcenter=1200.)
+    mesh = jp.ParticleField(pos + 1200., attrs=attrs).paint(resampler='tsc', interlacing=2, compensate=True)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.01}, ells=(0, 2, 4))
+    a = jp.compute_mesh2_spectrum(mesh, bin=b, los='firstpoint').value()
+    c = jp.compute_mesh2_spectrum(mesh, bin=b, los='firstpoint').value()
+    assert np.array_equal(a, c)
