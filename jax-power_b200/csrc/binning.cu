@@ -32,27 +32,6 @@ struct BinGeom {
   int backend;
 };
 
-// jnp.digitize(k, edges, right=False): number of edges <= k.
-__device__ __forceinline__ int digitize(const float *__restrict__ e, int nedges, float step,
-                                        float k) {
-  int g;
-  if (step > 0.f) {
-    float t = floorf((k - e[0]) / step) + 1.f;
-    g = t < 0.f ? 0 : (t > (float)nedges ? nedges : (int)t);
-    while (g > 0 && e[g - 1] > k) --g;
-    while (g < nedges && e[g] <= k) ++g;
-  } else {
-    int lo = 0, hi = nedges;  // first index with e[idx] > k
-    while (lo < hi) {
-      int mid = (lo + hi) >> 1;
-      if (e[mid] <= k) lo = mid + 1;
-      else hi = mid;
-    }
-    g = lo;
-  }
-  return g;
-}
-
 // Hermitian weight of stored mode z: 'jax' 1 + (kz > 0); 'jaxdecomp' counts the
 // mirrored half of a full complex grid (self-conjugate planes once).
 __device__ __forceinline__ float mode_weight(const BinGeom &g, int z) {
@@ -82,13 +61,52 @@ __device__ __forceinline__ float legendre(int ell, float x) {
   }
 }
 
+// Exact digitize on |k|^2: t_b = smallest float x with sqrt_rn(x) >= edges[b], so that
+// #{b : k2 >= t_b} == #{b : edges[b] <= sqrt_rn(k2)} (sqrt_rn is monotone); this is
+// jnp.digitize(sqrt(k2), edges, right=False) bit for bit, without a per-mode sqrt.
+__device__ float sqrt_threshold(float e) {
+  if (!(e > 0.f)) return -1.f;  // every k2 >= 0 passes
+  if (isinf(e)) return e;
+  float x = __fmul_rn(e, e);
+  while (__fsqrt_rn(x) < e) x = nextafterf(x, INFINITY);
+  for (;;) {
+    const float p = nextafterf(x, 0.f);
+    if (p >= 0.f && p < x && __fsqrt_rn(p) >= e) x = p;
+    else break;
+  }
+  return x;
+}
+
+// Bin index from k2 without prior state: guess from an approximate |k| then correct.
+__device__ __forceinline__ int bin_from_k2(const float *__restrict__ thr, int nedges, float e0,
+                                           float inv_step, float k2) {
+  int g;
+  if (inv_step > 0.f) {
+    const float k = k2 > 0.f ? k2 * rsqrtf(k2) : 0.f;
+    const float t = floorf((k - e0) * inv_step) + 1.f;
+    g = t < 0.f ? 0 : (t > (float)nedges ? nedges : (int)t);
+    while (g > 0 && k2 < thr[g - 1]) --g;
+    while (g < nedges && k2 >= thr[g]) ++g;
+  } else {
+    int lo = 0, hi = nedges;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (k2 >= thr[mid]) lo = mid + 1;
+      else hi = mid;
+    }
+    g = lo;
+  }
+  return g;
+}
+
 // ------------------------------------------------------------- per-mode ops
-struct ModesOp {  // nmodes and sum of w |k|
+// op(idx, i, j, z, kx, ky, kz, k2, w, v): values of stored mode (i, j, z), weight w.
+struct ModesOp {  // nmodes and sum of w |k| (|k| = sqrt_rn(k2), as the reference's float32 knorm)
   static constexpr int NV = 2;
-  __device__ void operator()(int64_t, int, int, int, float, float, float, float knorm, float w,
+  __device__ void operator()(int64_t, int, int, int, float, float, float, float k2, float w,
                              float v[NV]) const {
     v[0] = w;
-    v[1] = __fmul_rn(knorm, w);
+    v[1] = __fmul_rn(__fsqrt_rn(k2), w);
   }
 };
 
@@ -96,8 +114,8 @@ struct MeshOp {  // plain per-bin sum of a complex mesh value (BinMesh2SpectrumP
   const float2 *v;
   int remove_zero;
   static constexpr int NV = 2;
-  __device__ void operator()(int64_t idx, int i, int j, int z, float, float, float, float,
-                             float w, float out[NV]) const {
+  __device__ void operator()(int64_t idx, int i, int j, int z, float, float, float, float, float w,
+                             float out[NV]) const {
     const float2 a = v[idx];
     const bool zero = remove_zero && i == 0 && j == 0 && z == 0;
     out[0] = zero ? 0.f : __fmul_rn(a.x, w);
@@ -105,47 +123,39 @@ struct MeshOp {  // plain per-bin sum of a complex mesh value (BinMesh2SpectrumP
   }
 };
 
-struct GlobalOp {
+template <int N>
+struct GlobalOp {  // w * Re/Im(A) * L_ell(mu), A = |d1|^2 or conj(d1) d2 (mesh2.py:346-374)
   const float2 *d1;
   const float2 *d2;
   float los[3];
-  int nells;
   int ells[MAX_ELLS];
-  static constexpr int NV = MAX_ELLS;
+  static constexpr int NV = N;
   __device__ void operator()(int64_t idx, int i, int j, int z, float kx, float ky, float kz,
-                             float knorm, float w, float v[NV]) const {
+                             float k2, float w, float v[NV]) const {
     const float2 a = d1[idx];
     float re, im;
     if (d2) {
-      const float2 b = d2[idx];  // conj(a) * b
-      re = __fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y));
-      im = __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x));
+      const float2 b = d2[idx];
+      re = a.x * b.x + a.y * b.y;
+      im = a.x * b.y - a.y * b.x;
     } else {
-      re = __fadd_rn(__fmul_rn(a.x, a.x), __fmul_rn(a.y, a.y));
+      re = a.x * a.x + a.y * a.y;
       im = 0.f;
     }
     const bool zero = (i == 0 && j == 0 && z == 0);
-    const float num = __fadd_rn(__fadd_rn(__fadd_rn(0.f, __fmul_rn(kx, los[0])), __fmul_rn(ky, los[1])),
-                                __fmul_rn(kz, los[2]));
-    const float mu = __fdiv_rn(num, zero ? 1.f : knorm);
+    const float num = (kx * los[0] + ky * los[1]) + kz * los[2];
+    const float mu = k2 > 0.f ? num * rsqrtf(k2) : 0.f;  // |k|(0) = 1 in the reference: mu(0) = 0
 #pragma unroll
     for (int l = 0; l < NV; ++l) {
-      if (l < nells) {
-        const int ell = ells[l];
-        const float part = (ell & 1) ? im : re;
-        if (ell == 0) {
-          v[l] = __fmul_rn(part, w);
-        } else {
-          v[l] = zero ? 0.f : __fmul_rn(__fmul_rn(part, legendre(ell, mu)), w);
-        }
-      } else {
-        v[l] = 0.f;
-      }
+      const int ell = ells[l];
+      const float part = (ell & 1) ? im : re;
+      v[l] = ell == 0 ? part * w : (zero ? 0.f : part * legendre(ell, mu) * w);
     }
   }
 };
 
-struct FirstPointOp {
+template <int N>
+struct FirstPointOp {  // w * Re/Im(conj(sum_m F_m Y_lm(khat)) A0) (mesh2.py:293-344)
   const float2 *a0;
   const float2 *b0;
   const float2 *f;
@@ -153,172 +163,318 @@ struct FirstPointOp {
   int nterms;
   int term_ell[MAX_FP_TERMS];
   int term_m[MAX_FP_TERMS];
-  int nells;
   int ells[MAX_ELLS];
   int include_ell0;
-  static constexpr int NV = MAX_ELLS;
+  static constexpr int NV = N;
   __device__ void operator()(int64_t idx, int i, int j, int z, float kx, float ky, float kz,
-                             float knorm, float w, float v[NV]) const {
+                             float k2, float w, float v[NV]) const {
     const float2 A = a0[idx];
     const bool zero = (i == 0 && j == 0 && z == 0);
-    float xh = 0.f, yh = 0.f, zh = 0.f;
-    if (knorm != 0.f) {
-      xh = __fdiv_rn(kx, knorm);
-      yh = __fdiv_rn(ky, knorm);
-      zh = __fdiv_rn(kz, knorm);
-    }
+    const float rn = k2 > 0.f ? rsqrtf(k2) : 0.f;  // khat = k / |k|, 0 at k = 0
+    const float xh = kx * rn, yh = ky * rn, zh = kz * rn;
 #pragma unroll
     for (int l = 0; l < NV; ++l) {
       v[l] = 0.f;
-      if (l >= nells) continue;
       const int ell = ells[l];
       if (ell == 0) {
         if (!include_ell0) continue;
-        float re, im;
         if (b0) {
           const float2 B = b0[idx];
-          re = __fadd_rn(__fmul_rn(B.x, A.x), __fmul_rn(B.y, A.y));
-          im = __fsub_rn(__fmul_rn(B.x, A.y), __fmul_rn(B.y, A.x));
+          v[l] = (B.x * A.x + B.y * A.y) * w;
         } else {
-          re = __fadd_rn(__fmul_rn(A.x, A.x), __fmul_rn(A.y, A.y));
-          im = 0.f;
+          v[l] = (A.x * A.x + A.y * A.y) * w;
         }
-        (void)im;
-        v[l] = __fmul_rn(re, w);
         continue;
       }
       float sr = 0.f, si = 0.f;
-      bool any = false;
       for (int t = 0; t < nterms; ++t) {
         if (term_ell[t] != ell) continue;
         const float2 F = f[(int64_t)t * fstride + idx];
         const float y = ylm_eval(ell, term_m[t], xh, yh, zh);
-        sr = __fadd_rn(sr, __fmul_rn(F.x, y));
-        si = __fadd_rn(si, __fmul_rn(F.y, y));
-        any = true;
+        sr += F.x * y;
+        si += F.y * y;
       }
-      if (!any || zero) continue;
-      // conj(S) * A0
-      const float re = __fadd_rn(__fmul_rn(sr, A.x), __fmul_rn(si, A.y));
-      const float im = __fsub_rn(__fmul_rn(sr, A.y), __fmul_rn(si, A.x));
-      v[l] = __fmul_rn((ell & 1) ? im : re, w);
+      if (zero) continue;
+      const float re = sr * A.x + si * A.y;  // conj(S) * A0
+      const float im = sr * A.y - si * A.x;
+      v[l] = ((ell & 1) ? im : re) * w;
     }
   }
 };
 
-// ------------------------------------------------------------ the reduction
-template <class Op>
-__global__ void __launch_bounds__(BIN_THREADS) bin_kernel(BinGeom g, Op op,
-                                                          const float *__restrict__ edges,
-                                                          int nv, int nwarps_hist,
-                                                          double *__restrict__ partials) {
-  constexpr int NV = Op::NV;
+// Shared-memory layout of one binning CTA.
+struct BinSmem {
+  double *hist;  // [nwarps][nbins][NV]
+  float *thr;    // [nedges]
+  float *kz;     // [nz] (when tabulated)
+  float *kz2;    // [nz]
+};
+
+__device__ __forceinline__ BinSmem bin_smem_init(const BinGeom &g, const float *edges, int nv,
+                                                 int nwarps, bool tab) {
   extern __shared__ double smem[];
+  BinSmem s;
   const int nbins = g.nedges - 1;
-  const int hist_len = nbins * nv;
-  double *hist = smem;                                            // [warps][nbins][nv]
-  float *sedges = reinterpret_cast<float *>(smem + (size_t)nwarps_hist * hist_len);
+  s.hist = smem;
+  s.thr = reinterpret_cast<float *>(smem + (size_t)nwarps * nbins * nv);
+  s.kz = s.thr + ((g.nedges + 3) & ~3);
+  s.kz2 = s.kz + ((g.d.nz + 3) & ~3);
+  for (int i = threadIdx.x; i < nwarps * nbins * nv; i += blockDim.x) s.hist[i] = 0.;
+  for (int i = threadIdx.x; i < g.nedges; i += blockDim.x) s.thr[i] = sqrt_threshold(edges[i]);
+  if (tab)
+    for (int z = threadIdx.x; z < g.d.nz; z += blockDim.x) {
+      const float kz = kz_coord(g, z);
+      s.kz[z] = kz;
+      s.kz2[z] = __fmul_rn(kz, kz);
+    }
+  __syncthreads();
+  return s;
+}
+
+__device__ __forceinline__ void bin_smem_flush(const BinSmem &s, int hist_len, int nwarps,
+                                               double *__restrict__ partials) {
+  __syncthreads();
+  double *out = partials + (size_t)blockIdx.x * hist_len;
+  for (int e = threadIdx.x; e < hist_len; e += blockDim.x) {
+    double acc = 0.;
+    for (int w = 0; w < nwarps; ++w) acc += s.hist[(size_t)w * hist_len + e];
+    out[e] = acc;
+  }
+}
+
+// --------------------------------------------------------- row-run reduction
+// One warp per (i, j) row; lane l walks the contiguous run z in [l R, (l+1) R).  |k| is
+// non-decreasing along the run, so the bin only moves forward: interior segments of a run
+// belong to that lane alone and go straight to the warp's float64 histogram; the first
+// and last segments of every run are merged across lanes by one segmented scan per row.
+template <int NV, class Op>
+__global__ void __launch_bounds__(BIN_THREADS) bin_rows_kernel(BinGeom g, Op op,
+                                                               const float *__restrict__ edges,
+                                                               int nwarps_hist, int tab,
+                                                               double *__restrict__ partials) {
+  const int nbins = g.nedges - 1;
+  const int hist_len = nbins * NV;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nwarps = blockDim.x >> 5;
-  for (int i = threadIdx.x; i < nwarps * hist_len; i += blockDim.x) hist[i] = 0.;
-  for (int i = threadIdx.x; i < g.nedges; i += blockDim.x) sedges[i] = edges[i];
-  __syncthreads();
-
-  double *my = hist + (size_t)warp * hist_len;
+  const BinSmem s = bin_smem_init(g, edges, NV, nwarps_hist, tab);
+  double *my = s.hist + (size_t)warp * hist_len;
+  const float e0 = edges[0];
+  const float inv_step = g.step > 0.f ? 1.f / g.step : 0.f;
+  const int R = (g.d.nz + 31) / 32;
+  const int z0 = lane * R, z1 = min(g.d.nz, z0 + R);
   const int64_t nrows = (int64_t)g.d.n0 * g.d.n1;
+  constexpr int NONE = 0x7fffffff;
   for (int64_t row = (int64_t)blockIdx.x * nwarps + warp; row < nrows;
        row += (int64_t)gridDim.x * nwarps) {
     const int i = (int)(row / g.d.n1), j = (int)(row % g.d.n1);
     const float kx = kcoord(i, g.d.n0, g.kfun[0], false);
     const float ky = kcoord(j, g.d.n1, g.kfun[1], false);
     const float kxy = __fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky));  // (0 + kx^2) + ky^2
-    for (int z0 = 0; z0 < g.d.nz; z0 += 32) {
-      const int z = z0 + lane;
+    int cur = -1, lead = NONE, trail = NONE, nseg = 0;
+    float acc[NV], facc[NV];
+#pragma unroll
+    for (int c = 0; c < NV; ++c) acc[c] = facc[c] = 0.f;
+    for (int z = z0; z < z1; ++z) {
+      float kz, kz2;
+      if (tab) {
+        kz = s.kz[z];
+        kz2 = s.kz2[z];
+      } else {
+        kz = kz_coord(g, z);
+        kz2 = __fmul_rn(kz, kz);
+      }
+      const float k2 = __fadd_rn(kxy, kz2);
+      int gb = cur;
+      if (cur < 0) gb = bin_from_k2(s.thr, g.nedges, e0, inv_step, k2);
+      else
+        while (gb < g.nedges && k2 >= s.thr[gb]) ++gb;
+      if (gb != cur) {
+        if (cur >= 0) {  // close the current segment
+          if (nseg == 0) {
+            lead = cur;
+#pragma unroll
+            for (int c = 0; c < NV; ++c) facc[c] = acc[c];
+          } else if (cur >= 1 && cur <= nbins) {  // interior: exclusive to this lane
+#pragma unroll
+            for (int c = 0; c < NV; ++c) my[(size_t)(cur - 1) * NV + c] += (double)acc[c];
+          }
+          ++nseg;
+        }
+        cur = gb;
+#pragma unroll
+        for (int c = 0; c < NV; ++c) acc[c] = 0.f;
+      }
+      float v[NV];
+      op(row * g.d.nz + z, i, j, z, kx, ky, kz, k2, mode_weight(g, z), v);
+#pragma unroll
+      for (int c = 0; c < NV; ++c) acc[c] += v[c];
+    }
+    // leading (L, facc) and trailing (T, tacc) entries of this lane's run
+    float tacc[NV];
+    if (cur < 0) {  // empty run
+      lead = trail = NONE;
+    } else if (nseg == 0) {  // a single segment
+      lead = trail = cur;
+#pragma unroll
+      for (int c = 0; c < NV; ++c) facc[c] = tacc[c] = acc[c];
+    } else {
+      trail = cur;
+#pragma unroll
+      for (int c = 0; c < NV; ++c) tacc[c] = acc[c];
+    }
+    if (cur >= 0 && nseg == 0) {
+#pragma unroll
+      for (int c = 0; c < NV; ++c) facc[c] = 0.f;  // counted once, in the trailing entry
+    }
+    // inclusive segmented scan of trailing entries over lanes (keys are monotone)
+    float S[NV];
+#pragma unroll
+    for (int c = 0; c < NV; ++c) S[c] = tacc[c];
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int k = __shfl_up_sync(0xffffffffu, trail, d);
+      const bool ok = lane >= d && k == trail;
+#pragma unroll
+      for (int c = 0; c < NV; ++c) {
+        const float t = __shfl_up_sync(0xffffffffu, S[c], d);
+        if (ok) S[c] += t;
+      }
+    }
+    const int prev_trail = __shfl_up_sync(0xffffffffu, trail, 1);
+    float carry[NV];
+#pragma unroll
+    for (int c = 0; c < NV; ++c) {
+      const float t = __shfl_up_sync(0xffffffffu, S[c], 1);
+      carry[c] = (lane > 0 && prev_trail == lead) ? t : 0.f;
+    }
+    const int next_lead = __shfl_down_sync(0xffffffffu, lead, 1);
+    const int next_trail = __shfl_down_sync(0xffffffffu, trail, 1);
+    // a multi-segment lane writes its leading bin with the carry of the lanes before it
+    if (cur >= 0 && nseg > 0 && lead >= 1 && lead <= nbins) {
+#pragma unroll
+      for (int c = 0; c < NV; ++c) my[(size_t)(lead - 1) * NV + c] += (double)(facc[c] + carry[c]);
+    }
+    // the trailing total is written by the last lane of its key, unless the next lane
+    // starts a multi-segment run with that key (then that lane writes it)
+    const bool next_takes = lane < 31 && next_lead == trail;
+    const bool next_continues = lane < 31 && next_trail == trail;
+    if (cur >= 0 && !next_takes && !next_continues && trail >= 1 && trail <= nbins) {
+#pragma unroll
+      for (int c = 0; c < NV; ++c) my[(size_t)(trail - 1) * NV + c] += (double)S[c];
+    }
+    __syncwarp();
+  }
+  bin_smem_flush(s, hist_len, nwarps, partials);
+}
+
+// ------------------------------------------------------- chunk reduction
+// One warp per row, lanes on consecutive kz (coalesced loads of many meshes); one
+// segmented scan per 32 modes.  Used by the first-point estimator (14+ meshes per mode).
+template <int NV, class Op>
+__global__ void __launch_bounds__(BIN_THREADS) bin_chunks_kernel(BinGeom g, Op op,
+                                                                 const float *__restrict__ edges,
+                                                                 int nwarps_hist, int tab,
+                                                                 double *__restrict__ partials) {
+  const int nbins = g.nedges - 1;
+  const int hist_len = nbins * NV;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  const BinSmem s = bin_smem_init(g, edges, NV, nwarps_hist, tab);
+  double *my = s.hist + (size_t)warp * hist_len;
+  const float e0 = edges[0];
+  const float inv_step = g.step > 0.f ? 1.f / g.step : 0.f;
+  const int64_t nrows = (int64_t)g.d.n0 * g.d.n1;
+  for (int64_t row = (int64_t)blockIdx.x * nwarps + warp; row < nrows;
+       row += (int64_t)gridDim.x * nwarps) {
+    const int i = (int)(row / g.d.n1), j = (int)(row % g.d.n1);
+    const float kx = kcoord(i, g.d.n0, g.kfun[0], false);
+    const float ky = kcoord(j, g.d.n1, g.kfun[1], false);
+    const float kxy = __fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky));
+    for (int zc = 0; zc < g.d.nz; zc += 32) {
+      const int z = zc + lane;
       const bool valid = z < g.d.nz;
       float v[NV];
       int key = 0x7fffffff;
       if (valid) {
-        const float kz = kz_coord(g, z);
-        const float knorm = __fsqrt_rn(__fadd_rn(kxy, __fmul_rn(kz, kz)));
-        key = digitize(sedges, g.nedges, g.step, knorm);
-        op(row * g.d.nz + z, i, j, z, kx, ky, kz, knorm, mode_weight(g, z), v);
+        float kz, kz2;
+        if (tab) {
+          kz = s.kz[z];
+          kz2 = s.kz2[z];
+        } else {
+          kz = kz_coord(g, z);
+          kz2 = __fmul_rn(kz, kz);
+        }
+        const float k2 = __fadd_rn(kxy, kz2);
+        key = bin_from_k2(s.thr, g.nedges, e0, inv_step, k2);
+        op(row * g.d.nz + z, i, j, z, kx, ky, kz, k2, mode_weight(g, z), v);
       } else {
 #pragma unroll
         for (int c = 0; c < NV; ++c) v[c] = 0.f;
       }
-      // segmented inclusive scan over contiguous equal keys
       const int prev = __shfl_up_sync(0xffffffffu, key, 1);
-      const bool distinct = __all_sync(0xffffffffu, lane == 0 || prev != key);
-      if (!distinct) {
+      if (!__all_sync(0xffffffffu, lane == 0 || prev != key)) {
 #pragma unroll
-        for (int dlt = 1; dlt < 32; dlt <<= 1) {
-          const int ok = __shfl_up_sync(0xffffffffu, key, dlt) == key && lane >= dlt;
+        for (int d = 1; d < 32; d <<= 1) {
+          const bool ok = __shfl_up_sync(0xffffffffu, key, d) == key && lane >= d;
 #pragma unroll
           for (int c = 0; c < NV; ++c) {
-            if (c < nv) {
-              const float t = __shfl_up_sync(0xffffffffu, v[c], dlt);
-              if (ok) v[c] += t;
-            }
+            const float t = __shfl_up_sync(0xffffffffu, v[c], d);
+            if (ok) v[c] += t;
           }
         }
       }
       const int next = __shfl_down_sync(0xffffffffu, key, 1);
-      const bool tail = (lane == 31) || next != key;
-      if (valid && tail && key >= 1 && key <= nbins) {
-        double *h = my + (size_t)(key - 1) * nv;
+      if (valid && (lane == 31 || next != key) && key >= 1 && key <= nbins) {
 #pragma unroll
-        for (int c = 0; c < NV; ++c)
-          if (c < nv) h[c] += (double)v[c];
+        for (int c = 0; c < NV; ++c) my[(size_t)(key - 1) * NV + c] += (double)v[c];
       }
       __syncwarp();
     }
   }
-  __syncthreads();
-  double *out = partials + (size_t)blockIdx.x * hist_len;
-  for (int e = threadIdx.x; e < hist_len; e += blockDim.x) {
-    double s = 0.;
-    for (int w = 0; w < nwarps; ++w) s += hist[(size_t)w * hist_len + e];
-    out[e] = s;
-  }
+  bin_smem_flush(s, hist_len, nwarps, partials);
 }
 
-// out[e] (+)= sum over CTAs, in CTA order.
+// out[e] (+)= sum over CTAs, in CTA order, transposed to [value][bin].
 __global__ void bin_finalize_kernel(const double *__restrict__ partials, int nblocks,
-                                    int hist_len, int nv, int nbins, int nout_values,
-                                    int accumulate, double *__restrict__ out0,
-                                    double *__restrict__ out1) {
+                                    int hist_len, int nv, int nbins, int accumulate,
+                                    double *__restrict__ out0, double *__restrict__ out1) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < hist_len;
        e += gridDim.x * blockDim.x) {
-    double s = 0.;
-    for (int b = 0; b < nblocks; ++b) s += partials[(size_t)b * hist_len + e];
+    double acc = 0.;
+    for (int b = 0; b < nblocks; ++b) acc += partials[(size_t)b * hist_len + e];
     const int bin = e / nv, c = e % nv;
-    if (c >= nout_values) continue;
-    // transpose to [value][bin]
     double *dst = (c == 1 && out1) ? out1 : out0;
     const int64_t o = (c == 1 && out1) ? bin : (int64_t)c * nbins + bin;
-    dst[o] = accumulate ? dst[o] + s : s;
+    dst[o] = accumulate ? dst[o] + acc : acc;
   }
 }
 
 struct BinLaunch {
   int blocks;
   int nwarps;
+  int tab;
   size_t smem;
   size_t partial_bytes;
 };
 
-static bool plan_bins(const Dims &d, int nedges, int nv, BinLaunch *L) {
+static bool plan_bins(const Dims &d, int nedges, int nv, BinLaunch *L,
+                      size_t hist_elem = sizeof(double)) {
   const int nbins = nedges - 1;
-  const size_t per_warp = (size_t)nbins * nv * sizeof(double);
-  const size_t edge_bytes = align_up((size_t)nedges * sizeof(float), 16);
+  const size_t per_warp = (size_t)nbins * nv * hist_elem;
+  const size_t thr_bytes = (size_t)((nedges + 3) & ~3) * sizeof(float);
+  const size_t tab_bytes = 2 * (size_t)((d.nz + 3) & ~3) * sizeof(float);
   const size_t budget = 200 * 1024;
+  L->tab = tab_bytes <= 32 * 1024;
+  const size_t fixed = thr_bytes + (L->tab ? tab_bytes : 0);
   int nwarps = BIN_THREADS / 32;
-  if (per_warp + edge_bytes > budget) return false;
-  while (nwarps > 1 && (size_t)nwarps * per_warp + edge_bytes > budget) nwarps >>= 1;
+  if (per_warp + fixed > budget) return false;
+  while (nwarps > 1 && (size_t)nwarps * per_warp + fixed > budget) nwarps >>= 1;
   L->nwarps = nwarps;
-  L->smem = (size_t)nwarps * per_warp + edge_bytes;
+  L->smem = align_up((size_t)nwarps * per_warp, 16) + fixed;
   const int64_t nrows = (int64_t)d.n0 * d.n1;
-  const int per_sm = L->smem > 110 * 1024 ? 1 : (L->smem > 72 * 1024 ? 2 : 4);
+  int per_sm = (int)((228 * 1024) / (L->smem + 1024));
+  if (per_sm > 8) per_sm = 8;
+  if (per_sm < 1) per_sm = 1;
   int64_t blocks = (int64_t)per_sm * sm_count();
   const int64_t need = (nrows + nwarps - 1) / nwarps;
   if (blocks > need) blocks = need;
@@ -328,27 +484,296 @@ static bool plan_bins(const Dims &d, int nedges, int nv, BinLaunch *L) {
   return true;
 }
 
-template <class Op>
+template <int NV, class Op>
 static pk_status launch_bins(cudaStream_t s, const BinGeom &g, const Op &op, const float *edges,
-                             int nv, int nout_values, int accumulate, double *out0, double *out1,
+                             bool rows, int accumulate, double *out0, double *out1,
                              void *workspace, size_t workspace_bytes) {
   BinLaunch L;
-  PK_REQUIRE(plan_bins(g.d, g.nedges, nv, &L), PK_ERR_RANGE,
-             "too many bins x values (%d x %d) for the shared-memory histograms", g.nedges - 1, nv);
+  PK_REQUIRE(plan_bins(g.d, g.nedges, NV, &L), PK_ERR_RANGE,
+             "too many bins x values (%d x %d) for the shared-memory histograms", g.nedges - 1, NV);
   PK_REQUIRE(workspace && workspace_bytes >= L.partial_bytes, PK_ERR_WORKSPACE,
              "binning workspace too small: need %zu bytes, got %zu", L.partial_bytes,
              workspace_bytes);
   double *partials = static_cast<double *>(workspace);
-  PK_CUDA(cudaFuncSetAttribute(bin_kernel<Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)L.smem));
-  bin_kernel<Op><<<L.blocks, L.nwarps * 32, L.smem, s>>>(g, op, edges, nv, L.nwarps, partials);
+  if (rows) {
+    PK_CUDA(cudaFuncSetAttribute(bin_rows_kernel<NV, Op>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
+    bin_rows_kernel<NV, Op><<<L.blocks, L.nwarps * 32, L.smem, s>>>(g, op, edges, L.nwarps, L.tab,
+                                                                     partials);
+  } else {
+    PK_CUDA(cudaFuncSetAttribute(bin_chunks_kernel<NV, Op>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
+    bin_chunks_kernel<NV, Op><<<L.blocks, L.nwarps * 32, L.smem, s>>>(g, op, edges, L.nwarps,
+                                                                       L.tab, partials);
+  }
   PK_LAUNCH_CHECK();
-  const int hist_len = (g.nedges - 1) * nv;
+  const int hist_len = (g.nedges - 1) * NV;
   const int fb = (hist_len + 255) / 256;
-  bin_finalize_kernel<<<fb, 256, 0, s>>>(partials, L.blocks, hist_len, nv, g.nedges - 1,
-                                         nout_values, accumulate, out0, out1);
+  bin_finalize_kernel<<<fb, 256, 0, s>>>(partials, L.blocks, hist_len, NV, g.nedges - 1,
+                                         accumulate, out0, out1);
   PK_LAUNCH_CHECK();
   return PK_OK;
+}
+
+// ------------------------------------------------- global line of sight, fused
+// The hot binning pass of the global-los estimator (mesh2.py:346-374), written out for
+// throughput: per mode one complex load, |k|^2 from per-axis tables, the bin advanced
+// against exact |k|^2 thresholds, mu^2 = (k.los)^2 / k^2 by a reciprocal, and every
+// L_ell as Horner polynomials in mu^2 (times mu for odd ell).  Row runs and the per-row
+// segmented scan as in bin_rows_kernel.
+struct LegendreCoefs {
+  float c[MAX_ELLS][5];  // L_ell(mu) = mu^(ell % 2) * sum_p c[p] mu^(2p)
+  int odd[MAX_ELLS];
+  int any_odd;
+};
+
+__host__ inline void legendre_coefs(int ell, float c[5], int *odd) {
+  static const double table[9][5] = {
+      {1., 0., 0., 0., 0.},
+      {1., 0., 0., 0., 0.},
+      {-0.5, 1.5, 0., 0., 0.},
+      {-1.5, 2.5, 0., 0., 0.},
+      {0.375, -3.75, 4.375, 0., 0.},
+      {1.875, -8.75, 7.875, 0., 0.},
+      {-0.3125, 6.5625, -19.6875, 14.4375, 0.},
+      {-2.1875, 19.6875, -43.3125, 26.8125, 0.},
+      {0.2734375, -9.84375, 54.140625, -93.84375, 50.2734375}};
+  for (int p = 0; p < 5; ++p) c[p] = (float)table[ell][p];
+  *odd = ell & 1;
+}
+
+// Shared layout of the fused kernel: float32 warp histograms [nwarps][nbins][NV] (warp
+// partials), thresholds, kz tables.
+struct GlobalSmem {
+  float *hist;
+  float *thr;
+  float *kz;
+  float *kz2;
+};
+
+template <int NV, bool CROSS>
+__global__ void __launch_bounds__(BIN_THREADS) bin_global_kernel(
+    BinGeom g, const float2 *__restrict__ d1, const float2 *__restrict__ d2, float lx, float ly,
+    float lz, LegendreCoefs lc, int zero_l0, const float *__restrict__ edges, int nwarps_hist,
+    int tab, double *__restrict__ partials) {
+  const int nbins = g.nedges - 1;
+  const int hist_len = nbins * NV;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  extern __shared__ double smem[];
+  GlobalSmem s;
+  s.hist = reinterpret_cast<float *>(smem);
+  s.thr = s.hist + (((size_t)nwarps_hist * hist_len + 3) & ~(size_t)3);
+  s.kz = s.thr + ((g.nedges + 3) & ~3);
+  s.kz2 = s.kz + ((g.d.nz + 3) & ~3);
+  for (int q = threadIdx.x; q < nwarps_hist * hist_len; q += blockDim.x) s.hist[q] = 0.f;
+  for (int q = threadIdx.x; q < g.nedges; q += blockDim.x) s.thr[q] = sqrt_threshold(edges[q]);
+  if (tab)
+    for (int z = threadIdx.x; z < g.d.nz; z += blockDim.x) {
+      const float kzz = kz_coord(g, z);
+      s.kz[z] = kzz;
+      s.kz2[z] = __fmul_rn(kzz, kzz);
+    }
+  __syncthreads();
+  float *my = s.hist + (size_t)warp * hist_len;
+  const float e0 = edges[0];
+  const float inv_step = g.step > 0.f ? 1.f / g.step : 0.f;
+  const int R = (g.d.nz + 31) / 32;
+  const int z0 = lane * R, z1 = min(g.d.nz, z0 + R);
+  const int64_t nrows = (int64_t)g.d.n0 * g.d.n1;
+  const bool jaxw = g.backend == PK_BACKEND_JAX;
+  const int zself = (g.d.n2 % 2) == 0 ? g.d.nz - 1 : -1;  // self-conjugate last plane
+  constexpr int NONE = 0x7fffffff;
+  for (int64_t row = (int64_t)blockIdx.x * nwarps + warp; row < nrows;
+       row += (int64_t)gridDim.x * nwarps) {
+    const int i = (int)(row / g.d.n1), j = (int)(row % g.d.n1);
+    const float kx = kcoord(i, g.d.n0, g.kfun[0], false);
+    const float ky = kcoord(j, g.d.n1, g.kfun[1], false);
+    const float kxy = __fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky));
+    const float kl = kx * lx + ky * ly;
+    int cur = -1, lead = NONE, trail = NONE, nseg = 0;
+    float acc[NV], facc[NV];
+#pragma unroll
+    for (int c = 0; c < NV; ++c) acc[c] = facc[c] = 0.f;
+    const float2 *p1 = d1 + row * g.d.nz;
+    const float2 *p2 = CROSS ? d2 + row * g.d.nz : nullptr;
+    // the run's values are loaded RB at a time before use: many loads in flight per lane
+    constexpr int RB = CROSS ? 4 : 8;
+    for (int zb = z0; zb < z1; zb += RB) {
+      float2 va[RB], vb[CROSS ? RB : 1];
+#pragma unroll
+      for (int t = 0; t < RB; ++t) {
+        const int z = zb + t;
+        va[t] = z < z1 ? p1[z] : make_float2(0.f, 0.f);
+        if (CROSS) vb[t] = z < z1 ? p2[z] : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int t = 0; t < RB; ++t) {
+        const int z = zb + t;
+        if (z >= z1) break;
+        float kz, kz2;
+        if (tab) {
+          kz = s.kz[z];
+          kz2 = s.kz2[z];
+        } else {
+          kz = kz_coord(g, z);
+          kz2 = __fmul_rn(kz, kz);
+        }
+        const float k2 = __fadd_rn(kxy, kz2);
+        int gb = cur;
+        if (cur < 0) gb = bin_from_k2(s.thr, g.nedges, e0, inv_step, k2);
+        else
+          while (gb < g.nedges && k2 >= s.thr[gb]) ++gb;
+        if (gb != cur) {
+          if (cur >= 0) {
+            if (nseg == 0) {
+              lead = cur;
+#pragma unroll
+              for (int c = 0; c < NV; ++c) facc[c] = acc[c];
+            } else if (cur >= 1 && cur <= nbins) {
+#pragma unroll
+              for (int c = 0; c < NV; ++c) my[(size_t)(cur - 1) * NV + c] += acc[c];
+            }
+            ++nseg;
+          }
+          cur = gb;
+#pragma unroll
+          for (int c = 0; c < NV; ++c) acc[c] = 0.f;
+        }
+        const float2 a = va[t];
+        float re, im = 0.f;
+        if (CROSS) {
+          const float2 b = vb[CROSS ? t : 0];
+          re = a.x * b.x + a.y * b.y;
+          im = a.x * b.y - a.y * b.x;
+        } else {
+          re = a.x * a.x + a.y * a.y;
+        }
+        const float w = jaxw ? (z > 0 ? 2.f : 1.f) : ((z == 0 || z == zself) ? 1.f : 2.f);
+        const float num = kl + kz * lz;
+        const float rk2 = k2 > 0.f ? __frcp_rn(k2) : 0.f;
+        const float mu2 = num * num * rk2;
+        const float mu = lc.any_odd ? num * sqrtf(rk2) : 0.f;
+        const bool zero = (row == 0 && z == 0);  // remove_zero for ell > 0
+        const float rw = re * w, iw = im * w;
+#pragma unroll
+        for (int l = 0; l < NV; ++l) {
+          float L = lc.c[l][4];
+          L = L * mu2 + lc.c[l][3];
+          L = L * mu2 + lc.c[l][2];
+          L = L * mu2 + lc.c[l][1];
+          L = L * mu2 + lc.c[l][0];
+          if (lc.odd[l]) L *= mu;
+          const float part = lc.odd[l] ? iw : rw;
+          const bool drop = zero && !(zero_l0 & (1 << l));
+          acc[l] += drop ? 0.f : part * L;
+        }
+      }
+    }
+    float tacc[NV];
+    if (cur < 0) {
+      lead = trail = NONE;
+#pragma unroll
+      for (int c = 0; c < NV; ++c) tacc[c] = 0.f;
+    } else if (nseg == 0) {
+      lead = trail = cur;
+#pragma unroll
+      for (int c = 0; c < NV; ++c) {
+        tacc[c] = acc[c];
+        facc[c] = 0.f;
+      }
+    } else {
+      trail = cur;
+#pragma unroll
+      for (int c = 0; c < NV; ++c) tacc[c] = acc[c];
+    }
+    float S[NV];
+#pragma unroll
+    for (int c = 0; c < NV; ++c) S[c] = tacc[c];
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int k = __shfl_up_sync(0xffffffffu, trail, d);
+      const bool ok = lane >= d && k == trail;
+#pragma unroll
+      for (int c = 0; c < NV; ++c) {
+        const float t = __shfl_up_sync(0xffffffffu, S[c], d);
+        if (ok) S[c] += t;
+      }
+    }
+    const int prev_trail = __shfl_up_sync(0xffffffffu, trail, 1);
+    float carry[NV];
+#pragma unroll
+    for (int c = 0; c < NV; ++c) {
+      const float t = __shfl_up_sync(0xffffffffu, S[c], 1);
+      carry[c] = (lane > 0 && prev_trail == lead) ? t : 0.f;
+    }
+    const int next_lead = __shfl_down_sync(0xffffffffu, lead, 1);
+    const int next_trail = __shfl_down_sync(0xffffffffu, trail, 1);
+    if (cur >= 0 && nseg > 0 && lead >= 1 && lead <= nbins) {
+#pragma unroll
+      for (int c = 0; c < NV; ++c) my[(size_t)(lead - 1) * NV + c] += facc[c] + carry[c];
+    }
+    const bool next_takes = lane < 31 && next_lead == trail;
+    const bool next_continues = lane < 31 && next_trail == trail;
+    if (cur >= 0 && !next_takes && !next_continues && trail >= 1 && trail <= nbins) {
+#pragma unroll
+      for (int c = 0; c < NV; ++c) my[(size_t)(trail - 1) * NV + c] += S[c];
+    }
+    __syncwarp();
+  }
+  __syncthreads();  // warp partials (float32) finished in float64, in warp order
+  double *outp = partials + (size_t)blockIdx.x * hist_len;
+  for (int q = threadIdx.x; q < hist_len; q += blockDim.x) {
+    double a = 0.;
+    for (int w = 0; w < nwarps; ++w) a += (double)s.hist[(size_t)w * hist_len + q];
+    outp[q] = a;
+  }
+}
+
+template <int NV, bool CROSS>
+static pk_status launch_global(cudaStream_t st, const BinGeom &g, const float2 *d1,
+                               const float2 *d2, const float los[3], const LegendreCoefs &lc,
+                               int zero_l0, const float *edges, double *out, void *workspace,
+                               size_t workspace_bytes) {
+  BinLaunch L;
+  PK_REQUIRE(plan_bins(g.d, g.nedges, NV, &L, sizeof(float)), PK_ERR_RANGE,
+             "too many bins x values (%d x %d) for the shared-memory histograms", g.nedges - 1, NV);
+  PK_REQUIRE(workspace && workspace_bytes >= L.partial_bytes, PK_ERR_WORKSPACE,
+             "binning workspace too small: need %zu bytes, got %zu", L.partial_bytes,
+             workspace_bytes);
+  double *partials = static_cast<double *>(workspace);
+  PK_CUDA(cudaFuncSetAttribute(bin_global_kernel<NV, CROSS>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
+  bin_global_kernel<NV, CROSS><<<L.blocks, L.nwarps * 32, L.smem, st>>>(
+      g, d1, d2, los[0], los[1], los[2], lc, zero_l0, edges, L.nwarps, L.tab, partials);
+  PK_LAUNCH_CHECK();
+  const int hist_len = (g.nedges - 1) * NV;
+  bin_finalize_kernel<<<(hist_len + 255) / 256, 256, 0, st>>>(partials, L.blocks, hist_len, NV,
+                                                              g.nedges - 1, 0, out, nullptr);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+// Dispatch a runtime value count (1..MAX_ELLS) to the compile-time kernels.
+template <template <int> class OpT, class Fill>
+static pk_status dispatch_nv(int nv, Fill fill, cudaStream_t s, const BinGeom &g,
+                             const float *edges, bool rows, int accumulate, double *out,
+                             void *workspace, size_t workspace_bytes) {
+  switch (nv) {
+#define PK_NV_CASE(N)                                                                   \
+  case N: {                                                                             \
+    OpT<N> op;                                                                          \
+    fill(op);                                                                           \
+    return launch_bins<N>(s, g, op, edges, rows, accumulate, out, nullptr, workspace,   \
+                          workspace_bytes);                                             \
+  }
+    PK_NV_CASE(1) PK_NV_CASE(2) PK_NV_CASE(3) PK_NV_CASE(4) PK_NV_CASE(5) PK_NV_CASE(6)
+    PK_NV_CASE(7) PK_NV_CASE(8) PK_NV_CASE(9)
+#undef PK_NV_CASE
+    default:
+      set_error("unsupported number of multipoles %d", nv);
+      return PK_ERR_INVALID;
+  }
 }
 
 static pk_status make_geom(const int32_t meshsize[3], const float kfun[3], int nedges, float step,
@@ -378,12 +803,14 @@ extern "C" pk_status pk_bin_workspace_size(const int32_t meshsize[3], int nedges
              "invalid nedges / nvalues");
   size_t most = 0;
   for (int nv = 1; nv <= MAX_ELLS; ++nv) {  // launches pick their grid from nv
-    BinLaunch L;
-    if (!plan_bins(d, nedges, nv, &L)) {
-      PK_REQUIRE(nv > nvalues, PK_ERR_RANGE, "too many bins x values for the histograms");
-      break;
+    for (size_t elem : {sizeof(double), sizeof(float)}) {  // float64 / float32 warp histograms
+      BinLaunch L;
+      if (!plan_bins(d, nedges, nv, &L, elem)) {
+        PK_REQUIRE(nv > nvalues, PK_ERR_RANGE, "too many bins x values for the histograms");
+        continue;
+      }
+      if (L.partial_bytes > most) most = L.partial_bytes;
     }
-    if (L.partial_bytes > most) most = L.partial_bytes;
   }
   *bytes = most;
   return PK_OK;
@@ -397,8 +824,8 @@ extern "C" pk_status pk_bin_modes(void *stream, const int32_t meshsize[3], const
   pk_status st = make_geom(meshsize, kfun, nedges, step, backend, &g);
   if (st) return st;
   PK_REQUIRE(d_edges && d_nmodes && d_ksum, PK_ERR_INVALID, "null pointer");
-  return launch_bins((cudaStream_t)stream, g, ModesOp(), d_edges, 2, 2, 0, d_nmodes, d_ksum,
-                     workspace, workspace_bytes);
+  return launch_bins<2>((cudaStream_t)stream, g, ModesOp(), d_edges, true, 0, d_nmodes, d_ksum,
+                        workspace, workspace_bytes);
 }
 
 extern "C" pk_status pk_bin_mesh(void *stream, const void *value, const int32_t meshsize[3],
@@ -412,8 +839,8 @@ extern "C" pk_status pk_bin_mesh(void *stream, const void *value, const int32_t 
   MeshOp op;
   op.v = (const float2 *)value;
   op.remove_zero = remove_zero;
-  return launch_bins((cudaStream_t)stream, g, op, d_edges, 2, 2, 0, d_out, nullptr, workspace,
-                     workspace_bytes);
+  return launch_bins<2>((cudaStream_t)stream, g, op, d_edges, true, 0, d_out, nullptr, workspace,
+                        workspace_bytes);
 }
 
 extern "C" pk_status pk_bin_global(void *stream, const void *delta1, const void *delta2,
@@ -426,18 +853,33 @@ extern "C" pk_status pk_bin_global(void *stream, const void *delta1, const void 
   if (st) return st;
   PK_REQUIRE(delta1 && d_edges && d_out && los && ells, PK_ERR_INVALID, "null pointer");
   PK_REQUIRE(nells >= 1 && nells <= MAX_ELLS, PK_ERR_INVALID, "nells must be in 1..%d", MAX_ELLS);
-  GlobalOp op;
-  op.d1 = (const float2 *)delta1;
-  op.d2 = (const float2 *)delta2;
-  for (int a = 0; a < 3; ++a) op.los[a] = los[a];
-  op.nells = nells;
+  for (int l = 0; l < nells; ++l)
+    PK_REQUIRE(ells[l] >= 0 && ells[l] <= 8, PK_ERR_INVALID, "ell must be in 0..8");
+  LegendreCoefs lc;
+  lc.any_odd = 0;
+  int zero_l0 = 0;
   for (int l = 0; l < MAX_ELLS; ++l) {
-    op.ells[l] = l < nells ? ells[l] : 0;
-    PK_REQUIRE(l >= nells || (ells[l] >= 0 && ells[l] <= 8), PK_ERR_INVALID,
-               "ell must be in 0..8");
+    const int ell = l < nells ? ells[l] : 0;
+    legendre_coefs(ell, lc.c[l], &lc.odd[l]);
+    lc.any_odd |= (l < nells) && lc.odd[l];
+    if (l < nells && ell == 0) zero_l0 |= 1 << l;  // ell = 0 keeps the k = 0 mode
   }
-  return launch_bins((cudaStream_t)stream, g, op, d_edges, nells, nells, 0, d_out, nullptr,
-                     workspace, workspace_bytes);
+  cudaStream_t cs = (cudaStream_t)stream;
+  const float2 *a = (const float2 *)delta1, *b = (const float2 *)delta2;
+  switch (nells * 2 + (b ? 1 : 0)) {
+#define PK_GL_CASE(N)                                                                           \
+  case 2 * N:                                                                                   \
+    return launch_global<N, false>(cs, g, a, b, los, lc, zero_l0, d_edges, d_out, workspace,    \
+                                   workspace_bytes);                                            \
+  case 2 * N + 1:                                                                               \
+    return launch_global<N, true>(cs, g, a, b, los, lc, zero_l0, d_edges, d_out, workspace,     \
+                                  workspace_bytes);
+    PK_GL_CASE(1) PK_GL_CASE(2) PK_GL_CASE(3) PK_GL_CASE(4) PK_GL_CASE(5) PK_GL_CASE(6)
+    PK_GL_CASE(7) PK_GL_CASE(8) PK_GL_CASE(9)
+#undef PK_GL_CASE
+  }
+  set_error("unsupported number of multipoles %d", nells);
+  return PK_ERR_INVALID;
 }
 
 extern "C" pk_status pk_bin_firstpoint(void *stream, const void *a0, const void *b0,
@@ -455,22 +897,24 @@ extern "C" pk_status pk_bin_firstpoint(void *stream, const void *a0, const void 
              MAX_FP_TERMS);
   PK_REQUIRE(nterms == 0 || (f && term_ell && term_m), PK_ERR_INVALID, "null term arrays");
   PK_REQUIRE(nells >= 1 && nells <= MAX_ELLS, PK_ERR_INVALID, "nells must be in 1..%d", MAX_ELLS);
-  FirstPointOp op;
-  op.a0 = (const float2 *)a0;
-  op.b0 = (const float2 *)b0;
-  op.f = (const float2 *)f;
-  op.fstride = g.d.ncomplex();
-  op.nterms = nterms;
-  for (int t = 0; t < MAX_FP_TERMS; ++t) {
-    op.term_ell[t] = t < nterms ? term_ell[t] : -1;
-    op.term_m[t] = t < nterms ? term_m[t] : 0;
-    PK_REQUIRE(t >= nterms || (term_ell[t] >= 0 && term_ell[t] <= YLM_LMAX &&
-                               term_m[t] >= -term_ell[t] && term_m[t] <= term_ell[t]),
+  for (int t = 0; t < nterms; ++t)
+    PK_REQUIRE(term_ell[t] >= 0 && term_ell[t] <= YLM_LMAX && term_m[t] >= -term_ell[t] &&
+                   term_m[t] <= term_ell[t],
                PK_ERR_INVALID, "invalid (ell, m)");
-  }
-  op.nells = nells;
-  for (int l = 0; l < MAX_ELLS; ++l) op.ells[l] = l < nells ? ells[l] : 0;
-  op.include_ell0 = include_ell0;
-  return launch_bins((cudaStream_t)stream, g, op, d_edges, nells, nells, accumulate, d_out,
-                     nullptr, workspace, workspace_bytes);
+  const int64_t stride = g.d.ncomplex();
+  auto fill = [&](auto &op) {
+    op.a0 = (const float2 *)a0;
+    op.b0 = (const float2 *)b0;
+    op.f = (const float2 *)f;
+    op.fstride = stride;
+    op.nterms = nterms;
+    for (int t = 0; t < MAX_FP_TERMS; ++t) {
+      op.term_ell[t] = t < nterms ? term_ell[t] : -1;
+      op.term_m[t] = t < nterms ? term_m[t] : 0;
+    }
+    for (int l = 0; l < MAX_ELLS; ++l) op.ells[l] = l < nells ? ells[l] : 0;
+    op.include_ell0 = include_ell0;
+  };
+  return dispatch_nv<FirstPointOp>(nells, fill, (cudaStream_t)stream, g, d_edges, false,
+                                   accumulate, d_out, workspace, workspace_bytes);
 }

@@ -35,11 +35,9 @@ __device__ __forceinline__ float sinc_of(float kc) {
   return __fdiv_rn(sinf(px), px);
 }
 
-// (prod_d sinc)^(-order): lax.integer_pow by binary exponentiation, then 1/acc.
-__device__ __forceinline__ float compensation(const FourierParams &p, float k0, float k1,
-                                              float k2) {
-  float ker = __fmul_rn(__fmul_rn(sinc_of(k0), sinc_of(k1)), sinc_of(k2));
-  int y = p.comp_order;
+// (window)^(-order): lax.integer_pow by binary exponentiation, then the reciprocal.
+__device__ __forceinline__ float inverse_power(float ker, int order) {
+  int y = order;
   float acc = 1.f, x = ker;
   bool first = true;
   while (y > 0) {
@@ -54,76 +52,144 @@ __device__ __forceinline__ float compensation(const FourierParams &p, float k0, 
 }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(__fsub_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)),
-                     __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// Interlaced + compensated value of stored mode (i, j, z).
-__device__ __forceinline__ float2 combine(const FourierParams &p, const float2 *__restrict__ in,
-                                          int i, int j, int z) {
+__device__ __forceinline__ float2 expi(float t) {
+  float sn, cs;
+  sincosf(t, &sn, &cs);
+  return make_float2(cs, sn);
+}
+
+constexpr int IL_THREADS = 256;
+constexpr int IL_MAX_SHIFTS = 8;
+
+// Per-CTA table along kz (shared memory): for each shift s, e^{i s kz(z)} and, for the
+// 'jaxdecomp' semantics, e^{-i s kz(-z)} on the full grid; plus sinc(kz / 2pi).
+struct ZTable {
+  float2 *ph;    // [nshifts][nz]
+  float2 *phm;   // [nshifts][nz] (jaxdecomp)
+  float *sinc;   // [nz]
+};
+
+// Row factors: prod over x, y of the phase (divided by I) and of the sinc window.
+template <int NS>
+struct RowFactor {
+  float2 ph[NS];
+  float2 phm[NS];
+  float sinc;
+};
+
+template <int NS, bool FULL>
+__device__ __forceinline__ void row_factor(const FourierParams &p, int i, int j, RowFactor<NS> &r) {
   const Dims &d = p.d;
-  const bool full = p.backend == PK_BACKEND_JAXDECOMP;
+  constexpr bool full = FULL;
   const float k0 = ccoord(i, d.n0, p.cspacing[0], false);
   const float k1 = ccoord(j, d.n1, p.cspacing[1], false);
-  const float k2 = ccoord(z, d.n2, p.cspacing[2], !full);
-  const int64_t idx = ((int64_t)i * d.n1 + j) * d.nz + z;
+  const float kxy = k0 + k1;
+  const int i2 = (d.n0 - i) % d.n0, j2 = (d.n1 - j) % d.n1;
+  const float kxym = ccoord(i2, d.n0, p.cspacing[0], false) + ccoord(j2, d.n1, p.cspacing[1], false);
+  const float inv = 1.f / p.interlacing;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const float2 e = expi(p.shifts[s] * kxy);
+    r.ph[s] = make_float2(e.x * inv, e.y * inv);
+    if (full) {
+      const float2 m = expi(-p.shifts[s] * kxym);
+      r.phm[s] = make_float2(m.x * inv, m.y * inv);
+    }
+  }
+  r.sinc = p.comp_order > 0 ? __fmul_rn(sinc_of(k0), sinc_of(k1)) : 1.f;
+}
+
+// Interlaced + compensated value of stored mode (row r, z).
+template <int NS, bool FULL>
+__device__ __forceinline__ float2 combine_mode(const FourierParams &p, const RowFactor<NS> &r,
+                                               const ZTable &t, const float2 *__restrict__ in,
+                                               int64_t idx, int z) {
+  constexpr bool full = FULL;
   float2 acc;
-  if (p.nshifts == 1 && p.shifts[0] == 0.f) {
+  if (NS == 1) {
     acc = in[idx];
   } else {
-    const float ksum = __fadd_rn(__fadd_rn(k0, k1), k2);
-    float ksum_neg = 0.f;
-    if (full) {  // circular coordinates of the mirrored mode -k on the full grid
-      const int in0 = (d.n0 - i) % d.n0, in1 = (d.n1 - j) % d.n1, in2 = (d.n2 - z) % d.n2;
-      ksum_neg = __fadd_rn(__fadd_rn(ccoord(in0, d.n0, p.cspacing[0], false),
-                                     ccoord(in1, d.n1, p.cspacing[1], false)),
-                           ccoord(in2, d.n2, p.cspacing[2], false));
-    }
     acc = make_float2(0.f, 0.f);
-    for (int s = 0; s < p.nshifts; ++s) {
-      const float2 v = in[(int64_t)s * d.ncomplex() + idx];
-      float sn, cs;
-      sincosf(__fmul_rn(p.shifts[s], ksum), &sn, &cs);
-      float2 ph = make_float2(cs, sn);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const float2 v = in[(int64_t)s * p.d.ncomplex() + idx];
+      float2 ph = cmul(r.ph[s], t.ph[s * p.d.nz + z]);
       if (full) {  // Hermitian part of the full-grid phase: (e^{i t(k)} + e^{-i t(-k)}) / 2
-        float sn2, cs2;
-        sincosf(__fmul_rn(p.shifts[s], ksum_neg), &sn2, &cs2);
-        ph = make_float2(0.5f * (cs + cs2), 0.5f * (sn - sn2));
+        const float2 m = cmul(r.phm[s], t.phm[s * p.d.nz + z]);
+        ph = make_float2(0.5f * (ph.x + m.x), 0.5f * (ph.y + m.y));
       }
-      float2 t = cmul(v, ph);
-      t.x = __fdiv_rn(t.x, p.interlacing);  // value * phase / interlacing
-      t.y = __fdiv_rn(t.y, p.interlacing);
-      acc.x = __fadd_rn(acc.x, t.x);
-      acc.y = __fadd_rn(acc.y, t.y);
+      const float2 c = cmul(v, ph);
+      acc.x += c.x;
+      acc.y += c.y;
     }
   }
   if (p.comp_order > 0) {
-    const float c = compensation(p, k0, k1, k2);
-    acc.x = __fmul_rn(acc.x, c);
-    acc.y = __fmul_rn(acc.y, c);
+    const float c = inverse_power(__fmul_rn(r.sinc, t.sinc[z]), p.comp_order);
+    acc.x *= c;
+    acc.y *= c;
   }
   return acc;
 }
 
-__global__ void interlace_kernel(FourierParams p, const float2 *__restrict__ in,
-                                 float2 *__restrict__ out) {
+// One warp per (i, j) row of the Hermitian mesh; lanes stride kz (coalesced).
+template <int NS, bool FULL>
+__global__ void __launch_bounds__(IL_THREADS) interlace_kernel(FourierParams p,
+                                                               const float2 *__restrict__ in,
+                                                               float2 *__restrict__ out) {
+  extern __shared__ float4 ilsmem[];
   const Dims d = p.d;
-  const int64_t total = d.ncomplex();
-  const bool even = (d.n2 % 2) == 0;
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int z = (int)(idx % d.nz);
-    const int64_t r = idx / d.nz;
-    const int j = (int)(r % d.n1);
-    const int i = (int)(r / d.n1);
-    float2 v = combine(p, in, i, j, z);
-    if (p.for_c2r && (z == 0 || (even && z == d.nz - 1))) {
-      const float2 m = combine(p, in, (d.n0 - i) % d.n0, (d.n1 - j) % d.n1, z);
-      v = make_float2(0.5f * (v.x + m.x), 0.5f * (v.y - m.y));
+  constexpr bool full = FULL;
+  ZTable t;
+  t.ph = reinterpret_cast<float2 *>(ilsmem);
+  t.phm = t.ph + (size_t)p.nshifts * d.nz;
+  t.sinc = reinterpret_cast<float *>(t.phm + (full ? (size_t)p.nshifts * d.nz : 0));
+  for (int z = threadIdx.x; z < d.nz; z += blockDim.x) {
+    const float k2 = ccoord(z, d.n2, p.cspacing[2], !full);
+    const int zm = (d.n2 - z) % d.n2;
+    const float k2m = ccoord(zm, d.n2, p.cspacing[2], false);
+    for (int s = 0; s < p.nshifts; ++s) {
+      t.ph[s * d.nz + z] = expi(p.shifts[s] * k2);
+      if (full) t.phm[s * d.nz + z] = expi(-p.shifts[s] * k2m);
     }
-    v.x *= p.scale;
-    v.y *= p.scale;
-    out[idx] = v;
+    t.sinc[z] = sinc_of(k2);
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  const int64_t nrows = (int64_t)d.n0 * d.n1;
+  const bool even = (d.n2 % 2) == 0;
+  for (int64_t row = (int64_t)blockIdx.x * nwarps + warp; row < nrows;
+       row += (int64_t)gridDim.x * nwarps) {
+    const int i = (int)(row / d.n1), j = (int)(row % d.n1);
+    RowFactor<NS> rf, rm;
+    row_factor<NS, FULL>(p, i, j, rf);
+    const bool planes = p.for_c2r != 0;
+    const int im = (d.n0 - i) % d.n0, jm = (d.n1 - j) % d.n1;
+    if (planes) row_factor<NS, FULL>(p, im, jm, rm);
+    const int64_t rbase = row * d.nz;
+    const int64_t mbase = ((int64_t)im * d.n1 + jm) * d.nz;
+    // four kz per lane per iteration: 4 * NS independent loads in flight
+    for (int zb = lane; zb < d.nz; zb += 128) {
+      float2 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int z = zb + 32 * u;
+        v[u] = z < d.nz ? combine_mode<NS, FULL>(p, rf, t, in, rbase + z, z) : make_float2(0.f, 0.f);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int z = zb + 32 * u;
+        if (z >= d.nz) break;
+        if (planes && (z == 0 || (even && z == d.nz - 1))) {
+          const float2 m = combine_mode<NS, FULL>(p, rm, t, in, mbase + z, z);
+          v[u] = make_float2(0.5f * (v[u].x + m.x), 0.5f * (v[u].y - m.y));
+        }
+        out[rbase + z] = make_float2(v[u].x * p.scale, v[u].y * p.scale);
+      }
+    }
   }
 }
 
@@ -248,7 +314,7 @@ extern "C" pk_status pk_interlace_compensate(void *stream, const void *in, int n
   PK_REQUIRE(in && out, PK_ERR_INVALID, "null buffer");
   FourierParams p;
   PK_REQUIRE(make_dims(meshsize, &p.d), PK_ERR_INVALID, "invalid meshsize");
-  PK_REQUIRE(nshifts >= 1 && nshifts <= 8, PK_ERR_INVALID, "nshifts must be in 1..8");
+  PK_REQUIRE(nshifts >= 1 && nshifts <= IL_MAX_SHIFTS, PK_ERR_INVALID, "nshifts must be in 1..8");
   PK_REQUIRE(comp_order >= 0 && comp_order <= 4, PK_ERR_INVALID, "comp_order must be in 0..4");
   PK_REQUIRE(backend == PK_BACKEND_JAX || backend == PK_BACKEND_JAXDECOMP, PK_ERR_INVALID,
              "unknown backend %d", backend);
@@ -263,9 +329,33 @@ extern "C" pk_status pk_interlace_compensate(void *stream, const void *in, int n
   p.backend = backend;
   p.for_c2r = for_c2r;
   p.scale = scale;
-  const int threads = 256;
-  interlace_kernel<<<grid_for(p.d.ncomplex(), threads), threads, 0, (cudaStream_t)stream>>>(
-      p, (const float2 *)in, (float2 *)out);
+  const bool full = backend == PK_BACKEND_JAXDECOMP;
+  const size_t smem = ((size_t)nshifts * p.d.nz * (full ? 2 : 1)) * sizeof(float2) +
+                      (size_t)p.d.nz * sizeof(float);
+  PK_REQUIRE(smem <= 200 * 1024, PK_ERR_RANGE, "mesh too large along the last axis for the kz table");
+  const int64_t nrows = (int64_t)p.d.n0 * p.d.n1;
+  const int64_t want = (nrows + IL_THREADS / 32 - 1) / (IL_THREADS / 32);
+  const int64_t cap = 8LL * sm_count();
+  const int blocks = (int)(want < cap ? want : cap);
+  cudaStream_t st = (cudaStream_t)stream;
+  switch (nshifts * 2 + (full ? 1 : 0)) {
+#define PK_IL_CASE(N)                                                                          \
+  case 2 * N:                                                                                  \
+    PK_CUDA(cudaFuncSetAttribute(interlace_kernel<N, false>,                                   \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));     \
+    interlace_kernel<N, false><<<blocks, IL_THREADS, smem, st>>>(p, (const float2 *)in,        \
+                                                                 (float2 *)out);               \
+    break;                                                                                     \
+  case 2 * N + 1:                                                                              \
+    PK_CUDA(cudaFuncSetAttribute(interlace_kernel<N, true>,                                    \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));     \
+    interlace_kernel<N, true><<<blocks, IL_THREADS, smem, st>>>(p, (const float2 *)in,         \
+                                                                (float2 *)out);                \
+    break;
+    PK_IL_CASE(1) PK_IL_CASE(2) PK_IL_CASE(3) PK_IL_CASE(4) PK_IL_CASE(5) PK_IL_CASE(6)
+    PK_IL_CASE(7) PK_IL_CASE(8)
+#undef PK_IL_CASE
+  }
   PK_LAUNCH_CHECK();
   return PK_OK;
 }

@@ -45,7 +45,10 @@ __device__ __forceinline__ float normalise(float p, float half, float center, fl
 }
 
 __device__ __forceinline__ int wrapi(int i, int n) {
-  int r = i % n;
+  if (i >= 0 && i < n) return i;
+  if (i < 0 && i >= -n) return i + n;
+  if (i >= n && i < 2 * n) return i - n;
+  const int r = i % n;
   return r < 0 ? r + n : r;
 }
 
@@ -97,9 +100,18 @@ __device__ __forceinline__ int base_index(int order, float u) {
 
 __device__ __forceinline__ int offset_lo(int order) { return -((order - 1) / 2); }
 
-// Distinct tiles of the wrapped cell span [c - lo, c + hi] along one axis.
+// Distinct tiles of the wrapped cell span [c - lo, c + hi] along one axis.  When every
+// tile on the axis is at least as long as the span (the usual case), the span touches the
+// tiles of its two ends only.
 __device__ __forceinline__ int span_tiles(int c, int lo, int hi, int n, int tile, int nt,
                                           int out[3]) {
+  const int last = n - (nt - 1) * tile;
+  if (last >= lo + hi || nt == 1) {
+    const int a = wrapi(c - lo, n) / tile, b = wrapi(c + hi, n) / tile;
+    out[0] = a;
+    out[1] = b;
+    return a == b ? 1 : 2;
+  }
   int count = 0;
   for (int x = c - lo; x <= c + hi; ++x) {
     int t = wrapi(x, n) / tile;
@@ -125,6 +137,9 @@ __device__ __forceinline__ bool load_particle(const PaintGeom &g, const float *p
   return ok;
 }
 
+// Warp-aggregated tile counting / filling: lanes of a warp that reach the same tile
+// combine into one global atomic (the catalog is often sorted by cell, so neighbours
+// usually share tiles).
 template <bool FILL>
 __global__ void bucket_kernel(PaintGeom g, const float *__restrict__ pos,
                               const float *__restrict__ w, int64_t n,
@@ -133,121 +148,178 @@ __global__ void bucket_kernel(PaintGeom g, const float *__restrict__ pos,
                               unsigned *__restrict__ wmax_bits, int *__restrict__ status) {
   const int tiles[3] = {TILE0, TILE1, TILE2};
   const int ns[3] = {g.d.n0, g.d.n1, g.d.n2};
-  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
-       p += (int64_t)gridDim.x * blockDim.x) {
-    float u[3], wp;
-    if (!load_particle(g, pos, w, p, u, &wp) || !isfinite(wp)) {
-      if (!FILL && status) atomicExch(status, 1);
-      continue;
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t base = warp * 32; base < n; base += nwarps * 32) {
+    const int64_t p = base + lane;
+    float u[3] = {0.f, 0.f, 0.f}, wp = 0.f;
+    bool ok = false;
+    if (p < n) {
+      ok = load_particle(g, pos, w, p, u, &wp) && isfinite(wp);
+      if (!ok && !FILL && status) atomicExch(status, 1);
     }
-    if (!FILL) atomicMax(wmax_bits, __float_as_uint(fabsf(wp)));
-    int t[3][3], nt[3];
+    if (!FILL) {
+      const unsigned wb = __reduce_max_sync(FULL, ok ? __float_as_uint(fabsf(wp)) : 0u);
+      if (lane == 0 && wb) atomicMax(wmax_bits, wb);
+    }
+    int t[3][3], nt[3] = {0, 0, 0};
+    if (ok) {
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      int c = (int)floorf(u[d]);
-      nt[d] = span_tiles(c, g.reach_lo, g.reach_hi, ns[d], tiles[d], g.nt[d], t[d]);
+      for (int d = 0; d < 3; ++d) {
+        const int c = (int)floorf(u[d]);
+        nt[d] = span_tiles(c, g.reach_lo, g.reach_hi, ns[d], tiles[d], g.nt[d], t[d]);
+      }
     }
-    for (int a = 0; a < nt[0]; ++a)
-      for (int b = 0; b < nt[1]; ++b)
-        for (int c = 0; c < nt[2]; ++c) {
-          int tile = (t[0][a] * g.nt[1] + t[1][b]) * g.nt[2] + t[2][c];
-          if (!FILL) {
-            atomicAdd(counts + tile, 1u);
-          } else {
-            unsigned slot = atomicAdd(cursors + tile, 1u);
-            bucket[(int64_t)offsets[tile] + slot] = make_float4(u[0], u[1], u[2], wp);
-          }
-        }
+    const int ncopy = nt[0] * nt[1] * nt[2];
+    const int most = __reduce_max_sync(FULL, ncopy);
+    for (int k = 0; k < most; ++k) {
+      const bool act = k < ncopy;
+      const unsigned mask = __ballot_sync(FULL, act);
+      if (!act) continue;
+      const int c2 = k % nt[2], c1 = (k / nt[2]) % nt[1], c0 = k / (nt[2] * nt[1]);
+      const int tile = (t[0][c0] * g.nt[1] + t[1][c1]) * g.nt[2] + t[2][c2];
+      // one global atomic per distinct tile in the warp (sorted catalogs share tiles)
+      const int first = __ffs(mask) - 1;
+      const bool same = __all_sync(mask, tile == __shfl_sync(mask, tile, first));
+      const unsigned peers = same ? mask : __match_any_sync(mask, tile);
+      const int leader = __ffs(peers) - 1;
+      const unsigned group = __popc(peers);
+      if (!FILL) {
+        if (lane == leader) atomicAdd(counts + tile, group);
+      } else {
+        unsigned base0 = 0;
+        if (lane == leader) base0 = atomicAdd(cursors + tile, group);
+        const unsigned slot = __shfl_sync(peers, base0, leader) + __popc(peers & ((1u << lane) - 1u));
+        bucket[(int64_t)offsets[tile] + slot] = make_float4(u[0], u[1], u[2], wp);
+      }
+    }
   }
 }
 
-// 2^e with e chosen so that n * max|w| * 2^e < 2^62: exact fixed point.
-__device__ __forceinline__ double fixed_scale(unsigned wmax_bits, int64_t n) {
-  float wmax = __uint_as_float(wmax_bits);
-  if (!(wmax > 0.f) || !isfinite(wmax)) return 1099511627776.0;  // 2^40
-  int ew;
-  frexpf(wmax, &ew);  // wmax < 2^ew
-  int en = 64 - __clzll((unsigned long long)(n > 0 ? n : 1));  // n < 2^en
-  int e = 62 - ew - en;
-  return ldexp(1.0, e);
+// Fixed-point exponent e such that count * max|w| * 2^e < 2^62: every partial sum of a
+// tile's cells fits in a signed 64-bit integer (each particle adds at most |w| in total).
+__device__ __forceinline__ int fixed_exponent(unsigned wmax_bits, unsigned count) {
+  const float wmax = __uint_as_float(wmax_bits);
+  if (!(wmax > 0.f) || !isfinite(wmax)) return 40;
+  const int ew = (int)((wmax_bits >> 23) & 0xff) - 126;  // wmax < 2^ew
+  const int en = 32 - __clz(count > 0 ? count : 1);       // count < 2^en
+  return 62 - ew - en;
 }
 
-__global__ void __launch_bounds__(256) paint_tiles_kernel(
+__device__ __forceinline__ unsigned gcd_u(unsigned a, unsigned b) {
+  while (b) {
+    const unsigned t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+constexpr int PAINT_THREADS = 512;
+
+template <int ORDER>
+__global__ void __launch_bounds__(PAINT_THREADS) paint_tiles_kernel(
     PaintGeom g, const float4 *__restrict__ bucket, const int *__restrict__ offsets,
     const unsigned *__restrict__ wmax_bits, int64_t n, float *__restrict__ out) {
-  extern __shared__ unsigned long long acc[];  // [nshifts][TILE_CELLS]
+  // Per-cell 64-bit fixed point as two 32-bit words (native shared atomics): the low word's
+  // returned old value gives the exact carry into the high word, so the integer sum stays
+  // exact and independent of the order of the additions.
+  extern __shared__ unsigned acc32[];  // lo[nshifts][TILE_CELLS], hi[nshifts][TILE_CELLS]
+  __shared__ unsigned s_mult;
   const int tile = blockIdx.x;
   const int t2i = tile % g.nt[2];
   const int t1i = (tile / g.nt[2]) % g.nt[1];
   const int t0i = tile / (g.nt[2] * g.nt[1]);
-  const int lo0 = t0i * TILE0, lo1 = t1i * TILE1, lo2 = t2i * TILE2;
+  const int los[3] = {t0i * TILE0, t1i * TILE1, t2i * TILE2};
   const int begin = offsets[tile], end = offsets[tile + 1];
-  const int ncell = g.nshifts * TILE_CELLS;
-  const bool empty = (begin == end);
+  const unsigned count = (unsigned)(end - begin);
+  const bool vec = (g.d.n2 % 4) == 0;
 
-  if (!empty) {
-    for (int i = threadIdx.x; i < ncell; i += blockDim.x) acc[i] = 0ull;
+  if (count > 0) {
+    for (int i = threadIdx.x; i < 2 * g.nshifts * TILE_CELLS; i += blockDim.x) acc32[i] = 0u;
+    if (threadIdx.x == 0) {  // Fibonacci-hash stride coprime with count: a permutation
+      unsigned a = count > 2 ? ((unsigned)(0.6180339887 * count) | 1u) : 1u;
+      while (gcd_u(a, count) != 1u) a += 2u;
+      s_mult = a;
+    }
     __syncthreads();
-    const double scale = fixed_scale(*wmax_bits, n);
-    const int order = g.order;
-    const int olo = offset_lo(order);
-    for (int p = begin + threadIdx.x; p < end; p += blockDim.x) {
-      const float4 q = bucket[p];
+    const int fexp = fixed_exponent(*wmax_bits, count);
+    const float fscale = ldexpf(1.f, fexp);  // exact power-of-two scaling of each contribution
+    const unsigned mult = s_mult;
+    const int ns[3] = {g.d.n0, g.d.n1, g.d.n2};
+    const int tl[3] = {TILE0, TILE1, TILE2};
+    constexpr int OLO = -((ORDER - 1) / 2);
+    // permuted visiting order jdx = i * mult mod count, advanced incrementally
+    unsigned jdx = (unsigned)(((unsigned long long)threadIdx.x * mult) % count);
+    const unsigned jstep = (unsigned)(((unsigned long long)blockDim.x * mult) % count);
+    for (unsigned i = threadIdx.x; i < count; i += blockDim.x) {
+      const float4 q = bucket[begin + jdx];
+      jdx += jstep;
+      if (jdx >= count) jdx -= count;
       const float uq[3] = {q.x, q.y, q.z};
       for (int s = 0; s < g.nshifts; ++s) {
-        float k[3][MAX_ORDER];
-        int l[3][MAX_ORDER];
-        const int ns[3] = {g.d.n0, g.d.n1, g.d.n2};
-        const int los[3] = {lo0, lo1, lo2};
-        const int tl[3] = {TILE0, TILE1, TILE2};
+        float k[3][ORDER];
+        int l[3][ORDER];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
           const float u = __fadd_rn(uq[d], g.shifts[s]);
-          const int i0 = base_index(order, u);
+          const float fi0 = (ORDER & 1) ? rintf(u) : floorf(u);
+          const int i0 = (int)fi0;
+          // tile-relative cell of the first stencil point; stencil stays within one period
+          const int w0 = wrapi(i0 + OLO, ns[d]) - los[d];
 #pragma unroll
-          for (int o = 0; o < MAX_ORDER; ++o) {
-            if (o < order) {
-              const int idx = i0 + olo + o;
-              const float sd = fabsf(__fsub_rn((float)idx, u));
-              k[d][o] = bspline(order, sd);
-              int loc = wrapi(idx, ns[d]) - los[d];
-              l[d][o] = (loc >= 0 && loc < tl[d]) ? loc : -1;
-            }
+          for (int o = 0; o < ORDER; ++o) {
+            // (float)(i0 + OLO + o) exactly, without an int -> float conversion
+            k[d][o] = bspline(ORDER, fabsf(__fsub_rn(__fadd_rn(fi0, (float)(OLO + o)), u)));
+            int loc = w0 + o;
+            while (loc >= ns[d] - los[d]) loc -= ns[d];  // wrapped past the mesh end
+            l[d][o] = (loc >= 0 && loc < tl[d]) ? loc : -1;
           }
         }
-        unsigned long long *as = acc + s * TILE_CELLS;
-        for (int a = 0; a < order; ++a) {
-          if (l[0][a] < 0) continue;
-          for (int b = 0; b < order; ++b) {
-            if (l[1][b] < 0) continue;
+        unsigned *alo = acc32 + s * TILE_CELLS;
+        unsigned *ahi = acc32 + (g.nshifts + s) * TILE_CELLS;
+        const float wq = q.w;
+#pragma unroll
+        for (int a = 0; a < ORDER; ++a) {
+#pragma unroll
+          for (int b = 0; b < ORDER; ++b) {
             const float kab = __fmul_rn(k[0][a], k[1][b]);
+            const bool vab = (l[0][a] | l[1][b]) >= 0;
             const int rowoff = (l[0][a] * TILE1 + l[1][b]) * TILE2;
-            for (int c = 0; c < order; ++c) {
-              if (l[2][c] < 0) continue;
-              const float v = __fmul_rn(q.w, __fmul_rn(kab, k[2][c]));
-              const long long fx = __double2ll_rn((double)v * scale);
-              atomicAdd(as + rowoff + l[2][c], (unsigned long long)fx);
+#pragma unroll
+            for (int c = 0; c < ORDER; ++c) {
+              if (vab && l[2][c] >= 0) {
+                const float v = __fmul_rn(wq, __fmul_rn(kab, k[2][c]));  // weights * ker
+                const long long fx = __float2ll_rn(v * fscale);
+                const unsigned lo = (unsigned)fx;
+                const int cell = rowoff + l[2][c];
+                const unsigned old = atomicAdd(alo + cell, lo);
+                atomicAdd(ahi + cell, (unsigned)((int)(fx >> 32) + (old + lo < old ? 1 : 0)));
+              }
             }
           }
         }
       }
     }
     __syncthreads();
-    // convert and store
-    const double inv = 1.0 / scale;
-    const bool vec = (g.d.n2 % 4) == 0;
+    const double inv = ldexp(1.0, -fexp);
     for (int s = 0; s < g.nshifts; ++s) {
       float *mesh = out + (int64_t)s * g.d.nreal();
-      const unsigned long long *as = acc + s * TILE_CELLS;
+      const unsigned *alo = acc32 + s * TILE_CELLS;
+      const unsigned *ahi = acc32 + (g.nshifts + s) * TILE_CELLS;
       for (int i = threadIdx.x * 4; i < TILE_CELLS; i += blockDim.x * 4) {
         const int c2 = i % TILE2, c1 = (i / TILE2) % TILE1, c0 = i / (TILE2 * TILE1);
-        const int x0 = lo0 + c0, x1 = lo1 + c1, x2 = lo2 + c2;
+        const int x0 = los[0] + c0, x1 = los[1] + c1, x2 = los[2] + c2;
         if (x0 >= g.d.n0 || x1 >= g.d.n1) continue;
         const int64_t base = ((int64_t)x0 * g.d.n1 + x1) * g.d.n2 + x2;
         float v[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-          v[j] = __double2float_rn((double)(long long)as[i + j] * inv);
+        for (int j = 0; j < 4; ++j) {  // exact integer -> double, one rounding to float
+          const long long fx = (long long)(((unsigned long long)ahi[i + j] << 32) | alo[i + j]);
+          v[j] = __double2float_rn((double)fx * inv);
+        }
         if (vec) {
           if (x2 < g.d.n2) *reinterpret_cast<float4 *>(mesh + base) = make_float4(v[0], v[1], v[2], v[3]);
         } else {
@@ -258,12 +330,11 @@ __global__ void __launch_bounds__(256) paint_tiles_kernel(
       }
     }
   } else {
-    const bool vec = (g.d.n2 % 4) == 0;
     for (int s = 0; s < g.nshifts; ++s) {
       float *mesh = out + (int64_t)s * g.d.nreal();
       for (int i = threadIdx.x * 4; i < TILE_CELLS; i += blockDim.x * 4) {
         const int c2 = i % TILE2, c1 = (i / TILE2) % TILE1, c0 = i / (TILE2 * TILE1);
-        const int x0 = lo0 + c0, x1 = lo1 + c1, x2 = lo2 + c2;
+        const int x0 = los[0] + c0, x1 = los[1] + c1, x2 = los[2] + c2;
         if (x0 >= g.d.n0 || x1 >= g.d.n1) continue;
         const int64_t base = ((int64_t)x0 * g.d.n1 + x1) * g.d.n2 + x2;
         if (vec) {
@@ -482,10 +553,18 @@ extern "C" pk_status pk_paint(void *stream, const float *positions, const float 
                                                    cursors, bucket, nullptr, nullptr);
     PK_LAUNCH_CHECK();
   }
-  const size_t smem = (size_t)nshifts * TILE_CELLS * sizeof(unsigned long long);
-  PK_CUDA(cudaFuncSetAttribute(paint_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem));
-  paint_tiles_kernel<<<(unsigned)L.ntiles, 256, smem, s>>>(g, bucket, offsets, wmax, n, out);
+  const size_t smem = (size_t)nshifts * TILE_CELLS * 2 * sizeof(unsigned);
+  switch (order) {
+#define PK_ORDER_CASE(O)                                                                      \
+  case O:                                                                                     \
+    PK_CUDA(cudaFuncSetAttribute(paint_tiles_kernel<O>,                                       \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));    \
+    paint_tiles_kernel<O><<<(unsigned)L.ntiles, PAINT_THREADS, smem, s>>>(g, bucket, offsets, \
+                                                                          wmax, n, out);      \
+    break;
+    PK_ORDER_CASE(1) PK_ORDER_CASE(2) PK_ORDER_CASE(3) PK_ORDER_CASE(4)
+#undef PK_ORDER_CASE
+  }
   PK_LAUNCH_CHECK();
   return PK_OK;
 }
