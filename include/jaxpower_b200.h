@@ -142,6 +142,18 @@ pk_status pk_bin_global(void *stream, const void *delta1, const void *delta2,
                         int nells, const int32_t *ells, double *d_out, void *workspace,
                         size_t workspace_bytes);
 
+/* No counterpart in the reference.  pk_bin_global without a workspace argument, for
+ * callers that cannot allocate device memory when they call (a host callback, or a
+ * foreign runtime that owns the allocator): its scratch is a fixed 16 MiB static device
+ * array, held by every GPU that loads the library until exit.  Returns PK_ERR_RANGE when
+ * the bins x multipoles need more scratch than that.  The first call on a device looks
+ * the array's address up (make it before any stream capture); calls that overlap on the
+ * GPU share the array and race. */
+pk_status pk_bin_global_noalloc(void *stream, const void *delta1, const void *delta2,
+                                const int32_t meshsize[3], const float kfun[3],
+                                const float los[3], const float *d_edges, int nedges, float step,
+                                int backend, int nells, const int32_t *ells, double *d_out);
+
 /* First-point line of sight (mesh2.py:293-344), one batch of (ell, m) terms:
  * d_out[ill * nbins + b] (+)= sum over the bin of w * Re/Im(conj(S_ell) A0),
  * S_ell = sum_{m in batch} F_j(k) Y_ell,m(khat), F_j = r2c(rho Y_ell,m(xhat)).

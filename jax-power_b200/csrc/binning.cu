@@ -15,6 +15,8 @@
 // reproducible run to run.
 #include <math.h>
 
+#include <mutex>
+
 #include "common.cuh"
 #include "ylm_table.cuh"
 
@@ -917,4 +919,61 @@ extern "C" pk_status pk_bin_firstpoint(void *stream, const void *a0, const void 
   };
   return dispatch_nv<FirstPointOp>(nells, fill, (cudaStream_t)stream, g, d_edges, false,
                                    accumulate, d_out, workspace, workspace_bytes);
+}
+
+// ------------------------------------------------------------ allocation-free variant
+// Some callers cannot allocate device memory at the point of the call: code running
+// inside a host callback or a foreign runtime that owns the allocator (an XLA custom
+// call without a scratch operand, a plugin loaded by a host that forbids cudaMalloc after
+// start-up).  pk_bin_global_noalloc takes its scratch (the per-CTA partial histograms of
+// the global-los binning) from this fixed array instead of a caller workspace.
+//
+// - The array is NOALLOC_SCRATCH_BYTES = 16 MiB; every GPU that loads the library holds
+//   it until the process exits.
+// - Host code cannot use the symbol as a device address; the address is looked up once
+//   per device, with that device current, by cudaGetSymbolAddress.  The first call on a
+//   device does this set-up, so make that first call before any stream capture.
+// - Every call shares the array.  Each call overwrites all the partial rows it reads, so
+//   nothing needs clearing between calls, but calls that overlap on the GPU (different
+//   streams, or several host threads) race on it.
+constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)16 << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+static pk_status noalloc_scratch(void **out) {
+  static std::mutex lock;
+  static void *address[256] = {};
+  int dev = 0;
+  PK_CUDA(cudaGetDevice(&dev));
+  PK_REQUIRE(dev >= 0 && dev < 256, PK_ERR_RANGE, "device index %d out of range", dev);
+  std::lock_guard<std::mutex> guard(lock);
+  if (!address[dev]) {
+    void *p = nullptr;
+    PK_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    address[dev] = p;
+  }
+  *out = address[dev];
+  return PK_OK;
+}
+
+extern "C" pk_status pk_bin_global_noalloc(void *stream, const void *delta1, const void *delta2,
+                                           const int32_t meshsize[3], const float kfun[3],
+                                           const float los[3], const float *d_edges, int nedges,
+                                           float step, int backend, int nells, const int32_t *ells,
+                                           double *d_out) {
+  Dims d;
+  PK_REQUIRE(make_dims(meshsize, &d), PK_ERR_INVALID, "invalid meshsize");
+  PK_REQUIRE(nedges >= 2, PK_ERR_INVALID, "need at least 2 edges");
+  PK_REQUIRE(nells >= 1 && nells <= MAX_ELLS, PK_ERR_INVALID, "nells must be in 1..%d", MAX_ELLS);
+  BinLaunch L;
+  PK_REQUIRE(plan_bins(d, nedges, nells, &L, sizeof(float)), PK_ERR_RANGE,
+             "too many bins x multipoles (%d x %d)", nedges - 1, nells);
+  PK_REQUIRE(L.partial_bytes <= NOALLOC_SCRATCH_BYTES, PK_ERR_RANGE,
+             "pk_bin_global_noalloc: %d bins x %d multipoles need %zu bytes of scratch, more than "
+             "the fixed %zu; use pk_bin_global with a workspace",
+             nedges - 1, nells, L.partial_bytes, NOALLOC_SCRATCH_BYTES);
+  void *scratch = nullptr;
+  pk_status st = noalloc_scratch(&scratch);
+  if (st) return st;
+  return pk_bin_global(stream, delta1, delta2, meshsize, kfun, los, d_edges, nedges, step, backend,
+                       nells, ells, d_out, scratch, NOALLOC_SCRATCH_BYTES);
 }
