@@ -174,6 +174,46 @@ pk_status pk_ylm_premultiply(void *stream, const float *rho, const int32_t meshs
                              const float cellsize[3], const float offset[3], int nterms,
                              const int32_t *term_ell, const int32_t *term_m, float *out);
 
+/* ----------------------------------------------------------------- adjoints
+ * Hand-written backward passes (the reference differentiates this path with JAX
+ * autodiff: the transpose of the scatter is resamplers.read, resamplers.py:100-125, FFT
+ * adjoints come from XLA).  Conjugate cotangents are dL/dRe + i dL/dIm.  With
+ * for_c2r / from_real the Fourier-space cotangents are converted so that an
+ * unnormalised C2R yields the cotangent of the real mesh they were transformed from.
+ * Odd multipoles of auto spectra are identically zero and carry no gradient. */
+pk_status pk_adjoint_workspace_size(int nedges, size_t *bytes);
+
+/* Backward of pk_bin_global for an auto spectrum: out = 2 G delta with
+ * G = w_k sum_l coef[l * nbins + b] L_l(mu); coef is float32 (nells, nbins). */
+pk_status pk_bin_global_adjoint(void *stream, const void *delta, const int32_t meshsize[3],
+                                const float kfun[3], const float los[3], const float *d_edges,
+                                int nedges, float step, float edge0, int backend, int nells,
+                                const int32_t *ells, const float *d_coef, int for_c2r, void *out,
+                                void *workspace, size_t workspace_bytes);
+
+/* Backward of pk_bin_firstpoint (auto): cotangents of A0 (written or accumulated) and
+ * of each F_j of the batch (out_f[j]). */
+pk_status pk_bin_firstpoint_adjoint(void *stream, const void *a0, const void *f, int nterms,
+                                    const int32_t *term_ell, const int32_t *term_m,
+                                    const int32_t meshsize[3], const float kfun[3],
+                                    const float *d_edges, int nedges, float step, float edge0,
+                                    int backend, int nells, const int32_t *ells,
+                                    const float *d_coef, int for_c2r, void *out_a0,
+                                    int accumulate_a0, void *out_f, void *workspace,
+                                    size_t workspace_bytes);
+
+/* Backward of pk_interlace_compensate (mesh.py:2737-2752), 'jax' semantics: from the
+ * cotangent of the combined mesh (R = rfftn(rho_bar) if from_real, else the conjugate
+ * cotangent of the complex mesh) to nshifts Hermitian half-meshes whose unnormalised C2R
+ * are the cotangents of the painted shifted meshes. */
+pk_status pk_interlace_adjoint(void *stream, const void *in, int from_real, int nshifts,
+                               const int32_t meshsize[3], int comp_order, int backend, void *out);
+
+/* Backward of pk_ylm_premultiply: rho_bar += sum_j r_j Y_j(xhat). */
+pk_status pk_ylm_accumulate(void *stream, const float *r, const int32_t meshsize[3],
+                            const float cellsize[3], const float offset[3], int nterms,
+                            const int32_t *term_ell, const int32_t *term_m, float *rho_bar);
+
 #ifdef __cplusplus
 }
 #endif

@@ -436,19 +436,46 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_chunks_kernel(BinGeom g, Op o
   bin_smem_flush(s, hist_len, nwarps, partials);
 }
 
-// out[e] (+)= sum over CTAs, in CTA order, transposed to [value][bin].
-__global__ void bin_finalize_kernel(const double *__restrict__ partials, int nblocks,
-                                    int hist_len, int nv, int nbins, int accumulate,
-                                    double *__restrict__ out0, double *__restrict__ out1) {
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < hist_len;
-       e += gridDim.x * blockDim.x) {
+// out[e] (+)= sum over CTAs, transposed to [value][bin].  Deterministic two-level sum:
+// 8 threads per entry each add a fixed contiguous range of CTA rows (4 independent loads
+// in flight), then the 8 partials are added in a fixed order.
+constexpr int FIN_ENTRIES = 32, FIN_SPLIT = 8;
+__global__ void __launch_bounds__(FIN_ENTRIES * FIN_SPLIT) bin_finalize_kernel(
+    const double *__restrict__ partials, int nblocks, int hist_len, int nv, int nbins,
+    int accumulate, double *__restrict__ out0, double *__restrict__ out1) {
+  __shared__ double part[FIN_SPLIT][FIN_ENTRIES];
+  const int le = threadIdx.x % FIN_ENTRIES, sp = threadIdx.x / FIN_ENTRIES;
+  const int e = blockIdx.x * FIN_ENTRIES + le;
+  const int per = (nblocks + FIN_SPLIT - 1) / FIN_SPLIT;
+  const int b0 = sp * per, b1 = min(nblocks, b0 + per);
+  double a0 = 0., a1 = 0., a2 = 0., a3 = 0.;
+  if (e < hist_len) {
+    int b = b0;
+    for (; b + 3 < b1; b += 4) {
+      a0 += partials[(size_t)b * hist_len + e];
+      a1 += partials[(size_t)(b + 1) * hist_len + e];
+      a2 += partials[(size_t)(b + 2) * hist_len + e];
+      a3 += partials[(size_t)(b + 3) * hist_len + e];
+    }
+    for (; b < b1; ++b) a0 += partials[(size_t)b * hist_len + e];
+  }
+  part[sp][le] = (a0 + a1) + (a2 + a3);
+  __syncthreads();
+  if (sp == 0 && e < hist_len) {
     double acc = 0.;
-    for (int b = 0; b < nblocks; ++b) acc += partials[(size_t)b * hist_len + e];
+    for (int k = 0; k < FIN_SPLIT; ++k) acc += part[k][le];
     const int bin = e / nv, c = e % nv;
     double *dst = (c == 1 && out1) ? out1 : out0;
     const int64_t o = (c == 1 && out1) ? bin : (int64_t)c * nbins + bin;
     dst[o] = accumulate ? dst[o] + acc : acc;
   }
+}
+
+static void launch_finalize(cudaStream_t s, const double *partials, int nblocks, int hist_len,
+                            int nv, int nbins, int accumulate, double *out0, double *out1) {
+  const int grid = (hist_len + FIN_ENTRIES - 1) / FIN_ENTRIES;
+  bin_finalize_kernel<<<grid, FIN_ENTRIES * FIN_SPLIT, 0, s>>>(partials, nblocks, hist_len, nv, nbins,
+                                                               accumulate, out0, out1);
 }
 
 struct BinLaunch {
@@ -510,9 +537,7 @@ static pk_status launch_bins(cudaStream_t s, const BinGeom &g, const Op &op, con
   }
   PK_LAUNCH_CHECK();
   const int hist_len = (g.nedges - 1) * NV;
-  const int fb = (hist_len + 255) / 256;
-  bin_finalize_kernel<<<fb, 256, 0, s>>>(partials, L.blocks, hist_len, NV, g.nedges - 1,
-                                         accumulate, out0, out1);
+  launch_finalize(s, partials, L.blocks, hist_len, NV, g.nedges - 1, accumulate, out0, out1);
   PK_LAUNCH_CHECK();
   return PK_OK;
 }
@@ -750,8 +775,7 @@ static pk_status launch_global(cudaStream_t st, const BinGeom &g, const float2 *
       g, d1, d2, los[0], los[1], los[2], lc, zero_l0, edges, L.nwarps, L.tab, partials);
   PK_LAUNCH_CHECK();
   const int hist_len = (g.nedges - 1) * NV;
-  bin_finalize_kernel<<<(hist_len + 255) / 256, 256, 0, st>>>(partials, L.blocks, hist_len, NV,
-                                                              g.nedges - 1, 0, out, nullptr);
+  launch_finalize(st, partials, L.blocks, hist_len, NV, g.nedges - 1, 0, out, nullptr);
   PK_LAUNCH_CHECK();
   return PK_OK;
 }
@@ -976,4 +1000,286 @@ extern "C" pk_status pk_bin_global_noalloc(void *stream, const void *delta1, con
   if (st) return st;
   return pk_bin_global(stream, delta1, delta2, meshsize, kfun, los, d_edges, nedges, step, backend,
                        nells, ells, d_out, scratch, NOALLOC_SCRATCH_BYTES);
+}
+
+// ------------------------------------------------------------------ adjoints
+// Backward of the binned estimators.  Given per-bin cotangent coefficients
+// coef[l][b] (dLoss/dnum_l[b] times the estimator's per-bin factor, e.g. (2l+1)/nmodes),
+// each stored mode gets G_l(k) = w_k coef[l][b(k)] (ell > 0: 0 at k = 0) and the
+// conjugate cotangent (dL/dRe + i dL/dIm) of the mesh(es) it was computed from.  With
+// for_c2r the cotangent is divided by the C2R weight w' (2 off the self-conjugate
+// planes) and Hermitian-symmetrised on the kz = 0 / N/2 planes, so that an unnormalised
+// C2R of it is the cotangent of the real mesh the modes were transformed from.
+
+struct AdjGeom {
+  BinGeom g;
+  int nbins;
+  int nells;
+  int ells[MAX_ELLS];
+  LegendreCoefs lc;
+  float los[3];
+  float e0, inv_step;
+  int for_c2r;
+};
+
+// Bin index of a stored mode (thresholds in a global table).
+__device__ __forceinline__ int adj_bin(const AdjGeom &a, const float *thr, float k2) {
+  return bin_from_k2(thr, a.g.nedges, a.e0, a.inv_step, k2);
+}
+
+__device__ __forceinline__ float c2r_weight(const BinGeom &g, int z) {
+  return (z == 0 || ((g.d.n2 % 2) == 0 && z == g.d.nz - 1)) ? 1.f : 2.f;
+}
+
+__global__ void thresholds_kernel(const float *__restrict__ edges, int nedges,
+                                  float *__restrict__ thr) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nedges; i += gridDim.x * blockDim.x)
+    thr[i] = sqrt_threshold(edges[i]);
+}
+
+// global line of sight: gbar_k = 2 G_k delta_k, G_k = w_k sum_l coef_l[b] L_l(mu)
+__device__ __forceinline__ float2 global_adj_mode(const AdjGeom &a, const float *thr,
+                                                  const float *coef, const float2 *delta, int i,
+                                                  int j, int z) {
+  const BinGeom &g = a.g;
+  const float kx = kcoord(i, g.d.n0, g.kfun[0], false);
+  const float ky = kcoord(j, g.d.n1, g.kfun[1], false);
+  const float kz = kz_coord(g, z);
+  const float k2 = __fadd_rn(__fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky)), __fmul_rn(kz, kz));
+  const int b = adj_bin(a, thr, k2);
+  if (b < 1 || b > a.nbins) return make_float2(0.f, 0.f);
+  const float num = (kx * a.los[0] + ky * a.los[1]) + kz * a.los[2];
+  const float rk2 = k2 > 0.f ? 1.f / k2 : 0.f;
+  const float mu2 = num * num * rk2;
+  const float mu = num * sqrtf(rk2);
+  const bool zero = (i == 0 && j == 0 && z == 0);
+  float G = 0.f;
+  for (int l = 0; l < a.nells; ++l) {
+    if ((a.ells[l] > 0 && zero) || a.lc.odd[l]) continue;  // odd ell of an auto spectrum is 0
+    float L = a.lc.c[l][4];
+    L = L * mu2 + a.lc.c[l][3];
+    L = L * mu2 + a.lc.c[l][2];
+    L = L * mu2 + a.lc.c[l][1];
+    L = L * mu2 + a.lc.c[l][0];
+    if (a.lc.odd[l]) L *= mu;  // odd multipoles bin Im(A): handled by the caller's coef sign
+    G += coef[(size_t)l * a.nbins + (b - 1)] * L;
+  }
+  G *= mode_weight(g, z);
+  const float2 d = delta[((int64_t)i * g.d.n1 + j) * g.d.nz + z];
+  return make_float2(2.f * G * d.x, 2.f * G * d.y);
+}
+
+__global__ void global_adjoint_kernel(AdjGeom a, const float *__restrict__ thr,
+                                      const float *__restrict__ coef,
+                                      const float2 *__restrict__ delta,
+                                      float2 *__restrict__ out) {
+  const BinGeom &g = a.g;
+  const int64_t total = g.d.ncomplex();
+  const bool even = (g.d.n2 % 2) == 0;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int z = (int)(idx % g.d.nz);
+    const int64_t r = idx / g.d.nz;
+    const int j = (int)(r % g.d.n1), i = (int)(r / g.d.n1);
+    float2 v = global_adj_mode(a, thr, coef, delta, i, j, z);
+    if (a.for_c2r) {
+      if (z == 0 || (even && z == g.d.nz - 1)) {
+        const float2 m = global_adj_mode(a, thr, coef, delta, (g.d.n0 - i) % g.d.n0,
+                                         (g.d.n1 - j) % g.d.n1, z);
+        v = make_float2(0.5f * (v.x + m.x), 0.5f * (v.y - m.y));
+      } else {
+        v = make_float2(0.5f * v.x, 0.5f * v.y);
+      }
+    }
+    out[idx] = v;
+  }
+}
+
+// first point: per mode the cotangents of A0 and of each F_j in the batch.
+struct FPAdj {
+  int nterms;
+  int term_ell[MAX_FP_TERMS];
+  int term_m[MAX_FP_TERMS];
+  int term_l[MAX_FP_TERMS];  // index of the term's ell in ells
+};
+
+__device__ __forceinline__ void fp_adj_mode(const AdjGeom &a, const FPAdj &t, const float *thr,
+                                            const float *coef, const float2 *a0, const float2 *f,
+                                            int i, int j, int z, float2 *ga0, float2 *gf) {
+  const BinGeom &g = a.g;
+  const float kx = kcoord(i, g.d.n0, g.kfun[0], false);
+  const float ky = kcoord(j, g.d.n1, g.kfun[1], false);
+  const float kz = kz_coord(g, z);
+  const float k2 = __fadd_rn(__fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky)), __fmul_rn(kz, kz));
+  const int b = adj_bin(a, thr, k2);
+  const int64_t idx = ((int64_t)i * g.d.n1 + j) * g.d.nz + z;
+  const int64_t stride = g.d.ncomplex();
+  *ga0 = make_float2(0.f, 0.f);
+  for (int q = 0; q < t.nterms; ++q) gf[q] = make_float2(0.f, 0.f);
+  if (b < 1 || b > a.nbins) return;
+  const bool zero = (i == 0 && j == 0 && z == 0);
+  const float w = mode_weight(g, z);
+  const float rn = k2 > 0.f ? rsqrtf(k2) : 0.f;
+  const float xh = kx * rn, yh = ky * rn, zh = kz * rn;
+  const float2 A = a0[idx];
+  float2 acc = make_float2(0.f, 0.f);
+  for (int l = 0; l < a.nells; ++l)
+    if (a.ells[l] == 0) {  // ell = 0: |A0|^2 -> 2 G0 A0
+      const float G0 = w * coef[(size_t)l * a.nbins + (b - 1)];
+      acc.x += 2.f * G0 * A.x;
+      acc.y += 2.f * G0 * A.y;
+    }
+  if (!zero)
+    for (int q = 0; q < t.nterms; ++q) {
+      const int l = t.term_l[q];
+      const float G = w * coef[(size_t)l * a.nbins + (b - 1)];
+      const float y = ylm_eval(t.term_ell[q], t.term_m[q], xh, yh, zh);
+      const float2 F = f[(int64_t)q * stride + idx];
+      acc.x += G * y * F.x;  // d/dA0 of G Re(conj(S) A0) = G S
+      acc.y += G * y * F.y;
+      gf[q] = make_float2(G * y * A.x, G * y * A.y);  // d/dF of G Re(S conj(A0)) = G Y A0
+    }
+  *ga0 = acc;
+}
+
+__global__ void firstpoint_adjoint_kernel(AdjGeom a, FPAdj t, const float *__restrict__ thr,
+                                          const float *__restrict__ coef,
+                                          const float2 *__restrict__ a0,
+                                          const float2 *__restrict__ f,
+                                          float2 *__restrict__ out_a0, int accumulate_a0,
+                                          float2 *__restrict__ out_f) {
+  const BinGeom &g = a.g;
+  const int64_t total = g.d.ncomplex();
+  const bool even = (g.d.n2 % 2) == 0;
+  float2 gf[MAX_FP_TERMS], gfm[MAX_FP_TERMS];
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int z = (int)(idx % g.d.nz);
+    const int64_t r = idx / g.d.nz;
+    const int j = (int)(r % g.d.n1), i = (int)(r / g.d.n1);
+    float2 ga0;
+    fp_adj_mode(a, t, thr, coef, a0, f, i, j, z, &ga0, gf);
+    const bool plane = z == 0 || (even && z == g.d.nz - 1);
+    if (a.for_c2r) {
+      if (plane) {
+        float2 ga0m;
+        fp_adj_mode(a, t, thr, coef, a0, f, (g.d.n0 - i) % g.d.n0, (g.d.n1 - j) % g.d.n1, z,
+                    &ga0m, gfm);
+        ga0 = make_float2(0.5f * (ga0.x + ga0m.x), 0.5f * (ga0.y - ga0m.y));
+        for (int q = 0; q < t.nterms; ++q)
+          gf[q] = make_float2(0.5f * (gf[q].x + gfm[q].x), 0.5f * (gf[q].y - gfm[q].y));
+      } else {
+        ga0 = make_float2(0.5f * ga0.x, 0.5f * ga0.y);
+        for (int q = 0; q < t.nterms; ++q) gf[q] = make_float2(0.5f * gf[q].x, 0.5f * gf[q].y);
+      }
+    }
+    if (out_a0) {
+      if (accumulate_a0) {
+        const float2 o = out_a0[idx];
+        out_a0[idx] = make_float2(o.x + ga0.x, o.y + ga0.y);
+      } else {
+        out_a0[idx] = ga0;
+      }
+    }
+    for (int q = 0; q < t.nterms; ++q) out_f[(int64_t)q * total + idx] = gf[q];
+  }
+}
+
+static pk_status make_adj(const int32_t meshsize[3], const float kfun[3], int nedges, float step,
+                          int backend, int nells, const int32_t *ells, const float *d_edges,
+                          int for_c2r, AdjGeom *a) {
+  pk_status st = make_geom(meshsize, kfun, nedges, step, backend, &a->g);
+  if (st) return st;
+  PK_REQUIRE(d_edges && ells, PK_ERR_INVALID, "null pointer");
+  PK_REQUIRE(nells >= 1 && nells <= MAX_ELLS, PK_ERR_INVALID, "nells must be in 1..%d", MAX_ELLS);
+  a->nbins = nedges - 1;
+  a->nells = nells;
+  a->lc.any_odd = 0;
+  for (int l = 0; l < MAX_ELLS; ++l) {
+    a->ells[l] = l < nells ? ells[l] : 0;
+    PK_REQUIRE(l >= nells || (ells[l] >= 0 && ells[l] <= 8), PK_ERR_INVALID, "ell must be in 0..8");
+    legendre_coefs(a->ells[l], a->lc.c[l], &a->lc.odd[l]);
+  }
+  a->e0 = 0.f;  // refined on the device from edges[0]
+  a->inv_step = step > 0.f ? 1.f / step : 0.f;
+  a->for_c2r = for_c2r;
+  return PK_OK;
+}
+
+extern "C" pk_status pk_adjoint_workspace_size(int nedges, size_t *bytes) {
+  PK_REQUIRE(bytes && nedges >= 2, PK_ERR_INVALID, "invalid arguments");
+  *bytes = align_up((size_t)nedges * sizeof(float));
+  return PK_OK;
+}
+
+extern "C" pk_status pk_bin_global_adjoint(void *stream, const void *delta,
+                                           const int32_t meshsize[3], const float kfun[3],
+                                           const float los[3], const float *d_edges, int nedges,
+                                           float step, float edge0, int backend, int nells,
+                                           const int32_t *ells, const float *d_coef, int for_c2r,
+                                           void *out, void *workspace, size_t workspace_bytes) {
+  AdjGeom a;
+  pk_status st = make_adj(meshsize, kfun, nedges, step, backend, nells, ells, d_edges, for_c2r, &a);
+  if (st) return st;
+  PK_REQUIRE(delta && d_coef && out && los, PK_ERR_INVALID, "null pointer");
+  PK_REQUIRE(delta != out, PK_ERR_INVALID, "out must not alias delta");
+  PK_REQUIRE(workspace && workspace_bytes >= (size_t)nedges * sizeof(float), PK_ERR_WORKSPACE,
+             "adjoint workspace too small");
+  a.e0 = edge0;
+  for (int c = 0; c < 3; ++c) a.los[c] = los[c];
+  cudaStream_t s = (cudaStream_t)stream;
+  float *thr = static_cast<float *>(workspace);
+  thresholds_kernel<<<(nedges + 255) / 256, 256, 0, s>>>(d_edges, nedges, thr);
+  PK_LAUNCH_CHECK();
+  const int64_t total = a.g.d.ncomplex();
+  const int64_t want = (total + 255) / 256, cap = 32LL * sm_count();
+  global_adjoint_kernel<<<(int)(want < cap ? want : cap), 256, 0, s>>>(
+      a, thr, d_coef, (const float2 *)delta, (float2 *)out);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+extern "C" pk_status pk_bin_firstpoint_adjoint(void *stream, const void *a0, const void *f,
+                                               int nterms, const int32_t *term_ell,
+                                               const int32_t *term_m, const int32_t meshsize[3],
+                                               const float kfun[3], const float *d_edges,
+                                               int nedges, float step, float edge0, int backend,
+                                               int nells, const int32_t *ells,
+                                               const float *d_coef, int for_c2r, void *out_a0,
+                                               int accumulate_a0, void *out_f, void *workspace,
+                                               size_t workspace_bytes) {
+  AdjGeom a;
+  pk_status st = make_adj(meshsize, kfun, nedges, step, backend, nells, ells, d_edges, for_c2r, &a);
+  if (st) return st;
+  PK_REQUIRE(a0 && d_coef, PK_ERR_INVALID, "null pointer");
+  PK_REQUIRE(nterms >= 0 && nterms <= MAX_FP_TERMS, PK_ERR_INVALID, "nterms must be in 0..%d",
+             MAX_FP_TERMS);
+  PK_REQUIRE(nterms == 0 || (f && out_f && term_ell && term_m), PK_ERR_INVALID, "null term arrays");
+  PK_REQUIRE(workspace && workspace_bytes >= (size_t)nedges * sizeof(float), PK_ERR_WORKSPACE,
+             "adjoint workspace too small");
+  a.e0 = edge0;
+  FPAdj t;
+  t.nterms = nterms;
+  for (int q = 0; q < MAX_FP_TERMS; ++q) {
+    t.term_ell[q] = q < nterms ? term_ell[q] : 0;
+    t.term_m[q] = q < nterms ? term_m[q] : 0;
+    t.term_l[q] = -1;
+    for (int l = 0; l < nells && q < nterms; ++l)
+      if (ells[l] == term_ell[q]) t.term_l[q] = l;
+    PK_REQUIRE(q >= nterms || (t.term_l[q] >= 0 && term_ell[q] >= 1 && term_ell[q] <= YLM_LMAX &&
+                               term_m[q] >= -term_ell[q] && term_m[q] <= term_ell[q]),
+               PK_ERR_INVALID, "term (%d, %d) is not one of the requested multipoles",
+               q < nterms ? term_ell[q] : 0, q < nterms ? term_m[q] : 0);
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  float *thr = static_cast<float *>(workspace);
+  thresholds_kernel<<<(nedges + 255) / 256, 256, 0, s>>>(d_edges, nedges, thr);
+  PK_LAUNCH_CHECK();
+  const int64_t total = a.g.d.ncomplex();
+  const int64_t want = (total + 255) / 256, cap = 32LL * sm_count();
+  firstpoint_adjoint_kernel<<<(int)(want < cap ? want : cap), 256, 0, s>>>(
+      a, t, thr, d_coef, (const float2 *)a0, (const float2 *)f, (float2 *)out_a0, accumulate_a0,
+      (float2 *)out_f);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
 }

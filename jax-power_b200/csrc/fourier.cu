@@ -390,3 +390,123 @@ extern "C" pk_status pk_ylm_premultiply(void *stream, const float *rho, const in
   PK_LAUNCH_CHECK();
   return PK_OK;
 }
+
+// ------------------------------------------------------------------ adjoints
+// Backward of _paint's Fourier part (mesh.py:2737-2752) for the 'jax' semantics.  The
+// forward is delta = C / I sum_s e^{i theta_s} F_s, F_s = rfftn(rho_s), optionally
+// followed by irfftn.  Given the cotangent of the output (R = rfftn(rho_bar) when the
+// output was the real mesh rho, or the conjugate cotangent gbar of delta itself), this
+// writes for every shift h_s = sym(C e^{-i theta_s} X / I) with X = R / (N0 N1 N2) or
+// gbar / w', so that rho_bar_s = C2R(h_s) (unnormalised) is the cotangent of painted
+// mesh s.  sym() Hermitian-symmetrises the kz = 0 and N/2 planes.
+__global__ void __launch_bounds__(IL_THREADS) interlace_adjoint_kernel(
+    FourierParams p, const float2 *__restrict__ in, int from_real, float2 *__restrict__ out) {
+  const Dims d = p.d;
+  const int64_t total = d.ncomplex();
+  const bool even = (d.n2 % 2) == 0;
+  const float inv_n = 1.f / (float)d.nreal();
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int z = (int)(idx % d.nz);
+    const int64_t r = idx / d.nz;
+    const int j = (int)(r % d.n1), i = (int)(r / d.n1);
+    const bool plane = z == 0 || (even && z == d.nz - 1);
+    const int im = (d.n0 - i) % d.n0, jm = (d.n1 - j) % d.n1;
+    for (int s = 0; s < p.nshifts; ++s) {
+      float2 v[2];
+      for (int q = 0; q < (plane ? 2 : 1); ++q) {
+        const int ii = q ? im : i, jj = q ? jm : j;
+        const float k0 = ccoord(ii, d.n0, p.cspacing[0], false);
+        const float k1 = ccoord(jj, d.n1, p.cspacing[1], false);
+        const float k2 = ccoord(z, d.n2, p.cspacing[2], true);
+        float2 x = in[((int64_t)ii * d.n1 + jj) * d.nz + z];
+        const float scale = from_real ? inv_n : (plane ? 1.f : 0.5f);
+        float c = 1.f;
+        if (p.comp_order > 0)
+          c = inverse_power(__fmul_rn(__fmul_rn(sinc_of(k0), sinc_of(k1)), sinc_of(k2)), p.comp_order);
+        const float2 e = expi(-p.shifts[s] * ((k0 + k1) + k2));
+        const float f = c * scale / p.interlacing;
+        x = cmul(x, e);
+        v[q] = make_float2(x.x * f, x.y * f);
+      }
+      if (plane) v[0] = make_float2(0.5f * (v[0].x + v[1].x), 0.5f * (v[0].y - v[1].y));
+      out[(int64_t)s * total + idx] = v[0];
+    }
+  }
+}
+
+// rho_bar(x) += sum_j r_j(x) Y_j(xhat) (adjoint of the Y_lm premultiply).
+__global__ void ylm_accumulate_kernel(Dims d, float c0, float c1, float c2, float o0, float o1,
+                                      float o2, YlmTerms terms, const float *__restrict__ r,
+                                      float *__restrict__ rho_bar) {
+  const int64_t total = d.nreal();
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(idx % d.n2);
+    const int64_t rr = idx / d.n2;
+    const int j = (int)(rr % d.n1), i = (int)(rr / d.n1);
+    const float x = __fadd_rn(__fmul_rn((float)i, c0), o0);
+    const float y = __fadd_rn(__fmul_rn((float)j, c1), o1);
+    const float z = __fadd_rn(__fmul_rn((float)k, c2), o2);
+    const float xn = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z)));
+    float xh = 0.f, yh = 0.f, zh = 0.f;
+    if (xn != 0.f) {
+      xh = __fdiv_rn(x, xn);
+      yh = __fdiv_rn(y, xn);
+      zh = __fdiv_rn(z, xn);
+    }
+    float acc = rho_bar[idx];
+    for (int t = 0; t < terms.n; ++t)
+      acc += r[(int64_t)t * total + idx] * ylm_eval(terms.ell[t], terms.m[t], xh, yh, zh);
+    rho_bar[idx] = acc;
+  }
+}
+
+extern "C" pk_status pk_interlace_adjoint(void *stream, const void *in, int from_real,
+                                          int nshifts, const int32_t meshsize[3], int comp_order,
+                                          int backend, void *out) {
+  PK_REQUIRE(in && out && in != out, PK_ERR_INVALID, "null or aliased buffers");
+  FourierParams p;
+  PK_REQUIRE(make_dims(meshsize, &p.d), PK_ERR_INVALID, "invalid meshsize");
+  PK_REQUIRE(nshifts >= 1 && nshifts <= IL_MAX_SHIFTS, PK_ERR_INVALID, "nshifts must be in 1..8");
+  PK_REQUIRE(comp_order >= 0 && comp_order <= 4, PK_ERR_INVALID, "comp_order must be in 0..4");
+  PK_REQUIRE(backend == PK_BACKEND_JAX, PK_ERR_INVALID,
+             "the paint adjoint implements the 'jax' FFT semantics only");
+  const int ns[3] = {p.d.n0, p.d.n1, p.d.n2};
+  for (int a = 0; a < 3; ++a) p.cspacing[a] = (float)(2. * M_PI / ns[a]);
+  p.nshifts = nshifts;
+  for (int s = 0; s < IL_MAX_SHIFTS; ++s) p.shifts[s] = s < nshifts ? (float)s / (float)nshifts : 0.f;
+  p.interlacing = (float)nshifts;
+  p.comp_order = comp_order;
+  p.backend = backend;
+  p.for_c2r = 1;
+  p.scale = 1.f;
+  interlace_adjoint_kernel<<<grid_for(p.d.ncomplex(), IL_THREADS), IL_THREADS, 0,
+                             (cudaStream_t)stream>>>(p, (const float2 *)in, from_real,
+                                                     (float2 *)out);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+extern "C" pk_status pk_ylm_accumulate(void *stream, const float *r, const int32_t meshsize[3],
+                                       const float cellsize[3], const float offset[3], int nterms,
+                                       const int32_t *term_ell, const int32_t *term_m,
+                                       float *rho_bar) {
+  PK_REQUIRE(r && rho_bar && cellsize && offset, PK_ERR_INVALID, "null pointer");
+  Dims d;
+  PK_REQUIRE(make_dims(meshsize, &d), PK_ERR_INVALID, "invalid meshsize");
+  PK_REQUIRE(nterms >= 1 && nterms <= 32, PK_ERR_INVALID, "nterms must be in 1..32");
+  YlmTerms t;
+  t.n = nterms;
+  for (int j = 0; j < nterms; ++j) {
+    PK_REQUIRE(term_ell[j] >= 0 && term_ell[j] <= YLM_LMAX && term_m[j] >= -term_ell[j] &&
+                   term_m[j] <= term_ell[j],
+               PK_ERR_INVALID, "invalid (ell, m) = (%d, %d)", term_ell[j], term_m[j]);
+    t.ell[j] = term_ell[j];
+    t.m[j] = term_m[j];
+  }
+  ylm_accumulate_kernel<<<grid_for(d.nreal(), 256), 256, 0, (cudaStream_t)stream>>>(
+      d, cellsize[0], cellsize[1], cellsize[2], offset[0], offset[1], offset[2], t, r, rho_bar);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}

@@ -1,0 +1,171 @@
+"""Differentiable paint and power spectrum (hand-written adjoints, torch.autograd).
+
+The reference obtains gradients of this path from JAX autodiff (no custom rule: the
+transpose of the scatter-add is ``resamplers.read`` ``resamplers.py:100-125``, the
+position derivative comes through the kernels ``resamplers.py:57-63``, FFT adjoints from
+XLA).  Here each stage has an explicit adjoint in the CUDA library, wired into
+``torch.autograd.Function`` (the torch counterpart of ``jax.custom_vjp``):
+
+- ``paint_value(positions, weights, attrs, ...)`` -> mesh tensor (real or Hermitian complex);
+  backward: rfftn of the real cotangent, ``pk_interlace_adjoint`` (phases, compensation,
+  1/I), one C2R per shift, then ``pk_read`` with the window derivative (position and
+  weight cotangents), summed over shifts.
+- ``spectrum_value(mesh, attrs, bin, los)`` -> (nells, nbins) float64 multipoles
+  (``num_raw`` of ``compute_mesh2_spectrum``); backward: ``pk_bin_global_adjoint`` or
+  ``pk_bin_firstpoint_adjoint`` + C2R + ``pk_ylm_accumulate``.
+
+Gradients follow the 'jax' FFT semantics and even multipoles (odd auto multipoles are 0).
+"""
+import numpy as np
+import torch
+
+from . import _lib
+from . import resamplers
+from .mesh import MeshAttrs, _paint, _r2c, _c2r, _device, _as_positions, _as_weights, _workspace
+from .mesh2 import _spectrum_sums, _ell_factors, _los, _firstpoint_terms, _term_batch
+
+__all__ = ['paint_value', 'spectrum_value']
+
+
+def _c2r_unnormalised(h, meshsize):
+    return _c2r(h, meshsize, scale=False, destroy_input=True)
+
+
+class _Paint(torch.autograd.Function):
+
+    @staticmethod
+    def forward(ctx, positions, weights, attrs, order, interlacing, compensate, out):
+        resampler = {1: 'ngp', 2: 'cic', 3: 'tsc', 4: 'pcs'}[order]
+        mesh = _paint(attrs, positions.detach(), None if weights is None else weights.detach(), resampler=resampler,
+                      interlacing=interlacing, compensate=compensate, out=out)
+        ctx.save_for_backward(positions, weights if weights is not None else torch.empty(0, device=positions.device))
+        ctx.has_weights = weights is not None
+        ctx.cfg = (attrs, order, max(int(interlacing), 1), bool(compensate), out)
+        return mesh.value
+
+    @staticmethod
+    def backward(ctx, grad):
+        positions, weights = ctx.saved_tensors
+        weights = weights if ctx.has_weights else None
+        attrs, order, interlacing, compensate, out = ctx.cfg
+        meshsize = attrs.meshsize
+        grad = grad.contiguous()
+        if interlacing == 1 and not compensate and out == 'real':
+            rbars = grad[None]
+        else:
+            if out == 'real':
+                src, from_real = _r2c(grad, meshsize), 1
+            else:
+                src, from_real = grad.to(torch.complex64), 0
+            h = torch.empty((interlacing,) + tuple(src.shape), dtype=torch.complex64, device=src.device)
+            _lib.call('pk_interlace_adjoint', _lib.stream_handle(), _lib.ptr(src), from_real, interlacing,
+                      _lib.i32(meshsize), order if compensate else 0, attrs.backend_code, _lib.ptr(h))
+            rbars = _c2r_unnormalised(h, meshsize)
+        n = positions.shape[0]
+        gpos = torch.zeros((n, 3), dtype=torch.float32, device=positions.device)
+        gw = torch.zeros(n, dtype=torch.float32, device=positions.device)
+        pos = positions.detach().contiguous()
+        wts = None if weights is None else weights.detach().contiguous()
+        for s in range(interlacing):
+            shift = float(np.float32(s) / np.float32(interlacing))
+            _lib.call('pk_read', _lib.stream_handle(), _lib.ptr(rbars[s].contiguous()), _lib.ptr(pos), _lib.ptr(wts),
+                      n, _lib.i32(meshsize), _lib.f32(attrs.boxsize), _lib.f32(attrs.boxcenter),
+                      _lib.f32(attrs.cellsize), order, shift, 1., _lib.ptr(gw), _lib.ptr(gpos), 1)
+        return gpos, (gw if ctx.has_weights else None), None, None, None, None, None
+
+
+def paint_value(positions, weights=None, attrs=None, resampler='cic', interlacing=0, compensate=False,
+                out='real'):
+    """Differentiable ``ParticleField(positions, weights, attrs).paint(...)``: returns the mesh tensor."""
+    if attrs.fft_backend != 'jax' and (interlacing > 1 or compensate):
+        raise NotImplementedError("the paint adjoint implements fft_backend='jax'")
+    positions = positions if positions.is_cuda and positions.dtype == torch.float32 else _as_positions(positions)
+    if weights is not None and not (weights.is_cuda and weights.dtype == torch.float32):
+        weights = _as_weights(weights, positions.shape[0])
+    order = resamplers.get_resampler(resampler).order
+    return _Paint.apply(positions, weights, attrs, order, interlacing, compensate, out)
+
+
+class _Spectrum(torch.autograd.Function):
+
+    @staticmethod
+    def forward(ctx, value, attrs, bin, los):
+        is_complex = value.is_complex()
+        raw = _spectrum_sums(attrs, bin, los, rmesh=None if is_complex else value.detach(),
+                             cmesh=value.detach() if is_complex else None)
+        _, vlos, _ = _los(los)
+        factors = torch.tensor(_ell_factors(bin.ells, vlos), dtype=torch.float64, device=raw.device)
+        nmodes = torch.as_tensor(bin.nmodes, dtype=torch.float64, device=raw.device)
+        ctx.save_for_backward(value)
+        ctx.cfg = (attrs, bin, los, factors, nmodes)
+        return raw * factors[:, None] / nmodes
+
+    @staticmethod
+    def backward(ctx, grad):
+        (value,) = ctx.saved_tensors
+        attrs, bin, los, factors, nmodes = ctx.cfg
+        meshsize = attrs.meshsize
+        ells = bin.ells
+        if any(ell % 2 for ell in ells):
+            raise NotImplementedError('gradients of odd multipoles are not implemented')
+        coef = (grad * factors[:, None] / nmodes).to(torch.float32).contiguous()
+        _, vlos, swap = _los(los)
+        is_complex = value.is_complex()
+        nbytes = _lib.c_size_t()
+        _lib.call('pk_adjoint_workspace_size', len(bin._edges1d), _lib.ctypes.byref(nbytes))
+        ws = _workspace(nbytes.value)
+        stream = _lib.stream_handle()
+        edge0 = float(np.float32(bin._edges1d[0]))
+        common = (_lib.i32(meshsize), _lib.f32(attrs.kfun))
+        if vlos is not None:
+            delta = (value.detach() if is_complex else _r2c(value.detach(), meshsize)).contiguous()
+            out = torch.empty_like(delta)
+            _lib.call('pk_bin_global_adjoint', stream, _lib.ptr(delta), *common, _lib.f32(vlos), _lib.ptr(bin.d_edges),
+                      len(bin._edges1d), bin._step, edge0, attrs.backend_code, len(ells), _lib.i32(ells),
+                      _lib.ptr(coef), int(not is_complex), _lib.ptr(out), _lib.ptr(ws), ws.numel())
+            if is_complex:
+                return out, None, None, None
+            return _c2r_unnormalised(out, meshsize), None, None, None
+        if is_complex:
+            raise NotImplementedError('first-point gradients are implemented for real meshes')
+        rho = value.detach().contiguous()
+        A0 = _r2c(rho, meshsize).contiguous()
+        ga0 = torch.zeros_like(A0)
+        rho_bar = torch.zeros_like(rho)
+        terms = _firstpoint_terms(ells)
+        offset = (attrs.boxcenter - (attrs.boxsize / np.float32(2.)).astype('f4')).astype('f4')
+        if not terms:
+            _lib.call('pk_bin_firstpoint_adjoint', stream, _lib.ptr(A0), None, 0, None, None, *common,
+                      _lib.ptr(bin.d_edges), len(bin._edges1d), bin._step, edge0, attrs.backend_code, len(ells),
+                      _lib.i32(ells), _lib.ptr(coef), 1, _lib.ptr(ga0), 0, None, _lib.ptr(ws), ws.numel())
+        batch = _term_batch(attrs, len(terms)) if terms else 1
+        coef_rest = coef.clone()  # ell = 0 enters the A0 cotangent once, with the first batch
+        for l, ell in enumerate(ells):
+            if ell == 0:
+                coef_rest[l] = 0.
+        for start in range(0, len(terms), batch):
+            chunk = terms[start:start + batch]
+            nt = len(chunk)
+            t_ell, t_m = [t[0] for t in chunk], [t[1] for t in chunk]
+            real = torch.empty((nt,) + tuple(int(n) for n in meshsize), dtype=torch.float32, device=rho.device)
+            _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rho), _lib.i32(meshsize), _lib.f32(attrs.cellsize),
+                      _lib.f32(offset), nt, _lib.i32(t_ell), _lib.i32(t_m), _lib.ptr(real))
+            F = _r2c(real, meshsize)
+            gf = torch.empty_like(F)
+            _lib.call('pk_bin_firstpoint_adjoint', stream, _lib.ptr(A0), _lib.ptr(F), nt, _lib.i32(t_ell),
+                      _lib.i32(t_m), *common, _lib.ptr(bin.d_edges), len(bin._edges1d), bin._step, edge0,
+                      attrs.backend_code, len(ells), _lib.i32(ells), _lib.ptr(coef if start == 0 else coef_rest), 1,
+                      _lib.ptr(ga0), 1, _lib.ptr(gf), _lib.ptr(ws), ws.numel())
+            del F
+            r = _c2r_unnormalised(gf, meshsize)
+            _lib.call('pk_ylm_accumulate', stream, _lib.ptr(r), _lib.i32(meshsize), _lib.f32(attrs.cellsize),
+                      _lib.f32(offset), nt, _lib.i32(t_ell), _lib.i32(t_m), _lib.ptr(rho_bar))
+        rho_bar += _c2r_unnormalised(ga0, meshsize)
+        return rho_bar, None, None, None
+
+
+def spectrum_value(mesh, attrs=None, bin=None, los='z'):
+    """Differentiable multipoles ``num_raw`` (nells, nbins) float64 of ``compute_mesh2_spectrum``."""
+    value = mesh.value if hasattr(mesh, 'value') else mesh
+    attrs = attrs if attrs is not None else mesh.attrs
+    return _Spectrum.apply(value, attrs, bin, los)

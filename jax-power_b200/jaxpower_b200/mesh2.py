@@ -187,34 +187,49 @@ def _term_batch(mattrs, nterms):
     return int(max(1, min(nterms, 32, (0.4 * free) // per_term)))
 
 
-def compute_mesh2_spectrum(*meshes, bin=None, los='z'):
-    """Power-spectrum multipoles from mesh(es) (``mesh2.py:253-374``)."""
-    meshes, fields = _format_meshes(*meshes)
-    mattrs = meshes[0].attrs
+def _ell_factors(ells, vlos):
+    """Per-multipole factor of the binned sums: (2 ell + 1) global, 4 pi first point (1 for ell 0)."""
+    if vlos is None:
+        return [1. if ell == 0 else 4. * np.pi for ell in ells]
+    return [2. * ell + 1. for ell in ells]
+
+
+def _spectrum_sums(mattrs, bin, los, rmesh=None, cmesh=None, cmesh2=None, rmesh2=None):
+    """Raw per-bin sums (nells, nbins) float64 on the device (no host synchronisation).
+
+    Global los: sum of w Re/Im(conj(d1) d2) L_ell(mu) over each bin.  First point: the
+    sums of ``pk_bin_firstpoint`` over all (ell, m) terms.  ``rmesh`` / ``cmesh`` are the
+    real / Hermitian-complex values of the first mesh (either may be None), likewise for
+    the second mesh of a cross spectrum.
+    """
     meshsize = mattrs.meshsize
-    norm_value = np.float32(np.prod(meshsize.astype('f4'))) / np.float32(np.prod(mattrs.cellsize))
     los, vlos, swap = _los(los)
-    attrs = dict(los=vlos if vlos is not None else los)
     ells = bin.ells
     nbins = bin.nbins
     ws = bin._workspace()
     stream = _lib.stream_handle()
     raw = torch.zeros(len(ells) * nbins, dtype=torch.float64, device=_device())
+    cross = cmesh2 is not None or rmesh2 is not None
     if vlos is None:
-        if swap:
-            meshes = meshes[::-1]
-        rmesh1 = meshes[0]
-        auto = fields[1] == fields[0]
-        A0 = _2c(rmesh1 if auto else meshes[1]).value.contiguous()
-        B0 = None if auto else _2c(rmesh1).value.contiguous()
+        if swap and cross:
+            rmesh, cmesh, rmesh2, cmesh2 = rmesh2, cmesh2, rmesh, cmesh
+        if rmesh is None:
+            rmesh = _c2r(cmesh, meshsize)
+        if cross:
+            A0 = cmesh2 if cmesh2 is not None else _r2c(rmesh2, meshsize)
+            B0 = cmesh if cmesh is not None else _r2c(rmesh, meshsize)
+        else:
+            A0 = cmesh if cmesh is not None else _r2c(rmesh, meshsize)
+            B0 = None
+        A0 = A0.contiguous()
         terms = _firstpoint_terms(ells)
         if not terms:
             _lib.call('pk_bin_firstpoint', stream, _lib.ptr(A0), _lib.ptr(B0), None, 0, None, None,
                       _lib.i32(meshsize), _lib.f32(mattrs.kfun), _lib.ptr(bin.d_edges), len(bin._edges1d),
                       bin._step, mattrs.backend_code, len(ells), _lib.i32(ells), 1, 1, _lib.ptr(raw),
                       _lib.ptr(ws), ws.numel())
-        if terms:
-            rho = _2r(rmesh1).value.contiguous()
+        else:
+            rho = rmesh.contiguous()
             offset = (mattrs.boxcenter - (mattrs.boxsize / np.float32(2.)).astype('f4')).astype('f4')
             batch = _term_batch(mattrs, len(terms))
             real = torch.empty((batch,) + tuple(int(n) for n in meshsize), dtype=torch.float32, device=rho.device)
@@ -231,19 +246,43 @@ def compute_mesh2_spectrum(*meshes, bin=None, los='z'):
                           len(bin._edges1d), bin._step, mattrs.backend_code, len(ells), _lib.i32(ells),
                           include_ell0, 1, _lib.ptr(raw), _lib.ptr(ws), ws.numel())
                 del F
-        raw = raw.cpu().numpy().reshape(len(ells), nbins)
-        num = [raw[i] / bin.nmodes * (1. if ell == 0 else 4. * np.pi) for i, ell in enumerate(ells)]
+        raw = raw.reshape(len(ells), nbins)
         if swap:  # conj: odd multipoles (imaginary parts) change sign
-            num = [-n if ell % 2 else n for ell, n in zip(ells, num)]
-    else:
-        auto = fields[1] == fields[0]
-        d1 = _2c(meshes[0]).value.contiguous()
-        d2 = None if auto else _2c(meshes[1]).value.contiguous()
-        _lib.call('pk_bin_global', stream, _lib.ptr(d1), _lib.ptr(d2), _lib.i32(meshsize), _lib.f32(mattrs.kfun),
-                  _lib.f32(vlos), _lib.ptr(bin.d_edges), len(bin._edges1d), bin._step, mattrs.backend_code,
-                  len(ells), _lib.i32(ells), _lib.ptr(raw), _lib.ptr(ws), ws.numel())
-        raw = raw.cpu().numpy().reshape(len(ells), nbins)
-        num = [raw[i] / bin.nmodes * (2 * ell + 1) for i, ell in enumerate(ells)]
+            sign = torch.tensor([-1. if ell % 2 else 1. for ell in ells], dtype=raw.dtype, device=raw.device)
+            raw = raw * sign[:, None]
+        return raw
+    d1 = (cmesh if cmesh is not None else _r2c(rmesh, meshsize)).contiguous()
+    d2 = None
+    if cross:
+        d2 = (cmesh2 if cmesh2 is not None else _r2c(rmesh2, meshsize)).contiguous()
+    _lib.call('pk_bin_global', stream, _lib.ptr(d1), _lib.ptr(d2), _lib.i32(meshsize), _lib.f32(mattrs.kfun),
+              _lib.f32(vlos), _lib.ptr(bin.d_edges), len(bin._edges1d), bin._step, mattrs.backend_code,
+              len(ells), _lib.i32(ells), _lib.ptr(raw), _lib.ptr(ws), ws.numel())
+    return raw.reshape(len(ells), nbins)
+
+
+def _split(mesh):
+    if mesh is None:
+        return None, None
+    if isinstance(mesh, ComplexMeshField):
+        return None, mesh.value
+    return mesh.value, None
+
+
+def compute_mesh2_spectrum(*meshes, bin=None, los='z'):
+    """Power-spectrum multipoles from mesh(es) (``mesh2.py:253-374``)."""
+    meshes, fields = _format_meshes(*meshes)
+    mattrs = meshes[0].attrs
+    norm_value = np.float32(np.prod(mattrs.meshsize.astype('f4'))) / np.float32(np.prod(mattrs.cellsize))
+    los_name, vlos, swap = _los(los)
+    attrs = dict(los=vlos if vlos is not None else los_name)
+    ells = bin.ells
+    nbins = bin.nbins
+    r1, c1 = _split(meshes[0])
+    r2, c2 = (None, None) if fields[1] == fields[0] else _split(meshes[1])
+    raw = _spectrum_sums(mattrs, bin, los, rmesh=r1, cmesh=c1, rmesh2=r2, cmesh2=c2).cpu().numpy()
+    factors = _ell_factors(ells, vlos)
+    num = [raw[i] / bin.nmodes * factors[i] for i in range(len(ells))]
     norm = np.full(nbins, norm_value, dtype='f8')
     poles = [Mesh2SpectrumPole(k=bin.xavg, k_edges=bin.edges, nmodes=bin.nmodes, num_raw=num[i],
                                num_shotnoise=np.zeros(nbins), norm=norm,
