@@ -64,6 +64,21 @@ pk_status pk_paint(void *stream, const float *positions, const float *weights, i
                    int interlacing, int shift_begin, int nshifts, float *out,
                    void *workspace, size_t workspace_bytes, int *d_status);
 
+/* Batched paint of nmocks catalogs on the same mesh geometry in one set of launches:
+ * positions / weights are concatenated, d_offsets (device, int64, nmocks + 1) gives
+ * each catalog's range; out[(m * nshifts + j) * N0*N1*N2 + ...].  tile_config
+ * (0..3) selects the tile shape / CTA size (0: 8x16x32 cells, 512 threads; 1: 8x16x32,
+ * 256; 2: 8x8x32, 256; 3: 4x16x32, 256), for an autotuner.  pk_paint is the nmocks = 1,
+ * tile_config = 0 case. */
+pk_status pk_paint_batch_workspace_size(int64_t n, int nmocks, const int32_t meshsize[3],
+                                        int order, int nshifts, int tile_config, size_t *bytes);
+pk_status pk_paint_batch(void *stream, const float *positions, const float *weights,
+                         const int64_t *d_offsets, int64_t n, int nmocks,
+                         const int32_t meshsize[3], const float boxsize[3],
+                         const float boxcenter[3], const float cellsize[3], int order,
+                         int interlacing, int shift_begin, int nshifts, int tile_config,
+                         float *out, void *workspace, size_t workspace_bytes, int *d_status);
+
 /* Replaces resamplers.read (resamplers.py:100-125) via _read (mesh.py:2064-2110):
  * out[p] = sum_offsets mesh[wrap(i0 + off)] * W(u), u normalised as above plus
  * `shift`.  If grad (n, 3) is non-NULL, also writes
@@ -102,6 +117,12 @@ pk_status pk_interlace_compensate(void *stream, const void *in, int nshifts,
                                   const int32_t meshsize[3], int comp_order, int backend,
                                   int for_c2r, float scale, void *out);
 
+/* The same for nbatch independent sets of nshifts meshes (in: nbatch * nshifts meshes,
+ * out: nbatch meshes), in one launch. */
+pk_status pk_interlace_compensate_batch(void *stream, const void *in, int nbatch, int nshifts,
+                                        const int32_t meshsize[3], int comp_order, int backend,
+                                        int for_c2r, float scale, void *out);
+
 /* Multiply a real array by scale (e.g. the C2R normalisation). */
 pk_status pk_scale_real(void *stream, float *mesh, int64_t size, float scale);
 
@@ -122,6 +143,16 @@ pk_status pk_bin_modes(void *stream, const int32_t meshsize[3], const float kfun
                        const float *d_edges, int nedges, float step, int backend,
                        double *d_nmodes, double *d_ksum, void *workspace,
                        size_t workspace_bytes);
+
+/* pk_bin_global over nbatch meshes (delta1[b], delta2[b] contiguous) in one launch;
+ * d_out[(b * nells + ill) * nbins + bin]; workspace from pk_bin_batch_workspace_size. */
+pk_status pk_bin_batch_workspace_size(const int32_t meshsize[3], int nedges, int nvalues,
+                                      int nbatch, size_t *bytes);
+pk_status pk_bin_global_batch(void *stream, const void *delta1, const void *delta2, int nbatch,
+                              const int32_t meshsize[3], const float kfun[3], const float los[3],
+                              const float *d_edges, int nedges, float step, int backend,
+                              int nells, const int32_t *ells, double *d_out, void *workspace,
+                              size_t workspace_bytes);
 
 /* BinMesh2SpectrumPoles.__call__ (mesh2.py:100-119) numerator: per-bin sum of
  * w * value for a complex mesh; d_out[0 * nbins + b] real part,

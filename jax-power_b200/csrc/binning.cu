@@ -444,6 +444,8 @@ __global__ void __launch_bounds__(FIN_ENTRIES * FIN_SPLIT) bin_finalize_kernel(
     const double *__restrict__ partials, int nblocks, int hist_len, int nv, int nbins,
     int accumulate, double *__restrict__ out0, double *__restrict__ out1) {
   __shared__ double part[FIN_SPLIT][FIN_ENTRIES];
+  partials += (size_t)blockIdx.y * nblocks * hist_len;  // batch of histograms along y
+  out0 += (size_t)blockIdx.y * hist_len;
   const int le = threadIdx.x % FIN_ENTRIES, sp = threadIdx.x / FIN_ENTRIES;
   const int e = blockIdx.x * FIN_ENTRIES + le;
   const int per = (nblocks + FIN_SPLIT - 1) / FIN_SPLIT;
@@ -472,8 +474,9 @@ __global__ void __launch_bounds__(FIN_ENTRIES * FIN_SPLIT) bin_finalize_kernel(
 }
 
 static void launch_finalize(cudaStream_t s, const double *partials, int nblocks, int hist_len,
-                            int nv, int nbins, int accumulate, double *out0, double *out1) {
-  const int grid = (hist_len + FIN_ENTRIES - 1) / FIN_ENTRIES;
+                            int nv, int nbins, int accumulate, double *out0, double *out1,
+                            int nbatch = 1) {
+  const dim3 grid((hist_len + FIN_ENTRIES - 1) / FIN_ENTRIES, nbatch);
   bin_finalize_kernel<<<grid, FIN_ENTRIES * FIN_SPLIT, 0, s>>>(partials, nblocks, hist_len, nv, nbins,
                                                                accumulate, out0, out1);
 }
@@ -609,6 +612,10 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_global_kernel(
   const int z0 = lane * R, z1 = min(g.d.nz, z0 + R);
   const int64_t nrows = (int64_t)g.d.n0 * g.d.n1;
   const bool jaxw = g.backend == PK_BACKEND_JAX;
+  // batch of meshes along y: mesh blockIdx.y, its own partial rows
+  d1 += (int64_t)blockIdx.y * g.d.ncomplex();
+  if (CROSS) d2 += (int64_t)blockIdx.y * g.d.ncomplex();
+  partials += (size_t)blockIdx.y * gridDim.x * hist_len;
   const int zself = (g.d.n2 % 2) == 0 ? g.d.nz - 1 : -1;  // self-conjugate last plane
   constexpr int NONE = 0x7fffffff;
   for (int64_t row = (int64_t)blockIdx.x * nwarps + warp; row < nrows;
@@ -761,21 +768,21 @@ template <int NV, bool CROSS>
 static pk_status launch_global(cudaStream_t st, const BinGeom &g, const float2 *d1,
                                const float2 *d2, const float los[3], const LegendreCoefs &lc,
                                int zero_l0, const float *edges, double *out, void *workspace,
-                               size_t workspace_bytes) {
+                               size_t workspace_bytes, int nbatch) {
   BinLaunch L;
   PK_REQUIRE(plan_bins(g.d, g.nedges, NV, &L, sizeof(float)), PK_ERR_RANGE,
              "too many bins x values (%d x %d) for the shared-memory histograms", g.nedges - 1, NV);
-  PK_REQUIRE(workspace && workspace_bytes >= L.partial_bytes, PK_ERR_WORKSPACE,
-             "binning workspace too small: need %zu bytes, got %zu", L.partial_bytes,
+  PK_REQUIRE(workspace && workspace_bytes >= L.partial_bytes * nbatch, PK_ERR_WORKSPACE,
+             "binning workspace too small: need %zu bytes, got %zu", L.partial_bytes * nbatch,
              workspace_bytes);
   double *partials = static_cast<double *>(workspace);
   PK_CUDA(cudaFuncSetAttribute(bin_global_kernel<NV, CROSS>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
-  bin_global_kernel<NV, CROSS><<<L.blocks, L.nwarps * 32, L.smem, st>>>(
+  bin_global_kernel<NV, CROSS><<<dim3(L.blocks, nbatch), L.nwarps * 32, L.smem, st>>>(
       g, d1, d2, los[0], los[1], los[2], lc, zero_l0, edges, L.nwarps, L.tab, partials);
   PK_LAUNCH_CHECK();
   const int hist_len = (g.nedges - 1) * NV;
-  launch_finalize(st, partials, L.blocks, hist_len, NV, g.nedges - 1, 0, out, nullptr);
+  launch_finalize(st, partials, L.blocks, hist_len, NV, g.nedges - 1, 0, out, nullptr, nbatch);
   PK_LAUNCH_CHECK();
   return PK_OK;
 }
@@ -819,6 +826,18 @@ static pk_status make_geom(const int32_t meshsize[3], const float kfun[3], int n
 }  // namespace pk
 
 using namespace pk;
+
+extern "C" pk_status pk_bin_workspace_size(const int32_t meshsize[3], int nedges, int nvalues,
+                                           size_t *bytes);
+
+extern "C" pk_status pk_bin_batch_workspace_size(const int32_t meshsize[3], int nedges,
+                                                 int nvalues, int nbatch, size_t *bytes) {
+  PK_REQUIRE(nbatch >= 1, PK_ERR_INVALID, "nbatch must be >= 1");
+  pk_status st = pk_bin_workspace_size(meshsize, nedges, nvalues, bytes);
+  if (st) return st;
+  *bytes *= (size_t)nbatch;
+  return PK_OK;
+}
 
 extern "C" pk_status pk_bin_workspace_size(const int32_t meshsize[3], int nedges, int nvalues,
                                            size_t *bytes) {
@@ -869,11 +888,27 @@ extern "C" pk_status pk_bin_mesh(void *stream, const void *value, const int32_t 
                         workspace_bytes);
 }
 
+extern "C" pk_status pk_bin_global_batch(void *stream, const void *delta1, const void *delta2,
+                                         int nbatch, const int32_t meshsize[3], const float kfun[3],
+                                         const float los[3], const float *d_edges, int nedges,
+                                         float step, int backend, int nells, const int32_t *ells,
+                                         double *d_out, void *workspace, size_t workspace_bytes);
+
 extern "C" pk_status pk_bin_global(void *stream, const void *delta1, const void *delta2,
                                    const int32_t meshsize[3], const float kfun[3],
                                    const float los[3], const float *d_edges, int nedges,
                                    float step, int backend, int nells, const int32_t *ells,
                                    double *d_out, void *workspace, size_t workspace_bytes) {
+  return pk_bin_global_batch(stream, delta1, delta2, 1, meshsize, kfun, los, d_edges, nedges, step,
+                             backend, nells, ells, d_out, workspace, workspace_bytes);
+}
+
+extern "C" pk_status pk_bin_global_batch(void *stream, const void *delta1, const void *delta2,
+                                         int nbatch, const int32_t meshsize[3], const float kfun[3],
+                                         const float los[3], const float *d_edges, int nedges,
+                                         float step, int backend, int nells, const int32_t *ells,
+                                         double *d_out, void *workspace, size_t workspace_bytes) {
+  PK_REQUIRE(nbatch >= 1 && nbatch <= 65535, PK_ERR_INVALID, "nbatch must be in 1..65535");
   BinGeom g;
   pk_status st = make_geom(meshsize, kfun, nedges, step, backend, &g);
   if (st) return st;
@@ -896,10 +931,10 @@ extern "C" pk_status pk_bin_global(void *stream, const void *delta1, const void 
 #define PK_GL_CASE(N)                                                                           \
   case 2 * N:                                                                                   \
     return launch_global<N, false>(cs, g, a, b, los, lc, zero_l0, d_edges, d_out, workspace,    \
-                                   workspace_bytes);                                            \
+                                   workspace_bytes, nbatch);                                            \
   case 2 * N + 1:                                                                               \
     return launch_global<N, true>(cs, g, a, b, los, lc, zero_l0, d_edges, d_out, workspace,     \
-                                  workspace_bytes);
+                                  workspace_bytes, nbatch);
     PK_GL_CASE(1) PK_GL_CASE(2) PK_GL_CASE(3) PK_GL_CASE(4) PK_GL_CASE(5) PK_GL_CASE(6)
     PK_GL_CASE(7) PK_GL_CASE(8) PK_GL_CASE(9)
 #undef PK_GL_CASE

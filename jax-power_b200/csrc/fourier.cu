@@ -139,9 +139,12 @@ template <int NS, bool FULL>
 __global__ void __launch_bounds__(IL_THREADS) interlace_kernel(FourierParams p,
                                                                const float2 *__restrict__ in,
                                                                float2 *__restrict__ out) {
+  // (in / out are advanced to this block's mesh of the batch below)
   extern __shared__ float4 ilsmem[];
   const Dims d = p.d;
   constexpr bool full = FULL;
+  in += (int64_t)blockIdx.y * p.nshifts * d.ncomplex();  // batch of meshes along y
+  out += (int64_t)blockIdx.y * d.ncomplex();
   ZTable t;
   t.ph = reinterpret_cast<float2 *>(ilsmem);
   t.phm = t.ph + (size_t)p.nshifts * d.nz;
@@ -308,9 +311,23 @@ extern "C" pk_status pk_fft_plan_destroy(pk_fft_plan plan) {
   return PK_OK;
 }
 
+extern "C" pk_status pk_interlace_compensate_batch(void *stream, const void *in, int nbatch,
+                                                   int nshifts, const int32_t meshsize[3],
+                                                   int comp_order, int backend, int for_c2r,
+                                                   float scale, void *out);
+
 extern "C" pk_status pk_interlace_compensate(void *stream, const void *in, int nshifts,
                                              const int32_t meshsize[3], int comp_order,
                                              int backend, int for_c2r, float scale, void *out) {
+  return pk_interlace_compensate_batch(stream, in, 1, nshifts, meshsize, comp_order, backend,
+                                       for_c2r, scale, out);
+}
+
+extern "C" pk_status pk_interlace_compensate_batch(void *stream, const void *in, int nbatch,
+                                                   int nshifts, const int32_t meshsize[3],
+                                                   int comp_order, int backend, int for_c2r,
+                                                   float scale, void *out) {
+  PK_REQUIRE(nbatch >= 1 && nbatch <= 65535, PK_ERR_INVALID, "nbatch must be in 1..65535");
   PK_REQUIRE(in && out, PK_ERR_INVALID, "null buffer");
   FourierParams p;
   PK_REQUIRE(make_dims(meshsize, &p.d), PK_ERR_INVALID, "invalid meshsize");
@@ -336,7 +353,7 @@ extern "C" pk_status pk_interlace_compensate(void *stream, const void *in, int n
   const int64_t nrows = (int64_t)p.d.n0 * p.d.n1;
   const int64_t want = (nrows + IL_THREADS / 32 - 1) / (IL_THREADS / 32);
   const int64_t cap = 8LL * sm_count();
-  const int blocks = (int)(want < cap ? want : cap);
+  const dim3 blocks((unsigned)(want < cap ? want : cap), (unsigned)nbatch);
   cudaStream_t st = (cudaStream_t)stream;
   switch (nshifts * 2 + (full ? 1 : 0)) {
 #define PK_IL_CASE(N)                                                                          \

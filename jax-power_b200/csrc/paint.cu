@@ -1,21 +1,23 @@
 // Particle painting and reading (resampler scatter / gather) for sm_100a.
 //
 // Paint = resamplers.paint (resamplers.py:66-97) driven by _paint
-// (mesh.py:2673-2729) for all interlacing shifts at once.
+// (mesh.py:2673-2729) for all interlacing shifts at once, for one catalog or a batch of
+// catalogs (mocks) sharing a mesh geometry.
 //
 // Design (HBM-bound, deterministic, no global float atomics):
-//   1. pk_bucket_count: per particle, normalise the position exactly as the
-//      reference (float32 IEEE ops, mesh.py:2684), find every mesh tile its
-//      stencil can reach for any shift, and count it there (int atomics);
-//      also track max|w| (for the fixed-point scale).
+//   1. bucket_kernel<count>: per particle, normalise the position exactly as the
+//      reference (float32 IEEE ops, mesh.py:2684), find every mesh tile its stencil can
+//      reach for any shift (tiles of all mocks share one index space), and count it there
+//      (warp-aggregated int atomics); also track max|w| (fixed-point scale).
 //   2. exclusive scan of the tile counts (CUB).
-//   3. pk_bucket_fill: write (u, w) as a float4 into each reached tile's bucket.
-//   4. pk_paint_tiles: one CTA per tile: every shifted mesh of the tile is
-//      accumulated in shared memory as 64-bit fixed point (integer addition is
-//      associative, so the result does not depend on particle order or thread
-//      scheduling), then converted once to float32 and written with coalesced
-//      float4 stores.  Each output cell is written exactly once; the mesh is
-//      never memset.
+//   3. bucket_kernel<fill>: write (u, w) as a float4 into each reached tile's bucket.
+//   4. paint_tiles_kernel: one CTA per tile; every shifted mesh of the tile is accumulated
+//      in shared memory as 64-bit fixed point held in two 32-bit words (native shared
+//      atomics, exact carries), so the sum does not depend on the order of the additions;
+//      then it is converted once to float32 and written with coalesced float4 stores.
+//      Each output cell is written exactly once; the mesh is never memset.
+// Tile shapes / CTA sizes are compile-time configurations chosen by the caller's
+// autotuner (pk_paint uses configuration 0).
 #include <cub/device/device_scan.cuh>
 #include <math.h>
 
@@ -23,11 +25,36 @@
 
 namespace pk {
 
-constexpr int TILE0 = 8, TILE1 = 16, TILE2 = 32;
-constexpr int TILE_CELLS = TILE0 * TILE1 * TILE2;
 constexpr int MAX_SHIFTS = 4;
 constexpr int MAX_ORDER = 4;
 constexpr float MAX_CELL_COORD = 4194304.f;  // 2^22 cells
+constexpr int NUM_TILE_CONFIGS = 4;
+
+// Tile configurations: (cells along axes 0, 1, 2; threads per CTA).
+template <int C>
+struct TileConfig;
+template <>
+struct TileConfig<0> { static constexpr int T0 = 8, T1 = 16, T2 = 32, THREADS = 512; };
+template <>
+struct TileConfig<1> { static constexpr int T0 = 8, T1 = 16, T2 = 32, THREADS = 256; };
+template <>
+struct TileConfig<2> { static constexpr int T0 = 8, T1 = 8, T2 = 32, THREADS = 256; };
+template <>
+struct TileConfig<3> { static constexpr int T0 = 4, T1 = 16, T2 = 32, THREADS = 256; };
+
+static void tile_dims(int config, int t[3], int *threads) {
+  switch (config) {
+#define PK_TC(C)                       \
+  case C:                              \
+    t[0] = TileConfig<C>::T0;          \
+    t[1] = TileConfig<C>::T1;          \
+    t[2] = TileConfig<C>::T2;          \
+    *threads = TileConfig<C>::THREADS; \
+    return;
+    PK_TC(0) PK_TC(1) PK_TC(2) PK_TC(3)
+#undef PK_TC
+  }
+}
 
 struct PaintGeom {
   Dims d;
@@ -36,7 +63,11 @@ struct PaintGeom {
   int nshifts;
   float shifts[MAX_SHIFTS];
   int reach_lo, reach_hi;  // stencil reach below / above floor(u), all shifts
-  int nt[3];               // tiles per axis
+  int tile[3];             // tile shape
+  int nt[3];               // tiles per axis (one mock)
+  int64_t tiles_per_mock;
+  int nmocks;
+  const int64_t *offsets;  // device, nmocks + 1 particle offsets (NULL: one mock)
 };
 
 __device__ __forceinline__ float normalise(float p, float half, float center, float cell) {
@@ -119,7 +150,6 @@ __device__ __forceinline__ int span_tiles(int c, int lo, int hi, int n, int tile
     for (int k = 0; k < count; ++k) seen |= (out[k] == t);
     if (!seen && count < 3) out[count++] = t;
   }
-  (void)nt;
   return count;
 }
 
@@ -137,8 +167,20 @@ __device__ __forceinline__ bool load_particle(const PaintGeom &g, const float *p
   return ok;
 }
 
+// Mock of particle p (offsets sorted, offsets[0] = 0, offsets[nmocks] = n).
+__device__ __forceinline__ int mock_of(const PaintGeom &g, int64_t p) {
+  if (g.nmocks <= 1 || !g.offsets) return 0;
+  int lo = 0, hi = g.nmocks - 1;  // largest m with offsets[m] <= p
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(g.offsets + mid) <= p) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 // Warp-aggregated tile counting / filling: lanes of a warp that reach the same tile
-// combine into one global atomic (the catalog is often sorted by cell, so neighbours
+// combine into one global atomic (catalogs are often sorted by cell, so neighbours
 // usually share tiles).
 template <bool FILL>
 __global__ void bucket_kernel(PaintGeom g, const float *__restrict__ pos,
@@ -146,7 +188,6 @@ __global__ void bucket_kernel(PaintGeom g, const float *__restrict__ pos,
                               unsigned *__restrict__ counts, const int *__restrict__ offsets,
                               unsigned *__restrict__ cursors, float4 *__restrict__ bucket,
                               unsigned *__restrict__ wmax_bits, int *__restrict__ status) {
-  const int tiles[3] = {TILE0, TILE1, TILE2};
   const int ns[3] = {g.d.n0, g.d.n1, g.d.n2};
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -156,9 +197,11 @@ __global__ void bucket_kernel(PaintGeom g, const float *__restrict__ pos,
     const int64_t p = base + lane;
     float u[3] = {0.f, 0.f, 0.f}, wp = 0.f;
     bool ok = false;
+    int mock = 0;
     if (p < n) {
       ok = load_particle(g, pos, w, p, u, &wp) && isfinite(wp);
       if (!ok && !FILL && status) atomicExch(status, 1);
+      mock = mock_of(g, p);
     }
     if (!FILL) {
       const unsigned wb = __reduce_max_sync(FULL, ok ? __float_as_uint(fabsf(wp)) : 0u);
@@ -169,7 +212,7 @@ __global__ void bucket_kernel(PaintGeom g, const float *__restrict__ pos,
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         const int c = (int)floorf(u[d]);
-        nt[d] = span_tiles(c, g.reach_lo, g.reach_hi, ns[d], tiles[d], g.nt[d], t[d]);
+        nt[d] = span_tiles(c, g.reach_lo, g.reach_hi, ns[d], g.tile[d], g.nt[d], t[d]);
       }
     }
     const int ncopy = nt[0] * nt[1] * nt[2];
@@ -179,7 +222,8 @@ __global__ void bucket_kernel(PaintGeom g, const float *__restrict__ pos,
       const unsigned mask = __ballot_sync(FULL, act);
       if (!act) continue;
       const int c2 = k % nt[2], c1 = (k / nt[2]) % nt[1], c0 = k / (nt[2] * nt[1]);
-      const int tile = (t[0][c0] * g.nt[1] + t[1][c1]) * g.nt[2] + t[2][c2];
+      const int tile = (int)((int64_t)mock * g.tiles_per_mock +
+                             ((int64_t)t[0][c0] * g.nt[1] + t[1][c1]) * g.nt[2] + t[2][c2]);
       // one global atomic per distinct tile in the warp (sorted catalogs share tiles)
       const int first = __ffs(mask) - 1;
       const bool same = __all_sync(mask, tile == __shfl_sync(mask, tile, first));
@@ -217,28 +261,31 @@ __device__ __forceinline__ unsigned gcd_u(unsigned a, unsigned b) {
   return a;
 }
 
-constexpr int PAINT_THREADS = 512;
-
-template <int ORDER>
-__global__ void __launch_bounds__(PAINT_THREADS) paint_tiles_kernel(
+template <int ORDER, int CFG>
+__global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
     PaintGeom g, const float4 *__restrict__ bucket, const int *__restrict__ offsets,
-    const unsigned *__restrict__ wmax_bits, int64_t n, float *__restrict__ out) {
+    const unsigned *__restrict__ wmax_bits, float *__restrict__ out) {
+  using TC = TileConfig<CFG>;
+  constexpr int T0 = TC::T0, T1 = TC::T1, T2 = TC::T2, CELLS = T0 * T1 * T2;
   // Per-cell 64-bit fixed point as two 32-bit words (native shared atomics): the low word's
   // returned old value gives the exact carry into the high word, so the integer sum stays
   // exact and independent of the order of the additions.
-  extern __shared__ unsigned acc32[];  // lo[nshifts][TILE_CELLS], hi[nshifts][TILE_CELLS]
+  extern __shared__ unsigned acc32[];  // lo[nshifts][CELLS], hi[nshifts][CELLS]
   __shared__ unsigned s_mult;
-  const int tile = blockIdx.x;
+  const int64_t gtile = blockIdx.x;
+  const int mock = (int)(gtile / g.tiles_per_mock);
+  const int tile = (int)(gtile % g.tiles_per_mock);
   const int t2i = tile % g.nt[2];
   const int t1i = (tile / g.nt[2]) % g.nt[1];
   const int t0i = tile / (g.nt[2] * g.nt[1]);
-  const int los[3] = {t0i * TILE0, t1i * TILE1, t2i * TILE2};
-  const int begin = offsets[tile], end = offsets[tile + 1];
+  const int los[3] = {t0i * T0, t1i * T1, t2i * T2};
+  const int begin = offsets[gtile], end = offsets[gtile + 1];
   const unsigned count = (unsigned)(end - begin);
   const bool vec = (g.d.n2 % 4) == 0;
+  float *mock_out = out + (int64_t)mock * g.nshifts * g.d.nreal();
 
   if (count > 0) {
-    for (int i = threadIdx.x; i < 2 * g.nshifts * TILE_CELLS; i += blockDim.x) acc32[i] = 0u;
+    for (int i = threadIdx.x; i < 2 * g.nshifts * CELLS; i += blockDim.x) acc32[i] = 0u;
     if (threadIdx.x == 0) {  // Fibonacci-hash stride coprime with count: a permutation
       unsigned a = count > 2 ? ((unsigned)(0.6180339887 * count) | 1u) : 1u;
       while (gcd_u(a, count) != 1u) a += 2u;
@@ -249,9 +296,10 @@ __global__ void __launch_bounds__(PAINT_THREADS) paint_tiles_kernel(
     const float fscale = ldexpf(1.f, fexp);  // exact power-of-two scaling of each contribution
     const unsigned mult = s_mult;
     const int ns[3] = {g.d.n0, g.d.n1, g.d.n2};
-    const int tl[3] = {TILE0, TILE1, TILE2};
+    const int tl[3] = {T0, T1, T2};
     constexpr int OLO = -((ORDER - 1) / 2);
-    // permuted visiting order jdx = i * mult mod count, advanced incrementally
+    // permuted visiting order jdx = i * mult mod count (lanes of a warp far apart in the
+    // bucket, hence on different cells), advanced incrementally
     unsigned jdx = (unsigned)(((unsigned long long)threadIdx.x * mult) % count);
     const unsigned jstep = (unsigned)(((unsigned long long)blockDim.x * mult) % count);
     for (unsigned i = threadIdx.x; i < count; i += blockDim.x) {
@@ -278,8 +326,8 @@ __global__ void __launch_bounds__(PAINT_THREADS) paint_tiles_kernel(
             l[d][o] = (loc >= 0 && loc < tl[d]) ? loc : -1;
           }
         }
-        unsigned *alo = acc32 + s * TILE_CELLS;
-        unsigned *ahi = acc32 + (g.nshifts + s) * TILE_CELLS;
+        unsigned *alo = acc32 + s * CELLS;
+        unsigned *ahi = acc32 + (g.nshifts + s) * CELLS;
         const float wq = q.w;
 #pragma unroll
         for (int a = 0; a < ORDER; ++a) {
@@ -287,7 +335,7 @@ __global__ void __launch_bounds__(PAINT_THREADS) paint_tiles_kernel(
           for (int b = 0; b < ORDER; ++b) {
             const float kab = __fmul_rn(k[0][a], k[1][b]);
             const bool vab = (l[0][a] | l[1][b]) >= 0;
-            const int rowoff = (l[0][a] * TILE1 + l[1][b]) * TILE2;
+            const int rowoff = (l[0][a] * T1 + l[1][b]) * T2;
 #pragma unroll
             for (int c = 0; c < ORDER; ++c) {
               if (vab && l[2][c] >= 0) {
@@ -306,11 +354,11 @@ __global__ void __launch_bounds__(PAINT_THREADS) paint_tiles_kernel(
     __syncthreads();
     const double inv = ldexp(1.0, -fexp);
     for (int s = 0; s < g.nshifts; ++s) {
-      float *mesh = out + (int64_t)s * g.d.nreal();
-      const unsigned *alo = acc32 + s * TILE_CELLS;
-      const unsigned *ahi = acc32 + (g.nshifts + s) * TILE_CELLS;
-      for (int i = threadIdx.x * 4; i < TILE_CELLS; i += blockDim.x * 4) {
-        const int c2 = i % TILE2, c1 = (i / TILE2) % TILE1, c0 = i / (TILE2 * TILE1);
+      float *mesh = mock_out + (int64_t)s * g.d.nreal();
+      const unsigned *alo = acc32 + s * CELLS;
+      const unsigned *ahi = acc32 + (g.nshifts + s) * CELLS;
+      for (int i = threadIdx.x * 4; i < CELLS; i += blockDim.x * 4) {
+        const int c2 = i % T2, c1 = (i / T2) % T1, c0 = i / (T2 * T1);
         const int x0 = los[0] + c0, x1 = los[1] + c1, x2 = los[2] + c2;
         if (x0 >= g.d.n0 || x1 >= g.d.n1) continue;
         const int64_t base = ((int64_t)x0 * g.d.n1 + x1) * g.d.n2 + x2;
@@ -331,9 +379,9 @@ __global__ void __launch_bounds__(PAINT_THREADS) paint_tiles_kernel(
     }
   } else {
     for (int s = 0; s < g.nshifts; ++s) {
-      float *mesh = out + (int64_t)s * g.d.nreal();
-      for (int i = threadIdx.x * 4; i < TILE_CELLS; i += blockDim.x * 4) {
-        const int c2 = i % TILE2, c1 = (i / TILE2) % TILE1, c0 = i / (TILE2 * TILE1);
+      float *mesh = mock_out + (int64_t)s * g.d.nreal();
+      for (int i = threadIdx.x * 4; i < CELLS; i += blockDim.x * 4) {
+        const int c2 = i % T2, c1 = (i / T2) % T1, c0 = i / (T2 * T1);
         const int x0 = los[0] + c0, x1 = los[1] + c1, x2 = los[2] + c2;
         if (x0 >= g.d.n0 || x1 >= g.d.n1) continue;
         const int64_t base = ((int64_t)x0 * g.d.n1 + x1) * g.d.n2 + x2;
@@ -416,10 +464,12 @@ __global__ void read_kernel(PaintGeom g, const float *__restrict__ mesh,
 
 static bool fill_geom(const int32_t meshsize[3], const float boxsize[3], const float boxcenter[3],
                       const float cellsize[3], int order, int nshifts, const float *shifts,
-                      PaintGeom *g) {
+                      int config, int nmocks, PaintGeom *g) {
   if (!make_dims(meshsize, &g->d)) return false;
   if (order < 1 || order > MAX_ORDER) return false;
   if (nshifts < 1 || nshifts > MAX_SHIFTS) return false;
+  if (config < 0 || config >= NUM_TILE_CONFIGS) return false;
+  if (nmocks < 1) return false;
   for (int d = 0; d < 3; ++d) {
     g->half[d] = boxsize[d] / 2.f;
     g->center[d] = boxcenter[d];
@@ -436,8 +486,12 @@ static bool fill_geom(const int32_t meshsize[3], const float boxsize[3], const f
   const int hi = order - 1 - (order - 1) / 2;
   g->reach_lo = (order - 1) / 2;
   g->reach_hi = hi + (order & 1 ? 1 : 0) + (shifted ? 1 : 0);
-  const int tiles[3] = {TILE0, TILE1, TILE2};
-  for (int d = 0; d < 3; ++d) g->nt[d] = (meshsize[d] + tiles[d] - 1) / tiles[d];
+  int threads;
+  tile_dims(config, g->tile, &threads);
+  for (int d = 0; d < 3; ++d) g->nt[d] = (meshsize[d] + g->tile[d] - 1) / g->tile[d];
+  g->tiles_per_mock = (int64_t)g->nt[0] * g->nt[1] * g->nt[2];
+  g->nmocks = nmocks;
+  g->offsets = nullptr;
   return true;
 }
 
@@ -456,12 +510,13 @@ struct PaintLayout {
 };
 
 static pk_status paint_layout(int64_t n, const PaintGeom &g, PaintLayout *L) {
-  L->ntiles = (int64_t)g.nt[0] * g.nt[1] * g.nt[2];
+  L->ntiles = g.tiles_per_mock * g.nmocks;
+  PK_REQUIRE(L->ntiles < (int64_t)INT32_MAX / 2, PK_ERR_RANGE, "too many tiles (%lld)",
+             (long long)L->ntiles);
   const int span = g.reach_lo + g.reach_hi + 1;
-  const int tiles[3] = {TILE0, TILE1, TILE2};
   const int ns[3] = {g.d.n0, g.d.n1, g.d.n2};
   int64_t copies = 1;
-  for (int d = 0; d < 3; ++d) copies *= max_copies_axis(ns[d], tiles[d], g.nt[d], span);
+  for (int d = 0; d < 3; ++d) copies *= max_copies_axis(ns[d], g.tile[d], g.nt[d], span);
   L->max_entries = n * copies;
   PK_REQUIRE(L->max_entries < (int64_t)INT32_MAX, PK_ERR_RANGE,
              "too many particles for one paint call (%lld x %lld tile copies)", (long long)n,
@@ -480,52 +535,14 @@ static pk_status paint_layout(int64_t n, const PaintGeom &g, PaintLayout *L) {
   return PK_OK;
 }
 
-}  // namespace pk
-
-using namespace pk;
-
-extern "C" pk_status pk_paint_workspace_size(int64_t n, const int32_t meshsize[3], int order,
-                                             int nshifts, size_t *bytes) {
-  PK_REQUIRE(bytes, PK_ERR_INVALID, "bytes is NULL");
-  PK_REQUIRE(n >= 0, PK_ERR_INVALID, "negative particle count");
-  float box[3] = {1.f, 1.f, 1.f}, cen[3] = {0.f, 0.f, 0.f}, cell[3] = {1.f, 1.f, 1.f};
-  // worst-case reach: any nonzero shift
-  float shifts[MAX_SHIFTS] = {0.f, 0.5f, 0.5f, 0.5f};
-  if (nshifts > MAX_SHIFTS) nshifts = MAX_SHIFTS;
-  PaintGeom g;
-  PK_REQUIRE(fill_geom(meshsize, box, cen, cell, order, nshifts, shifts, &g), PK_ERR_INVALID,
-             "invalid meshsize / order (1..4) / nshifts (1..%d)", MAX_SHIFTS);
-  PaintLayout L;
-  pk_status st = paint_layout(n, g, &L);
-  if (st) return st;
-  *bytes = L.total;
-  return PK_OK;
-}
-
-extern "C" pk_status pk_paint(void *stream, const float *positions, const float *weights,
-                              int64_t n, const int32_t meshsize[3], const float boxsize[3],
-                              const float boxcenter[3], const float cellsize[3], int order,
-                              int interlacing, int shift_begin, int nshifts, float *out,
-                              void *workspace, size_t workspace_bytes, int *d_status) {
-  PK_REQUIRE(out, PK_ERR_INVALID, "out is NULL");
-  PK_REQUIRE(n == 0 || positions, PK_ERR_INVALID, "positions is NULL");
-  PK_REQUIRE(boxsize && boxcenter && cellsize, PK_ERR_INVALID, "geometry pointer is NULL");
-  PK_REQUIRE(interlacing >= 1 && shift_begin >= 0 && shift_begin + nshifts <= interlacing,
-             PK_ERR_INVALID, "invalid interlacing %d / shift range [%d, %d)", interlacing,
-             shift_begin, shift_begin + nshifts);
-  float shifts[MAX_SHIFTS];
-  for (int s = 0; s < MAX_SHIFTS; ++s)  // arange(I) * 1. / I in float32 (mesh.py:2679)
-    shifts[s] = s < nshifts ? (float)(shift_begin + s) / (float)interlacing : 0.f;
-  PaintGeom g;
-  PK_REQUIRE(fill_geom(meshsize, boxsize, boxcenter, cellsize, order, nshifts, shifts, &g),
-             PK_ERR_INVALID, "invalid meshsize / order (1..4) / nshifts (1..%d) / cellsize",
-             MAX_SHIFTS);
+static pk_status paint_run(cudaStream_t s, const float *positions, const float *weights,
+                           int64_t n, PaintGeom g, int config, float *out, void *workspace,
+                           size_t workspace_bytes, int *d_status) {
   PaintLayout L;
   pk_status st = paint_layout(n, g, &L);
   if (st) return st;
   PK_REQUIRE(workspace && workspace_bytes >= L.total, PK_ERR_WORKSPACE,
              "paint workspace too small: need %zu bytes, got %zu", L.total, workspace_bytes);
-  cudaStream_t s = (cudaStream_t)stream;
   Carver c(workspace);
   unsigned *counts = c.take<unsigned>(L.ntiles + 1);
   int *offsets = c.take<int>(L.ntiles + 1);
@@ -553,20 +570,98 @@ extern "C" pk_status pk_paint(void *stream, const float *positions, const float 
                                                    cursors, bucket, nullptr, nullptr);
     PK_LAUNCH_CHECK();
   }
-  const size_t smem = (size_t)nshifts * TILE_CELLS * 2 * sizeof(unsigned);
-  switch (order) {
-#define PK_ORDER_CASE(O)                                                                      \
-  case O:                                                                                     \
-    PK_CUDA(cudaFuncSetAttribute(paint_tiles_kernel<O>,                                       \
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));    \
-    paint_tiles_kernel<O><<<(unsigned)L.ntiles, PAINT_THREADS, smem, s>>>(g, bucket, offsets, \
-                                                                          wmax, n, out);      \
+  int tdims[3], tthreads;
+  tile_dims(config, tdims, &tthreads);
+  const size_t smem = (size_t)g.nshifts * tdims[0] * tdims[1] * tdims[2] * 2 * sizeof(unsigned);
+  switch (config * 8 + g.order) {
+#define PK_PAINT_CASE(C, O)                                                                    \
+  case C * 8 + O:                                                                              \
+    PK_CUDA(cudaFuncSetAttribute(paint_tiles_kernel<O, C>,                                     \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));     \
+    paint_tiles_kernel<O, C><<<(unsigned)L.ntiles, TileConfig<C>::THREADS, smem, s>>>(        \
+        g, bucket, offsets, wmax, out);                                                        \
     break;
-    PK_ORDER_CASE(1) PK_ORDER_CASE(2) PK_ORDER_CASE(3) PK_ORDER_CASE(4)
-#undef PK_ORDER_CASE
+#define PK_PAINT_CFG(C) PK_PAINT_CASE(C, 1) PK_PAINT_CASE(C, 2) PK_PAINT_CASE(C, 3) PK_PAINT_CASE(C, 4)
+    PK_PAINT_CFG(0) PK_PAINT_CFG(1) PK_PAINT_CFG(2) PK_PAINT_CFG(3)
+#undef PK_PAINT_CFG
+#undef PK_PAINT_CASE
   }
   PK_LAUNCH_CHECK();
   return PK_OK;
+}
+
+static pk_status make_shifts(int interlacing, int shift_begin, int nshifts, float shifts[MAX_SHIFTS]) {
+  PK_REQUIRE(interlacing >= 1 && shift_begin >= 0 && nshifts >= 1 && nshifts <= MAX_SHIFTS &&
+                 shift_begin + nshifts <= interlacing,
+             PK_ERR_INVALID, "invalid interlacing %d / shift range [%d, %d)", interlacing,
+             shift_begin, shift_begin + nshifts);
+  for (int s = 0; s < MAX_SHIFTS; ++s)  // arange(I) * 1. / I in float32 (mesh.py:2679)
+    shifts[s] = s < nshifts ? (float)(shift_begin + s) / (float)interlacing : 0.f;
+  return PK_OK;
+}
+
+}  // namespace pk
+
+using namespace pk;
+
+extern "C" pk_status pk_paint_batch_workspace_size(int64_t n, int nmocks, const int32_t meshsize[3],
+                                                   int order, int nshifts, int tile_config,
+                                                   size_t *bytes) {
+  PK_REQUIRE(bytes, PK_ERR_INVALID, "bytes is NULL");
+  PK_REQUIRE(n >= 0, PK_ERR_INVALID, "negative particle count");
+  float box[3] = {1.f, 1.f, 1.f}, cen[3] = {0.f, 0.f, 0.f}, cell[3] = {1.f, 1.f, 1.f};
+  // worst-case reach: any nonzero shift
+  float shifts[MAX_SHIFTS] = {0.f, 0.5f, 0.5f, 0.5f};
+  if (nshifts > MAX_SHIFTS) nshifts = MAX_SHIFTS;
+  PaintGeom g;
+  PK_REQUIRE(fill_geom(meshsize, box, cen, cell, order, nshifts, shifts, tile_config, nmocks, &g),
+             PK_ERR_INVALID,
+             "invalid meshsize / order (1..4) / nshifts (1..%d) / tile config / nmocks", MAX_SHIFTS);
+  PaintLayout L;
+  pk_status st = paint_layout(n, g, &L);
+  if (st) return st;
+  *bytes = L.total;
+  return PK_OK;
+}
+
+extern "C" pk_status pk_paint_workspace_size(int64_t n, const int32_t meshsize[3], int order,
+                                             int nshifts, size_t *bytes) {
+  return pk_paint_batch_workspace_size(n, 1, meshsize, order, nshifts, 0, bytes);
+}
+
+extern "C" pk_status pk_paint_batch(void *stream, const float *positions, const float *weights,
+                                    const int64_t *d_offsets, int64_t n, int nmocks,
+                                    const int32_t meshsize[3], const float boxsize[3],
+                                    const float boxcenter[3], const float cellsize[3], int order,
+                                    int interlacing, int shift_begin, int nshifts, int tile_config,
+                                    float *out, void *workspace, size_t workspace_bytes,
+                                    int *d_status) {
+  PK_REQUIRE(out, PK_ERR_INVALID, "out is NULL");
+  PK_REQUIRE(n == 0 || positions, PK_ERR_INVALID, "positions is NULL");
+  PK_REQUIRE(boxsize && boxcenter && cellsize, PK_ERR_INVALID, "geometry pointer is NULL");
+  PK_REQUIRE(nmocks == 1 || d_offsets, PK_ERR_INVALID, "offsets are required for several mocks");
+  float shifts[MAX_SHIFTS];
+  pk_status st = make_shifts(interlacing, shift_begin, nshifts, shifts);
+  if (st) return st;
+  PaintGeom g;
+  PK_REQUIRE(fill_geom(meshsize, boxsize, boxcenter, cellsize, order, nshifts, shifts, tile_config,
+                       nmocks, &g),
+             PK_ERR_INVALID,
+             "invalid meshsize / order (1..4) / nshifts (1..%d) / cellsize / tile config / nmocks",
+             MAX_SHIFTS);
+  g.offsets = nmocks > 1 ? d_offsets : nullptr;
+  return paint_run((cudaStream_t)stream, positions, weights, n, g, tile_config, out, workspace,
+                   workspace_bytes, d_status);
+}
+
+extern "C" pk_status pk_paint(void *stream, const float *positions, const float *weights,
+                              int64_t n, const int32_t meshsize[3], const float boxsize[3],
+                              const float boxcenter[3], const float cellsize[3], int order,
+                              int interlacing, int shift_begin, int nshifts, float *out,
+                              void *workspace, size_t workspace_bytes, int *d_status) {
+  return pk_paint_batch(stream, positions, weights, nullptr, n, 1, meshsize, boxsize, boxcenter,
+                        cellsize, order, interlacing, shift_begin, nshifts, 0, out, workspace,
+                        workspace_bytes, d_status);
 }
 
 extern "C" pk_status pk_read(void *stream, const float *mesh, const float *positions,
@@ -578,7 +673,7 @@ extern "C" pk_status pk_read(void *stream, const float *mesh, const float *posit
   PK_REQUIRE(out || grad, PK_ERR_INVALID, "nothing to write (out and grad NULL)");
   float shifts[MAX_SHIFTS] = {0.f, 0.f, 0.f, 0.f};
   PaintGeom g;
-  PK_REQUIRE(fill_geom(meshsize, boxsize, boxcenter, cellsize, order, 1, shifts, &g),
+  PK_REQUIRE(fill_geom(meshsize, boxsize, boxcenter, cellsize, order, 1, shifts, 0, 1, &g),
              PK_ERR_INVALID, "invalid meshsize / order / cellsize");
   if (n == 0) return PK_OK;
   const int threads = 256;

@@ -30,6 +30,14 @@ SIGNATURES = {
     'pk_paint_workspace_size': [c_int64, c_int32_p, c_int, c_int, ctypes.POINTER(c_size_t)],
     'pk_paint': [c_void_p, c_void_p, c_void_p, c_int64, c_int32_p, c_float_p, c_float_p, c_float_p,
                  c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_size_t, c_void_p],
+    'pk_paint_batch_workspace_size': [c_int64, c_int, c_int32_p, c_int, c_int, c_int, ctypes.POINTER(c_size_t)],
+    'pk_paint_batch': [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int, c_int32_p, c_float_p, c_float_p,
+                       c_float_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_size_t, c_void_p],
+    'pk_interlace_compensate_batch': [c_void_p, c_void_p, c_int, c_int, c_int32_p, c_int, c_int, c_int, c_float,
+                                      c_void_p],
+    'pk_bin_batch_workspace_size': [c_int32_p, c_int, c_int, c_int, ctypes.POINTER(c_size_t)],
+    'pk_bin_global_batch': [c_void_p, c_void_p, c_void_p, c_int, c_int32_p, c_float_p, c_float_p, c_void_p,
+                            c_int, c_float, c_int, c_int, c_int32_p, c_void_p, c_void_p, c_size_t],
     'pk_read': [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32_p, c_float_p, c_float_p,
                 c_float_p, c_int, c_float, c_float, c_void_p, c_void_p, c_int],
     'pk_fft_plan_create': [c_int32_p, c_int, c_int, ctypes.POINTER(c_void_p)],
