@@ -159,6 +159,105 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- batched mocks
+
+BATCHED = dict(workload='256 lognormal periodic mocks, N_p log-uniform in [1e5, 4e6], meshsize in {128, 192, 256}, '
+                        'box 1000, TSC, interlacing 2, compensate, los z, ells (0,2,4), k step 0.005 up to k_Nyq(128)',
+               nmocks=256, meshsizes=[128, 192, 256], np_range=[1e5, 4e6], boxsize=1000., interlacing=2, seed=7)
+
+
+def run_batched(nmocks=256, fp64_subset=3, group=32):
+    """Plain per-mock GPU loop vs batched launches (CUDA graph) on the same mocks."""
+    import torch
+    import jaxpower_b200 as jp
+    from jaxpower_b200.mock import lognormal_particles, power_law_pk
+    from jaxpower_b200.batch import BatchedSpectra
+    B = BATCHED
+    rng = np.random.default_rng(B['seed'])
+    lo, hi = np.log(B['np_range'][0]), np.log(B['np_range'][1])
+    targets = np.exp(rng.uniform(lo, hi, nmocks))
+    sizes = rng.choice(B['meshsizes'], nmocks)
+    kmax = float(np.pi * min(B['meshsizes']) / B['boxsize'])
+    edges = np.arange(0., kmax, 0.005)
+    mocks = []
+    for i in range(nmocks):
+        attrs = jp.MeshAttrs(meshsize=int(sizes[i]), boxsize=B['boxsize'])
+        pos = lognormal_particles(attrs, power_law_pk(), targets[i] / B['boxsize']**3, seed=1000 + i)
+        mocks.append((int(sizes[i]), pos))
+    bins = {n: jp.BinMesh2SpectrumPoles(jp.MeshAttrs(meshsize=n, boxsize=B['boxsize']), edges=edges, ells=(0, 2, 4))
+            for n in B['meshsizes']}
+    attrs_of = {n: jp.MeshAttrs(meshsize=n, boxsize=B['boxsize']) for n in B['meshsizes']}
+    torch.cuda.synchronize()
+
+    def plain(i):
+        n, pos = mocks[i]
+        mesh = jp.ParticleField(pos, attrs=attrs_of[n]).paint(resampler='tsc', interlacing=B['interlacing'],
+                                                             compensate=True, out='complex')
+        return np.array([p.num_raw for p in jp.compute_mesh2_spectrum(mesh, bin=bins[n], los='z')])
+
+    for i in range(3):
+        plain(i)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain_out = [plain(i) for i in range(nmocks)]
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    # batched: groups of `group` mocks of the same mesh size, one graph each
+    runners, inputs = [], []
+    for n in B['meshsizes']:
+        idx = [i for i in range(nmocks) if mocks[i][0] == n]
+        for start in range(0, len(idx), group):
+            sel = idx[start:start + group]
+            counts = [mocks[i][1].shape[0] for i in sel]
+            bs = BatchedSpectra(attrs_of[n], bins[n], counts, resampler='tsc', interlacing=B['interlacing'])
+            runners.append((sel, bs))
+            inputs.append(torch.cat([mocks[i][1] for i in sel]))
+    for (sel, bs), x in zip(runners, inputs):  # warm-up replays
+        bs.positions.copy_(x)
+        bs()
+    torch.cuda.synchronize()
+    batched_out = [None] * nmocks
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    results = []
+    for (sel, bs), x in zip(runners, inputs):
+        results.append(bs(x))
+    end.record()
+    torch.cuda.synchronize()
+    t_batched = start.elapsed_time(end) / 1e3
+    for (sel, bs), r in zip(runners, results):
+        r = r.cpu().numpy()
+        for j, i in enumerate(sel):
+            batched_out[i] = r[j]
+    plain_arr, batched_arr = np.array(plain_out), np.array(batched_out)
+    norm = np.array([[(n / B['boxsize'])**3 * n**3] for n, _ in mocks])  # N^3 / V_cell
+    p_plain = (plain_arr / norm[:, :, None]).reshape(nmocks, -1)
+    p_batched = (batched_arr / norm[:, :, None]).reshape(nmocks, -1)
+    scale0 = np.abs(p_plain[:, :len(edges) - 1]).max()
+    rel_batched = float(np.abs(p_batched - p_plain).max() / scale0)
+    cov_plain, cov_batched = np.cov(p_plain.T), np.cov(p_batched.T)
+    cov_rel = float(np.abs(cov_batched - cov_plain).max() / np.abs(np.diag(cov_plain)).max())
+    # float64 per-mock oracle loop on a subset of the smallest catalogs
+    from oracle.coords import Geometry
+    from oracle import paint as opaint
+    from oracle.spectrum import Bins, compute_mesh2_spectrum
+    order = sorted(range(nmocks), key=lambda i: (mocks[i][0], mocks[i][1].shape[0]))[:fp64_subset]
+    err64 = 0.
+    for i in order:
+        n, pos = mocks[i]
+        geom = Geometry(n, B['boxsize'], 0., dtype=np.float64)
+        ref = compute_mesh2_spectrum(opaint.paint(geom, pos.cpu().numpy().astype('f8'), None, 'tsc', B['interlacing'], True,
+                                                  'complex'), Bins(geom, edges=edges, ells=(0, 2, 4)), los='z')['num_raw']
+        err64 = max(err64, float(np.abs(batched_arr[i] - ref).max() / np.abs(ref[0]).max()))
+    return dict(B, nparticles_total=int(sum(m[1].shape[0] for m in mocks)),
+                plain_spectra_per_s=nmocks / t_plain, batched_spectra_per_s=nmocks / t_batched,
+                speedup=t_plain / t_batched, batched_vs_plain_max_rel=rel_batched,
+                covariance_max_rel_vs_plain=cov_rel, fp64_subset=len(order), fp64_max_rel=err64,
+                tile_configs=sorted({bs.tile_config for _, bs in runners}), graphs=len(runners),
+                timing='plain: wall clock of the per-mock public-API loop (host-synchronous per mock); '
+                       'batched: CUDA events around the graph replays (inputs resident)')
+
+
 # ----------------------------------------------------------------------------- GPU arm
 
 def run_ours(args):
@@ -256,6 +355,8 @@ def run_ours(args):
             'e2e': {'value': e2e_value, 'unit': 'spectra/s', 'h2d_bytes_per_step': int(npart * 12),
                     'd2h_bytes_per_step': int(len(W['ells']) * nbins * 8)},
             'gpu_launches': int(launches), 'stages': stage_report, 'clocks': clocks.summary()}
+    if rank == 0 and world == 1 and not args.no_batched:
+        line['batched'] = run_batched()
     if rank == 0 and world == 1 and not args.no_cpu:
         seconds, desc, cores = cpu_sample(meshsize=args.cpu_meshsize)
         line['cpu_baseline'] = {'value': 1. / seconds, 'unit': 'spectra/s', 'cores': cores, 'kind': 'port',
@@ -277,6 +378,7 @@ def main():
     parser.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
     parser.add_argument('--no-e2e', action='store_true', help='skip the end-to-end (host buffers) measurement')
     parser.add_argument('--meshsize', type=int, default=0, help='smaller mesh of the same workload (profiling)')
+    parser.add_argument('--no-batched', action='store_true', help='skip the batched-mocks measurement')
     args = parser.parse_args()
     if args.impl == 'reference':
         run_reference(args)
