@@ -35,6 +35,18 @@ WORKLOAD = dict(workload='lognormal mock 512^3, ~5e6 particles, TSC, interlacing
                          'ells (0,2,4), k step 0.005', meshsize=512, boxsize=1000., nbar=5e-3, resampler='tsc',
                 interlacing=3, compensate=True, los='z', ells=[0, 2, 4], k_step=0.005, seed=42)
 
+LEARNED = dict(workload='learned aliasing correction: lognormal mocks (benchmark P(k), N~1e6, box 1000), CIC at '
+                        '128^3 corrected towards the same catalog at 512^3; no interlacing, compensate, los z, '
+                        'ells (0,2,4), k step 0.01', low=128, high=512, gen_meshsize=256, boxsize=1000., nbar=1e-3,
+               resampler='cic', interlacing=0, kstep=0.01, ntrain=4096, nheld=512, steps=4000, batch=4096,
+               kmax_fraction_eval=0.8, seed0=100000)
+
+CUTSKY = dict(workload='cut-sky FKP, first-point los, with adjoint: ~2e6 clustered data (lognormal) and 2e7 randoms, '
+                       'r in [1000, 2000] Mpc/h, 60 deg cap, Gaussian n(r) (1500, 250), FKP weights 1/(1+n 1e4), '
+                       'boxpad 2, meshsize 512, TSC, interlacing 3, compensate, ells (0,2,4), k step 0.005',
+              ndata=2e6, nrandoms=2e7, meshsize=512, boxpad=2., resampler='tsc', interlacing=3, ells=(0, 2, 4),
+              k_step=0.005, ell_weights=(1., 0.5, 0.25), fd_step=0.25, seed=11)
+
 # kernel launches issued by each C-ABI entry point (ours, including CUB's scan kernels)
 LAUNCHES = {'pk_paint': 5, 'pk_interlace_compensate': 1, 'pk_bin_global': 2, 'pk_bin_firstpoint': 2,
             'pk_bin_modes': 2, 'pk_bin_mesh': 2, 'pk_scale_real': 1, 'pk_ylm_premultiply': 1, 'pk_read': 1}
@@ -258,6 +270,217 @@ def run_batched(nmocks=256, fp64_subset=3, group=32):
                        'batched: CUDA events around the graph replays (inputs resident)')
 
 
+def run_cutsky(reps=3):
+    """Cut-sky FKP first-point multipoles at 512^3 and the gradient of sum_l w_l P_l with
+    respect to the data positions (hand-written adjoints), checked by central differences."""
+    import torch
+    import jaxpower_b200 as jp
+    from jaxpower_b200.mock import cutsky_particles
+    from jaxpower_b200.autodiff import paint_value, spectrum_value
+    C = dict(CUTSKY)
+    data, randoms, wd, wr = cutsky_particles(ndata=C['ndata'], nrandoms=C['nrandoms'], seed=C['seed'])
+    attrs = jp.get_mesh_attrs(data, randoms, meshsize=C['meshsize'], boxpad=C['boxpad'])
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': C['k_step']}, ells=C['ells'])
+    fkp = jp.FKPField(jp.ParticleField(data, wd, attrs=attrs), jp.ParticleField(randoms, wr, attrs=attrs))
+    norm = jp.compute_fkp2_normalization(fkp, bin=b)
+    shotnoise = jp.compute_fkp2_shotnoise(fkp, bin=b)
+
+    def forward():
+        mesh = fkp.paint(resampler=C['resampler'], interlacing=C['interlacing'], compensate=True, out='real')
+        return jp.compute_mesh2_spectrum(mesh, bin=b, los='firstpoint')
+
+    def events(fn, n):
+        fn()
+        torch.cuda.synchronize()
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(n):
+            out = fn()
+        e.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(e) / 1e3 / n, out
+
+    t_fwd, poles = events(forward, reps)
+    alpha = float(wd.double().sum() / wr.double().sum())
+    weights = torch.cat([wd, -alpha * wr])
+    coef = torch.tensor(C['ell_weights'], dtype=torch.float64, device='cuda')[:, None]
+    scale = 1. / float(np.abs(poles.get(0).num_raw).max())
+
+    def loss(xd):
+        mesh = paint_value(torch.cat([xd, randoms]), weights, attrs, C['resampler'], C['interlacing'], True, 'real')
+        return (coef * spectrum_value(mesh, attrs, b, 'firstpoint')).sum() * scale
+
+    def fwd_bwd():
+        xd = data.clone().requires_grad_(True)
+        value = loss(xd)
+        value.backward()
+        return value.detach(), xd.grad
+
+    t_grad, (value, grad) = events(fwd_bwd, reps)
+    g = torch.Generator(device='cuda').manual_seed(5)
+    v = torch.randn(data.shape, generator=g, device='cuda')
+    v /= torch.linalg.norm(v, dim=1, keepdim=True)
+    h = C['fd_step']
+    with torch.no_grad():
+        lp, lm = float(loss(data + h * v)), float(loss(data - h * v))
+    fd = (lp - lm) / (2 * h)
+    ad = float((grad.double() * v.double()).sum())
+    consistency = float(abs(value.item() - float(
+        (coef.cpu().numpy() * np.array([p.num_raw for p in poles])).sum() * scale)))
+    return dict(C, ndata=int(data.shape[0]), nrandoms=int(randoms.shape[0]), boxsize=[float(x) for x in attrs.boxsize],
+                nbins=int(b.nbins), spectra_per_s=1. / t_fwd, seconds_forward=t_fwd,
+                seconds_forward_backward=t_grad, norm=float(np.mean(norm)),
+                shotnoise_ell0=float(np.mean(shotnoise[0])) if np.ndim(shotnoise) > 1 else float(np.mean(shotnoise)),
+                gradient_check={'directional_ad': ad, 'directional_fd': fd, 'rel_err': abs(ad - fd) / abs(fd),
+                                'fd_step_mpc': h, 'direction': 'random unit vector per data particle'},
+                value_api_vs_autodiff_abs=consistency,
+                timing='CUDA events, positions resident; forward = FKPField.paint + compute_mesh2_spectrum; '
+                       'forward_backward = differentiable paint + spectrum + backward to data positions')
+
+
+def run_learned(ntrain=None, nheld=None, steps=None):
+    """Train the learned correction on the GPU and evaluate it on held-out mocks."""
+    import torch
+    import jaxpower_b200 as jp
+    from jaxpower_b200.learned import (LearnedCorrection, mock_spectra, spectrum_errors, ensemble_bias,
+                                      ensemble_bias_significance)
+    L = dict(LEARNED)
+    ntrain = ntrain or L['ntrain']
+    nheld = nheld or L['nheld']
+    t0 = time.perf_counter()
+    data = mock_spectra(range(L['seed0'], L['seed0'] + ntrain + nheld), meshsizes=(L['low'], L['high']),
+                        boxsize=L['boxsize'], nbar=L['nbar'], gen_meshsize=L['gen_meshsize'],
+                        resampler=L['resampler'], interlacing=L['interlacing'], kstep=L['kstep'], group=16)
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    train = dict(data, nparticles=data['nparticles'][:ntrain],
+                 spectra={n: v[:ntrain] for n, v in data['spectra'].items()})
+    t0 = time.perf_counter()
+    corr, report = LearnedCorrection.train(train, L['low'], L['high'], steps=steps or L['steps'], batch=L['batch'],
+                                           resampler=L['resampler'], interlacing=L['interlacing'])
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    low, high = data['spectra'][L['low']][ntrain:], data['spectra'][L['high']][ntrain:]
+    npart = data['nparticles'][ntrain:]
+    fixed = corr(low, npart)
+    kmax = L['kmax_fraction_eval'] * np.pi * L['low'] / L['boxsize']
+    e_plain, _ = spectrum_errors(low, high, data['k'], kmax)
+    e_corr, _ = spectrum_errors(fixed, high, data['k'], kmax)
+    # table baseline: the training-set mean of (P_fine - P_coarse) / P0_coarse per (ell, bin)
+    tl, th = train['spectra'][L['low']], train['spectra'][L['high']]
+    table = ((th - tl) / tl[:, :1]).mean(axis=0)
+    e_table, _ = spectrum_errors(low + table[None] * low[:, :1], high, data['k'], kmax)
+    bias_corr, bias_plain = ensemble_bias(fixed, high, data['k'], kmax), ensemble_bias(low, high, data['k'], kmax)
+    _, bin_corr = spectrum_errors(fixed, high, data['k'], kmax)
+    _, bin_plain = spectrum_errors(low, high, data['k'], kmax)
+    _, bin_table = spectrum_errors(low + table[None] * low[:, :1], high, data['k'], kmax)
+
+    # time per spectrum, one catalog resident on the device, public API, host-synchronous
+    from jaxpower_b200.mock import lognormal_particles, power_law_pk
+    attrs_lo = jp.MeshAttrs(meshsize=L['low'], boxsize=L['boxsize'])
+    attrs_hi = jp.MeshAttrs(meshsize=L['high'], boxsize=L['boxsize'])
+    pos = lognormal_particles(jp.MeshAttrs(meshsize=L['gen_meshsize'], boxsize=L['boxsize']), power_law_pk(),
+                              L['nbar'], seed=7)
+    b_lo = jp.BinMesh2SpectrumPoles(attrs_lo, edges=data['edges'], ells=(0, 2, 4))
+    b_hi = jp.BinMesh2SpectrumPoles(attrs_hi, edges=data['edges'], ells=(0, 2, 4))
+
+    def plain(attrs, b):
+        mesh = jp.ParticleField(pos, attrs=attrs).paint(resampler=L['resampler'], interlacing=L['interlacing'],
+                                                        compensate=True, out='complex')
+        return np.array([p.value() for p in jp.compute_mesh2_spectrum(mesh, bin=b, los='z')])
+
+    norm_lo = float(np.prod([L['low']] * 3))**2 / pos.shape[0]**2
+
+    def learned():
+        return corr(plain(attrs_lo, b_lo) * norm_lo, pos.shape[0])
+
+    def timed(fn, reps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t) / reps
+
+    t_hi = timed(lambda: plain(attrs_hi, b_hi), 20)
+    t_lo = timed(lambda: plain(attrs_lo, b_lo), 50)
+    t_learned = timed(learned, 50)
+    # batched: 16 resident catalogs per CUDA-graph replay, timed with CUDA events; the
+    # correction runs on the device on the batch's multipoles
+    from jaxpower_b200.batch import BatchedSpectra
+    from jaxpower_b200.learned import spectrum_norm
+    gen = jp.MeshAttrs(meshsize=L['gen_meshsize'], boxsize=L['boxsize'])
+    cats = [lognormal_particles(gen, power_law_pk(), L['nbar'], seed=900 + i) for i in range(16)]
+    counts = [c.shape[0] for c in cats]
+    allpos = torch.cat(cats)
+    bs_lo = BatchedSpectra(attrs_lo, b_lo, counts, resampler=L['resampler'], interlacing=L['interlacing'])
+    bs_hi = BatchedSpectra(attrs_hi, b_hi, counts, resampler=L['resampler'], interlacing=L['interlacing'])
+    nrm_lo = torch.as_tensor(spectrum_norm(attrs_lo.meshsize, L['boxsize'], counts), device='cuda')[:, None, None]
+    npart16 = np.array(counts, dtype='f8')
+
+    def events(fn, reps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            out = fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / 1e3 / reps / 16, out
+
+    bs_lo(allpos), bs_hi(allpos)
+    tb_hi, _ = events(lambda: bs_hi(), 5)
+    tb_lo, _ = events(lambda: bs_lo(), 20)
+    tb_learned, _ = events(lambda: corr(bs_lo() * nrm_lo, npart16), 20)
+    return dict(L, ntrain=ntrain, nheld=nheld, nbins=int(len(data['k'])),
+                train_samples=int(report['ntrain'] * 3 * len(data['k'])),
+                corrected_bins=report['corrected_bins'], total_bins=report['total_bins'],
+                final_loss=float(report['loss_history'][-1]),
+                heldout_max_rel_err={'learned': {'median': float(np.median(e_corr)),
+                                                 'p95': float(np.percentile(e_corr, 95)), 'max': float(e_corr.max())},
+                                     'plain_128': {'median': float(np.median(e_plain)),
+                                                   'p95': float(np.percentile(e_plain, 95)),
+                                                   'max': float(e_plain.max())},
+                                     'mean_table_128': {'median': float(np.median(e_table)),
+                                                        'p95': float(np.percentile(e_table, 95)),
+                                                        'max': float(e_table.max())}},
+                frac_heldout_within_0p5pct=float((e_corr <= 5e-3).mean()),
+                heldout_bias_max={'learned': float(bias_corr.max()), 'plain_128': float(bias_plain.max()),
+                                  'mean_table_128': float(ensemble_bias(low + table[None] * low[:, :1], high,
+                                                                        data['k'], kmax).max()),
+                                  'per_ell_learned': [float(b) for b in bias_corr.max(axis=1)],
+                                  'per_ell_plain_128': [float(b) for b in bias_plain.max(axis=1)]},
+                heldout_bias_in_standard_errors={
+                    'learned': ensemble_bias_significance(fixed, high, data['k'], kmax),
+                    'plain_128': ensemble_bias_significance(low, high, data['k'], kmax),
+                    'mean_table_128': ensemble_bias_significance(low + table[None] * low[:, :1], high, data['k'],
+                                                                 kmax)},
+                heldout_rms_rel_err_per_ell={'learned': [float(v) for v in np.sqrt((bin_corr**2).mean(axis=(0, 2)))],
+                                             'plain_128': [float(v) for v in np.sqrt((bin_plain**2).mean(axis=(0, 2)))],
+                                             'mean_table_128': [float(v) for v in
+                                                                np.sqrt((bin_table**2).mean(axis=(0, 2)))]},
+                heldout_median_rel_err_worst_bin={
+                    'learned': float(np.median(bin_corr, axis=0).max()),
+                    'plain_128': float(np.median(bin_plain, axis=0).max()),
+                    'mean_table_128': float(np.median(bin_table, axis=0).max())},
+                bias_definition='max over (ell, k <= 0.8 k_Nyq(128)) of |mean over held-out mocks of '
+                                '(P_ell - P_ell(512^3))| / mean P_0(512^3)',
+                error_definition='per held-out mock: max over k <= 0.8 k_Nyq(128) and ell in (0,2,4) of '
+                                 '|P_ell - P_ell(512^3)| / P_0(512^3)',
+                seconds_per_spectrum={'plain_512': t_hi, 'plain_128': t_lo, 'learned_128': t_learned},
+                speedup_learned_vs_plain_512=t_hi / t_learned,
+                batched_seconds_per_spectrum={'plain_512': tb_hi, 'plain_128': tb_lo, 'learned_128': tb_learned},
+                batched_speedup_learned_vs_plain_512=tb_hi / tb_learned,
+                seconds_data_generation=t_data, seconds_training=t_train,
+                timing='seconds_per_spectrum: wall clock through the public API (paint + spectrum + host '
+                       'read-back), one resident catalog; batched_*: CUDA events around BatchedSpectra graph '
+                       'replays of 16 resident catalogs (+ the on-device correction), per spectrum')
+
+
 # ----------------------------------------------------------------------------- GPU arm
 
 def run_ours(args):
@@ -357,6 +580,10 @@ def run_ours(args):
             'gpu_launches': int(launches), 'stages': stage_report, 'clocks': clocks.summary()}
     if rank == 0 and world == 1 and not args.no_batched:
         line['batched'] = run_batched()
+    if rank == 0 and world == 1 and not args.no_cutsky:
+        line['cutsky'] = run_cutsky()
+    if rank == 0 and world == 1 and not args.no_learned:
+        line['learned'] = run_learned()
     if rank == 0 and world == 1 and not args.no_cpu:
         seconds, desc, cores = cpu_sample(meshsize=args.cpu_meshsize)
         line['cpu_baseline'] = {'value': 1. / seconds, 'unit': 'spectra/s', 'cores': cores, 'kind': 'port',
@@ -379,6 +606,8 @@ def main():
     parser.add_argument('--no-e2e', action='store_true', help='skip the end-to-end (host buffers) measurement')
     parser.add_argument('--meshsize', type=int, default=0, help='smaller mesh of the same workload (profiling)')
     parser.add_argument('--no-batched', action='store_true', help='skip the batched-mocks measurement')
+    parser.add_argument('--no-learned', action='store_true', help='skip training / evaluating the learned correction')
+    parser.add_argument('--no-cutsky', action='store_true', help='skip the cut-sky FKP first-point measurement')
     args = parser.parse_args()
     if args.impl == 'reference':
         run_reference(args)

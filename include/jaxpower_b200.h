@@ -245,6 +245,44 @@ pk_status pk_ylm_accumulate(void *stream, const float *r, const int32_t meshsize
                             const float cellsize[3], const float offset[3], int nterms,
                             const int32_t *term_ell, const int32_t *term_m, float *rho_bar);
 
+/* ---- learned aliasing correction: BF16 MLP (16 -> 128 -> 128 -> 128 -> 1, SiLU) ----
+ * No counterpart in the reference (the learned correction is a new method).  Parameters
+ * are one flat float32 array of pk_mlp_num_params() entries (W0 [128][16], b0 [128],
+ * W1 [128][128], b1, W2 [128][128], b2, W3 [8][128] (row 0 used), b3 [8] (entry 0 used))
+ * and its bf16 copy in the same layout; matrices are row-major (out x in).  Inputs are
+ * float32 rows of 16 features; idx (may be NULL) gathers the rows / targets of a batch. */
+int pk_mlp_num_params(void);
+
+/* wb = bf16(w), round to nearest even. */
+pk_status pk_mlp_cast(void *stream, const float *w, void *wb);
+
+/* y[i] = MLP(x[idx[i]]), bf16 operands with float32 accumulation, float32 biases.  With
+ * z and h (float32 [3][batch][128]) also stores the hidden pre-activations / activations
+ * for pk_mlp_backward. */
+pk_status pk_mlp_forward(void *stream, const float *x, const int32_t *idx, int batch, const void *wb,
+                         const float *w, float *y, float *z, float *h);
+
+/* Weighted MSE: loss = sum_i w_j (y_i - t_j)^2 / batch with j = idx[i]; dy = dloss/dy.
+ * weight and loss may be NULL. */
+pk_status pk_mlp_mse(void *stream, const float *y, const float *target, const float *weight,
+                     const int32_t *idx, int batch, float *dy, float *loss);
+
+pk_status pk_mlp_backward_workspace_size(int batch, size_t *bytes);
+
+/* grad = d(sum_i dy_i y_i)/d(params) from the stored z, h (deterministic: per-CTA partial
+ * gradients added in a fixed order). */
+pk_status pk_mlp_backward(void *stream, const float *x, const int32_t *idx, int batch, const void *wb,
+                          const float *z, const float *h, const float *dy, float *grad,
+                          void *workspace, size_t workspace_bytes);
+
+/* AdamW step on w (and its bf16 copy wb): t = *step (device int, steps taken so far),
+ * learning rate lr_table[min(t, ntable - 1)] (device), bias corrections 1 - beta^(t + 1),
+ * then *step = t + 1.  Everything the step depends on lives on the device, so a captured
+ * CUDA graph of training steps replays with a learning-rate schedule. */
+pk_status pk_mlp_adam(void *stream, float *w, void *wb, float *m, float *v, const float *grad,
+                      const float *lr_table, int ntable, int32_t *step, float beta1, float beta2,
+                      float eps, float weight_decay);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,393 @@
+// Small BF16 MLP for the learned aliasing correction of low-resolution spectra:
+// 4 dense layers (16 -> 128 -> 128 -> 128 -> 1), SiLU activations, BF16 weights and
+// activations as tensor-core operands with FP32 accumulation (mma.sync m16n8k16 bf16),
+// FP32 master weights, biases and Adam state.
+//   - mlp_forward_kernel: one warp per 16 samples, layer by layer through shared memory;
+//     optionally keeps pre-activations Z and activations H for the backward pass;
+//   - mlp_mse_kernel: weighted mean-squared-error loss and its gradient dL/dy (one CTA,
+//     fixed-order reduction);
+//   - mlp_backward_kernel: per CTA (64 samples) the weight and bias gradients of its
+//     samples, written as one partial row; mlp_reduce_kernel adds the rows in CTA order,
+//     so the gradient is deterministic;
+//   - mlp_adam_kernel: AdamW update of the FP32 master weights and their BF16 copies.
+// Samples can be gathered through an index array (minibatches of a resident training set).
+// There is no counterpart in the reference: the learned correction is a new method.
+#include <cuda_bf16.h>
+#include <math.h>
+
+#include "common.cuh"
+
+namespace pk {
+
+constexpr int MLP_IN = 16;      // padded input features
+constexpr int MLP_H = 128;      // hidden width
+constexpr int MLP_OUT = 8;      // padded output rows of the last layer (row 0 used)
+constexpr int MLP_WARPS = 4;    // warps per CTA
+constexpr int MLP_ROWS = 16;    // samples per warp
+constexpr int MLP_CTA_ROWS = MLP_WARPS * MLP_ROWS;
+constexpr int MLP_LD = MLP_H + 8;  // padded shared-memory row (bank-conflict-free fragments)
+
+// Parameter layout (float32 master weights and their bf16 copies share it):
+//   W0 [H][IN], b0 [H], W1 [H][H], b1 [H], W2 [H][H], b2 [H], W3 [OUT][H], b3 [OUT]
+constexpr int OFF_W0 = 0;
+constexpr int OFF_B0 = OFF_W0 + MLP_H * MLP_IN;
+constexpr int OFF_W1 = OFF_B0 + MLP_H;
+constexpr int OFF_B1 = OFF_W1 + MLP_H * MLP_H;
+constexpr int OFF_W2 = OFF_B1 + MLP_H;
+constexpr int OFF_B2 = OFF_W2 + MLP_H * MLP_H;
+constexpr int OFF_W3 = OFF_B2 + MLP_H;
+constexpr int OFF_B3 = OFF_W3 + MLP_OUT * MLP_H;
+constexpr int MLP_NPARAMS = OFF_B3 + MLP_OUT;
+
+__device__ __forceinline__ float sigmoid(float z) { return 1.f / (1.f + expf(-z)); }
+
+__device__ __forceinline__ unsigned pack_raw(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+  return (unsigned)__bfloat16_as_ushort(lo) | ((unsigned)__bfloat16_as_ushort(hi) << 16);
+}
+
+// D(16x8) += A(16x16, row-major) * B(16x8, column-major); bf16 operands, f32 accumulators.
+__device__ __forceinline__ void mma16816(float d[4], const unsigned a[4], const unsigned b[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+      "{%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// Operand fragments through accessors: A(r, k), r < 16, k < 16; B(k, n), k < 16, n < 8.
+// Lane (g = lane / 4, t = lane % 4) holds A rows g, g + 8, columns 2t, 2t + 1, 2t + 8, 2t + 9
+// and B rows 2t, 2t + 1, 2t + 8, 2t + 9 of column g (the PTX m16n8k16 fragment layout).
+template <class FA>
+__device__ __forceinline__ void load_a(unsigned a[4], FA A) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  a[0] = pack_raw(A(g, 2 * t), A(g, 2 * t + 1));
+  a[1] = pack_raw(A(g + 8, 2 * t), A(g + 8, 2 * t + 1));
+  a[2] = pack_raw(A(g, 2 * t + 8), A(g, 2 * t + 9));
+  a[3] = pack_raw(A(g + 8, 2 * t + 8), A(g + 8, 2 * t + 9));
+}
+
+template <class FB>
+__device__ __forceinline__ void load_b(unsigned b[2], FB B) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  b[0] = pack_raw(B(2 * t, g), B(2 * t + 1, g));
+  b[1] = pack_raw(B(2 * t + 8, g), B(2 * t + 9, g));
+}
+
+// Accumulator q of this lane sits at row acc_row(q), column acc_col(q) of the 16x8 tile.
+__device__ __forceinline__ int acc_row(int q) { return ((threadIdx.x & 31) >> 2) + (q >= 2 ? 8 : 0); }
+__device__ __forceinline__ int acc_col(int q) { return 2 * (threadIdx.x & 3) + (q & 1); }
+
+// One warp: acc (16 x NT*8) = act (16 x K) W^T, W [NT*8][K] bf16 row-major (out x in).
+template <int K, int NT>
+__device__ __forceinline__ void dense_warp(const __nv_bfloat16 (*act)[MLP_LD],
+                                           const __nv_bfloat16 *__restrict__ W, float acc[NT][4]) {
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[nt][q] = 0.f;
+#pragma unroll 2
+  for (int kk = 0; kk < K; kk += 16) {
+    unsigned a[4];
+    load_a(a, [&](int r, int k) { return act[r][kk + k]; });
+#pragma unroll
+    for (int nt = 0; nt < NT; ++nt) {
+      unsigned b[2];
+      load_b(b, [&](int k, int n) { return W[(nt * 8 + n) * K + kk + k]; });
+      mma16816(acc[nt], a, b);
+    }
+  }
+}
+
+__device__ __forceinline__ int sample_of(const int *__restrict__ idx, int row) {
+  return idx ? idx[row] : row;
+}
+
+// Forward pass.  X [*][MLP_IN] float32 (zero-padded features), rows gathered through idx
+// (or the first `batch` rows); y [batch].  With Z and H, stores the pre-activations
+// Z[l][batch][H] and activations H[l][batch][H] of the hidden layers l < 3.
+__global__ void __launch_bounds__(MLP_WARPS * 32) mlp_forward_kernel(
+    const float *__restrict__ X, const int *__restrict__ idx, int batch,
+    const __nv_bfloat16 *__restrict__ Wb, const float *__restrict__ Wf, float *__restrict__ y,
+    float *__restrict__ Z, float *__restrict__ H) {
+  __shared__ __nv_bfloat16 act_all[MLP_WARPS][MLP_ROWS][MLP_LD];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row0 = (blockIdx.x * MLP_WARPS + warp) * MLP_ROWS;
+  __nv_bfloat16(*act)[MLP_LD] = act_all[warp];
+  for (int i = lane; i < MLP_ROWS * MLP_IN; i += 32) {
+    const int r = i / MLP_IN, c = i % MLP_IN;
+    const float v = (row0 + r < batch) ? X[(int64_t)sample_of(idx, row0 + r) * MLP_IN + c] : 0.f;
+    act[r][c] = __float2bfloat16_rn(v);
+  }
+  __syncwarp();
+  for (int l = 0; l < 3; ++l) {
+    float acc[MLP_H / 8][4];
+    if (l == 0) dense_warp<MLP_IN, MLP_H / 8>(act, Wb + OFF_W0, acc);
+    else dense_warp<MLP_H, MLP_H / 8>(act, Wb + (l == 1 ? OFF_W1 : OFF_W2), acc);
+    const float *bias = Wf + (l == 0 ? OFF_B0 : (l == 1 ? OFF_B1 : OFF_B2));
+    __syncwarp();
+#pragma unroll
+    for (int nt = 0; nt < MLP_H / 8; ++nt)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int r = acc_row(q), c = nt * 8 + acc_col(q);
+        const float z = acc[nt][q] + bias[c];
+        const float h = z * sigmoid(z);
+        act[r][c] = __float2bfloat16_rn(h);
+        if (Z && row0 + r < batch) {
+          Z[((int64_t)l * batch + row0 + r) * MLP_H + c] = z;
+          H[((int64_t)l * batch + row0 + r) * MLP_H + c] = h;
+        }
+      }
+    __syncwarp();
+  }
+  float acc[1][4];
+  dense_warp<MLP_H, 1>(act, Wb + OFF_W3, acc);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int r = acc_row(q);
+    if (acc_col(q) == 0 && row0 + r < batch) y[row0 + r] = acc[0][q] + Wf[OFF_B3];
+  }
+}
+
+// loss = sum_i w_i (y_i - t_i)^2 / batch, dy_i = 2 w_i (y_i - t_i) / batch; one CTA,
+// fixed-order reduction.  Targets and sample weights are gathered through idx.
+constexpr int MSE_THREADS = 1024;
+__global__ void __launch_bounds__(MSE_THREADS) mlp_mse_kernel(
+    const float *__restrict__ y, const float *__restrict__ target, const float *__restrict__ weight,
+    const int *__restrict__ idx, int batch, float *__restrict__ dy, float *__restrict__ loss) {
+  __shared__ double part[MSE_THREADS / 32];
+  double s = 0.;
+  const float inv = 1.f / (float)batch;
+  for (int i = threadIdx.x; i < batch; i += MSE_THREADS) {
+    const int j = sample_of(idx, i);
+    const float w = weight ? weight[j] : 1.f;
+    const float d = y[i] - target[j];
+    dy[i] = 2.f * w * d * inv;
+    s += (double)(w * d * d);
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.;
+    for (int w = 0; w < MSE_THREADS / 32; ++w) t += part[w];
+    if (loss) *loss = (float)(t / batch);
+  }
+}
+
+struct BackwardShared {
+  __nv_bfloat16 dz[MLP_CTA_ROWS][MLP_LD];   // dL/dZ of the current layer (bf16 operand)
+  __nv_bfloat16 hin[MLP_CTA_ROWS][MLP_LD];  // the layer's input activations (bf16)
+  float dzf[MLP_CTA_ROWS][MLP_H];           // dL/dZ in float (bias gradients)
+  float dh[MLP_CTA_ROWS][MLP_H];            // dL/dH of the current layer
+};
+
+// Backward pass of the loss gradient dy [batch].  Each CTA writes the gradients of its
+// 64 samples into partial[blockIdx.x][MLP_NPARAMS].  The operands are rounded as in the
+// forward pass: dW = bf16(dZ)^T bf16(A), dH_prev = bf16(dZ) bf16(W), both in f32.
+__global__ void __launch_bounds__(MLP_WARPS * 32) mlp_backward_kernel(
+    const float *__restrict__ X, const int *__restrict__ idx, int batch,
+    const __nv_bfloat16 *__restrict__ Wb, const float *__restrict__ Z, const float *__restrict__ H,
+    const float *__restrict__ dy, float *__restrict__ partial) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BackwardShared &sh = *reinterpret_cast<BackwardShared *>(smem_raw);
+  const int warp = threadIdx.x >> 5;
+  const int cta_row0 = blockIdx.x * MLP_CTA_ROWS;
+  float *out = partial + (size_t)blockIdx.x * MLP_NPARAMS;
+  // output layer y = bf16(H2) . W3[0] + b3:  dH2 = dy W3[0], dW3[0] = sum dy bf16(H2), db3 = sum dy
+  for (int i = threadIdx.x; i < MLP_CTA_ROWS * MLP_H; i += blockDim.x) {
+    const int r = i / MLP_H, c = i % MLP_H, row = cta_row0 + r;
+    const float g = row < batch ? dy[row] : 0.f;
+    sh.dh[r][c] = g * __bfloat162float(Wb[OFF_W3 + c]);
+  }
+  for (int c = threadIdx.x; c < MLP_H; c += blockDim.x) {
+    float s = 0.f;
+    for (int r = 0; r < MLP_CTA_ROWS; ++r) {
+      const int row = cta_row0 + r;
+      if (row < batch)
+        s += dy[row] * __bfloat162float(__float2bfloat16_rn(H[((int64_t)2 * batch + row) * MLP_H + c]));
+    }
+    out[OFF_W3 + c] = s;
+  }
+  for (int c = MLP_H + threadIdx.x; c < MLP_OUT * MLP_H + MLP_OUT; c += blockDim.x) {
+    float s = 0.f;
+    if (c == MLP_OUT * MLP_H)
+      for (int r = 0; r < MLP_CTA_ROWS; ++r)
+        if (cta_row0 + r < batch) s += dy[cta_row0 + r];
+    out[OFF_W3 + c] = s;  // unused output rows and bias entries get zero gradient
+  }
+  __syncthreads();
+  for (int l = 2; l >= 0; --l) {
+    for (int i = threadIdx.x; i < MLP_CTA_ROWS * MLP_H; i += blockDim.x) {
+      const int r = i / MLP_H, c = i % MLP_H, row = cta_row0 + r;
+      float g = 0.f, hv = 0.f;
+      if (row < batch) {
+        const float z = Z[((int64_t)l * batch + row) * MLP_H + c];
+        const float s = sigmoid(z);
+        g = sh.dh[r][c] * (s * (1.f + z * (1.f - s)));
+        if (l > 0) hv = H[((int64_t)(l - 1) * batch + row) * MLP_H + c];
+        else if (c < MLP_IN) hv = X[(int64_t)sample_of(idx, row) * MLP_IN + c];
+      }
+      sh.dzf[r][c] = g;
+      sh.dz[r][c] = __float2bfloat16_rn(g);
+      sh.hin[r][c] = __float2bfloat16_rn(hv);
+    }
+    __syncthreads();
+    const int boff = l == 0 ? OFF_B0 : (l == 1 ? OFF_B1 : OFF_B2);
+    for (int c = threadIdx.x; c < MLP_H; c += blockDim.x) {
+      float s = 0.f;
+      for (int r = 0; r < MLP_CTA_ROWS; ++r) s += sh.dzf[r][c];
+      out[boff + c] = s;
+    }
+    // dW[n][k] = sum_r dZ[r][n] A[r][k]: M = 128 outputs (2 m-tiles per warp), N = inputs,
+    // reduction over the CTA's 64 samples
+    const int K = l == 0 ? MLP_IN : MLP_H;
+    const int woff = l == 0 ? OFF_W0 : (l == 1 ? OFF_W1 : OFF_W2);
+    for (int mt = warp * 2; mt < warp * 2 + 2; ++mt) {
+      unsigned a[MLP_CTA_ROWS / 16][4];
+#pragma unroll
+      for (int ks = 0; ks < MLP_CTA_ROWS / 16; ++ks)
+        load_a(a[ks], [&](int m, int k) { return sh.dz[ks * 16 + k][mt * 16 + m]; });
+      for (int nt = 0; nt < K / 8; ++nt) {
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int ks = 0; ks < MLP_CTA_ROWS / 16; ++ks) {
+          unsigned b[2];
+          load_b(b, [&](int k, int n) { return sh.hin[ks * 16 + k][nt * 8 + n]; });
+          mma16816(acc, a[ks], b);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          out[woff + (mt * 16 + acc_row(q)) * K + nt * 8 + acc_col(q)] = acc[q];
+      }
+    }
+    if (l > 0) {
+      // dH_prev = dZ W: rows = the warp's 16 samples, N = 128 inputs, reduction over outputs
+      __syncthreads();
+      const __nv_bfloat16 *W = Wb + (l == 1 ? OFF_W1 : OFF_W2);
+      for (int nt = 0; nt < MLP_H / 8; ++nt) {
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 2
+        for (int kk = 0; kk < MLP_H; kk += 16) {
+          unsigned a[4], b[2];
+          load_a(a, [&](int r, int k) { return sh.dz[warp * 16 + r][kk + k]; });
+          load_b(b, [&](int k, int n) { return W[(kk + k) * MLP_H + nt * 8 + n]; });
+          mma16816(acc, a, b);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) sh.dh[warp * 16 + acc_row(q)][nt * 8 + acc_col(q)] = acc[q];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// grad[p] = sum over the CTA partial rows, in CTA order.
+__global__ void mlp_reduce_kernel(const float *__restrict__ partial, int nblocks, float *__restrict__ grad) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < MLP_NPARAMS; p += gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int b = 0; b < nblocks; ++b) s += partial[(size_t)b * MLP_NPARAMS + p];
+    grad[p] = s;
+  }
+}
+
+// AdamW step t + 1 with t = *step (then *step = t + 1): m, v moments, bias corrections
+// 1 - beta^(t+1), decoupled weight decay, learning rate lr_table[min(t, ntable - 1)].  One
+// CTA, so the step counter advances after every thread has read it; the whole training
+// step can then be replayed from a CUDA graph.
+constexpr int ADAM_THREADS = 1024;
+__global__ void __launch_bounds__(ADAM_THREADS) mlp_adam_kernel(
+    float *__restrict__ w, __nv_bfloat16 *__restrict__ wb, float *__restrict__ m, float *__restrict__ v,
+    const float *__restrict__ g, const float *__restrict__ lr_table, int ntable, int *__restrict__ step,
+    float beta1, float beta2, float eps, float wd) {
+  const int t = *step;
+  const float rate = lr_table[min(t, ntable - 1)];
+  const float c1 = 1.f - powf(beta1, (float)(t + 1)), c2 = 1.f - powf(beta2, (float)(t + 1));
+  for (int p = threadIdx.x; p < MLP_NPARAMS; p += ADAM_THREADS) {
+    const float gp = g[p];
+    const float mp = beta1 * m[p] + (1.f - beta1) * gp;
+    const float vp = beta2 * v[p] + (1.f - beta2) * gp * gp;
+    m[p] = mp;
+    v[p] = vp;
+    const float wp = w[p] - rate * ((mp / c1) / (sqrtf(vp / c2) + eps) + wd * w[p]);
+    w[p] = wp;
+    wb[p] = __float2bfloat16_rn(wp);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *step = t + 1;
+}
+
+__global__ void mlp_cast_kernel(const float *__restrict__ w, __nv_bfloat16 *__restrict__ wb) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < MLP_NPARAMS; p += gridDim.x * blockDim.x)
+    wb[p] = __float2bfloat16_rn(w[p]);
+}
+
+}  // namespace pk
+
+using namespace pk;
+
+extern "C" int pk_mlp_num_params(void) { return MLP_NPARAMS; }
+
+extern "C" pk_status pk_mlp_cast(void *stream, const float *w, void *wb) {
+  PK_REQUIRE(w && wb, PK_ERR_INVALID, "mlp_cast: null pointer");
+  mlp_cast_kernel<<<(MLP_NPARAMS + 255) / 256, 256, 0, (cudaStream_t)stream>>>(w, (__nv_bfloat16 *)wb);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+extern "C" pk_status pk_mlp_forward(void *stream, const float *x, const int *idx, int batch, const void *wb,
+                                    const float *w, float *y, float *z, float *h) {
+  PK_REQUIRE(x && wb && w && y && batch >= 0, PK_ERR_INVALID, "mlp_forward: invalid arguments");
+  PK_REQUIRE((z == nullptr) == (h == nullptr), PK_ERR_INVALID, "mlp_forward: z and h go together");
+  if (batch == 0) return PK_OK;
+  const int blocks = (batch + MLP_CTA_ROWS - 1) / MLP_CTA_ROWS;
+  mlp_forward_kernel<<<blocks, MLP_WARPS * 32, 0, (cudaStream_t)stream>>>(
+      x, idx, batch, (const __nv_bfloat16 *)wb, w, y, z, h);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+extern "C" pk_status pk_mlp_mse(void *stream, const float *y, const float *target, const float *weight,
+                                const int *idx, int batch, float *dy, float *loss) {
+  PK_REQUIRE(y && target && dy && batch > 0, PK_ERR_INVALID, "mlp_mse: invalid arguments");
+  mlp_mse_kernel<<<1, MSE_THREADS, 0, (cudaStream_t)stream>>>(y, target, weight, idx, batch, dy, loss);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+extern "C" pk_status pk_mlp_backward_workspace_size(int batch, size_t *bytes) {
+  PK_REQUIRE(bytes && batch >= 0, PK_ERR_INVALID, "mlp_backward_workspace_size: invalid arguments");
+  const int blocks = (batch + MLP_CTA_ROWS - 1) / MLP_CTA_ROWS;
+  *bytes = (size_t)(blocks > 0 ? blocks : 1) * MLP_NPARAMS * sizeof(float);
+  return PK_OK;
+}
+
+extern "C" pk_status pk_mlp_backward(void *stream, const float *x, const int *idx, int batch, const void *wb,
+                                     const float *z, const float *h, const float *dy, float *grad,
+                                     void *workspace, size_t workspace_bytes) {
+  PK_REQUIRE(x && wb && z && h && dy && grad && batch > 0, PK_ERR_INVALID, "mlp_backward: invalid arguments");
+  const int blocks = (batch + MLP_CTA_ROWS - 1) / MLP_CTA_ROWS;
+  PK_REQUIRE(workspace && workspace_bytes >= (size_t)blocks * MLP_NPARAMS * sizeof(float), PK_ERR_WORKSPACE,
+             "mlp_backward: workspace too small");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int smem = (int)sizeof(BackwardShared);
+  PK_CUDA(cudaFuncSetAttribute(mlp_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  float *partial = static_cast<float *>(workspace);
+  mlp_backward_kernel<<<blocks, MLP_WARPS * 32, smem, s>>>(x, idx, batch, (const __nv_bfloat16 *)wb, z, h, dy,
+                                                           partial);
+  PK_LAUNCH_CHECK();
+  mlp_reduce_kernel<<<(MLP_NPARAMS + 255) / 256, 256, 0, s>>>(partial, blocks, grad);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+extern "C" pk_status pk_mlp_adam(void *stream, float *w, void *wb, float *m, float *v, const float *grad,
+                                 const float *lr_table, int ntable, int *step, float beta1, float beta2,
+                                 float eps, float weight_decay) {
+  PK_REQUIRE(w && wb && m && v && grad && lr_table && step && ntable >= 1, PK_ERR_INVALID,
+             "mlp_adam: invalid arguments");
+  mlp_adam_kernel<<<1, ADAM_THREADS, 0, (cudaStream_t)stream>>>(w, (__nv_bfloat16 *)wb, m, v, grad, lr_table,
+                                                                ntable, step, beta1, beta2, eps, weight_decay);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}

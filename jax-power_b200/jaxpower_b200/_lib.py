@@ -69,6 +69,15 @@ SIGNATURES = {
                           c_void_p],
     'pk_ylm_premultiply': [c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_int, c_int32_p,
                            c_int32_p, c_void_p],
+    'pk_mlp_num_params': [],
+    'pk_mlp_cast': [c_void_p, c_void_p, c_void_p],
+    'pk_mlp_forward': [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p],
+    'pk_mlp_mse': [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p],
+    'pk_mlp_backward_workspace_size': [c_int, ctypes.POINTER(c_size_t)],
+    'pk_mlp_backward': [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                        c_void_p, c_size_t],
+    'pk_mlp_adam': [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p,
+                    c_float, c_float, c_float, c_float],
 }
 
 _lib = None

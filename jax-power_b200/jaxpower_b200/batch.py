@@ -31,8 +31,8 @@ class BatchedSpectra:
     bin : BinMesh2SpectrumPoles on ``attrs``
     counts : particles per catalog (the concatenated positions follow this order)
     resampler, interlacing, compensate, los : as ``ParticleField.paint`` / ``compute_mesh2_spectrum``
-    tile_config : paint tile configuration, or None to autotune
-    graph : capture the batch in a CUDA graph (replayed by every call)
+    tile_config : paint tile configuration, or None to autotune on the first call's inputs
+    graph : capture the batch in a CUDA graph (at the first call, replayed by every call)
     """
 
     def __init__(self, attrs, bin, counts, resampler='tsc', interlacing=2, compensate=True, los='z',
@@ -70,19 +70,28 @@ class BatchedSpectra:
         self.plan = _plan(shape, M * I, 0)
         factors = torch.tensor(_ell_factors(bin.ells, self.vlos), dtype=torch.float64, device=dev)
         self.scale = factors[:, None] / torch.as_tensor(bin.nmodes, dtype=torch.float64, device=dev)[None, :]
-        if tile_config is None:
-            key = make_key('paint', shape, self.order, I, M, int(np.log2(max(self.n // max(M, 1), 1))))
-            tile_config = best_tile_config(key, self._paint_with)
         self.tile_config = tile_config
-        self.paint_ws = self._paint_workspace(tile_config)
+        self.use_graph = bool(graph)
         self.graph = None
-        if graph:
+        self.paint_ws = None
+        self._ready = False
+
+    def _prepare(self):
+        """Autotune (on the first real inputs), allocate the paint workspace, capture the graph."""
+        if self.tile_config is None:
+            shape = tuple(int(s) for s in self.attrs.meshsize)
+            key = make_key('paint', shape, self.order, self.interlacing, self.nmocks,
+                           int(np.log2(max(self.n // max(self.nmocks, 1), 1))))
+            self.tile_config = best_tile_config(key, self._paint_with)
+        self.paint_ws = self._paint_workspace(self.tile_config)
+        if self.use_graph:
             self._enqueue()  # warm-up outside capture
             torch.cuda.synchronize()
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g):
                 self._enqueue()
             self.graph = g
+        self._ready = True
 
     def _paint_workspace(self, config):
         nbytes = _lib.c_size_t()
@@ -123,6 +132,8 @@ class BatchedSpectra:
             if self.weights is None:
                 raise ValueError('construct with weights=True to pass weights')
             self.weights.copy_(weights)
+        if not self._ready:
+            self._prepare()
         if self.graph is not None:
             self.graph.replay()
         else:

@@ -8,6 +8,10 @@
   Poisson counts with mean nbar V_cell (1 + delta_LN) per cell, positions uniform
   within each cell.
 - ``generate_uniform_particles`` (``mock.py:180-207``): uniform positions in the box.
+- ``cutsky_particles`` (not in the reference; the cut-sky FKP benchmark catalog): data
+  and randoms in a spherical shell within a cap around +z seen from the origin, with a
+  Gaussian radial density n(r); data clustered by a lognormal field, FKP weights
+  1 / (1 + n(r) P0).
 
 Random streams are torch's CUDA Philox generator, seeded; they are not
 jax.random streams.
@@ -17,7 +21,8 @@ import torch
 
 from .mesh import MeshAttrs, RealMeshField, ParticleField, _r2c, _c2r, _device
 
-__all__ = ['power_law_pk', 'generate_gaussian_mesh', 'lognormal_particles', 'generate_uniform_particles']
+__all__ = ['power_law_pk', 'generate_gaussian_mesh', 'lognormal_particles', 'generate_uniform_particles',
+           'cutsky_particles']
 
 
 def power_law_pk(amplitude=2e4, k0=0.1, index=-1.5, kcut=0.5):
@@ -86,3 +91,84 @@ def generate_uniform_particles(mattrs, size, seed=42, exchange=False, **kwargs):
     center = torch.as_tensor(mattrs.boxcenter, device=u.device)
     positions = box * u - box / 2. + center
     return ParticleField(positions, attrs=mattrs, **kwargs)
+
+
+def _radial_profile(rmin, rmax, rmean, rsigma, ndata, solid_angle, ngrid=4096):
+    """n(r) = A exp(-(r - rmean)^2 / (2 rsigma^2)) normalised to ndata objects in the shell;
+    returns (n(r) as a torch function, (r grid, CDF of r^2 n(r)) for inverse sampling)."""
+    r = np.linspace(rmin, rmax, ngrid)
+    shape = np.exp(-0.5 * ((r - rmean) / rsigma)**2)
+    dens = shape * r**2
+    cdf = np.concatenate([[0.], np.cumsum(0.5 * (dens[1:] + dens[:-1]) * np.diff(r))])
+    amplitude = ndata / (solid_angle * cdf[-1])
+
+    def nofr(x):
+        return amplitude * torch.exp(-0.5 * ((x - rmean) / rsigma)**2)
+
+    return nofr, (r, cdf / cdf[-1])
+
+
+def cutsky_particles(ndata=2e6, nrandoms=2e7, rmin=1000., rmax=2000., half_angle=60., rmean=1500., rsigma=250.,
+                     power=None, fkp_p0=1e4, gen_meshsize=256, seed=42):
+    """Cut-sky data and randoms seen from the origin (float32 device tensors).
+
+    Randoms: exactly ``nrandoms`` points, cos(theta) uniform in [cos(half_angle), 1],
+    phi uniform, r drawn from r^2 n(r) on [rmin, rmax].  Data: Poisson counts with mean
+    n(r_c) V_cell (1 + delta_LN) in the cells of a ``gen_meshsize`` lognormal field over the
+    survey's bounding cube, positions uniform in each cell, then cut to the shell and cap
+    (about ``ndata`` objects).  Returns (data, randoms, data_weights, randoms_weights) with
+    FKP weights 1 / (1 + n(r) fkp_p0).
+    """
+    dev = _device()
+    power = power or power_law_pk()
+    cosmin = float(np.cos(np.radians(half_angle)))
+    solid = 2. * np.pi * (1. - cosmin)
+    nofr, (rgrid, cdf) = _radial_profile(rmin, rmax, rmean, rsigma, float(ndata), solid)
+    g = _generator(seed)
+
+    def sample_r(u):
+        return torch.as_tensor(np.interp(u.cpu().numpy(), cdf, rgrid), dtype=torch.float32, device=dev)
+
+    def to_cartesian(r, mu, phi):
+        st = torch.sqrt(torch.clamp(1. - mu * mu, min=0.))
+        return torch.stack([r * st * torch.cos(phi), r * st * torch.sin(phi), r * mu], dim=1).to(torch.float32)
+
+    nr = int(nrandoms)
+    u = torch.rand((nr, 3), generator=g, device=dev, dtype=torch.float64)
+    randoms = to_cartesian(sample_r(u[:, 0]).double(), cosmin + (1. - cosmin) * u[:, 1], 2. * np.pi * u[:, 2])
+    # lognormal field over the bounding cube of the survey
+    smax = rmax * np.sin(np.radians(half_angle)) if half_angle < 90. else rmax
+    lo = np.array([-smax, -smax, min(rmin * cosmin, rmax * cosmin)])
+    hi = np.array([smax, smax, rmax])
+    box = float((hi - lo).max())
+    center = 0.5 * (lo + hi)
+    attrs = MeshAttrs(meshsize=gen_meshsize, boxsize=box, boxcenter=center)
+    delta = generate_gaussian_mesh(attrs, power, seed=seed + 1).value
+    sigma2 = float(delta.double().pow(2).mean())
+    lam = torch.exp(delta - 0.5 * sigma2)
+    del delta
+    cell = float(box / gen_meshsize)
+    idx = torch.arange(gen_meshsize, device=dev, dtype=torch.float32)
+    cx = (idx + 0.5) * cell + float(center[0] - box / 2)
+    cy = (idx + 0.5) * cell + float(center[1] - box / 2)
+    cz = (idx + 0.5) * cell + float(center[2] - box / 2)
+    rc = torch.sqrt(cx[:, None, None]**2 + cy[None, :, None]**2 + cz[None, None, :]**2)
+    lam.mul_(nofr(rc) * cell**3)
+    del rc
+    counts = torch.poisson(lam, generator=_generator(seed + 2)).to(torch.int64).reshape(-1)
+    del lam
+    cells = torch.repeat_interleave(torch.arange(counts.numel(), device=dev), counts)
+    del counts
+    n = gen_meshsize
+    ijk = torch.stack([cells // (n * n), (cells // n) % n, cells % n], dim=1).to(torch.float32)
+    del cells
+    ud = torch.rand(ijk.shape, generator=g, device=dev, dtype=torch.float32)
+    origin = torch.as_tensor(center - box / 2., dtype=torch.float32, device=dev)
+    data = (ijk + ud) * cell + origin
+    del ijk, ud
+    r = torch.linalg.norm(data.double(), dim=1)
+    keep = (r >= rmin) & (r <= rmax) & (data[:, 2].double() >= cosmin * r)
+    data = data[keep].contiguous()
+    wd = (1. / (1. + nofr(torch.linalg.norm(data.double(), dim=1)) * fkp_p0)).to(torch.float32)
+    wr = (1. / (1. + nofr(torch.linalg.norm(randoms.double(), dim=1)) * fkp_p0)).to(torch.float32)
+    return data, randoms.contiguous(), wd, wr
