@@ -63,7 +63,8 @@ struct PaintGeom {
   int nshifts;
   float shifts[MAX_SHIFTS];
   int reach_lo, reach_hi;  // stencil reach below / above floor(u), all shifts
-  int tile[3];             // tile shape
+  int tile[3];             // tile shape (powers of two)
+  int tshift[3];           // log2 of the tile shape
   int nt[3];               // tiles per axis (one mock)
   int64_t tiles_per_mock;
   int nmocks;
@@ -134,22 +135,28 @@ __device__ __forceinline__ int offset_lo(int order) { return -((order - 1) / 2);
 // Distinct tiles of the wrapped cell span [c - lo, c + hi] along one axis.  When every
 // tile on the axis is at least as long as the span (the usual case), the span touches the
 // tiles of its two ends only.
-__device__ __forceinline__ int span_tiles(int c, int lo, int hi, int n, int tile, int nt,
+__device__ __forceinline__ int span_tiles(int c, int lo, int hi, int n, int tshift, int nt,
                                           int out[3]) {
-  const int last = n - (nt - 1) * tile;
+  const int last = n - ((nt - 1) << tshift);
   if (last >= lo + hi || nt == 1) {
-    const int a = wrapi(c - lo, n) / tile, b = wrapi(c + hi, n) / tile;
+    const int a = wrapi(c - lo, n) >> tshift, b = wrapi(c + hi, n) >> tshift;
     out[0] = a;
     out[1] = b;
     return a == b ? 1 : 2;
   }
-  int count = 0;
+  // short last tile: up to 3 distinct tiles, kept in registers (no dynamic indexing)
+  int count = 0, t0 = -1, t1 = -1, t2 = -1;
   for (int x = c - lo; x <= c + hi; ++x) {
-    int t = wrapi(x, n) / tile;
-    bool seen = false;
-    for (int k = 0; k < count; ++k) seen |= (out[k] == t);
-    if (!seen && count < 3) out[count++] = t;
+    const int t = wrapi(x, n) >> tshift;
+    if (t == t0 || t == t1 || t == t2) continue;
+    if (count == 0) t0 = t;
+    else if (count == 1) t1 = t;
+    else if (count == 2) t2 = t;
+    count += count < 3;
   }
+  out[0] = t0;
+  out[1] = t1;
+  out[2] = t2;
   return count;
 }
 
@@ -179,9 +186,28 @@ __device__ __forceinline__ int mock_of(const PaintGeom &g, int64_t p) {
   return lo;
 }
 
-// Warp-aggregated tile counting / filling: lanes of a warp that reach the same tile
-// combine into one global atomic (catalogs are often sorted by cell, so neighbours
-// usually share tiles).
+// Mock of particle base + lane for a warp's 32 consecutive particles: one search by lane 0
+// when the whole warp lies in one mock (the usual case), else one per lane.
+__device__ __forceinline__ int warp_mock_of(const PaintGeom &g, int64_t base, int64_t n) {
+  if (g.nmocks <= 1 || !g.offsets) return 0;
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  int m0 = 0;
+  bool same = false;
+  if (lane == 0) {
+    m0 = mock_of(g, base);
+    const int64_t last = min(base + 31, n - 1);
+    same = __ldg(g.offsets + m0 + 1) > last;
+  }
+  m0 = __shfl_sync(FULL, m0, 0);
+  same = __shfl_sync(FULL, (int)same, 0) != 0;
+  if (same) return m0;
+  return base + lane < n ? mock_of(g, base + lane) : m0;
+}
+
+// Warp-aggregated tile counting / filling: a run of consecutive lanes that reach the same
+// tile makes one global atomic (catalogs are often sorted by cell, so neighbouring
+// particles usually share tiles); the lanes of a run then fill consecutive bucket slots.
 template <bool FILL>
 __global__ void bucket_kernel(PaintGeom g, const float *__restrict__ pos,
                               const float *__restrict__ w, int64_t n,
@@ -198,10 +224,10 @@ __global__ void bucket_kernel(PaintGeom g, const float *__restrict__ pos,
     float u[3] = {0.f, 0.f, 0.f}, wp = 0.f;
     bool ok = false;
     int mock = 0;
+    mock = warp_mock_of(g, base, n);
     if (p < n) {
       ok = load_particle(g, pos, w, p, u, &wp) && isfinite(wp);
       if (!ok && !FILL && status) atomicExch(status, 1);
-      mock = mock_of(g, p);
     }
     if (!FILL) {
       const unsigned wb = __reduce_max_sync(FULL, ok ? __float_as_uint(fabsf(wp)) : 0u);
@@ -212,31 +238,46 @@ __global__ void bucket_kernel(PaintGeom g, const float *__restrict__ pos,
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         const int c = (int)floorf(u[d]);
-        nt[d] = span_tiles(c, g.reach_lo, g.reach_hi, ns[d], g.tile[d], g.nt[d], t[d]);
+        nt[d] = span_tiles(c, g.reach_lo, g.reach_hi, ns[d], g.tshift[d], g.nt[d], t[d]);
       }
     }
-    const int ncopy = nt[0] * nt[1] * nt[2];
-    const int most = __reduce_max_sync(FULL, ncopy);
-    for (int k = 0; k < most; ++k) {
-      const bool act = k < ncopy;
-      const unsigned mask = __ballot_sync(FULL, act);
-      if (!act) continue;
-      const int c2 = k % nt[2], c1 = (k / nt[2]) % nt[1], c0 = k / (nt[2] * nt[1]);
-      const int tile = (int)((int64_t)mock * g.tiles_per_mock +
-                             ((int64_t)t[0][c0] * g.nt[1] + t[1][c1]) * g.nt[2] + t[2][c2]);
-      // one global atomic per distinct tile in the warp (sorted catalogs share tiles)
-      const int first = __ffs(mask) - 1;
-      const bool same = __all_sync(mask, tile == __shfl_sync(mask, tile, first));
-      const unsigned peers = same ? mask : __match_any_sync(mask, tile);
-      const int leader = __ffs(peers) - 1;
-      const unsigned group = __popc(peers);
-      if (!FILL) {
-        if (lane == leader) atomicAdd(counts + tile, group);
-      } else {
-        unsigned base0 = 0;
-        if (lane == leader) base0 = atomicAdd(cursors + tile, group);
-        const unsigned slot = __shfl_sync(peers, base0, leader) + __popc(peers & ((1u << lane) - 1u));
-        bucket[(int64_t)offsets[tile] + slot] = make_float4(u[0], u[1], u[2], wp);
+    const int m0 = __reduce_max_sync(FULL, nt[0]), m1 = __reduce_max_sync(FULL, nt[1]),
+              m2 = __reduce_max_sync(FULL, nt[2]);
+    const int64_t mbase = (int64_t)mock * g.tiles_per_mock;
+    // the copies in (axis 0, 1, 2) order; loop bounds are warp-uniform
+#pragma unroll
+    for (int c0 = 0; c0 < 3; ++c0) {
+      if (c0 >= m0) break;
+#pragma unroll
+      for (int c1 = 0; c1 < 3; ++c1) {
+        if (c1 >= m1) break;
+#pragma unroll
+        for (int c2 = 0; c2 < 3; ++c2) {
+          if (c2 >= m2) break;
+          const bool act = c0 < nt[0] && c1 < nt[1] && c2 < nt[2];
+          int tile = -1;
+          if (act) tile = (int)(mbase + ((int64_t)t[0][c0] * g.nt[1] + t[1][c1]) * g.nt[2] + t[2][c2]);
+          // runs of consecutive lanes with the same tile (catalogs sorted by cell give long
+          // runs) share one global atomic; a run ends at the next leader or inactive lane
+          const int prev = __shfl_up_sync(FULL, tile, 1);
+          const bool lead = act && (lane == 0 || prev != tile);
+          const unsigned leads = __ballot_sync(FULL, lead);
+          const unsigned ends = leads | ~__ballot_sync(FULL, act);
+          const unsigned above = lane == 31 ? 0u : (ends & (0xffffffffu << (lane + 1)));
+          const unsigned runlen = (unsigned)((above ? __ffs(above) - 1 : 32) - lane);
+          if (!FILL) {
+            if (lead) atomicAdd(counts + tile, runlen);
+          } else {
+            unsigned base0 = 0;
+            if (lead) base0 = atomicAdd(cursors + tile, runlen);
+            const unsigned upto = leads & (lane == 31 ? 0xffffffffu : ((2u << lane) - 1u));
+            const int my_lead = upto ? 31 - __clz(upto) : lane;
+            const unsigned base1 = __shfl_sync(FULL, base0, my_lead);
+            if (act)
+              bucket[(int64_t)offsets[tile] + base1 + (unsigned)(lane - my_lead)] =
+                  make_float4(u[0], u[1], u[2], wp);
+          }
+        }
       }
     }
   }
@@ -261,6 +302,38 @@ __device__ __forceinline__ unsigned gcd_u(unsigned a, unsigned b) {
   return a;
 }
 
+// Shared-memory atomics on 32-bit shared-window addresses.
+__device__ __forceinline__ unsigned atom_add_shared(unsigned addr, unsigned v) {
+  unsigned old;
+  asm volatile("atom.shared.add.u32 %0, [%1], %2;" : "=r"(old) : "r"(addr), "r"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ void red_add_shared(unsigned addr, unsigned v) {
+  asm volatile("red.shared.add.u32 [%0], %1;" : : "r"(addr), "r"(v) : "memory");
+}
+
+// bspline() for a compile-time order with both polynomial pieces evaluated and selected
+// (same float32 operations as bspline(), no data-dependent branch).
+template <int ORDER>
+__device__ __forceinline__ float bspline_sel(float s) {
+  if (ORDER == 1) return 1.f;
+  if (ORDER == 2) return __fsub_rn(1.f, s);
+  if (ORDER == 3) {
+    const float inner = __fsub_rn(0.75f, __fmul_rn(s, s));
+    const float t = __fsub_rn(1.5f, s);
+    const float outer = __fmul_rn(0.5f, __fmul_rn(t, t));
+    return s <= 0.5f ? inner : outer;
+  }
+  const float sixth = 0.16666667f;
+  const float s2 = __fmul_rn(s, s);
+  const float s3 = __fmul_rn(s, s2);
+  const float inner = __fmul_rn(sixth, __fadd_rn(__fsub_rn(4.f, __fmul_rn(6.f, s2)), __fmul_rn(3.f, s3)));
+  const float t = __fsub_rn(2.f, s);
+  const float outer = __fmul_rn(sixth, __fmul_rn(t, __fmul_rn(t, t)));
+  return s <= 1.f ? inner : outer;
+}
+
 template <int ORDER, int CFG>
 __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
     PaintGeom g, const float4 *__restrict__ bucket, const int *__restrict__ offsets,
@@ -270,7 +343,7 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
   // Per-cell 64-bit fixed point as two 32-bit words (native shared atomics): the low word's
   // returned old value gives the exact carry into the high word, so the integer sum stays
   // exact and independent of the order of the additions.
-  extern __shared__ unsigned acc32[];  // lo[nshifts][CELLS], hi[nshifts][CELLS]
+  extern __shared__ unsigned acc32[];  // lo[nshifts][CELLS], hi[nshifts][CELLS], scratch[64]
   __shared__ unsigned s_mult;
   const int64_t gtile = blockIdx.x;
   const int mock = (int)(gtile / g.tiles_per_mock);
@@ -298,6 +371,9 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
     const int ns[3] = {g.d.n0, g.d.n1, g.d.n2};
     const int tl[3] = {T0, T1, T2};
     constexpr int OLO = -((ORDER - 1) / 2);
+    // a stencil wraps past the mesh end at most once when every axis has >= ORDER cells
+    const bool one_wrap = g.d.n0 >= ORDER && g.d.n1 >= ORDER && g.d.n2 >= ORDER;
+    const unsigned acc_base = (unsigned)__cvta_generic_to_shared(acc32);
     // permuted visiting order jdx = i * mult mod count (lanes of a warp far apart in the
     // bucket, hence on different cells), advanced incrementally
     unsigned jdx = (unsigned)(((unsigned long long)threadIdx.x * mult) % count);
@@ -307,6 +383,8 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
       jdx += jstep;
       if (jdx >= count) jdx -= count;
       const float uq[3] = {q.x, q.y, q.z};
+      // w 2^fexp is exact, so (w 2^fexp) * ker rounds like the reference's w * ker, scaled
+      const float wq = q.w * fscale;
       for (int s = 0; s < g.nshifts; ++s) {
         float k[3][ORDER];
         int l[3][ORDER];
@@ -317,18 +395,24 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
           const int i0 = (int)fi0;
           // tile-relative cell of the first stencil point; stencil stays within one period
           const int w0 = wrapi(i0 + OLO, ns[d]) - los[d];
+          const int lim = ns[d] - los[d];
 #pragma unroll
           for (int o = 0; o < ORDER; ++o) {
             // (float)(i0 + OLO + o) exactly, without an int -> float conversion
-            k[d][o] = bspline(ORDER, fabsf(__fsub_rn(__fadd_rn(fi0, (float)(OLO + o)), u)));
+            k[d][o] = bspline_sel<ORDER>(fabsf(__fsub_rn(__fadd_rn(fi0, (float)(OLO + o)), u)));
             int loc = w0 + o;
-            while (loc >= ns[d] - los[d]) loc -= ns[d];  // wrapped past the mesh end
+            if (one_wrap) {
+              loc -= loc >= lim ? ns[d] : 0;
+            } else {
+#pragma unroll
+              for (int r = 0; r < ORDER - 1; ++r) loc -= loc >= lim ? ns[d] : 0;  // tiny meshes
+            }
             l[d][o] = (loc >= 0 && loc < tl[d]) ? loc : -1;
           }
         }
-        unsigned *alo = acc32 + s * CELLS;
-        unsigned *ahi = acc32 + (g.nshifts + s) * CELLS;
-        const float wq = q.w;
+        const unsigned dummy = acc_base + 4u * (unsigned)(2 * g.nshifts * CELLS + (threadIdx.x & 31));
+        const unsigned lo_base = acc_base + 4u * (unsigned)(s * CELLS);
+        const unsigned hi_base = acc_base + 4u * (unsigned)((g.nshifts + s) * CELLS);
 #pragma unroll
         for (int a = 0; a < ORDER; ++a) {
 #pragma unroll
@@ -338,14 +422,15 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
             const int rowoff = (l[0][a] * T1 + l[1][b]) * T2;
 #pragma unroll
             for (int c = 0; c < ORDER; ++c) {
-              if (vab && l[2][c] >= 0) {
-                const float v = __fmul_rn(wq, __fmul_rn(kab, k[2][c]));  // weights * ker
-                const long long fx = __float2ll_rn(v * fscale);
-                const unsigned lo = (unsigned)fx;
-                const int cell = rowoff + l[2][c];
-                const unsigned old = atomicAdd(alo + cell, lo);
-                atomicAdd(ahi + cell, (unsigned)((int)(fx >> 32) + (old + lo < old ? 1 : 0)));
-              }
+              const bool valid = vab && l[2][c] >= 0;
+              const float v = __fmul_rn(wq, __fmul_rn(kab, k[2][c]));  // (w * ker) 2^fexp
+              const long long fx = __float2ll_rn(v);
+              const unsigned lo = (unsigned)fx;
+              // invalid cells go to this lane's scratch words (never read): no branch, and
+              // the scratch words of a warp sit in distinct banks
+              const unsigned off = 4u * (unsigned)(rowoff + l[2][c]);
+              const unsigned old = atom_add_shared(valid ? lo_base + off : dummy, lo);
+              red_add_shared(valid ? hi_base + off : dummy + 128u, (unsigned)((int)(fx >> 32) + (old + lo < old ? 1 : 0)));
             }
           }
         }
@@ -488,7 +573,12 @@ static bool fill_geom(const int32_t meshsize[3], const float boxsize[3], const f
   g->reach_hi = hi + (order & 1 ? 1 : 0) + (shifted ? 1 : 0);
   int threads;
   tile_dims(config, g->tile, &threads);
-  for (int d = 0; d < 3; ++d) g->nt[d] = (meshsize[d] + g->tile[d] - 1) / g->tile[d];
+  for (int d = 0; d < 3; ++d) {
+    g->nt[d] = (meshsize[d] + g->tile[d] - 1) / g->tile[d];
+    g->tshift[d] = 0;
+    while ((1 << g->tshift[d]) < g->tile[d]) ++g->tshift[d];
+    if ((1 << g->tshift[d]) != g->tile[d]) return false;
+  }
   g->tiles_per_mock = (int64_t)g->nt[0] * g->nt[1] * g->nt[2];
   g->nmocks = nmocks;
   g->offsets = nullptr;
@@ -572,7 +662,8 @@ static pk_status paint_run(cudaStream_t s, const float *positions, const float *
   }
   int tdims[3], tthreads;
   tile_dims(config, tdims, &tthreads);
-  const size_t smem = (size_t)g.nshifts * tdims[0] * tdims[1] * tdims[2] * 2 * sizeof(unsigned);
+  // accumulators (lo, hi words per shift and cell) + 64 scratch words for masked-off lanes
+  const size_t smem = ((size_t)g.nshifts * tdims[0] * tdims[1] * tdims[2] * 2 + 64) * sizeof(unsigned);
   switch (config * 8 + g.order) {
 #define PK_PAINT_CASE(C, O)                                                                    \
   case C * 8 + O:                                                                              \
