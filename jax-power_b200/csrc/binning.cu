@@ -581,7 +581,9 @@ struct GlobalSmem {
   float *kz2;
 };
 
-template <int NV, bool CROSS>
+// EVEN: every multipole even with ell <= 4 (L_ell a polynomial of degree <= 2 in mu^2, no
+// odd parts), the usual (0, 2, 4) case; otherwise the general form (degree 4, odd ell).
+template <int NV, bool CROSS, bool EVEN>
 __global__ void __launch_bounds__(BIN_THREADS) bin_global_kernel(
     BinGeom g, const float2 *__restrict__ d1, const float2 *__restrict__ d2, float lx, float ly,
     float lz, LegendreCoefs lc, int zero_l0, const float *__restrict__ edges, int nwarps_hist,
@@ -685,22 +687,32 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_global_kernel(
         }
         const float w = jaxw ? (z > 0 ? 2.f : 1.f) : ((z == 0 || z == zself) ? 1.f : 2.f);
         const float num = kl + kz * lz;
-        const float rk2 = k2 > 0.f ? __frcp_rn(k2) : 0.f;
+        const float rk2 = k2 > 0.f ? __fdividef(1.f, k2) : 0.f;  // mu^2 enters L_ell only
         const float mu2 = num * num * rk2;
-        const float mu = lc.any_odd ? num * sqrtf(rk2) : 0.f;
         const bool zero = (row == 0 && z == 0);  // remove_zero for ell > 0
-        const float rw = re * w, iw = im * w;
+        const float rw = re * w;
+        if (EVEN) {
 #pragma unroll
-        for (int l = 0; l < NV; ++l) {
-          float L = lc.c[l][4];
-          L = L * mu2 + lc.c[l][3];
-          L = L * mu2 + lc.c[l][2];
-          L = L * mu2 + lc.c[l][1];
-          L = L * mu2 + lc.c[l][0];
-          if (lc.odd[l]) L *= mu;
-          const float part = lc.odd[l] ? iw : rw;
-          const bool drop = zero && !(zero_l0 & (1 << l));
-          acc[l] += drop ? 0.f : part * L;
+          for (int l = 0; l < NV; ++l) {
+            const float L = __fmaf_rn(__fmaf_rn(lc.c[l][2], mu2, lc.c[l][1]), mu2, lc.c[l][0]);
+            const bool drop = zero && !(zero_l0 & (1 << l));
+            acc[l] += drop ? 0.f : rw * L;
+          }
+        } else {
+          const float mu = lc.any_odd ? num * sqrtf(rk2) : 0.f;
+          const float iw = im * w;
+#pragma unroll
+          for (int l = 0; l < NV; ++l) {
+            float L = lc.c[l][4];
+            L = L * mu2 + lc.c[l][3];
+            L = L * mu2 + lc.c[l][2];
+            L = L * mu2 + lc.c[l][1];
+            L = L * mu2 + lc.c[l][0];
+            if (lc.odd[l]) L *= mu;
+            const float part = lc.odd[l] ? iw : rw;
+            const bool drop = zero && !(zero_l0 & (1 << l));
+            acc[l] += drop ? 0.f : part * L;
+          }
         }
       }
     }
@@ -764,7 +776,7 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_global_kernel(
   }
 }
 
-template <int NV, bool CROSS>
+template <int NV, bool CROSS, bool EVEN>
 static pk_status launch_global(cudaStream_t st, const BinGeom &g, const float2 *d1,
                                const float2 *d2, const float los[3], const LegendreCoefs &lc,
                                int zero_l0, const float *edges, double *out, void *workspace,
@@ -776,9 +788,9 @@ static pk_status launch_global(cudaStream_t st, const BinGeom &g, const float2 *
              "binning workspace too small: need %zu bytes, got %zu", L.partial_bytes * nbatch,
              workspace_bytes);
   double *partials = static_cast<double *>(workspace);
-  PK_CUDA(cudaFuncSetAttribute(bin_global_kernel<NV, CROSS>,
+  PK_CUDA(cudaFuncSetAttribute(bin_global_kernel<NV, CROSS, EVEN>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
-  bin_global_kernel<NV, CROSS><<<dim3(L.blocks, nbatch), L.nwarps * 32, L.smem, st>>>(
+  bin_global_kernel<NV, CROSS, EVEN><<<dim3(L.blocks, nbatch), L.nwarps * 32, L.smem, st>>>(
       g, d1, d2, los[0], los[1], los[2], lc, zero_l0, edges, L.nwarps, L.tab, partials);
   PK_LAUNCH_CHECK();
   const int hist_len = (g.nedges - 1) * NV;
@@ -918,23 +930,31 @@ extern "C" pk_status pk_bin_global_batch(void *stream, const void *delta1, const
     PK_REQUIRE(ells[l] >= 0 && ells[l] <= 8, PK_ERR_INVALID, "ell must be in 0..8");
   LegendreCoefs lc;
   lc.any_odd = 0;
-  int zero_l0 = 0;
+  int zero_l0 = 0, max_ell = 0;
   for (int l = 0; l < MAX_ELLS; ++l) {
     const int ell = l < nells ? ells[l] : 0;
     legendre_coefs(ell, lc.c[l], &lc.odd[l]);
     lc.any_odd |= (l < nells) && lc.odd[l];
     if (l < nells && ell == 0) zero_l0 |= 1 << l;  // ell = 0 keeps the k = 0 mode
+    if (l < nells && ell > max_ell) max_ell = ell;
   }
+  const bool even = !lc.any_odd && max_ell <= 4;
   cudaStream_t cs = (cudaStream_t)stream;
   const float2 *a = (const float2 *)delta1, *b = (const float2 *)delta2;
-  switch (nells * 2 + (b ? 1 : 0)) {
+  switch (nells * 4 + (b ? 2 : 0) + (even ? 1 : 0)) {
 #define PK_GL_CASE(N)                                                                           \
-  case 2 * N:                                                                                   \
-    return launch_global<N, false>(cs, g, a, b, los, lc, zero_l0, d_edges, d_out, workspace,    \
-                                   workspace_bytes, nbatch);                                            \
-  case 2 * N + 1:                                                                               \
-    return launch_global<N, true>(cs, g, a, b, los, lc, zero_l0, d_edges, d_out, workspace,     \
-                                  workspace_bytes, nbatch);
+  case 4 * N:                                                                                   \
+    return launch_global<N, false, false>(cs, g, a, b, los, lc, zero_l0, d_edges, d_out,        \
+                                          workspace, workspace_bytes, nbatch);                  \
+  case 4 * N + 1:                                                                               \
+    return launch_global<N, false, true>(cs, g, a, b, los, lc, zero_l0, d_edges, d_out,         \
+                                         workspace, workspace_bytes, nbatch);                   \
+  case 4 * N + 2:                                                                               \
+    return launch_global<N, true, false>(cs, g, a, b, los, lc, zero_l0, d_edges, d_out,         \
+                                         workspace, workspace_bytes, nbatch);                   \
+  case 4 * N + 3:                                                                               \
+    return launch_global<N, true, true>(cs, g, a, b, los, lc, zero_l0, d_edges, d_out,          \
+                                        workspace, workspace_bytes, nbatch);
     PK_GL_CASE(1) PK_GL_CASE(2) PK_GL_CASE(3) PK_GL_CASE(4) PK_GL_CASE(5) PK_GL_CASE(6)
     PK_GL_CASE(7) PK_GL_CASE(8) PK_GL_CASE(9)
 #undef PK_GL_CASE
