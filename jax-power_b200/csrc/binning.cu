@@ -264,11 +264,11 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_rows_kernel(BinGeom g, Op op,
   const float inv_step = g.step > 0.f ? 1.f / g.step : 0.f;
   const int R = (g.d.nz + 31) / 32;
   const int z0 = lane * R, z1 = min(g.d.nz, z0 + R);
-  const int64_t nrows = (int64_t)g.d.n0 * g.d.n1;
   constexpr int NONE = 0x7fffffff;
-  for (int64_t row = (int64_t)blockIdx.x * nwarps + warp; row < nrows;
-       row += (int64_t)gridDim.x * nwarps) {
-    const int i = (int)(row / g.d.n1), j = (int)(row % g.d.n1);
+  for (RowWalker rw((int64_t)blockIdx.x * nwarps + warp, (int64_t)gridDim.x * nwarps, g.d.n1); rw.i < g.d.n0;
+       rw.next()) {
+    const int i = rw.i, j = rw.j;
+    const int64_t row = (int64_t)i * g.d.n1 + j;
     const float kx = kcoord(i, g.d.n0, g.kfun[0], false);
     const float ky = kcoord(j, g.d.n1, g.kfun[1], false);
     const float kxy = __fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky));  // (0 + kx^2) + ky^2
@@ -385,10 +385,10 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_chunks_kernel(BinGeom g, Op o
   double *my = s.hist + (size_t)warp * hist_len;
   const float e0 = edges[0];
   const float inv_step = g.step > 0.f ? 1.f / g.step : 0.f;
-  const int64_t nrows = (int64_t)g.d.n0 * g.d.n1;
-  for (int64_t row = (int64_t)blockIdx.x * nwarps + warp; row < nrows;
-       row += (int64_t)gridDim.x * nwarps) {
-    const int i = (int)(row / g.d.n1), j = (int)(row % g.d.n1);
+  for (RowWalker rw((int64_t)blockIdx.x * nwarps + warp, (int64_t)gridDim.x * nwarps, g.d.n1); rw.i < g.d.n0;
+       rw.next()) {
+    const int i = rw.i, j = rw.j;
+    const int64_t row = (int64_t)i * g.d.n1 + j;
     const float kx = kcoord(i, g.d.n0, g.kfun[0], false);
     const float ky = kcoord(j, g.d.n1, g.kfun[1], false);
     const float kxy = __fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky));
@@ -612,7 +612,6 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_global_kernel(
   const float inv_step = g.step > 0.f ? 1.f / g.step : 0.f;
   const int R = (g.d.nz + 31) / 32;
   const int z0 = lane * R, z1 = min(g.d.nz, z0 + R);
-  const int64_t nrows = (int64_t)g.d.n0 * g.d.n1;
   const bool jaxw = g.backend == PK_BACKEND_JAX;
   // batch of meshes along y: mesh blockIdx.y, its own partial rows
   d1 += (int64_t)blockIdx.y * g.d.ncomplex();
@@ -620,9 +619,10 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_global_kernel(
   partials += (size_t)blockIdx.y * gridDim.x * hist_len;
   const int zself = (g.d.n2 % 2) == 0 ? g.d.nz - 1 : -1;  // self-conjugate last plane
   constexpr int NONE = 0x7fffffff;
-  for (int64_t row = (int64_t)blockIdx.x * nwarps + warp; row < nrows;
-       row += (int64_t)gridDim.x * nwarps) {
-    const int i = (int)(row / g.d.n1), j = (int)(row % g.d.n1);
+  for (RowWalker rw((int64_t)blockIdx.x * nwarps + warp, (int64_t)gridDim.x * nwarps, g.d.n1); rw.i < g.d.n0;
+       rw.next()) {
+    const int i = rw.i, j = rw.j;
+    const int64_t row = (int64_t)i * g.d.n1 + j;
     const float kx = kcoord(i, g.d.n0, g.kfun[0], false);
     const float ky = kcoord(j, g.d.n1, g.kfun[1], false);
     const float kxy = __fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky));
@@ -1131,11 +1131,10 @@ __global__ void global_adjoint_kernel(AdjGeom a, const float *__restrict__ thr,
   const BinGeom &g = a.g;
   const int64_t total = g.d.ncomplex();
   const bool even = (g.d.n2 % 2) == 0;
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int z = (int)(idx % g.d.nz);
-    const int64_t r = idx / g.d.nz;
-    const int j = (int)(r % g.d.n1), i = (int)(r / g.d.n1);
+  const int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  IndexWalker3 w(start, stride, g.d.n1, g.d.nz);
+  for (int64_t idx = start; idx < total; idx += stride, w.next()) {
+    const int i = w.i, j = w.j, z = w.k;
     float2 v = global_adj_mode(a, thr, coef, delta, i, j, z);
     if (a.for_c2r) {
       if (z == 0 || (even && z == g.d.nz - 1)) {
@@ -1207,11 +1206,10 @@ __global__ void firstpoint_adjoint_kernel(AdjGeom a, FPAdj t, const float *__res
   const int64_t total = g.d.ncomplex();
   const bool even = (g.d.n2 % 2) == 0;
   float2 gf[MAX_FP_TERMS], gfm[MAX_FP_TERMS];
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int z = (int)(idx % g.d.nz);
-    const int64_t r = idx / g.d.nz;
-    const int j = (int)(r % g.d.n1), i = (int)(r / g.d.n1);
+  const int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  IndexWalker3 w(start, stride, g.d.n1, g.d.nz);
+  for (int64_t idx = start; idx < total; idx += stride, w.next()) {
+    const int i = w.i, j = w.j, z = w.k;
     float2 ga0;
     fp_adj_mode(a, t, thr, coef, a0, f, i, j, z, &ga0, gf);
     const bool plane = z == 0 || (even && z == g.d.nz - 1);

@@ -100,4 +100,54 @@ struct Complex {
   float re, im;
 };
 
+// Row-major (i, j) rows of an n0 x n1 grid visited from `start` with a fixed `stride`,
+// advanced without a division per step (one 64-bit division at construction).
+struct RowWalker {
+  int i, j, si, sj, n1;
+  __device__ __forceinline__ RowWalker(int64_t start, int64_t stride, int n1_) : n1(n1_) {
+    i = (int)(start / n1_);
+    j = (int)(start % n1_);
+    si = (int)(stride / n1_);
+    sj = (int)(stride % n1_);
+  }
+  __device__ __forceinline__ void next() {
+    j += sj;
+    i += si;
+    if (j >= n1) {
+      j -= n1;
+      ++i;
+    }
+  }
+};
+
+// (i, j, k) of a row-major n0 x n1 x n2 grid visited from `start` with a fixed `stride`
+// (grid-stride loops), advanced with carries instead of a division per element.
+struct IndexWalker3 {
+  int i, j, k, si, sj, sk, n1, n2;
+  __device__ __forceinline__ IndexWalker3(int64_t start, int64_t stride, int n1_, int n2_)
+      : n1(n1_), n2(n2_) {
+    k = (int)(start % n2_);
+    const int64_t r = start / n2_;
+    j = (int)(r % n1_);
+    i = (int)(r / n1_);
+    sk = (int)(stride % n2_);
+    const int64_t sr = stride / n2_;
+    sj = (int)(sr % n1_);
+    si = (int)(sr / n1_);
+  }
+  __device__ __forceinline__ void next() {
+    k += sk;
+    j += sj;
+    i += si;
+    if (k >= n2) {
+      k -= n2;
+      ++j;
+    }
+    if (j >= n1) {
+      j -= n1;
+      ++i;
+    }
+  }
+};
+
 }  // namespace pk

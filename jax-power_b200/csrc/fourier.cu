@@ -162,11 +162,11 @@ __global__ void __launch_bounds__(IL_THREADS) interlace_kernel(FourierParams p,
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nwarps = blockDim.x >> 5;
-  const int64_t nrows = (int64_t)d.n0 * d.n1;
   const bool even = (d.n2 % 2) == 0;
-  for (int64_t row = (int64_t)blockIdx.x * nwarps + warp; row < nrows;
-       row += (int64_t)gridDim.x * nwarps) {
-    const int i = (int)(row / d.n1), j = (int)(row % d.n1);
+  for (RowWalker rw((int64_t)blockIdx.x * nwarps + warp, (int64_t)gridDim.x * nwarps, d.n1); rw.i < d.n0;
+       rw.next()) {
+    const int i = rw.i, j = rw.j;
+    const int64_t row = (int64_t)i * d.n1 + j;
     RowFactor<NS> rf, rm;
     row_factor<NS, FULL>(p, i, j, rf);
     const bool planes = p.for_c2r != 0;
@@ -213,12 +213,10 @@ __global__ void ylm_premultiply_kernel(Dims d, float c0, float c1, float c2, flo
                                        float o2, YlmTerms terms, const float *__restrict__ rho,
                                        float *__restrict__ out) {
   const int64_t total = d.nreal();
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int k = (int)(idx % d.n2);
-    const int64_t r = idx / d.n2;
-    const int j = (int)(r % d.n1);
-    const int i = (int)(r / d.n1);
+  const int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  IndexWalker3 w(start, stride, d.n1, d.n2);
+  for (int64_t idx = start; idx < total; idx += stride, w.next()) {
+    const int i = w.i, j = w.j, k = w.k;
     // rcoords: arange(n) * cellsize + (boxcenter - boxsize / 2)
     const float x = __fadd_rn(__fmul_rn((float)i, c0), o0);
     const float y = __fadd_rn(__fmul_rn((float)j, c1), o1);
@@ -422,11 +420,10 @@ __global__ void __launch_bounds__(IL_THREADS) interlace_adjoint_kernel(
   const int64_t total = d.ncomplex();
   const bool even = (d.n2 % 2) == 0;
   const float inv_n = 1.f / (float)d.nreal();
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int z = (int)(idx % d.nz);
-    const int64_t r = idx / d.nz;
-    const int j = (int)(r % d.n1), i = (int)(r / d.n1);
+  const int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  IndexWalker3 w(start, stride, d.n1, d.nz);
+  for (int64_t idx = start; idx < total; idx += stride, w.next()) {
+    const int i = w.i, j = w.j, z = w.k;
     const bool plane = z == 0 || (even && z == d.nz - 1);
     const int im = (d.n0 - i) % d.n0, jm = (d.n1 - j) % d.n1;
     for (int s = 0; s < p.nshifts; ++s) {
@@ -457,11 +454,10 @@ __global__ void ylm_accumulate_kernel(Dims d, float c0, float c1, float c2, floa
                                       float o2, YlmTerms terms, const float *__restrict__ r,
                                       float *__restrict__ rho_bar) {
   const int64_t total = d.nreal();
-  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (int64_t)gridDim.x * blockDim.x) {
-    const int k = (int)(idx % d.n2);
-    const int64_t rr = idx / d.n2;
-    const int j = (int)(rr % d.n1), i = (int)(rr / d.n1);
+  const int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  IndexWalker3 w(start, stride, d.n1, d.n2);
+  for (int64_t idx = start; idx < total; idx += stride, w.next()) {
+    const int i = w.i, j = w.j, k = w.k;
     const float x = __fadd_rn(__fmul_rn((float)i, c0), o0);
     const float y = __fadd_rn(__fmul_rn((float)j, c1), o1);
     const float z = __fadd_rn(__fmul_rn((float)k, c2), o2);
