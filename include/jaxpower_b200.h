@@ -173,6 +173,20 @@ pk_status pk_bin_global(void *stream, const void *delta1, const void *delta2,
                         int nells, const int32_t *ells, double *d_out, void *workspace,
                         size_t workspace_bytes);
 
+/* pk_bin_global_batch of the meshes that pk_interlace_compensate(_batch) would form
+ * (for_c2r = 0, scale 1), without storing them: each mode is combined on the fly from
+ * the nshifts interlaced, uncompensated R2C meshes (shifted: nbatch x nshifts Hermitian
+ * meshes, mesh s of batch b at shifted + (b * nshifts + s) * N_c) with compensation
+ * order comp_order, then binned.  Same outputs and workspace as pk_bin_global_batch.
+ * Takes up to 3 even multipoles (ell <= 4) and up to 4 shifts (PK_ERR_RANGE otherwise).
+ * No reference counterpart: the reference stores the combined mesh (mesh.py:2737-2752)
+ * and then bins it (mesh2.py:346-374). */
+pk_status pk_bin_global_interlaced(void *stream, const void *shifted, int nbatch, int nshifts,
+                                   int comp_order, const int32_t meshsize[3], const float kfun[3],
+                                   const float los[3], const float *d_edges, int nedges, float step,
+                                   int backend, int nells, const int32_t *ells, double *d_out,
+                                   void *workspace, size_t workspace_bytes);
+
 /* No counterpart in the reference.  pk_bin_global without a workspace argument, for
  * callers that cannot allocate device memory when they call (a host callback, or a
  * foreign runtime that owns the allocator): its scratch is a fixed 16 MiB static device

@@ -18,6 +18,7 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "fourier_common.cuh"
 #include "ylm_table.cuh"
 
 namespace pk {
@@ -583,11 +584,17 @@ struct GlobalSmem {
 
 // EVEN: every multipole even with ell <= 4 (L_ell a polynomial of degree <= 2 in mu^2, no
 // odd parts), the usual (0, 2, 4) case; otherwise the general form (degree 4, odd ell).
-template <int NV, bool CROSS, bool EVEN>
-__global__ void __launch_bounds__(BIN_THREADS) bin_global_kernel(
+// NS > 0: the mesh is not stored; each mode is formed on the fly from NS interlaced,
+// uncompensated meshes at d1 (mesh s at d1 + s N_c), exactly as pk_interlace_compensate
+// forms it (fp: its parameters; FULL: 'jaxdecomp' semantics), which saves writing and
+// reading back the combined mesh (that form gets a larger register budget: 2 CTAs per SM
+// instead of 4).
+template <int NV, bool CROSS, bool EVEN, int NS = 0, bool FULL = false>
+__global__ void __launch_bounds__(BIN_THREADS, NS > 0 ? 2 : 4) bin_global_kernel(
     BinGeom g, const float2 *__restrict__ d1, const float2 *__restrict__ d2, float lx, float ly,
     float lz, LegendreCoefs lc, int zero_l0, const float *__restrict__ edges, int nwarps_hist,
-    int tab, double *__restrict__ partials) {
+    int tab, double *__restrict__ partials, FourierParams fp) {
+  constexpr int NSR = NS > 0 ? NS : 1;
   const int nbins = g.nedges - 1;
   const int hist_len = nbins * NV;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -598,6 +605,11 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_global_kernel(
   s.thr = s.hist + (((size_t)nwarps_hist * hist_len + 3) & ~(size_t)3);
   s.kz = s.thr + ((g.nedges + 3) & ~3);
   s.kz2 = s.kz + ((g.d.nz + 3) & ~3);
+  ZTable zt;
+  if (NS > 0) {
+    zt = ztable_at(s.kz2 + ((g.d.nz + 3) & ~3), fp, FULL);
+    fill_ztable<FULL>(fp, zt);
+  }
   for (int q = threadIdx.x; q < nwarps_hist * hist_len; q += blockDim.x) s.hist[q] = 0.f;
   for (int q = threadIdx.x; q < g.nedges; q += blockDim.x) s.thr[q] = sqrt_threshold(edges[q]);
   if (tab)
@@ -614,7 +626,7 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_global_kernel(
   const int z0 = lane * R, z1 = min(g.d.nz, z0 + R);
   const bool jaxw = g.backend == PK_BACKEND_JAX;
   // batch of meshes along y: mesh blockIdx.y, its own partial rows
-  d1 += (int64_t)blockIdx.y * g.d.ncomplex();
+  d1 += (int64_t)blockIdx.y * (NS > 0 ? NS : 1) * g.d.ncomplex();
   if (CROSS) d2 += (int64_t)blockIdx.y * g.d.ncomplex();
   partials += (size_t)blockIdx.y * gridDim.x * hist_len;
   const int zself = (g.d.n2 % 2) == 0 ? g.d.nz - 1 : -1;  // self-conjugate last plane
@@ -627,6 +639,8 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_global_kernel(
     const float ky = kcoord(j, g.d.n1, g.kfun[1], false);
     const float kxy = __fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky));
     const float kl = kx * lx + ky * ly;
+    RowFactor<NSR> rf;
+    if (NS > 0) row_factor<NSR, FULL>(fp, i, j, rf);
     int cur = -1, lead = NONE, trail = NONE, nseg = 0;
     float acc[NV], facc[NV];
 #pragma unroll
@@ -634,13 +648,16 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_global_kernel(
     const float2 *p1 = d1 + row * g.d.nz;
     const float2 *p2 = CROSS ? d2 + row * g.d.nz : nullptr;
     // the run's values are loaded RB at a time before use: many loads in flight per lane
-    constexpr int RB = CROSS ? 4 : 8;
+    constexpr int RB = (CROSS || NS > 1) ? 4 : 8;
     for (int zb = z0; zb < z1; zb += RB) {
       float2 va[RB], vb[CROSS ? RB : 1];
 #pragma unroll
       for (int t = 0; t < RB; ++t) {
         const int z = zb + t;
-        va[t] = z < z1 ? p1[z] : make_float2(0.f, 0.f);
+        if (NS > 0)
+          va[t] = z < z1 ? combine_mode<NSR, FULL>(fp, rf, zt, d1, row * g.d.nz + z, z) : make_float2(0.f, 0.f);
+        else
+          va[t] = z < z1 ? p1[z] : make_float2(0.f, 0.f);
         if (CROSS) vb[t] = z < z1 ? p2[z] : make_float2(0.f, 0.f);
       }
 #pragma unroll
@@ -776,22 +793,32 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_global_kernel(
   }
 }
 
-template <int NV, bool CROSS, bool EVEN>
+template <int NV, bool CROSS, bool EVEN, int NS = 0, bool FULL = false>
 static pk_status launch_global(cudaStream_t st, const BinGeom &g, const float2 *d1,
                                const float2 *d2, const float los[3], const LegendreCoefs &lc,
                                int zero_l0, const float *edges, double *out, void *workspace,
-                               size_t workspace_bytes, int nbatch) {
+                               size_t workspace_bytes, int nbatch,
+                               const FourierParams *fp = nullptr) {
   BinLaunch L;
   PK_REQUIRE(plan_bins(g.d, g.nedges, NV, &L, sizeof(float)), PK_ERR_RANGE,
              "too many bins x values (%d x %d) for the shared-memory histograms", g.nedges - 1, NV);
+  FourierParams fpv{};
+  if (NS > 0) {
+    fpv = *fp;
+    // the kz tables (binning and interlacing) always live in shared memory on this path
+    if (!L.tab) L.smem += 2 * (size_t)((g.d.nz + 3) & ~3) * sizeof(float);
+    L.tab = 1;
+    L.smem += ztable_bytes(g.d, NS, FULL);
+    PK_REQUIRE(L.smem <= 227 * 1024, PK_ERR_RANGE, "mesh too large along the last axis for the fused pass");
+  }
   PK_REQUIRE(workspace && workspace_bytes >= L.partial_bytes * nbatch, PK_ERR_WORKSPACE,
              "binning workspace too small: need %zu bytes, got %zu", L.partial_bytes * nbatch,
              workspace_bytes);
   double *partials = static_cast<double *>(workspace);
-  PK_CUDA(cudaFuncSetAttribute(bin_global_kernel<NV, CROSS, EVEN>,
+  PK_CUDA(cudaFuncSetAttribute(bin_global_kernel<NV, CROSS, EVEN, NS, FULL>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
-  bin_global_kernel<NV, CROSS, EVEN><<<dim3(L.blocks, nbatch), L.nwarps * 32, L.smem, st>>>(
-      g, d1, d2, los[0], los[1], los[2], lc, zero_l0, edges, L.nwarps, L.tab, partials);
+  bin_global_kernel<NV, CROSS, EVEN, NS, FULL><<<dim3(L.blocks, nbatch), L.nwarps * 32, L.smem, st>>>(
+      g, d1, d2, los[0], los[1], los[2], lc, zero_l0, edges, L.nwarps, L.tab, partials, fpv);
   PK_LAUNCH_CHECK();
   const int hist_len = (g.nedges - 1) * NV;
   launch_finalize(st, partials, L.blocks, hist_len, NV, g.nedges - 1, 0, out, nullptr, nbatch);
@@ -960,6 +987,54 @@ extern "C" pk_status pk_bin_global_batch(void *stream, const void *delta1, const
 #undef PK_GL_CASE
   }
   set_error("unsupported number of multipoles %d", nells);
+  return PK_ERR_INVALID;
+}
+
+extern "C" pk_status pk_bin_global_interlaced(void *stream, const void *shifted, int nbatch, int nshifts,
+                                              int comp_order, const int32_t meshsize[3], const float kfun[3],
+                                              const float los[3], const float *d_edges, int nedges, float step,
+                                              int backend, int nells, const int32_t *ells, double *d_out,
+                                              void *workspace, size_t workspace_bytes) {
+  PK_REQUIRE(nbatch >= 1 && nbatch <= 65535, PK_ERR_INVALID, "nbatch must be in 1..65535");
+  BinGeom g;
+  pk_status st = make_geom(meshsize, kfun, nedges, step, backend, &g);
+  if (st) return st;
+  PK_REQUIRE(shifted && d_edges && d_out && los && ells, PK_ERR_INVALID, "null pointer");
+  PK_REQUIRE(nells >= 1 && nells <= MAX_ELLS, PK_ERR_INVALID, "nells must be in 1..%d", MAX_ELLS);
+  FourierParams fp;
+  PK_REQUIRE(make_fourier_params(meshsize, nshifts, comp_order, backend, 0, 1.f, &fp), PK_ERR_INVALID,
+             "invalid meshsize / nshifts (1..8) / comp_order (0..4)");
+  LegendreCoefs lc;
+  lc.any_odd = 0;
+  int zero_l0 = 0, max_ell = 0;
+  for (int l = 0; l < MAX_ELLS; ++l) {
+    const int ell = l < nells ? ells[l] : 0;
+    PK_REQUIRE(l >= nells || (ell >= 0 && ell <= 8), PK_ERR_INVALID, "ell must be in 0..8");
+    legendre_coefs(ell, lc.c[l], &lc.odd[l]);
+    lc.any_odd |= (l < nells) && lc.odd[l];
+    if (l < nells && ell == 0) zero_l0 |= 1 << l;  // ell = 0 keeps the k = 0 mode
+    if (l < nells && ell > max_ell) max_ell = ell;
+  }
+  PK_REQUIRE(!lc.any_odd && max_ell <= 4 && nells <= 3 && nshifts <= 4, PK_ERR_RANGE,
+             "the fused pass takes up to 3 even multipoles (ell <= 4) and up to 4 shifts; "
+             "combine with pk_interlace_compensate and bin with pk_bin_global instead");
+  cudaStream_t cs = (cudaStream_t)stream;
+  const float2 *a = (const float2 *)shifted;
+  const bool full = backend == PK_BACKEND_JAXDECOMP;
+  switch ((nells * 8 + nshifts) * 2 + (full ? 1 : 0)) {
+#define PK_GI_CASE(N, S)                                                                          \
+  case (N * 8 + S) * 2:                                                                           \
+    return launch_global<N, false, true, S, false>(cs, g, a, nullptr, los, lc, zero_l0, d_edges,  \
+                                                   d_out, workspace, workspace_bytes, nbatch, &fp); \
+  case (N * 8 + S) * 2 + 1:                                                                       \
+    return launch_global<N, false, true, S, true>(cs, g, a, nullptr, los, lc, zero_l0, d_edges,   \
+                                                  d_out, workspace, workspace_bytes, nbatch, &fp);
+#define PK_GI_N(N) PK_GI_CASE(N, 1) PK_GI_CASE(N, 2) PK_GI_CASE(N, 3) PK_GI_CASE(N, 4)
+    PK_GI_N(1) PK_GI_N(2) PK_GI_N(3)
+#undef PK_GI_N
+#undef PK_GI_CASE
+  }
+  set_error("unsupported fused binning configuration");
   return PK_ERR_INVALID;
 }
 

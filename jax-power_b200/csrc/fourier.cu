@@ -4,6 +4,7 @@
 #include <math.h>
 
 #include "common.cuh"
+#include "fourier_common.cuh"
 #include "ylm_table.cuh"
 
 struct pk_fft_plan_s {
@@ -15,124 +16,7 @@ struct pk_fft_plan_s {
 
 namespace pk {
 
-struct FourierParams {
-  Dims d;
-  float cspacing[3];  // float32(2 pi / N_d): circular spacing (mesh.py:1627-1629)
-  int nshifts;
-  float shifts[8];
-  float interlacing;
-  int comp_order;
-  int backend;
-  int for_c2r;
-  float scale;
-};
-
-// jnp.sinc(k / 2pi) with the reference's float32 operations (resamplers.py:21).
-__device__ __forceinline__ float sinc_of(float kc) {
-  const float x = __fdiv_rn(kc, 6.2831855f);  // float32(2 pi)
-  if (x == 0.f) return 1.f;
-  const float px = __fmul_rn(3.1415927f, x);
-  return __fdiv_rn(sinf(px), px);
-}
-
-// (window)^(-order): lax.integer_pow by binary exponentiation, then the reciprocal.
-__device__ __forceinline__ float inverse_power(float ker, int order) {
-  int y = order;
-  float acc = 1.f, x = ker;
-  bool first = true;
-  while (y > 0) {
-    if (y & 1) {
-      acc = first ? x : __fmul_rn(acc, x);
-      first = false;
-    }
-    y >>= 1;
-    if (y > 0) x = __fmul_rn(x, x);
-  }
-  return __fdiv_rn(1.f, acc);
-}
-
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-
-__device__ __forceinline__ float2 expi(float t) {
-  float sn, cs;
-  sincosf(t, &sn, &cs);
-  return make_float2(cs, sn);
-}
-
 constexpr int IL_THREADS = 256;
-constexpr int IL_MAX_SHIFTS = 8;
-
-// Per-CTA table along kz (shared memory): for each shift s, e^{i s kz(z)} and, for the
-// 'jaxdecomp' semantics, e^{-i s kz(-z)} on the full grid; plus sinc(kz / 2pi).
-struct ZTable {
-  float2 *ph;    // [nshifts][nz]
-  float2 *phm;   // [nshifts][nz] (jaxdecomp)
-  float *sinc;   // [nz]
-};
-
-// Row factors: prod over x, y of the phase (divided by I) and of the sinc window.
-template <int NS>
-struct RowFactor {
-  float2 ph[NS];
-  float2 phm[NS];
-  float sinc;
-};
-
-template <int NS, bool FULL>
-__device__ __forceinline__ void row_factor(const FourierParams &p, int i, int j, RowFactor<NS> &r) {
-  const Dims &d = p.d;
-  constexpr bool full = FULL;
-  const float k0 = ccoord(i, d.n0, p.cspacing[0], false);
-  const float k1 = ccoord(j, d.n1, p.cspacing[1], false);
-  const float kxy = k0 + k1;
-  const int i2 = (d.n0 - i) % d.n0, j2 = (d.n1 - j) % d.n1;
-  const float kxym = ccoord(i2, d.n0, p.cspacing[0], false) + ccoord(j2, d.n1, p.cspacing[1], false);
-  const float inv = 1.f / p.interlacing;
-#pragma unroll
-  for (int s = 0; s < NS; ++s) {
-    const float2 e = expi(p.shifts[s] * kxy);
-    r.ph[s] = make_float2(e.x * inv, e.y * inv);
-    if (full) {
-      const float2 m = expi(-p.shifts[s] * kxym);
-      r.phm[s] = make_float2(m.x * inv, m.y * inv);
-    }
-  }
-  r.sinc = p.comp_order > 0 ? __fmul_rn(sinc_of(k0), sinc_of(k1)) : 1.f;
-}
-
-// Interlaced + compensated value of stored mode (row r, z).
-template <int NS, bool FULL>
-__device__ __forceinline__ float2 combine_mode(const FourierParams &p, const RowFactor<NS> &r,
-                                               const ZTable &t, const float2 *__restrict__ in,
-                                               int64_t idx, int z) {
-  constexpr bool full = FULL;
-  float2 acc;
-  if (NS == 1) {
-    acc = in[idx];
-  } else {
-    acc = make_float2(0.f, 0.f);
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      const float2 v = in[(int64_t)s * p.d.ncomplex() + idx];
-      float2 ph = cmul(r.ph[s], t.ph[s * p.d.nz + z]);
-      if (full) {  // Hermitian part of the full-grid phase: (e^{i t(k)} + e^{-i t(-k)}) / 2
-        const float2 m = cmul(r.phm[s], t.phm[s * p.d.nz + z]);
-        ph = make_float2(0.5f * (ph.x + m.x), 0.5f * (ph.y + m.y));
-      }
-      const float2 c = cmul(v, ph);
-      acc.x += c.x;
-      acc.y += c.y;
-    }
-  }
-  if (p.comp_order > 0) {
-    const float c = inverse_power(__fmul_rn(r.sinc, t.sinc[z]), p.comp_order);
-    acc.x *= c;
-    acc.y *= c;
-  }
-  return acc;
-}
 
 // One warp per (i, j) row of the Hermitian mesh; lanes stride kz (coalesced).
 template <int NS, bool FULL>
@@ -145,20 +29,8 @@ __global__ void __launch_bounds__(IL_THREADS) interlace_kernel(FourierParams p,
   constexpr bool full = FULL;
   in += (int64_t)blockIdx.y * p.nshifts * d.ncomplex();  // batch of meshes along y
   out += (int64_t)blockIdx.y * d.ncomplex();
-  ZTable t;
-  t.ph = reinterpret_cast<float2 *>(ilsmem);
-  t.phm = t.ph + (size_t)p.nshifts * d.nz;
-  t.sinc = reinterpret_cast<float *>(t.phm + (full ? (size_t)p.nshifts * d.nz : 0));
-  for (int z = threadIdx.x; z < d.nz; z += blockDim.x) {
-    const float k2 = ccoord(z, d.n2, p.cspacing[2], !full);
-    const int zm = (d.n2 - z) % d.n2;
-    const float k2m = ccoord(zm, d.n2, p.cspacing[2], false);
-    for (int s = 0; s < p.nshifts; ++s) {
-      t.ph[s * d.nz + z] = expi(p.shifts[s] * k2);
-      if (full) t.phm[s * d.nz + z] = expi(-p.shifts[s] * k2m);
-    }
-    t.sinc[z] = sinc_of(k2);
-  }
+  ZTable t = ztable_at(ilsmem, p, full);
+  fill_ztable<FULL>(p, t);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nwarps = blockDim.x >> 5;

@@ -53,6 +53,8 @@ SIGNATURES = {
                     c_void_p, c_void_p, c_size_t],
     'pk_bin_global': [c_void_p, c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_void_p,
                       c_int, c_float, c_int, c_int, c_int32_p, c_void_p, c_void_p, c_size_t],
+    'pk_bin_global_interlaced': [c_void_p, c_void_p, c_int, c_int, c_int, c_int32_p, c_float_p, c_float_p, c_void_p,
+                                 c_int, c_float, c_int, c_int, c_int32_p, c_void_p, c_void_p, c_size_t],
     'pk_bin_global_noalloc': [c_void_p, c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_void_p,
                               c_int, c_float, c_int, c_int, c_int32_p, c_void_p],
     'pk_bin_firstpoint': [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int32_p, c_int32_p,

@@ -3,8 +3,10 @@
 The reference computes mock spectra one at a time (``ParticleField.paint`` +
 ``compute_mesh2_spectrum`` per mock, ``mesh.py:2604-2754`` / ``mesh2.py:253-374``).  Here
 a batch of catalogs goes through one paint launch sequence (``pk_paint_batch``: tiles of
-every mock in one grid), one batched cuFFT R2C, one ``pk_interlace_compensate_batch`` and
-one ``pk_bin_global_batch``, all on static buffers and captured once in a CUDA graph;
+every mock in one grid), one batched cuFFT R2C and one ``pk_bin_global_interlaced`` (the
+interlaced, compensated meshes binned as they are formed, never stored; for other
+multipole sets ``pk_interlace_compensate_batch`` then ``pk_bin_global_batch``), all on
+static buffers and captured once in a CUDA graph;
 each further batch of the same sizes is a graph replay.  The paint tile configuration is
 picked by the autotuner (``autotune.py``).
 
@@ -17,7 +19,7 @@ from . import _lib
 from . import resamplers
 from .autotune import best_tile_config, make_key
 from .mesh import _plan, _device, _workspace
-from .mesh2 import _los, _ell_factors
+from .mesh2 import _los, _ell_factors, _fusable
 
 __all__ = ['BatchedSpectra']
 
@@ -59,7 +61,10 @@ class BatchedSpectra:
         M, I = self.nmocks, self.interlacing
         self.real = torch.empty((M, I) + shape, dtype=torch.float32, device=dev)
         self.cplx = torch.empty((M, I, shape[0], shape[1], nz), dtype=torch.complex64, device=dev)
-        self.comb = torch.empty((M, shape[0], shape[1], nz), dtype=torch.complex64, device=dev)
+        # even multipoles (ell <= 4): bin straight from the shifted meshes, no combined mesh
+        self.fused = _fusable(bin.ells)
+        self.comb = None if self.fused else torch.empty((M, shape[0], shape[1], nz), dtype=torch.complex64,
+                                                         device=dev)
         self.nells, self.nbins = len(bin.ells), bin.nbins
         self.raw = torch.zeros(M * self.nells * self.nbins, dtype=torch.float64, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -113,6 +118,12 @@ class BatchedSpectra:
         stream = _lib.stream_handle()
         self._paint_with(self.tile_config, self.paint_ws)
         _lib.call('pk_fft_exec', self.plan, stream, _lib.ptr(self.real), _lib.ptr(self.cplx))
+        if self.fused:
+            _lib.call('pk_bin_global_interlaced', stream, _lib.ptr(self.cplx), self.nmocks, self.interlacing,
+                      self.order if self.compensate else 0, _lib.i32(a.meshsize), _lib.f32(a.kfun), _lib.f32(self.vlos),
+                      _lib.ptr(b.d_edges), len(b._edges1d), b._step, a.backend_code, self.nells, _lib.i32(b.ells),
+                      _lib.ptr(self.raw), _lib.ptr(self.bin_ws), self.bin_ws.numel())
+            return
         _lib.call('pk_interlace_compensate_batch', stream, _lib.ptr(self.cplx), self.nmocks, self.interlacing,
                   _lib.i32(a.meshsize), self.order if self.compensate else 0, a.backend_code, 0, 1.,
                   _lib.ptr(self.comb))

@@ -11,7 +11,8 @@ features of the coarse spectrum
     log(nbar V_cell)
 
 to the correction r = (P_ell,fine - P_ell,coarse) / P0,coarse, as the training-set mean of r
-per (ell, k bin) plus the network's standardised, realisation-dependent deviation from it.
+per (ell, k bin) plus the network's standardised, realisation-dependent deviation from it
+(calibrated so that its mean over the training mocks is zero in every bin).
 
 ``LearnedCorrection`` keeps the plain compensated coarse estimator as its fallback: it
 applies the network only to spectra whose configuration (mesh, box, resampler,
@@ -365,6 +366,14 @@ class LearnedCorrection:
         ts = (res / tstd[None, :, None]).reshape(-1)
         self.mlp = MLP(seed=seed)
         history = self.mlp.fit(xs, ts, steps=steps, batch=batch, lr=lr, seed=seed)
+        # calibrate: the network's mean predicted deviation over the training set, per
+        # (ell, bin), is folded into the table, so the mean correction over the training mocks
+        # is exactly the training-set mean (the network keeps only the realisation-dependent
+        # part)
+        y = torch.cat([self.mlp(xs[i:i + 65536].to(torch.float32)) for i in range(0, xs.shape[0], 65536)])
+        ybar = (y.double().reshape(ntr, nl, nb) * tstd[None, :, None]).mean(dim=0)
+        self.tmean = (table - ybar).cpu().numpy()
+        self.__dict__.pop('_dev_cache', None)
         # choose the bins to correct on the held-out mocks
         self.mask = np.ones((nl, nb), dtype=bool)
         corr = self._apply(p_low[ntr:], npart[ntr:], use_mask=False).cpu().numpy()

@@ -609,7 +609,9 @@ def _paint(attrs, positions, weights=None, resampler='cic', interlacing=0, compe
     """``_paint`` (``mesh.py:2673-2754``) on the GPU.
 
     Paint every interlacing shift in one tiled pass, batched R2C, then one fused
-    interlacing + compensation pass (which also folds the C2R normalisation).
+    interlacing + compensation pass (which also folds the C2R normalisation).  With
+    ``out='complex'`` that pass is deferred until the mesh's value is needed (a spectrum
+    of the mesh is binned from the shifted meshes directly).
     """
     order = resamplers.get_resampler(resampler).order
     interlacing = max(int(interlacing), 1)
@@ -625,6 +627,8 @@ def _paint(attrs, positions, weights=None, resampler='cic', interlacing=0, compe
         return ComplexMeshField(_r2c(meshes[0], meshsize), attrs=attrs)
     cmeshes = _r2c(meshes, meshsize)
     del meshes
+    if out != 'real':
+        return _InterlacedComplexMeshField(cmeshes, attrs, order if compensate else 0)
     for_c2r = out == 'real'
     scale = float(np.float32(1. / np.prod(meshsize))) if for_c2r else 1.
     combined = torch.empty(cmeshes.shape[1:], dtype=torch.complex64, device=positions.device)
@@ -635,6 +639,50 @@ def _paint(attrs, positions, weights=None, resampler='cic', interlacing=0, compe
     if for_c2r:
         return RealMeshField(_c2r(combined, meshsize, scale=False, destroy_input=True), attrs=attrs)
     return ComplexMeshField(combined, attrs=attrs)
+
+
+class _InterlacedComplexMeshField(ComplexMeshField):
+    """The complex mesh of ``paint(..., out='complex')`` with interlacing or compensation,
+    kept as its interlaced, uncompensated shifted meshes until its value is needed.
+
+    ``value`` forms the combined mesh (``pk_interlace_compensate``) on first access and
+    keeps it; ``compute_mesh2_spectrum`` bins an untouched field straight from the shifted
+    meshes (``pk_bin_global_interlaced``: the same numbers, without writing the combined
+    mesh and reading it back).  Everything else sees an ordinary ``ComplexMeshField``.
+    """
+
+    def __init__(self, shifted, attrs, comp_order):
+        self._shifted = shifted
+        self._comp_order = int(comp_order)
+        self._value = None
+        self.attrs = attrs
+
+    @property
+    def value(self):
+        if self._value is None:
+            meshsize = self.attrs.meshsize
+            combined = torch.empty(self._shifted.shape[1:], dtype=torch.complex64, device=self._shifted.device)
+            _lib.call('pk_interlace_compensate', _lib.stream_handle(), _lib.ptr(self._shifted),
+                      self._shifted.shape[0], _lib.i32(meshsize), self._comp_order, self.attrs.backend_code, 0,
+                      1., _lib.ptr(combined))
+            self._value = combined
+            self._shifted = None
+        return self._value
+
+    @value.setter
+    def value(self, v):
+        self._value = v
+        self._shifted = None
+
+    @property
+    def lazy(self):
+        """(shifted meshes, compensation order) while the combined mesh is not formed, else None."""
+        return None if self._shifted is None else (self._shifted, self._comp_order)
+
+    def clone(self, **kwargs):
+        if not kwargs or (set(kwargs) == {'attrs'} and kwargs['attrs'] is self.attrs):
+            return self
+        return ComplexMeshField(kwargs.pop('value', self.value), attrs=kwargs.pop('attrs', self.attrs)).clone(**kwargs)
 
 
 def _read(mesh, positions, resampler='cic', compensate=False, halo_add=0):

@@ -261,6 +261,27 @@ def _spectrum_sums(mattrs, bin, los, rmesh=None, cmesh=None, cmesh2=None, rmesh2
     return raw.reshape(len(ells), nbins)
 
 
+def _fusable(ells):
+    """Multipoles the fused interlace + binning pass takes (up to 3 even ells <= 4)."""
+    return len(ells) <= 3 and all(ell % 2 == 0 and ell <= 4 for ell in ells)
+
+
+def _interlaced_sums(mattrs, bin, vlos, shifted, comp_order):
+    """Global-los raw sums (nells, nbins) float64 of the mesh that interlacing ``shifted``
+    ((nshifts, N0, N1, N2/2+1) R2C meshes) with compensation order ``comp_order`` would give,
+    without forming it (``pk_bin_global_interlaced``)."""
+    nbytes = _lib.c_size_t()
+    _lib.call('pk_bin_batch_workspace_size', _lib.i32(mattrs.meshsize), len(bin._edges1d), len(bin.ells), 1,
+              _lib.ctypes.byref(nbytes))
+    ws = _workspace(nbytes.value)
+    out = torch.zeros(len(bin.ells) * bin.nbins, dtype=torch.float64, device=shifted.device)
+    _lib.call('pk_bin_global_interlaced', _lib.stream_handle(), _lib.ptr(shifted), 1, shifted.shape[0],
+              int(comp_order), _lib.i32(mattrs.meshsize), _lib.f32(mattrs.kfun), _lib.f32(vlos), _lib.ptr(bin.d_edges),
+              len(bin._edges1d), bin._step, mattrs.backend_code, len(bin.ells), _lib.i32(bin.ells), _lib.ptr(out),
+              _lib.ptr(ws), ws.numel())
+    return out.reshape(len(bin.ells), bin.nbins)
+
+
 def _split(mesh):
     if mesh is None:
         return None, None
@@ -278,9 +299,13 @@ def compute_mesh2_spectrum(*meshes, bin=None, los='z'):
     attrs = dict(los=vlos if vlos is not None else los_name)
     ells = bin.ells
     nbins = bin.nbins
-    r1, c1 = _split(meshes[0])
-    r2, c2 = (None, None) if fields[1] == fields[0] else _split(meshes[1])
-    raw = _spectrum_sums(mattrs, bin, los, rmesh=r1, cmesh=c1, rmesh2=r2, cmesh2=c2).cpu().numpy()
+    lazy = getattr(meshes[0], 'lazy', None) if fields[1] == fields[0] else None
+    if lazy is not None and vlos is not None and _fusable(ells):
+        raw = _interlaced_sums(mattrs, bin, vlos, *lazy).cpu().numpy()
+    else:
+        r1, c1 = _split(meshes[0])
+        r2, c2 = (None, None) if fields[1] == fields[0] else _split(meshes[1])
+        raw = _spectrum_sums(mattrs, bin, los, rmesh=r1, cmesh=c1, rmesh2=r2, cmesh2=c2).cpu().numpy()
     factors = _ell_factors(ells, vlos)
     num = [raw[i] / bin.nmodes * factors[i] for i in range(len(ells))]
     norm = np.full(nbins, norm_value, dtype='f8')
