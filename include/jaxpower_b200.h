@@ -276,6 +276,13 @@ pk_status pk_mlp_cast(void *stream, const float *w, void *wb);
 pk_status pk_mlp_forward(void *stream, const float *x, const int32_t *idx, int batch, const void *wb,
                          const float *w, float *y, float *z, float *h);
 
+/* pk_mlp_forward on the 5th-generation tensor cores (tcgen05.mma, bf16 operands in shared
+ * memory, float32 accumulators in tensor memory), 128 samples per CTA.  Same inputs and
+ * outputs as pk_mlp_forward (wb 16-byte aligned).  d_status (device int, may be NULL) is
+ * set to 1 if a tensor-core step did not complete within its bounded wait. */
+pk_status pk_mlp_forward_tc(void *stream, const float *x, const int32_t *idx, int batch, const void *wb,
+                            const float *w, float *y, float *z, float *h, int32_t *d_status);
+
 /* Weighted MSE: loss = sum_i w_j (y_i - t_j)^2 / batch with j = idx[i]; dy = dloss/dy.
  * weight and loss may be NULL. */
 pk_status pk_mlp_mse(void *stream, const float *y, const float *target, const float *weight,

@@ -149,6 +149,208 @@ __global__ void __launch_bounds__(MLP_WARPS * 32) mlp_forward_kernel(
   }
 }
 
+// ------------------------------------------------------------- tcgen05 forward pass
+// The same network on the 5th-generation tensor cores.  One CTA (4 warps) takes 128
+// samples; each layer is D[128 x N] = A[128 x K] B[N x K]^T with A (bf16 activations) and
+// B (bf16 weights, out x in) in shared memory in the no-swizzle K-major canonical layout
+// and D (float32) in tensor memory: one elected thread issues the K / 16
+// tcgen05.mma.kind::f16 instructions and commits them to an mbarrier; after the (bounded)
+// wait, warp w reads rows 32w..32w+31 of D with tcgen05.ld, adds the bias, applies SiLU
+// and writes the next layer's bf16 operand back to shared memory.
+constexpr int TC_ROWS = 128;
+constexpr int TC_THREADS = 128;
+constexpr int TC_N3 = 16;  // last layer's N (rows 8..15 of its weight tile are zero)
+constexpr int TC_TMEM_COLS = 128;
+constexpr unsigned TC_WAIT_LIMIT = 1u << 22;  // mbarrier polls before giving up
+constexpr size_t TC_SMEM = 4096 + 32768 + 32768 + 4096 + 4096 + 32768 + 64;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Byte offset of element (r, k) of an R x K bf16 matrix in the canonical no-swizzle
+// K-major layout: 8 x 8 core matrices of 128 contiguous bytes (row r & 7 at 16 (r & 7),
+// column k & 7 at 2 (k & 7)), laid out by row group, then by group of 8 columns.
+__device__ __forceinline__ uint32_t canon_off(int r, int k, int K) {
+  return (uint32_t)((((r >> 3) * (K >> 3)) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+// Shared-memory matrix descriptor (sm_100): start address, leading byte offset (between the
+// two 8-column groups of one K = 16 step), stride byte offset (between row groups), all >> 4;
+// descriptor version 1 at bit 46; no swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// kind::f16 instruction descriptor: f32 accumulator (bits 4-5 = 1), bf16 A and B (bits 7-9,
+// 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24 (M = 128).
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      :
+      : "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (unsigned it = 0; it < TC_WAIT_LIMIT; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void async_proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 32 consecutive float32 columns of this thread's tensor-memory lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t v[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+        "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+        "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// rows [0, rows) of a row-major bf16 matrix (rows x K) into the canonical layout of a
+// (rows_total x K) tile; rows [rows, rows_total) are zero.  16-byte chunks.
+__device__ __forceinline__ void load_canon(unsigned char *dst, const __nv_bfloat16 *__restrict__ src, int rows,
+                                           int rows_total, int K) {
+  const int chunks = rows_total * (K >> 3);
+  for (int c = threadIdx.x; c < chunks; c += blockDim.x) {
+    const int r = c / (K >> 3), kc = c % (K >> 3);
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (r < rows) v = *reinterpret_cast<const uint4 *>(src + (size_t)r * K + kc * 8);
+    *reinterpret_cast<uint4 *>(dst + canon_off(r, kc * 8, K)) = v;
+  }
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1) mlp_forward_tc_kernel(
+    const float *__restrict__ X, const int *__restrict__ idx, int batch, const __nv_bfloat16 *__restrict__ Wb,
+    const float *__restrict__ Wf, float *__restrict__ y, float *__restrict__ Z, float *__restrict__ H,
+    int *__restrict__ status) {
+  extern __shared__ __align__(1024) unsigned char tcsm[];
+  unsigned char *sW0 = tcsm, *sW1 = sW0 + 4096, *sW2 = sW1 + 32768, *sW3 = sW2 + 32768, *sA0 = sW3 + 4096,
+                *sA = sA0 + 4096;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sA + 32768);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int row = blockIdx.x * TC_ROWS + tid;  // this thread's sample (and D lane)
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(TC_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");  // visible to the commit
+  }
+  load_canon(sW0, Wb + OFF_W0, MLP_H, MLP_H, MLP_IN);
+  load_canon(sW1, Wb + OFF_W1, MLP_H, MLP_H, MLP_H);
+  load_canon(sW2, Wb + OFF_W2, MLP_H, MLP_H, MLP_H);
+  load_canon(sW3, Wb + OFF_W3, MLP_OUT, TC_N3, MLP_H);
+  {  // input features of this thread's sample (bf16, zero past the batch)
+    const bool in = row < batch;
+    const float *xr = X + (int64_t)(in ? sample_of(idx, row) : 0) * MLP_IN;
+#pragma unroll
+    for (int kc = 0; kc < MLP_IN; kc += 8) {
+      unsigned pk[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float a = in ? xr[kc + 2 * q] : 0.f, b = in ? xr[kc + 2 * q + 1] : 0.f;
+        pk[q] = pack_raw(__float2bfloat16_rn(a), __float2bfloat16_rn(b));
+      }
+      *reinterpret_cast<uint4 *>(sA0 + canon_off(tid, kc, MLP_IN)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+    }
+  }
+  async_proxy_fence();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+  bool ok = true;
+  for (int l = 0; l < 4 && ok; ++l) {
+    const int K = l == 0 ? MLP_IN : MLP_H;
+    const int N = l == 3 ? TC_N3 : MLP_H;
+    const unsigned char *A = l == 0 ? sA0 : sA;
+    const unsigned char *B = l == 0 ? sW0 : (l == 1 ? sW1 : (l == 2 ? sW2 : sW3));
+    if (tid == 0) {
+      const uint32_t idesc = umma_idesc_bf16(N);
+      const uint32_t sbo = (uint32_t)(K >> 3) * 128u;
+      for (int j = 0; j < K / 16; ++j)
+        tc_mma(tmem, umma_desc(smem_u32(A) + 256u * j, 128u, sbo), umma_desc(smem_u32(B) + 256u * j, 128u, sbo),
+               idesc, j > 0 ? 1u : 0u);
+      tc_commit(smem_u32(bar));
+    }
+    ok = __syncthreads_and(mbar_wait(smem_u32(bar), (uint32_t)(l & 1)) ? 1 : 0) != 0;
+    tc_fence_after();
+    if (!ok) break;
+    if (l < 3) {
+      const float *bias = Wf + (l == 0 ? OFF_B0 : (l == 1 ? OFF_B1 : OFF_B2));
+      for (int c0 = 0; c0 < MLP_H; c0 += 32) {
+        uint32_t v[32];
+        tmem_ld32(lane_addr + (uint32_t)c0, v);
+#pragma unroll
+        for (int c = 0; c < 32; c += 8) {
+          unsigned pk[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const float z0 = __uint_as_float(v[c + 2 * q]) + bias[c0 + c + 2 * q];
+            const float z1 = __uint_as_float(v[c + 2 * q + 1]) + bias[c0 + c + 2 * q + 1];
+            const float h0 = z0 * sigmoid(z0), h1 = z1 * sigmoid(z1);
+            pk[q] = pack_raw(__float2bfloat16_rn(h0), __float2bfloat16_rn(h1));
+            if (Z && row < batch) {
+              const int64_t o = ((int64_t)l * batch + row) * MLP_H + c0 + c + 2 * q;
+              Z[o] = z0;
+              Z[o + 1] = z1;
+              H[o] = h0;
+              H[o + 1] = h1;
+            }
+          }
+          *reinterpret_cast<uint4 *>(sA + canon_off(tid, c0 + c, MLP_H)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        }
+      }
+      async_proxy_fence();
+      tc_fence_before();
+      __syncthreads();
+      tc_fence_after();
+    } else {
+      uint32_t v[32];
+      tmem_ld32(lane_addr, v);
+      if (row < batch) y[row] = __uint_as_float(v[0]) + Wf[OFF_B3];
+    }
+  }
+  if (!ok && tid == 0 && status) atomicExch(status, 1);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS)
+                 : "memory");
+}
+
 // loss = sum_i w_i (y_i - t_i)^2 / batch, dy_i = 2 w_i (y_i - t_i) / batch; one CTA,
 // fixed-order reduction.  Targets and sample weights are gathered through idx.
 constexpr int MSE_THREADS = 1024;
@@ -343,6 +545,20 @@ extern "C" pk_status pk_mlp_forward(void *stream, const float *x, const int *idx
   const int blocks = (batch + MLP_CTA_ROWS - 1) / MLP_CTA_ROWS;
   mlp_forward_kernel<<<blocks, MLP_WARPS * 32, 0, (cudaStream_t)stream>>>(
       x, idx, batch, (const __nv_bfloat16 *)wb, w, y, z, h);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+extern "C" pk_status pk_mlp_forward_tc(void *stream, const float *x, const int *idx, int batch, const void *wb,
+                                       const float *w, float *y, float *z, float *h, int *d_status) {
+  PK_REQUIRE(x && wb && w && y && batch >= 0, PK_ERR_INVALID, "mlp_forward_tc: invalid arguments");
+  PK_REQUIRE((z == nullptr) == (h == nullptr), PK_ERR_INVALID, "mlp_forward_tc: z and h go together");
+  PK_REQUIRE(((uintptr_t)wb & 15u) == 0, PK_ERR_INVALID, "mlp_forward_tc: bf16 weights must be 16-byte aligned");
+  if (batch == 0) return PK_OK;
+  PK_CUDA(cudaFuncSetAttribute(mlp_forward_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+  const int blocks = (batch + TC_ROWS - 1) / TC_ROWS;
+  mlp_forward_tc_kernel<<<blocks, TC_THREADS, TC_SMEM, (cudaStream_t)stream>>>(
+      x, idx, batch, (const __nv_bfloat16 *)wb, w, y, z, h, d_status);
   PK_LAUNCH_CHECK();
   return PK_OK;
 }

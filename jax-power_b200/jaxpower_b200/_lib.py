@@ -74,6 +74,8 @@ SIGNATURES = {
     'pk_mlp_num_params': [],
     'pk_mlp_cast': [c_void_p, c_void_p, c_void_p],
     'pk_mlp_forward': [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p],
+    'pk_mlp_forward_tc': [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                          c_void_p],
     'pk_mlp_mse': [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p],
     'pk_mlp_backward_workspace_size': [c_int, ctypes.POINTER(c_size_t)],
     'pk_mlp_backward': [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,

@@ -4,7 +4,8 @@ Not in the reference: a new method on top of its estimator.  A catalog painted o
 coarse mesh (here CIC, 128^3) gives multipoles biased by aliasing near the Nyquist
 frequency; the same catalog painted on a 4x finer mesh gives the label.  A small BF16
 MLP (``MLP``: 16 -> 128 -> 128 -> 128 -> 1, SiLU, bf16 tensor-core operands with float32
-accumulation; forward, backward and AdamW kernels in ``csrc/mlp.cu``) maps per-bin
+accumulation; forward pass on the tcgen05 tensor cores (accumulators in tensor memory),
+backward and AdamW kernels, all in ``csrc/mlp.cu``) maps per-bin
 features of the coarse spectrum
 
     k / k_Nyq, (k / k_Nyq)^2, one-hot ell, log(nbar P0), P2 / P0, P4 / P0, P_ell / P0,
@@ -78,6 +79,7 @@ class MLP:
         self.m = torch.zeros(n, dtype=torch.float32, device=dev)
         self.v = torch.zeros(n, dtype=torch.float32, device=dev)
         self.step = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)  # set if a tensor-core wait ran out
         _lib.call('pk_mlp_cast', _lib.stream_handle(), _lib.ptr(self.w), _lib.ptr(self.wb))
 
     def params(self, name):
@@ -105,9 +107,14 @@ class MLP:
         if cache:
             z = torch.empty((3, b, HIDDEN), dtype=torch.float32, device=x.device)
             h = torch.empty_like(z)
-        _lib.call('pk_mlp_forward', _lib.stream_handle(), _lib.ptr(x), None, b, _lib.ptr(self.wb), _lib.ptr(self.w),
-                  _lib.ptr(y), _lib.ptr(z), _lib.ptr(h))
+        _lib.call('pk_mlp_forward_tc', _lib.stream_handle(), _lib.ptr(x), None, b, _lib.ptr(self.wb),
+                  _lib.ptr(self.w), _lib.ptr(y), _lib.ptr(z), _lib.ptr(h), _lib.ptr(self.status))
         return (y, (z, h)) if cache else y
+
+    def check(self):
+        """Raise if a tensor-core step of an earlier forward pass did not complete (synchronises)."""
+        if int(self.status.item()):
+            raise RuntimeError('MLP forward: a tensor-core step did not complete within its wait limit')
 
     __call__ = forward
 
@@ -165,8 +172,8 @@ class MLP:
             stream = _lib.stream_handle()
             for s in range(nb):
                 idx = _lib.ctypes.c_void_p(perm.data_ptr() + 4 * s * batch)
-                _lib.call('pk_mlp_forward', stream, _lib.ptr(x), idx, batch, _lib.ptr(self.wb), _lib.ptr(self.w),
-                          _lib.ptr(y), _lib.ptr(z), _lib.ptr(h))
+                _lib.call('pk_mlp_forward_tc', stream, _lib.ptr(x), idx, batch, _lib.ptr(self.wb), _lib.ptr(self.w),
+                          _lib.ptr(y), _lib.ptr(z), _lib.ptr(h), _lib.ptr(self.status))
                 _lib.call('pk_mlp_mse', stream, _lib.ptr(y), _lib.ptr(target), _lib.ptr(weight), idx, batch,
                           _lib.ptr(dy), _lib.ctypes.c_void_p(losses.data_ptr() + 4 * s))
                 _lib.call('pk_mlp_backward', stream, _lib.ptr(x), idx, batch, _lib.ptr(self.wb), _lib.ptr(z),
@@ -192,7 +199,9 @@ class MLP:
             else:
                 epoch()
             history.append(losses.mean())
-        return torch.stack(history).cpu().numpy()
+        out = torch.stack(history).cpu().numpy()
+        self.check()
+        return out
 
     def state(self):
         return self.w.detach().cpu().numpy().copy()

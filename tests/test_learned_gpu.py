@@ -38,6 +38,33 @@ def test_forward_matches_oracle(batch):
     assert err.max() < 2e-3
 
 
+@pytest.mark.parametrize('batch', [1, 127, 128, 129, 3000])
+def test_tcgen05_forward_matches_mma_forward(batch):
+    """The tcgen05 forward pass (accumulators in tensor memory) against the mma.sync one and
+    the oracle, outputs and stored pre-activations / activations."""
+    from jaxpower_b200 import _lib
+    flat = _flat(7)
+    mlp = _mlp(flat)
+    x = torch.as_tensor(np.random.default_rng(8).normal(size=(batch, omlp.IN)).astype('f4')).cuda()
+    outs = []
+    for name in ('pk_mlp_forward', 'pk_mlp_forward_tc'):
+        y = torch.empty(batch, device='cuda')
+        z = torch.empty((3, batch, omlp.H), device='cuda')
+        h = torch.empty_like(z)
+        extra = (_lib.ptr(mlp.status),) if name.endswith('_tc') else ()
+        _lib.call(name, _lib.stream_handle(), _lib.ptr(x), None, batch, _lib.ptr(mlp.wb), _lib.ptr(mlp.w),
+                  _lib.ptr(y), _lib.ptr(z), _lib.ptr(h), *extra)
+        outs.append((y.cpu().numpy(), z.cpu().numpy(), h.cpu().numpy()))
+    mlp.check()
+    (y0, z0, h0), (y1, z1, h1) = outs
+    scale = max(np.abs(y0).max(), 1e-3)
+    assert np.abs(y1 - y0).max() <= 1e-5 * scale
+    assert np.allclose(z1, z0, rtol=0, atol=1e-5 * np.abs(z0).max())
+    assert np.allclose(h1, h0, rtol=0, atol=1e-5 * np.abs(h0).max())
+    ref, _ = omlp.forward(flat.astype('f8'), x.cpu().numpy())
+    assert np.median(np.abs(y1 - ref)) < 2e-6 * max(np.abs(ref).max(), 1e-3)
+
+
 def test_gradient_matches_oracle():
     flat = _flat(2)
     rng = np.random.default_rng(3)
