@@ -338,6 +338,30 @@ def run_cutsky(reps=3):
                        'forward_backward = differentiable paint + spectrum + backward to data positions')
 
 
+def run_mlp_forward(batch=1 << 20, reps=20):
+    """Throughput of the correction network's tcgen05 forward pass on a batch of random
+    feature rows (dense FLOPs 2 (16 + 2 x 128 + 16) x 128 per row; the padded output layer
+    counts at its computed width 16)."""
+    import torch
+    from jaxpower_b200.learned import MLP
+    mlp = MLP(seed=3)
+    x = torch.randn((batch, 16), generator=torch.Generator(device='cuda').manual_seed(4), device='cuda')
+    for _ in range(3):
+        mlp(x)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        mlp(x)
+    b.record()
+    torch.cuda.synchronize()
+    mlp.check()
+    seconds = a.elapsed_time(b) / 1e3 / reps
+    flops = 2. * (16 + 2 * 128 + 16) * 128 * batch
+    return dict(batch=batch, seconds=seconds, rows_per_s=batch / seconds, tflops=flops / seconds / 1e12,
+                timing='CUDA events around %d forward passes (inputs resident)' % reps)
+
+
 def run_learned(ntrain=None, nheld=None, steps=None):
     """Train the learned correction on the GPU and evaluate it on held-out mocks."""
     import torch
@@ -584,6 +608,7 @@ def run_ours(args):
         line['cutsky'] = run_cutsky()
     if rank == 0 and world == 1 and not args.no_learned:
         line['learned'] = run_learned()
+        line['learned']['mlp_forward'] = run_mlp_forward()
     if rank == 0 and world == 1 and not args.no_cpu:
         seconds, desc, cores = cpu_sample(meshsize=args.cpu_meshsize)
         line['cpu_baseline'] = {'value': 1. / seconds, 'unit': 'spectra/s', 'cores': cores, 'kind': 'port',
@@ -608,7 +633,12 @@ def main():
     parser.add_argument('--no-batched', action='store_true', help='skip the batched-mocks measurement')
     parser.add_argument('--no-learned', action='store_true', help='skip training / evaluating the learned correction')
     parser.add_argument('--no-cutsky', action='store_true', help='skip the cut-sky FKP first-point measurement')
+    parser.add_argument('--mlp-forward-only', action='store_true',
+                        help='only time the correction network forward pass (profiling aid)')
     args = parser.parse_args()
+    if args.mlp_forward_only:
+        print(json.dumps({'mlp_forward': run_mlp_forward()}), flush=True)
+        return
     if args.impl == 'reference':
         run_reference(args)
     else:

@@ -156,7 +156,8 @@ __global__ void __launch_bounds__(MLP_WARPS * 32) mlp_forward_kernel(
 // and D (float32) in tensor memory: one elected thread issues the K / 16
 // tcgen05.mma.kind::f16 instructions and commits them to an mbarrier; after the (bounded)
 // wait, warp w reads rows 32w..32w+31 of D with tcgen05.ld, adds the bias, applies SiLU
-// and writes the next layer's bf16 operand back to shared memory.
+// and writes the next layer's bf16 operand back to shared memory.  CTAs are persistent
+// (two per SM): the weights are loaded into shared memory once per CTA.
 constexpr int TC_ROWS = 128;
 constexpr int TC_THREADS = 128;
 constexpr int TC_N3 = 16;  // last layer's N (rows 8..15 of its weight tile are zero)
@@ -256,7 +257,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mlp_forward_tc_kernel(
   uint64_t *bar = reinterpret_cast<uint64_t *>(sA + 32768);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
   const int tid = threadIdx.x, warp = tid >> 5;
-  const int row = blockIdx.x * TC_ROWS + tid;  // this thread's sample (and D lane)
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
                  "r"(TC_TMEM_COLS)
@@ -271,76 +271,88 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mlp_forward_tc_kernel(
   load_canon(sW1, Wb + OFF_W1, MLP_H, MLP_H, MLP_H);
   load_canon(sW2, Wb + OFF_W2, MLP_H, MLP_H, MLP_H);
   load_canon(sW3, Wb + OFF_W3, MLP_OUT, TC_N3, MLP_H);
-  {  // input features of this thread's sample (bf16, zero past the batch)
-    const bool in = row < batch;
-    const float *xr = X + (int64_t)(in ? sample_of(idx, row) : 0) * MLP_IN;
-#pragma unroll
-    for (int kc = 0; kc < MLP_IN; kc += 8) {
-      unsigned pk[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const float a = in ? xr[kc + 2 * q] : 0.f, b = in ? xr[kc + 2 * q + 1] : 0.f;
-        pk[q] = pack_raw(__float2bfloat16_rn(a), __float2bfloat16_rn(b));
-      }
-      *reinterpret_cast<uint4 *>(sA0 + canon_off(tid, kc, MLP_IN)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-    }
-  }
-  async_proxy_fence();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
   const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+  const int ntiles = (batch + TC_ROWS - 1) / TC_ROWS;
   bool ok = true;
-  for (int l = 0; l < 4 && ok; ++l) {
-    const int K = l == 0 ? MLP_IN : MLP_H;
-    const int N = l == 3 ? TC_N3 : MLP_H;
-    const unsigned char *A = l == 0 ? sA0 : sA;
-    const unsigned char *B = l == 0 ? sW0 : (l == 1 ? sW1 : (l == 2 ? sW2 : sW3));
-    if (tid == 0) {
-      const uint32_t idesc = umma_idesc_bf16(N);
-      const uint32_t sbo = (uint32_t)(K >> 3) * 128u;
-      for (int j = 0; j < K / 16; ++j)
-        tc_mma(tmem, umma_desc(smem_u32(A) + 256u * j, 128u, sbo), umma_desc(smem_u32(B) + 256u * j, 128u, sbo),
-               idesc, j > 0 ? 1u : 0u);
-      tc_commit(smem_u32(bar));
-    }
-    ok = __syncthreads_and(mbar_wait(smem_u32(bar), (uint32_t)(l & 1)) ? 1 : 0) != 0;
-    tc_fence_after();
-    if (!ok) break;
-    if (l < 3) {
-      const float *bias = Wf + (l == 0 ? OFF_B0 : (l == 1 ? OFF_B1 : OFF_B2));
-      for (int c0 = 0; c0 < MLP_H; c0 += 32) {
-        uint32_t v[32];
-        tmem_ld32(lane_addr + (uint32_t)c0, v);
+  uint32_t phase = 0;
+  // persistent: the weights stay in shared memory while the CTA walks its 128-row tiles
+  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const int row = tile * TC_ROWS + tid;  // this thread's sample (and D lane)
+    {  // input features of this thread's sample (bf16, zero past the batch)
+      const bool in = row < batch;
+      const float *xr = X + (int64_t)(in ? sample_of(idx, row) : 0) * MLP_IN;
 #pragma unroll
-        for (int c = 0; c < 32; c += 8) {
-          unsigned pk[4];
+      for (int kc = 0; kc < MLP_IN; kc += 8) {
+        unsigned pk[4];
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const float z0 = __uint_as_float(v[c + 2 * q]) + bias[c0 + c + 2 * q];
-            const float z1 = __uint_as_float(v[c + 2 * q + 1]) + bias[c0 + c + 2 * q + 1];
-            const float h0 = z0 * sigmoid(z0), h1 = z1 * sigmoid(z1);
-            pk[q] = pack_raw(__float2bfloat16_rn(h0), __float2bfloat16_rn(h1));
-            if (Z && row < batch) {
-              const int64_t o = ((int64_t)l * batch + row) * MLP_H + c0 + c + 2 * q;
-              Z[o] = z0;
-              Z[o + 1] = z1;
-              H[o] = h0;
-              H[o + 1] = h1;
-            }
-          }
-          *reinterpret_cast<uint4 *>(sA + canon_off(tid, c0 + c, MLP_H)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        for (int q = 0; q < 4; ++q) {
+          const float a = in ? xr[kc + 2 * q] : 0.f, b = in ? xr[kc + 2 * q + 1] : 0.f;
+          pk[q] = pack_raw(__float2bfloat16_rn(a), __float2bfloat16_rn(b));
         }
+        *reinterpret_cast<uint4 *>(sA0 + canon_off(tid, kc, MLP_IN)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
       }
+    }
+    async_proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    for (int l = 0; l < 4 && ok; ++l) {
+      const int K = l == 0 ? MLP_IN : MLP_H;
+      const int N = l == 3 ? TC_N3 : MLP_H;
+      const unsigned char *A = l == 0 ? sA0 : sA;
+      const unsigned char *B = l == 0 ? sW0 : (l == 1 ? sW1 : (l == 2 ? sW2 : sW3));
+      if (tid == 0) {
+        const uint32_t idesc = umma_idesc_bf16(N);
+        const uint32_t sbo = (uint32_t)(K >> 3) * 128u;
+        for (int j = 0; j < K / 16; ++j)
+          tc_mma(tmem, umma_desc(smem_u32(A) + 256u * j, 128u, sbo), umma_desc(smem_u32(B) + 256u * j, 128u, sbo),
+                 idesc, j > 0 ? 1u : 0u);
+        tc_commit(smem_u32(bar));
+      }
+      ok = __syncthreads_and(mbar_wait(smem_u32(bar), phase & 1u) ? 1 : 0) != 0;
+      ++phase;
+      tc_fence_after();
+      if (!ok) break;
+      if (l < 3) {
+        const float *bias = Wf + (l == 0 ? OFF_B0 : (l == 1 ? OFF_B1 : OFF_B2));
+        for (int c0 = 0; c0 < MLP_H; c0 += 32) {
+          uint32_t v[32];
+          tmem_ld32(lane_addr + (uint32_t)c0, v);
+#pragma unroll
+          for (int c = 0; c < 32; c += 8) {
+            unsigned pk[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const float z0 = __uint_as_float(v[c + 2 * q]) + bias[c0 + c + 2 * q];
+              const float z1 = __uint_as_float(v[c + 2 * q + 1]) + bias[c0 + c + 2 * q + 1];
+              const float h0 = z0 * sigmoid(z0), h1 = z1 * sigmoid(z1);
+              pk[q] = pack_raw(__float2bfloat16_rn(h0), __float2bfloat16_rn(h1));
+              if (Z && row < batch) {
+                const int64_t o = ((int64_t)l * batch + row) * MLP_H + c0 + c + 2 * q;
+                Z[o] = z0;
+                Z[o + 1] = z1;
+                H[o] = h0;
+                H[o + 1] = h1;
+              }
+            }
+            *reinterpret_cast<uint4 *>(sA + canon_off(tid, c0 + c, MLP_H)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+          }
+        }
+      } else {
+        uint32_t v[32];
+        tmem_ld32(lane_addr, v);
+        if (row < batch) y[row] = __uint_as_float(v[0]) + Wf[OFF_B3];
+      }
+      // the next MMA (this tile's next layer or the next tile's first) reads shared memory
+      // written above and overwrites the accumulators read above
       async_proxy_fence();
       tc_fence_before();
       __syncthreads();
       tc_fence_after();
-    } else {
-      uint32_t v[32];
-      tmem_ld32(lane_addr, v);
-      if (row < batch) y[row] = __uint_as_float(v[0]) + Wf[OFF_B3];
     }
   }
   if (!ok && tid == 0 && status) atomicExch(status, 1);
@@ -556,7 +568,8 @@ extern "C" pk_status pk_mlp_forward_tc(void *stream, const float *x, const int *
   PK_REQUIRE(((uintptr_t)wb & 15u) == 0, PK_ERR_INVALID, "mlp_forward_tc: bf16 weights must be 16-byte aligned");
   if (batch == 0) return PK_OK;
   PK_CUDA(cudaFuncSetAttribute(mlp_forward_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
-  const int blocks = (batch + TC_ROWS - 1) / TC_ROWS;
+  const int ntiles = (batch + TC_ROWS - 1) / TC_ROWS;
+  const int blocks = ntiles < 2 * sm_count() ? ntiles : 2 * sm_count();  // persistent, 2 CTAs per SM
   mlp_forward_tc_kernel<<<blocks, TC_THREADS, TC_SMEM, (cudaStream_t)stream>>>(
       x, idx, batch, (const __nv_bfloat16 *)wb, w, y, z, h, d_status);
   PK_LAUNCH_CHECK();
