@@ -587,10 +587,13 @@ struct GlobalSmem {
 // NS > 0: the mesh is not stored; each mode is formed on the fly from NS interlaced,
 // uncompensated meshes at d1 (mesh s at d1 + s N_c), exactly as pk_interlace_compensate
 // forms it (fp: its parameters; FULL: 'jaxdecomp' semantics), which saves writing and
-// reading back the combined mesh (that form gets a larger register budget: 2 CTAs per SM
-// instead of 4).
+// reading back the combined mesh (that form gets a larger register budget: 3 CTAs per SM
+// instead of 4, the fastest of 2 / 3 / 4 measured at 128^3 batches and 512^3).
+#ifndef PK_FUSED_MIN_CTAS
+#define PK_FUSED_MIN_CTAS 3
+#endif
 template <int NV, bool CROSS, bool EVEN, int NS = 0, bool FULL = false>
-__global__ void __launch_bounds__(BIN_THREADS, NS > 0 ? 2 : 4) bin_global_kernel(
+__global__ void __launch_bounds__(BIN_THREADS, NS > 0 ? PK_FUSED_MIN_CTAS : 4) bin_global_kernel(
     BinGeom g, const float2 *__restrict__ d1, const float2 *__restrict__ d2, float lx, float ly,
     float lz, LegendreCoefs lc, int zero_l0, const float *__restrict__ edges, int nwarps_hist,
     int tab, double *__restrict__ partials, FourierParams fp) {
