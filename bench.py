@@ -52,6 +52,57 @@ LAUNCHES = {'pk_paint': 5, 'pk_interlace_compensate': 1, 'pk_bin_global': 2, 'pk
             'pk_bin_modes': 2, 'pk_bin_mesh': 2, 'pk_scale_real': 1, 'pk_ylm_premultiply': 1, 'pk_read': 1}
 
 
+# ncu DRAM read + write of one pk_paint call of the 512^3 workload above (its count and fill
+# bucket passes and the tile pass, one-pass metrics on the full-size workload); the event
+# timing supplies the duration
+PAINT_TRAFFIC_512 = 59694336 + 11008 + 59890688 + 107570176 + 169368576 + 1547861504
+
+C0 = dict(workload='uniform catalog 1e5 particles in a 1000 Mpc/h cube (seed 0), meshsize 64, CIC, no interlacing, '
+                   'compensate, los z, ells (0,2,4), k step 0.01', nparticles=100000, meshsize=64, boxsize=1000.,
+          resampler='cic', interlacing=0, compensate=True, k_step=0.01, seed=0)
+
+
+def run_c0(reps=50):
+    """The reference's CPU-runnable configuration: GPU spectra/s through the public API
+    (positions resident) beside the oracle's float32 pipeline on the host, and their
+    difference (parity of the two on these inputs)."""
+    import torch
+    import jaxpower_b200 as jp
+    from oracle.coords import Geometry
+    from oracle import paint as opaint
+    from oracle.spectrum import Bins, compute_mesh2_spectrum as ospectrum
+    c = C0
+    rng = np.random.default_rng(c['seed'])
+    pos = (rng.uniform(0., c['boxsize'], (c['nparticles'], 3))).astype('f4')
+    attrs = jp.MeshAttrs(meshsize=c['meshsize'], boxsize=c['boxsize'], boxcenter=c['boxsize'] / 2.)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': c['k_step']}, ells=(0, 2, 4))
+    dpos = torch.as_tensor(pos).cuda()
+
+    def gpu():
+        mesh = jp.ParticleField(dpos, attrs=attrs).paint(resampler=c['resampler'], interlacing=c['interlacing'],
+                                                         compensate=c['compensate'], out='complex')
+        return jp.compute_mesh2_spectrum(mesh, bin=b, los='z')
+
+    for _ in range(3):
+        gpu()
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(reps):
+        res = gpu()
+    torch.cuda.synchronize()
+    t_gpu = (time.perf_counter() - t) / reps
+    geom = Geometry(c['meshsize'], c['boxsize'], c['boxsize'] / 2.)
+    t = time.perf_counter()
+    ref = ospectrum(opaint.paint(geom, pos, None, c['resampler'], c['interlacing'], c['compensate'], 'complex'),
+                    Bins(geom, step=c['k_step'], ells=(0, 2, 4)), los='z')['num_raw']
+    t_cpu = time.perf_counter() - t
+    got = np.array([p.num_raw for p in res])
+    return dict(c, gpu_spectra_per_s=1. / t_gpu, cpu_oracle_spectra_per_s=1. / t_cpu, cpu_cores=os.cpu_count(),
+                max_rel_diff_vs_oracle=float(np.abs(got - ref).max() / np.abs(ref[0]).max()),
+                timing='GPU: wall clock per spectrum through the public API with host read-back (positions '
+                       'resident); CPU: the oracle float32 pipeline, one run')
+
+
 def measured_peaks():
     path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
     if os.path.exists(path):
@@ -598,12 +649,16 @@ def run_ours(args):
                            l2='inputs larger than L2 (512 MiB meshes per shift)', out='complex'),
             'roofline': {'bound': 'hbm', 'kernel': dominant, 'achieved': achieved, 'peak': peak,
                          'peak_kind': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak,
-                         'algorithmic_bytes': abytes, 'traffic': None},
+                         'algorithmic_bytes': abytes,
+                         'traffic': float(PAINT_TRAFFIC_512) if (dominant == 'pk_paint' and W['meshsize'] == 512) else None,
+                         'traffic_source': 'ncu dram read+write of the pk_paint kernels, this workload at 512^3'},
             'e2e': {'value': e2e_value, 'unit': 'spectra/s', 'h2d_bytes_per_step': int(npart * 12),
                     'd2h_bytes_per_step': int(len(W['ells']) * nbins * 8)},
             'gpu_launches': int(launches), 'stages': stage_report, 'clocks': clocks.summary()}
     if rank == 0 and world == 1 and not args.no_batched:
         line['batched'] = run_batched()
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line['c0'] = run_c0()
     if rank == 0 and world == 1 and not args.no_cutsky:
         line['cutsky'] = run_cutsky()
     if rank == 0 and world == 1 and not args.no_learned:
