@@ -173,6 +173,29 @@ pk_status pk_bin_global(void *stream, const void *delta1, const void *delta2,
                         int nells, const int32_t *ells, double *d_out, void *workspace,
                         size_t workspace_bytes);
 
+/* --------------------------------------------------- correlation function (real space)
+ * Binning on the real-space separation grid of BinMesh2CorrelationPoles
+ * (mesh2.py:124-192, _make_edges2('real'), mesh2.py:25-62): separation coordinates
+ * s_d = fftfreq(n_d)[i] * cellsize_d * n_d on the full real mesh (unit weights), bins of
+ * |s| by exact |s|^2 thresholds as for k.  Workspace from pk_bin_separation_workspace_size. */
+pk_status pk_bin_separation_workspace_size(const int32_t meshsize[3], int nedges, int nvalues,
+                                           size_t *bytes);
+
+/* Per-bin number of separations (d_nmodes) and sum of |s| (d_ssum), float64. */
+pk_status pk_bin_separation_modes(void *stream, const int32_t meshsize[3], const float cellsize[3],
+                                  const float *d_edges, int nedges, float step, double *d_nmodes,
+                                  double *d_ssum, void *workspace, size_t workspace_bytes);
+
+/* Fixed line of sight branch of compute_mesh2_correlation (mesh2.py:465-499): for each
+ * multipole ell (nells <= 3) the per-bin sum of value(s) L_ell(mu), mu = s.los / |s|
+ * (|s| = 1 at s = 0), the s = 0 cell dropped for ell > 0; value is a real mesh (float32,
+ * e.g. c2r(|delta_k|^2)).  d_out: (nells, nbins) float64 sums (divide by nmodes,
+ * times 2 ell + 1). */
+pk_status pk_bin_separation_global(void *stream, const float *value, const int32_t meshsize[3],
+                                   const float cellsize[3], const float los[3], const float *d_edges,
+                                   int nedges, float step, int nells, const int32_t *ells,
+                                   double *d_out, void *workspace, size_t workspace_bytes);
+
 /* pk_bin_global_batch of the meshes that pk_interlace_compensate(_batch) would form
  * (for_c2r = 0, scale 1), without storing them: each mode is combined on the fly from
  * the nshifts interlaced, uncompensated R2C meshes (shifted: nbatch x nshifts Hermitian

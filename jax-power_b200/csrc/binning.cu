@@ -28,16 +28,18 @@ constexpr int MAX_FP_TERMS = 32;
 constexpr int MAX_ELLS = 9;
 
 struct BinGeom {
-  Dims d;
-  float kfun[3];
+  Dims d;          // separation grid: d.nz = n2 (the full real mesh)
+  float kfun[3];   // separation grid: the cell size
   int nedges;
   float step;  // > 0: uniform edges
   int backend;
+  int sep;     // 1: real-space separation grid (fftfreq * cellsize * n, unit weights)
 };
 
 // Hermitian weight of stored mode z: 'jax' 1 + (kz > 0); 'jaxdecomp' counts the
 // mirrored half of a full complex grid (self-conjugate planes once).
 __device__ __forceinline__ float mode_weight(const BinGeom &g, int z) {
+  if (g.sep) return 1.f;
   if (g.backend == PK_BACKEND_JAX) return z > 0 ? 2.f : 1.f;
   const bool selfconj = (z == 0) || ((g.d.n2 % 2) == 0 && z == g.d.nz - 1);
   return selfconj ? 1.f : 2.f;
@@ -45,7 +47,7 @@ __device__ __forceinline__ float mode_weight(const BinGeom &g, int z) {
 
 __device__ __forceinline__ float kz_coord(const BinGeom &g, int z) {
   // jaxdecomp: full-grid fftfreq (the Nyquist index is -N/2); jax: rfftfreq
-  return kcoord(z, g.d.n2, g.kfun[2], g.backend == PK_BACKEND_JAX);
+  return kcoord(z, g.d.n2, g.kfun[2], !g.sep && g.backend == PK_BACKEND_JAX);
 }
 
 // Legendre polynomials with the reference's float32 expression order (utils.py:341-360).
@@ -123,6 +125,28 @@ struct MeshOp {  // plain per-bin sum of a complex mesh value (BinMesh2SpectrumP
     const bool zero = remove_zero && i == 0 && j == 0 && z == 0;
     out[0] = zero ? 0.f : __fmul_rn(a.x, w);
     out[1] = zero ? 0.f : __fmul_rn(a.y, w);
+  }
+};
+
+// w * value * L_ell(mu) of a real mesh on the separation grid, mu = s.los / |s| (|s|(0) = 1);
+// the s = 0 cell is dropped for ell > 0 (compute_mesh2_correlation, mesh2.py:479-489).
+template <int N>
+struct SepLegendreOp {
+  const float *v;
+  float los[3];
+  int ells[MAX_ELLS];
+  static constexpr int NV = N;
+  __device__ void operator()(int64_t idx, int i, int j, int z, float sx, float sy, float sz, float s2,
+                             float w, float out[NV]) const {
+    const float a = v[idx] * w;
+    const bool zero = (i == 0 && j == 0 && z == 0);
+    const float num = (sx * los[0] + sy * los[1]) + sz * los[2];
+    const float mu = s2 > 0.f ? __fdiv_rn(num, __fsqrt_rn(s2)) : 0.f;
+#pragma unroll
+    for (int l = 0; l < NV; ++l) {
+      const int ell = ells[l];
+      out[l] = ell == 0 ? a : (zero ? 0.f : a * legendre(ell, mu));
+    }
   }
 };
 
@@ -250,7 +274,9 @@ __device__ __forceinline__ void bin_smem_flush(const BinSmem &s, int hist_len, i
 // non-decreasing along the run, so the bin only moves forward: interior segments of a run
 // belong to that lane alone and go straight to the warp's float64 histogram; the first
 // and last segments of every run are merged across lanes by one segmented scan per row.
-template <int NV, class Op>
+// SEP (real-space separation grid): |s| grows along z over z in [0, P), P = (n2 + 1) / 2, and
+// along decreasing z over [P, n2); each row is walked as these two monotone half-rows.
+template <int NV, class Op, bool SEP = false>
 __global__ void __launch_bounds__(BIN_THREADS) bin_rows_kernel(BinGeom g, Op op,
                                                                const float *__restrict__ edges,
                                                                int nwarps_hist, int tab,
@@ -263,12 +289,15 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_rows_kernel(BinGeom g, Op op,
   double *my = s.hist + (size_t)warp * hist_len;
   const float e0 = edges[0];
   const float inv_step = g.step > 0.f ? 1.f / g.step : 0.f;
-  const int R = (g.d.nz + 31) / 32;
-  const int z0 = lane * R, z1 = min(g.d.nz, z0 + R);
   constexpr int NONE = 0x7fffffff;
-  for (RowWalker rw((int64_t)blockIdx.x * nwarps + warp, (int64_t)gridDim.x * nwarps, g.d.n1); rw.i < g.d.n0;
-       rw.next()) {
-    const int i = rw.i, j = rw.j;
+  const int npos = SEP ? (g.d.n2 + 1) / 2 : g.d.nz;  // length of the first half-row
+  for (RowWalker rw((int64_t)blockIdx.x * nwarps + warp, (int64_t)gridDim.x * nwarps, g.d.n1 * (SEP ? 2 : 1));
+       rw.i < g.d.n0; rw.next()) {
+    const int i = rw.i, j = SEP ? (rw.j >> 1) : rw.j;
+    const int half = SEP ? (rw.j & 1) : 0;
+    const int len = half ? g.d.n2 - npos : npos;
+    const int R = (len + 31) / 32;
+    const int z0 = lane * R, z1 = min(len, z0 + R);
     const int64_t row = (int64_t)i * g.d.n1 + j;
     const float kx = kcoord(i, g.d.n0, g.kfun[0], false);
     const float ky = kcoord(j, g.d.n1, g.kfun[1], false);
@@ -277,7 +306,8 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_rows_kernel(BinGeom g, Op op,
     float acc[NV], facc[NV];
 #pragma unroll
     for (int c = 0; c < NV; ++c) acc[c] = facc[c] = 0.f;
-    for (int z = z0; z < z1; ++z) {
+    for (int t = z0; t < z1; ++t) {
+      const int z = half ? g.d.n2 - 1 - t : t;
       float kz, kz2;
       if (tab) {
         kz = s.kz[z];
@@ -517,7 +547,7 @@ static bool plan_bins(const Dims &d, int nedges, int nv, BinLaunch *L,
   return true;
 }
 
-template <int NV, class Op>
+template <int NV, class Op, bool SEP = false>
 static pk_status launch_bins(cudaStream_t s, const BinGeom &g, const Op &op, const float *edges,
                              bool rows, int accumulate, double *out0, double *out1,
                              void *workspace, size_t workspace_bytes) {
@@ -529,10 +559,10 @@ static pk_status launch_bins(cudaStream_t s, const BinGeom &g, const Op &op, con
              workspace_bytes);
   double *partials = static_cast<double *>(workspace);
   if (rows) {
-    PK_CUDA(cudaFuncSetAttribute(bin_rows_kernel<NV, Op>,
+    PK_CUDA(cudaFuncSetAttribute(bin_rows_kernel<NV, Op, SEP>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
-    bin_rows_kernel<NV, Op><<<L.blocks, L.nwarps * 32, L.smem, s>>>(g, op, edges, L.nwarps, L.tab,
-                                                                     partials);
+    bin_rows_kernel<NV, Op, SEP><<<L.blocks, L.nwarps * 32, L.smem, s>>>(g, op, edges, L.nwarps, L.tab,
+                                                                          partials);
   } else {
     PK_CUDA(cudaFuncSetAttribute(bin_chunks_kernel<NV, Op>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
@@ -862,6 +892,7 @@ static pk_status make_geom(const int32_t meshsize[3], const float kfun[3], int n
   g->nedges = nedges;
   g->step = step;
   g->backend = backend;
+  g->sep = 0;
   return PK_OK;
 }
 
@@ -1038,6 +1069,64 @@ extern "C" pk_status pk_bin_global_interlaced(void *stream, const void *shifted,
 #undef PK_GI_CASE
   }
   set_error("unsupported fused binning configuration");
+  return PK_ERR_INVALID;
+}
+
+static pk_status make_sep_geom(const int32_t meshsize[3], const float cellsize[3], int nedges, float step,
+                               BinGeom *g) {
+  pk_status st = make_geom(meshsize, cellsize, nedges, step, PK_BACKEND_JAX, g);
+  if (st) return st;
+  g->sep = 1;
+  g->d.nz = g->d.n2;  // the full real mesh
+  return PK_OK;
+}
+
+extern "C" pk_status pk_bin_separation_workspace_size(const int32_t meshsize[3], int nedges, int nvalues,
+                                                      size_t *bytes) {
+  PK_REQUIRE(bytes && meshsize, PK_ERR_INVALID, "null pointer");
+  Dims d;
+  PK_REQUIRE(make_dims(meshsize, &d), PK_ERR_INVALID, "invalid meshsize");
+  d.nz = d.n2;
+  BinLaunch L;
+  PK_REQUIRE(plan_bins(d, nedges, nvalues, &L), PK_ERR_RANGE, "too many bins x values (%d x %d)", nedges - 1,
+             nvalues);
+  *bytes = L.partial_bytes;
+  return PK_OK;
+}
+
+extern "C" pk_status pk_bin_separation_modes(void *stream, const int32_t meshsize[3], const float cellsize[3],
+                                             const float *d_edges, int nedges, float step, double *d_nmodes,
+                                             double *d_ssum, void *workspace, size_t workspace_bytes) {
+  BinGeom g;
+  pk_status st = make_sep_geom(meshsize, cellsize, nedges, step, &g);
+  if (st) return st;
+  PK_REQUIRE(d_edges && d_nmodes && d_ssum, PK_ERR_INVALID, "null pointer");
+  return launch_bins<2, ModesOp, true>((cudaStream_t)stream, g, ModesOp(), d_edges, true, 0, d_nmodes, d_ssum,
+                                       workspace, workspace_bytes);
+}
+
+extern "C" pk_status pk_bin_separation_global(void *stream, const float *value, const int32_t meshsize[3],
+                                              const float cellsize[3], const float los[3], const float *d_edges,
+                                              int nedges, float step, int nells, const int32_t *ells,
+                                              double *d_out, void *workspace, size_t workspace_bytes) {
+  BinGeom g;
+  pk_status st = make_sep_geom(meshsize, cellsize, nedges, step, &g);
+  if (st) return st;
+  PK_REQUIRE(value && d_edges && d_out && los && ells, PK_ERR_INVALID, "null pointer");
+  PK_REQUIRE(nells >= 1 && nells <= 3, PK_ERR_INVALID, "nells must be in 1..3");
+  for (int l = 0; l < nells; ++l) PK_REQUIRE(ells[l] >= 0 && ells[l] <= 8, PK_ERR_INVALID, "ell must be in 0..8");
+  cudaStream_t cs = (cudaStream_t)stream;
+#define PK_SEP_CASE(N)                                                                             \
+  if (nells == N) {                                                                                \
+    SepLegendreOp<N> op;                                                                           \
+    op.v = value;                                                                                  \
+    for (int a = 0; a < 3; ++a) op.los[a] = los[a];                                                \
+    for (int l = 0; l < MAX_ELLS; ++l) op.ells[l] = l < nells ? ells[l] : 0;                       \
+    return launch_bins<N, SepLegendreOp<N>, true>(cs, g, op, d_edges, true, 0, d_out, nullptr, workspace, \
+                                                  workspace_bytes);                                \
+  }
+  PK_SEP_CASE(1) PK_SEP_CASE(2) PK_SEP_CASE(3)
+#undef PK_SEP_CASE
   return PK_ERR_INVALID;
 }
 

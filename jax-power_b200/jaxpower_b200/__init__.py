@@ -10,10 +10,11 @@ and the ``resamplers`` namespaces.  All computation runs in the CUDA library
 from . import resamplers
 from .mesh import (MeshAttrs, BaseMeshField, RealMeshField, ComplexMeshField, ParticleField, FKPField,
                    get_mesh_attrs, next_fft_size, r2c, c2r, apply, read, paint)
-from .mesh2 import (BinMesh2SpectrumPoles, compute_mesh2_spectrum, compute_mesh2, compute_fkp2_normalization,
+from .mesh2 import (BinMesh2SpectrumPoles, BinMesh2CorrelationPoles, compute_mesh2_spectrum,
+                    compute_mesh2_correlation, compute_mesh2, compute_fkp2_normalization,
                     compute_fkp2_shotnoise, compute_box2_normalization, compute_normalization,
                     compute_box_normalization)
-from .types import Mesh2SpectrumPole, Mesh2SpectrumPoles
+from .types import Mesh2SpectrumPole, Mesh2SpectrumPoles, Mesh2CorrelationPole, Mesh2CorrelationPoles
 from ._lib import load as load_library, LIBRARY_PATH
 
 __version__ = '0.1.0'

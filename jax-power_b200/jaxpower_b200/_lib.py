@@ -53,6 +53,11 @@ SIGNATURES = {
                     c_void_p, c_void_p, c_size_t],
     'pk_bin_global': [c_void_p, c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_void_p,
                       c_int, c_float, c_int, c_int, c_int32_p, c_void_p, c_void_p, c_size_t],
+    'pk_bin_separation_workspace_size': [c_int32_p, c_int, c_int, ctypes.POINTER(c_size_t)],
+    'pk_bin_separation_modes': [c_void_p, c_int32_p, c_float_p, c_void_p, c_int, c_float, c_void_p, c_void_p,
+                                c_void_p, c_size_t],
+    'pk_bin_separation_global': [c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_void_p, c_int, c_float,
+                                 c_int, c_int32_p, c_void_p, c_void_p, c_size_t],
     'pk_bin_global_interlaced': [c_void_p, c_void_p, c_int, c_int, c_int, c_int32_p, c_float_p, c_float_p, c_void_p,
                                  c_int, c_float, c_int, c_int, c_int32_p, c_void_p, c_void_p, c_size_t],
     'pk_bin_global_noalloc': [c_void_p, c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_void_p,

@@ -232,18 +232,23 @@ class MeshAttrs:
     ccoords = kcoords
 
     def rcoords(self, kind='position', sparse=None):
-        """Cell-corner positions (``mesh.py:1594-1603``), torch float32."""
+        """Cell-corner positions, indices or separations (``mesh.py:1594-1603``), torch float32."""
         toret = []
         for axis in range(3):
             n = int(self.meshsize[axis])
             if kind == 'index':
                 toret.append(np.arange(n, dtype='i4'))
                 continue
+            if kind == 'separation':  # fftfreq(n) * cellsize * n (mesh.py:392-394), float32
+                sf = np.where(np.arange(n) < (n + 1) // 2, np.arange(n), np.arange(n) - n).astype('f4')
+                x = ((sf / np.float32(n)).astype('f4') * np.float32(self.cellsize[axis])).astype('f4') * np.float32(n)
+                toret.append(x.astype('f4'))
+                continue
             x = (np.arange(n, dtype='f4') * self.cellsize[axis]).astype('f4')
             if kind == 'position':
                 off = np.float32(self.boxcenter[axis] - np.float32(self.boxsize[axis] / np.float32(2.)))
                 x = (x + off).astype('f4')
-            elif kind != 'separation':
+            else:
                 raise ValueError('unknown kind {}'.format(kind))
             toret.append(x)
         return _meshgrid(toret, sparse)

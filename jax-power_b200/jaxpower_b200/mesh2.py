@@ -20,7 +20,7 @@ import torch
 from . import _lib
 from .mesh import (MeshAttrs, BaseMeshField, RealMeshField, ComplexMeshField, ParticleField, FKPField,
                    _r2c, _c2r, _workspace, _device, _paint, get_mesh_attrs)
-from .types import Mesh2SpectrumPole, Mesh2SpectrumPoles
+from .types import Mesh2SpectrumPole, Mesh2SpectrumPoles, Mesh2CorrelationPole, Mesh2CorrelationPoles
 
 __all__ = ['BinMesh2SpectrumPoles', 'compute_mesh2_spectrum', 'compute_mesh2', 'compute_fkp2_normalization',
            'compute_fkp2_shotnoise', 'compute_box2_normalization', 'compute_normalization',
@@ -135,6 +135,139 @@ class BinMesh2SpectrumPoles:
                   self.mattrs.backend_code, int(bool(remove_zero)), _lib.ptr(out), _lib.ptr(ws), ws.numel())
         out = out.cpu().numpy()
         return (out[:self.nbins] + 1j * out[self.nbins:]) / self.nmodes
+
+
+class BinMesh2CorrelationPoles:
+    """Binning operator for mesh to correlation function (``mesh2.py:124-192``).
+
+    Separations are the real-space grid ``fftfreq(n) * cellsize * n`` of the full mesh
+    (``mesh.py:1590-1603``, kind 'separation'), every cell with unit weight; bins of |s|
+    (exact |s|^2 thresholds on the GPU).
+
+    Parameters
+    ----------
+    mattrs : MeshAttrs or mesh field
+    edges : array, dict ('min', 'max' (default cellsize * min(meshsize) / 2), 'step') or None
+    ells : int or tuple
+    mode_oversampling : only 0; basis : only the default (configuration-space) binning
+    """
+
+    def __init__(self, mattrs, edges=None, ells=0, mode_oversampling=0, basis=None, klimit=None, batch_size=None):
+        if not isinstance(mattrs, MeshAttrs):
+            mattrs = mattrs.attrs
+        if mode_oversampling:
+            raise NotImplementedError('mode_oversampling > 0 is not supported on the GPU path')
+        if basis == 'bessel':
+            raise NotImplementedError("basis='bessel' is not supported on the GPU path")
+        self.mattrs = mattrs
+        self.ells = _format_ells(ells)
+        self.basis = basis
+        vec0 = np.float32(mattrs.cellsize.min())
+        if edges is None:
+            edges = {}
+        if isinstance(edges, dict):
+            step = edges.get('step', None)
+            vecmax = np.float32(np.float32(vec0 * np.float32(np.min(mattrs.meshsize))) / np.float32(2.))
+            if step is None:
+                edges = self._find_unique_edges(vec0, edges.get('min', 0.), edges.get('max', np.inf))
+            else:
+                edges = np.arange(edges.get('min', 0.), edges.get('max', float(vecmax)), step)
+        edges = np.asarray(edges, dtype='f8')
+        if edges.ndim == 2:
+            edges = np.append(edges[:, 0], edges[-1, 1])
+        self._edges1d = edges
+        self.edges = np.column_stack([edges[:-1], edges[1:]])
+        self._step = _uniform_step(edges.astype('f4'))
+        self.d_edges = torch.as_tensor(edges.astype('f4'), device=_device())
+        nbins = len(edges) - 1
+        nmodes = torch.empty(nbins, dtype=torch.float64, device=_device())
+        ssum = torch.empty(nbins, dtype=torch.float64, device=_device())
+        ws = self._workspace()
+        _lib.call('pk_bin_separation_modes', _lib.stream_handle(), _lib.i32(mattrs.meshsize), _lib.f32(mattrs.cellsize),
+                  _lib.ptr(self.d_edges), len(edges), self._step, _lib.ptr(nmodes), _lib.ptr(ssum), _lib.ptr(ws),
+                  ws.numel())
+        self.nmodes = nmodes.cpu().numpy()
+        with np.errstate(invalid='ignore', divide='ignore'):
+            self.xavg = ssum.cpu().numpy() / self.nmodes
+
+    def _workspace(self):
+        nbytes = _lib.c_size_t()
+        _lib.call('pk_bin_separation_workspace_size', _lib.i32(self.mattrs.meshsize), len(self._edges1d), 3,
+                  _lib.ctypes.byref(nbytes))
+        return _workspace(nbytes.value)
+
+    def _find_unique_edges(self, x0, xmin=0., xmax=np.inf):
+        """``_find_unique_edges`` (``mesh.py:2789-2811``): mid-points between unique |s|."""
+        sx, sy, sz = self.mattrs.rcoords(kind='separation', sparse=True)
+        x2 = ((sx * sx + sy * sy) + sz * sz).reshape(-1)
+        x2 = x2[(x2 >= xmin**2) & (x2 <= xmax**2)]
+        key = (x2.double() / (0.5 * float(x0))**2 + 0.5).to(torch.int64)
+        _, inverse = torch.unique(key, return_inverse=True)
+        first = torch.full((int(inverse.max()) + 1,), x2.numel(), dtype=torch.int64, device=x2.device)
+        first.scatter_reduce_(0, inverse, torch.arange(x2.numel(), device=x2.device), reduce='amin')
+        x = torch.sqrt(x2[first]).cpu().numpy().astype('f8')
+        tmp = (x[:-1] + x[1:]) / 2.
+        return np.concatenate([[tmp[0] - (x[1] - x[0])], tmp, [tmp[-1] + (x[-1] - x[-2])]])
+
+    @property
+    def nbins(self):
+        return len(self._edges1d) - 1
+
+    def _sums(self, value, ells, los=(0., 0., 1.)):
+        value = value.to(device=_device(), dtype=torch.float32).contiguous()
+        out = torch.empty(len(ells) * self.nbins, dtype=torch.float64, device=value.device)
+        ws = self._workspace()
+        _lib.call('pk_bin_separation_global', _lib.stream_handle(), _lib.ptr(value), _lib.i32(self.mattrs.meshsize),
+                  _lib.f32(self.mattrs.cellsize), _lib.f32(los), _lib.ptr(self.d_edges), len(self._edges1d),
+                  self._step, len(ells), _lib.i32(ells), _lib.ptr(out), _lib.ptr(ws), ws.numel())
+        return out.reshape(len(ells), self.nbins)
+
+    def __call__(self, mesh, ell=0, remove_zero=False):
+        """Per-bin mean of a real mesh (``mesh2.py:162-192``, configuration-space basis)."""
+        value = mesh.value if isinstance(mesh, BaseMeshField) else mesh
+        if not isinstance(value, torch.Tensor):
+            value = torch.as_tensor(np.asarray(value))
+        if remove_zero:
+            value = value.clone()
+            value.view(-1)[0] = 0.
+        return self._sums(value, (0,))[0].cpu().numpy() / self.nmodes
+
+
+def compute_mesh2_correlation(*meshes, bin=None, los='z'):
+    """Correlation-function multipoles from mesh(es) (``mesh2.py:377-504``), fixed line of sight.
+
+    A = c2r(|delta_k|^2) (or c2r(conj(delta1_k) delta2_k)); xi_ell = (2 ell + 1) <A L_ell(mu)>
+    per |s| bin (the s = 0 cell dropped for ell > 0); num_raw = xi_ell / V_cell.
+    """
+    meshes, fields = _format_meshes(*meshes)
+    mattrs = meshes[0].attrs
+    norm_value = np.float32(np.prod(mattrs.meshsize.astype('f4'))) / np.float32(np.prod(mattrs.cellsize))
+    los_name, vlos, swap = _los(los)
+    if vlos is None:
+        raise NotImplementedError('first-point / end-point correlation multipoles are not implemented on the GPU path')
+    ells = bin.ells
+    meshsize = mattrs.meshsize
+
+    def _c(mesh):
+        return mesh.value if isinstance(mesh, ComplexMeshField) else _r2c(mesh.value, meshsize)
+
+    c1 = _c(meshes[0])
+    if fields[1] == fields[0]:
+        prod = (c1.real * c1.real + c1.imag * c1.imag).to(torch.complex64)
+    else:
+        prod = torch.conj(c1) * _c(meshes[1])
+    A = _c2r(prod.contiguous(), meshsize)
+    del prod
+    raw = bin._sums(A, ells, los=vlos).cpu().numpy()
+    cellvol = float(np.prod(mattrs.cellsize.astype('f8')))
+    norm = np.full(bin.nbins, norm_value, dtype='f8')
+    poles = []
+    for i, ell in enumerate(ells):
+        num = raw[i] / bin.nmodes * (1. if ell == 0 else 2. * ell + 1.)
+        poles.append(Mesh2CorrelationPole(s=bin.xavg, s_edges=bin.edges, nmodes=bin.nmodes, num_raw=num / cellvol,
+                                          norm=norm, volume=cellvol * bin.nmodes, ell=ell,
+                                          attrs=dict(los=vlos)))
+    return Mesh2CorrelationPoles(poles)
 
 
 def _format_meshes(*meshes, fields=None):
@@ -317,9 +450,12 @@ def compute_mesh2_spectrum(*meshes, bin=None, los='z'):
 
 
 def compute_mesh2(*meshes, bin=None, los='z'):
+    """``compute_mesh2`` (``mesh2.py:225-250``): dispatch on the binning operator."""
     if isinstance(bin, BinMesh2SpectrumPoles):
         return compute_mesh2_spectrum(*meshes, bin=bin, los=los)
-    raise NotImplementedError('only BinMesh2SpectrumPoles is supported')
+    if isinstance(bin, BinMesh2CorrelationPoles):
+        return compute_mesh2_correlation(*meshes, bin=bin, los=los)
+    raise NotImplementedError('bin must be a BinMesh2SpectrumPoles or BinMesh2CorrelationPoles')
 
 
 # ---------------------------------------------------------------------- normalisation

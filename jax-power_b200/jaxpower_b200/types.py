@@ -11,7 +11,7 @@ normalisation that reproduces the reference's golden ``value().std()``),
 """
 import numpy as np
 
-__all__ = ['Mesh2SpectrumPole', 'Mesh2SpectrumPoles']
+__all__ = ['Mesh2SpectrumPole', 'Mesh2SpectrumPoles', 'Mesh2CorrelationPole', 'Mesh2CorrelationPoles']
 
 
 class Mesh2SpectrumPole:
@@ -77,7 +77,7 @@ class Mesh2SpectrumPoles:
             return self
         if np.ndim(ells) == 0:
             return self.poles[self.ells.index(int(ells))]
-        return Mesh2SpectrumPoles([self.poles[self.ells.index(int(e))] for e in ells])
+        return self.__class__([self.poles[self.ells.index(int(e))] for e in ells])
 
     def value(self):
         return np.concatenate([p.value() for p in self.poles])
@@ -88,7 +88,31 @@ class Mesh2SpectrumPoles:
         for i, p in enumerate(self.poles):
             kw = {k: (v[i] if isinstance(v, (list, tuple)) else v) for k, v in kwargs.items()}
             poles.append(p.clone(**kw))
-        return Mesh2SpectrumPoles(poles)
+        return self.__class__(poles)
 
     def __repr__(self):
         return 'Mesh2SpectrumPoles(ells={})'.format(self.ells)
+
+
+class Mesh2CorrelationPole(Mesh2SpectrumPole):
+    """Correlation-function multipole: ``s``, ``s_edges`` in place of ``k``, ``k_edges``."""
+
+    _fields = ('s', 's_edges', 'nmodes', 'num_raw', 'num_shotnoise', 'norm', 'volume')
+
+    def __init__(self, s, s_edges, nmodes, num_raw, num_shotnoise=None, norm=None, volume=None, ell=0,
+                 attrs=None):
+        super().__init__(s, s_edges, nmodes, num_raw, num_shotnoise=num_shotnoise, norm=norm, volume=volume,
+                         ell=ell, attrs=attrs)
+        self.s, self.s_edges = self.k, self.k_edges
+
+    def coords(self, name='s'):
+        return getattr(self, name)
+
+    def __repr__(self):
+        return 'Mesh2CorrelationPole(ell={}, nbins={})'.format(self.ell, self.s.size)
+
+
+class Mesh2CorrelationPoles(Mesh2SpectrumPoles):
+
+    def __repr__(self):
+        return 'Mesh2CorrelationPoles(ells={})'.format(self.ells)

@@ -260,3 +260,81 @@ def norm_geometry(geom, cellsize=10.):
         meshsize = meshsize + 1
         boxsize = (cell * meshsize.astype(dt)).astype(dt)
     return Geometry(meshsize, boxsize=boxsize, boxcenter=geom.boxcenter, dtype=dt, backend=geom.backend)
+
+
+def separation_coords(geom):
+    """``MeshAttrs.rcoords(kind='separation')`` (``mesh.py:392-394``): fftfreq(n) * cellsize * n."""
+    dt = geom.dtype
+    out = []
+    for axis in range(3):
+        n = int(geom.meshsize[axis])
+        sf = np.where(np.arange(n) < (n + 1) // 2, np.arange(n), np.arange(n) - n).astype(dt)
+        x = ((sf / dt.type(n)).astype(dt) * geom.cellsize[axis]).astype(dt) * dt.type(n)
+        shape = [1, 1, 1]
+        shape[axis] = n
+        out.append(x.astype(dt).reshape(shape))
+    return out
+
+
+class CorrelationBins:
+    """``BinMesh2CorrelationPoles(mattrs, edges={'step': step}, ells)`` restated
+    (``mesh2.py:124-192``, ``_make_edges2('real')`` ``mesh2.py:25-62``): |s| of the separation
+    grid binned by ``digitize``; unit weights."""
+
+    def __init__(self, geom, step=None, edges=None, ells=(0, 2, 4)):
+        dt = geom.dtype
+        self.geom = geom
+        self.ells = tuple(sorted((ells,) if np.ndim(ells) == 0 else ells))
+        if edges is None:
+            vec0 = geom.cellsize.min()
+            vecmax = dt.type(vec0 * dt.type(np.min(geom.meshsize))) / dt.type(2.)
+            edges = np.arange(0., float(vecmax), step)
+        self.edges = np.asarray(edges, dtype='f8')
+        sx, sy, sz = separation_coords(geom)
+        s2 = (((dt.type(0.) + sx * sx).astype(dt) + sy * sy).astype(dt) + sz * sz).astype(dt)
+        self.snorm = np.sqrt(s2).astype(dt)
+        self.ibin = np.searchsorted(self.edges.astype(dt), self.snorm.ravel(), side='right').reshape(self.snorm.shape)
+        nb = len(self.edges) + 1
+        self.nmodes = np.bincount(self.ibin.ravel(), minlength=nb)[1:-1].astype('f8')
+        ssum = np.bincount(self.ibin.ravel(), weights=self.snorm.ravel().astype('f8'), minlength=nb)[1:-1]
+        with np.errstate(invalid='ignore', divide='ignore'):
+            self.xavg = ssum / self.nmodes
+
+    @property
+    def nbins(self):
+        return len(self.edges) - 1
+
+    def __call__(self, value, remove_zero=False):
+        value = np.array(value, dtype='f8', copy=True)
+        if remove_zero:
+            value[0, 0, 0] = 0.
+        nb = len(self.edges) + 1
+        return np.bincount(self.ibin.ravel(), weights=value.ravel(), minlength=nb)[1:-1] / self.nmodes
+
+
+def compute_mesh2_correlation(mesh, bins, los='z', mesh2=None):
+    """Fixed line-of-sight branch of ``compute_mesh2_correlation`` (``mesh2.py:465-499``):
+    A = c2r(|delta|^2) (or c2r(conj(d1) d2)), xi_0 = bin(A), xi_ell = (2 ell + 1) bin(A L_ell(mu))
+    (s = 0 dropped), mu = s.los / |s| with |s|(0) = 1; num_raw = xi / V_cell."""
+    geom = bins.geom
+    dt = geom.dtype
+    d1 = _to_complex(geom, mesh)
+    if mesh2 is None:
+        prod = (d1.real**2 + d1.imag**2).astype(d1.dtype)
+    else:
+        prod = np.conj(d1) * _to_complex(geom, mesh2)
+    A = c2r(geom, prod)
+    vlos = {'x': (1., 0., 0.), 'y': (0., 1., 0.), 'z': (0., 0., 1.)}[los] if isinstance(los, str) else los
+    sx, sy, sz = separation_coords(geom)
+    s = bins.snorm.copy()
+    s[0, 0, 0] = 1.
+    mu = ((sx * dt.type(vlos[0]) + sy * dt.type(vlos[1])) + sz * dt.type(vlos[2])) / s
+    cellvol = float(np.prod(geom.cellsize.astype('f8')))
+    out = {}
+    for ell in bins.ells:
+        if ell == 0:
+            num = bins(A)
+        else:
+            num = (2 * ell + 1) * bins(A * legendre(ell, mu.astype(dt)), remove_zero=True)
+        out[ell] = num / cellvol
+    return {'num_raw': np.array([out[ell] for ell in bins.ells]), 'nmodes': bins.nmodes, 'xavg': bins.xavg}
