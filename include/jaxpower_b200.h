@@ -196,6 +196,17 @@ pk_status pk_bin_separation_global(void *stream, const float *value, const int32
                                    int nedges, float step, int nells, const int32_t *ells,
                                    double *d_out, void *workspace, size_t workspace_bytes);
 
+/* First-point correlation function (mesh2.py:423-451): carry += sum_j r_j Y_j(shat) over
+ * nterms real meshes r_j (r + j N_r), shat the unit separation vector of the grid
+ * fftfreq(n) * cellsize * n (0 at s = 0), real Y_lm as pk_ylm_premultiply. */
+pk_status pk_ylm_separation_accumulate(void *stream, const float *r, const int32_t meshsize[3],
+                                       const float cellsize[3], int nterms, const int32_t *term_ell,
+                                       const int32_t *term_m, float *carry);
+
+/* out_t = conj(f_t) * a for nterms complex meshes f_t (f + t n) of n complex64 values each
+ * (the conj(F) A0 products of the first-point estimators). */
+pk_status pk_conj_multiply(void *stream, const void *f, const void *a, int nterms, int64_t n, void *out);
+
 /* pk_bin_global_batch of the meshes that pk_interlace_compensate(_batch) would form
  * (for_c2r = 0, scale 1), without storing them: each mode is combined on the fly from
  * the nshifts interlaced, uncompensated R2C meshes (shifted: nbatch x nshifts Hermitian

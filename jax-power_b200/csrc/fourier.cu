@@ -347,6 +347,44 @@ __global__ void ylm_accumulate_kernel(Dims d, float c0, float c1, float c2, floa
   }
 }
 
+// carry(s) += sum_t r_t(s) Y_t(shat) on the real-space separation grid
+// s_d = fftfreq(n_d)[i] * cellsize_d * n_d (the first-point correlation function,
+// mesh2.py:436-446); shat = 0 at s = 0.
+__global__ void ylm_separation_accumulate_kernel(Dims d, float c0, float c1, float c2, YlmTerms terms,
+                                                 const float *__restrict__ r, float *__restrict__ carry) {
+  const int64_t total = d.nreal();
+  const int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  IndexWalker3 w(start, stride, d.n1, d.n2);
+  for (int64_t idx = start; idx < total; idx += stride, w.next()) {
+    const float x = kcoord(w.i, d.n0, c0, false);
+    const float y = kcoord(w.j, d.n1, c1, false);
+    const float z = kcoord(w.k, d.n2, c2, false);
+    const float xn = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z)));
+    float xh = 0.f, yh = 0.f, zh = 0.f;
+    if (xn != 0.f) {
+      xh = __fdiv_rn(x, xn);
+      yh = __fdiv_rn(y, xn);
+      zh = __fdiv_rn(z, xn);
+    }
+    float acc = carry[idx];
+    for (int t = 0; t < terms.n; ++t)
+      acc += r[(int64_t)t * total + idx] * ylm_eval(terms.ell[t], terms.m[t], xh, yh, zh);
+    carry[idx] = acc;
+  }
+}
+
+// out_t = conj(f_t) * a for nterms complex meshes f_t of n modes each.
+__global__ void conj_multiply_kernel(const float2 *__restrict__ f, const float2 *__restrict__ a, int nterms,
+                                     int64_t n, float2 *__restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float2 b = a[i];
+    for (int t = 0; t < nterms; ++t) {
+      const float2 v = f[(int64_t)t * n + i];
+      out[(int64_t)t * n + i] = make_float2(v.x * b.x + v.y * b.y, v.x * b.y - v.y * b.x);
+    }
+  }
+}
+
 extern "C" pk_status pk_interlace_adjoint(void *stream, const void *in, int from_real,
                                           int nshifts, const int32_t meshsize[3], int comp_order,
                                           int backend, void *out) {
@@ -392,6 +430,38 @@ extern "C" pk_status pk_ylm_accumulate(void *stream, const float *r, const int32
   }
   ylm_accumulate_kernel<<<grid_for(d.nreal(), 256), 256, 0, (cudaStream_t)stream>>>(
       d, cellsize[0], cellsize[1], cellsize[2], offset[0], offset[1], offset[2], t, r, rho_bar);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+extern "C" pk_status pk_ylm_separation_accumulate(void *stream, const float *r, const int32_t meshsize[3],
+                                                  const float cellsize[3], int nterms, const int32_t *term_ell,
+                                                  const int32_t *term_m, float *carry) {
+  PK_REQUIRE(r && carry && cellsize && term_ell && term_m, PK_ERR_INVALID, "null pointer");
+  Dims d;
+  PK_REQUIRE(make_dims(meshsize, &d), PK_ERR_INVALID, "invalid meshsize");
+  PK_REQUIRE(nterms >= 1 && nterms <= 32, PK_ERR_INVALID, "nterms must be in 1..32");
+  YlmTerms t;
+  t.n = nterms;
+  for (int j = 0; j < nterms; ++j) {
+    PK_REQUIRE(term_ell[j] >= 0 && term_ell[j] <= YLM_LMAX && term_m[j] >= -term_ell[j] &&
+                   term_m[j] <= term_ell[j],
+               PK_ERR_INVALID, "invalid (ell, m) = (%d, %d)", term_ell[j], term_m[j]);
+    t.ell[j] = term_ell[j];
+    t.m[j] = term_m[j];
+  }
+  ylm_separation_accumulate_kernel<<<grid_for(d.nreal(), 256), 256, 0, (cudaStream_t)stream>>>(
+      d, cellsize[0], cellsize[1], cellsize[2], t, r, carry);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+extern "C" pk_status pk_conj_multiply(void *stream, const void *f, const void *a, int nterms, int64_t n,
+                                      void *out) {
+  PK_REQUIRE(f && a && out && nterms >= 1 && n >= 0, PK_ERR_INVALID, "invalid arguments");
+  if (n == 0) return PK_OK;
+  conj_multiply_kernel<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>((const float2 *)f, (const float2 *)a,
+                                                                            nterms, n, (float2 *)out);
   PK_LAUNCH_CHECK();
   return PK_OK;
 }

@@ -234,39 +234,87 @@ class BinMesh2CorrelationPoles:
 
 
 def compute_mesh2_correlation(*meshes, bin=None, los='z'):
-    """Correlation-function multipoles from mesh(es) (``mesh2.py:377-504``), fixed line of sight.
+    """Correlation-function multipoles from mesh(es) (``mesh2.py:377-504``).
 
-    A = c2r(|delta_k|^2) (or c2r(conj(delta1_k) delta2_k)); xi_ell = (2 ell + 1) <A L_ell(mu)>
-    per |s| bin (the s = 0 cell dropped for ell > 0); num_raw = xi_ell / V_cell.
+    Fixed line of sight: A = c2r(|delta_k|^2) (or c2r(conj(delta1_k) delta2_k));
+    xi_ell = (2 ell + 1) <A L_ell(mu)> per |s| bin (the s = 0 cell dropped for ell > 0).
+    First point: xi_0 = <c2r(|A0|^2)>, xi_ell = 4 pi <sum_m c2r(conj(r2c(rho Y_lm(xhat))) A0)
+    Y_lm(shat)> (s = 0 dropped).  num_raw = xi_ell / V_cell.
     """
     meshes, fields = _format_meshes(*meshes)
     mattrs = meshes[0].attrs
     norm_value = np.float32(np.prod(mattrs.meshsize.astype('f4'))) / np.float32(np.prod(mattrs.cellsize))
     los_name, vlos, swap = _los(los)
-    if vlos is None:
-        raise NotImplementedError('first-point / end-point correlation multipoles are not implemented on the GPU path')
     ells = bin.ells
     meshsize = mattrs.meshsize
+    auto = fields[1] == fields[0]
 
     def _c(mesh):
         return mesh.value if isinstance(mesh, ComplexMeshField) else _r2c(mesh.value, meshsize)
 
-    c1 = _c(meshes[0])
-    if fields[1] == fields[0]:
-        prod = (c1.real * c1.real + c1.imag * c1.imag).to(torch.complex64)
+    def _r(mesh):
+        return mesh.value if isinstance(mesh, RealMeshField) else _c2r(mesh.value, meshsize)
+
+    if vlos is None:  # first point (end point: the meshes swapped), mesh2.py:414-463
+        if swap and not auto:
+            meshes = meshes[::-1]
+        A0 = _c(meshes[0] if auto else meshes[1]).contiguous()
+        sums = {}
+        if 0 in ells:
+            if auto:
+                prod = (A0.real * A0.real + A0.imag * A0.imag).to(torch.complex64)
+            else:
+                prod = torch.conj(_c(meshes[0])) * A0
+            sums[0] = bin._sums(_c2r(prod.contiguous(), meshsize), (0,))[0]
+            del prod
+        nonzero = [ell for ell in ells if ell != 0]
+        if nonzero:
+            rho = _r(meshes[0]).contiguous()
+            offset = (mattrs.boxcenter - (mattrs.boxsize / np.float32(2.)).astype('f4')).astype('f4')
+            stream = _lib.stream_handle()
+            for ell in nonzero:
+                terms = [(ell, m) for m in range(-ell, ell + 1)]
+                carry = torch.zeros_like(rho)
+                batch = _term_batch(mattrs, len(terms))
+                for start in range(0, len(terms), batch):
+                    chunk = terms[start:start + batch]
+                    nt = len(chunk)
+                    t_ell, t_m = [t[0] for t in chunk], [t[1] for t in chunk]
+                    real = torch.empty((nt,) + tuple(int(n) for n in meshsize), dtype=torch.float32, device=rho.device)
+                    _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rho), _lib.i32(meshsize),
+                              _lib.f32(mattrs.cellsize), _lib.f32(offset), nt, _lib.i32(t_ell), _lib.i32(t_m),
+                              _lib.ptr(real))
+                    F = _r2c(real, meshsize)
+                    _lib.call('pk_conj_multiply', stream, _lib.ptr(F), _lib.ptr(A0), nt, A0.numel(), _lib.ptr(F))
+                    real = _c2r(F, meshsize, destroy_input=True)
+                    del F
+                    _lib.call('pk_ylm_separation_accumulate', stream, _lib.ptr(real), _lib.i32(meshsize),
+                              _lib.f32(mattrs.cellsize), nt, _lib.i32(t_ell), _lib.i32(t_m), _lib.ptr(carry))
+                    del real
+                carry.view(-1)[0] = 0.  # remove_zero
+                sums[ell] = 4. * np.pi * bin._sums(carry, (0,))[0]
+                del carry
+        raw = torch.stack([sums[ell] for ell in ells]).cpu().numpy()
+        factors = [1.] * len(ells)
+        attrs = dict(los=los_name)
     else:
-        prod = torch.conj(c1) * _c(meshes[1])
-    A = _c2r(prod.contiguous(), meshsize)
-    del prod
-    raw = bin._sums(A, ells, los=vlos).cpu().numpy()
+        c1 = _c(meshes[0])
+        if auto:
+            prod = (c1.real * c1.real + c1.imag * c1.imag).to(torch.complex64)
+        else:
+            prod = torch.conj(c1) * _c(meshes[1])
+        A = _c2r(prod.contiguous(), meshsize)
+        del prod
+        raw = bin._sums(A, ells, los=vlos).cpu().numpy()
+        factors = [1. if ell == 0 else 2. * ell + 1. for ell in ells]
+        attrs = dict(los=vlos)
     cellvol = float(np.prod(mattrs.cellsize.astype('f8')))
     norm = np.full(bin.nbins, norm_value, dtype='f8')
     poles = []
     for i, ell in enumerate(ells):
-        num = raw[i] / bin.nmodes * (1. if ell == 0 else 2. * ell + 1.)
+        num = raw[i] / bin.nmodes * factors[i]
         poles.append(Mesh2CorrelationPole(s=bin.xavg, s_edges=bin.edges, nmodes=bin.nmodes, num_raw=num / cellvol,
-                                          norm=norm, volume=cellvol * bin.nmodes, ell=ell,
-                                          attrs=dict(los=vlos)))
+                                          norm=norm, volume=cellvol * bin.nmodes, ell=ell, attrs=attrs))
     return Mesh2CorrelationPoles(poles)
 
 

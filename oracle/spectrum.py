@@ -338,3 +338,30 @@ def compute_mesh2_correlation(mesh, bins, los='z', mesh2=None):
             num = (2 * ell + 1) * bins(A * legendre(ell, mu.astype(dt)), remove_zero=True)
         out[ell] = num / cellvol
     return {'num_raw': np.array([out[ell] for ell in bins.ells]), 'nmodes': bins.nmodes, 'xavg': bins.xavg}
+
+
+def compute_mesh2_correlation_firstpoint(mesh, bins, mesh2=None, swap=False):
+    """First-point branch of ``compute_mesh2_correlation`` (``mesh2.py:414-463``):
+    xi_0 = bin(c2r(|A0|^2)), xi_ell = 4 pi bin(sum_m c2r(conj(r2c(rho Y_lm(xhat))) A0) Y_lm(shat))
+    with the s = 0 cell dropped; num_raw = xi / V_cell."""
+    geom = bins.geom
+    dt = geom.dtype
+    m1, m2 = (mesh2, mesh) if (swap and mesh2 is not None) else (mesh, mesh2)
+    A0 = _to_complex(geom, m1 if m2 is None else m2)
+    rho = _to_real(geom, m1)
+    xvec = rcoords(geom)
+    svec = separation_coords(geom)
+    cellvol = float(np.prod(geom.cellsize.astype('f8')))
+    out = []
+    for ell in bins.ells:
+        if ell == 0:
+            prod = (A0.real**2 + A0.imag**2).astype(A0.dtype) if m2 is None else np.conj(_to_complex(geom, m1)) * A0
+            out.append(bins(c2r(geom, prod)) / cellvol)
+            continue
+        carry = np.zeros(geom.rshape, dtype=dt)
+        for m in range(-ell, ell + 1):
+            Y = get_ylm(ell, m)
+            F = r2c(geom, (rho * Y(*xvec)).astype(dt))
+            carry = (carry + c2r(geom, np.conj(F) * A0) * Y(*svec)).astype(dt)
+        out.append(4. * np.pi * bins(carry, remove_zero=True) / cellvol)
+    return {'num_raw': np.array(out), 'nmodes': bins.nmodes, 'xavg': bins.xavg}

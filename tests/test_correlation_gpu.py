@@ -60,3 +60,29 @@ def test_correlation_matches_oracle(los, cross, meshsize):
         assert np.allclose(pole.s, ob.xavg, rtol=1e-6, equal_nan=True)
         assert np.allclose(pole.num_raw, ref['num_raw'][i], rtol=0, atol=1e-5 * scale), ell
     assert np.isfinite(got.get(0).value()).all()
+
+
+@pytest.mark.parametrize('los,cross', [('firstpoint', False), ('firstpoint', True), ('endpoint', True)])
+def test_firstpoint_correlation_matches_oracle(los, cross):
+    import jaxpower_b200 as jp
+    from oracle.spectrum import compute_mesh2_correlation_firstpoint as ofp
+    meshsize, boxsize, boxcenter = (24, 28, 20), np.array([600., 700., 500.]), np.array([800., -200., 900.])
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=boxcenter)
+    geom = Geometry(meshsize, boxsize, boxcenter)
+    pos1 = _catalog(20000, boxsize, 5) + boxcenter.astype('f4')
+    pos2 = _catalog(15000, boxsize, 6) + boxcenter.astype('f4')
+    m1 = jp.ParticleField(pos1, attrs=attrs).paint(resampler='cic', interlacing=2, compensate=True, out='real')
+    o1 = opaint.paint(geom, pos1, None, 'cic', 2, True, 'real')
+    b = jp.BinMesh2CorrelationPoles(attrs, edges={'step': 30.}, ells=(0, 2, 4))
+    ob = CorrelationBins(geom, step=30., ells=(0, 2, 4))
+    if cross:
+        m2 = jp.ParticleField(pos2, attrs=attrs).paint(resampler='tsc', out='complex')
+        o2 = opaint.paint(geom, pos2, None, 'tsc', 0, False, 'complex')
+        got = jp.compute_mesh2_correlation(m1, m2, bin=b, los=los)
+        ref = ofp(o1, ob, mesh2=o2, swap=los == 'endpoint')
+    else:
+        got = jp.compute_mesh2_correlation(m1, bin=b, los=los)
+        ref = ofp(o1, ob)
+    scale = np.abs(ref['num_raw'][0]).max()
+    for i, ell in enumerate((0, 2, 4)):
+        assert np.allclose(got.get(ell).num_raw, ref['num_raw'][i], rtol=0, atol=2e-5 * scale), ell
