@@ -15,11 +15,12 @@
 // reproducible run to run.
 #include <math.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "common.cuh"
 #include "fourier_common.cuh"
-#include "ylm_table.cuh"
+#include "ylm_block.cuh"
 
 namespace pk {
 
@@ -467,13 +468,163 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_chunks_kernel(BinGeom g, Op o
   bin_smem_flush(s, hist_len, nwarps, partials);
 }
 
+// ------------------------------------------- first point, whole-ell term blocks
+// The first-point pass (mesh2.py:293-344) when the terms are whole ells (mask MASK, every
+// m of each ell in order): the F_lm of a mode are loaded together, Y_lm(khat) are
+// compile-time polynomials at fixed register indices, and the modes are walked as one
+// flat sequence of 32-mode chunks (a warp owns a contiguous range of chunks; a chunk may
+// span rows, so bin keys carry the row's low 5 bits and equal bins of different rows stay
+// separate runs -- a chunk spans at most 32 rows -- and the run tails of different rows,
+// which may share a bin, add into the histogram one row after the other).  Values: 0 = the
+// ell = 0 product, then one per ell of MASK, ascending.  Per mode the arithmetic is
+// FirstPointOp's, term for term.
+
+// sr + i si = sum_m F_{ELL m} Y_{ELL m}, terms T .. T + 2 ELL, in m order.
+template <int ELL, int M, int T, int NT>
+__device__ __forceinline__ void fp_ylm_sum(const float2 (&F)[NT], float x, float y, float z, float &sr,
+                                           float &si) {
+  const float yv = ylm_eval(ELL, M, x, y, z);
+  sr += F[T].x * yv;
+  si += F[T].y * yv;
+  if constexpr (M < ELL) fp_ylm_sum<ELL, M + 1, T + 1>(F, x, y, z, sr, si);
+}
+
+template <int MASK, int ELL, int T, int V, int NT, int NV>
+__device__ __forceinline__ void fp_block_values(const float2 (&F)[NT], float x, float y, float z, float2 A,
+                                                bool zero, float w, float (&v)[NV]) {
+  if constexpr (ELL <= YLM_LMAX) {
+    if constexpr ((MASK >> ELL) & 1) {
+      float sr = 0.f, si = 0.f;
+      fp_ylm_sum<ELL, -ELL, T>(F, x, y, z, sr, si);
+      const float re = sr * A.x + si * A.y;  // conj(S) * A0
+      const float im = sr * A.y - si * A.x;
+      v[V] = zero ? 0.f : ((ELL & 1) ? im : re) * w;
+      fp_block_values<MASK, ELL + 1, T + 2 * ELL + 1, V + 1>(F, x, y, z, A, zero, w, v);
+    } else {
+      fp_block_values<MASK, ELL + 1, T, V>(F, x, y, z, A, zero, w, v);
+    }
+  }
+}
+
+template <int MASK, bool CROSS>
+__global__ void __launch_bounds__(BIN_THREADS) bin_firstpoint_kernel(
+    BinGeom g, const float2 *__restrict__ a0, const float2 *__restrict__ b0, const float2 *__restrict__ f,
+    int64_t fstride, const float *__restrict__ edges, int nwarps_hist, int tab, int64_t chunks_per_warp,
+    double *__restrict__ partials) {
+  constexpr int NT = ylm_mask_terms(MASK);
+  constexpr int NV = ylm_mask_ells(MASK) + 1;
+  const int nbins = g.nedges - 1;
+  const int hist_len = nbins * NV;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  const BinSmem s = bin_smem_init(g, edges, NV, nwarps_hist, tab);
+  double *my = s.hist + (size_t)warp * hist_len;
+  const float e0 = edges[0];
+  const float inv_step = g.step > 0.f ? 1.f / g.step : 0.f;
+  const int nz = g.d.nz, n1 = g.d.n1;
+  const int64_t total = g.d.ncomplex();
+  const int64_t nchunks = (total + 31) / 32;
+  const int64_t c0 = ((int64_t)blockIdx.x * nwarps + warp) * chunks_per_warp;
+  const int64_t c1 = min(nchunks, c0 + chunks_per_warp);
+  if (c0 < c1) {
+    int64_t m = c0 * 32 + lane;
+    int z = (int)(m % nz);
+    int j = (int)((m / nz) % n1);
+    int i = (int)(m / ((int64_t)nz * n1));
+    int ic = -1, jc = -1;
+    float kx = 0.f, ky = 0.f, kxy = 0.f;
+    for (int64_t c = c0; c < c1; ++c, m += 32) {
+      const bool valid = m < total;
+      float v[NV];
+      int key = 0x7fffffff, bin = 0;
+      if (valid) {
+        if (i != ic || j != jc) {
+          kx = kcoord(i, g.d.n0, g.kfun[0], false);
+          ky = kcoord(j, n1, g.kfun[1], false);
+          kxy = __fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky));
+          ic = i;
+          jc = j;
+        }
+        float kz, kz2;
+        if (tab) {
+          kz = s.kz[z];
+          kz2 = s.kz2[z];
+        } else {
+          kz = kz_coord(g, z);
+          kz2 = __fmul_rn(kz, kz);
+        }
+        const float k2 = __fadd_rn(kxy, kz2);
+        bin = bin_from_k2(s.thr, g.nedges, e0, inv_step, k2);
+        key = bin | ((int)((i * n1 + j) & 31) << 16);
+        float2 F[NT];
+#pragma unroll
+        for (int t = 0; t < NT; ++t) F[t] = __ldcs(f + (int64_t)t * fstride + m);
+        const float2 A = a0[m];
+        const float w = mode_weight(g, z);
+        if (CROSS) {
+          const float2 B = b0[m];
+          v[0] = (B.x * A.x + B.y * A.y) * w;
+        } else {
+          v[0] = (A.x * A.x + A.y * A.y) * w;
+        }
+        const bool zero = (i == 0 && j == 0 && z == 0);
+        const float rn = k2 > 0.f ? rsqrtf(k2) : 0.f;  // khat = k / |k|, 0 at k = 0
+        fp_block_values<MASK, 0, 0, 1>(F, kx * rn, ky * rn, kz * rn, A, zero, w, v);
+      } else {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) v[q] = 0.f;
+      }
+      const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+      if (!__all_sync(0xffffffffu, lane == 0 || prev != key)) {
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const bool ok = __shfl_up_sync(0xffffffffu, key, d) == key && lane >= d;
+#pragma unroll
+          for (int q = 0; q < NV; ++q) {
+            const float t = __shfl_up_sync(0xffffffffu, v[q], d);
+            if (ok) v[q] += t;
+          }
+        }
+      }
+      const int next = __shfl_down_sync(0xffffffffu, key, 1);
+      const bool tail = valid && (lane == 31 || next != key) && bin >= 1 && bin <= nbins;
+      // a bin has one run tail per row: the rows of the chunk write in turn
+      const int row = i * n1 + j;
+      const int roff = row - __shfl_sync(0xffffffffu, row, 0);
+      const int nrow = __reduce_max_sync(0xffffffffu, valid ? roff : 0);
+      for (int p = 0; p <= nrow; ++p) {
+        if (tail && roff == p) {
+#pragma unroll
+          for (int q = 0; q < NV; ++q) my[(size_t)(bin - 1) * NV + q] += (double)v[q];
+        }
+        __syncwarp();
+      }
+      z += 32;
+      while (z >= nz) {
+        z -= nz;
+        if (++j == n1) {
+          j = 0;
+          ++i;
+        }
+      }
+    }
+  }
+  bin_smem_flush(s, hist_len, nwarps, partials);
+}
+
+// Output row of each value (n = 0: value c goes to row c); a negative row drops the value.
+struct RowMap {
+  int n;
+  int row[MAX_ELLS + 1];
+};
+
 // out[e] (+)= sum over CTAs, transposed to [value][bin].  Deterministic two-level sum:
 // 8 threads per entry each add a fixed contiguous range of CTA rows (4 independent loads
 // in flight), then the 8 partials are added in a fixed order.
 constexpr int FIN_ENTRIES = 32, FIN_SPLIT = 8;
 __global__ void __launch_bounds__(FIN_ENTRIES * FIN_SPLIT) bin_finalize_kernel(
     const double *__restrict__ partials, int nblocks, int hist_len, int nv, int nbins,
-    int accumulate, double *__restrict__ out0, double *__restrict__ out1) {
+    int accumulate, double *__restrict__ out0, double *__restrict__ out1, RowMap map) {
   __shared__ double part[FIN_SPLIT][FIN_ENTRIES];
   partials += (size_t)blockIdx.y * nblocks * hist_len;  // batch of histograms along y
   out0 += (size_t)blockIdx.y * hist_len;
@@ -498,18 +649,20 @@ __global__ void __launch_bounds__(FIN_ENTRIES * FIN_SPLIT) bin_finalize_kernel(
     double acc = 0.;
     for (int k = 0; k < FIN_SPLIT; ++k) acc += part[k][le];
     const int bin = e / nv, c = e % nv;
+    const int r = map.n ? map.row[c] : c;
+    if (r < 0) return;
     double *dst = (c == 1 && out1) ? out1 : out0;
-    const int64_t o = (c == 1 && out1) ? bin : (int64_t)c * nbins + bin;
+    const int64_t o = (c == 1 && out1) ? bin : (int64_t)r * nbins + bin;
     dst[o] = accumulate ? dst[o] + acc : acc;
   }
 }
 
 static void launch_finalize(cudaStream_t s, const double *partials, int nblocks, int hist_len,
                             int nv, int nbins, int accumulate, double *out0, double *out1,
-                            int nbatch = 1) {
+                            int nbatch = 1, RowMap map = RowMap{}) {
   const dim3 grid((hist_len + FIN_ENTRIES - 1) / FIN_ENTRIES, nbatch);
   bin_finalize_kernel<<<grid, FIN_ENTRIES * FIN_SPLIT, 0, s>>>(partials, nblocks, hist_len, nv, nbins,
-                                                               accumulate, out0, out1);
+                                                               accumulate, out0, out1, map);
 }
 
 struct BinLaunch {
@@ -1130,6 +1283,51 @@ extern "C" pk_status pk_bin_separation_global(void *stream, const float *value, 
   return PK_ERR_INVALID;
 }
 
+template <int MASK, bool CROSS>
+static pk_status launch_firstpoint_block(cudaStream_t s, const BinGeom &g, const float2 *a0, const float2 *b0,
+                                         const float2 *f, const float *edges, const RowMap &map, double *out,
+                                         void *workspace, size_t workspace_bytes) {
+  constexpr int NV = ylm_mask_ells(MASK) + 1;
+  BinLaunch L;
+  PK_REQUIRE(plan_bins(g.d, g.nedges, NV, &L), PK_ERR_RANGE,
+             "too many bins x values (%d x %d) for the shared-memory histograms", g.nedges - 1, NV);
+  auto kernel = bin_firstpoint_kernel<MASK, CROSS>;
+  PK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
+  int per_sm = 0;
+  PK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, L.nwarps * 32, L.smem));
+  if (per_sm < 1) per_sm = 1;
+  // one wave of resident CTAs, the chunks split evenly over their warps
+  const int64_t nchunks = (g.d.ncomplex() + 31) / 32;
+  int64_t blocks = std::min<int64_t>(L.blocks, (int64_t)per_sm * sm_count());
+  const int64_t cpw = (nchunks + blocks * L.nwarps - 1) / (blocks * L.nwarps);
+  blocks = ((nchunks + cpw - 1) / cpw + L.nwarps - 1) / L.nwarps;
+  const int hist_len = (g.nedges - 1) * NV;
+  const size_t need = (size_t)blocks * hist_len * sizeof(double);
+  PK_REQUIRE(workspace && workspace_bytes >= need, PK_ERR_WORKSPACE,
+             "binning workspace too small: need %zu bytes, got %zu", need, workspace_bytes);
+  double *partials = static_cast<double *>(workspace);
+  kernel<<<(int)blocks, L.nwarps * 32, L.smem, s>>>(g, a0, b0, f, g.d.ncomplex(), edges, L.nwarps, L.tab, cpw,
+                                                    partials);
+  PK_LAUNCH_CHECK();
+  launch_finalize(s, partials, (int)blocks, hist_len, NV, g.nedges - 1, 1, out, nullptr, 1, map);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+static pk_status dispatch_firstpoint_block(int mask, cudaStream_t s, const BinGeom &g, const float2 *a0,
+                                           const float2 *b0, const float2 *f, const float *edges,
+                                           const RowMap &map, double *out, void *workspace,
+                                           size_t workspace_bytes) {
+#define PK_FP_BLOCK_CASE(M)                                                                            \
+  if (mask == (M))                                                                                     \
+    return b0 ? launch_firstpoint_block<M, true>(s, g, a0, b0, f, edges, map, out, workspace, workspace_bytes) \
+              : launch_firstpoint_block<M, false>(s, g, a0, b0, f, edges, map, out, workspace, workspace_bytes);
+  PK_YLM_MASKS(PK_FP_BLOCK_CASE)
+#undef PK_FP_BLOCK_CASE
+  set_error("no first-point kernel for term mask 0x%x", mask);
+  return PK_ERR_INVALID;
+}
+
 extern "C" pk_status pk_bin_firstpoint(void *stream, const void *a0, const void *b0,
                                        const void *f, int nterms, const int32_t *term_ell,
                                        const int32_t *term_m, const int32_t meshsize[3],
@@ -1149,6 +1347,28 @@ extern "C" pk_status pk_bin_firstpoint(void *stream, const void *a0, const void 
     PK_REQUIRE(term_ell[t] >= 0 && term_ell[t] <= YLM_LMAX && term_m[t] >= -term_ell[t] &&
                    term_m[t] <= term_ell[t],
                PK_ERR_INVALID, "invalid (ell, m)");
+  // whole ells (every m, in order) and distinct output ells: the compiled per-mask kernel
+  const int mask = ylm_terms_mask(nterms, term_ell, term_m);
+  bool distinct = true;
+  for (int l = 0; l < nells; ++l)
+    for (int q = 0; q < l; ++q) distinct &= ells[l] != ells[q];
+  if (nterms > 0 && mask && ylm_mask_compiled(mask) && distinct) {
+    RowMap map{};
+    map.n = 1;
+    auto row_of = [&](int ell) {
+      for (int l = 0; l < nells; ++l)
+        if (ells[l] == ell) return l;
+      return -1;
+    };
+    map.row[0] = include_ell0 ? row_of(0) : -1;
+    int q = 1;
+    for (int ell = 1; ell <= YLM_LMAX; ++ell)
+      if ((mask >> ell) & 1) map.row[q++] = row_of(ell);
+    cudaStream_t cs = (cudaStream_t)stream;
+    if (!accumulate) PK_CUDA(cudaMemsetAsync(d_out, 0, (size_t)nells * (nedges - 1) * sizeof(double), cs));
+    return dispatch_firstpoint_block(mask, cs, g, (const float2 *)a0, (const float2 *)b0, (const float2 *)f,
+                                     d_edges, map, d_out, workspace, workspace_bytes);
+  }
   const int64_t stride = g.d.ncomplex();
   auto fill = [&](auto &op) {
     op.a0 = (const float2 *)a0;
@@ -1405,6 +1625,114 @@ __global__ void firstpoint_adjoint_kernel(AdjGeom a, FPAdj t, const float *__res
   }
 }
 
+// firstpoint_adjoint_kernel for whole-ell term blocks (mask MASK): the same per-mode
+// arithmetic with every term at a fixed register index and Y_lm as compile-time polynomials.
+struct FPAdjRows {
+  int row[YLM_LMAX + 1];  // row of each ell of the mask in ells (coef rows)
+};
+
+template <int ELL, int M, int T, int NT>
+__device__ __forceinline__ void fp_adj_terms(float G, float x, float y, float z, float2 A,
+                                             const float2 *__restrict__ f, int64_t stride, int64_t idx,
+                                             float2 &acc, float2 (&gf)[NT]) {
+  const float yv = ylm_eval(ELL, M, x, y, z);
+  const float2 F = f[(int64_t)T * stride + idx];
+  acc.x += G * yv * F.x;  // d/dA0 of G Re(conj(S) A0) = G S
+  acc.y += G * yv * F.y;
+  gf[T] = make_float2(G * yv * A.x, G * yv * A.y);  // d/dF of G Re(S conj(A0)) = G Y A0
+  if constexpr (M < ELL) fp_adj_terms<ELL, M + 1, T + 1>(G, x, y, z, A, f, stride, idx, acc, gf);
+}
+
+template <int MASK, int ELL, int T, int NT>
+__device__ __forceinline__ void fp_adj_ells(const FPAdjRows &r, const float *__restrict__ coef, int nbins, int b,
+                                            float w, float x, float y, float z, float2 A,
+                                            const float2 *__restrict__ f, int64_t stride, int64_t idx, float2 &acc,
+                                            float2 (&gf)[NT]) {
+  if constexpr (ELL <= YLM_LMAX) {
+    if constexpr ((MASK >> ELL) & 1) {
+      const float G = w * coef[(size_t)r.row[ELL] * nbins + (b - 1)];
+      fp_adj_terms<ELL, -ELL, T>(G, x, y, z, A, f, stride, idx, acc, gf);
+      fp_adj_ells<MASK, ELL + 1, T + 2 * ELL + 1>(r, coef, nbins, b, w, x, y, z, A, f, stride, idx, acc, gf);
+    } else {
+      fp_adj_ells<MASK, ELL + 1, T>(r, coef, nbins, b, w, x, y, z, A, f, stride, idx, acc, gf);
+    }
+  }
+}
+
+template <int MASK, int NT>
+__device__ __forceinline__ void fp_adj_block_mode(const AdjGeom &a, const FPAdjRows &r, const float *thr,
+                                                  const float *coef, const float2 *__restrict__ a0,
+                                                  const float2 *__restrict__ f, int i, int j, int z, float2 &ga0,
+                                                  float2 (&gf)[NT]) {
+  const BinGeom &g = a.g;
+  const float kx = kcoord(i, g.d.n0, g.kfun[0], false);
+  const float ky = kcoord(j, g.d.n1, g.kfun[1], false);
+  const float kz = kz_coord(g, z);
+  const float k2 = __fadd_rn(__fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky)), __fmul_rn(kz, kz));
+  const int b = adj_bin(a, thr, k2);
+  const int64_t idx = ((int64_t)i * g.d.n1 + j) * g.d.nz + z;
+  ga0 = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int q = 0; q < NT; ++q) gf[q] = make_float2(0.f, 0.f);
+  if (b < 1 || b > a.nbins) return;
+  const bool zero = (i == 0 && j == 0 && z == 0);
+  const float w = mode_weight(g, z);
+  const float rn = k2 > 0.f ? rsqrtf(k2) : 0.f;
+  const float2 A = a0[idx];
+  float2 acc = make_float2(0.f, 0.f);
+  for (int l = 0; l < a.nells; ++l)
+    if (a.ells[l] == 0) {  // ell = 0: |A0|^2 -> 2 G0 A0
+      const float G0 = w * coef[(size_t)l * a.nbins + (b - 1)];
+      acc.x += 2.f * G0 * A.x;
+      acc.y += 2.f * G0 * A.y;
+    }
+  if (!zero)
+    fp_adj_ells<MASK, 0, 0>(r, coef, a.nbins, b, w, kx * rn, ky * rn, kz * rn, A, f, g.d.ncomplex(), idx, acc, gf);
+  ga0 = acc;
+}
+
+template <int MASK>
+__global__ void __launch_bounds__(256) firstpoint_adjoint_block_kernel(
+    AdjGeom a, FPAdjRows r, const float *__restrict__ thr, const float *__restrict__ coef,
+    const float2 *__restrict__ a0, const float2 *__restrict__ f, float2 *__restrict__ out_a0, int accumulate_a0,
+    float2 *__restrict__ out_f) {
+  constexpr int NT = ylm_mask_terms(MASK);
+  const BinGeom &g = a.g;
+  const int64_t total = g.d.ncomplex();
+  const bool even = (g.d.n2 % 2) == 0;
+  const int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  IndexWalker3 w(start, stride, g.d.n1, g.d.nz);
+  for (int64_t idx = start; idx < total; idx += stride, w.next()) {
+    const int i = w.i, j = w.j, z = w.k;
+    float2 ga0, gf[NT];
+    fp_adj_block_mode<MASK>(a, r, thr, coef, a0, f, i, j, z, ga0, gf);
+    if (a.for_c2r) {
+      if (z == 0 || (even && z == g.d.nz - 1)) {
+        float2 ga0m, gfm[NT];
+        fp_adj_block_mode<MASK>(a, r, thr, coef, a0, f, (g.d.n0 - i) % g.d.n0, (g.d.n1 - j) % g.d.n1, z, ga0m,
+                                gfm);
+        ga0 = make_float2(0.5f * (ga0.x + ga0m.x), 0.5f * (ga0.y - ga0m.y));
+#pragma unroll
+        for (int q = 0; q < NT; ++q) gf[q] = make_float2(0.5f * (gf[q].x + gfm[q].x), 0.5f * (gf[q].y - gfm[q].y));
+      } else {
+        ga0 = make_float2(0.5f * ga0.x, 0.5f * ga0.y);
+#pragma unroll
+        for (int q = 0; q < NT; ++q) gf[q] = make_float2(0.5f * gf[q].x, 0.5f * gf[q].y);
+      }
+    }
+    if (out_a0) {
+      if (accumulate_a0) {
+        const float2 o = out_a0[idx];
+        out_a0[idx] = make_float2(o.x + ga0.x, o.y + ga0.y);
+      } else {
+        out_a0[idx] = ga0;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NT; ++q) __stcs(out_f + (int64_t)q * total + idx, gf[q]);
+  }
+}
+
 static pk_status make_adj(const int32_t meshsize[3], const float kfun[3], int nedges, float step,
                           int backend, int nells, const int32_t *ells, const float *d_edges,
                           int for_c2r, AdjGeom *a) {
@@ -1497,6 +1825,21 @@ extern "C" pk_status pk_bin_firstpoint_adjoint(void *stream, const void *a0, con
   PK_LAUNCH_CHECK();
   const int64_t total = a.g.d.ncomplex();
   const int64_t want = (total + 255) / 256, cap = 32LL * sm_count();
+  const int mask = ylm_terms_mask(nterms, term_ell, term_m);
+  if (nterms > 0 && mask && ylm_mask_compiled(mask)) {
+    FPAdjRows r{};
+    for (int q = 0; q < nterms; ++q) r.row[term_ell[q]] = t.term_l[q];
+#define PK_FP_ADJ_CASE(M)                                                                                \
+  if (mask == (M)) {                                                                                     \
+    firstpoint_adjoint_block_kernel<M><<<(int)(want < cap ? want : cap), 256, 0, s>>>(                   \
+        a, r, thr, d_coef, (const float2 *)a0, (const float2 *)f, (float2 *)out_a0, accumulate_a0,       \
+        (float2 *)out_f);                                                                                \
+    PK_LAUNCH_CHECK();                                                                                   \
+    return PK_OK;                                                                                        \
+  }
+    PK_YLM_MASKS(PK_FP_ADJ_CASE)
+#undef PK_FP_ADJ_CASE
+  }
   firstpoint_adjoint_kernel<<<(int)(want < cap ? want : cap), 256, 0, s>>>(
       a, t, thr, d_coef, (const float2 *)a0, (const float2 *)f, (float2 *)out_a0, accumulate_a0,
       (float2 *)out_f);

@@ -5,7 +5,7 @@
 
 #include "common.cuh"
 #include "fourier_common.cuh"
-#include "ylm_table.cuh"
+#include "ylm_block.cuh"
 
 struct pk_fft_plan_s {
   cufftHandle handle;
@@ -103,6 +103,87 @@ __global__ void ylm_premultiply_kernel(Dims d, float c0, float c1, float c2, flo
     const float v = rho[idx];
     for (int t = 0; t < terms.n; ++t)
       out[(int64_t)t * total + idx] = __fmul_rn(v, ylm_eval(terms.ell[t], terms.m[t], xh, yh, zh));
+  }
+}
+
+// ylm_premultiply_kernel for whole-ell term lists (mask MASK): four consecutive cells
+// along the last axis per thread (one float4 load of rho, one float4 store per term), each
+// Y_lm a compile-time polynomial.  Needs n2 % 4 == 0.
+template <int MASK>
+__global__ void __launch_bounds__(256) ylm_premultiply_block_kernel(Dims d, float c0, float c1, float c2,
+                                                                   float o0, float o1, float o2,
+                                                                   const float4 *__restrict__ rho,
+                                                                   float4 *__restrict__ out) {
+  constexpr int NT = ylm_mask_terms(MASK);
+  const int64_t nquad = d.nreal() / 4;
+  const int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  IndexWalker3 w(start, stride, d.n1, d.n2 / 4);
+  for (int64_t q = start; q < nquad; q += stride, w.next()) {
+    const float x = __fadd_rn(__fmul_rn((float)w.i, c0), o0);
+    const float y = __fadd_rn(__fmul_rn((float)w.j, c1), o1);
+    const float xy2 = __fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y));
+    const float4 r = __ldcs(rho + q);
+    const float rv[4] = {r.x, r.y, r.z, r.w};
+    float val[4][NT];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const float z = __fadd_rn(__fmul_rn((float)(4 * w.k + u), c2), o2);
+      const float xn = __fsqrt_rn(__fadd_rn(xy2, __fmul_rn(z, z)));
+      float xh = 0.f, yh = 0.f, zh = 0.f;
+      if (xn != 0.f) {
+        xh = __fdiv_rn(x, xn);
+        yh = __fdiv_rn(y, xn);
+        zh = __fdiv_rn(z, xn);
+      }
+      float yl[NT];
+      ylm_block<MASK>(xh, yh, zh, yl);
+#pragma unroll
+      for (int t = 0; t < NT; ++t) val[u][t] = __fmul_rn(rv[u], yl[t]);
+    }
+#pragma unroll
+    for (int t = 0; t < NT; ++t)
+      __stcs(out + (int64_t)t * nquad + q, make_float4(val[0][t], val[1][t], val[2][t], val[3][t]));
+  }
+}
+
+// ylm_accumulate_kernel for whole-ell term lists (mask MASK), four cells per thread.
+template <int MASK>
+__global__ void __launch_bounds__(256) ylm_accumulate_block_kernel(Dims d, float c0, float c1, float c2,
+                                                                  float o0, float o1, float o2,
+                                                                  const float4 *__restrict__ r,
+                                                                  float4 *__restrict__ rho_bar) {
+  constexpr int NT = ylm_mask_terms(MASK);
+  const int64_t nquad = d.nreal() / 4;
+  const int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  IndexWalker3 w(start, stride, d.n1, d.n2 / 4);
+  for (int64_t q = start; q < nquad; q += stride, w.next()) {
+    const float x = __fadd_rn(__fmul_rn((float)w.i, c0), o0);
+    const float y = __fadd_rn(__fmul_rn((float)w.j, c1), o1);
+    const float xy2 = __fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y));
+    float4 rv[NT];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) rv[t] = __ldcs(r + (int64_t)t * nquad + q);
+    const float4 b = rho_bar[q];
+    float acc[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const float z = __fadd_rn(__fmul_rn((float)(4 * w.k + u), c2), o2);
+      const float xn = __fsqrt_rn(__fadd_rn(xy2, __fmul_rn(z, z)));
+      float xh = 0.f, yh = 0.f, zh = 0.f;
+      if (xn != 0.f) {
+        xh = __fdiv_rn(x, xn);
+        yh = __fdiv_rn(y, xn);
+        zh = __fdiv_rn(z, xn);
+      }
+      float yl[NT];
+      ylm_block<MASK>(xh, yh, zh, yl);
+#pragma unroll
+      for (int t = 0; t < NT; ++t) {
+        const float4 v = rv[t];
+        acc[u] += (u == 0 ? v.x : u == 1 ? v.y : u == 2 ? v.z : v.w) * yl[t];
+      }
+    }
+    rho_bar[q] = make_float4(acc[0], acc[1], acc[2], acc[3]);
   }
 }
 
@@ -272,6 +353,21 @@ extern "C" pk_status pk_ylm_premultiply(void *stream, const float *rho, const in
     t.ell[j] = term_ell[j];
     t.m[j] = term_m[j];
   }
+  const int mask = ylm_terms_mask(nterms, term_ell, term_m);
+  const bool aligned = ((uintptr_t)rho % 16) == 0 && ((uintptr_t)out % 16) == 0;
+  if (mask && ylm_mask_compiled(mask) && d.n2 % 4 == 0 && aligned) {
+    const int grid = grid_for(d.nreal() / 4, 256);
+#define PK_YLM_PRE_CASE(M)                                                                        \
+  if (mask == (M)) {                                                                              \
+    ylm_premultiply_block_kernel<M><<<grid, 256, 0, (cudaStream_t)stream>>>(                      \
+        d, cellsize[0], cellsize[1], cellsize[2], offset[0], offset[1], offset[2], (const float4 *)rho, \
+        (float4 *)out);                                                                           \
+    PK_LAUNCH_CHECK();                                                                            \
+    return PK_OK;                                                                                 \
+  }
+    PK_YLM_MASKS(PK_YLM_PRE_CASE)
+#undef PK_YLM_PRE_CASE
+  }
   ylm_premultiply_kernel<<<grid_for(d.nreal(), 256), 256, 0, (cudaStream_t)stream>>>(
       d, cellsize[0], cellsize[1], cellsize[2], offset[0], offset[1], offset[2], t, rho, out);
   PK_LAUNCH_CHECK();
@@ -427,6 +523,21 @@ extern "C" pk_status pk_ylm_accumulate(void *stream, const float *r, const int32
                PK_ERR_INVALID, "invalid (ell, m) = (%d, %d)", term_ell[j], term_m[j]);
     t.ell[j] = term_ell[j];
     t.m[j] = term_m[j];
+  }
+  const int mask = ylm_terms_mask(nterms, term_ell, term_m);
+  const bool aligned = ((uintptr_t)r % 16) == 0 && ((uintptr_t)rho_bar % 16) == 0;
+  if (mask && ylm_mask_compiled(mask) && d.n2 % 4 == 0 && aligned) {
+    const int grid = grid_for(d.nreal() / 4, 256);
+#define PK_YLM_ACC_CASE(M)                                                                        \
+  if (mask == (M)) {                                                                              \
+    ylm_accumulate_block_kernel<M><<<grid, 256, 0, (cudaStream_t)stream>>>(                       \
+        d, cellsize[0], cellsize[1], cellsize[2], offset[0], offset[1], offset[2], (const float4 *)r, \
+        (float4 *)rho_bar);                                                                       \
+    PK_LAUNCH_CHECK();                                                                            \
+    return PK_OK;                                                                                 \
+  }
+    PK_YLM_MASKS(PK_YLM_ACC_CASE)
+#undef PK_YLM_ACC_CASE
   }
   ylm_accumulate_kernel<<<grid_for(d.nreal(), 256), 256, 0, (cudaStream_t)stream>>>(
       d, cellsize[0], cellsize[1], cellsize[2], offset[0], offset[1], offset[2], t, r, rho_bar);

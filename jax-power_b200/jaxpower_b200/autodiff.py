@@ -22,7 +22,7 @@ import torch
 from . import _lib
 from . import resamplers
 from .mesh import MeshAttrs, _paint, _r2c, _c2r, _device, _as_positions, _as_weights, _workspace
-from .mesh2 import _spectrum_sums, _ell_factors, _los, _firstpoint_terms, _term_batch
+from .mesh2 import _spectrum_sums, _ell_factors, _los, _firstpoint_terms, _term_batches
 
 __all__ = ['paint_value', 'spectrum_value']
 
@@ -138,13 +138,11 @@ class _Spectrum(torch.autograd.Function):
             _lib.call('pk_bin_firstpoint_adjoint', stream, _lib.ptr(A0), None, 0, None, None, *common,
                       _lib.ptr(bin.d_edges), len(bin._edges1d), bin._step, edge0, attrs.backend_code, len(ells),
                       _lib.i32(ells), _lib.ptr(coef), 1, _lib.ptr(ga0), 0, None, _lib.ptr(ws), ws.numel())
-        batch = _term_batch(attrs, len(terms)) if terms else 1
         coef_rest = coef.clone()  # ell = 0 enters the A0 cotangent once, with the first batch
         for l, ell in enumerate(ells):
             if ell == 0:
                 coef_rest[l] = 0.
-        for start in range(0, len(terms), batch):
-            chunk = terms[start:start + batch]
+        for ib, chunk in enumerate(_term_batches(attrs, ells)):
             nt = len(chunk)
             t_ell, t_m = [t[0] for t in chunk], [t[1] for t in chunk]
             real = torch.empty((nt,) + tuple(int(n) for n in meshsize), dtype=torch.float32, device=rho.device)
@@ -154,7 +152,7 @@ class _Spectrum(torch.autograd.Function):
             gf = torch.empty_like(F)
             _lib.call('pk_bin_firstpoint_adjoint', stream, _lib.ptr(A0), _lib.ptr(F), nt, _lib.i32(t_ell),
                       _lib.i32(t_m), *common, _lib.ptr(bin.d_edges), len(bin._edges1d), bin._step, edge0,
-                      attrs.backend_code, len(ells), _lib.i32(ells), _lib.ptr(coef if start == 0 else coef_rest), 1,
+                      attrs.backend_code, len(ells), _lib.i32(ells), _lib.ptr(coef if ib == 0 else coef_rest), 1,
                       _lib.ptr(ga0), 1, _lib.ptr(gf), _lib.ptr(ws), ws.numel())
             del F
             r = _c2r_unnormalised(gf, meshsize)

@@ -368,6 +368,32 @@ def _term_batch(mattrs, nterms):
     return int(max(1, min(nterms, 32, (0.4 * free) // per_term)))
 
 
+def _term_batches(mattrs, ells):
+    """First-point terms grouped into transforms that fit in memory, whole ells kept together.
+
+    Ells are taken in ascending order, every m of an ell in one batch when it fits (the
+    kernels have compiled forms for whole-ell term lists); an ell larger than a batch is
+    split.
+    """
+    terms = _firstpoint_terms(sorted(ells))
+    if not terms:
+        return []
+    batch = _term_batch(mattrs, len(terms))
+    out, cur = [], []
+    for ell in sorted(ell for ell in ells if ell > 0):
+        block = [(ell, m) for m in range(-ell, ell + 1)]
+        if len(cur) + len(block) > batch and cur:
+            out.append(cur)
+            cur = []
+        if len(block) > batch:
+            out += [block[i:i + batch] for i in range(0, len(block), batch)]
+        else:
+            cur = cur + block
+    if cur:
+        out.append(cur)
+    return out
+
+
 def _ell_factors(ells, vlos):
     """Per-multipole factor of the binned sums: (2 ell + 1) global, 4 pi first point (1 for ell 0)."""
     if vlos is None:
@@ -412,16 +438,16 @@ def _spectrum_sums(mattrs, bin, los, rmesh=None, cmesh=None, cmesh2=None, rmesh2
         else:
             rho = rmesh.contiguous()
             offset = (mattrs.boxcenter - (mattrs.boxsize / np.float32(2.)).astype('f4')).astype('f4')
-            batch = _term_batch(mattrs, len(terms))
-            real = torch.empty((batch,) + tuple(int(n) for n in meshsize), dtype=torch.float32, device=rho.device)
-            for start in range(0, len(terms), batch):
-                chunk = terms[start:start + batch]
+            batches = _term_batches(mattrs, ells)
+            real = torch.empty((max(map(len, batches)),) + tuple(int(n) for n in meshsize), dtype=torch.float32,
+                               device=rho.device)
+            for ib, chunk in enumerate(batches):
                 nt = len(chunk)
                 t_ell, t_m = [t[0] for t in chunk], [t[1] for t in chunk]
                 _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rho), _lib.i32(meshsize), _lib.f32(mattrs.cellsize),
                           _lib.f32(offset), nt, _lib.i32(t_ell), _lib.i32(t_m), _lib.ptr(real))
                 F = _r2c(real[:nt], meshsize)
-                include_ell0 = int(start == 0 and 0 in ells)  # ell = 0 rides on the first batch
+                include_ell0 = int(ib == 0 and 0 in ells)  # ell = 0 rides on the first batch
                 _lib.call('pk_bin_firstpoint', stream, _lib.ptr(A0), _lib.ptr(B0), _lib.ptr(F), nt, _lib.i32(t_ell),
                           _lib.i32(t_m), _lib.i32(meshsize), _lib.f32(mattrs.kfun), _lib.ptr(bin.d_edges),
                           len(bin._edges1d), bin._step, mattrs.backend_code, len(ells), _lib.i32(ells),
