@@ -48,7 +48,7 @@ CUTSKY = dict(workload='cut-sky FKP, first-point los, with adjoint: ~2e6 cluster
               k_step=0.005, ell_weights=(1., 0.5, 0.25), fd_step=0.25, seed=11)
 
 # kernel launches issued by each C-ABI entry point (ours, including CUB's scan kernels)
-LAUNCHES = {'pk_paint': 5, 'pk_interlace_compensate': 1, 'pk_bin_global': 2, 'pk_bin_firstpoint': 2,
+LAUNCHES = {'pk_paint': 5, 'pk_paint_batch': 5, 'pk_interlace_compensate': 1, 'pk_bin_global': 2, 'pk_bin_firstpoint': 2,
             'pk_bin_modes': 2, 'pk_bin_mesh': 2, 'pk_scale_real': 1, 'pk_ylm_premultiply': 1, 'pk_read': 1}
 
 
@@ -115,7 +115,7 @@ def measured_peaks():
 def algorithmic_bytes(name, npart, meshsize, interlacing, nells):
     nr = float(meshsize)**3
     nc = float(meshsize)**2 * (meshsize // 2 + 1)
-    if name == 'pk_paint':  # read positions (+weights) once, write one float32 mesh per shift
+    if name in ('pk_paint', 'pk_paint_batch'):  # read positions (+weights) once, write one float32 mesh per shift
         return 16. * npart + 4. * nr * interlacing
     if name == 'pk_interlace_compensate':
         return 8. * nc * (interlacing + 1)
@@ -650,7 +650,8 @@ def run_ours(args):
             'roofline': {'bound': 'hbm', 'kernel': dominant, 'achieved': achieved, 'peak': peak,
                          'peak_kind': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak,
                          'algorithmic_bytes': abytes,
-                         'traffic': float(PAINT_TRAFFIC_512) if (dominant == 'pk_paint' and W['meshsize'] == 512) else None,
+                         'traffic': float(PAINT_TRAFFIC_512) if (dominant in ('pk_paint', 'pk_paint_batch')
+                                                                 and W['meshsize'] == 512) else None,
                          'traffic_source': 'ncu dram read+write of the pk_paint kernels, this workload at 512^3'},
             'e2e': {'value': e2e_value, 'unit': 'spectra/s', 'h2d_bytes_per_step': int(npart * 12),
                     'd2h_bytes_per_step': int(len(W['ells']) * nbins * 8)},

@@ -91,6 +91,17 @@ pk_status pk_read(void *stream, const float *mesh, const float *positions,
                   int order, float shift, float scale, float *out, float *grad,
                   int accumulate);
 
+/* pk_read over the `interlacing` shifted meshes of an interlaced paint, mesh s at
+ * meshes + s * N0 N1 N2 read at u + s / interlacing (the transpose of the shifted
+ * paints of _paint, mesh.py:2737-2752): out[p] and grad[p] are the sums over s, added
+ * in shift order, of what pk_read gives for each mesh (bit for bit the same as one
+ * accumulating pk_read per shift). */
+pk_status pk_read_interlaced(void *stream, const float *meshes, int interlacing,
+                             const float *positions, const float *weights, int64_t n,
+                             const int32_t meshsize[3], const float boxsize[3],
+                             const float boxcenter[3], const float cellsize[3], int order,
+                             float scale, float *out, float *grad, int accumulate);
+
 /* ------------------------------------------------------------------- FFT
  * cuFFT plans for the reference's r2c / c2r (mesh.py:1679-1719): batch meshes
  * of shape meshsize, contiguous, out of place.  Both directions are

@@ -382,37 +382,67 @@ extern "C" pk_status pk_ylm_premultiply(void *stream, const float *rho, const in
 // writes for every shift h_s = sym(C e^{-i theta_s} X / I) with X = R / (N0 N1 N2) or
 // gbar / w', so that rho_bar_s = C2R(h_s) (unnormalised) is the cotangent of painted
 // mesh s.  sym() Hermitian-symmetrises the kz = 0 and N/2 planes.
-__global__ void __launch_bounds__(IL_THREADS) interlace_adjoint_kernel(
-    FourierParams p, const float2 *__restrict__ in, int from_real, float2 *__restrict__ out) {
+// The phase and window are the forward's per-axis factors (row factor x kz table), so this
+// is the exact transpose of interlace_kernel's arithmetic: e^{-i theta_s} / I = conj of the
+// forward phase, C = the same window product.  One warp per (i, j) row, four kz per lane.
+template <int NS>
+__global__ void __launch_bounds__(IL_THREADS) interlace_adjoint_kernel(FourierParams p,
+                                                                       const float2 *__restrict__ in,
+                                                                       int from_real,
+                                                                       float2 *__restrict__ out) {
+  extern __shared__ float4 ilsmem[];
   const Dims d = p.d;
+  ZTable t = ztable_at(ilsmem, p, false);
+  fill_ztable<false>(p, t);
+  __syncthreads();
   const int64_t total = d.ncomplex();
   const bool even = (d.n2 % 2) == 0;
   const float inv_n = 1.f / (float)d.nreal();
-  const int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
-  IndexWalker3 w(start, stride, d.n1, d.nz);
-  for (int64_t idx = start; idx < total; idx += stride, w.next()) {
-    const int i = w.i, j = w.j, z = w.k;
-    const bool plane = z == 0 || (even && z == d.nz - 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  for (RowWalker rw((int64_t)blockIdx.x * nwarps + warp, (int64_t)gridDim.x * nwarps, d.n1); rw.i < d.n0;
+       rw.next()) {
+    const int i = rw.i, j = rw.j;
     const int im = (d.n0 - i) % d.n0, jm = (d.n1 - j) % d.n1;
-    for (int s = 0; s < p.nshifts; ++s) {
-      float2 v[2];
-      for (int q = 0; q < (plane ? 2 : 1); ++q) {
-        const int ii = q ? im : i, jj = q ? jm : j;
-        const float k0 = ccoord(ii, d.n0, p.cspacing[0], false);
-        const float k1 = ccoord(jj, d.n1, p.cspacing[1], false);
-        const float k2 = ccoord(z, d.n2, p.cspacing[2], true);
-        float2 x = in[((int64_t)ii * d.n1 + jj) * d.nz + z];
-        const float scale = from_real ? inv_n : (plane ? 1.f : 0.5f);
-        float c = 1.f;
-        if (p.comp_order > 0)
-          c = inverse_power(__fmul_rn(__fmul_rn(sinc_of(k0), sinc_of(k1)), sinc_of(k2)), p.comp_order);
-        const float2 e = expi(-p.shifts[s] * ((k0 + k1) + k2));
-        const float f = c * scale / p.interlacing;
-        x = cmul(x, e);
-        v[q] = make_float2(x.x * f, x.y * f);
+    RowFactor<NS> rf, rm;
+    row_factor<NS, false>(p, i, j, rf);
+    row_factor<NS, false>(p, im, jm, rm);
+    const int64_t rbase = ((int64_t)i * d.n1 + j) * d.nz;
+    const int64_t mbase = ((int64_t)im * d.n1 + jm) * d.nz;
+    for (int zb = lane; zb < d.nz; zb += 128) {
+      float2 x[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int z = zb + 32 * u;
+        x[u] = z < d.nz ? in[rbase + z] : make_float2(0.f, 0.f);
       }
-      if (plane) v[0] = make_float2(0.5f * (v[0].x + v[1].x), 0.5f * (v[0].y - v[1].y));
-      out[(int64_t)s * total + idx] = v[0];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int z = zb + 32 * u;
+        if (z >= d.nz) break;
+        const bool plane = z == 0 || (even && z == d.nz - 1);
+        const float scale = from_real ? inv_n : (plane ? 1.f : 0.5f);
+        const float c = (p.comp_order > 0 ? rf.comp * t.comp[z] : 1.f) * scale;
+        float2 xm = make_float2(0.f, 0.f);
+        float cm = 0.f;
+        if (plane) {
+          xm = in[mbase + z];
+          cm = (p.comp_order > 0 ? rm.comp * t.comp[z] : 1.f) * scale;
+        }
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          const float2 ph = cmul(rf.ph[s], t.ph[s * d.nz + z]);
+          float2 v = cmul(x[u], make_float2(ph.x, -ph.y));
+          v = make_float2(v.x * c, v.y * c);
+          if (plane) {
+            const float2 phm = cmul(rm.ph[s], t.ph[s * d.nz + z]);
+            float2 m = cmul(xm, make_float2(phm.x, -phm.y));
+            m = make_float2(m.x * cm, m.y * cm);
+            v = make_float2(0.5f * (v.x + m.x), 0.5f * (v.y - m.y));
+          }
+          out[(int64_t)s * total + rbase + z] = v;
+        }
+      }
     }
   }
 }
@@ -500,9 +530,25 @@ extern "C" pk_status pk_interlace_adjoint(void *stream, const void *in, int from
   p.backend = backend;
   p.for_c2r = 1;
   p.scale = 1.f;
-  interlace_adjoint_kernel<<<grid_for(p.d.ncomplex(), IL_THREADS), IL_THREADS, 0,
-                             (cudaStream_t)stream>>>(p, (const float2 *)in, from_real,
-                                                     (float2 *)out);
+  const size_t smem = ztable_bytes(p.d, nshifts, false);
+  PK_REQUIRE(smem <= 200 * 1024, PK_ERR_RANGE, "mesh too large along the last axis for the kz table");
+  const int64_t nrows = (int64_t)p.d.n0 * p.d.n1;
+  const int64_t want = (nrows + IL_THREADS / 32 - 1) / (IL_THREADS / 32);
+  const int64_t cap = 8LL * sm_count();
+  const int blocks = (int)(want < cap ? want : cap);
+  cudaStream_t st = (cudaStream_t)stream;
+  switch (nshifts) {
+#define PK_ILA_CASE(N)                                                                                 \
+  case N:                                                                                              \
+    PK_CUDA(cudaFuncSetAttribute(interlace_adjoint_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                 (int)smem));                                                          \
+    interlace_adjoint_kernel<N><<<blocks, IL_THREADS, smem, st>>>(p, (const float2 *)in, from_real,      \
+                                                                  (float2 *)out);                      \
+    break;
+    PK_ILA_CASE(1) PK_ILA_CASE(2) PK_ILA_CASE(3) PK_ILA_CASE(4) PK_ILA_CASE(5) PK_ILA_CASE(6)
+    PK_ILA_CASE(7) PK_ILA_CASE(8)
+#undef PK_ILA_CASE
+  }
   PK_LAUNCH_CHECK();
   return PK_OK;
 }

@@ -69,6 +69,7 @@ struct PaintGeom {
   int64_t tiles_per_mock;
   int nmocks;
   const int64_t *offsets;  // device, nmocks + 1 particle offsets (NULL: one mock)
+  int64_t n;               // particles (one mock)
 };
 
 __device__ __forceinline__ float normalise(float p, float half, float center, float cell) {
@@ -283,23 +284,16 @@ __global__ void bucket_kernel(PaintGeom g, const float *__restrict__ pos,
   }
 }
 
-// Fixed-point exponent e such that count * max|w| * 2^e < 2^62: every partial sum of a
-// tile's cells fits in a signed 64-bit integer (each particle adds at most |w| in total).
-__device__ __forceinline__ int fixed_exponent(unsigned wmax_bits, unsigned count) {
+// Fixed-point exponent e such that count * max|w| * 2^e < 2^62, count = the particles of the
+// catalog: every partial sum of a cell fits in a signed 64-bit integer (each particle adds
+// at most |w| to a cell).  It depends on the catalog only, not on the tiling, so every tile
+// configuration rounds each contribution identically and paints the same bits.
+__device__ __forceinline__ int fixed_exponent(unsigned wmax_bits, long long count) {
   const float wmax = __uint_as_float(wmax_bits);
   if (!(wmax > 0.f) || !isfinite(wmax)) return 40;
   const int ew = (int)((wmax_bits >> 23) & 0xff) - 126;  // wmax < 2^ew
-  const int en = 32 - __clz(count > 0 ? count : 1);       // count < 2^en
+  const int en = 64 - __clzll(count > 0 ? count : 1);     // count < 2^en
   return 62 - ew - en;
-}
-
-__device__ __forceinline__ unsigned gcd_u(unsigned a, unsigned b) {
-  while (b) {
-    const unsigned t = a % b;
-    a = b;
-    b = t;
-  }
-  return a;
 }
 
 // Shared-memory atomics on 32-bit shared-window addresses.
@@ -343,8 +337,7 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
   // Per-cell 64-bit fixed point as two 32-bit words (native shared atomics): the low word's
   // returned old value gives the exact carry into the high word, so the integer sum stays
   // exact and independent of the order of the additions.
-  extern __shared__ unsigned acc32[];  // lo[nshifts][CELLS], hi[nshifts][CELLS], scratch[64]
-  __shared__ unsigned s_mult;
+  extern __shared__ __align__(16) unsigned acc32[];  // lo[nshifts][CELLS], hi[nshifts][CELLS], scratch[64]
   const int64_t gtile = blockIdx.x;
   const int mock = (int)(gtile / g.tiles_per_mock);
   const int tile = (int)(gtile % g.tiles_per_mock);
@@ -358,34 +351,40 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
   float *mock_out = out + (int64_t)mock * g.nshifts * g.d.nreal();
 
   if (count > 0) {
-    for (int i = threadIdx.x; i < 2 * g.nshifts * CELLS; i += blockDim.x) acc32[i] = 0u;
-    if (threadIdx.x == 0) {  // Fibonacci-hash stride coprime with count: a permutation
-      unsigned a = count > 2 ? ((unsigned)(0.6180339887 * count) | 1u) : 1u;
-      while (gcd_u(a, count) != 1u) a += 2u;
-      s_mult = a;
+    {
+      uint4 *z4 = reinterpret_cast<uint4 *>(acc32);  // 2 nshifts CELLS words, CELLS % 4 == 0
+      for (int i = threadIdx.x; i < (2 * g.nshifts * CELLS) / 4; i += blockDim.x) z4[i] = make_uint4(0u, 0u, 0u, 0u);
     }
     __syncthreads();
-    const int fexp = fixed_exponent(*wmax_bits, count);
+    const long long ncat = g.offsets ? (long long)(g.offsets[mock + 1] - g.offsets[mock]) : (long long)g.n;
+    const int fexp = fixed_exponent(*wmax_bits, ncat);
     const float fscale = ldexpf(1.f, fexp);  // exact power-of-two scaling of each contribution
-    const unsigned mult = s_mult;
     const int ns[3] = {g.d.n0, g.d.n1, g.d.n2};
     const int tl[3] = {T0, T1, T2};
     constexpr int OLO = -((ORDER - 1) / 2);
     // a stencil wraps past the mesh end at most once when every axis has >= ORDER cells
     const bool one_wrap = g.d.n0 >= ORDER && g.d.n1 >= ORDER && g.d.n2 >= ORDER;
     const unsigned acc_base = (unsigned)__cvta_generic_to_shared(acc32);
-    // permuted visiting order jdx = i * mult mod count (lanes of a warp far apart in the
-    // bucket, hence on different cells), advanced incrementally
-    unsigned jdx = (unsigned)(((unsigned long long)threadIdx.x * mult) % count);
-    const unsigned jstep = (unsigned)(((unsigned long long)blockDim.x * mult) % count);
-    for (unsigned i = threadIdx.x; i < count; i += blockDim.x) {
-      const float4 q = bucket[begin + jdx];
-      jdx += jstep;
-      if (jdx >= count) jdx -= count;
+    // The bucket is cut into 32 runs of S entries; lane l of a warp takes entry l S + jj of
+    // slot jj, so the lanes of a warp sit S entries apart (on different cells: bucket order
+    // follows the particles' input order, often spatial) and every entry is visited once.
+    // A slot paints all shifts of its entries; a sparse tile (fewer slots than warps) splits
+    // its slots per shift instead, so that its few entries still spread over all warps.
+    const int nwarps = blockDim.x >> 5, lane = threadIdx.x & 31;
+    const unsigned S = (count + 31) >> 5;
+    const bool split = S < (unsigned)nwarps;
+    const unsigned nslots = split ? S * (unsigned)g.nshifts : S;
+    for (unsigned j = threadIdx.x >> 5; j < nslots; j += (unsigned)nwarps) {
+      const unsigned jj = split ? j % S : j;
+      const int s_begin = split ? (int)(j / S) : 0, s_end = split ? s_begin + 1 : g.nshifts;
+      const unsigned e = lane * S + jj;
+      const bool has = e < count;
+      const float4 q = bucket[begin + (has ? e : 0u)];
       const float uq[3] = {q.x, q.y, q.z};
-      // w 2^fexp is exact, so (w 2^fexp) * ker rounds like the reference's w * ker, scaled
-      const float wq = q.w * fscale;
-      for (int s = 0; s < g.nshifts; ++s) {
+      // w 2^fexp is exact, so (w 2^fexp) * ker rounds like the reference's w * ker, scaled;
+      // lanes past the end of the bucket add zeros (to their scratch words)
+      const float wq = has ? q.w * fscale : 0.f;
+      for (int s = s_begin; s < s_end; ++s) {
         float k[3][ORDER];
         int l[3][ORDER];
 #pragma unroll
@@ -418,7 +417,7 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
 #pragma unroll
           for (int b = 0; b < ORDER; ++b) {
             const float kab = __fmul_rn(k[0][a], k[1][b]);
-            const bool vab = (l[0][a] | l[1][b]) >= 0;
+            const bool vab = has && (l[0][a] | l[1][b]) >= 0;
             const int rowoff = (l[0][a] * T1 + l[1][b]) * T2;
 #pragma unroll
             for (int c = 0; c < ORDER; ++c) {
@@ -447,10 +446,13 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
         const int x0 = los[0] + c0, x1 = los[1] + c1, x2 = los[2] + c2;
         if (x0 >= g.d.n0 || x1 >= g.d.n1) continue;
         const int64_t base = ((int64_t)x0 * g.d.n1 + x1) * g.d.n2 + x2;
+        const uint4 lo4 = *reinterpret_cast<const uint4 *>(alo + i);
+        const uint4 hi4 = *reinterpret_cast<const uint4 *>(ahi + i);
+        const unsigned los4[4] = {lo4.x, lo4.y, lo4.z, lo4.w}, his4[4] = {hi4.x, hi4.y, hi4.z, hi4.w};
         float v[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {  // exact integer -> double, one rounding to float
-          const long long fx = (long long)(((unsigned long long)ahi[i + j] << 32) | alo[i + j]);
+          const long long fx = (long long)(((unsigned long long)his4[j] << 32) | los4[j]);
           v[j] = __double2float_rn((double)fx * inv);
         }
         if (vec) {
@@ -482,44 +484,45 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
   }
 }
 
-// Gather (resamplers.read) plus the position gradient of paint's adjoint.
-__global__ void read_kernel(PaintGeom g, const float *__restrict__ mesh,
-                            const float *__restrict__ pos, const float *__restrict__ w,
-                            int64_t n, float shift, float scale, float *__restrict__ out,
-                            float *__restrict__ grad, int accumulate) {
+// Gather (resamplers.read) plus the position gradient of paint's adjoint, read at u + shift.
+template <int ORDER>
+__global__ void __launch_bounds__(256) read_kernel(PaintGeom g, const float *__restrict__ mesh, float shift,
+                                                   const float *__restrict__ pos, const float *__restrict__ w,
+                                                   int64_t n, float scale, float *__restrict__ out,
+                                                   float *__restrict__ grad, int accumulate) {
   const int ns[3] = {g.d.n0, g.d.n1, g.d.n2};
-  const int order = g.order;
-  const int olo = offset_lo(order);
+  constexpr int OLO = -((ORDER - 1) / 2);
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
        p += (int64_t)gridDim.x * blockDim.x) {
     float u[3], wp;
     load_particle(g, pos, w, p, u, &wp);
-    float k[3][MAX_ORDER], dk[3][MAX_ORDER];
-    int idx[3][MAX_ORDER];
+    float k[3][ORDER], dk[3][ORDER];
+    int idx[3][ORDER];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const float ud = __fadd_rn(u[d], shift);
-      const int i0 = base_index(order, ud);
+      const int i0 = base_index(ORDER, ud);
 #pragma unroll
-      for (int o = 0; o < MAX_ORDER; ++o) {
-        if (o < order) {
-          const int ii = i0 + olo + o;
-          const float diff = __fsub_rn((float)ii, ud);
-          const float sd = fabsf(diff);
-          k[d][o] = bspline(order, sd);
-          // ds/du = -sign(idx - u); sign(0) = 0 as in JAX's abs derivative
-          const float sgn = diff > 0.f ? -1.f : (diff < 0.f ? 1.f : 0.f);
-          dk[d][o] = bspline_deriv(order, sd) * sgn;
-          idx[d][o] = wrapi(ii, ns[d]);
-        }
+      for (int q = 0; q < ORDER; ++q) {
+        const int ii = i0 + OLO + q;
+        const float diff = __fsub_rn((float)ii, ud);
+        const float sd = fabsf(diff);
+        k[d][q] = bspline(ORDER, sd);
+        // ds/du = -sign(idx - u); sign(0) = 0 as in JAX's abs derivative
+        const float sgn = diff > 0.f ? -1.f : (diff < 0.f ? 1.f : 0.f);
+        dk[d][q] = bspline_deriv(ORDER, sd) * sgn;
+        idx[d][q] = wrapi(ii, ns[d]);
       }
     }
     float acc = 0.f, g0 = 0.f, g1 = 0.f, g2 = 0.f;
-    for (int a = 0; a < order; ++a)
-      for (int b = 0; b < order; ++b) {
+#pragma unroll
+    for (int a = 0; a < ORDER; ++a)
+#pragma unroll
+      for (int b = 0; b < ORDER; ++b) {
         const int64_t row = ((int64_t)idx[0][a] * g.d.n1 + idx[1][b]) * g.d.n2;
         const float kab = __fmul_rn(k[0][a], k[1][b]);
-        for (int c = 0; c < order; ++c) {
+#pragma unroll
+        for (int c = 0; c < ORDER; ++c) {
           const float m = mesh[row + idx[2][c]];
           acc = __fadd_rn(acc, __fmul_rn(m, __fmul_rn(kab, k[2][c])));
           if (grad) {
@@ -545,6 +548,26 @@ __global__ void read_kernel(PaintGeom g, const float *__restrict__ mesh,
       }
     }
   }
+}
+
+static pk_status launch_read(cudaStream_t stream, const PaintGeom &g, const float *mesh, float shift,
+                             const float *positions, const float *weights, int64_t n, float scale, float *out,
+                             float *grad, int accumulate) {
+  if (n == 0) return PK_OK;
+  const int threads = 256;
+  const int64_t want = (n + threads - 1) / threads;
+  const int blocks = (int)(want < 64LL * sm_count() ? want : 64LL * sm_count());
+  switch (g.order) {
+#define PK_READ_CASE(O)                                                                                   \
+  case O:                                                                                                 \
+    read_kernel<O><<<blocks, threads, 0, stream>>>(g, mesh, shift, positions, weights, n, scale, out, grad, \
+                                                   accumulate);                                           \
+    break;
+    PK_READ_CASE(1) PK_READ_CASE(2) PK_READ_CASE(3) PK_READ_CASE(4)
+#undef PK_READ_CASE
+  }
+  PK_LAUNCH_CHECK();
+  return PK_OK;
 }
 
 static bool fill_geom(const int32_t meshsize[3], const float boxsize[3], const float boxcenter[3],
@@ -582,6 +605,7 @@ static bool fill_geom(const int32_t meshsize[3], const float boxsize[3], const f
   g->tiles_per_mock = (int64_t)g->nt[0] * g->nt[1] * g->nt[2];
   g->nmocks = nmocks;
   g->offsets = nullptr;
+  g->n = 0;
   return true;
 }
 
@@ -629,6 +653,7 @@ static pk_status paint_run(cudaStream_t s, const float *positions, const float *
                            int64_t n, PaintGeom g, int config, float *out, void *workspace,
                            size_t workspace_bytes, int *d_status) {
   PaintLayout L;
+  g.n = n;
   pk_status st = paint_layout(n, g, &L);
   if (st) return st;
   PK_REQUIRE(workspace && workspace_bytes >= L.total, PK_ERR_WORKSPACE,
@@ -766,12 +791,28 @@ extern "C" pk_status pk_read(void *stream, const float *mesh, const float *posit
   PaintGeom g;
   PK_REQUIRE(fill_geom(meshsize, boxsize, boxcenter, cellsize, order, 1, shifts, 0, 1, &g),
              PK_ERR_INVALID, "invalid meshsize / order / cellsize");
-  if (n == 0) return PK_OK;
-  const int threads = 256;
-  const int64_t want = (n + threads - 1) / threads;
-  const int blocks = (int)(want < 64LL * sm_count() ? want : 64LL * sm_count());
-  read_kernel<<<blocks, threads, 0, (cudaStream_t)stream>>>(g, mesh, positions, weights, n,
-                                                            shift, scale, out, grad, accumulate);
-  PK_LAUNCH_CHECK();
+  return launch_read((cudaStream_t)stream, g, mesh, shift, positions, weights, n, scale, out, grad, accumulate);
+}
+
+extern "C" pk_status pk_read_interlaced(void *stream, const float *meshes, int interlacing,
+                                        const float *positions, const float *weights, int64_t n,
+                                        const int32_t meshsize[3], const float boxsize[3],
+                                        const float boxcenter[3], const float cellsize[3], int order,
+                                        float scale, float *out, float *grad, int accumulate) {
+  PK_REQUIRE(meshes && (n == 0 || positions), PK_ERR_INVALID, "meshes / positions is NULL");
+  PK_REQUIRE(out || grad, PK_ERR_INVALID, "nothing to write (out and grad NULL)");
+  PK_REQUIRE(interlacing >= 1 && interlacing <= 8, PK_ERR_INVALID, "interlacing must be in 1..8");
+  float shifts[MAX_SHIFTS] = {0.f, 0.f, 0.f, 0.f};
+  PaintGeom g;
+  PK_REQUIRE(fill_geom(meshsize, boxsize, boxcenter, cellsize, order, 1, shifts, 0, 1, &g),
+             PK_ERR_INVALID, "invalid meshsize / order / cellsize");
+  // one pass per shifted mesh, each adding into the previous: a pass reads a single mesh,
+  // whose random-access working set the L2 holds far better than all meshes at once
+  for (int s = 0; s < interlacing; ++s) {
+    pk_status st = launch_read((cudaStream_t)stream, g, meshes + (int64_t)s * g.d.nreal(),
+                               (float)s / (float)interlacing, positions, weights, n, scale, out, grad,
+                               s > 0 || accumulate);
+    if (st) return st;
+  }
   return PK_OK;
 }

@@ -40,6 +40,8 @@ SIGNATURES = {
                             c_int, c_float, c_int, c_int, c_int32_p, c_void_p, c_void_p, c_size_t],
     'pk_read': [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32_p, c_float_p, c_float_p,
                 c_float_p, c_int, c_float, c_float, c_void_p, c_void_p, c_int],
+    'pk_read_interlaced': [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int64, c_int32_p, c_float_p, c_float_p,
+                           c_float_p, c_int, c_float, c_void_p, c_void_p, c_int],
     'pk_fft_plan_create': [c_int32_p, c_int, c_int, ctypes.POINTER(c_void_p)],
     'pk_fft_exec': [c_void_p, c_void_p, c_void_p, c_void_p],
     'pk_fft_plan_destroy': [c_void_p],

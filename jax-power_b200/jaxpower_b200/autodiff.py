@@ -8,11 +8,13 @@ XLA).  Here each stage has an explicit adjoint in the CUDA library, wired into
 
 - ``paint_value(positions, weights, attrs, ...)`` -> mesh tensor (real or Hermitian complex);
   backward: rfftn of the real cotangent, ``pk_interlace_adjoint`` (phases, compensation,
-  1/I), one C2R per shift, then ``pk_read`` with the window derivative (position and
-  weight cotangents), summed over shifts.
+  1/I), one C2R per shift, then ``pk_read_interlaced`` with the window derivative (position
+  and weight cotangents) over all shifted meshes.
 - ``spectrum_value(mesh, attrs, bin, los)`` -> (nells, nbins) float64 multipoles
   (``num_raw`` of ``compute_mesh2_spectrum``); backward: ``pk_bin_global_adjoint`` or
-  ``pk_bin_firstpoint_adjoint`` + C2R + ``pk_ylm_accumulate``.
+  ``pk_bin_firstpoint_adjoint`` + C2R + ``pk_ylm_accumulate``.  The first-point forward
+  keeps A0 and the transformed Y_lm-weighted meshes resident (when they fit in a third of
+  the free memory), so the backward pass does not transform them again.
 
 Gradients follow the 'jax' FFT semantics and even multipoles (odd auto multipoles are 0).
 """
@@ -62,16 +64,15 @@ class _Paint(torch.autograd.Function):
                       _lib.i32(meshsize), order if compensate else 0, attrs.backend_code, _lib.ptr(h))
             rbars = _c2r_unnormalised(h, meshsize)
         n = positions.shape[0]
-        gpos = torch.zeros((n, 3), dtype=torch.float32, device=positions.device)
-        gw = torch.zeros(n, dtype=torch.float32, device=positions.device)
+        gpos = torch.empty((n, 3), dtype=torch.float32, device=positions.device)
+        gw = torch.empty(n, dtype=torch.float32, device=positions.device) if ctx.has_weights else None
         pos = positions.detach().contiguous()
         wts = None if weights is None else weights.detach().contiguous()
-        for s in range(interlacing):
-            shift = float(np.float32(s) / np.float32(interlacing))
-            _lib.call('pk_read', _lib.stream_handle(), _lib.ptr(rbars[s].contiguous()), _lib.ptr(pos), _lib.ptr(wts),
-                      n, _lib.i32(meshsize), _lib.f32(attrs.boxsize), _lib.f32(attrs.boxcenter),
-                      _lib.f32(attrs.cellsize), order, shift, 1., _lib.ptr(gw), _lib.ptr(gpos), 1)
-        return gpos, (gw if ctx.has_weights else None), None, None, None, None, None
+        # the gathers over the shifted meshes: mesh s read at u + s / I, summed in shift order
+        _lib.call('pk_read_interlaced', _lib.stream_handle(), _lib.ptr(rbars.contiguous()), interlacing, _lib.ptr(pos),
+                  _lib.ptr(wts), n, _lib.i32(meshsize), _lib.f32(attrs.boxsize), _lib.f32(attrs.boxcenter),
+                  _lib.f32(attrs.cellsize), order, 1., _lib.ptr(gw), _lib.ptr(gpos), 0)
+        return gpos, gw, None, None, None, None, None
 
 
 def paint_value(positions, weights=None, attrs=None, resampler='cic', interlacing=0, compensate=False,
@@ -91,9 +92,12 @@ class _Spectrum(torch.autograd.Function):
     @staticmethod
     def forward(ctx, value, attrs, bin, los):
         is_complex = value.is_complex()
-        raw = _spectrum_sums(attrs, bin, los, rmesh=None if is_complex else value.detach(),
-                             cmesh=value.detach() if is_complex else None)
         _, vlos, _ = _los(los)
+        # first point: A0 and the transformed Y_lm-weighted meshes stay resident for backward
+        keep = {} if (vlos is None and not is_complex and ctx.needs_input_grad[0]) else None
+        raw = _spectrum_sums(attrs, bin, los, rmesh=None if is_complex else value.detach(),
+                             cmesh=value.detach() if is_complex else None, keep=keep)
+        ctx.keep = keep
         factors = torch.tensor(_ell_factors(bin.ells, vlos), dtype=torch.float64, device=raw.device)
         nmodes = torch.as_tensor(bin.nmodes, dtype=torch.float64, device=raw.device)
         ctx.save_for_backward(value)
@@ -129,7 +133,9 @@ class _Spectrum(torch.autograd.Function):
         if is_complex:
             raise NotImplementedError('first-point gradients are implemented for real meshes')
         rho = value.detach().contiguous()
-        A0 = _r2c(rho, meshsize).contiguous()
+        keep = ctx.keep if ctx.keep else {}
+        ctx.keep = None
+        A0 = keep['A0'] if 'A0' in keep else _r2c(rho, meshsize).contiguous()
         ga0 = torch.zeros_like(A0)
         rho_bar = torch.zeros_like(rho)
         terms = _firstpoint_terms(ells)
@@ -142,13 +148,20 @@ class _Spectrum(torch.autograd.Function):
         for l, ell in enumerate(ells):
             if ell == 0:
                 coef_rest[l] = 0.
-        for ib, chunk in enumerate(_term_batches(attrs, ells)):
+        kept = keep.pop('F', None)
+        batches = [chunk for chunk, _ in kept] if kept else _term_batches(attrs, ells)
+        for ib, chunk in enumerate(batches):
             nt = len(chunk)
             t_ell, t_m = [t[0] for t in chunk], [t[1] for t in chunk]
-            real = torch.empty((nt,) + tuple(int(n) for n in meshsize), dtype=torch.float32, device=rho.device)
-            _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rho), _lib.i32(meshsize), _lib.f32(attrs.cellsize),
-                      _lib.f32(offset), nt, _lib.i32(t_ell), _lib.i32(t_m), _lib.ptr(real))
-            F = _r2c(real, meshsize)
+            if kept:
+                F = kept[ib][1]
+                kept[ib] = None
+            else:
+                real = torch.empty((nt,) + tuple(int(n) for n in meshsize), dtype=torch.float32, device=rho.device)
+                _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rho), _lib.i32(meshsize), _lib.f32(attrs.cellsize),
+                          _lib.f32(offset), nt, _lib.i32(t_ell), _lib.i32(t_m), _lib.ptr(real))
+                F = _r2c(real, meshsize)
+                del real
             gf = torch.empty_like(F)
             _lib.call('pk_bin_firstpoint_adjoint', stream, _lib.ptr(A0), _lib.ptr(F), nt, _lib.i32(t_ell),
                       _lib.i32(t_m), *common, _lib.ptr(bin.d_edges), len(bin._edges1d), bin._step, edge0,

@@ -47,6 +47,18 @@ def make_key(*parts):
     return '|'.join([torch.cuda.get_device_name()] + [str(p) for p in parts])
 
 
+def cached_tile_config(key, default=0):
+    """The tuned configuration of ``key`` when there is one (memory or file), else ``default``."""
+    with _lock:
+        if key in _cache:
+            return _cache[key]
+        table = _load()
+        if key in table:
+            _cache[key] = int(table[key]['config'])
+            return _cache[key]
+    return default
+
+
 def best_tile_config(key, run, repeats=3):
     """Fastest tile configuration for ``key``; ``run(config)`` enqueues one paint."""
     if os.environ.get('PK_AUTOTUNE', '1') == '0':

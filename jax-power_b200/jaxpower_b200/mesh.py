@@ -588,24 +588,48 @@ class ParticleField:
                       compensate=compensate, out=out)
 
 
-def _paint_shifts(attrs, positions, weights, order, interlacing, status=None):
-    """All shifted real meshes, (I, N0, N1, N2) float32, through pk_paint (≤ 4 shifts per launch)."""
-    interlacing = max(int(interlacing), 1)
+def _paint_call(attrs, positions, weights, order, interlacing, begin, count, out, status, config):
+    """One pk_paint_batch launch sequence (a single catalog) with tile configuration ``config``."""
     n = positions.shape[0]
+    shape = _lib.i32(attrs.meshsize)
+    nbytes = _lib.c_size_t()
+    _lib.call('pk_paint_batch_workspace_size', n, 1, shape, order, count, config, _lib.ctypes.byref(nbytes))
+    ws = _workspace(nbytes.value)
+    _lib.call('pk_paint_batch', _lib.stream_handle(), _lib.ptr(positions), _lib.ptr(weights), None, n, 1, shape,
+              _lib.f32(attrs.boxsize), _lib.f32(attrs.boxcenter), _lib.f32(attrs.cellsize), order, interlacing, begin,
+              count, config, _lib.ptr(out), _lib.ptr(ws), nbytes.value, _lib.ptr(status))
+
+
+def _paint_config(attrs, positions, weights, order, interlacing, group, out, status):
+    """Tile configuration of the paint pass, autotuned once per (mesh, order, shifts, N octave).
+
+    Every configuration paints the same bits (the fixed-point scale depends on the catalog
+    only), so the choice affects the speed alone.  Under CUDA graph capture nothing is timed:
+    a tuned value is used when there is one, else configuration 0.
+    """
+    from .autotune import best_tile_config, make_key, cached_tile_config
+    n = positions.shape[0]
+    key = make_key('paint', tuple(int(s) for s in attrs.meshsize), order, group,
+                   int(round(2. * math.log2(max(n, 2)))))
+    if torch.cuda.is_current_stream_capturing():
+        return cached_tile_config(key, default=0)
+    return best_tile_config(key, lambda config: _paint_call(attrs, positions, weights, order, interlacing, 0, group,
+                                                            out, status, config))
+
+
+def _paint_shifts(attrs, positions, weights, order, interlacing, status=None):
+    """All shifted real meshes, (I, N0, N1, N2) float32, through pk_paint_batch (≤ 4 shifts per launch)."""
+    interlacing = max(int(interlacing), 1)
     shape = tuple(int(s) for s in attrs.meshsize)
     meshes = torch.empty((interlacing,) + shape, dtype=torch.float32, device=positions.device)
     group = min(interlacing, 4)
-    nbytes = _lib.c_size_t()
-    _lib.call('pk_paint_workspace_size', n, _lib.i32(shape), order, group, _lib.ctypes.byref(nbytes))
-    ws = _workspace(nbytes.value)
     if status is None:
         status = torch.zeros(1, dtype=torch.int32, device=positions.device)
+    config = _paint_config(attrs, positions, weights, order, interlacing, group, meshes[:group], status)
     for begin in range(0, interlacing, group):
         count = min(group, interlacing - begin)
-        out = meshes[begin:begin + count]
-        _lib.call('pk_paint', _lib.stream_handle(), _lib.ptr(positions), _lib.ptr(weights), n,
-                  _lib.i32(shape), _lib.f32(attrs.boxsize), _lib.f32(attrs.boxcenter), _lib.f32(attrs.cellsize),
-                  order, interlacing, begin, count, _lib.ptr(out), _lib.ptr(ws), nbytes.value, _lib.ptr(status))
+        _paint_call(attrs, positions, weights, order, interlacing, begin, count, meshes[begin:begin + count], status,
+                    config)
     return meshes, status
 
 

@@ -401,13 +401,16 @@ def _ell_factors(ells, vlos):
     return [2. * ell + 1. for ell in ells]
 
 
-def _spectrum_sums(mattrs, bin, los, rmesh=None, cmesh=None, cmesh2=None, rmesh2=None):
+def _spectrum_sums(mattrs, bin, los, rmesh=None, cmesh=None, cmesh2=None, rmesh2=None, keep=None):
     """Raw per-bin sums (nells, nbins) float64 on the device (no host synchronisation).
 
     Global los: sum of w Re/Im(conj(d1) d2) L_ell(mu) over each bin.  First point: the
     sums of ``pk_bin_firstpoint`` over all (ell, m) terms.  ``rmesh`` / ``cmesh`` are the
     real / Hermitian-complex values of the first mesh (either may be None), likewise for
-    the second mesh of a cross spectrum.
+    the second mesh of a cross spectrum.  ``keep`` (a dict, first point only): receives
+    A0 and the transformed Y_lm-weighted meshes of every term batch, ``keep['F']`` a list of
+    (terms, F), when they fit in a third of the free device memory (the backward pass
+    then reuses them instead of transforming again).
     """
     meshsize = mattrs.meshsize
     los, vlos, swap = _los(los)
@@ -441,6 +444,12 @@ def _spectrum_sums(mattrs, bin, los, rmesh=None, cmesh=None, cmesh2=None, rmesh2
             batches = _term_batches(mattrs, ells)
             real = torch.empty((max(map(len, batches)),) + tuple(int(n) for n in meshsize), dtype=torch.float32,
                                device=rho.device)
+            if keep is not None:
+                per_term = 8 * A0.numel()
+                if len(terms) * per_term < torch.cuda.mem_get_info()[0] / 3:
+                    keep['A0'], keep['F'] = A0, []
+                else:
+                    keep = None
             for ib, chunk in enumerate(batches):
                 nt = len(chunk)
                 t_ell, t_m = [t[0] for t in chunk], [t[1] for t in chunk]
@@ -452,6 +461,8 @@ def _spectrum_sums(mattrs, bin, los, rmesh=None, cmesh=None, cmesh2=None, rmesh2
                           _lib.i32(t_m), _lib.i32(meshsize), _lib.f32(mattrs.kfun), _lib.ptr(bin.d_edges),
                           len(bin._edges1d), bin._step, mattrs.backend_code, len(ells), _lib.i32(ells),
                           include_ell0, 1, _lib.ptr(raw), _lib.ptr(ws), ws.numel())
+                if keep is not None:
+                    keep['F'].append((chunk, F))
                 del F
         raw = raw.reshape(len(ells), nbins)
         if swap:  # conj: odd multipoles (imaginary parts) change sign

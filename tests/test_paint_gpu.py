@@ -134,6 +134,59 @@ def test_read_matches_oracle(resampler):
     assert np.allclose(got, ref, rtol=1e-5, atol=1e-5)
 
 
+@pytest.mark.parametrize('order,interlacing', [(1, 2), (2, 3), (3, 3), (4, 4)])
+def test_read_interlaced_equals_per_shift_reads(order, interlacing):
+    """pk_read_interlaced gives, bit for bit, the sum of pk_read over the shifted meshes
+    (accumulated in shift order), for the read values and the position gradient."""
+    from jaxpower_b200 import _lib as L
+    meshsize, boxsize, boxcenter = (16, 20, 12), np.array([50., 60., 40.], dtype='f4'), np.array([1., -2., 3.], dtype='f4')
+    rng = np.random.default_rng(9)
+    meshes = torch.as_tensor(rng.normal(size=(interlacing,) + meshsize).astype('f4')).cuda()
+    pos, w = _catalog(5000, 1.1 * boxsize, boxcenter, seed=10)
+    pos = torch.as_tensor(pos).cuda().contiguous()
+    w = torch.as_tensor(w).cuda().contiguous()
+    n = pos.shape[0]
+    cellsize = (boxsize / np.asarray(meshsize)).astype('f4')
+    geo = (L.i32(meshsize), L.f32(boxsize), L.f32(boxcenter), L.f32(cellsize), order)
+    out_a = torch.zeros(n, device='cuda')
+    grad_a = torch.zeros((n, 3), device='cuda')
+    for s in range(interlacing):
+        shift = float(np.float32(s) / np.float32(interlacing))
+        L.call('pk_read', L.stream_handle(), L.ptr(meshes[s]), L.ptr(pos), L.ptr(w), n, *geo, shift, 0.5,
+               L.ptr(out_a), L.ptr(grad_a), 1)
+    out_b = torch.full((n,), 3., device='cuda')
+    grad_b = torch.full((n, 3), 3., device='cuda')
+    L.call('pk_read_interlaced', L.stream_handle(), L.ptr(meshes), interlacing, L.ptr(pos), L.ptr(w), n, *geo, 0.5,
+           L.ptr(out_b), L.ptr(grad_b), 0)
+    assert torch.equal(out_a, out_b)
+    assert torch.equal(grad_a, grad_b)
+
+
+@pytest.mark.parametrize('resampler', ['cic', 'tsc', 'pcs'])
+def test_paint_same_bits_for_every_tile_config(resampler):
+    """The fixed-point scale depends on the catalog only: all tile configurations (and so the
+    autotuner's choice) paint identical meshes."""
+    from jaxpower_b200 import _lib as L
+    from jaxpower_b200.mesh import _paint_call
+    jp = _jp()
+    pos, w = _catalog(300000, [500.] * 3, [0.] * 3, seed=12)
+    pos[:1000] = pos[0]  # a dense clump (many particles on a few cells)
+    w[::7] *= -0.5
+    attrs = jp.MeshAttrs(meshsize=(64, 48, 32), boxsize=500.)
+    order = {'cic': 2, 'tsc': 3, 'pcs': 4}[resampler]
+    pos = torch.as_tensor(pos).cuda()
+    w = torch.as_tensor(w).cuda()
+    status = torch.zeros(1, dtype=torch.int32, device='cuda')
+    outs = []
+    for config in range(4):
+        out = torch.empty((3,) + tuple(attrs.meshsize), dtype=torch.float32, device='cuda')
+        _paint_call(attrs, pos, w, order, 3, 0, 3, out, status, config)
+        outs.append(out)
+    for out in outs[1:]:
+        assert torch.equal(out, outs[0])
+    assert int(status.item()) == 0
+
+
 def test_paint_deterministic():
     jp = _jp()
     pos, w = _catalog(200000, [1000.] * 3, [0.] * 3, seed=11)
