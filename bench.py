@@ -389,6 +389,58 @@ def run_cutsky(reps=3):
                        'forward_backward = differentiable paint + spectrum + backward to data positions')
 
 
+def run_paint_only(meshsize=None, reps=3, config=0):
+    """Profiling aid: the benchmark catalog (generated at 512^3) painted with TSC and 3
+    interlacing shifts at ``meshsize`` through pk_paint_batch with tile configuration ``config``,
+    one warm-up and ``reps`` timed calls; nothing else is on the device meanwhile."""
+    import torch
+    import jaxpower_b200 as jp
+    from jaxpower_b200.mesh import _paint_call
+    from jaxpower_b200.mock import lognormal_particles, power_law_pk
+    W = WORKLOAD
+    pos = lognormal_particles(jp.MeshAttrs(meshsize=W['meshsize'], boxsize=W['boxsize'], boxcenter=0.),
+                              power_law_pk(), W['nbar'], seed=W['seed']).contiguous()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    n = meshsize or W['meshsize']
+    attrs = jp.MeshAttrs(meshsize=n, boxsize=W['boxsize'], boxcenter=0.)
+    out = torch.empty((W['interlacing'], n, n, n), dtype=torch.float32, device='cuda')
+    status = torch.zeros(1, dtype=torch.int32, device='cuda')
+    _paint_call(attrs, pos, None, 3, W['interlacing'], 0, W['interlacing'], out, status, config)  # warm-up
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        _paint_call(attrs, pos, None, 3, W['interlacing'], 0, W['interlacing'], out, status, config)
+    b.record()
+    torch.cuda.synchronize()
+    return dict(nparticles=int(pos.shape[0]), meshsize=n, tile_config=config, ms_per_paint=a.elapsed_time(b) / reps,
+                status=int(status.item()))
+
+
+def run_cutsky_forward_only(meshsize=None, reps=3):
+    """Profiling aid: the cut-sky FKP first-point forward pipeline (paint + spectrum) ``reps``
+    times, at ``meshsize`` (default that of the cut-sky workload)."""
+    import torch
+    import jaxpower_b200 as jp
+    from jaxpower_b200.mock import cutsky_particles
+    C = dict(CUTSKY)
+    data, randoms, wd, wr = cutsky_particles(ndata=C['ndata'], nrandoms=C['nrandoms'], seed=C['seed'])
+    attrs = jp.get_mesh_attrs(data, randoms, meshsize=meshsize or C['meshsize'], boxpad=C['boxpad'])
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': C['k_step']}, ells=C['ells'])
+    fkp = jp.FKPField(jp.ParticleField(data, wd, attrs=attrs), jp.ParticleField(randoms, wr, attrs=attrs))
+    a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for r in range(reps + 1):
+        if r == 1:
+            a.record()
+        mesh = fkp.paint(resampler=C['resampler'], interlacing=C['interlacing'], compensate=True, out='real')
+        poles = jp.compute_mesh2_spectrum(mesh, bin=b, los='firstpoint')
+        del mesh
+    e.record()
+    torch.cuda.synchronize()
+    return dict(meshsize=int(attrs.meshsize[0]), ms_per_spectrum=a.elapsed_time(e) / reps,
+                p0_sum=float(np.sum(poles.get(0).num_raw)))
+
+
 def run_mlp_forward(batch=1 << 20, reps=20):
     """Throughput of the correction network's tcgen05 forward pass on a batch of random
     feature rows (dense FLOPs 2 (16 + 2 x 128 + 16) x 128 per row; the padded output layer
@@ -691,9 +743,19 @@ def main():
     parser.add_argument('--no-cutsky', action='store_true', help='skip the cut-sky FKP first-point measurement')
     parser.add_argument('--mlp-forward-only', action='store_true',
                         help='only time the correction network forward pass (profiling aid)')
+    parser.add_argument('--paint-only', action='store_true',
+                        help='only paint the benchmark catalog (at --meshsize if given; profiling aid)')
+    parser.add_argument('--cutsky-forward-only', action='store_true',
+                        help='only run the cut-sky first-point forward pipeline (at --meshsize if given; profiling aid)')
     args = parser.parse_args()
     if args.mlp_forward_only:
         print(json.dumps({'mlp_forward': run_mlp_forward()}), flush=True)
+        return
+    if args.paint_only:
+        print(json.dumps({'paint': run_paint_only(args.meshsize or None)}), flush=True)
+        return
+    if args.cutsky_forward_only:
+        print(json.dumps({'cutsky_forward': run_cutsky_forward_only(args.meshsize or None)}), flush=True)
         return
     if args.impl == 'reference':
         run_reference(args)
