@@ -383,8 +383,9 @@ extern "C" pk_status pk_ylm_premultiply(void *stream, const float *rho, const in
 // gbar / w', so that rho_bar_s = C2R(h_s) (unnormalised) is the cotangent of painted
 // mesh s.  sym() Hermitian-symmetrises the kz = 0 and N/2 planes.
 // The phase and window are the forward's per-axis factors (row factor x kz table), so this
-// is the exact transpose of interlace_kernel's arithmetic: e^{-i theta_s} / I = conj of the
-// forward phase, C = the same window product.  One warp per (i, j) row, four kz per lane.
+// is the transpose of interlace_kernel's arithmetic: e^{-i theta_s} = conj of the forward
+// phase, C / I = the same row scale times the kz window.  One warp per (i, j) row, four kz
+// per lane.
 template <int NS>
 __global__ void __launch_bounds__(IL_THREADS) interlace_adjoint_kernel(FourierParams p,
                                                                        const float2 *__restrict__ in,
@@ -422,12 +423,12 @@ __global__ void __launch_bounds__(IL_THREADS) interlace_adjoint_kernel(FourierPa
         if (z >= d.nz) break;
         const bool plane = z == 0 || (even && z == d.nz - 1);
         const float scale = from_real ? inv_n : (plane ? 1.f : 0.5f);
-        const float c = (p.comp_order > 0 ? rf.comp * t.comp[z] : 1.f) * scale;
+        const float c = rf.scale * t.comp[z] * scale;
         float2 xm = make_float2(0.f, 0.f);
         float cm = 0.f;
         if (plane) {
           xm = in[mbase + z];
-          cm = (p.comp_order > 0 ? rm.comp * t.comp[z] : 1.f) * scale;
+          cm = rm.scale * t.comp[z] * scale;
         }
 #pragma unroll
         for (int s = 0; s < NS; ++s) {

@@ -61,19 +61,19 @@ __device__ __forceinline__ float2 expi(float t) {
 constexpr int IL_MAX_SHIFTS = 8;
 
 // Per-CTA table along kz (shared memory): for each shift s, e^{i s kz(z)} and, for the
-// 'jaxdecomp' semantics, e^{-i s kz(-z)} on the full grid; plus sinc(kz / 2pi).
+// 'jaxdecomp' semantics, e^{-i s kz(-z)} on the full grid; plus sinc(kz / 2pi)^-p.
 struct ZTable {
   float2 *ph;    // [nshifts][nz]
   float2 *phm;   // [nshifts][nz] (jaxdecomp)
   float *comp;   // [nz]: sinc(kz / 2pi)^-p (1 without compensation)
 };
 
-// Row factors: prod over x, y of the phase (divided by I) and of the sinc window.
+// Row factors: the phase over x, y per shift, and the row's real scale.
 template <int NS>
 struct RowFactor {
   float2 ph[NS];
   float2 phm[NS];
-  float comp;  // (sinc(kx / 2pi) sinc(ky / 2pi))^-p (1 without compensation)
+  float scale;  // (sinc(kx / 2pi) sinc(ky / 2pi))^-p / I (1 / I without compensation)
 };
 
 template <int NS, bool FULL>
@@ -88,46 +88,36 @@ __device__ __forceinline__ void row_factor(const FourierParams &p, int i, int j,
   const float inv = 1.f / p.interlacing;
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
-    const float2 e = expi(p.shifts[s] * kxy);
-    r.ph[s] = make_float2(e.x * inv, e.y * inv);
-    if (full) {
-      const float2 m = expi(-p.shifts[s] * kxym);
-      r.phm[s] = make_float2(m.x * inv, m.y * inv);
-    }
+    r.ph[s] = expi(p.shifts[s] * kxy);
+    if (full) r.phm[s] = expi(-p.shifts[s] * kxym);
   }
-  r.comp = p.comp_order > 0 ? inverse_power(__fmul_rn(sinc_of(k0), sinc_of(k1)), p.comp_order) : 1.f;
+  r.scale = (p.comp_order > 0 ? inverse_power(__fmul_rn(sinc_of(k0), sinc_of(k1)), p.comp_order) : 1.f) * inv;
 }
 
-// Interlaced + compensated value of stored mode (row r, z).
+// Interlaced + compensated value of stored mode (row r, z): shift 0 has phase 1, so its
+// value enters as is; the others are rotated by their phase; the sum is scaled once by the
+// window and 1 / I.
 template <int NS, bool FULL>
 __device__ __forceinline__ float2 combine_mode(const FourierParams &p, const RowFactor<NS> &r,
                                                const ZTable &t, const float2 *__restrict__ in,
                                                int64_t idx, int z) {
   constexpr bool full = FULL;
-  float2 acc;
-  if (NS == 1) {
-    acc = in[idx];
-  } else {
-    acc = make_float2(0.f, 0.f);
+  float2 acc = in[idx];
+  const int64_t mesh = p.d.ncomplex();
 #pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      const float2 v = in[(int64_t)s * p.d.ncomplex() + idx];
-      float2 ph = cmul(r.ph[s], t.ph[s * p.d.nz + z]);
-      if (full) {  // Hermitian part of the full-grid phase: (e^{i t(k)} + e^{-i t(-k)}) / 2
-        const float2 m = cmul(r.phm[s], t.phm[s * p.d.nz + z]);
-        ph = make_float2(0.5f * (ph.x + m.x), 0.5f * (ph.y + m.y));
-      }
-      const float2 c = cmul(v, ph);
-      acc.x += c.x;
-      acc.y += c.y;
+  for (int s = 1; s < NS; ++s) {
+    const float2 v = in[s * mesh + idx];
+    float2 ph = cmul(r.ph[s], t.ph[s * p.d.nz + z]);
+    if (full) {  // Hermitian part of the full-grid phase: (e^{i t(k)} + e^{-i t(-k)}) / 2
+      const float2 m = cmul(r.phm[s], t.phm[s * p.d.nz + z]);
+      ph = make_float2(0.5f * (ph.x + m.x), 0.5f * (ph.y + m.y));
     }
+    const float2 c = cmul(v, ph);
+    acc.x += c.x;
+    acc.y += c.y;
   }
-  if (p.comp_order > 0) {
-    const float c = r.comp * t.comp[z];
-    acc.x *= c;
-    acc.y *= c;
-  }
-  return acc;
+  const float c = r.scale * t.comp[z];
+  return make_float2(acc.x * c, acc.y * c);
 }
 
 // Fill the per-CTA kz table (all threads of the block; call __syncthreads() after).
