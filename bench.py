@@ -258,7 +258,7 @@ def run_batched(nmocks=256, fp64_subset=3, group=32):
                                                              compensate=True, out='complex')
         return np.array([p.num_raw for p in jp.compute_mesh2_spectrum(mesh, bin=bins[n], los='z')])
 
-    for i in range(3):
+    for i in range(nmocks):  # warm-up pass: plans, tile autotuning per (mesh, particle-count) key
         plain(i)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -378,8 +378,10 @@ def run_cutsky(reps=3):
     ad = float((grad.double() * v.double()).sum())
     consistency = float(abs(value.item() - float(
         (coef.cpu().numpy() * np.array([p.num_raw for p in poles])).sum() * scale)))
+    from jaxpower_b200.mesh2 import _term_batches
     return dict(C, ndata=int(data.shape[0]), nrandoms=int(randoms.shape[0]), boxsize=[float(x) for x in attrs.boxsize],
-                nbins=int(b.nbins), spectra_per_s=1. / t_fwd, seconds_forward=t_fwd,
+                nbins=int(b.nbins), term_batches=[len(t) for t in _term_batches(attrs, C['ells'])],
+                spectra_per_s=1. / t_fwd, seconds_forward=t_fwd,
                 seconds_forward_backward=t_grad, norm=float(np.mean(norm)),
                 shotnoise_ell0=float(np.mean(shotnoise[0])) if np.ndim(shotnoise) > 1 else float(np.mean(shotnoise)),
                 gradient_check={'directional_ad': ad, 'directional_fd': fd, 'rel_err': abs(ad - fd) / abs(fd),

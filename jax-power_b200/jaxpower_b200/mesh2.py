@@ -359,13 +359,18 @@ def _firstpoint_terms(ells):
     return [(ell, m) for ell in ells if ell > 0 for m in range(-ell, ell + 1)]
 
 
+def _free_device_memory():
+    """Bytes free on the device plus those torch's caching allocator holds unused."""
+    free, _ = torch.cuda.mem_get_info()
+    return free + torch.cuda.memory_reserved() - torch.cuda.memory_allocated()
+
+
 def _term_batch(mattrs, nterms):
     """How many (ell, m) terms to transform at once, given free device memory."""
     nr = int(np.prod(mattrs.meshsize))
     nc = int(mattrs.meshsize[0]) * int(mattrs.meshsize[1]) * (int(mattrs.meshsize[2]) // 2 + 1)
     per_term = 4 * nr + 8 * nc
-    free, _ = torch.cuda.mem_get_info()
-    return int(max(1, min(nterms, 32, (0.4 * free) // per_term)))
+    return int(max(1, min(nterms, 32, (0.4 * _free_device_memory()) // per_term)))
 
 
 def _term_batches(mattrs, ells):
@@ -446,7 +451,7 @@ def _spectrum_sums(mattrs, bin, los, rmesh=None, cmesh=None, cmesh2=None, rmesh2
                                device=rho.device)
             if keep is not None:
                 per_term = 8 * A0.numel()
-                if len(terms) * per_term < torch.cuda.mem_get_info()[0] / 3:
+                if len(terms) * per_term < _free_device_memory() / 3:
                     keep['A0'], keep['F'] = A0, []
                 else:
                     keep = None

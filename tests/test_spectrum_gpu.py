@@ -61,11 +61,14 @@ def _random_field(meshsize, boxsize, seed=0, n=200000):
     return pos
 
 
+# (64, 48, 40): short stored rows, the flat-chunk binning kernel; (24, 16, 256): long rows
+# (129 stored modes), the row-run kernel
+@pytest.mark.parametrize('meshsize', [(64, 48, 40), (24, 16, 256)])
 @pytest.mark.parametrize('los', ['x', 'z', (0.2, 0.3, 0.9327379053088815)])
 @pytest.mark.parametrize('out', ['real', 'complex'])
-def test_global_los_matches_oracle(los, out):
+def test_global_los_matches_oracle(los, out, meshsize):
     jp = _jp()
-    meshsize, boxsize, step = (64, 48, 40), np.array([1000., 800., 700.]), 0.01
+    boxsize, step = np.array([1000., 800., 700.]), 0.01
     pos = _random_field(meshsize, boxsize, seed=1)
     attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize)
     mesh = jp.ParticleField(pos, attrs=attrs).paint(resampler='tsc', interlacing=3, compensate=True, out=out)
