@@ -8,10 +8,19 @@ reference's tests use: ``value()`` = (num_raw - num_shotnoise) / norm (the
 normalisation that reproduces the reference's golden ``value().std()``),
 ``clone(norm=..., num_shotnoise=...)``, ``get(ells=...)``, ``values(name)``,
 ``coords('k')``, ``ells``.  Arrays are NumPy float64 on the host.
+
+On disk (``write`` / ``read``, the names lsstypes exports and ``types.py:5-7`` re-exports):
+lsstypes' own HDF5 layout is not available here (neither lsstypes nor h5py is installed),
+so an observable is stored as one NumPy ``.npz`` archive of its state: the class name, the
+multipoles, and per pole every field, ``ell`` and ``attrs`` (as JSON).  ``read`` gives back
+an object equal field for field.
 """
+import json
+
 import numpy as np
 
-__all__ = ['Mesh2SpectrumPole', 'Mesh2SpectrumPoles', 'Mesh2CorrelationPole', 'Mesh2CorrelationPoles']
+__all__ = ['Mesh2SpectrumPole', 'Mesh2SpectrumPoles', 'Mesh2CorrelationPole', 'Mesh2CorrelationPoles',
+           'read', 'write']
 
 
 class Mesh2SpectrumPole:
@@ -54,6 +63,18 @@ class Mesh2SpectrumPole:
     def __repr__(self):
         return 'Mesh2SpectrumPole(ell={}, nbins={})'.format(self.ell, self.k.size)
 
+    def state(self):
+        state = {name: getattr(self, name) for name in self._fields}
+        state.update(ell=self.ell, attrs=self.attrs)
+        return state
+
+    @classmethod
+    def from_state(cls, state):
+        return cls(**state)
+
+    def write(self, filename):
+        write(filename, self)
+
 
 class Mesh2SpectrumPoles:
 
@@ -93,6 +114,9 @@ class Mesh2SpectrumPoles:
     def __repr__(self):
         return 'Mesh2SpectrumPoles(ells={})'.format(self.ells)
 
+    def write(self, filename):
+        write(filename, self)
+
 
 class Mesh2CorrelationPole(Mesh2SpectrumPole):
     """Correlation-function multipole: ``s``, ``s_edges`` in place of ``k``, ``k_edges``."""
@@ -116,3 +140,67 @@ class Mesh2CorrelationPoles(Mesh2SpectrumPoles):
 
     def __repr__(self):
         return 'Mesh2CorrelationPoles(ells={})'.format(self.ells)
+
+
+_CLASSES = {cls.__name__: cls for cls in (Mesh2SpectrumPole, Mesh2SpectrumPoles, Mesh2CorrelationPole,
+                                          Mesh2CorrelationPoles)}
+_POLE_OF = {'Mesh2SpectrumPoles': Mesh2SpectrumPole, 'Mesh2CorrelationPoles': Mesh2CorrelationPole}
+
+
+def _pole_arrays(prefix, pole):
+    out = {}
+    for name, value in pole.state().items():
+        if name == 'attrs':
+            out[prefix + 'attrs'] = np.array(json.dumps(value, default=lambda o: np.asarray(o).tolist()))
+        elif value is None:
+            out[prefix + name + '.none'] = np.array(True)
+        else:
+            out[prefix + name] = np.asarray(value)
+    return out
+
+
+def _pole_state(prefix, archive):
+    state = {}
+    for key in archive.files:
+        if not key.startswith(prefix):
+            continue
+        name = key[len(prefix):]
+        if name == 'attrs':
+            state['attrs'] = json.loads(str(archive[key]))
+        elif name.endswith('.none'):
+            state[name[:-len('.none')]] = None
+        elif name == 'ell':
+            state['ell'] = int(archive[key])
+        elif name == 'volume':
+            state['volume'] = archive[key][()] if archive[key].ndim == 0 else archive[key]
+        else:
+            state[name] = archive[key]
+    return state
+
+
+def write(filename, observable):
+    """Save a (list of) multipole(s) to ``filename`` (NumPy ``.npz``)."""
+    name = type(observable).__name__
+    if name not in _CLASSES:
+        raise TypeError('cannot write {}'.format(type(observable)))
+    arrays = {'__class__': np.array(name)}
+    if isinstance(observable, Mesh2SpectrumPoles):
+        arrays['__npoles__'] = np.array(len(observable))
+        for i, pole in enumerate(observable):
+            arrays.update(_pole_arrays('pole{:d}/'.format(i), pole))
+    else:
+        arrays.update(_pole_arrays('pole/', observable))
+    with open(filename, 'wb') as f:
+        np.savez(f, **arrays)
+
+
+def read(filename):
+    """Load what ``write`` saved."""
+    with np.load(filename, allow_pickle=False) as archive:
+        name = str(archive['__class__'])
+        if name in _POLE_OF:
+            pole_cls = _POLE_OF[name]
+            poles = [pole_cls.from_state(_pole_state('pole{:d}/'.format(i), archive))
+                     for i in range(int(archive['__npoles__']))]
+            return _CLASSES[name](poles)
+        return _CLASSES[name].from_state(_pole_state('pole/', archive))

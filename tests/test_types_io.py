@@ -1,0 +1,57 @@
+"""Observable I/O: write / read round trips of the multipole containers (CPU)."""
+import numpy as np
+
+from jaxpower_b200.types import (Mesh2SpectrumPole, Mesh2SpectrumPoles, Mesh2CorrelationPole,
+                                 Mesh2CorrelationPoles, read, write)
+
+
+def _poles(cls_pole, cls_poles, rng):
+    edges = np.linspace(0., 0.2, 11)
+    poles = []
+    for ell in (0, 2, 4):
+        num = rng.normal(size=10) + (1j * rng.normal(size=10) if ell == 2 else 0.)
+        poles.append(cls_pole(0.5 * (edges[:-1] + edges[1:]), np.column_stack([edges[:-1], edges[1:]]),
+                              rng.integers(1, 100, 10), num, num_shotnoise=(3. if ell == 0 else 0.),
+                              norm=2.5, volume=1e9, ell=ell, attrs={'los': 'firstpoint', 'meshsize': [64, 64, 64]}))
+    return cls_poles(poles)
+
+
+def _same(a, b):
+    assert type(a) is type(b)
+    assert a.ells == b.ells
+    for p, q in zip(a, b):
+        for name in p._fields:
+            x, y = getattr(p, name), getattr(q, name)
+            if x is None:
+                assert y is None
+            else:
+                assert np.array_equal(np.asarray(x), np.asarray(y)), name
+        assert p.ell == q.ell and p.attrs == q.attrs
+        assert np.array_equal(p.value(), q.value())
+
+
+def test_write_read_spectrum_poles(tmp_path):
+    poles = _poles(Mesh2SpectrumPole, Mesh2SpectrumPoles, np.random.default_rng(0))
+    fn = str(tmp_path / 'poles.npz')
+    poles.write(fn)
+    _same(poles, read(fn))
+    single = poles.get(2)
+    write(str(tmp_path / 'pole.npz'), single)
+    back = read(str(tmp_path / 'pole.npz'))
+    assert isinstance(back, Mesh2SpectrumPole) and back.ell == 2
+    assert np.array_equal(back.num_raw, single.num_raw)
+
+
+def test_write_read_correlation_poles(tmp_path):
+    poles = _poles(Mesh2CorrelationPole, Mesh2CorrelationPoles, np.random.default_rng(1))
+    fn = str(tmp_path / 'xi.npz')
+    write(fn, poles)
+    back = read(fn)
+    _same(poles, back)
+    assert np.array_equal(back.get(0).s, poles.get(0).s)
+
+
+def test_package_read_is_the_observable_reader():
+    import jaxpower_b200 as jp
+    from jaxpower_b200 import types
+    assert jp.read is types.read and jp.write is types.write
