@@ -150,20 +150,28 @@ __global__ void __launch_bounds__(MLP_WARPS * 32) mlp_forward_kernel(
 }
 
 // ------------------------------------------------------------- tcgen05 forward pass
-// The same network on the 5th-generation tensor cores.  One CTA (4 warps) takes 128
-// samples; each layer is D[128 x N] = A[128 x K] B[N x K]^T with A (bf16 activations) and
-// B (bf16 weights, out x in) in shared memory in the no-swizzle K-major canonical layout
-// and D (float32) in tensor memory: one elected thread issues the K / 16
+// The same network on the 5th-generation tensor cores.  One CTA (8 warps, two warpgroups)
+// takes 128 samples; each layer is D[128 x N] = A[128 x K] B[N x K]^T with A (bf16
+// activations) and B (bf16 weights, out x in) in shared memory in the no-swizzle K-major
+// canonical layout and D (float32) in tensor memory: one elected thread issues the K / 16
 // tcgen05.mma.kind::f16 instructions and commits them to an mbarrier; after the (bounded)
-// wait, warp w reads rows 32w..32w+31 of D with tcgen05.ld, adds the bias, applies SiLU
-// and writes the next layer's bf16 operand back to shared memory.  CTAs are persistent
-// (two per SM): the weights are loaded into shared memory once per CTA.
+// wait, warp w reads rows 32 (w % 4) .. +31 of D (its warpgroup's lane quarter) and columns
+// 64 (w / 4) .. +63 with tcgen05.ld, adds the bias (shared memory), applies SiLU and writes
+// the next layer's bf16 operand back to shared memory.  The epilogue is the longest part of
+// a layer, so the two warpgroups split its columns.  CTAs are persistent (two per SM): the
+// weights and biases are loaded into shared memory once per CTA.
+#ifndef PK_TC_GROUPS
+#define PK_TC_GROUPS 2
+#endif
 constexpr int TC_ROWS = 128;
-constexpr int TC_THREADS = 128;
+constexpr int TC_GROUPS = PK_TC_GROUPS;         // warpgroups per CTA, each a share of the columns
+constexpr int TC_THREADS = 128 * TC_GROUPS;
+constexpr int TC_COLS = 128 / TC_GROUPS;         // accumulator columns per warpgroup
+constexpr int TC_FEAT = MLP_IN / TC_GROUPS;      // input features per thread
 constexpr int TC_N3 = 16;  // last layer's N (rows 8..15 of its weight tile are zero)
 constexpr int TC_TMEM_COLS = 128;
 constexpr unsigned TC_WAIT_LIMIT = 1u << 22;  // mbarrier polls before giving up
-constexpr size_t TC_SMEM = 4096 + 32768 + 32768 + 4096 + 4096 + 32768 + 64;
+constexpr size_t TC_SMEM = 4096 + 32768 + 32768 + 4096 + 4096 + 32768 + 3 * 128 * 4 + 64;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -247,16 +255,19 @@ __device__ __forceinline__ void load_canon(unsigned char *dst, const __nv_bfloat
   }
 }
 
-__global__ void __launch_bounds__(TC_THREADS, 1) mlp_forward_tc_kernel(
+__global__ void __launch_bounds__(TC_THREADS, TC_GROUPS >= 4 ? 2 : 1) mlp_forward_tc_kernel(
     const float *__restrict__ X, const int *__restrict__ idx, int batch, const __nv_bfloat16 *__restrict__ Wb,
     const float *__restrict__ Wf, float *__restrict__ y, float *__restrict__ Z, float *__restrict__ H,
     int *__restrict__ status) {
   extern __shared__ __align__(1024) unsigned char tcsm[];
   unsigned char *sW0 = tcsm, *sW1 = sW0 + 4096, *sW2 = sW1 + 32768, *sW3 = sW2 + 32768, *sA0 = sW3 + 4096,
                 *sA = sA0 + 4096;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sA + 32768);
+  float *sBias = reinterpret_cast<float *>(sA + 32768);  // b0, b1, b2
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sBias + 3 * MLP_H);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
   const int tid = threadIdx.x, warp = tid >> 5;
+  const int r = tid & (TC_ROWS - 1);  // this thread's row of the tile (and D lane)
+  const int half = tid >> 7;          // warpgroup: its share of the columns
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
                  "r"(TC_TMEM_COLS)
@@ -271,30 +282,33 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mlp_forward_tc_kernel(
   load_canon(sW1, Wb + OFF_W1, MLP_H, MLP_H, MLP_H);
   load_canon(sW2, Wb + OFF_W2, MLP_H, MLP_H, MLP_H);
   load_canon(sW3, Wb + OFF_W3, MLP_OUT, TC_N3, MLP_H);
+  for (int q = tid; q < 3 * MLP_H; q += TC_THREADS)
+    sBias[q] = Wf[(q < MLP_H ? OFF_B0 : (q < 2 * MLP_H ? OFF_B1 : OFF_B2)) + q % MLP_H];
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
-  const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+  const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
   const int ntiles = (batch + TC_ROWS - 1) / TC_ROWS;
   bool ok = true;
   uint32_t phase = 0;
   // persistent: the weights stay in shared memory while the CTA walks its 128-row tiles
   for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    const int row = tile * TC_ROWS + tid;  // this thread's sample (and D lane)
-    {  // input features of this thread's sample (bf16, zero past the batch)
+    const int row = tile * TC_ROWS + r;  // this thread's sample
+    {  // input features of this thread's sample, its warpgroup's share (bf16, zero past the batch)
       const bool in = row < batch;
       const float *xr = X + (int64_t)(in ? sample_of(idx, row) : 0) * MLP_IN;
+      const int kc = TC_FEAT * half;
+      unsigned pk[TC_FEAT / 2];
 #pragma unroll
-      for (int kc = 0; kc < MLP_IN; kc += 8) {
-        unsigned pk[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const float a = in ? xr[kc + 2 * q] : 0.f, b = in ? xr[kc + 2 * q + 1] : 0.f;
-          pk[q] = pack_raw(__float2bfloat16_rn(a), __float2bfloat16_rn(b));
-        }
-        *reinterpret_cast<uint4 *>(sA0 + canon_off(tid, kc, MLP_IN)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+      for (int q = 0; q < TC_FEAT / 2; ++q) {
+        const float a = in ? xr[kc + 2 * q] : 0.f, b = in ? xr[kc + 2 * q + 1] : 0.f;
+        pk[q] = pack_raw(__float2bfloat16_rn(a), __float2bfloat16_rn(b));
       }
+      if constexpr (TC_FEAT == 8)
+        *reinterpret_cast<uint4 *>(sA0 + canon_off(r, kc, MLP_IN)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+      else
+        *reinterpret_cast<uint2 *>(sA0 + canon_off(r, kc, MLP_IN)) = make_uint2(pk[0], pk[1]);
     }
     async_proxy_fence();
     tc_fence_before();
@@ -318,8 +332,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mlp_forward_tc_kernel(
       tc_fence_after();
       if (!ok) break;
       if (l < 3) {
-        const float *bias = Wf + (l == 0 ? OFF_B0 : (l == 1 ? OFF_B1 : OFF_B2));
-        for (int c0 = 0; c0 < MLP_H; c0 += 32) {
+        const float *bias = sBias + l * MLP_H;
+        for (int c0 = TC_COLS * half; c0 < TC_COLS * half + TC_COLS; c0 += 32) {
           uint32_t v[32];
           tmem_ld32(lane_addr + (uint32_t)c0, v);
 #pragma unroll
@@ -339,10 +353,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mlp_forward_tc_kernel(
                 H[o + 1] = h1;
               }
             }
-            *reinterpret_cast<uint4 *>(sA + canon_off(tid, c0 + c, MLP_H)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+            *reinterpret_cast<uint4 *>(sA + canon_off(r, c0 + c, MLP_H)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
           }
         }
-      } else {
+      } else if (half == 0) {
         uint32_t v[32];
         tmem_ld32(lane_addr, v);
         if (row < batch) y[row] = __uint_as_float(v[0]) + Wf[OFF_B3];
