@@ -48,14 +48,16 @@ CUTSKY = dict(workload='cut-sky FKP, first-point los, with adjoint: ~2e6 cluster
               k_step=0.005, ell_weights=(1., 0.5, 0.25), fd_step=0.25, seed=11)
 
 # kernel launches issued by each C-ABI entry point (ours, including CUB's scan kernels)
-LAUNCHES = {'pk_paint': 5, 'pk_paint_batch': 5, 'pk_interlace_compensate': 1, 'pk_bin_global': 2, 'pk_bin_firstpoint': 2,
-            'pk_bin_modes': 2, 'pk_bin_mesh': 2, 'pk_scale_real': 1, 'pk_ylm_premultiply': 1, 'pk_read': 1}
+LAUNCHES = {'pk_paint': 5, 'pk_paint_batch': 5, 'pk_interlace_compensate': 1, 'pk_interlace_compensate_batch': 1,
+            'pk_bin_global': 2, 'pk_bin_global_batch': 2, 'pk_bin_global_interlaced': 2, 'pk_bin_firstpoint': 2,
+            'pk_bin_modes': 2, 'pk_bin_mesh': 2, 'pk_scale_real': 1, 'pk_ylm_premultiply': 1, 'pk_read': 1,
+            'pk_read_interlaced': 3}
 
 
 # ncu DRAM read + write of one pk_paint call of the 512^3 workload above (its count and fill
 # bucket passes and the tile pass, one-pass metrics on the full-size workload); the event
 # timing supplies the duration
-PAINT_TRAFFIC_512 = 59694336 + 11008 + 59890688 + 107570176 + 169368576 + 1547861504
+PAINT_TRAFFIC_512 = 59694592 + 19712 + 59912448 + 107955200 + 168512768 + 1549412352
 
 C0 = dict(workload='uniform catalog 1e5 particles in a 1000 Mpc/h cube (seed 0), meshsize 64, CIC, no interlacing, '
                    'compensate, los z, ells (0,2,4), k step 0.01', nparticles=100000, meshsize=64, boxsize=1000.,
