@@ -20,7 +20,8 @@ applies the network only to spectra whose configuration (mesh, box, resampler,
 interlacing, compensation, multipoles, k edges) matches the training one and whose
 features lie inside the training range, and only in bins where, on held-out mocks, the
 corrected spectrum was closer to the fine-mesh result than the plain one (the plain
-estimator is the judge of the network's error).  Elsewhere it returns the plain values.
+estimator is the reference the network's error is measured against).  Elsewhere it
+returns the plain values.
 
 Training catalogs are lognormal mocks generated on the GPU by ``mock.lognormal_particles``
 and measured at both resolutions by ``batch.BatchedSpectra``.

@@ -3,7 +3,7 @@
 Bin membership (|k| in float32, jnp.digitize against float32 edges) must be
 bit-exact: nmodes and index sums per bin match exactly.  P_ell must agree with
 the oracle's float64 accumulation of the same float32 per-mode products within
-1e-5 relative (north-star tolerance), measured against max |P_0|.
+1e-5 relative, measured against max |P_0|.
 """
 import json
 import os
