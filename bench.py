@@ -673,16 +673,41 @@ def run_ours(args):
     # ---- end to end: pinned host positions -> device each step, multipoles back to host
     e2e_value = None
     if not args.no_e2e:
+        # every step copies its positions from pinned host memory and reads its multipoles
+        # back to the host; the copy of step k + 1 runs on a copy stream while step k computes
+        # (two device buffers, events order the copy after the step that last used the buffer)
         host = torch.empty(positions.shape, dtype=torch.float32, pin_memory=True)
         host.copy_(positions)
-        for _ in range(args.warmup):
-            step(host.to('cuda', non_blocking=True))
+        bufs = [torch.empty_like(positions) for _ in range(2)]
+        copied = [torch.cuda.Event() for _ in range(2)]
+        used = [torch.cuda.Event() for _ in range(2)]
+        copy_stream = torch.cuda.Stream()
+        compute = torch.cuda.current_stream()
+
+        def issue_copy(k):
+            with torch.cuda.stream(copy_stream):
+                copy_stream.wait_event(used[k % 2])
+                bufs[k % 2].copy_(host, non_blocking=True)
+                copied[k % 2].record(copy_stream)
+
+        def run_steps(n):
+            copy_stream.wait_stream(compute)  # the first copy starts after the timing event
+            issue_copy(0)
+            for k in range(n):
+                if k + 1 < n:
+                    issue_copy(k + 1)
+                compute.wait_event(copied[k % 2])
+                res = step(bufs[k % 2])
+                used[k % 2].record(compute)
+                _ = res.value()
+
+        for e in used:
+            e.record(compute)
+        run_steps(args.warmup)
         barrier()
         start2, end2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start2.record()
-        for _ in range(args.steps):
-            res = step(host.to('cuda', non_blocking=True))
-            _ = res.value()
+        run_steps(args.steps)
         end2.record()
         torch.cuda.synchronize()
         elapsed2 = max_over_ranks(start2.elapsed_time(end2) / 1e3)
