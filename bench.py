@@ -123,6 +123,8 @@ def algorithmic_bytes(name, npart, meshsize, interlacing, nells):
         return 8. * nc * (interlacing + 1)
     if name in ('pk_bin_global', 'pk_bin_mesh'):
         return 8. * nc
+    if name == 'pk_bin_global_interlaced':  # the shifted meshes read once
+        return 8. * nc * interlacing
     return None
 
 
@@ -719,7 +721,7 @@ def run_ours(args):
     ours = {k: v for k, v in stages.items() if k != 'pk_fft_exec' and k in LAUNCHES}
     dominant = max(ours, key=lambda k: ours[k]['total_ms'])
     abytes = algorithmic_bytes(dominant, npart, W['meshsize'], W['interlacing'], len(W['ells']))
-    achieved = abytes / (ours[dominant]['mean_ms'] * 1e-3) / 1e9
+    achieved = abytes / (ours[dominant]['mean_ms'] * 1e-3) / 1e9 if abytes else None
     launches = sum(LAUNCHES.get(k, 0) * v['calls'] for k, v in stages.items())
     stage_report = {k: {'calls': v['calls'], 'mean_ms': round(v['mean_ms'], 4),
                         'share': round(v['total_ms'] / (elapsed * 1e3), 4)} for k, v in stages.items()}
@@ -729,7 +731,7 @@ def run_ours(args):
             'config': dict(W, nparticles=int(npart), parallelism='replicas' if world > 1 else 'single',
                            l2='inputs larger than L2 (512 MiB meshes per shift)', out='complex'),
             'roofline': {'bound': 'hbm', 'kernel': dominant, 'achieved': achieved, 'peak': peak,
-                         'peak_kind': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak,
+                         'peak_kind': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak if achieved else None,
                          'algorithmic_bytes': abytes,
                          'traffic': float(PAINT_TRAFFIC_512) if (dominant in ('pk_paint', 'pk_paint_batch')
                                                                  and W['meshsize'] == 512) else None,

@@ -108,6 +108,31 @@ def test_firstpoint_matches_oracle(los, cross):
         assert np.allclose(got, ref['num_raw'][i], rtol=0, atol=RTOL * scale), (ell, np.abs(got - ref['num_raw'][i]).max() / scale)
 
 
+@pytest.mark.parametrize('los', ['z', 'firstpoint'])
+@pytest.mark.parametrize('meshsize', [(32, 24, 20), (16, 16, 200)])
+def test_nonuniform_edges_match_oracle(los, meshsize):
+    """Explicit, non-uniform k edges (no step: bins found by binary search on the exact |k|^2
+    thresholds), starting above k = 0 and ending below k_Nyq, so modes fall on both sides."""
+    jp = _jp()
+    boxsize, boxcenter = np.array([600., 500., 400.]), (0. if los == 'z' else 700.)
+    rng = np.random.default_rng(9)
+    value = rng.normal(size=meshsize).astype('f4')
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=boxcenter)
+    kny = float(np.pi * min(np.asarray(meshsize) / boxsize))
+    edges = np.unique(np.concatenate([[0.013], 0.013 + np.cumsum(rng.uniform(0.005, 0.03, 40))]))
+    edges = edges[edges < 0.9 * kny].astype('f8')
+    b = jp.BinMesh2SpectrumPoles(attrs, edges=edges, ells=(0, 2, 4))
+    res = jp.compute_mesh2_spectrum(jp.RealMeshField(torch.as_tensor(value).cuda(), attrs=attrs), bin=b, los=los)
+    geom = Geometry(meshsize, boxsize, boxcenter)
+    ob = Bins(geom, edges=edges, ells=(0, 2, 4))
+    assert np.array_equal(b.nmodes, ob.nmodes)
+    ref = ospectrum(value, ob, los=los)
+    scale = np.abs(ref['num_raw'][0]).max()
+    for i, ell in enumerate(ob.ells):
+        got = res.get(ell).num_raw
+        assert np.allclose(got, ref['num_raw'][i], rtol=0, atol=RTOL * scale), (ell, np.abs(got - ref['num_raw'][i]).max() / scale)
+
+
 def test_paint_jit_golden_gpu():
     """tests/test_mesh.py:211: mesh.std() of TSC / interlacing 3 / compensated paint."""
     jp = _jp()
