@@ -770,13 +770,18 @@ struct GlobalSmem {
 // NS > 0: the mesh is not stored; each mode is formed on the fly from NS interlaced,
 // uncompensated meshes at d1 (mesh s at d1 + s N_c), exactly as pk_interlace_compensate
 // forms it (fp: its parameters; FULL: 'jaxdecomp' semantics), which saves writing and
-// reading back the combined mesh (that form gets a larger register budget: 3 CTAs per SM
-// instead of 4, the fastest of 2 / 3 / 4 measured at 128^3 batches and 512^3).
+// reading back the combined mesh.  MINB: CTAs per SM the register budget is sized for.  The
+// fused form of a single mesh takes 3 (512^3, 3 shifts: 0.83 ms against 0.89 with 4 and 0.93
+// with 2), batches of meshes 4 (29 x 192^3, 2 shifts: 1.58 ms against 1.78 with 3; 32 x 256^3:
+// 3.34 against 3.76).
 #ifndef PK_FUSED_MIN_CTAS
 #define PK_FUSED_MIN_CTAS 3
 #endif
-template <int NV, bool CROSS, bool EVEN, int NS = 0, bool FULL = false>
-__global__ void __launch_bounds__(BIN_THREADS, NS > 0 ? PK_FUSED_MIN_CTAS : 4) bin_global_kernel(
+#ifndef PK_FUSED_BATCH_MIN_CTAS
+#define PK_FUSED_BATCH_MIN_CTAS 4
+#endif
+template <int NV, bool CROSS, bool EVEN, int NS = 0, bool FULL = false, int MINB = (NS > 0 ? PK_FUSED_MIN_CTAS : 4)>
+__global__ void __launch_bounds__(BIN_THREADS, MINB) bin_global_kernel(
     BinGeom g, const float2 *__restrict__ d1, const float2 *__restrict__ d2, float lx, float ly,
     float lz, LegendreCoefs lc, int zero_l0, const float *__restrict__ edges, int nwarps_hist,
     int tab, double *__restrict__ partials, FourierParams fp) {
@@ -1189,10 +1194,13 @@ static pk_status launch_global(cudaStream_t st, const BinGeom &g, const float2 *
     kernel<<<dim3(blocks, nbatch), L.nwarps * 32, L.smem, st>>>(g, d1, d2, los[0], los[1], los[2], lc, zero_l0,
                                                                edges, L.nwarps, cpw, partials, fpv);
   } else {
-    PK_CUDA(cudaFuncSetAttribute(bin_global_kernel<NV, CROSS, EVEN, NS, FULL>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
-    bin_global_kernel<NV, CROSS, EVEN, NS, FULL><<<dim3(L.blocks, nbatch), L.nwarps * 32, L.smem, st>>>(
-        g, d1, d2, los[0], los[1], los[2], lc, zero_l0, edges, L.nwarps, L.tab, partials, fpv);
+    constexpr int MINB1 = NS > 0 ? PK_FUSED_MIN_CTAS : 4;
+    constexpr int MINB2 = NS > 0 ? PK_FUSED_BATCH_MIN_CTAS : 4;
+    auto kernel = nbatch > 1 ? bin_global_kernel<NV, CROSS, EVEN, NS, FULL, MINB2>
+                             : bin_global_kernel<NV, CROSS, EVEN, NS, FULL, MINB1>;
+    PK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
+    kernel<<<dim3(L.blocks, nbatch), L.nwarps * 32, L.smem, st>>>(g, d1, d2, los[0], los[1], los[2], lc, zero_l0,
+                                                                  edges, L.nwarps, L.tab, partials, fpv);
   }
   PK_LAUNCH_CHECK();
   launch_finalize(st, partials, blocks, hist_len, NV, g.nedges - 1, 0, out, nullptr, nbatch);
