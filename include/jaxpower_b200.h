@@ -67,9 +67,10 @@ pk_status pk_paint(void *stream, const float *positions, const float *weights, i
 /* Batched paint of nmocks catalogs on the same mesh geometry in one set of launches:
  * positions / weights are concatenated, d_offsets (device, int64, nmocks + 1) gives
  * each catalog's range; out[(m * nshifts + j) * N0*N1*N2 + ...].  tile_config
- * (0..3) selects the tile shape / CTA size (0: 8x16x32 cells, 512 threads; 1: 8x16x32,
- * 256; 2: 8x8x32, 256; 3: 4x16x32, 256), for an autotuner.  pk_paint is the nmocks = 1,
- * tile_config = 0 case. */
+ * (0..7) selects the tile shape / CTA size (0: 8x16x32 cells, 512 threads; 1: 8x16x32,
+ * 256; 2: 8x8x32, 256; 3: 4x16x32, 256; 4..7: the same with shared-memory rows swizzled
+ * against bank conflicts), for an autotuner; every configuration paints the same bits.
+ * pk_paint is the nmocks = 1, tile_config = 4 case. */
 pk_status pk_paint_batch_workspace_size(int64_t n, int nmocks, const int32_t meshsize[3],
                                         int order, int nshifts, int tile_config, size_t *bytes);
 pk_status pk_paint_batch(void *stream, const float *positions, const float *weights,

@@ -13,7 +13,7 @@ import threading
 
 import torch
 
-NUM_TILE_CONFIGS = 4
+NUM_TILE_CONFIGS = 8
 _cache = {}
 _lock = threading.Lock()
 

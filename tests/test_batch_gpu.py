@@ -16,7 +16,7 @@ def _mocks(counts, boxsize, seed=0):
     return [(rng.uniform(-0.5, 0.5, (c, 3)) * boxsize).astype('f4') for c in counts]
 
 
-@pytest.mark.parametrize('tile_config', [0, 1, 2, 3, None])
+@pytest.mark.parametrize('tile_config', [0, 1, 2, 3, 4, 6, None])
 def test_batched_matches_single(tile_config):
     import jaxpower_b200 as jp
     from jaxpower_b200.batch import BatchedSpectra

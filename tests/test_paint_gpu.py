@@ -178,7 +178,7 @@ def test_paint_same_bits_for_every_tile_config(resampler):
     w = torch.as_tensor(w).cuda()
     status = torch.zeros(1, dtype=torch.int32, device='cuda')
     outs = []
-    for config in range(4):
+    for config in range(8):
         out = torch.empty((3,) + tuple(attrs.meshsize), dtype=torch.float32, device='cuda')
         _paint_call(attrs, pos, w, order, 3, 0, 3, out, status, config)
         outs.append(out)
