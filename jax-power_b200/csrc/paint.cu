@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
   // Per-cell 64-bit fixed point as two 32-bit words (native shared atomics): the low word's
   // returned old value gives the exact carry into the high word, so the integer sum stays
   // exact and independent of the order of the additions.
-  extern __shared__ __align__(16) unsigned acc32[];  // lo[nshifts][CELLS], hi[nshifts][CELLS], scratch[64]
+  extern __shared__ __align__(16) unsigned acc32[];  // lo[nshifts][CELLS], scratch[32], hi[nshifts][CELLS], scratch[32]
   const int64_t gtile = blockIdx.x;
   const int mock = (int)(gtile / g.tiles_per_mock);
   const int tile = (int)(gtile % g.tiles_per_mock);
@@ -368,7 +368,7 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
   if (count > 0) {
     {
       uint4 *z4 = reinterpret_cast<uint4 *>(acc32);  // 2 nshifts CELLS words, CELLS % 4 == 0
-      for (int i = threadIdx.x; i < (2 * g.nshifts * CELLS) / 4; i += blockDim.x) z4[i] = make_uint4(0u, 0u, 0u, 0u);
+      for (int i = threadIdx.x; i < (2 * g.nshifts * CELLS + 64) / 4; i += blockDim.x) z4[i] = make_uint4(0u, 0u, 0u, 0u);
     }
     __syncthreads();
     const long long ncat = g.offsets ? (long long)(g.offsets[mock + 1] - g.offsets[mock]) : (long long)g.n;
@@ -424,9 +424,11 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
             l[d][o] = (loc >= 0 && loc < tl[d]) ? loc : -1;
           }
         }
-        const unsigned dummy = acc_base + 4u * (unsigned)(2 * g.nshifts * CELLS + (threadIdx.x & 31));
+        // layout: lo[nshifts][CELLS], 32 scratch words, hi[nshifts][CELLS], 32 scratch words, so
+        // that every high word (scratch included) sits a fixed distance after its low word
+        const unsigned dummy = acc_base + 4u * (unsigned)(g.nshifts * CELLS + (threadIdx.x & 31));
+        const unsigned hi_delta = 4u * (unsigned)(g.nshifts * CELLS + 32);
         const unsigned lo_base = acc_base + 4u * (unsigned)(s * CELLS);
-        const unsigned hi_base = acc_base + 4u * (unsigned)((g.nshifts + s) * CELLS);
 #pragma unroll
         for (int a = 0; a < ORDER; ++a) {
 #pragma unroll
@@ -444,8 +446,9 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
               // invalid cells go to this lane's scratch words (never read): no branch, and
               // the scratch words of a warp sit in distinct banks
               const unsigned off = 4u * (unsigned)(rowoff + (l[2][c] ^ sw));
-              const unsigned old = atom_add_shared(valid ? lo_base + off : dummy, lo);
-              red_add_shared(valid ? hi_base + off : dummy + 128u, (unsigned)((int)(fx >> 32) + (old + lo < old ? 1 : 0)));
+              const unsigned addr = valid ? lo_base + off : dummy;
+              const unsigned old = atom_add_shared(addr, lo);
+              red_add_shared(addr + hi_delta, (unsigned)((int)(fx >> 32) + (old + lo < old ? 1 : 0)));
             }
           }
         }
@@ -456,7 +459,7 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
     for (int s = 0; s < g.nshifts; ++s) {
       float *mesh = mock_out + (int64_t)s * g.d.nreal();
       const unsigned *alo = acc32 + s * CELLS;
-      const unsigned *ahi = acc32 + (g.nshifts + s) * CELLS;
+      const unsigned *ahi = acc32 + g.nshifts * CELLS + 32 + s * CELLS;
       for (int i = threadIdx.x * 4; i < CELLS; i += blockDim.x * 4) {
         const int c2 = i % T2, c1 = (i / T2) % T1, c0 = i / (T2 * T1);
         const int x0 = los[0] + c0, x1 = los[1] + c1, x2 = los[2] + c2;
