@@ -310,6 +310,13 @@ __device__ __forceinline__ void red_add_shared(unsigned addr, unsigned v) {
   asm volatile("red.shared.add.u32 [%0], %1;" : : "r"(addr), "r"(v) : "memory");
 }
 
+// hi + the carry out of old + lo (the low word's addition), with the add's carry flag.
+__device__ __forceinline__ unsigned add_carry_hi(unsigned old, unsigned lo, unsigned hi) {
+  unsigned r;
+  asm("{\n\t.reg .u32 t;\n\tadd.cc.u32 t, %1, %2;\n\taddc.u32 %0, %3, 0;\n\t}" : "=r"(r) : "r"(old), "r"(lo), "r"(hi));
+  return r;
+}
+
 // bspline() for a compile-time order with both polynomial pieces evaluated and selected
 // (same float32 operations as bspline(), no data-dependent branch).
 template <int ORDER>
@@ -429,26 +436,31 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
         const unsigned dummy = acc_base + 4u * (unsigned)(g.nshifts * CELLS + (threadIdx.x & 31));
         const unsigned hi_delta = 4u * (unsigned)(g.nshifts * CELLS + 32);
         const unsigned lo_base = acc_base + 4u * (unsigned)(s * CELLS);
+        unsigned zoff[ORDER];  // byte offset of each stencil z in a row
+        bool zin[ORDER];
+#pragma unroll
+        for (int c = 0; c < ORDER; ++c) {
+          zoff[c] = 4u * (unsigned)l[2][c];
+          zin[c] = l[2][c] >= 0;
+        }
 #pragma unroll
         for (int a = 0; a < ORDER; ++a) {
 #pragma unroll
           for (int b = 0; b < ORDER; ++b) {
             const float kab = __fmul_rn(k[0][a], k[1][b]);
             const bool vab = has && (l[0][a] | l[1][b]) >= 0;
-            const int rowoff = (l[0][a] * T1 + l[1][b]) * T2;
-            const int sw = paint_swizzle<TC::SWZ>(l[0][a], l[1][b]);
+            const unsigned rowbase = lo_base + 4u * (unsigned)((l[0][a] * T1 + l[1][b]) * T2);
+            const unsigned sw4 = 4u * (unsigned)paint_swizzle<TC::SWZ>(l[0][a], l[1][b]);
 #pragma unroll
             for (int c = 0; c < ORDER; ++c) {
-              const bool valid = vab && l[2][c] >= 0;
               const float v = __fmul_rn(wq, __fmul_rn(kab, k[2][c]));  // (w * ker) 2^fexp
               const long long fx = __float2ll_rn(v);
               const unsigned lo = (unsigned)fx;
               // invalid cells go to this lane's scratch words (never read): no branch, and
               // the scratch words of a warp sit in distinct banks
-              const unsigned off = 4u * (unsigned)(rowoff + (l[2][c] ^ sw));
-              const unsigned addr = valid ? lo_base + off : dummy;
+              const unsigned addr = (vab && zin[c]) ? rowbase + (zoff[c] ^ sw4) : dummy;
               const unsigned old = atom_add_shared(addr, lo);
-              red_add_shared(addr + hi_delta, (unsigned)((int)(fx >> 32) + (old + lo < old ? 1 : 0)));
+              red_add_shared(addr + hi_delta, add_carry_hi(old, lo, (unsigned)(fx >> 32)));
             }
           }
         }
