@@ -317,6 +317,32 @@ __device__ __forceinline__ unsigned add_carry_hi(unsigned old, unsigned lo, unsi
   return r;
 }
 
+// bspline() at stencil point O (0 .. ORDER - 1) of a compile-time order.  Which polynomial
+// piece applies is known from O: with i0 = rint(u) (odd order) or floor(u) (even order) the
+// distance s = |i0 + OLO + O - u| lies in [0, 0.5] for TSC's middle point and in [0.5, 1.5]
+// for its outer ones, in [0, 1] for PCS's two middle points and in [1, 2] for its outer ones
+// (float32 rounding cannot cross these representable bounds).  At a shared bound both pieces
+// give the same float32 value (TSC 0.5 at s = 0.5, PCS 1/6 at s = 1), so this equals
+// bspline() bit for bit without evaluating the other piece.
+template <int ORDER, int O>
+__device__ __forceinline__ float bspline_at(float s) {
+  if (ORDER == 1) return 1.f;
+  if (ORDER == 2) return __fsub_rn(1.f, s);
+  if (ORDER == 3) {
+    if (O == 1) return __fsub_rn(0.75f, __fmul_rn(s, s));
+    const float t = __fsub_rn(1.5f, s);
+    return __fmul_rn(0.5f, __fmul_rn(t, t));
+  }
+  const float sixth = 0.16666667f;
+  if (O == 1 || O == 2) {
+    const float s2 = __fmul_rn(s, s);
+    const float s3 = __fmul_rn(s, s2);
+    return __fmul_rn(sixth, __fadd_rn(__fsub_rn(4.f, __fmul_rn(6.f, s2)), __fmul_rn(3.f, s3)));
+  }
+  const float t = __fsub_rn(2.f, s);
+  return __fmul_rn(sixth, __fmul_rn(t, __fmul_rn(t, t)));
+}
+
 // bspline() for a compile-time order with both polynomial pieces evaluated and selected
 // (same float32 operations as bspline(), no data-dependent branch).
 template <int ORDER>
@@ -417,10 +443,13 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
           // tile-relative cell of the first stencil point; stencil stays within one period
           const int w0 = wrapi(i0 + OLO, ns[d]) - los[d];
           const int lim = ns[d] - los[d];
+          k[d][0] = bspline_at<ORDER, 0>(fabsf(__fsub_rn(__fadd_rn(fi0, (float)OLO), u)));
+          if (ORDER > 1) k[d][ORDER > 1 ? 1 : 0] = bspline_at<ORDER, 1>(fabsf(__fsub_rn(__fadd_rn(fi0, (float)(OLO + 1)), u)));
+          if (ORDER > 2) k[d][ORDER > 2 ? 2 : 0] = bspline_at<ORDER, 2>(fabsf(__fsub_rn(__fadd_rn(fi0, (float)(OLO + 2)), u)));
+          if (ORDER > 3) k[d][ORDER > 3 ? 3 : 0] = bspline_at<ORDER, 3>(fabsf(__fsub_rn(__fadd_rn(fi0, (float)(OLO + 3)), u)));
 #pragma unroll
           for (int o = 0; o < ORDER; ++o) {
-            // (float)(i0 + OLO + o) exactly, without an int -> float conversion
-            k[d][o] = bspline_sel<ORDER>(fabsf(__fsub_rn(__fadd_rn(fi0, (float)(OLO + o)), u)));
+            // (float)(i0 + OLO + o) exactly above, without an int -> float conversion
             int loc = w0 + o;
             if (one_wrap) {
               loc -= loc >= lim ? ns[d] : 0;
