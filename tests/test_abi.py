@@ -49,3 +49,32 @@ def test_status_codes_without_gpu(lib):
     assert lib.pk_paint_workspace_size(1000, _lib.i32([0, 64, 64]), 2, 1, ctypes.byref(nbytes)) == 1
     assert lib.pk_bin_workspace_size(_lib.i32([64, 64, 64]), 21, 3, ctypes.byref(nbytes)) in (0, 2)
     assert lib.pk_version().startswith(b'jaxpower_b200')
+
+
+def test_argument_errors_of_later_entries_without_gpu(lib):
+    """Entry points reject bad arguments before any launch (fake, never dereferenced
+    pointers stand for device buffers)."""
+    from jaxpower_b200 import _lib
+    fake = ctypes.c_void_p(4096)
+    nbytes = ctypes.c_size_t()
+    ms = _lib.i32([32, 32, 32])
+    # paint tile configurations 0..7 (4..7 swizzled); 8 is out of range
+    assert lib.pk_paint_batch_workspace_size(1000, 1, ms, 3, 3, 7, ctypes.byref(nbytes)) == 0
+    assert lib.pk_paint_batch_workspace_size(1000, 1, ms, 3, 3, 8, ctypes.byref(nbytes)) == 1
+    geo = (ms, _lib.f32([100.] * 3), _lib.f32([0.] * 3), _lib.f32([100. / 32] * 3), 3)
+    # interlaced read: interlacing out of range, NULL meshes
+    assert lib.pk_read_interlaced(None, fake, 0, fake, None, 10, *geo, 1., fake, fake, 0) == 1
+    assert lib.pk_read_interlaced(None, fake, 9, fake, None, 10, *geo, 1., fake, fake, 0) == 1
+    assert lib.pk_read_interlaced(None, None, 3, fake, None, 10, *geo, 1., fake, fake, 0) == 1
+    assert b'NULL' in lib.pk_last_error() or b'null' in lib.pk_last_error()
+    # Y_lm premultiply: no terms, or an (ell, m) outside |m| <= ell <= 8
+    cs, off = _lib.f32([1.] * 3), _lib.f32([0.] * 3)
+    assert lib.pk_ylm_premultiply(None, fake, ms, cs, off, 0, _lib.i32([2]), _lib.i32([0]), fake) == 1
+    assert lib.pk_ylm_premultiply(None, fake, ms, cs, off, 1, _lib.i32([2]), _lib.i32([3]), fake) == 1
+    assert lib.pk_ylm_premultiply(None, fake, ms, cs, off, 1, _lib.i32([9]), _lib.i32([0]), fake) == 1
+    # first-point binning: too many terms, bad number of multipoles
+    kf, ells = _lib.f32([0.01] * 3), _lib.i32([0, 2, 4])
+    assert lib.pk_bin_firstpoint(None, fake, None, fake, 33, _lib.i32([2] * 33), _lib.i32([0] * 33), ms, kf, fake,
+                                 10, 0.01, 0, 3, ells, 1, 0, fake, fake, 1 << 20) == 1
+    assert lib.pk_bin_firstpoint(None, fake, None, fake, 5, _lib.i32([2] * 5), _lib.i32(range(-2, 3)), ms, kf, fake,
+                                 10, 0.01, 0, 0, ells, 1, 0, fake, fake, 1 << 20) == 1
