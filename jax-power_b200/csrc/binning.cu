@@ -838,8 +838,13 @@ __global__ void __launch_bounds__(BIN_THREADS, MINB) bin_global_kernel(
     for (int c = 0; c < NV; ++c) acc[c] = facc[c] = 0.f;
     const float2 *p1 = d1 + row * g.d.nz;
     const float2 *p2 = CROSS ? d2 + row * g.d.nz : nullptr;
-    // the run's values are loaded RB at a time before use: many loads in flight per lane
-    constexpr int RB = (CROSS || NS > 1) ? 4 : 8;
+    // the run's values are loaded RB at a time before use: several loads in flight per lane
+    // (with 3 shifted meshes, RB = 2 measured 0.81 ms at 512^3 against 0.83 for 4 and 0.91
+    // for 8: the wider batches cost registers)
+#ifndef PK_FUSED_RB
+#define PK_FUSED_RB 2
+#endif
+    constexpr int RB = CROSS ? 4 : (NS > 1 ? PK_FUSED_RB : 8);
     for (int zb = z0; zb < z1; zb += RB) {
       float2 va[RB], vb[CROSS ? RB : 1];
 #pragma unroll

@@ -20,7 +20,7 @@ import torch
 from . import _lib
 from .mesh import (MeshAttrs, BaseMeshField, RealMeshField, ComplexMeshField, ParticleField, FKPField,
                    _r2c, _c2r, _workspace, _device, _paint, get_mesh_attrs)
-from .types import Mesh2SpectrumPole, Mesh2SpectrumPoles, Mesh2CorrelationPole, Mesh2CorrelationPoles
+from .types import Mesh2SpectrumPole, Mesh2SpectrumPoles, Mesh2CorrelationPole, Mesh2CorrelationPoles, DeferredRows
 
 __all__ = ['BinMesh2SpectrumPoles', 'compute_mesh2_spectrum', 'compute_mesh2', 'compute_fkp2_normalization',
            'compute_fkp2_shotnoise', 'compute_box2_normalization', 'compute_normalization',
@@ -524,15 +524,15 @@ def compute_mesh2_spectrum(*meshes, bin=None, los='z'):
     nbins = bin.nbins
     lazy = getattr(meshes[0], 'lazy', None) if fields[1] == fields[0] else None
     if lazy is not None and vlos is not None and _fusable(ells):
-        raw = _interlaced_sums(mattrs, bin, vlos, *lazy).cpu().numpy()
+        raw = _interlaced_sums(mattrs, bin, vlos, *lazy)
     else:
         r1, c1 = _split(meshes[0])
         r2, c2 = (None, None) if fields[1] == fields[0] else _split(meshes[1])
-        raw = _spectrum_sums(mattrs, bin, los, rmesh=r1, cmesh=c1, rmesh2=r2, cmesh2=c2).cpu().numpy()
-    factors = _ell_factors(ells, vlos)
-    num = [raw[i] / bin.nmodes * factors[i] for i in range(len(ells))]
+        raw = _spectrum_sums(mattrs, bin, los, rmesh=r1, cmesh=c1, rmesh2=r2, cmesh2=c2)
+    # the sums stay on the device until num_raw is first read (one read-back for all poles)
+    num = DeferredRows(raw, bin.nmodes, _ell_factors(ells, vlos))
     norm = np.full(nbins, norm_value, dtype='f8')
-    poles = [Mesh2SpectrumPole(k=bin.xavg, k_edges=bin.edges, nmodes=bin.nmodes, num_raw=num[i],
+    poles = [Mesh2SpectrumPole(k=bin.xavg, k_edges=bin.edges, nmodes=bin.nmodes, num_raw=num.row(i),
                                num_shotnoise=np.zeros(nbins), norm=norm,
                                volume=float(np.prod(mattrs.kfun.astype('f8'))) * bin.nmodes, ell=ell, attrs=attrs)
              for i, ell in enumerate(ells)]

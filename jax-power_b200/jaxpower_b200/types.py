@@ -7,7 +7,10 @@ unpinned dependency.  This module keeps the fields the estimator fills
 reference's tests use: ``value()`` = (num_raw - num_shotnoise) / norm (the
 normalisation that reproduces the reference's golden ``value().std()``),
 ``clone(norm=..., num_shotnoise=...)``, ``get(ells=...)``, ``values(name)``,
-``coords('k')``, ``ells``.  Arrays are NumPy float64 on the host.
+``coords('k')``, ``ells``.  Arrays are NumPy float64 on the host.  ``num_raw`` may be given
+as a deferred value (``DeferredRows``): the estimator's per-bin sums stay on the device and
+are read back, once for all multipoles, when ``num_raw`` is first used, so that computing a
+spectrum does not wait for the GPU (as JAX arrays do not).
 
 On disk (``write`` / ``read``, the names lsstypes exports and ``types.py:5-7`` re-exports):
 lsstypes' own HDF5 layout is not available here (neither lsstypes nor h5py is installed),
@@ -20,7 +23,41 @@ import json
 import numpy as np
 
 __all__ = ['Mesh2SpectrumPole', 'Mesh2SpectrumPoles', 'Mesh2CorrelationPole', 'Mesh2CorrelationPoles',
-           'read', 'write']
+           'DeferredRows', 'read', 'write']
+
+
+class DeferredRows:
+    """Rows of a device tensor of per-bin sums, read back to the host on first use.
+
+    ``row(i)`` gives a deferred row: ``scale[i] * sums[i] / divisor`` in float64, computed
+    on the host from the one read-back of the whole tensor that all rows share.
+    """
+
+    def __init__(self, sums, divisor, scales):
+        self._sums = sums
+        self._host = None
+        self._divisor = np.asarray(divisor, dtype='f8')
+        self._scales = list(scales)
+        self.shape = tuple(sums.shape[1:])
+
+    def _read(self):
+        if self._host is None:
+            self._host = self._sums.cpu().numpy()
+            self._sums = None
+        return self._host
+
+    def row(self, i):
+        return _DeferredRow(self, i)
+
+
+class _DeferredRow:
+
+    def __init__(self, rows, i):
+        self.rows, self.i, self.shape = rows, i, rows.shape
+
+    def get(self):
+        r = self.rows
+        return r._read()[self.i] / r._divisor * r._scales[self.i]
 
 
 class Mesh2SpectrumPole:
@@ -32,14 +69,32 @@ class Mesh2SpectrumPole:
         self.k = np.asarray(k, dtype='f8')
         self.k_edges = np.asarray(k_edges, dtype='f8')
         self.nmodes = np.asarray(nmodes, dtype='f8')
-        self.num_raw = np.asarray(num_raw)
+        if isinstance(num_raw, _DeferredRow):
+            self._num_raw, self._deferred = None, num_raw
+            shape = num_raw.shape
+            if num_shotnoise is None or norm is None:
+                shape = self.num_raw.shape  # zeros_like / ones_like need the values' type
+        else:
+            self._num_raw, self._deferred = np.asarray(num_raw), None
+            shape = self._num_raw.shape
         self.num_shotnoise = np.zeros_like(self.num_raw) if num_shotnoise is None else \
-            np.broadcast_to(np.asarray(num_shotnoise), self.num_raw.shape).copy()
+            np.broadcast_to(np.asarray(num_shotnoise), shape).copy()
         self.norm = np.ones_like(self.num_raw, dtype='f8') if norm is None else \
-            np.broadcast_to(np.asarray(norm, dtype='f8'), self.num_raw.shape).copy()
+            np.broadcast_to(np.asarray(norm, dtype='f8'), shape).copy()
         self.volume = volume
         self.ell = int(ell)
         self.attrs = dict(attrs or {})
+
+    @property
+    def num_raw(self):
+        if self._num_raw is None:
+            self._num_raw = np.asarray(self._deferred.get())
+            self._deferred = None
+        return self._num_raw
+
+    @num_raw.setter
+    def num_raw(self, value):
+        self._num_raw, self._deferred = np.asarray(value), None
 
     def value(self):
         return (self.num_raw - self.num_shotnoise) / self.norm
