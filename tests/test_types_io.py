@@ -55,3 +55,28 @@ def test_package_read_is_the_observable_reader():
     import jaxpower_b200 as jp
     from jaxpower_b200 import types
     assert jp.read is types.read and jp.write is types.write
+
+
+def test_deferred_rows_read_once_and_match(tmp_path):
+    """Per-bin sums left on the device are read back on first use, once for all poles, and
+    give the values the eager construction gives."""
+    import torch
+    from jaxpower_b200.types import DeferredRows
+    rng = np.random.default_rng(3)
+    raw = rng.normal(size=(3, 10))
+    nmodes = rng.integers(1, 50, 10).astype('f8')
+    factors = [1., 5., 9.]
+    edges = np.column_stack([np.arange(10.), np.arange(1., 11.)])
+    rows = DeferredRows(torch.as_tensor(raw), nmodes, factors)
+    lazy = Mesh2SpectrumPoles([Mesh2SpectrumPole(np.arange(10.), edges, nmodes, rows.row(i), num_shotnoise=np.zeros(10),
+                                                 norm=np.full(10, 2.), ell=ell) for i, ell in enumerate((0, 2, 4))])
+    eager = Mesh2SpectrumPoles([Mesh2SpectrumPole(np.arange(10.), edges, nmodes, raw[i] / nmodes * factors[i],
+                                                  num_shotnoise=np.zeros(10), norm=np.full(10, 2.), ell=ell)
+                                for i, ell in enumerate((0, 2, 4))])
+    assert rows._host is None  # nothing read yet
+    assert np.array_equal(lazy.get(2).num_raw, eager.get(2).num_raw)
+    assert rows._sums is None and rows._host is not None  # one read-back, tensor released
+    assert np.array_equal(lazy.value(), eager.value())
+    fn = str(tmp_path / 'lazy.npz')
+    lazy.write(fn)
+    _same(eager, read(fn))
