@@ -57,7 +57,7 @@ LAUNCHES = {'pk_paint': 5, 'pk_paint_batch': 5, 'pk_interlace_compensate': 1, 'p
 # ncu DRAM read + write of one pk_paint call of the 512^3 workload above (its count and fill
 # bucket passes and the tile pass, one-pass metrics on the full-size workload); the event
 # timing supplies the duration
-PAINT_TRAFFIC_512 = 59694080 + 20992 + 59942400 + 108002560 + 169201152 + 1547410432
+PAINT_TRAFFIC_512 = 59693824 + 15360 + 59910400 + 107581184 + 168319488 + 1547460096
 
 C0 = dict(workload='uniform catalog 1e5 particles in a 1000 Mpc/h cube (seed 0), meshsize 64, CIC, no interlacing, '
                    'compensate, los z, ells (0,2,4), k step 0.01', nparticles=100000, meshsize=64, boxsize=1000.,
