@@ -343,27 +343,6 @@ __device__ __forceinline__ float bspline_at(float s) {
   return __fmul_rn(sixth, __fmul_rn(t, __fmul_rn(t, t)));
 }
 
-// bspline() for a compile-time order with both polynomial pieces evaluated and selected
-// (same float32 operations as bspline(), no data-dependent branch).
-template <int ORDER>
-__device__ __forceinline__ float bspline_sel(float s) {
-  if (ORDER == 1) return 1.f;
-  if (ORDER == 2) return __fsub_rn(1.f, s);
-  if (ORDER == 3) {
-    const float inner = __fsub_rn(0.75f, __fmul_rn(s, s));
-    const float t = __fsub_rn(1.5f, s);
-    const float outer = __fmul_rn(0.5f, __fmul_rn(t, t));
-    return s <= 0.5f ? inner : outer;
-  }
-  const float sixth = 0.16666667f;
-  const float s2 = __fmul_rn(s, s);
-  const float s3 = __fmul_rn(s, s2);
-  const float inner = __fmul_rn(sixth, __fadd_rn(__fsub_rn(4.f, __fmul_rn(6.f, s2)), __fmul_rn(3.f, s3)));
-  const float t = __fsub_rn(2.f, s);
-  const float outer = __fmul_rn(sixth, __fmul_rn(t, __fmul_rn(t, t)));
-  return s <= 1.f ? inner : outer;
-}
-
 // Shared-memory position of tile cell (x, y, z) in the swizzled configurations: row (x, y)
 // holds its z in an order XORed by a multiple of 4 that varies with the row, so that the same
 // z in neighbouring rows and planes falls in different banks (groups of 4 consecutive z stay
