@@ -780,7 +780,8 @@ struct GlobalSmem {
 #ifndef PK_FUSED_BATCH_MIN_CTAS
 #define PK_FUSED_BATCH_MIN_CTAS 4
 #endif
-template <int NV, bool CROSS, bool EVEN, int NS = 0, bool FULL = false, int MINB = (NS > 0 ? PK_FUSED_MIN_CTAS : 4)>
+template <int NV, bool CROSS, bool EVEN, int NS = 0, bool FULL = false, int MINB = (NS > 0 ? PK_FUSED_MIN_CTAS : 4),
+          bool XY = false>
 __global__ void __launch_bounds__(BIN_THREADS, MINB) bin_global_kernel(
     BinGeom g, const float2 *__restrict__ d1, const float2 *__restrict__ d2, float lx, float ly,
     float lz, LegendreCoefs lc, int zero_l0, const float *__restrict__ edges, int nwarps_hist,
@@ -831,7 +832,7 @@ __global__ void __launch_bounds__(BIN_THREADS, MINB) bin_global_kernel(
     const float kxy = __fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky));
     const float kl = kx * lx + ky * ly;
     RowFactor<NSR> rf;
-    if (NS > 0) row_factor<NSR, FULL>(fp, i, j, rf);
+    if (NS > 0) row_factor<NSR, FULL, XY>(fp, zt, i, j, rf);
     int cur = -1, lead = NONE, trail = NONE, nseg = 0;
     float acc[NV], facc[NV];
 #pragma unroll
@@ -994,7 +995,7 @@ __global__ void __launch_bounds__(BIN_THREADS, MINB) bin_global_kernel(
 // of chunks, bin keys carry the row's low 5 bits, one segmented scan per chunk, and the run
 // tails of different rows add into the warp's float32 histogram one row after the other.
 // A lane recomputes its row's factors (k_x, k_y, phases, window) when it enters a new row.
-template <int NV, bool CROSS, bool EVEN, int NS = 0, bool FULL = false>
+template <int NV, bool CROSS, bool EVEN, int NS = 0, bool FULL = false, bool XY = false>
 __global__ void __launch_bounds__(BIN_THREADS, NS > 0 ? PK_FUSED_MIN_CTAS : 4) bin_global_flat_kernel(
     BinGeom g, const float2 *__restrict__ d1, const float2 *__restrict__ d2, float lx, float ly,
     float lz, LegendreCoefs lc, int zero_l0, const float *__restrict__ edges, int nwarps_hist,
@@ -1055,7 +1056,7 @@ __global__ void __launch_bounds__(BIN_THREADS, NS > 0 ? PK_FUSED_MIN_CTAS : 4) b
           const float ky = kcoord(j, n1, g.kfun[1], false);
           kxy = __fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky));
           kl = kx * lx + ky * ly;
-          if (NS > 0) row_factor<NSR, FULL>(fp, i, j, rf);
+          if (NS > 0) row_factor<NSR, FULL, XY>(fp, zt, i, j, rf);
           ic = i;
           jc = j;
         }
@@ -1185,7 +1186,9 @@ static pk_status launch_global(cudaStream_t st, const BinGeom &g, const float2 *
       L.smem += 2 * (size_t)((g.d.nz + 3) & ~3) * sizeof(float);
       PK_REQUIRE(L.smem <= 227 * 1024, PK_ERR_RANGE, "mesh too large along the last axis for the kz table");
     }
-    auto kernel = bin_global_flat_kernel<NV, CROSS, EVEN, NS, FULL>;
+    const bool xy = NS > 0 && use_xy_tables(g.d);  // per-axis phase / window tables
+    auto kernel = xy ? bin_global_flat_kernel<NV, CROSS, EVEN, NS, FULL, NS != 0>
+                     : bin_global_flat_kernel<NV, CROSS, EVEN, NS, FULL, false>;
     PK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
     int per_sm = 0;
     PK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, L.nwarps * 32, L.smem));
@@ -1201,8 +1204,11 @@ static pk_status launch_global(cudaStream_t st, const BinGeom &g, const float2 *
   } else {
     constexpr int MINB1 = NS > 0 ? PK_FUSED_MIN_CTAS : 4;
     constexpr int MINB2 = NS > 0 ? PK_FUSED_BATCH_MIN_CTAS : 4;
-    auto kernel = nbatch > 1 ? bin_global_kernel<NV, CROSS, EVEN, NS, FULL, MINB2>
-                             : bin_global_kernel<NV, CROSS, EVEN, NS, FULL, MINB1>;
+    const bool xy = NS > 0 && use_xy_tables(g.d);  // per-axis phase / window tables
+    auto kernel = nbatch > 1 ? (xy ? bin_global_kernel<NV, CROSS, EVEN, NS, FULL, MINB2, NS != 0>
+                                   : bin_global_kernel<NV, CROSS, EVEN, NS, FULL, MINB2, false>)
+                             : (xy ? bin_global_kernel<NV, CROSS, EVEN, NS, FULL, MINB1, NS != 0>
+                                   : bin_global_kernel<NV, CROSS, EVEN, NS, FULL, MINB1, false>);
     PK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
     kernel<<<dim3(L.blocks, nbatch), L.nwarps * 32, L.smem, st>>>(g, d1, d2, los[0], los[1], los[2], lc, zero_l0,
                                                                   edges, L.nwarps, L.tab, partials, fpv);

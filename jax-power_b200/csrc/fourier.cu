@@ -40,10 +40,10 @@ __global__ void __launch_bounds__(IL_THREADS) interlace_kernel(FourierParams p,
     const int i = rw.i, j = rw.j;
     const int64_t row = (int64_t)i * d.n1 + j;
     RowFactor<NS> rf, rm;
-    row_factor<NS, FULL>(p, i, j, rf);
+    row_factor_rt<NS, FULL>(p, t, i, j, rf);
     const bool planes = p.for_c2r != 0;
     const int im = (d.n0 - i) % d.n0, jm = (d.n1 - j) % d.n1;
-    if (planes) row_factor<NS, FULL>(p, im, jm, rm);
+    if (planes) row_factor_rt<NS, FULL>(p, t, im, jm, rm);
     const int64_t rbase = row * d.nz;
     const int64_t mbase = ((int64_t)im * d.n1 + jm) * d.nz;
     // four kz per lane per iteration: 4 * NS independent loads in flight
@@ -298,9 +298,8 @@ extern "C" pk_status pk_interlace_compensate_batch(void *stream, const void *in,
   p.for_c2r = for_c2r;
   p.scale = scale;
   const bool full = backend == PK_BACKEND_JAXDECOMP;
-  const size_t smem = ((size_t)nshifts * p.d.nz * (full ? 2 : 1)) * sizeof(float2) +
-                      (size_t)p.d.nz * sizeof(float);
-  PK_REQUIRE(smem <= 200 * 1024, PK_ERR_RANGE, "mesh too large along the last axis for the kz table");
+  const size_t smem = ztable_bytes(p.d, nshifts, full);
+  PK_REQUIRE(smem <= 200 * 1024, PK_ERR_RANGE, "mesh too large for the per-axis tables");
   const int64_t nrows = (int64_t)p.d.n0 * p.d.n1;
   const int64_t want = (nrows + IL_THREADS / 32 - 1) / (IL_THREADS / 32);
   const int64_t cap = 8LL * sm_count();
@@ -406,8 +405,8 @@ __global__ void __launch_bounds__(IL_THREADS) interlace_adjoint_kernel(FourierPa
     const int i = rw.i, j = rw.j;
     const int im = (d.n0 - i) % d.n0, jm = (d.n1 - j) % d.n1;
     RowFactor<NS> rf, rm;
-    row_factor<NS, false>(p, i, j, rf);
-    row_factor<NS, false>(p, im, jm, rm);
+    row_factor_rt<NS, false>(p, t, i, j, rf);
+    row_factor_rt<NS, false>(p, t, im, jm, rm);
     const int64_t rbase = ((int64_t)i * d.n1 + j) * d.nz;
     const int64_t mbase = ((int64_t)im * d.n1 + jm) * d.nz;
     for (int zb = lane; zb < d.nz; zb += 128) {
@@ -532,7 +531,7 @@ extern "C" pk_status pk_interlace_adjoint(void *stream, const void *in, int from
   p.for_c2r = 1;
   p.scale = 1.f;
   const size_t smem = ztable_bytes(p.d, nshifts, false);
-  PK_REQUIRE(smem <= 200 * 1024, PK_ERR_RANGE, "mesh too large along the last axis for the kz table");
+  PK_REQUIRE(smem <= 200 * 1024, PK_ERR_RANGE, "mesh too large for the per-axis tables");
   const int64_t nrows = (int64_t)p.d.n0 * p.d.n1;
   const int64_t want = (nrows + IL_THREADS / 32 - 1) / (IL_THREADS / 32);
   const int64_t cap = 8LL * sm_count();

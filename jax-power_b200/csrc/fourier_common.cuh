@@ -60,13 +60,27 @@ __device__ __forceinline__ float2 expi(float t) {
 
 constexpr int IL_MAX_SHIFTS = 8;
 
-// Per-CTA table along kz (shared memory): for each shift s, e^{i s kz(z)} and, for the
-// 'jaxdecomp' semantics, e^{-i s kz(-z)} on the full grid; plus sinc(kz / 2pi)^-p.
+// Per-CTA tables (shared memory).  Along kz: for each shift s, e^{i s kz(z)} and, for the
+// 'jaxdecomp' semantics, e^{-i s kz(-z)} on the full grid; plus sinc(kz / 2pi)^-p.  Along
+// kx and ky (when use_xy_tables): e^{i s k(i)} per shift and sinc(k / 2pi), from which the
+// per-row factors are formed with a complex product and a multiply instead of sines and
+// divisions per row.
 struct ZTable {
   float2 *ph;    // [nshifts][nz]
   float2 *phm;   // [nshifts][nz] (jaxdecomp)
+  float2 *phx;   // [nshifts][n0]
+  float2 *phy;   // [nshifts][n1]
   float *comp;   // [nz]: sinc(kz / 2pi)^-p (1 without compensation)
+  float *sx;     // [n0]: sinc(kx / 2pi)
+  float *sy;     // [n1]: sinc(ky / 2pi)
 };
+
+// The x / y tables are kept for meshes with n0 + n1 <= 512: they replace the per-row sines
+// and divisions, which matters on short rows (batched 128^3..256^3 fused binning: 15-27 %
+// faster), while on long rows the per-row cost is small and the tables' shared memory would
+// be taken from the L1 cache that the row walk's strided loads rely on (512^3: 1.04 ms with
+// the tables against 0.81 ms without).
+__host__ __device__ inline bool use_xy_tables(const Dims &d) { return d.n0 + d.n1 <= 512; }
 
 // Row factors: the phase over x, y per shift, and the row's real scale.
 template <int NS>
@@ -76,22 +90,46 @@ struct RowFactor {
   float scale;  // (sinc(kx / 2pi) sinc(ky / 2pi))^-p / I (1 / I without compensation)
 };
 
-template <int NS, bool FULL>
-__device__ __forceinline__ void row_factor(const FourierParams &p, int i, int j, RowFactor<NS> &r) {
+// XY (the tables exist, use_xy_tables): e^{i s kx} e^{i s ky} (and, jaxdecomp, the conjugate
+// of the mirrored row's) and the window product sinc(kx / 2pi) sinc(ky / 2pi) from the
+// per-axis tables; else computed for the row: e^{i s (kx + ky)} and the same window product.
+template <int NS, bool FULL, bool XY>
+__device__ __forceinline__ void row_factor(const FourierParams &p, const ZTable &t, int i, int j,
+                                           RowFactor<NS> &r) {
   const Dims &d = p.d;
   constexpr bool full = FULL;
-  const float k0 = ccoord(i, d.n0, p.cspacing[0], false);
-  const float k1 = ccoord(j, d.n1, p.cspacing[1], false);
-  const float kxy = k0 + k1;
-  const int i2 = (d.n0 - i) % d.n0, j2 = (d.n1 - j) % d.n1;
-  const float kxym = ccoord(i2, d.n0, p.cspacing[0], false) + ccoord(j2, d.n1, p.cspacing[1], false);
   const float inv = 1.f / p.interlacing;
+  const int i2 = (d.n0 - i) % d.n0, j2 = (d.n1 - j) % d.n1;
+  if constexpr (!XY) {
+    const float k0 = ccoord(i, d.n0, p.cspacing[0], false);
+    const float k1 = ccoord(j, d.n1, p.cspacing[1], false);
+    const float kxy = k0 + k1;
+    const float kxym = ccoord(i2, d.n0, p.cspacing[0], false) + ccoord(j2, d.n1, p.cspacing[1], false);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      r.ph[s] = expi(p.shifts[s] * kxy);
+      if (full) r.phm[s] = expi(-p.shifts[s] * kxym);
+    }
+    r.scale = (p.comp_order > 0 ? inverse_power(__fmul_rn(sinc_of(k0), sinc_of(k1)), p.comp_order) : 1.f) * inv;
+    return;
+  }
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
-    r.ph[s] = expi(p.shifts[s] * kxy);
-    if (full) r.phm[s] = expi(-p.shifts[s] * kxym);
+    r.ph[s] = cmul(t.phx[s * d.n0 + i], t.phy[s * d.n1 + j]);
+    if (full) {
+      const float2 m = cmul(t.phx[s * d.n0 + i2], t.phy[s * d.n1 + j2]);
+      r.phm[s] = make_float2(m.x, -m.y);
+    }
   }
-  r.scale = (p.comp_order > 0 ? inverse_power(__fmul_rn(sinc_of(k0), sinc_of(k1)), p.comp_order) : 1.f) * inv;
+  r.scale = (p.comp_order > 0 ? inverse_power(__fmul_rn(t.sx[i], t.sy[j]), p.comp_order) : 1.f) * inv;
+}
+
+// row_factor with the table choice made at run time (kernels where it is not register-critical).
+template <int NS, bool FULL>
+__device__ __forceinline__ void row_factor_rt(const FourierParams &p, const ZTable &t, int i, int j,
+                                              RowFactor<NS> &r) {
+  if (use_xy_tables(p.d)) row_factor<NS, FULL, true>(p, t, i, j, r);
+  else row_factor<NS, FULL, false>(p, t, i, j, r);
 }
 
 // Interlaced + compensated value of stored mode (row r, z): shift 0 has phase 1, so its
@@ -134,19 +172,32 @@ __device__ __forceinline__ void fill_ztable(const FourierParams &p, ZTable &t) {
     }
     t.comp[z] = p.comp_order > 0 ? inverse_power(sinc_of(k2), p.comp_order) : 1.f;
   }
+  for (int i = threadIdx.x; use_xy_tables(d) && i < d.n0 + d.n1; i += blockDim.x) {
+    const bool x = i < d.n0;
+    const int a = x ? i : i - d.n0;
+    const float k = x ? ccoord(a, d.n0, p.cspacing[0], false) : ccoord(a, d.n1, p.cspacing[1], false);
+    for (int s = 0; s < p.nshifts; ++s) (x ? t.phx[s * d.n0 + a] : t.phy[s * d.n1 + a]) = expi(p.shifts[s] * k);
+    (x ? t.sx[a] : t.sy[a]) = sinc_of(k);
+  }
 }
 
-// Bytes of the kz table for nshifts shifts.
+// Bytes of the tables for nshifts shifts.
 inline size_t ztable_bytes(const Dims &d, int nshifts, bool full) {
-  return ((size_t)nshifts * d.nz * (full ? 2 : 1)) * sizeof(float2) + (size_t)d.nz * sizeof(float);
+  const size_t nxy = use_xy_tables(d) ? (size_t)d.n0 + d.n1 : 0;
+  return ((size_t)nshifts * (d.nz * (full ? 2 : 1) + nxy)) * sizeof(float2) + (d.nz + nxy) * sizeof(float);
 }
 
-// Lay the kz table out from `base` (shared memory, 8-byte aligned).
+// Lay the tables out from `base` (shared memory, 8-byte aligned).
 __device__ __forceinline__ ZTable ztable_at(void *base, const FourierParams &p, bool full) {
   ZTable t;
   t.ph = reinterpret_cast<float2 *>(base);
   t.phm = t.ph + (size_t)p.nshifts * p.d.nz;
-  t.comp = reinterpret_cast<float *>(t.phm + (full ? (size_t)p.nshifts * p.d.nz : 0));
+  const bool xy = use_xy_tables(p.d);
+  t.phx = t.phm + (full ? (size_t)p.nshifts * p.d.nz : 0);
+  t.phy = t.phx + (xy ? (size_t)p.nshifts * p.d.n0 : 0);
+  t.comp = reinterpret_cast<float *>(t.phy + (xy ? (size_t)p.nshifts * p.d.n1 : 0));
+  t.sx = t.comp + p.d.nz;
+  t.sy = t.sx + (xy ? p.d.n0 : 0);
   return t;
 }
 
