@@ -29,8 +29,10 @@ __global__ void __launch_bounds__(IL_THREADS) interlace_kernel(FourierParams p,
   constexpr bool full = FULL;
   in += (int64_t)blockIdx.y * p.nshifts * d.ncomplex();  // batch of meshes along y
   out += (int64_t)blockIdx.y * d.ncomplex();
-  ZTable t = ztable_at(ilsmem, p, full);
-  fill_ztable<FULL>(p, t);
+  const bool xy = use_xy_tables(d);
+  ZTable t = xy ? ztable_at<XY_SMEM>(ilsmem, p, full) : ztable_at<XY_NONE>(ilsmem, p, full);
+  if (xy) fill_ztable<FULL, XY_SMEM>(p, t);
+  else fill_ztable<FULL, XY_NONE>(p, t);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nwarps = blockDim.x >> 5;
@@ -298,7 +300,8 @@ extern "C" pk_status pk_interlace_compensate_batch(void *stream, const void *in,
   p.for_c2r = for_c2r;
   p.scale = scale;
   const bool full = backend == PK_BACKEND_JAXDECOMP;
-  const size_t smem = ztable_bytes(p.d, nshifts, full);
+  p.gxy = nullptr;
+  const size_t smem = ztable_bytes(p.d, nshifts, full, use_xy_tables(p.d));
   PK_REQUIRE(smem <= 200 * 1024, PK_ERR_RANGE, "mesh too large for the per-axis tables");
   const int64_t nrows = (int64_t)p.d.n0 * p.d.n1;
   const int64_t want = (nrows + IL_THREADS / 32 - 1) / (IL_THREADS / 32);
@@ -392,8 +395,10 @@ __global__ void __launch_bounds__(IL_THREADS) interlace_adjoint_kernel(FourierPa
                                                                        float2 *__restrict__ out) {
   extern __shared__ float4 ilsmem[];
   const Dims d = p.d;
-  ZTable t = ztable_at(ilsmem, p, false);
-  fill_ztable<false>(p, t);
+  const bool xy = use_xy_tables(d);
+  ZTable t = xy ? ztable_at<XY_SMEM>(ilsmem, p, false) : ztable_at<XY_NONE>(ilsmem, p, false);
+  if (xy) fill_ztable<false, XY_SMEM>(p, t);
+  else fill_ztable<false, XY_NONE>(p, t);
   __syncthreads();
   const int64_t total = d.ncomplex();
   const bool even = (d.n2 % 2) == 0;
@@ -530,7 +535,8 @@ extern "C" pk_status pk_interlace_adjoint(void *stream, const void *in, int from
   p.backend = backend;
   p.for_c2r = 1;
   p.scale = 1.f;
-  const size_t smem = ztable_bytes(p.d, nshifts, false);
+  p.gxy = nullptr;
+  const size_t smem = ztable_bytes(p.d, nshifts, false, use_xy_tables(p.d));
   PK_REQUIRE(smem <= 200 * 1024, PK_ERR_RANGE, "mesh too large for the per-axis tables");
   const int64_t nrows = (int64_t)p.d.n0 * p.d.n1;
   const int64_t want = (nrows + IL_THREADS / 32 - 1) / (IL_THREADS / 32);

@@ -22,6 +22,10 @@ struct FourierParams {
   int backend;
   int for_c2r;
   float scale;
+  // Per-axis tables in global memory (phx [nshifts][n0], phy [nshifts][n1], then sx [n0] and
+  // sy [n1] as floats), filled by fill_xy_tables_kernel; NULL: the kernel keeps them in shared
+  // memory (when use_xy_tables) or computes its row factors.
+  float2 *gxy;
 };
 
 // jnp.sinc(k / 2pi) with the reference's float32 operations (resamplers.py:21).
@@ -158,8 +162,13 @@ __device__ __forceinline__ float2 combine_mode(const FourierParams &p, const Row
   return make_float2(acc.x * c, acc.y * c);
 }
 
-// Fill the per-CTA kz table (all threads of the block; call __syncthreads() after).
-template <bool FULL>
+// Where a kernel's per-axis x / y tables are: none (row factors computed per row), in shared
+// memory, or in global memory (FourierParams::gxy).
+enum { XY_NONE = 0, XY_SMEM = 1, XY_GLOBAL = 2 };
+
+// Fill the per-CTA kz table (and, XY_SMEM, the x / y tables; all threads of the block; call
+// __syncthreads() after).
+template <bool FULL, int XYM>
 __device__ __forceinline__ void fill_ztable(const FourierParams &p, ZTable &t) {
   const Dims &d = p.d;
   for (int z = threadIdx.x; z < d.nz; z += blockDim.x) {
@@ -172,7 +181,7 @@ __device__ __forceinline__ void fill_ztable(const FourierParams &p, ZTable &t) {
     }
     t.comp[z] = p.comp_order > 0 ? inverse_power(sinc_of(k2), p.comp_order) : 1.f;
   }
-  for (int i = threadIdx.x; use_xy_tables(d) && i < d.n0 + d.n1; i += blockDim.x) {
+  for (int i = threadIdx.x; XYM == XY_SMEM && i < d.n0 + d.n1; i += blockDim.x) {
     const bool x = i < d.n0;
     const int a = x ? i : i - d.n0;
     const float k = x ? ccoord(a, d.n0, p.cspacing[0], false) : ccoord(a, d.n1, p.cspacing[1], false);
@@ -181,24 +190,36 @@ __device__ __forceinline__ void fill_ztable(const FourierParams &p, ZTable &t) {
   }
 }
 
-// Bytes of the tables for nshifts shifts.
-inline size_t ztable_bytes(const Dims &d, int nshifts, bool full) {
-  const size_t nxy = use_xy_tables(d) ? (size_t)d.n0 + d.n1 : 0;
+// Bytes of the shared-memory tables for nshifts shifts (xy: with the per-axis ones).
+inline size_t ztable_bytes(const Dims &d, int nshifts, bool full, bool xy) {
+  const size_t nxy = xy ? (size_t)d.n0 + d.n1 : 0;
   return ((size_t)nshifts * (d.nz * (full ? 2 : 1) + nxy)) * sizeof(float2) + (d.nz + nxy) * sizeof(float);
 }
 
 // Lay the tables out from `base` (shared memory, 8-byte aligned).
+template <int XYM>
 __device__ __forceinline__ ZTable ztable_at(void *base, const FourierParams &p, bool full) {
   ZTable t;
   t.ph = reinterpret_cast<float2 *>(base);
   t.phm = t.ph + (size_t)p.nshifts * p.d.nz;
-  const bool xy = use_xy_tables(p.d);
+  constexpr bool xy = XYM == XY_SMEM;
   t.phx = t.phm + (full ? (size_t)p.nshifts * p.d.nz : 0);
   t.phy = t.phx + (xy ? (size_t)p.nshifts * p.d.n0 : 0);
   t.comp = reinterpret_cast<float *>(t.phy + (xy ? (size_t)p.nshifts * p.d.n1 : 0));
   t.sx = t.comp + p.d.nz;
   t.sy = t.sx + (xy ? p.d.n0 : 0);
+  if (XYM == XY_GLOBAL) {  // per-axis tables in global memory
+    t.phx = p.gxy;
+    t.phy = t.phx + (size_t)p.nshifts * p.d.n0;
+    t.sx = reinterpret_cast<float *>(t.phy + (size_t)p.nshifts * p.d.n1);
+    t.sy = t.sx + p.d.n0;
+  }
   return t;
+}
+
+// Bytes of the global per-axis tables for nshifts shifts.
+inline size_t xy_table_bytes(const Dims &d, int nshifts) {
+  return (size_t)nshifts * (d.n0 + d.n1) * sizeof(float2) + (size_t)(d.n0 + d.n1) * sizeof(float);
 }
 
 // Interlacing shifts s / I and circular spacings: the host-side set-up of FourierParams.
@@ -215,6 +236,7 @@ inline bool make_fourier_params(const int32_t meshsize[3], int nshifts, int comp
   p->backend = backend;
   p->for_c2r = for_c2r;
   p->scale = scale;
+  p->gxy = nullptr;
   return true;
 }
 
