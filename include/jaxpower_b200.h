@@ -208,6 +208,28 @@ pk_status pk_bin_separation_global(void *stream, const float *value, const int32
                                    int nedges, float step, int nells, const int32_t *ells,
                                    double *d_out, void *workspace, size_t workspace_bytes);
 
+/* Window matrix of the global line-of-sight power spectrum, mesh input power
+ * (compute_mesh2_spectrum_window, mesh2.py:1031-1131).  'jax' (rfftn) layout only.
+ *
+ * pk_window_fill: ncolumns (<= 16) half-complex meshes, column c at out + c N_c:
+ *   scale * L_ellin(mu) + 0i where klo[c] <= |k| < khi[c], 0 elsewhere (mesh2.py:1123),
+ *   |k| = sqrt((kx^2 + ky^2) + kz^2), mu = k.los / |k| (|k| = 1 at k = 0), float32.
+ * pk_window_multiply: meshes[c n + i] *= q[i] for c < ncolumns (16-byte aligned buffers);
+ *   the real-space product Q * c2r(A) of mesh2.py:1124.
+ * pk_bin_window: per bin and output multipole the float64 sum of w Re(A) L_ell(mu) over the
+ *   stored modes, k = 0 dropped for every ell, odd ell 0 (the reference bins
+ *   A (L_ell(mu) + L_ell(-mu))); A is `value` (half-complex, complex64) or, when value is
+ *   NULL, the periodic column scale * L_ellin(mu) 1{klo <= |k| < khi} formed per mode.
+ *   d_out: (nells, nbins); divide by nmodes and multiply by (2 ell + 1) / N. */
+pk_status pk_window_fill(void *stream, const int32_t meshsize[3], const float kfun[3], int backend,
+                         const float los[3], int ellin, float scale, int ncolumns, const float *klo,
+                         const float *khi, void *out);
+pk_status pk_window_multiply(void *stream, float *meshes, int ncolumns, const float *q, int64_t n);
+pk_status pk_bin_window(void *stream, const void *value, const int32_t meshsize[3], const float kfun[3],
+                        const float los[3], const float *d_edges, int nedges, float step, int backend,
+                        int nells, const int32_t *ells, int ellin, float klo, float khi, float scale,
+                        double *d_out, void *workspace, size_t workspace_bytes);
+
 /* First-point correlation function (mesh2.py:423-451): carry += sum_j r_j Y_j(shat) over
  * nterms real meshes r_j (r + j N_r), shat the unit separation vector of the grid
  * fftfreq(n) * cellsize * n (0 at s = 0), real Y_lm as pk_ylm_premultiply. */

@@ -1519,6 +1519,98 @@ extern "C" pk_status pk_bin_separation_global(void *stream, const float *value, 
   return PK_ERR_INVALID;
 }
 
+// ------------------------------------------------------------ window matrix
+// compute_mesh2_spectrum_window, global line of sight, mesh input power (mesh2.py:1031-1131).
+// Column (ell_in, [k_lo, k_hi)) of the window is the binned Re(A) L_ell(mu) of
+//   A = N 1{k_lo <= |k| < k_hi} L_ell_in(mu)             (periodic box), or
+//   A = r2c(Q c2r(N 1{k_lo <= |k| < k_hi} L_ell_in(mu)))  (selection Q = c2r(W1 W2*) / N),
+// with |k| = sqrt((kx^2 + ky^2) + kz^2) and mu = k.los / |k| (|k| = 1 at k = 0) in float32.
+// The reference bins Aell * (L_ell(mu) + L_ell(-mu)) for odd ell, which is zero term by term.
+
+constexpr int WINDOW_MAX_COLUMNS = 16;
+
+struct WindowColumns {
+  float klo[WINDOW_MAX_COLUMNS], khi[WINDOW_MAX_COLUMNS];
+};
+
+__device__ __forceinline__ float window_mu(float kx, float ky, float kz, float k2, const float los[3],
+                                           float *knorm) {
+  const float num = __fadd_rn(__fadd_rn(__fmul_rn(kx, los[0]), __fmul_rn(ky, los[1])), __fmul_rn(kz, los[2]));
+  *knorm = __fsqrt_rn(k2);
+  return __fdiv_rn(num, k2 > 0.f ? *knorm : 1.f);
+}
+
+// ncol half-complex meshes (column c at out + c N_c): N 1{k_lo[c] <= |k| < k_hi[c]} L_ell_in(mu) + 0i.
+__global__ void window_fill_kernel(Dims d, float kf0, float kf1, float kf2, float l0, float l1, float l2,
+                                   int ellin, float scale, int ncol, WindowColumns cols, float2 *__restrict__ out) {
+  const int64_t nc = d.ncomplex();
+  const float los[3] = {l0, l1, l2};
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nc; q += (int64_t)gridDim.x * blockDim.x) {
+    const int z = (int)(q % d.nz);
+    const int64_t row = q / d.nz;
+    const int j = (int)(row % d.n1), i = (int)(row / d.n1);
+    const float kx = kcoord(i, d.n0, kf0, false), ky = kcoord(j, d.n1, kf1, false);
+    const float kz = kcoord(z, d.n2, kf2, true);
+    const float k2 = __fadd_rn(__fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky)), __fmul_rn(kz, kz));
+    float knorm;
+    const float mu = window_mu(kx, ky, kz, k2, los, &knorm);
+    const float v = __fmul_rn(legendre(ellin, mu), scale);
+    for (int c = 0; c < ncol; ++c) {
+      const bool in = knorm >= cols.klo[c] && knorm < cols.khi[c];
+      out[(int64_t)c * nc + q] = make_float2(in ? v : 0.f, 0.f);
+    }
+  }
+}
+
+// meshes[c N + q] *= q[q] for c < ncol (float4 when N is a multiple of 4).
+__global__ void window_multiply_kernel(float *__restrict__ meshes, const float *__restrict__ qmesh, int64_t n,
+                                       int ncol) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  if ((n & 3) == 0) {
+    const int64_t n4 = n >> 2;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n4; t += stride) {
+      const float4 w = reinterpret_cast<const float4 *>(qmesh)[t];
+      for (int c = 0; c < ncol; ++c) {
+        float4 *p = reinterpret_cast<float4 *>(meshes + (int64_t)c * n) + t;
+        float4 v = *p;
+        v.x *= w.x; v.y *= w.y; v.z *= w.z; v.w *= w.w;
+        *p = v;
+      }
+    }
+  } else {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += stride) {
+      const float w = qmesh[t];
+      for (int c = 0; c < ncol; ++c) meshes[(int64_t)c * n + t] *= w;
+    }
+  }
+}
+
+// w Re(A) L_ell(mu) per mode, k = 0 dropped for every ell (_bin of the reference passes
+// remove_zero=True); A read from a mesh, or formed from the column (periodic box).
+template <int N>
+struct WindowOp {
+  const float2 *v;
+  float los[3];
+  int ells[MAX_ELLS];
+  int ellin;
+  float klo, khi, scale;
+  static constexpr int NV = N;
+  __device__ void operator()(int64_t idx, int i, int j, int z, float kx, float ky, float kz, float k2, float w,
+                             float out[NV]) const {
+    float knorm;
+    const float mu = window_mu(kx, ky, kz, k2, los, &knorm);
+    float a;
+    if (v) a = v[idx].x;
+    else a = (knorm >= klo && knorm < khi) ? __fmul_rn(legendre(ellin, mu), scale) : 0.f;
+    const bool zero = (i == 0 && j == 0 && z == 0);
+#pragma unroll
+    for (int l = 0; l < NV; ++l) {
+      const int ell = ells[l];
+      out[l] = (zero || (ell & 1)) ? 0.f : __fmul_rn(__fmul_rn(a, legendre(ell, mu)), w);
+    }
+  }
+};
+
 template <int MASK, bool CROSS>
 static pk_status launch_firstpoint_block(cudaStream_t s, const BinGeom &g, const float2 *a0, const float2 *b0,
                                          const float2 *f, const float *edges, const RowMap &map, double *out,
@@ -2081,4 +2173,66 @@ extern "C" pk_status pk_bin_firstpoint_adjoint(void *stream, const void *a0, con
       (float2 *)out_f);
   PK_LAUNCH_CHECK();
   return PK_OK;
+}
+
+extern "C" pk_status pk_window_fill(void *stream, const int32_t meshsize[3], const float kfun[3], int backend,
+                                    const float los[3], int ellin, float scale, int ncolumns, const float *klo,
+                                    const float *khi, void *out) {
+  Dims d;
+  PK_REQUIRE(make_dims(meshsize, &d), PK_ERR_INVALID, "invalid meshsize");
+  PK_REQUIRE(backend == PK_BACKEND_JAX, PK_ERR_INVALID, "the window fill takes the 'jax' (rfftn) layout");
+  PK_REQUIRE(kfun && los && klo && khi && out, PK_ERR_INVALID, "null pointer");
+  PK_REQUIRE(ellin >= 0 && ellin <= 8, PK_ERR_INVALID, "ellin must be in 0..8");
+  PK_REQUIRE(ncolumns >= 1 && ncolumns <= WINDOW_MAX_COLUMNS, PK_ERR_INVALID, "ncolumns must be in 1..%d",
+             WINDOW_MAX_COLUMNS);
+  WindowColumns cols;
+  for (int c = 0; c < WINDOW_MAX_COLUMNS; ++c) {
+    cols.klo[c] = c < ncolumns ? klo[c] : 0.f;
+    cols.khi[c] = c < ncolumns ? khi[c] : 0.f;
+  }
+  const int64_t nc = d.ncomplex();
+  const int64_t want = (nc + 255) / 256;
+  const int blocks = (int)(want < (int64_t)sm_count() * 8 ? want : (int64_t)sm_count() * 8);
+  window_fill_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(d, kfun[0], kfun[1], kfun[2], los[0], los[1],
+                                                                  los[2], ellin, scale, ncolumns, cols,
+                                                                  (float2 *)out);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+extern "C" pk_status pk_window_multiply(void *stream, float *meshes, int ncolumns, const float *q, int64_t n) {
+  PK_REQUIRE(meshes && q, PK_ERR_INVALID, "null pointer");
+  PK_REQUIRE(n >= 1 && ncolumns >= 1, PK_ERR_INVALID, "empty meshes");
+  PK_REQUIRE(((uintptr_t)meshes & 15) == 0 && ((uintptr_t)q & 15) == 0, PK_ERR_INVALID,
+             "meshes must be 16-byte aligned");
+  const int64_t want = ((n & 3) == 0 ? n / 4 : n + 255) / 256 + 1;
+  const int blocks = (int)(want < (int64_t)sm_count() * 8 ? want : (int64_t)sm_count() * 8);
+  window_multiply_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(meshes, q, n, ncolumns);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+extern "C" pk_status pk_bin_window(void *stream, const void *value, const int32_t meshsize[3], const float kfun[3],
+                                   const float los[3], const float *d_edges, int nedges, float step, int backend,
+                                   int nells, const int32_t *ells, int ellin, float klo, float khi, float scale,
+                                   double *d_out, void *workspace, size_t workspace_bytes) {
+  BinGeom g;
+  pk_status st = make_geom(meshsize, kfun, nedges, step, backend, &g);
+  if (st) return st;
+  PK_REQUIRE(backend == PK_BACKEND_JAX, PK_ERR_INVALID, "the window binning takes the 'jax' (rfftn) layout");
+  PK_REQUIRE(d_edges && d_out && los && ells, PK_ERR_INVALID, "null pointer");
+  PK_REQUIRE(nells >= 1 && nells <= MAX_ELLS, PK_ERR_INVALID, "nells must be in 1..%d", MAX_ELLS);
+  PK_REQUIRE(ellin >= 0 && ellin <= 8, PK_ERR_INVALID, "ellin must be in 0..8");
+  for (int l = 0; l < nells; ++l) PK_REQUIRE(ells[l] >= 0 && ells[l] <= 8, PK_ERR_INVALID, "ell must be in 0..8");
+  auto fill = [&](auto &op) {
+    op.v = (const float2 *)value;
+    for (int a = 0; a < 3; ++a) op.los[a] = los[a];
+    for (int l = 0; l < MAX_ELLS; ++l) op.ells[l] = l < nells ? ells[l] : 0;
+    op.ellin = ellin;
+    op.klo = klo;
+    op.khi = khi;
+    op.scale = scale;
+  };
+  return dispatch_nv<WindowOp>(nells, fill, (cudaStream_t)stream, g, d_edges, true, 0, d_out, workspace,
+                               workspace_bytes);
 }

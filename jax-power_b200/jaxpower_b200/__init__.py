@@ -13,8 +13,9 @@ from .mesh import (MeshAttrs, BaseMeshField, RealMeshField, ComplexMeshField, Pa
 from .mesh2 import (BinMesh2SpectrumPoles, BinMesh2CorrelationPoles, compute_mesh2_spectrum,
                     compute_mesh2_correlation, compute_mesh2, compute_fkp2_normalization,
                     compute_fkp2_shotnoise, compute_box2_normalization, compute_normalization,
-                    compute_box_normalization)
-from .types import Mesh2SpectrumPole, Mesh2SpectrumPoles, Mesh2CorrelationPole, Mesh2CorrelationPoles, read, write
+                    compute_box_normalization, compute_mesh2_spectrum_window)
+from .types import (Mesh2SpectrumPole, Mesh2SpectrumPoles, Mesh2CorrelationPole, Mesh2CorrelationPoles, WindowMatrix,
+                    read, write)
 from ._lib import load as load_library, LIBRARY_PATH
 
 __version__ = '0.1.0'

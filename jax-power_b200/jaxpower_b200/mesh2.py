@@ -24,7 +24,7 @@ from .types import Mesh2SpectrumPole, Mesh2SpectrumPoles, Mesh2CorrelationPole, 
 
 __all__ = ['BinMesh2SpectrumPoles', 'compute_mesh2_spectrum', 'compute_mesh2', 'compute_fkp2_normalization',
            'compute_fkp2_shotnoise', 'compute_box2_normalization', 'compute_normalization',
-           'compute_box_normalization']
+           'compute_box_normalization', 'compute_mesh2_spectrum_window']
 
 
 def _format_ells(ells):
@@ -641,3 +641,154 @@ def compute_fkp2_shotnoise(*fkps, bin=None, fields=None):
     if bin is not None:
         return [shotnoise * (ell == 0) * np.ones(bin.nbins) for ell in bin.ells]
     return shotnoise
+
+
+def _window_edges(edgesin, ellsin):
+    if hasattr(edgesin, 'ells') and hasattr(edgesin, 'poles'):  # a multipole container: its ells and k edges
+        ellsin = edgesin.ells
+        edgesin = next(iter(edgesin)).k_edges
+    edgesin = np.asarray(edgesin, dtype='f8')
+    if edgesin.ndim != 2:
+        edgesin = np.column_stack([edgesin[:-1], edgesin[1:]])
+    if np.ndim(ellsin) == 0:
+        ellsin = (ellsin,)
+    return edgesin, [int(ell) for ell in ellsin]
+
+
+def _window_batch(mattrs, batch_size):
+    """Columns per pass of the selection-function window: B half-complex inputs, their real
+    transforms and the transformed products must fit (about 16 N bytes per column)."""
+    n = int(np.prod(mattrs.meshsize))
+    fit = max(int(_free_device_memory() // (20 * n)), 1)
+    limit = 16 if batch_size is None else max(int(batch_size), 1)
+    return max(min(fit, limit, 16), 1)
+
+
+def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='z', buffer=None, batch_size=None,
+                                  pbar=False, norm=None, flags=tuple()):
+    """Window matrix of the power-spectrum multipoles (``mesh2.py:921-1482``).
+
+    Global line of sight ('x', 'y', 'z' or a 3-vector) with the input power defined on the
+    mesh (no 'smooth' / 'infinite' flag).  Column (ell_in, [k_lo, k_hi)) is the estimator
+    applied to ``A = N 1{k_lo <= |k| < k_hi} L_ell_in(mu)``:
+
+    - periodic box (a ``MeshAttrs`` given): A is binned as it is, formed per mode inside the
+      binning kernel (``pk_bin_window`` without a mesh); when the input edges are the output
+      bins one pass per ell_in fills the diagonal, as the reference does (mesh2.py:1113-1118);
+    - selection function (one or two meshes W): ``Q = c2r(W1 W2*) / N`` and
+      ``A <- r2c(Q c2r(A))``, up to 16 columns per batched FFT pair (``pk_window_fill``,
+      cuFFT C2R, ``pk_window_multiply``, cuFFT R2C, ``pk_bin_window``).
+
+    Row (ell, k bin) is ``(2 ell + 1) / (1 + ell % 2) rnorm bin(A (L_ell(mu) + L_ell(-mu)))``,
+    k = 0 dropped, with ``rnorm = (N / V_cell) / norm / N``; odd ell rows are 0 (the
+    reference's Legendre sum vanishes for odd ell).  Returns a ``WindowMatrix`` of shape
+    (len(ells) nbins, len(ellsin) len(edgesin)).  ``buffer`` and ``pbar`` are accepted and
+    have no effect; ``batch_size`` caps the columns per FFT batch.  The first-point line of
+    sight, the 'smooth' / 'infinite' flags and the 'jaxdecomp' backend raise
+    ``NotImplementedError``.
+    """
+    from .types import WindowMatrix
+    flags = tuple(flags)
+    if 'smooth' in flags or 'infinite' in flags:
+        raise NotImplementedError("the 'smooth' and 'infinite' window flags are not supported on the GPU path")
+    meshes, fields = _format_meshes(*meshes)
+    periodic = isinstance(meshes[0], MeshAttrs)
+    if periodic:
+        assert fields[1] == fields[0]
+        mattrs = meshes[0]
+    else:
+        mattrs = meshes[0].attrs
+    if mattrs.fft_backend != 'jax':
+        raise NotImplementedError("the window matrix takes the 'jax' FFT backend")
+    los, vlos, swap = _los(los)
+    if vlos is None:
+        raise NotImplementedError('the window matrix of the first-point / end-point line of sight is not supported')
+    f4 = np.float32
+    ells = bin.ells
+    nbins, nells = bin.nbins, len(ells)
+    meshsize = mattrs.meshsize
+    N = f4(np.prod(meshsize.astype('f4'), dtype='f4'))
+    _norm = f4(N / f4(np.prod(mattrs.cellsize, dtype='f4')))
+    norm = np.asarray(_norm if norm is None else norm, dtype='f4')
+    if norm.ndim <= 1:
+        norm = norm * np.ones(nells, dtype='f4')
+    rnorm = (_norm / norm / N).astype('f4')
+    edgesin, ellsin = _window_edges(edgesin, ellsin)
+    nin = len(edgesin)
+    klo, khi = edgesin[:, 0].astype('f4'), edgesin[:, -1].astype('f4')
+
+    stream = _lib.stream_handle()
+    ws = bin._workspace()
+    args_geom = (_lib.i32(meshsize), _lib.f32(mattrs.kfun), _lib.f32(vlos))
+    args_bins = (_lib.ptr(bin.d_edges), len(bin._edges1d), bin._step, mattrs.backend_code, nells, _lib.i32(ells))
+
+    def bin_window(out, value, ellin, lo, hi):
+        _lib.call('pk_bin_window', stream, _lib.ptr(value) if value is not None else None, *args_geom, *args_bins,
+                  int(ellin), float(lo), float(hi), float(N), _lib.ptr(out), _lib.ptr(ws), ws.numel())
+
+    common = False
+    if periodic:
+        bedges = bin.edges
+        mask_in = np.all(edgesin >= bedges[0], axis=-1) & np.all(edgesin <= bedges[-1], axis=-1)
+        mask_edges = np.all(bedges >= edgesin[0], axis=-1) & np.all(bedges <= edgesin[-1], axis=-1)
+        common = mask_edges.sum() == mask_in.sum() and np.allclose(edgesin[mask_in], bedges[mask_edges])
+
+    if common:
+        sums = torch.empty((len(ellsin), nells, nbins), dtype=torch.float64, device=_device())
+        for iin, ellin in enumerate(ellsin):
+            bin_window(sums[iin], None, ellin, -np.inf, np.inf)
+    else:
+        sums = torch.empty((len(ellsin), nin, nells, nbins), dtype=torch.float64, device=_device())
+        if periodic:
+            for iin, ellin in enumerate(ellsin):
+                for e in range(nin):
+                    bin_window(sums[iin, e], None, ellin, klo[e], khi[e])
+        else:
+            A1 = _2c(meshes[0]).value.contiguous()
+            A2 = A1 if fields[1] == fields[0] else _2c(meshes[1]).value.contiguous()
+            prod = torch.empty_like(A1)
+            _lib.call('pk_conj_multiply', stream, _lib.ptr(A2), _lib.ptr(A1), 1, A1.numel(), _lib.ptr(prod))
+            Q = _c2r(prod, meshsize, destroy_input=True)
+            del prod, A1, A2
+            _lib.call('pk_scale_real', stream, _lib.ptr(Q), Q.numel(), float(f4(1.) / N))
+            nreal = Q.numel()
+            B = _window_batch(mattrs, batch_size)
+            cshape = tuple(int(n) for n in meshsize[:2]) + (int(meshsize[2]) // 2 + 1,)
+            for iin, ellin in enumerate(ellsin):
+                for e0 in range(0, nin, B):
+                    nb = min(B, nin - e0)
+                    cols = torch.empty((nb,) + cshape, dtype=torch.complex64, device=_device())
+                    _lib.call('pk_window_fill', stream, *args_geom[:2], mattrs.backend_code, args_geom[2], int(ellin),
+                              float(N), nb, _lib.f32(klo[e0:e0 + nb]), _lib.f32(khi[e0:e0 + nb]), _lib.ptr(cols))
+                    real = _c2r(cols, meshsize, destroy_input=True)
+                    del cols
+                    _lib.call('pk_window_multiply', stream, _lib.ptr(real), nb, _lib.ptr(Q), nreal)
+                    cols = _r2c(real, meshsize)
+                    del real
+                    for b in range(nb):
+                        bin_window(sums[iin, e0 + b], cols[b], ellin, 0., 0.)
+                    del cols
+    sums = sums.cpu().numpy()
+    with np.errstate(invalid='ignore', divide='ignore'):
+        factor = np.array([(2 * ell + 1) / (1 + ell % 2) * rnorm[ill] for ill, ell in enumerate(ells)])
+        spectra = sums / bin.nmodes * factor[:, None]  # (..., nells, nbins)
+    if common:
+        wmat = []
+        rows = np.flatnonzero(mask_in)
+        for iin in range(len(ellsin)):
+            w = np.zeros((nin, nells, nbins), dtype='f8')
+            for ill in range(nells):
+                w[rows, ill, np.flatnonzero(mask_edges)] = spectra[iin, ill][mask_edges]
+            wmat.append(w.reshape(nin, -1))
+    else:
+        wmat = [spectra[iin].reshape(nin, -1) for iin in range(len(ellsin))]
+    wmat = np.concatenate(wmat, axis=0).T
+
+    observable = Mesh2SpectrumPoles([Mesh2SpectrumPole(k=bin.xavg, k_edges=bin.edges, nmodes=bin.nmodes,
+                                                       num_raw=np.zeros(nbins), num_shotnoise=np.zeros(nbins),
+                                                       norm=np.ones(nbins) * norm[ill], ell=ell)
+                                     for ill, ell in enumerate(ells)])
+    kin = np.mean(edgesin, axis=-1)
+    theory = Mesh2SpectrumPoles([Mesh2SpectrumPole(k=kin, k_edges=edgesin, nmodes=np.ones(nin), num_raw=np.zeros(nin),
+                                                   ell=ellin) for ellin in ellsin])
+    return WindowMatrix(observable=observable, theory=theory, value=wmat)

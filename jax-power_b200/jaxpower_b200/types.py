@@ -23,7 +23,7 @@ import json
 import numpy as np
 
 __all__ = ['Mesh2SpectrumPole', 'Mesh2SpectrumPoles', 'Mesh2CorrelationPole', 'Mesh2CorrelationPoles',
-           'DeferredRows', 'read', 'write']
+           'WindowMatrix', 'DeferredRows', 'read', 'write']
 
 
 class DeferredRows:
@@ -197,8 +197,40 @@ class Mesh2CorrelationPoles(Mesh2SpectrumPoles):
         return 'Mesh2CorrelationPoles(ells={})'.format(self.ells)
 
 
+class WindowMatrix:
+    """Window matrix (the lsstypes ``WindowMatrix`` built at ``mesh2.py:1462-1482``).
+
+    ``value`` (observable size, theory size) maps the theory multipoles, flattened ell by ell,
+    to the binned multipoles: ``observable`` (``Mesh2SpectrumPoles`` on the output k bins,
+    ``norm`` the window's normalisation, ``num_raw`` zero) and ``theory`` (one
+    ``Mesh2SpectrumPole`` per input ell on the input k edges, ``k`` their mid-points).
+    """
+
+    def __init__(self, observable, theory, value):
+        self.observable = observable
+        self.theory = theory
+        self.value = np.asarray(value)
+
+    @property
+    def shape(self):
+        return self.value.shape
+
+    def dot(self, theory):
+        """``value @ theory``, the theory given as a flat vector or one array per input ell."""
+        if not isinstance(theory, np.ndarray) or theory.ndim != 1:
+            theory = np.concatenate([np.ravel(t) for t in theory])
+        return self.value.dot(theory)
+
+    def write(self, filename):
+        write(filename, self)
+
+    def __repr__(self):
+        return 'WindowMatrix(shape={}, ells={}, ellsin={})'.format(self.shape, self.observable.ells,
+                                                                   self.theory.ells)
+
+
 _CLASSES = {cls.__name__: cls for cls in (Mesh2SpectrumPole, Mesh2SpectrumPoles, Mesh2CorrelationPole,
-                                          Mesh2CorrelationPoles)}
+                                          Mesh2CorrelationPoles, WindowMatrix)}
 _POLE_OF = {'Mesh2SpectrumPoles': Mesh2SpectrumPole, 'Mesh2CorrelationPoles': Mesh2CorrelationPole}
 
 
@@ -239,7 +271,14 @@ def write(filename, observable):
     if name not in _CLASSES:
         raise TypeError('cannot write {}'.format(type(observable)))
     arrays = {'__class__': np.array(name)}
-    if isinstance(observable, Mesh2SpectrumPoles):
+    if isinstance(observable, WindowMatrix):
+        arrays['value'] = observable.value
+        for part in ('observable', 'theory'):
+            poles = getattr(observable, part)
+            arrays['{}/npoles'.format(part)] = np.array(len(poles))
+            for i, pole in enumerate(poles):
+                arrays.update(_pole_arrays('{}/pole{:d}/'.format(part, i), pole))
+    elif isinstance(observable, Mesh2SpectrumPoles):
         arrays['__npoles__'] = np.array(len(observable))
         for i, pole in enumerate(observable):
             arrays.update(_pole_arrays('pole{:d}/'.format(i), pole))
@@ -253,6 +292,11 @@ def read(filename):
     """Load what ``write`` saved."""
     with np.load(filename, allow_pickle=False) as archive:
         name = str(archive['__class__'])
+        if name == 'WindowMatrix':
+            parts = [Mesh2SpectrumPoles([Mesh2SpectrumPole.from_state(_pole_state('{}/pole{:d}/'.format(part, i), archive))
+                                         for i in range(int(archive['{}/npoles'.format(part)]))])
+                     for part in ('observable', 'theory')]
+            return WindowMatrix(*parts, value=archive['value'])
         if name in _POLE_OF:
             pole_cls = _POLE_OF[name]
             poles = [pole_cls.from_state(_pole_state('pole{:d}/'.format(i), archive))

@@ -168,6 +168,79 @@ def compute_mesh2_spectrum(mesh, bins, los='z', accum='f64', mesh2=None):
                 volume=np.prod(geom.kfun.astype('f8')) * bins.nmodes)
 
 
+
+def compute_mesh2_spectrum_window(bins, edgesin, ellsin, los='z', meshes=None, norm=None):
+    """``compute_mesh2_spectrum_window(*meshes or mattrs, edgesin=, ellsin=, bin=bins, los=)``,
+    global line of sight, input power on the mesh (``mesh2.py:921-1131``, ``1462-1482``).
+
+    ``meshes``: None (periodic box: ``MeshAttrs`` given) or one / two real selection meshes.
+    Returns the window matrix, (len(ells) nbins, len(ellsin) len(edgesin)), float64.
+    """
+    geom = bins.geom
+    dt = geom.dtype
+    t = dt.type
+    ells = bins.ells
+    N = t(np.prod(geom.meshsize.astype(dt)))
+    _norm = t(N / t(np.prod(geom.cellsize.astype(dt))))
+    norm = np.asarray(_norm if norm is None else norm, dtype=dt)
+    if norm.ndim <= 1:
+        norm = norm * np.ones(len(ells), dtype=dt)
+    rnorm = (_norm / norm / N).astype(dt)
+    vlos = np.zeros(3)
+    if isinstance(los, str):
+        vlos['xyz'.index(los)] = 1.
+    else:
+        vlos = np.asarray(los, dtype='f8')
+    edgesin = np.asarray(edgesin, dtype='f8')
+    if edgesin.ndim != 2:
+        edgesin = np.column_stack([edgesin[:-1], edgesin[1:]])
+    edgesin_dt = edgesin.astype(dt)
+    Q, common = None, False
+    if meshes is not None:
+        W = [_to_complex(geom, m) for m in meshes]
+        W2 = W[0] if len(W) == 1 else W[1]
+        Q = (c2r(geom, (W[0] * np.conj(W2)).astype(W[0].dtype)) / N).astype(dt)
+    else:
+        bedges = np.column_stack([bins.edges[:-1], bins.edges[1:]])
+        mask_in = np.all(edgesin >= bedges[0], axis=-1) & np.all(edgesin <= bedges[-1], axis=-1)
+        mask_edges = np.all(bedges >= edgesin[0], axis=-1) & np.all(bedges <= edgesin[-1], axis=-1)
+        common = mask_edges.sum() == mask_in.sum() and np.allclose(edgesin[mask_in], bedges[mask_edges])
+    kvec = kcoords(geom)
+    knorm = bins.knorm()
+    kl = [(kk * t(ll)).astype(dt) for kk, ll in zip(kvec, vlos)]
+    num = (((t(0.) + kl[0]).astype(dt) + kl[1]).astype(dt) + kl[2]).astype(dt)
+    mu = (num / np.where(knorm == 0., t(1.), knorm)).astype(dt)
+
+    def _bin(A):
+        spectrum = []
+        for ill, ell in enumerate(ells):
+            leg = legendre(ell, mu)
+            odd = ell % 2
+            if odd:
+                leg = (leg + legendre(ell, (-mu).astype(dt))).astype(dt)
+            spectrum.append((2 * ell + 1) / (1 + odd) * bins((A * leg).astype(A.dtype), remove_zero=True) * rnorm[ill])
+        return np.concatenate(spectrum)
+
+    wmat = []
+    for ellin in ellsin:
+        legin = legendre(ellin, mu)
+        if common:
+            spectrum = _bin((legin * N).astype(np.complex64))
+            nb = bins.nbins
+            w = np.zeros((len(edgesin), len(ells), nb), dtype=spectrum.dtype)
+            for ill in range(len(ells)):
+                w[np.flatnonzero(mask_in), ill, np.flatnonzero(mask_edges)] = spectrum[ill * nb:(ill + 1) * nb][mask_edges]
+            wmat.append(w.reshape(len(edgesin), -1))
+            continue
+        rows = []
+        for lo, hi in edgesin_dt:
+            A = (((knorm >= lo) & (knorm < hi)) * legin * N).astype(np.complex64)
+            if Q is not None:
+                A = r2c(geom, (Q * c2r(geom, A)).astype(dt))
+            rows.append(_bin(A))
+        wmat.append(np.array(rows))
+    return np.real(np.concatenate(wmat, axis=0).T)
+
 # --------------------------------------------------------------------------- FKP
 
 def next_fft_size(n, primes=(2, 3, 5, 7), divisors=()):

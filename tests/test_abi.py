@@ -78,3 +78,25 @@ def test_argument_errors_of_later_entries_without_gpu(lib):
                                  10, 0.01, 0, 3, ells, 1, 0, fake, fake, 1 << 20) == 1
     assert lib.pk_bin_firstpoint(None, fake, None, fake, 5, _lib.i32([2] * 5), _lib.i32(range(-2, 3)), ms, kf, fake,
                                  10, 0.01, 0, 0, ells, 1, 0, fake, fake, 1 << 20) == 1
+
+
+def test_window_argument_errors_without_gpu(lib):
+    """Window-matrix entry points: column count, multipole range, layout and NULL checks."""
+    from jaxpower_b200 import _lib
+    fake = ctypes.c_void_p(4096)
+    ms, kf, los = _lib.i32([32, 32, 32]), _lib.f32([0.01] * 3), _lib.f32([0., 0., 1.])
+    lo, hi = _lib.f32([0.] * 17), _lib.f32([0.1] * 17)
+    assert lib.pk_window_fill(None, ms, kf, 0, los, 2, 1., 0, lo, hi, fake) == 1
+    assert lib.pk_window_fill(None, ms, kf, 0, los, 2, 1., 17, lo, hi, fake) == 1
+    assert lib.pk_window_fill(None, ms, kf, 0, los, 9, 1., 1, lo, hi, fake) == 1
+    assert lib.pk_window_fill(None, ms, kf, 1, los, 2, 1., 1, lo, hi, fake) == 1  # jaxdecomp layout
+    assert lib.pk_window_fill(None, ms, kf, 0, los, 2, 1., 1, lo, hi, None) == 1
+    assert lib.pk_window_multiply(None, fake, 1, ctypes.c_void_p(4100), 64) == 1  # misaligned
+    assert lib.pk_window_multiply(None, fake, 0, fake, 64) == 1
+    ells = _lib.i32([0, 2, 4])
+    assert lib.pk_bin_window(None, None, ms, kf, los, fake, 10, 0.01, 0, 0, ells, 0, 0., 1., 1., fake, fake,
+                             1 << 20) == 1
+    assert lib.pk_bin_window(None, None, ms, kf, los, fake, 10, 0.01, 0, 3, ells, 10, 0., 1., 1., fake, fake,
+                             1 << 20) == 1
+    assert lib.pk_bin_window(None, None, ms, kf, los, None, 10, 0.01, 0, 3, ells, 0, 0., 1., 1., fake, fake,
+                             1 << 20) == 1

@@ -1,0 +1,50 @@
+"""Window matrix of the power-spectrum multipoles (global line of sight): the oracle's own
+identities, on the CPU.
+
+- A periodic box with input edges equal to the output bins fills the diagonal in one pass
+  per input multipole (mesh2.py:1113-1118); the selection-function path with W = 1
+  (Q = c2r(|r2c(1)|^2) / N = 1) walks every input bin through c2r and r2c and must give the
+  same matrix.
+- The (ell = 0, ell_in = 0) diagonal of the periodic window is 1 in every bin, except the
+  first, which loses the k = 0 mode: (nmodes - 1) / nmodes.
+"""
+import numpy as np
+import pytest
+
+from oracle.coords import Geometry
+from oracle.spectrum import Bins, compute_mesh2_spectrum_window as owindow
+
+
+@pytest.mark.parametrize('los', ['z', [0.6, 0., 0.8]])
+def test_window_selection_of_ones_is_periodic(los):
+    geom = Geometry((16, 12, 10), (400., 300., 250.))
+    bins = Bins(geom, step=0.02, ells=(0, 2, 4))
+    periodic = owindow(bins, bins.edges, (0, 2, 4), los=los)
+    ones = owindow(bins, bins.edges, (0, 2, 4), los=los, meshes=[np.ones(geom.rshape, dtype='f4')])
+    nb = bins.nbins
+    assert periodic.shape == ones.shape == (3 * nb, 3 * len(bins.edges) - 3)
+    fin = np.isfinite(periodic)
+    assert np.array_equal(fin, np.isfinite(ones))
+    scale = np.abs(periodic[fin]).max()
+    assert np.allclose(periodic[fin], ones[fin], atol=2e-5 * scale)
+    # periodic: every (ell, ell_in) block diagonal
+    block = periodic[:nb, :nb]
+    off = block - np.diag(np.diag(block))
+    assert np.all(off[np.isfinite(off)] == 0.)
+    expect = np.ones(nb)
+    expect[0] = (bins.nmodes[0] - 1.) / bins.nmodes[0]
+    assert np.allclose(np.diag(block), expect, rtol=1e-6)
+
+
+def test_window_theory_vector_of_a_constant_power():
+    """W @ P_in for a constant monopole P_in = 1 gives 1 in every monopole bin (no k = 0)."""
+    geom = Geometry((12, 12, 12), (300., 300., 300.))
+    bins = Bins(geom, step=0.03, ells=(0, 2))
+    edgesin = np.arange(0., 0.4, 0.01)
+    w = owindow(bins, edgesin, (0,), los='x')
+    got = w.dot(np.ones(len(edgesin) - 1))
+    nb = bins.nbins
+    expect = np.ones(nb)
+    expect[0] = (bins.nmodes[0] - 1.) / bins.nmodes[0]
+    assert np.allclose(got[:nb], expect, rtol=1e-6)
+    assert np.allclose(got[nb:], 0., atol=1e-6)  # isotropic input: no quadrupole
