@@ -230,6 +230,17 @@ pk_status pk_bin_window(void *stream, const void *value, const int32_t meshsize[
                         int nells, const int32_t *ells, int ellin, float klo, float khi, float scale,
                         double *d_out, void *workspace, size_t workspace_bytes);
 
+/* Periodic window, all columns of disjoint input bins in one pass: d_edges (nedges, float32,
+ * ascending) is the union of the output and input edges; for each of npairs (<= 9) pairs
+ * (pair_ell, pair_ellin) the float64 sum per merged interval of
+ * w scale L_ellin(mu) L_ell(mu) (k = 0 dropped, odd ell 0).  Each merged interval lies in
+ * one output bin and at most one input bin; the caller adds the intervals into the window.
+ * d_out: (npairs, nedges - 1). */
+pk_status pk_bin_window_pairs(void *stream, const int32_t meshsize[3], const float kfun[3], const float los[3],
+                              const float *d_edges, int nedges, float step, int backend, int npairs,
+                              const int32_t *pair_ell, const int32_t *pair_ellin, float scale, double *d_out,
+                              void *workspace, size_t workspace_bytes);
+
 /* First-point correlation function (mesh2.py:423-451): carry += sum_j r_j Y_j(shat) over
  * nterms real meshes r_j (r + j N_r), shat the unit separation vector of the grid
  * fftfreq(n) * cellsize * n (0 at s = 0), real Y_lm as pk_ylm_premultiply. */

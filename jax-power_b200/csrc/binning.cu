@@ -1611,6 +1611,29 @@ struct WindowOp {
   }
 };
 
+// Periodic window, every column of an ell_in at once: binned on the union of the output and
+// input edges, each merged interval lies in one (output bin, input bin) pair, so value l is
+// w N L_ell_in[l](mu) L_ell[l](mu) (the per-column product, same rounding) for pairs
+// (ell[l], ell_in[l]).
+template <int N>
+struct WindowPairsOp {
+  float los[3];
+  int ell[MAX_ELLS], ellin[MAX_ELLS];
+  float scale;
+  static constexpr int NV = N;
+  __device__ void operator()(int64_t, int i, int j, int z, float kx, float ky, float kz, float k2, float w,
+                             float out[NV]) const {
+    float knorm;
+    const float mu = window_mu(kx, ky, kz, k2, los, &knorm);
+    const bool zero = (i == 0 && j == 0 && z == 0);
+#pragma unroll
+    for (int l = 0; l < NV; ++l) {
+      const float a = __fmul_rn(legendre(ellin[l], mu), scale);
+      out[l] = (zero || (ell[l] & 1)) ? 0.f : __fmul_rn(__fmul_rn(a, legendre(ell[l], mu)), w);
+    }
+  }
+};
+
 template <int MASK, bool CROSS>
 static pk_status launch_firstpoint_block(cudaStream_t s, const BinGeom &g, const float2 *a0, const float2 *b0,
                                          const float2 *f, const float *edges, const RowMap &map, double *out,
@@ -2235,4 +2258,30 @@ extern "C" pk_status pk_bin_window(void *stream, const void *value, const int32_
   };
   return dispatch_nv<WindowOp>(nells, fill, (cudaStream_t)stream, g, d_edges, true, 0, d_out, workspace,
                                workspace_bytes);
+}
+
+extern "C" pk_status pk_bin_window_pairs(void *stream, const int32_t meshsize[3], const float kfun[3],
+                                         const float los[3], const float *d_edges, int nedges, float step,
+                                         int backend, int npairs, const int32_t *pair_ell,
+                                         const int32_t *pair_ellin, float scale, double *d_out, void *workspace,
+                                         size_t workspace_bytes) {
+  BinGeom g;
+  pk_status st = make_geom(meshsize, kfun, nedges, step, backend, &g);
+  if (st) return st;
+  PK_REQUIRE(backend == PK_BACKEND_JAX, PK_ERR_INVALID, "the window binning takes the 'jax' (rfftn) layout");
+  PK_REQUIRE(d_edges && d_out && los && pair_ell && pair_ellin, PK_ERR_INVALID, "null pointer");
+  PK_REQUIRE(npairs >= 1 && npairs <= MAX_ELLS, PK_ERR_INVALID, "npairs must be in 1..%d", MAX_ELLS);
+  for (int l = 0; l < npairs; ++l)
+    PK_REQUIRE(pair_ell[l] >= 0 && pair_ell[l] <= 8 && pair_ellin[l] >= 0 && pair_ellin[l] <= 8, PK_ERR_INVALID,
+               "ell must be in 0..8");
+  auto fill = [&](auto &op) {
+    for (int a = 0; a < 3; ++a) op.los[a] = los[a];
+    for (int l = 0; l < MAX_ELLS; ++l) {
+      op.ell[l] = l < npairs ? pair_ell[l] : 0;
+      op.ellin[l] = l < npairs ? pair_ellin[l] : 0;
+    }
+    op.scale = scale;
+  };
+  return dispatch_nv<WindowPairsOp>(npairs, fill, (cudaStream_t)stream, g, d_edges, true, 0, d_out, workspace,
+                                    workspace_bytes);
 }

@@ -664,6 +664,40 @@ def _window_batch(mattrs, batch_size):
     return max(min(fit, limit, 16), 1)
 
 
+def _window_merged(mattrs, bin, vlos, ells, ellsin, klo, khi, N):
+    """Periodic window columns of disjoint, ascending input bins [klo, khi) in one binning
+    pass per 9 (ell, ell_in) pairs, on the union of the output and input edges (float32, as
+    |k| is compared): each merged interval lies in one output bin b and at most one input
+    bin e, and its sums are added to column e, row b.  Returns (len(ellsin), nin, nells, nbins)."""
+    eout = bin._edges1d.astype('f4')
+    merged = np.unique(np.concatenate([eout, klo, khi]).astype('f4'))
+    merged = merged[(merged >= eout[0]) & (merged <= eout[-1])]
+    m0 = merged[:-1]
+    b = np.searchsorted(eout, m0, side='right') - 1
+    e = np.searchsorted(klo, m0, side='right') - 1
+    inside = (e >= 0) & (merged[1:] <= khi[np.maximum(e, 0)]) & (b >= 0) & (b < bin.nbins)
+    pairs = [(ill, iin) for iin in range(len(ellsin)) for ill, ell in enumerate(ells) if ell % 2 == 0]
+    nm = len(merged) - 1
+    out = np.zeros((len(ellsin), len(klo), len(ells), bin.nbins), dtype='f8')
+    if not pairs or nm < 1:
+        return out
+    d_edges = torch.as_tensor(merged, device=_device())
+    nbytes = _lib.c_size_t()
+    _lib.call('pk_bin_workspace_size', _lib.i32(mattrs.meshsize), len(merged), 9, _lib.ctypes.byref(nbytes))
+    ws = _workspace(nbytes.value)
+    raw = torch.empty((len(pairs), nm), dtype=torch.float64, device=_device())
+    for p0 in range(0, len(pairs), 9):
+        chunk = pairs[p0:p0 + 9]
+        _lib.call('pk_bin_window_pairs', _lib.stream_handle(), _lib.i32(mattrs.meshsize), _lib.f32(mattrs.kfun),
+                  _lib.f32(vlos), _lib.ptr(d_edges), len(merged), _uniform_step(merged), mattrs.backend_code,
+                  len(chunk), _lib.i32([ells[ill] for ill, _ in chunk]), _lib.i32([ellsin[iin] for _, iin in chunk]),
+                  float(N), _lib.ptr(raw[p0:p0 + len(chunk)]), _lib.ptr(ws), ws.numel())
+    raw = raw.cpu().numpy()
+    for q, (ill, iin) in enumerate(pairs):
+        np.add.at(out[iin, :, ill], (e[inside], b[inside]), raw[q, inside])
+    return out
+
+
 def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='z', buffer=None, batch_size=None,
                                   pbar=False, norm=None, flags=tuple()):
     """Window matrix of the power-spectrum multipoles (``mesh2.py:921-1482``).
@@ -673,8 +707,10 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     applied to ``A = N 1{k_lo <= |k| < k_hi} L_ell_in(mu)``:
 
     - periodic box (a ``MeshAttrs`` given): A is binned as it is, formed per mode inside the
-      binning kernel (``pk_bin_window`` without a mesh); when the input edges are the output
-      bins one pass per ell_in fills the diagonal, as the reference does (mesh2.py:1113-1118);
+      binning kernel; when the input edges are the output bins one pass per ell_in fills the
+      diagonal, as the reference does (mesh2.py:1113-1118); disjoint ascending input bins take
+      one pass for all columns on the merged edges (``pk_bin_window_pairs``), other input
+      edges one pass per column (``pk_bin_window`` without a mesh);
     - selection function (one or two meshes W): ``Q = c2r(W1 W2*) / N`` and
       ``A <- r2c(Q c2r(A))``, up to 16 columns per batched FFT pair (``pk_window_fill``,
       cuFFT C2R, ``pk_window_multiply``, cuFFT R2C, ``pk_bin_window``).
@@ -739,7 +775,9 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
             bin_window(sums[iin], None, ellin, -np.inf, np.inf)
     else:
         sums = torch.empty((len(ellsin), nin, nells, nbins), dtype=torch.float64, device=_device())
-        if periodic:
+        if periodic and nin > 1 and np.all(khi > klo) and np.all(klo[1:] >= khi[:-1]):
+            sums = _window_merged(mattrs, bin, vlos, ells, ellsin, klo, khi, N)
+        elif periodic:
             for iin, ellin in enumerate(ellsin):
                 for e in range(nin):
                     bin_window(sums[iin, e], None, ellin, klo[e], khi[e])
@@ -768,7 +806,7 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
                     for b in range(nb):
                         bin_window(sums[iin, e0 + b], cols[b], ellin, 0., 0.)
                     del cols
-    sums = sums.cpu().numpy()
+    sums = sums.cpu().numpy() if isinstance(sums, torch.Tensor) else sums
     with np.errstate(invalid='ignore', divide='ignore'):
         factor = np.array([(2 * ell + 1) / (1 + ell % 2) * rnorm[ill] for ill, ell in enumerate(ells)])
         spectra = sums / bin.nmodes * factor[:, None]  # (..., nells, nbins)

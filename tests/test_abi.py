@@ -100,3 +100,7 @@ def test_window_argument_errors_without_gpu(lib):
                              1 << 20) == 1
     assert lib.pk_bin_window(None, None, ms, kf, los, None, 10, 0.01, 0, 3, ells, 0, 0., 1., 1., fake, fake,
                              1 << 20) == 1
+    pe, pi = _lib.i32([0] * 10), _lib.i32([0] * 10)
+    assert lib.pk_bin_window_pairs(None, ms, kf, los, fake, 10, 0., 0, 0, pe, pi, 1., fake, fake, 1 << 20) == 1
+    assert lib.pk_bin_window_pairs(None, ms, kf, los, fake, 10, 0., 0, 10, pe, pi, 1., fake, fake, 1 << 20) == 1
+    assert lib.pk_bin_window_pairs(None, ms, kf, los, fake, 10, 0., 1, 3, pe, pi, 1., fake, fake, 1 << 20) == 1

@@ -26,14 +26,24 @@ def _check(got, ref):
 @pytest.mark.parametrize('meshsize', [(16, 12, 10), (24, 20, 16)])
 @pytest.mark.parametrize('los', ['z', [0.6, 0., 0.8]])
 @pytest.mark.parametrize('ells', [(0, 2, 4), (0, 1, 2)])
-@pytest.mark.parametrize('common', [True, False])
-def test_periodic_window_matches_oracle(meshsize, los, ells, common):
+@pytest.mark.parametrize('kind', ['common', 'disjoint', 'overlapping'])
+def test_periodic_window_matches_oracle(meshsize, los, ells, kind):
+    """Input edges equal to the output bins (diagonal fill), disjoint input bins with gaps and
+    a range past the output bins (one pass on the merged edges), overlapping input bins (one
+    pass per column)."""
     import jaxpower_b200 as jp
     boxsize = np.array([400., 300., 250.])
     attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize)
     b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.02}, ells=ells)
     ob = Bins(Geometry(meshsize, boxsize), step=0.02, ells=ells)
-    edgesin = b._edges1d if common else np.arange(0., 0.3, 0.013)
+    if kind == 'common':
+        edgesin = b._edges1d
+    elif kind == 'disjoint':
+        a = np.arange(0.004, 0.5, 0.013)
+        edgesin = np.column_stack([a[:-1], a[:-1] + 0.009])
+    else:
+        a = np.arange(0., 0.3, 0.013)
+        edgesin = np.column_stack([a[:-2], a[2:]])
     w = jp.compute_mesh2_spectrum_window(attrs, edgesin=edgesin, ellsin=(0, 2, 4), bin=b, los=los)
     ref = owindow(ob, edgesin, (0, 2, 4), los=los)
     _check(w.value, ref)
