@@ -767,6 +767,7 @@ struct GlobalSmem {
 
 // EVEN: every multipole even with ell <= 4 (L_ell a polynomial of degree <= 2 in mu^2, no
 // odd parts), the usual (0, 2, 4) case; otherwise the general form (degree 4, odd ell).
+// NS < 0: the binned value is Re(d1) itself, linear in the mesh (window-matrix columns).
 // NS > 0: the mesh is not stored; each mode is formed on the fly from NS interlaced,
 // uncompensated meshes at d1 (mesh s at d1 + s N_c), exactly as pk_interlace_compensate
 // forms it (fp: its parameters; FULL: 'jaxdecomp' semantics), which saves writing and
@@ -897,7 +898,7 @@ __global__ void __launch_bounds__(BIN_THREADS, MINB) bin_global_kernel(
           re = a.x * b.x + a.y * b.y;
           im = a.x * b.y - a.y * b.x;
         } else {
-          re = a.x * a.x + a.y * a.y;
+          re = NS < 0 ? a.x : a.x * a.x + a.y * a.y;
         }
         const float w = jaxw ? (z > 0 ? 2.f : 1.f) : ((z == 0 || z == zself) ? 1.f : 2.f);
         const float num = kl + kz * lz;
@@ -1071,7 +1072,7 @@ __global__ void __launch_bounds__(BIN_THREADS, NS > 0 ? PK_FUSED_MIN_CTAS : 4) b
           re = a.x * b.x + a.y * b.y;
           im = a.x * b.y - a.y * b.x;
         } else {
-          re = a.x * a.x + a.y * a.y;
+          re = NS < 0 ? a.x : a.x * a.x + a.y * a.y;
         }
         const float w = jaxw ? (z > 0 ? 2.f : 1.f) : ((z == 0 || z == zself) ? 1.f : 2.f);
         const float num = kl + kz * lz;
@@ -1209,7 +1210,7 @@ static pk_status launch_global(cudaStream_t st, const BinGeom &g, const float2 *
   const int hist_len = (g.nedges - 1) * NV;
   int blocks = L.blocks;
   if (g.d.nz < PK_GLOBAL_FLAT_NZ) {
-    if (NS == 0 && !L.tab) {  // the flat kernel always tabulates kz
+    if (NS <= 0 && !L.tab) {  // the flat kernel always tabulates kz
       L.smem += 2 * (size_t)((g.d.nz + 3) & ~3) * sizeof(float);
       PK_REQUIRE(L.smem <= 227 * 1024, PK_ERR_RANGE, "mesh too large along the last axis for the kz table");
     }
@@ -1586,7 +1587,7 @@ __global__ void window_multiply_kernel(float *__restrict__ meshes, const float *
 }
 
 // w Re(A) L_ell(mu) per mode, k = 0 dropped for every ell (_bin of the reference passes
-// remove_zero=True); A read from a mesh, or formed from the column (periodic box).
+// remove_zero=True); A formed from the column (periodic box), or read from v if set.
 template <int N>
 struct WindowOp {
   const float2 *v;
@@ -1607,6 +1608,33 @@ struct WindowOp {
     for (int l = 0; l < NV; ++l) {
       const int ell = ells[l];
       out[l] = (zero || (ell & 1)) ? 0.f : __fmul_rn(__fmul_rn(a, legendre(ell, mu)), w);
+    }
+  }
+};
+
+// The same row for a mesh A (the selection-function columns): no |k| comparison is made, so
+// mu^2 = (k.los)^2 / k^2 by a fast reciprocal and L_ell as Horner polynomials in mu^2 (odd
+// ell: zero coefficients).
+template <int N>
+struct WindowMeshOp {
+  const float2 *v;
+  float los[3];
+  float c[MAX_ELLS][5];
+  static constexpr int NV = N;
+  __device__ void operator()(int64_t idx, int i, int j, int z, float kx, float ky, float kz, float k2, float w,
+                             float out[NV]) const {
+    const float num = (kx * los[0] + ky * los[1]) + kz * los[2];
+    const float rk2 = k2 > 0.f ? __fdividef(1.f, k2) : 0.f;
+    const float mu2 = num * num * rk2;
+    const float a = (i == 0 && j == 0 && z == 0) ? 0.f : v[idx].x * w;
+#pragma unroll
+    for (int l = 0; l < NV; ++l) {
+      float L = c[l][4];
+      L = L * mu2 + c[l][3];
+      L = L * mu2 + c[l][2];
+      L = L * mu2 + c[l][1];
+      L = L * mu2 + c[l][0];
+      out[l] = a * L;
     }
   }
 };
@@ -2247,8 +2275,22 @@ extern "C" pk_status pk_bin_window(void *stream, const void *value, const int32_
   PK_REQUIRE(nells >= 1 && nells <= MAX_ELLS, PK_ERR_INVALID, "nells must be in 1..%d", MAX_ELLS);
   PK_REQUIRE(ellin >= 0 && ellin <= 8, PK_ERR_INVALID, "ellin must be in 0..8");
   for (int l = 0; l < nells; ++l) PK_REQUIRE(ells[l] >= 0 && ells[l] <= 8, PK_ERR_INVALID, "ell must be in 0..8");
+  if (value) {
+    auto fill = [&](auto &op) {
+      op.v = (const float2 *)value;
+      for (int a = 0; a < 3; ++a) op.los[a] = los[a];
+      for (int l = 0; l < MAX_ELLS; ++l) {
+        int odd = 0;
+        legendre_coefs(l < nells ? ells[l] : 0, op.c[l], &odd);
+        if (odd)
+          for (int q = 0; q < 5; ++q) op.c[l][q] = 0.f;
+      }
+    };
+    return dispatch_nv<WindowMeshOp>(nells, fill, (cudaStream_t)stream, g, d_edges, true, 0, d_out, workspace,
+                                     workspace_bytes);
+  }
   auto fill = [&](auto &op) {
-    op.v = (const float2 *)value;
+    op.v = nullptr;
     for (int a = 0; a < 3; ++a) op.los[a] = los[a];
     for (int l = 0; l < MAX_ELLS; ++l) op.ells[l] = l < nells ? ells[l] : 0;
     op.ellin = ellin;
@@ -2284,4 +2326,43 @@ extern "C" pk_status pk_bin_window_pairs(void *stream, const int32_t meshsize[3]
   };
   return dispatch_nv<WindowPairsOp>(npairs, fill, (cudaStream_t)stream, g, d_edges, true, 0, d_out, workspace,
                                     workspace_bytes);
+}
+
+extern "C" pk_status pk_bin_window_batch(void *stream, const void *value, int nbatch, const int32_t meshsize[3],
+                                         const float kfun[3], const float los[3], const float *d_edges, int nedges,
+                                         float step, int backend, int nells, const int32_t *ells, double *d_out,
+                                         void *workspace, size_t workspace_bytes) {
+  PK_REQUIRE(nbatch >= 1 && nbatch <= 65535, PK_ERR_INVALID, "nbatch must be in 1..65535");
+  BinGeom g;
+  pk_status st = make_geom(meshsize, kfun, nedges, step, backend, &g);
+  if (st) return st;
+  PK_REQUIRE(backend == PK_BACKEND_JAX, PK_ERR_INVALID, "the window binning takes the 'jax' (rfftn) layout");
+  PK_REQUIRE(value && d_edges && d_out && los && ells, PK_ERR_INVALID, "null pointer");
+  PK_REQUIRE(nells >= 1 && nells <= 5, PK_ERR_INVALID, "nells must be in 1..5");
+  LegendreCoefs lc;
+  lc.any_odd = 0;
+  int max_ell = 0;
+  for (int l = 0; l < MAX_ELLS; ++l) {
+    const int ell = l < nells ? ells[l] : 0;
+    if (l < nells) PK_REQUIRE(ell >= 0 && ell <= 8 && ell % 2 == 0, PK_ERR_INVALID, "ell must be even, 0..8");
+    legendre_coefs(ell, lc.c[l], &lc.odd[l]);
+    if (l < nells && ell > max_ell) max_ell = ell;
+  }
+  const bool even = max_ell <= 4;
+  cudaStream_t cs = (cudaStream_t)stream;
+  const float2 *a = (const float2 *)value;
+  // k = 0 dropped for every ell: no ell keeps it (zero_l0 = 0)
+  switch (nells * 2 + (even ? 1 : 0)) {
+#define PK_WB_CASE(N)                                                                                       \
+  case 2 * N:                                                                                               \
+    return launch_global<N, false, false, -1>(cs, g, a, nullptr, los, lc, 0, d_edges, d_out, workspace,     \
+                                              workspace_bytes, nbatch);                                     \
+  case 2 * N + 1:                                                                                           \
+    return launch_global<N, false, true, -1>(cs, g, a, nullptr, los, lc, 0, d_edges, d_out, workspace,      \
+                                             workspace_bytes, nbatch);
+    PK_WB_CASE(1) PK_WB_CASE(2) PK_WB_CASE(3) PK_WB_CASE(4) PK_WB_CASE(5)
+#undef PK_WB_CASE
+  }
+  set_error("unsupported number of multipoles %d", nells);
+  return PK_ERR_INVALID;
 }

@@ -713,7 +713,8 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
       edges one pass per column (``pk_bin_window`` without a mesh);
     - selection function (one or two meshes W): ``Q = c2r(W1 W2*) / N`` and
       ``A <- r2c(Q c2r(A))``, up to 16 columns per batched FFT pair (``pk_window_fill``,
-      cuFFT C2R, ``pk_window_multiply``, cuFFT R2C, ``pk_bin_window``).
+      cuFFT C2R, ``pk_window_multiply`` with the C2R's 1 / N folded into Q, cuFFT R2C,
+      ``pk_bin_window_batch``: the fused binning pass, linear in A, over the batch).
 
     Row (ell, k bin) is ``(2 ell + 1) / (1 + ell % 2) rnorm bin(A (L_ell(mu) + L_ell(-mu)))``,
     k = 0 dropped, with ``rnorm = (N / V_cell) / norm / N``; odd ell rows are 0 (the
@@ -786,25 +787,36 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
             A2 = A1 if fields[1] == fields[0] else _2c(meshes[1]).value.contiguous()
             prod = torch.empty_like(A1)
             _lib.call('pk_conj_multiply', stream, _lib.ptr(A2), _lib.ptr(A1), 1, A1.numel(), _lib.ptr(prod))
-            Q = _c2r(prod, meshsize, destroy_input=True)
+            # Q = c2r(W1 W2*) / N, times the 1 / N of every column's c2r (taken unscaled)
+            Q = _c2r(prod, meshsize, scale=False, destroy_input=True)
             del prod, A1, A2
-            _lib.call('pk_scale_real', stream, _lib.ptr(Q), Q.numel(), float(f4(1.) / N))
+            _lib.call('pk_scale_real', stream, _lib.ptr(Q), Q.numel(), float(np.float64(f4(1.) / N) ** 3))
             nreal = Q.numel()
             B = _window_batch(mattrs, batch_size)
             cshape = tuple(int(n) for n in meshsize[:2]) + (int(meshsize[2]) // 2 + 1,)
+            even = [ill for ill, ell in enumerate(ells) if ell % 2 == 0]
+            sums.zero_()
+            if even:
+                nbytes = _lib.c_size_t()
+                _lib.call('pk_bin_batch_workspace_size', _lib.i32(meshsize), len(bin._edges1d), len(even), B,
+                          _lib.ctypes.byref(nbytes))
+                wsb = _workspace(nbytes.value)
+                raw = torch.empty((B, len(even), nbins), dtype=torch.float64, device=_device())
             for iin, ellin in enumerate(ellsin):
-                for e0 in range(0, nin, B):
+                for e0 in range(0, nin if even else 0, B):
                     nb = min(B, nin - e0)
                     cols = torch.empty((nb,) + cshape, dtype=torch.complex64, device=_device())
                     _lib.call('pk_window_fill', stream, *args_geom[:2], mattrs.backend_code, args_geom[2], int(ellin),
                               float(N), nb, _lib.f32(klo[e0:e0 + nb]), _lib.f32(khi[e0:e0 + nb]), _lib.ptr(cols))
-                    real = _c2r(cols, meshsize, destroy_input=True)
+                    real = _c2r(cols, meshsize, scale=False, destroy_input=True)
                     del cols
                     _lib.call('pk_window_multiply', stream, _lib.ptr(real), nb, _lib.ptr(Q), nreal)
                     cols = _r2c(real, meshsize)
                     del real
-                    for b in range(nb):
-                        bin_window(sums[iin, e0 + b], cols[b], ellin, 0., 0.)
+                    _lib.call('pk_bin_window_batch', stream, _lib.ptr(cols), nb, *args_geom, _lib.ptr(bin.d_edges),
+                              len(bin._edges1d), bin._step, mattrs.backend_code, len(even),
+                              _lib.i32([ells[ill] for ill in even]), _lib.ptr(raw), _lib.ptr(wsb), wsb.numel())
+                    sums[iin, e0:e0 + nb, even] = raw[:nb]
                     del cols
     sums = sums.cpu().numpy() if isinstance(sums, torch.Tensor) else sums
     with np.errstate(invalid='ignore', divide='ignore'):

@@ -50,10 +50,12 @@ def test_periodic_window_matches_oracle(meshsize, los, ells, kind):
     assert w.observable.ells == tuple(ells) and w.theory.ells == (0, 2, 4)
 
 
-@pytest.mark.parametrize('meshsize', [(16, 12, 10), (20, 16, 12)])
+@pytest.mark.parametrize('meshsize', [(16, 12, 10), (20, 16, 12), (10, 8, 182)])
 @pytest.mark.parametrize('los', ['x', [0., 0.6, 0.8]])
 @pytest.mark.parametrize('cross', [False, True])
 def test_selection_window_matches_oracle(meshsize, los, cross):
+    """Short last axes take the flat chunk walk of the fused binning pass, (10, 8, 182) its
+    row-run walk."""
     import jaxpower_b200 as jp
     boxsize = np.array([500., 400., 300.])
     rng = np.random.default_rng(3)
@@ -63,6 +65,10 @@ def test_selection_window_matches_oracle(meshsize, los, cross):
     ob = Bins(Geometry(meshsize, boxsize), step=0.02, ells=(0, 2, 4))
     edgesin = np.arange(0., 0.25, 0.012)  # 20 input bins: batches of 6 leave a ragged last one
     meshes = [attrs.create(kind='real', fill=torch.as_tensor(s)) for s in (sel if cross else sel[:1])]
+    ells = (0, 1, 2, 4) if cross else (0, 2, 4)
+    if cross:
+        b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.02}, ells=ells)
+        ob = Bins(Geometry(meshsize, boxsize), step=0.02, ells=ells)
     w = jp.compute_mesh2_spectrum_window(*meshes, edgesin=edgesin, ellsin=(0, 2), bin=b, los=los, batch_size=6)
     ref = owindow(ob, edgesin, (0, 2), los=los, meshes=(sel if cross else sel[:1]))
     _check(w.value, ref)
