@@ -209,7 +209,7 @@ pk_status pk_bin_separation_global(void *stream, const float *value, const int32
                                    double *d_out, void *workspace, size_t workspace_bytes);
 
 /* Window matrix of the global line-of-sight power spectrum, mesh input power
- * (compute_mesh2_spectrum_window, mesh2.py:1031-1131).  'jax' (rfftn) layout only.
+ * (compute_mesh2_spectrum_window, mesh2.py:1013-1133).  'jax' (rfftn) layout only.
  *
  * pk_window_fill: ncolumns (<= 16) half-complex meshes, column c at out + c N_c:
  *   scale * L_ellin(mu) + 0i where klo[c] <= |k| < khi[c], 0 elsewhere (mesh2.py:1123),

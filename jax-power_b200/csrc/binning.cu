@@ -1521,7 +1521,7 @@ extern "C" pk_status pk_bin_separation_global(void *stream, const float *value, 
 }
 
 // ------------------------------------------------------------ window matrix
-// compute_mesh2_spectrum_window, global line of sight, mesh input power (mesh2.py:1031-1131).
+// compute_mesh2_spectrum_window, global line of sight, mesh input power (mesh2.py:1013-1133).
 // Column (ell_in, [k_lo, k_hi)) of the window is the binned Re(A) L_ell(mu) of
 //   A = N 1{k_lo <= |k| < k_hi} L_ell_in(mu)             (periodic box), or
 //   A = r2c(Q c2r(N 1{k_lo <= |k| < k_hi} L_ell_in(mu)))  (selection Q = c2r(W1 W2*) / N),

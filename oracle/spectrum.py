@@ -171,7 +171,7 @@ def compute_mesh2_spectrum(mesh, bins, los='z', accum='f64', mesh2=None):
 
 def compute_mesh2_spectrum_window(bins, edgesin, ellsin, los='z', meshes=None, norm=None):
     """``compute_mesh2_spectrum_window(*meshes or mattrs, edgesin=, ellsin=, bin=bins, los=)``,
-    global line of sight, input power on the mesh (``mesh2.py:921-1131``, ``1462-1482``).
+    global line of sight, input power on the mesh (``mesh2.py:921-1133``, ``1462-1482``).
 
     ``meshes``: None (periodic box: ``MeshAttrs`` given) or one / two real selection meshes.
     Returns the window matrix, (len(ells) nbins, len(ellsin) len(edgesin)), float64.
