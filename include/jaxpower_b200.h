@@ -230,15 +230,16 @@ pk_status pk_bin_window(void *stream, const void *value, const int32_t meshsize[
                         int nells, const int32_t *ells, int ellin, float klo, float khi, float scale,
                         double *d_out, void *workspace, size_t workspace_bytes);
 
-/* Selection-function window columns, nbatch (<= 65535) half-complex meshes A (value + b N_c):
- * per mesh, bin and even ell (nells <= 5) the float64 sum of w Re(A) L_ell(mu) over the stored
- * modes, k = 0 dropped (the fused global-los binning pass, linear in A).  Odd ell rows of the
- * window are zero and are not asked for.  workspace: pk_bin_batch_workspace_size(meshsize,
- * nedges, nells, nbatch).  d_out: (nbatch, nells, nbins). */
+/* Selection-function window columns and mean spectra (compute_mesh2_spectrum_mean,
+ * mesh2.py:1569-1605), nbatch (<= 65535) half-complex meshes A (value + b N_c): per mesh, bin
+ * and even ell (nells <= 5) the float64 sum of w Re(A) L_ell(mu) over the stored modes, k = 0
+ * dropped when remove_zero (the fused global-los binning pass, linear in A).  Odd ell rows
+ * are zero in both (L_ell(mu) + L_ell(-mu) = 0) and are not asked for.  workspace:
+ * pk_bin_batch_workspace_size(meshsize, nedges, nells, nbatch).  d_out: (nbatch, nells, nbins). */
 pk_status pk_bin_window_batch(void *stream, const void *value, int nbatch, const int32_t meshsize[3],
                               const float kfun[3], const float los[3], const float *d_edges, int nedges,
-                              float step, int backend, int nells, const int32_t *ells, double *d_out,
-                              void *workspace, size_t workspace_bytes);
+                              float step, int backend, int nells, const int32_t *ells, int remove_zero,
+                              double *d_out, void *workspace, size_t workspace_bytes);
 
 /* Periodic window, all columns of disjoint input bins in one pass: d_edges (nedges, float32,
  * ascending) is the union of the output and input edges; for each of npairs (<= 9) pairs

@@ -2330,8 +2330,8 @@ extern "C" pk_status pk_bin_window_pairs(void *stream, const int32_t meshsize[3]
 
 extern "C" pk_status pk_bin_window_batch(void *stream, const void *value, int nbatch, const int32_t meshsize[3],
                                          const float kfun[3], const float los[3], const float *d_edges, int nedges,
-                                         float step, int backend, int nells, const int32_t *ells, double *d_out,
-                                         void *workspace, size_t workspace_bytes) {
+                                         float step, int backend, int nells, const int32_t *ells, int remove_zero,
+                                         double *d_out, void *workspace, size_t workspace_bytes) {
   PK_REQUIRE(nbatch >= 1 && nbatch <= 65535, PK_ERR_INVALID, "nbatch must be in 1..65535");
   BinGeom g;
   pk_status st = make_geom(meshsize, kfun, nedges, step, backend, &g);
@@ -2351,14 +2351,15 @@ extern "C" pk_status pk_bin_window_batch(void *stream, const void *value, int nb
   const bool even = max_ell <= 4;
   cudaStream_t cs = (cudaStream_t)stream;
   const float2 *a = (const float2 *)value;
-  // k = 0 dropped for every ell: no ell keeps it (zero_l0 = 0)
+  // remove_zero: k = 0 dropped for every ell (no ell keeps it), else kept for all
+  const int keep = remove_zero ? 0 : (1 << nells) - 1;
   switch (nells * 2 + (even ? 1 : 0)) {
 #define PK_WB_CASE(N)                                                                                       \
   case 2 * N:                                                                                               \
-    return launch_global<N, false, false, -1>(cs, g, a, nullptr, los, lc, 0, d_edges, d_out, workspace,     \
+    return launch_global<N, false, false, -1>(cs, g, a, nullptr, los, lc, keep, d_edges, d_out, workspace,  \
                                               workspace_bytes, nbatch);                                     \
   case 2 * N + 1:                                                                                           \
-    return launch_global<N, false, true, -1>(cs, g, a, nullptr, los, lc, 0, d_edges, d_out, workspace,      \
+    return launch_global<N, false, true, -1>(cs, g, a, nullptr, los, lc, keep, d_edges, d_out, workspace,   \
                                              workspace_bytes, nbatch);
     PK_WB_CASE(1) PK_WB_CASE(2) PK_WB_CASE(3) PK_WB_CASE(4) PK_WB_CASE(5)
 #undef PK_WB_CASE

@@ -13,7 +13,8 @@ from .mesh import (MeshAttrs, BaseMeshField, RealMeshField, ComplexMeshField, Pa
 from .mesh2 import (BinMesh2SpectrumPoles, BinMesh2CorrelationPoles, compute_mesh2_spectrum,
                     compute_mesh2_correlation, compute_mesh2, compute_fkp2_normalization,
                     compute_fkp2_shotnoise, compute_box2_normalization, compute_normalization,
-                    compute_box_normalization, compute_mesh2_spectrum_window)
+                    compute_box_normalization, compute_mesh2_spectrum_window,
+                    compute_mesh2_spectrum_mean)
 from .types import (Mesh2SpectrumPole, Mesh2SpectrumPoles, Mesh2CorrelationPole, Mesh2CorrelationPoles, WindowMatrix,
                     read, write)
 from ._lib import load as load_library, LIBRARY_PATH

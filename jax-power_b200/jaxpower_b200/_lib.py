@@ -67,7 +67,7 @@ SIGNATURES = {
                        c_float_p, c_void_p],
     'pk_window_multiply': [c_void_p, c_void_p, c_int, c_void_p, c_int64],
     'pk_bin_window_batch': [c_void_p, c_void_p, c_int, c_int32_p, c_float_p, c_float_p, c_void_p, c_int, c_float,
-                            c_int, c_int, c_int32_p, c_void_p, c_void_p, c_size_t],
+                            c_int, c_int, c_int32_p, c_int, c_void_p, c_void_p, c_size_t],
     'pk_bin_window_pairs': [c_void_p, c_int32_p, c_float_p, c_float_p, c_void_p, c_int, c_float, c_int, c_int,
                             c_int32_p, c_int32_p, c_float, c_void_p, c_void_p, c_size_t],
     'pk_bin_window': [c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_void_p, c_int, c_float, c_int, c_int,

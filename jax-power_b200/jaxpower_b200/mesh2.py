@@ -24,7 +24,7 @@ from .types import Mesh2SpectrumPole, Mesh2SpectrumPoles, Mesh2CorrelationPole, 
 
 __all__ = ['BinMesh2SpectrumPoles', 'compute_mesh2_spectrum', 'compute_mesh2', 'compute_fkp2_normalization',
            'compute_fkp2_shotnoise', 'compute_box2_normalization', 'compute_normalization',
-           'compute_box_normalization', 'compute_mesh2_spectrum_window']
+           'compute_box_normalization', 'compute_mesh2_spectrum_window', 'compute_mesh2_spectrum_mean']
 
 
 def _format_ells(ells):
@@ -815,7 +815,7 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
                     del real
                     _lib.call('pk_bin_window_batch', stream, _lib.ptr(cols), nb, *args_geom, _lib.ptr(bin.d_edges),
                               len(bin._edges1d), bin._step, mattrs.backend_code, len(even),
-                              _lib.i32([ells[ill] for ill in even]), _lib.ptr(raw), _lib.ptr(wsb), wsb.numel())
+                              _lib.i32([ells[ill] for ill in even]), 1, _lib.ptr(raw), _lib.ptr(wsb), wsb.numel())
                     sums[iin, e0:e0 + nb, even] = raw[:nb]
                     del cols
     sums = sums.cpu().numpy() if isinstance(sums, torch.Tensor) else sums
@@ -842,3 +842,137 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     theory = Mesh2SpectrumPoles([Mesh2SpectrumPole(k=kin, k_edges=edgesin, nmodes=np.ones(nin), num_raw=np.zeros(nin),
                                                    ell=ellin) for ellin in ellsin])
     return WindowMatrix(observable=observable, theory=theory, value=wmat)
+
+
+_LEGENDRE_COEFS = {0: (1.,), 1: (0., 1.), 2: (-1. / 2., 0., 3. / 2.), 3: (0., -3. / 2., 0., 5. / 2.),
+                   4: (3. / 8., 0., -15. / 4., 0., 35. / 8.), 5: (0., 15. / 8., 0., -35. / 4., 0., 63. / 8.),
+                   6: (-5. / 16., 0., 105. / 16., 0., -315. / 16., 0., 231. / 16.),
+                   7: (0., -35. / 16., 0., 315. / 16., 0., -693. / 16., 0., 429. / 16.),
+                   8: (35. / 128., 0., -315. / 32., 0., 3465. / 64., 0., -3003. / 32., 0., 6435. / 128.)}
+
+
+def _legendre(ell, x):
+    """L_ell(x) (``utils.py:341-352``) of a device tensor, for theory evaluation on the k grid."""
+    out = torch.zeros_like(x)
+    for c in reversed(_LEGENDRE_COEFS[ell]):
+        out = out * x + c
+    return out
+
+
+def _theory_poles(theory):
+    """Split the ``theory`` argument of compute_mesh2_spectrum_mean (``mesh2.py:1538-1566``)."""
+    poles, kin = theory, None
+    if isinstance(poles, tuple) and isinstance(poles[-1], str):
+        poles = poles[0] if len(poles) == 2 else poles[:-1]
+    if isinstance(poles, tuple):
+        kin, poles = poles
+    if isinstance(poles, Mesh2SpectrumPoles):
+        edges = np.asarray(next(iter(poles)).k_edges, dtype='f8')
+        kin = np.append(edges[..., 0], edges[-1, 1])
+        poles = {ell: poles.get(ell).value() for ell in poles.ells}
+    if isinstance(poles, list):
+        poles = {ell: pole for ell, pole in zip((0, 2, 4), poles)}
+    return kin, poles
+
+
+def compute_mesh2_spectrum_mean(*meshes, theory, bin=None, los='z'):
+    """Mean power-spectrum multipoles from a theory (``mesh2.py:1485-1605``), global line of sight.
+
+    ``theory``: a callable of the k vector (list of three broadcastable device tensors), a
+    dict {ell: callable of |k| or array}, a list (ells 0, 2, 4), ``(kin, poles)`` with array
+    poles, or a ``Mesh2SpectrumPoles``; arrays are read per mode from the bin containing |k|
+    (order-0 ``Interpolator1D``, ``utils.py:507-537``: on ``kin`` as edges when it has one
+    more entry than the poles, else on mid-point edges around ``kin``; 0 outside).
+    ``A = P(k) N / V_cell`` on the half-complex grid (evaluated with torch: the theory is user
+    code), then ``A <- r2c(Q c2r(A))`` with ``Q = c2r(W1 W2*)`` for a selection function, else
+    ``A <- N A``; each even ell is ``(2 ell + 1) bin(A L_ell(mu))`` with k = 0 kept, in one
+    fused binning pass (``pk_bin_window_batch``); odd ell is 0.  The first-point line of
+    sight and the 'jaxdecomp' layout raise ``NotImplementedError``.
+    """
+    meshes, fields = _format_meshes(*meshes)
+    periodic = isinstance(meshes[0], MeshAttrs)
+    if periodic:
+        assert fields[1] == fields[0]
+        mattrs = meshes[0]
+    else:
+        mattrs = meshes[0].attrs
+    if mattrs.fft_backend != 'jax':
+        raise NotImplementedError("the mean spectrum takes the 'jax' FFT backend")
+    los, vlos, swap = _los(los)
+    if vlos is None:
+        raise NotImplementedError('the mean spectrum of the first-point / end-point line of sight is not supported')
+    meshsize = mattrs.meshsize
+    if periodic:
+        N = float(np.prod(meshsize.astype('f8')))
+        norm = N / float(np.prod(mattrs.cellsize.astype('f8')))
+    else:
+        N = np.float32(np.prod(meshsize.astype('f4'), dtype='f4'))
+        norm = np.float32(N / np.float32(np.prod(mattrs.cellsize, dtype='f4')))
+    rnorm = norm / N
+    ells = bin.ells
+    kin, poles = _theory_poles(theory)
+    kvec = mattrs.kcoords(sparse=True)
+    knorm = torch.sqrt(kvec[0] ** 2 + kvec[1] ** 2 + kvec[2] ** 2)
+    mu = (kvec[0] * float(vlos[0]) + kvec[1] * float(vlos[1]) + kvec[2] * float(vlos[2])) / \
+        torch.where(knorm == 0., torch.ones_like(knorm), knorm)
+    if callable(poles):
+        pk = poles(kvec)
+    else:
+        pk = 0.
+        for ell, pole in poles.items():
+            if callable(pole):
+                value = pole(knorm)
+            else:
+                pole = np.asarray(pole, dtype='f8')
+                kin_ = np.asarray(kin, dtype='f8')
+                if len(kin_) == len(pole) + 1:
+                    edges = kin_
+                else:
+                    tmp = (kin_[:-1] + kin_[1:]) / 2.
+                    edges = np.concatenate([[tmp[0] - (kin_[1] - kin_[0])], tmp, [tmp[-1] + (kin_[-1] - kin_[-2])]])
+                d_edges = torch.as_tensor(edges.astype('f4'), device=knorm.device)
+                idx = torch.bucketize(knorm, d_edges, right=True) - 1
+                inside = (idx >= 0) & (idx <= len(edges) - 2)
+                table = torch.as_tensor(pole.astype('f4'), device=knorm.device)
+                value = torch.where(inside, table[idx.clamp(0, len(pole) - 1)], torch.zeros_like(knorm))
+            pk = pk + value * _legendre(int(ell), mu)
+    cshape = tuple(int(n) for n in meshsize[:2]) + (int(meshsize[2]) // 2 + 1,)
+    A = torch.zeros(cshape, dtype=torch.complex64, device=_device())
+    A.real.copy_(torch.as_tensor(pk * rnorm, device=_device()).to(torch.float32).expand(cshape))
+    stream = _lib.stream_handle()
+    if periodic:
+        A = A * float(N)
+    else:
+        A1 = _2c(meshes[0]).value.contiguous()
+        A2 = A1 if fields[1] == fields[0] else _2c(meshes[1]).value.contiguous()
+        prod = torch.empty_like(A1)
+        _lib.call('pk_conj_multiply', stream, _lib.ptr(A2), _lib.ptr(A1), 1, A1.numel(), _lib.ptr(prod))
+        # Q = c2r(W1 W2*) (irfftn's 1 / N), times the 1 / N of the c2r of A, taken unscaled
+        Q = _c2r(prod, meshsize, scale=False, destroy_input=True)
+        del prod, A1, A2
+        _lib.call('pk_scale_real', stream, _lib.ptr(Q), Q.numel(), float(np.float64(np.float32(1.) / N) ** 2))
+        real = _c2r(A, meshsize, scale=False, destroy_input=True)
+        _lib.call('pk_window_multiply', stream, _lib.ptr(real), 1, _lib.ptr(Q), Q.numel())
+        A = _r2c(real, meshsize)
+        del real, Q
+    A = A.contiguous()
+    even = [ill for ill, ell in enumerate(ells) if ell % 2 == 0]
+    num = np.zeros((len(ells), bin.nbins))
+    if even:
+        nbytes = _lib.c_size_t()
+        _lib.call('pk_bin_batch_workspace_size', _lib.i32(meshsize), len(bin._edges1d), len(even), 1,
+                  _lib.ctypes.byref(nbytes))
+        ws = _workspace(nbytes.value)
+        raw = torch.empty((len(even), bin.nbins), dtype=torch.float64, device=_device())
+        _lib.call('pk_bin_window_batch', stream, _lib.ptr(A), 1, _lib.i32(meshsize), _lib.f32(mattrs.kfun),
+                  _lib.f32(vlos), _lib.ptr(bin.d_edges), len(bin._edges1d), bin._step, mattrs.backend_code, len(even),
+                  _lib.i32([ells[ill] for ill in even]), 0, _lib.ptr(raw), _lib.ptr(ws), ws.numel())
+        raw = raw.cpu().numpy()
+        with np.errstate(invalid='ignore', divide='ignore'):
+            for q, ill in enumerate(even):
+                num[ill] = (2 * ells[ill] + 1) * raw[q] / bin.nmodes
+    volume = float(np.prod(mattrs.kfun.astype('f8'))) * bin.nmodes
+    return Mesh2SpectrumPoles([Mesh2SpectrumPole(k=bin.xavg, k_edges=bin.edges, nmodes=bin.nmodes, num_raw=num[ill],
+                                                 norm=np.ones(bin.nbins) * norm, volume=volume, ell=ell,
+                                                 attrs=dict(los=np.asarray(vlos).tolist()))
+                               for ill, ell in enumerate(ells)])

@@ -241,6 +241,58 @@ def compute_mesh2_spectrum_window(bins, edgesin, ellsin, los='z', meshes=None, n
         wmat.append(np.array(rows))
     return np.real(np.concatenate(wmat, axis=0).T)
 
+
+def compute_mesh2_spectrum_mean(bins, theory, los='z', meshes=None):
+    """``compute_mesh2_spectrum_mean(*meshes or mattrs, theory=, bin=bins, los=)``, global line of
+    sight (``mesh2.py:1485-1605``).  ``theory``: a callable of the k vector or a dict
+    {ell: callable of |k|}.  ``meshes``: None (periodic box, float64 normalisation as the
+    reference's ``rdtype = float``) or one / two real selection meshes.
+
+    Returns num_raw (nells, nbins) and norm.
+    """
+    geom = bins.geom
+    dt = geom.dtype
+    t = dt.type
+    ells = bins.ells
+    if meshes is None:
+        N = float(np.prod(geom.meshsize.astype('f8')))
+        norm = N / float(np.prod(geom.cellsize.astype('f8')))
+    else:
+        N = t(np.prod(geom.meshsize.astype(dt)))
+        norm = t(N / t(np.prod(geom.cellsize.astype(dt))))
+    rnorm = norm / N
+    vlos = np.zeros(3)
+    if isinstance(los, str):
+        vlos['xyz'.index(los)] = 1.
+    else:
+        vlos = np.asarray(los, dtype='f8')
+    kvec = kcoords(geom)
+    knorm = bins.knorm()
+    kl = [(kk * t(ll)).astype(dt) for kk, ll in zip(kvec, vlos)]
+    num = (((t(0.) + kl[0]).astype(dt) + kl[1]).astype(dt) + kl[2]).astype(dt)
+    mu = (num / np.where(knorm == 0., t(1.), knorm)).astype(dt)
+    if callable(theory):
+        pk = theory(kvec)
+    else:
+        pk = sum(np.asarray(pole(knorm)) * legendre(ell, mu) for ell, pole in theory.items())
+    A = np.broadcast_to(np.asarray(pk * rnorm, dtype=dt), geom.cshape).astype(np.complex64)
+    if meshes is not None:
+        W = [_to_complex(geom, m) for m in meshes]
+        W2 = W[0] if len(W) == 1 else W[1]
+        Q = c2r(geom, (W[0] * np.conj(W2)).astype(W[0].dtype))
+        A = r2c(geom, (Q * c2r(geom, A)).astype(dt))
+    else:
+        A = (A * N).astype(np.complex64)
+    out = []
+    for ell in ells:
+        leg = legendre(ell, mu)
+        odd = ell % 2
+        if odd:
+            leg = (leg + legendre(ell, (-mu).astype(dt))).astype(dt)
+        value = (2 * ell + 1) / (1 + odd) * bins((A * leg).astype(A.dtype))
+        out.append(np.real(value) if ell % 2 == 0 else np.imag(value))
+    return dict(num_raw=np.array(out), norm=norm)
+
 # --------------------------------------------------------------------------- FKP
 
 def next_fft_size(n, primes=(2, 3, 5, 7), divisors=()):

@@ -105,8 +105,8 @@ def test_window_argument_errors_without_gpu(lib):
     assert lib.pk_bin_window_pairs(None, ms, kf, los, fake, 10, 0., 0, 10, pe, pi, 1., fake, fake, 1 << 20) == 1
     assert lib.pk_bin_window_pairs(None, ms, kf, los, fake, 10, 0., 1, 3, pe, pi, 1., fake, fake, 1 << 20) == 1
     ev = _lib.i32([0, 2, 4, 6, 8, 0])
-    assert lib.pk_bin_window_batch(None, fake, 1, ms, kf, los, fake, 10, 0.01, 0, 6, ev, fake, fake, 1 << 20) == 1
-    assert lib.pk_bin_window_batch(None, fake, 1, ms, kf, los, fake, 10, 0.01, 0, 2, _lib.i32([0, 1]), fake, fake,
+    assert lib.pk_bin_window_batch(None, fake, 1, ms, kf, los, fake, 10, 0.01, 0, 6, ev, 1, fake, fake, 1 << 20) == 1
+    assert lib.pk_bin_window_batch(None, fake, 1, ms, kf, los, fake, 10, 0.01, 0, 2, _lib.i32([0, 1]), 1, fake, fake,
                                    1 << 20) == 1
-    assert lib.pk_bin_window_batch(None, fake, 0, ms, kf, los, fake, 10, 0.01, 0, 2, ev, fake, fake, 1 << 20) == 1
-    assert lib.pk_bin_window_batch(None, None, 1, ms, kf, los, fake, 10, 0.01, 0, 2, ev, fake, fake, 1 << 20) == 1
+    assert lib.pk_bin_window_batch(None, fake, 0, ms, kf, los, fake, 10, 0.01, 0, 2, ev, 1, fake, fake, 1 << 20) == 1
+    assert lib.pk_bin_window_batch(None, None, 1, ms, kf, los, fake, 10, 0.01, 0, 2, ev, 1, fake, fake, 1 << 20) == 1

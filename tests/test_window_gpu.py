@@ -90,3 +90,65 @@ def test_window_norm_and_io(tmp_path):
     assert np.array_equal(back.value, w1.value, equal_nan=True)
     assert back.observable.ells == (0, 2) and back.theory.ells == (0, 2)
     assert np.array_equal(back.theory.get(0).k_edges, w1.theory.get(0).k_edges)
+
+
+def _pk0(k):
+    return 1e4 * (k + 0.02) ** -1.5
+
+
+def _pk2(k):
+    return 3e3 * (k + 0.03) ** -1.2
+
+
+@pytest.mark.parametrize('los', ['z', [0.6, 0., 0.8]])
+@pytest.mark.parametrize('selection', [None, 'auto', 'cross'])
+@pytest.mark.parametrize('meshsize', [(16, 12, 10), (10, 8, 182)])
+def test_mean_spectrum_matches_oracle(los, selection, meshsize):
+    """compute_mesh2_spectrum_mean with theory multipoles (callables of |k|): periodic box and
+    selection functions; k = 0 kept, odd ell 0."""
+    import jaxpower_b200 as jp
+    from oracle.spectrum import compute_mesh2_spectrum_mean as omean
+    boxsize = np.array([500., 400., 300.])
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize)
+    ells = (0, 1, 2, 4)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.02}, ells=ells)
+    ob = Bins(Geometry(meshsize, boxsize), step=0.02, ells=ells)
+    rng = np.random.default_rng(5)
+    sel = [rng.uniform(0.5, 1.5, meshsize).astype('f4') for _ in range(2)]
+    theory = {0: _pk0, 2: _pk2}
+    if selection is None:
+        got = jp.compute_mesh2_spectrum_mean(attrs, theory=theory, bin=b, los=los)
+        ref = omean(ob, theory, los=los)
+    else:
+        use = sel if selection == 'cross' else sel[:1]
+        meshes = [attrs.create(kind='real', fill=torch.as_tensor(s)) for s in use]
+        got = jp.compute_mesh2_spectrum_mean(*meshes, theory=theory, bin=b, los=los)
+        ref = omean(ob, theory, los=los, meshes=use)
+    num = np.array([p.num_raw for p in got])
+    _check(num, ref['num_raw'])
+    assert np.allclose(got.get(0).norm, ref['norm'], rtol=1e-6)
+    assert np.all(got.get(1).num_raw == 0.)
+
+
+def test_mean_spectrum_theory_forms():
+    """A callable of the k vector, array poles on input edges, and the periodic identity
+    mean(P = const) = const."""
+    import jaxpower_b200 as jp
+    from oracle.spectrum import compute_mesh2_spectrum_mean as omean
+    meshsize, boxsize = (16, 16, 16), np.array([400., 400., 400.])
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.02}, ells=(0, 2))
+    ob = Bins(Geometry(meshsize, boxsize), step=0.02, ells=(0, 2))
+
+    def pkvec(kvec):
+        k2 = kvec[0] ** 2 + kvec[1] ** 2 + kvec[2] ** 2
+        return 5e3 / (1. + 100. * k2) * (1. + 0.5 * kvec[2] ** 2 / (k2 + 1e-6))
+
+    got = jp.compute_mesh2_spectrum_mean(attrs, theory=pkvec, bin=b, los='z')
+    ref = omean(ob, pkvec, los='z')
+    _check(np.array([p.num_raw for p in got]), ref['num_raw'])
+    # array poles on edges: a constant monopole over the whole k range gives value() = 1
+    kin = np.array([0., 1.])
+    const = jp.compute_mesh2_spectrum_mean(attrs, theory=(kin, {0: np.array([1.])}), bin=b, los='z')
+    v = const.get(0).value()
+    assert np.allclose(v[np.isfinite(v)], 1., rtol=1e-6)
