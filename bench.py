@@ -423,6 +423,46 @@ def run_paint_only(meshsize=None, reps=3, config=4):
                 status=int(status.item()))
 
 
+def run_window_only(meshsize=None, reps=2):
+    """Profiling aid: window matrices of the global-los multipoles (0, 2, 4), ells_in (0, 2, 4), on
+    a (2000 Mpc/h)^3 box at ``meshsize`` (default 512), output k step 0.005: a selection function
+    (uniform random W in [0.5, 1.5]) with 20 input bins of width 0.01 (60 columns), and the
+    periodic box with the same input bins (one merged pass) and with the output bins as input
+    (diagonal).  One warm-up and ``reps`` timed calls each, device time by CUDA events, with the
+    per-entry-point split of the selection window (``tracing.Timeline``)."""
+    import torch
+    import jaxpower_b200 as jp
+    from jaxpower_b200.tracing import Timeline
+    n = meshsize or 512
+    attrs = jp.MeshAttrs(meshsize=n, boxsize=2000.)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.005}, ells=(0, 2, 4))
+    gen = torch.Generator(device='cuda').manual_seed(0)
+    sel = attrs.create(kind='real', fill=torch.rand((n, n, n), generator=gen, device='cuda') + 0.5)
+    edgesin = np.linspace(0.001, 0.201, 21)
+    cases = {'selection_60_columns': lambda: jp.compute_mesh2_spectrum_window(sel, edgesin=edgesin, ellsin=(0, 2, 4),
+                                                                              bin=b, los='z'),
+             'periodic_60_columns': lambda: jp.compute_mesh2_spectrum_window(attrs, edgesin=edgesin, ellsin=(0, 2, 4),
+                                                                             bin=b, los='z'),
+             'periodic_diagonal': lambda: jp.compute_mesh2_spectrum_window(attrs, edgesin=b._edges1d,
+                                                                           ellsin=(0, 2, 4), bin=b, los='z')}
+    out = dict(meshsize=n)
+    for name, fn in cases.items():
+        fn()
+        torch.cuda.synchronize()
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        e.record()
+        torch.cuda.synchronize()
+        out[name + '_ms'] = a.elapsed_time(e) / reps
+    with Timeline() as tl:
+        cases['selection_60_columns']()
+    torch.cuda.synchronize()
+    out['selection_split_ms'] = {k: round(v['total_ms'], 3) for k, v in tl.summary().items()}
+    return out
+
+
 def run_cutsky_forward_only(meshsize=None, reps=3):
     """Profiling aid: the cut-sky FKP first-point forward pipeline (paint + spectrum) ``reps``
     times, at ``meshsize`` (default that of the cut-sky workload)."""
@@ -776,6 +816,8 @@ def main():
                         help='only time the correction network forward pass (profiling aid)')
     parser.add_argument('--paint-only', action='store_true',
                         help='only paint the benchmark catalog (at --meshsize if given; profiling aid)')
+    parser.add_argument('--window-only', action='store_true',
+                        help='only time window matrices (at --meshsize if given; profiling aid)')
     parser.add_argument('--cutsky-forward-only', action='store_true',
                         help='only run the cut-sky first-point forward pipeline (at --meshsize if given; profiling aid)')
     args = parser.parse_args()
@@ -784,6 +826,9 @@ def main():
         return
     if args.paint_only:
         print(json.dumps({'paint': run_paint_only(args.meshsize or None)}), flush=True)
+        return
+    if args.window_only:
+        print(json.dumps({'window': run_window_only(args.meshsize or None)}), flush=True)
         return
     if args.cutsky_forward_only:
         print(json.dumps({'cutsky_forward': run_cutsky_forward_only(args.meshsize or None)}), flush=True)
