@@ -74,7 +74,10 @@ _PLANS = {}
 
 
 def _plan(meshsize, batch, direction):
-    key = (torch.cuda.current_device(), tuple(int(n) for n in meshsize), int(batch), int(direction))
+    # one plan per stream: a cuFFT plan owns one work area, so transforms enqueued on different
+    # streams (which may run concurrently) must not share a plan
+    key = (torch.cuda.current_device(), tuple(int(n) for n in meshsize), int(batch), int(direction),
+           torch.cuda.current_stream().cuda_stream)
     plan = _PLANS.get(key)
     if plan is None:
         handle = _lib.c_void_p()
