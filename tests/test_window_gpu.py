@@ -84,6 +84,9 @@ def test_window_norm_and_io(tmp_path):
     fin = np.isfinite(w1.value)
     assert np.allclose(w2.value[fin], w1.value[fin] * default / np.float32(128.), rtol=1e-6)
     assert np.allclose(w2.observable.get(0).norm, 128.)
+    # input edges and multipoles taken from a multipole container (mesh2.py:996-998)
+    w3 = jp.compute_mesh2_spectrum_window(attrs, edgesin=w1.observable, bin=b)
+    assert w3.theory.ells == (0, 2) and np.array_equal(w3.value, w1.value, equal_nan=True)
     fn = tmp_path / 'window.npz'
     w1.write(str(fn))
     back = jp.read(str(fn))
@@ -152,3 +155,9 @@ def test_mean_spectrum_theory_forms():
     const = jp.compute_mesh2_spectrum_mean(attrs, theory=(kin, {0: np.array([1.])}), bin=b, los='z')
     v = const.get(0).value()
     assert np.allclose(v[np.isfinite(v)], 1., rtol=1e-6)
+    # a multipole container as the theory: its values read per mode from its k bins
+    poles = jp.Mesh2SpectrumPoles([jp.Mesh2SpectrumPole(k=b.xavg, k_edges=b.edges, nmodes=b.nmodes,
+                                                        num_raw=np.full(b.nbins, 2.), ell=ell) for ell in (0, 2)])
+    both = jp.compute_mesh2_spectrum_mean(attrs, theory=poles, bin=b, los='z')
+    v = both.get(0).value()
+    assert np.allclose(v[np.isfinite(v)][1:], 2., rtol=1e-5)
