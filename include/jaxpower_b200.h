@@ -241,6 +241,17 @@ pk_status pk_bin_window_batch(void *stream, const void *value, int nbatch, const
                               float step, int backend, int nells, const int32_t *ells, int remove_zero,
                               double *d_out, void *workspace, size_t workspace_bytes);
 
+/* First-point mean spectrum (compute_mesh2_spectrum_mean, mesh2.py:1607-1664).
+ * pk_ylm_kgrid_multiply: for nterms (<= 32) real Y_lm, out_t (+)= scale value(k) Y_t(khat) on
+ *   the half-complex 'jax' grid (khat = k / |k|, 0 at k = 0; out_t at out + t N_c).
+ * pk_sum_products: out[i] (+)= sum_t coef[t] a[t n + i] b[t n + i] over nterms (<= 32) pairs of
+ *   real meshes (the Q = sum 4 pi / (2 ell1 + 1) xi G of mesh2.py:1641-1644). */
+pk_status pk_ylm_kgrid_multiply(void *stream, const void *value, const int32_t meshsize[3], const float kfun[3],
+                                int nterms, const int32_t *term_ell, const int32_t *term_m, float scale,
+                                int accumulate, void *out);
+pk_status pk_sum_products(void *stream, float *out, const float *a, const float *b, int nterms, const float *coef,
+                          int64_t n, int accumulate);
+
 /* Periodic window, all columns of disjoint input bins in one pass: d_edges (nedges, float32,
  * ascending) is the union of the output and input edges; for each of npairs (<= 9) pairs
  * (pair_ell, pair_ellin) the float64 sum per merged interval of

@@ -628,3 +628,91 @@ extern "C" pk_status pk_conj_multiply(void *stream, const void *f, const void *a
   PK_LAUNCH_CHECK();
   return PK_OK;
 }
+
+// ------------------------------------------------------ first-point mean spectrum
+// compute_mesh2_spectrum_mean, first-point line of sight (mesh2.py:1607-1664): products of a
+// half-complex mesh with real Y_lm(khat) (khat = k / |k|, 0 at k = 0, as the first-point
+// estimator), and sums of real-mesh products.
+constexpr int KGRID_MAX_TERMS = 32;
+
+struct KgridTerms {
+  int ell[KGRID_MAX_TERMS], m[KGRID_MAX_TERMS];
+};
+
+struct ProductCoefs {
+  float c[KGRID_MAX_TERMS];
+};
+
+__global__ void ylm_kgrid_kernel(Dims d, float kf0, float kf1, float kf2, int nterms, KgridTerms t, float scale,
+                                 int accumulate, const float2 *__restrict__ value, float2 *__restrict__ out) {
+  const int64_t nc = d.ncomplex();
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nc; q += (int64_t)gridDim.x * blockDim.x) {
+    const int z = (int)(q % d.nz);
+    const int64_t row = q / d.nz;
+    const int j = (int)(row % d.n1), i = (int)(row / d.n1);
+    const float kx = kcoord(i, d.n0, kf0, false), ky = kcoord(j, d.n1, kf1, false);
+    const float kz = kcoord(z, d.n2, kf2, true);
+    const float k2 = __fadd_rn(__fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky)), __fmul_rn(kz, kz));
+    const float rn = k2 > 0.f ? rsqrtf(k2) : 0.f;
+    const float2 v = value[q];
+    for (int s = 0; s < nterms; ++s) {
+      const float y = ylm_eval(t.ell[s], t.m[s], kx * rn, ky * rn, kz * rn) * scale;
+      float2 *o = out + (int64_t)s * nc + q;
+      float2 r = make_float2(v.x * y, v.y * y);
+      if (accumulate) {
+        const float2 p = *o;
+        r.x += p.x;
+        r.y += p.y;
+      }
+      *o = r;
+    }
+  }
+}
+
+// out[i] (+)= sum_t coef[t] a[t n + i] b[t n + i]
+__global__ void sum_products_kernel(float *__restrict__ out, const float *__restrict__ a, const float *__restrict__ b,
+                                    int nterms, ProductCoefs coef, int64_t n, int accumulate) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float acc = accumulate ? out[i] : 0.f;
+    for (int t = 0; t < nterms; ++t)
+      acc += coef.c[t] * (a[(int64_t)t * n + i] * b[(int64_t)t * n + i]);
+    out[i] = acc;
+  }
+}
+
+extern "C" pk_status pk_ylm_kgrid_multiply(void *stream, const void *value, const int32_t meshsize[3],
+                                           const float kfun[3], int nterms, const int32_t *term_ell,
+                                           const int32_t *term_m, float scale, int accumulate, void *out) {
+  Dims d;
+  PK_REQUIRE(make_dims(meshsize, &d), PK_ERR_INVALID, "invalid meshsize");
+  PK_REQUIRE(value && kfun && term_ell && term_m && out, PK_ERR_INVALID, "null pointer");
+  PK_REQUIRE(nterms >= 1 && nterms <= KGRID_MAX_TERMS, PK_ERR_INVALID, "nterms must be in 1..%d", KGRID_MAX_TERMS);
+  KgridTerms t;
+  for (int s = 0; s < KGRID_MAX_TERMS; ++s) {
+    t.ell[s] = s < nterms ? term_ell[s] : 0;
+    t.m[s] = s < nterms ? term_m[s] : 0;
+    if (s < nterms)
+      PK_REQUIRE(t.ell[s] >= 0 && t.ell[s] <= YLM_LMAX && t.m[s] >= -t.ell[s] && t.m[s] <= t.ell[s], PK_ERR_INVALID,
+                 "invalid (ell, m) = (%d, %d)", t.ell[s], t.m[s]);
+  }
+  const int64_t want = (d.ncomplex() + 255) / 256;
+  const int blocks = (int)(want < (int64_t)sm_count() * 8 ? want : (int64_t)sm_count() * 8);
+  ylm_kgrid_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(d, kfun[0], kfun[1], kfun[2], nterms, t, scale,
+                                                              accumulate, (const float2 *)value, (float2 *)out);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+extern "C" pk_status pk_sum_products(void *stream, float *out, const float *a, const float *b, int nterms,
+                                     const float *coef, int64_t n, int accumulate) {
+  PK_REQUIRE(out && a && b && coef, PK_ERR_INVALID, "null pointer");
+  PK_REQUIRE(nterms >= 1 && nterms <= KGRID_MAX_TERMS, PK_ERR_INVALID, "nterms must be in 1..%d", KGRID_MAX_TERMS);
+  PK_REQUIRE(n >= 1, PK_ERR_INVALID, "empty meshes");
+  ProductCoefs c;
+  for (int s = 0; s < KGRID_MAX_TERMS; ++s) c.c[s] = s < nterms ? coef[s] : 0.f;
+  const int64_t want = (n + 255) / 256;
+  const int blocks = (int)(want < (int64_t)sm_count() * 8 ? want : (int64_t)sm_count() * 8);
+  sum_products_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(out, a, b, nterms, c, n, accumulate);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}

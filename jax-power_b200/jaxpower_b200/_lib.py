@@ -68,6 +68,9 @@ SIGNATURES = {
     'pk_window_multiply': [c_void_p, c_void_p, c_int, c_void_p, c_int64],
     'pk_bin_window_batch': [c_void_p, c_void_p, c_int, c_int32_p, c_float_p, c_float_p, c_void_p, c_int, c_float,
                             c_int, c_int, c_int32_p, c_int, c_void_p, c_void_p, c_size_t],
+    'pk_ylm_kgrid_multiply': [c_void_p, c_void_p, c_int32_p, c_float_p, c_int, c_int32_p, c_int32_p, c_float,
+                              c_int, c_void_p],
+    'pk_sum_products': [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_float_p, c_int64, c_int],
     'pk_bin_window_pairs': [c_void_p, c_int32_p, c_float_p, c_float_p, c_void_p, c_int, c_float, c_int, c_int,
                             c_int32_p, c_int32_p, c_float, c_void_p, c_void_p, c_size_t],
     'pk_bin_window': [c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_void_p, c_int, c_float, c_int, c_int,

@@ -875,6 +875,89 @@ def _theory_poles(theory):
     return kin, poles
 
 
+def _firstpoint_mean(meshes, fields, periodic, mattrs, bin, poles, get_theory, swap, N, norm, rnorm):
+    """First-point branch of compute_mesh2_spectrum_mean (``mesh2.py:1607-1664``, theory line of
+    sight 'firstpoint', wide-angle order 0).  For each output (ell, m):
+
+        Q = sum over theory (ell1, m1) of 4 pi / (2 ell1 + 1) xi_{ell1 m1} G,
+        xi_{ell1 m1} = c2r(P_ell1(k) rnorm Y_{ell1 m1}(khat)),
+        G = c2r(conj(r2c(W1 Y_{ell m}(xhat) Y_{ell1 m1}(xhat))) A0),   A0 = r2c(W2),
+        A_ell += r2c(Q) Y_{ell m}(khat),
+
+    then 4 pi bin(A_ell) (k = 0 kept), real part for even ell, imaginary for odd, conjugated
+    for the end point.  W = 1 for a periodic box.  Kernels: pk_ylm_premultiply (twice, for
+    the product of two Y_lm), cuFFT, pk_conj_multiply, pk_sum_products, pk_ylm_kgrid_multiply,
+    pk_bin_mesh."""
+    if not isinstance(poles, dict):
+        raise NotImplementedError('the first-point mean spectrum takes theory multipoles, not a callable of k')
+    poles = {(ell if isinstance(ell, tuple) else (ell, 0)): pole for ell, pole in poles.items()}
+    if any(wa != 0 for _, wa in poles):
+        raise NotImplementedError('wide-angle orders > 0 are not supported')
+    meshsize = mattrs.meshsize
+    stream = _lib.stream_handle()
+    if swap:
+        meshes = meshes[::-1]
+    if periodic:
+        rmesh1 = torch.ones(tuple(int(n) for n in meshsize), dtype=torch.float32, device=_device())
+        A0 = _r2c(rmesh1, meshsize)
+    else:
+        rmesh1 = _2r(meshes[0]).value.contiguous()
+        A0 = _2c(meshes[0] if fields[1] == fields[0] else meshes[1]).value.contiguous()
+    offset = (mattrs.boxcenter - (mattrs.boxsize / np.float32(2.)).astype('f4')).astype('f4')
+    cshape = tuple(int(n) for n in meshsize[:2]) + (int(meshsize[2]) // 2 + 1,)
+    rshape = tuple(int(n) for n in meshsize)
+    nreal = int(np.prod(rshape))
+    geo = (_lib.i32(meshsize), _lib.f32(mattrs.cellsize), _lib.f32(offset))
+    # xi_{ell1 m1}, every theory term, kept for all output terms
+    terms1 = [(ell1, m1) for (ell1, _) in poles for m1 in range(-ell1, ell1 + 1)]
+    if len(terms1) > 32:
+        raise NotImplementedError('at most 32 theory (ell, m) terms')
+    coef = np.array([4. * np.pi / (2 * ell1 + 1) for ell1, _ in terms1], dtype='f4')
+    xi_c = torch.empty((len(terms1),) + cshape, dtype=torch.complex64, device=_device())
+    t0 = 0
+    for (ell1, wa), pole in poles.items():
+        kernel = torch.zeros(cshape, dtype=torch.complex64, device=_device())
+        kernel.real.copy_((get_theory(pole) * rnorm).to(torch.float32).expand(cshape))
+        n1 = 2 * ell1 + 1
+        _lib.call('pk_ylm_kgrid_multiply', stream, _lib.ptr(kernel), _lib.i32(meshsize), _lib.f32(mattrs.kfun), n1,
+                  _lib.i32([ell1] * n1), _lib.i32(list(range(-ell1, ell1 + 1))), 1., 0, _lib.ptr(xi_c[t0:t0 + n1]))
+        t0 += n1
+    xi = _c2r(xi_c, meshsize, destroy_input=True)
+    del xi_c
+    t_ell, t_m = _lib.i32([t[0] for t in terms1]), _lib.i32([t[1] for t in terms1])
+    num = []
+    r1 = torch.empty((1,) + rshape, dtype=torch.float32, device=_device())
+    R = torch.empty((len(terms1),) + rshape, dtype=torch.float32, device=_device())
+    Q = torch.empty(rshape, dtype=torch.float32, device=_device())
+    for ell in bin.ells:
+        Aell = torch.zeros(cshape, dtype=torch.complex64, device=_device())
+        for m in range(-ell, ell + 1):
+            _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rmesh1), *geo, 1, _lib.i32([ell]), _lib.i32([m]),
+                      _lib.ptr(r1))
+            _lib.call('pk_ylm_premultiply', stream, _lib.ptr(r1), *geo, len(terms1), t_ell, t_m, _lib.ptr(R))
+            F = _r2c(R, meshsize)
+            _lib.call('pk_conj_multiply', stream, _lib.ptr(F), _lib.ptr(A0), len(terms1), A0.numel(), _lib.ptr(F))
+            G = _c2r(F, meshsize, destroy_input=True)
+            del F
+            _lib.call('pk_sum_products', stream, _lib.ptr(Q), _lib.ptr(xi), _lib.ptr(G), len(terms1), _lib.f32(coef),
+                      nreal, 0)
+            del G
+            FQ = _r2c(Q, meshsize)
+            _lib.call('pk_ylm_kgrid_multiply', stream, _lib.ptr(FQ), _lib.i32(meshsize), _lib.f32(mattrs.kfun), 1,
+                      _lib.i32([ell]), _lib.i32([m]), 1., 1, _lib.ptr(Aell))
+            del FQ
+        value = bin(Aell)  # per-bin mean, k = 0 kept
+        value = 4. * np.pi * value
+        if swap:
+            value = np.conj(value)
+        num.append(value.real if ell % 2 == 0 else value.imag)
+    volume = float(np.prod(mattrs.kfun.astype('f8'))) * bin.nmodes
+    return Mesh2SpectrumPoles([Mesh2SpectrumPole(k=bin.xavg, k_edges=bin.edges, nmodes=bin.nmodes, num_raw=num[ill],
+                                                 norm=np.ones(bin.nbins) * norm, volume=volume, ell=ell,
+                                                 attrs=dict(los='firstpoint' if not swap else 'endpoint'))
+                               for ill, ell in enumerate(bin.ells)])
+
+
 def compute_mesh2_spectrum_mean(*meshes, theory, bin=None, los='z'):
     """Mean power-spectrum multipoles from a theory (``mesh2.py:1485-1605``), global line of sight.
 
@@ -886,8 +969,9 @@ def compute_mesh2_spectrum_mean(*meshes, theory, bin=None, los='z'):
     ``A = P(k) N / V_cell`` on the half-complex grid (evaluated with torch: the theory is user
     code), then ``A <- r2c(Q c2r(A))`` with ``Q = c2r(W1 W2*)`` for a selection function, else
     ``A <- N A``; each even ell is ``(2 ell + 1) bin(A L_ell(mu))`` with k = 0 kept, in one
-    fused binning pass (``pk_bin_window_batch``); odd ell is 0.  The first-point line of
-    sight and the 'jaxdecomp' layout raise ``NotImplementedError``.
+    fused binning pass (``pk_bin_window_batch``); odd ell is 0.  The first-point / end-point
+    line of sight takes theory multipoles (wide-angle order 0) through ``_firstpoint_mean``.
+    The 'jaxdecomp' layout raises ``NotImplementedError``.
     """
     meshes, fields = _format_meshes(*meshes)
     periodic = isinstance(meshes[0], MeshAttrs)
@@ -899,8 +983,6 @@ def compute_mesh2_spectrum_mean(*meshes, theory, bin=None, los='z'):
     if mattrs.fft_backend != 'jax':
         raise NotImplementedError("the mean spectrum takes the 'jax' FFT backend")
     los, vlos, swap = _los(los)
-    if vlos is None:
-        raise NotImplementedError('the mean spectrum of the first-point / end-point line of sight is not supported')
     meshsize = mattrs.meshsize
     if periodic:
         N = float(np.prod(meshsize.astype('f8')))
@@ -913,6 +995,25 @@ def compute_mesh2_spectrum_mean(*meshes, theory, bin=None, los='z'):
     kin, poles = _theory_poles(theory)
     kvec = mattrs.kcoords(sparse=True)
     knorm = torch.sqrt(kvec[0] ** 2 + kvec[1] ** 2 + kvec[2] ** 2)
+
+    def get_theory(pole):
+        if callable(pole):
+            return pole(knorm)
+        pole = np.asarray(pole, dtype='f8')
+        kin_ = np.asarray(kin, dtype='f8')
+        if len(kin_) == len(pole) + 1:
+            edges = kin_
+        else:
+            tmp = (kin_[:-1] + kin_[1:]) / 2.
+            edges = np.concatenate([[tmp[0] - (kin_[1] - kin_[0])], tmp, [tmp[-1] + (kin_[-1] - kin_[-2])]])
+        d_edges = torch.as_tensor(edges.astype('f4'), device=knorm.device)
+        idx = torch.bucketize(knorm, d_edges, right=True) - 1
+        inside = (idx >= 0) & (idx <= len(edges) - 2)
+        table = torch.as_tensor(pole.astype('f4'), device=knorm.device)
+        return torch.where(inside, table[idx.clamp(0, len(pole) - 1)], torch.zeros_like(knorm))
+
+    if vlos is None:
+        return _firstpoint_mean(meshes, fields, periodic, mattrs, bin, poles, get_theory, swap, N, norm, rnorm)
     mu = (kvec[0] * float(vlos[0]) + kvec[1] * float(vlos[1]) + kvec[2] * float(vlos[2])) / \
         torch.where(knorm == 0., torch.ones_like(knorm), knorm)
     if callable(poles):
@@ -920,22 +1021,7 @@ def compute_mesh2_spectrum_mean(*meshes, theory, bin=None, los='z'):
     else:
         pk = 0.
         for ell, pole in poles.items():
-            if callable(pole):
-                value = pole(knorm)
-            else:
-                pole = np.asarray(pole, dtype='f8')
-                kin_ = np.asarray(kin, dtype='f8')
-                if len(kin_) == len(pole) + 1:
-                    edges = kin_
-                else:
-                    tmp = (kin_[:-1] + kin_[1:]) / 2.
-                    edges = np.concatenate([[tmp[0] - (kin_[1] - kin_[0])], tmp, [tmp[-1] + (kin_[-1] - kin_[-2])]])
-                d_edges = torch.as_tensor(edges.astype('f4'), device=knorm.device)
-                idx = torch.bucketize(knorm, d_edges, right=True) - 1
-                inside = (idx >= 0) & (idx <= len(edges) - 2)
-                table = torch.as_tensor(pole.astype('f4'), device=knorm.device)
-                value = torch.where(inside, table[idx.clamp(0, len(pole) - 1)], torch.zeros_like(knorm))
-            pk = pk + value * _legendre(int(ell), mu)
+            pk = pk + get_theory(pole) * _legendre(int(ell[0] if isinstance(ell, tuple) else ell), mu)
     cshape = tuple(int(n) for n in meshsize[:2]) + (int(meshsize[2]) // 2 + 1,)
     A = torch.zeros(cshape, dtype=torch.complex64, device=_device())
     A.real.copy_(torch.as_tensor(pk * rnorm, device=_device()).to(torch.float32).expand(cshape))

@@ -293,6 +293,57 @@ def compute_mesh2_spectrum_mean(bins, theory, los='z', meshes=None):
         out.append(np.real(value) if ell % 2 == 0 else np.imag(value))
     return dict(num_raw=np.array(out), norm=norm)
 
+
+def compute_mesh2_spectrum_mean_firstpoint(bins, theory, meshes=None, swap=False):
+    """``compute_mesh2_spectrum_mean(..., theory=dict, los='firstpoint' / 'endpoint')``
+    (``mesh2.py:1607-1664``, wide-angle order 0): for each output (ell, m),
+    ``Q = sum_{ell1 m1} 4 pi / (2 ell1 + 1) xi_{ell1 m1} c2r(conj(r2c(W1 Y_lm(xhat) Y_l1m1(xhat))) A0)``,
+    ``xi = c2r(P_ell1(|k|) rnorm Y_l1m1(khat))``, ``A_ell += r2c(Q) Y_lm(khat)``; then
+    ``4 pi bin(A_ell)``.  ``theory``: {ell: callable of |k|}; ``meshes``: None (periodic) or
+    one / two real selection meshes.  Returns num_raw (nells, nbins)."""
+    geom = bins.geom
+    dt = geom.dtype
+    t = dt.type
+    if meshes is None:
+        N = float(np.prod(geom.meshsize.astype('f8')))
+        norm = N / float(np.prod(geom.cellsize.astype('f8')))
+        meshes = [np.ones(geom.rshape, dtype=dt)]
+    else:
+        N = t(np.prod(geom.meshsize.astype(dt)))
+        norm = t(N / t(np.prod(geom.cellsize.astype(dt))))
+        meshes = list(meshes)
+    rnorm = norm / N
+    if swap:
+        meshes = meshes[::-1]
+    rmesh1 = _to_real(geom, meshes[0])
+    A0 = _to_complex(geom, meshes[0] if len(meshes) == 1 else meshes[1])
+    xvec = rcoords(geom)
+    kvec = kcoords(geom)
+    knorm = bins.knorm()
+    xi = {}
+    for ell1, pole in theory.items():
+        kernel = (np.asarray(pole(knorm)) * rnorm).astype(dt)
+        for m1 in range(-ell1, ell1 + 1):
+            xi[ell1, m1] = c2r(geom, (kernel * get_ylm(ell1, m1)(*kvec)).astype(np.complex64))
+    out = []
+    for ell in bins.ells:
+        Aell = np.zeros(geom.cshape, dtype=np.complex64)
+        for m in range(-ell, ell + 1):
+            Ylm = get_ylm(ell, m)
+            Q = np.zeros(geom.rshape, dtype=dt)
+            for ell1 in theory:
+                for m1 in range(-ell1, ell1 + 1):
+                    Y1 = get_ylm(ell1, m1)
+                    F = r2c(geom, ((rmesh1 * Ylm(*xvec)).astype(dt) * Y1(*xvec)).astype(dt))
+                    G = c2r(geom, (np.conj(F) * A0).astype(np.complex64))
+                    Q = (Q + t(4. * np.pi / (2 * ell1 + 1)) * xi[ell1, m1] * G).astype(dt)
+            Aell = (Aell + r2c(geom, Q) * Ylm(*kvec)).astype(np.complex64)
+        value = 4. * np.pi * bins(Aell)
+        if swap:
+            value = np.conj(value)
+        out.append(np.real(value) if ell % 2 == 0 else np.imag(value))
+    return np.array(out)
+
 # --------------------------------------------------------------------------- FKP
 
 def next_fft_size(n, primes=(2, 3, 5, 7), divisors=()):

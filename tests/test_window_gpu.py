@@ -161,3 +161,28 @@ def test_mean_spectrum_theory_forms():
     both = jp.compute_mesh2_spectrum_mean(attrs, theory=poles, bin=b, los='z')
     v = both.get(0).value()
     assert np.allclose(v[np.isfinite(v)][1:], 2., rtol=1e-5)
+
+
+@pytest.mark.parametrize('selection', [None, 'auto', 'cross'])
+@pytest.mark.parametrize('los', ['firstpoint', 'endpoint'])
+def test_firstpoint_mean_spectrum_matches_oracle(selection, los):
+    """First-point / end-point mean spectrum (theory multipoles 0 and 2) against the oracle."""
+    import jaxpower_b200 as jp
+    from oracle.spectrum import compute_mesh2_spectrum_mean_firstpoint as omean_fp
+    meshsize, boxsize = (16, 12, 10), np.array([500., 400., 300.])
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=(900., -200., 300.))
+    ells = (0, 1, 2)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.02}, ells=ells)
+    ob = Bins(Geometry(meshsize, boxsize, (900., -200., 300.)), step=0.02, ells=ells)
+    rng = np.random.default_rng(9)
+    sel = [rng.uniform(0.5, 1.5, meshsize).astype('f4') for _ in range(2)]
+    theory = {0: _pk0, 2: _pk2}
+    if selection is None:
+        got = jp.compute_mesh2_spectrum_mean(attrs, theory=theory, bin=b, los=los)
+        ref = omean_fp(ob, theory, swap=los == 'endpoint')
+    else:
+        use = sel if selection == 'cross' else sel[:1]
+        meshes = [attrs.create(kind='real', fill=torch.as_tensor(s)) for s in use]
+        got = jp.compute_mesh2_spectrum_mean(*meshes, theory=theory, bin=b, los=los)
+        ref = omean_fp(ob, theory, meshes=use, swap=los == 'endpoint')
+    _check(np.array([p.num_raw for p in got]), ref)
