@@ -241,7 +241,7 @@ pk_status pk_bin_window_batch(void *stream, const void *value, int nbatch, const
                               float step, int backend, int nells, const int32_t *ells, int remove_zero,
                               double *d_out, void *workspace, size_t workspace_bytes);
 
-/* First-point mean spectrum (compute_mesh2_spectrum_mean, mesh2.py:1607-1664).
+/* First-point mean spectrum (compute_mesh2_spectrum_mean, mesh2.py:1607-1669).
  * pk_ylm_kgrid_multiply: for nterms (<= 32) real Y_lm, out_t (+)= scale value(k) Y_t(khat) on
  *   the half-complex 'jax' grid (khat = k / |k|, 0 at k = 0; out_t at out + t N_c).
  * pk_sum_products: out[i] (+)= sum_t coef[t] a[t n + i] b[t n + i] over nterms (<= 32) pairs of

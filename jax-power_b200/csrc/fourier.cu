@@ -630,7 +630,7 @@ extern "C" pk_status pk_conj_multiply(void *stream, const void *f, const void *a
 }
 
 // ------------------------------------------------------ first-point mean spectrum
-// compute_mesh2_spectrum_mean, first-point line of sight (mesh2.py:1607-1664): products of a
+// compute_mesh2_spectrum_mean, first-point line of sight (mesh2.py:1607-1669): products of a
 // half-complex mesh with real Y_lm(khat) (khat = k / |k|, 0 at k = 0, as the first-point
 // estimator), and sums of real-mesh products.
 constexpr int KGRID_MAX_TERMS = 32;

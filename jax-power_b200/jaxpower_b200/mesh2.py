@@ -876,7 +876,7 @@ def _theory_poles(theory):
 
 
 def _firstpoint_mean(meshes, fields, periodic, mattrs, bin, poles, get_theory, swap, N, norm, rnorm):
-    """First-point branch of compute_mesh2_spectrum_mean (``mesh2.py:1607-1664``, theory line of
+    """First-point branch of compute_mesh2_spectrum_mean (``mesh2.py:1607-1669``, theory line of
     sight 'firstpoint', wide-angle order 0).  For each output (ell, m):
 
         Q = sum over theory (ell1, m1) of 4 pi / (2 ell1 + 1) xi_{ell1 m1} G,

@@ -296,7 +296,7 @@ def compute_mesh2_spectrum_mean(bins, theory, los='z', meshes=None):
 
 def compute_mesh2_spectrum_mean_firstpoint(bins, theory, meshes=None, swap=False):
     """``compute_mesh2_spectrum_mean(..., theory=dict, los='firstpoint' / 'endpoint')``
-    (``mesh2.py:1607-1664``, wide-angle order 0): for each output (ell, m),
+    (``mesh2.py:1607-1669``, wide-angle order 0): for each output (ell, m),
     ``Q = sum_{ell1 m1} 4 pi / (2 ell1 + 1) xi_{ell1 m1} c2r(conj(r2c(W1 Y_lm(xhat) Y_l1m1(xhat))) A0)``,
     ``xi = c2r(P_ell1(|k|) rnorm Y_l1m1(khat))``, ``A_ell += r2c(Q) Y_lm(khat)``; then
     ``4 pi bin(A_ell)``.  ``theory``: {ell: callable of |k|}; ``meshes``: None (periodic) or
