@@ -863,6 +863,8 @@ def _theory_poles(theory):
     """Split the ``theory`` argument of compute_mesh2_spectrum_mean (``mesh2.py:1538-1566``)."""
     poles, kin = theory, None
     if isinstance(poles, tuple) and isinstance(poles[-1], str):
+        if poles[-1] != 'firstpoint':
+            raise NotImplementedError("theory line of sight '{}' is not supported (only 'firstpoint')".format(poles[-1]))
         poles = poles[0] if len(poles) == 2 else poles[:-1]
     if isinstance(poles, tuple):
         kin, poles = poles

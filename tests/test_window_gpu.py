@@ -186,3 +186,8 @@ def test_firstpoint_mean_spectrum_matches_oracle(selection, los):
         got = jp.compute_mesh2_spectrum_mean(*meshes, theory=theory, bin=b, los=los)
         ref = omean_fp(ob, theory, meshes=use, swap=los == 'endpoint')
     _check(np.array([p.num_raw for p in got]), ref)
+    if selection is None and los == 'firstpoint':
+        tagged = jp.compute_mesh2_spectrum_mean(attrs, theory=(theory, 'firstpoint'), bin=b, los=los)
+        assert np.array_equal(np.array([p.num_raw for p in tagged]), np.array([p.num_raw for p in got]))
+        with pytest.raises(NotImplementedError):
+            jp.compute_mesh2_spectrum_mean(attrs, theory=(theory, 'local'), bin=b, los=los)
