@@ -861,10 +861,11 @@ def _legendre(ell, x):
 
 def _theory_poles(theory):
     """Split the ``theory`` argument of compute_mesh2_spectrum_mean (``mesh2.py:1538-1566``)."""
-    poles, kin = theory, None
+    poles, kin, theory_los = theory, None, 'firstpoint'
     if isinstance(poles, tuple) and isinstance(poles[-1], str):
-        if poles[-1] != 'firstpoint':
-            raise NotImplementedError("theory line of sight '{}' is not supported (only 'firstpoint')".format(poles[-1]))
+        theory_los = poles[-1]
+        if theory_los not in ('firstpoint', 'local'):
+            raise NotImplementedError("theory line of sight '{}' is not supported".format(theory_los))
         poles = poles[0] if len(poles) == 2 else poles[:-1]
     if isinstance(poles, tuple):
         kin, poles = poles
@@ -874,10 +875,28 @@ def _theory_poles(theory):
         poles = {ell: poles.get(ell).value() for ell in poles.ells}
     if isinstance(poles, list):
         poles = {ell: pole for ell, pole in zip((0, 2, 4), poles)}
-    return kin, poles
+    return kin, poles, theory_los
 
 
-def _firstpoint_mean(meshes, fields, periodic, mattrs, bin, poles, get_theory, swap, N, norm, rnorm):
+def _local_theory_pairs(poles, get_theory, rnorm):
+    """Kernels of the 'local' theory line of sight (``mesh2.py:1647-1661``): for (ell1, ell2) in
+    {0, 2}^2, K = rnorm sum coeff P_ell (coefficients of L_ell1 L_ell2 on L_0, L_2, L_4), and every
+    (ell1 m1, ell2 m2) pair with its weight (4 pi)^2 / ((2 ell1 + 1) (2 ell2 + 1))."""
+    coeff2 = {(0, 0): [(0, 1.), (4, -7. / 18.)], (0, 2): [(2, 1. / 2.), (4, -5. / 18.)], (2, 2): [(4, 35. / 18.)]}
+    coeff2[2, 0] = coeff2[0, 2]
+    pairs = []
+    for ell1 in (0, 2):
+        for ell2 in (0, 2):
+            kernel = sum(coeff * get_theory(poles[ell, 0]) for ell, coeff in coeff2[ell1, ell2]) * rnorm
+            weight = (4. * np.pi) ** 2 / ((2 * ell1 + 1) * (2 * ell2 + 1))
+            for m1 in range(-ell1, ell1 + 1):
+                for m2 in range(-ell2, ell2 + 1):
+                    pairs.append(((ell1, m1), (ell2, m2), kernel, weight))
+    return pairs
+
+
+def _firstpoint_mean(meshes, fields, periodic, mattrs, bin, poles, get_theory, swap, N, norm, rnorm,
+                     theory_los='firstpoint'):
     """First-point branch of compute_mesh2_spectrum_mean (``mesh2.py:1607-1669``, theory line of
     sight 'firstpoint', wide-angle order 0).  For each output (ell, m):
 
@@ -910,6 +929,9 @@ def _firstpoint_mean(meshes, fields, periodic, mattrs, bin, poles, get_theory, s
     rshape = tuple(int(n) for n in meshsize)
     nreal = int(np.prod(rshape))
     geo = (_lib.i32(meshsize), _lib.f32(mattrs.cellsize), _lib.f32(offset))
+    if theory_los == 'local':
+        return _local_mean(rmesh1, A0, meshes, fields, periodic, mattrs, bin, poles, get_theory, swap, norm, rnorm,
+                           geo)
     # xi_{ell1 m1}, every theory term, kept for all output terms
     terms1 = [(ell1, m1) for (ell1, _) in poles for m1 in range(-ell1, ell1 + 1)]
     if len(terms1) > 32:
@@ -960,6 +982,77 @@ def _firstpoint_mean(meshes, fields, periodic, mattrs, bin, poles, get_theory, s
                                for ill, ell in enumerate(bin.ells)])
 
 
+def _local_mean(rmesh1, A0, meshes, fields, periodic, mattrs, bin, poles, get_theory, swap, norm, rnorm, geo):
+    """'local' theory line of sight of the first-point mean spectrum (``mesh2.py:1646-1661``):
+    for each output (ell, m), Q = sum over pairs (l1 m1, l2 m2) of
+    w xi_pair c2r(conj(r2c(W1 Y_lm Y_l1m1)) r2c(W2 Y_l2m2)), with
+    xi_pair = c2r(K_l1l2(k) Y_l1m1(khat) Y_l2m2(-khat)) (ell2 even: Y_l2m2(-khat) = Y_l2m2(khat))."""
+    meshsize = mattrs.meshsize
+    stream = _lib.stream_handle()
+    cshape = tuple(int(n) for n in meshsize[:2]) + (int(meshsize[2]) // 2 + 1,)
+    rshape = tuple(int(n) for n in meshsize)
+    nreal = int(np.prod(rshape))
+    kf = _lib.f32(mattrs.kfun)
+    if periodic:
+        rmesh2 = rmesh1
+    else:
+        rmesh2 = rmesh1 if fields[1] == fields[0] else _2r(meshes[1]).value.contiguous()
+    terms = [(0, 0)] + [(2, m) for m in range(-2, 3)]
+    t_ell, t_m = _lib.i32([t[0] for t in terms]), _lib.i32([t[1] for t in terms])
+    # B_{l2 m2} = r2c(W2 Y_l2m2(xhat))
+    R = torch.empty((len(terms),) + rshape, dtype=torch.float32, device=_device())
+    _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rmesh2), *geo, len(terms), t_ell, t_m, _lib.ptr(R))
+    B = _r2c(R, meshsize)
+    pairs = _local_theory_pairs(poles, get_theory, rnorm)
+    # xi of every pair, in pair order
+    xi_c = torch.empty((len(pairs),) + cshape, dtype=torch.complex64, device=_device())
+    tmp = torch.empty((1,) + cshape, dtype=torch.complex64, device=_device())
+    for p, ((l1, m1), (l2, m2), kernel, _) in enumerate(pairs):
+        kc = torch.zeros(cshape, dtype=torch.complex64, device=_device())
+        kc.real.copy_(torch.as_tensor(kernel, device=_device()).to(torch.float32).expand(cshape))
+        _lib.call('pk_ylm_kgrid_multiply', stream, _lib.ptr(kc), _lib.i32(meshsize), kf, 1, _lib.i32([l1]),
+                  _lib.i32([m1]), 1., 0, _lib.ptr(tmp))
+        _lib.call('pk_ylm_kgrid_multiply', stream, _lib.ptr(tmp), _lib.i32(meshsize), kf, 1, _lib.i32([l2]),
+                  _lib.i32([m2]), 1., 0, _lib.ptr(xi_c[p]))
+    xi = _c2r(xi_c, meshsize, destroy_input=True)
+    del xi_c, tmp
+    weights = np.array([w for *_, w in pairs], dtype='f4')
+    index = {t: i for i, t in enumerate(terms)}
+    r1 = torch.empty((1,) + rshape, dtype=torch.float32, device=_device())
+    P = torch.empty((len(pairs),) + cshape, dtype=torch.complex64, device=_device())
+    Q = torch.empty(rshape, dtype=torch.float32, device=_device())
+    num = []
+    for ell in bin.ells:
+        Aell = torch.zeros(cshape, dtype=torch.complex64, device=_device())
+        for m in range(-ell, ell + 1):
+            _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rmesh1), *geo, 1, _lib.i32([ell]), _lib.i32([m]),
+                      _lib.ptr(r1))
+            _lib.call('pk_ylm_premultiply', stream, _lib.ptr(r1), *geo, len(terms), t_ell, t_m, _lib.ptr(R))
+            F = _r2c(R, meshsize)
+            for p, (t1, t2, _, _) in enumerate(pairs):
+                _lib.call('pk_conj_multiply', stream, _lib.ptr(F[index[t1]]), _lib.ptr(B[index[t2]]), 1,
+                          B[0].numel(), _lib.ptr(P[p]))
+            G = _c2r(P, meshsize, destroy_input=True)
+            for p0 in range(0, len(pairs), 32):
+                nt = min(32, len(pairs) - p0)
+                _lib.call('pk_sum_products', stream, _lib.ptr(Q), _lib.ptr(xi[p0:p0 + nt]), _lib.ptr(G[p0:p0 + nt]),
+                          nt, _lib.f32(weights[p0:p0 + nt]), nreal, int(p0 > 0))
+            del G, F
+            FQ = _r2c(Q, meshsize)
+            _lib.call('pk_ylm_kgrid_multiply', stream, _lib.ptr(FQ), _lib.i32(meshsize), kf, 1, _lib.i32([ell]),
+                      _lib.i32([m]), 1., 1, _lib.ptr(Aell))
+            del FQ
+        value = 4. * np.pi * bin(Aell)
+        if swap:
+            value = np.conj(value)
+        num.append(value.real if ell % 2 == 0 else value.imag)
+    volume = float(np.prod(mattrs.kfun.astype('f8'))) * bin.nmodes
+    return Mesh2SpectrumPoles([Mesh2SpectrumPole(k=bin.xavg, k_edges=bin.edges, nmodes=bin.nmodes, num_raw=num[ill],
+                                                 norm=np.ones(bin.nbins) * norm, volume=volume, ell=ell,
+                                                 attrs=dict(los='firstpoint' if not swap else 'endpoint'))
+                               for ill, ell in enumerate(bin.ells)])
+
+
 def compute_mesh2_spectrum_mean(*meshes, theory, bin=None, los='z'):
     """Mean power-spectrum multipoles from a theory (``mesh2.py:1485-1605``), global line of sight.
 
@@ -994,7 +1087,7 @@ def compute_mesh2_spectrum_mean(*meshes, theory, bin=None, los='z'):
         norm = np.float32(N / np.float32(np.prod(mattrs.cellsize, dtype='f4')))
     rnorm = norm / N
     ells = bin.ells
-    kin, poles = _theory_poles(theory)
+    kin, poles, theory_los = _theory_poles(theory)
     kvec = mattrs.kcoords(sparse=True)
     knorm = torch.sqrt(kvec[0] ** 2 + kvec[1] ** 2 + kvec[2] ** 2)
 
@@ -1015,7 +1108,8 @@ def compute_mesh2_spectrum_mean(*meshes, theory, bin=None, los='z'):
         return torch.where(inside, table[idx.clamp(0, len(pole) - 1)], torch.zeros_like(knorm))
 
     if vlos is None:
-        return _firstpoint_mean(meshes, fields, periodic, mattrs, bin, poles, get_theory, swap, N, norm, rnorm)
+        return _firstpoint_mean(meshes, fields, periodic, mattrs, bin, poles, get_theory, swap, N, norm, rnorm,
+                                theory_los=theory_los)
     mu = (kvec[0] * float(vlos[0]) + kvec[1] * float(vlos[1]) + kvec[2] * float(vlos[2])) / \
         torch.where(knorm == 0., torch.ones_like(knorm), knorm)
     if callable(poles):

@@ -294,7 +294,7 @@ def compute_mesh2_spectrum_mean(bins, theory, los='z', meshes=None):
     return dict(num_raw=np.array(out), norm=norm)
 
 
-def compute_mesh2_spectrum_mean_firstpoint(bins, theory, meshes=None, swap=False):
+def compute_mesh2_spectrum_mean_firstpoint(bins, theory, meshes=None, swap=False, theory_los='firstpoint'):
     """``compute_mesh2_spectrum_mean(..., theory=dict, los='firstpoint' / 'endpoint')``
     (``mesh2.py:1607-1669``, wide-angle order 0): for each output (ell, m),
     ``Q = sum_{ell1 m1} 4 pi / (2 ell1 + 1) xi_{ell1 m1} c2r(conj(r2c(W1 Y_lm(xhat) Y_l1m1(xhat))) A0)``,
@@ -320,6 +320,37 @@ def compute_mesh2_spectrum_mean_firstpoint(bins, theory, meshes=None, swap=False
     xvec = rcoords(geom)
     kvec = kcoords(geom)
     knorm = bins.knorm()
+    if theory_los == 'local':  # mesh2.py:1646-1661
+        rmesh2 = rmesh1 if len(meshes) == 1 else _to_real(geom, meshes[1])
+        coeff2 = {(0, 0): [(0, 1.), (4, -7. / 18.)], (0, 2): [(2, 1. / 2.), (4, -5. / 18.)], (2, 2): [(4, 35. / 18.)]}
+        coeff2[2, 0] = coeff2[0, 2]
+        xil, Bl = {}, {}
+        for ell1 in (0, 2):
+            for ell2 in (0, 2):
+                kernel = (sum(c * np.asarray(theory[ell](knorm)) for ell, c in coeff2[ell1, ell2]) * rnorm).astype(dt)
+                for m1 in range(-ell1, ell1 + 1):
+                    for m2 in range(-ell2, ell2 + 1):
+                        y = (kernel * get_ylm(ell1, m1)(*kvec)).astype(dt) * get_ylm(ell2, m2)(*[-kk for kk in kvec])
+                        xil[ell1, m1, ell2, m2] = c2r(geom, y.astype(np.complex64))
+        for ell2 in (0, 2):
+            for m2 in range(-ell2, ell2 + 1):
+                Bl[ell2, m2] = r2c(geom, (rmesh2 * get_ylm(ell2, m2)(*xvec)).astype(dt))
+        out = []
+        for ell in bins.ells:
+            Aell = np.zeros(geom.cshape, dtype=np.complex64)
+            for m in range(-ell, ell + 1):
+                Ylm = get_ylm(ell, m)
+                Q = np.zeros(geom.rshape, dtype=dt)
+                for (ell1, m1, ell2, m2), x in xil.items():
+                    F = r2c(geom, ((rmesh1 * Ylm(*xvec)).astype(dt) * get_ylm(ell1, m1)(*xvec)).astype(dt))
+                    G = c2r(geom, (np.conj(F) * Bl[ell2, m2]).astype(np.complex64))
+                    Q = (Q + t((4. * np.pi) ** 2 / ((2 * ell1 + 1) * (2 * ell2 + 1))) * x * G).astype(dt)
+                Aell = (Aell + r2c(geom, Q) * Ylm(*kvec)).astype(np.complex64)
+            value = 4. * np.pi * bins(Aell)
+            if swap:
+                value = np.conj(value)
+            out.append(np.real(value) if ell % 2 == 0 else np.imag(value))
+        return np.array(out)
     xi = {}
     for ell1, pole in theory.items():
         kernel = (np.asarray(pole(knorm)) * rnorm).astype(dt)

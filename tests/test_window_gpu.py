@@ -190,4 +190,27 @@ def test_firstpoint_mean_spectrum_matches_oracle(selection, los):
         tagged = jp.compute_mesh2_spectrum_mean(attrs, theory=(theory, 'firstpoint'), bin=b, los=los)
         assert np.array_equal(np.array([p.num_raw for p in tagged]), np.array([p.num_raw for p in got]))
         with pytest.raises(NotImplementedError):
-            jp.compute_mesh2_spectrum_mean(attrs, theory=(theory, 'local'), bin=b, los=los)
+            jp.compute_mesh2_spectrum_mean(attrs, theory=(theory, 'other'), bin=b, los=los)
+
+
+@pytest.mark.parametrize('selection', [None, 'auto', 'cross'])
+def test_local_theory_mean_spectrum_matches_oracle(selection):
+    """Mean spectrum with the 'local' theory line of sight (theory multipoles 0, 2, 4)."""
+    import jaxpower_b200 as jp
+    from oracle.spectrum import compute_mesh2_spectrum_mean_firstpoint as omean_fp
+    meshsize, boxsize, center = (12, 10, 8), np.array([500., 400., 300.]), (900., -200., 300.)
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=center)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.02}, ells=(0, 2))
+    ob = Bins(Geometry(meshsize, boxsize, center), step=0.02, ells=(0, 2))
+    rng = np.random.default_rng(11)
+    sel = [rng.uniform(0.5, 1.5, meshsize).astype('f4') for _ in range(2)]
+    theory = {0: _pk0, 2: _pk2, 4: lambda k: 1e3 * (k + 0.05) ** -1.}
+    if selection is None:
+        got = jp.compute_mesh2_spectrum_mean(attrs, theory=(theory, 'local'), bin=b, los='firstpoint')
+        ref = omean_fp(ob, theory, theory_los='local')
+    else:
+        use = sel if selection == 'cross' else sel[:1]
+        meshes = [attrs.create(kind='real', fill=torch.as_tensor(s)) for s in use]
+        got = jp.compute_mesh2_spectrum_mean(*meshes, theory=(theory, 'local'), bin=b, los='firstpoint')
+        ref = omean_fp(ob, theory, meshes=use, theory_los='local')
+    _check(np.array([p.num_raw for p in got]), ref)
