@@ -720,9 +720,10 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     k = 0 dropped, with ``rnorm = (N / V_cell) / norm / N``; odd ell rows are 0 (the
     reference's Legendre sum vanishes for odd ell).  Returns a ``WindowMatrix`` of shape
     (len(ells) nbins, len(ellsin) len(edgesin)).  ``buffer`` and ``pbar`` are accepted and
-    have no effect; ``batch_size`` caps the columns per FFT batch.  The first-point line of
-    sight, the 'smooth' / 'infinite' flags and the 'jaxdecomp' backend raise
-    ``NotImplementedError``.
+    have no effect; ``batch_size`` caps the columns per FFT batch.  The first-point /
+    end-point line of sight (theory line of sight 'firstpoint', wide-angle order 0) goes
+    through ``_firstpoint_window``.  The 'local' theory line of sight, the 'smooth' /
+    'infinite' flags and the 'jaxdecomp' backend raise ``NotImplementedError``.
     """
     from .types import WindowMatrix
     flags = tuple(flags)
@@ -738,8 +739,6 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     if mattrs.fft_backend != 'jax':
         raise NotImplementedError("the window matrix takes the 'jax' FFT backend")
     los, vlos, swap = _los(los)
-    if vlos is None:
-        raise NotImplementedError('the window matrix of the first-point / end-point line of sight is not supported')
     f4 = np.float32
     ells = bin.ells
     nbins, nells = bin.nbins, len(ells)
@@ -750,6 +749,22 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     if norm.ndim <= 1:
         norm = norm * np.ones(nells, dtype='f4')
     rnorm = (_norm / norm / N).astype('f4')
+    if vlos is None:
+        theory_los = 'firstpoint'
+        if isinstance(ellsin, (tuple, list)) and len(ellsin) == 2 and isinstance(ellsin[1], str):
+            ellsin, theory_los = ellsin
+        if theory_los != 'firstpoint':
+            raise NotImplementedError("theory line of sight '{}' is not supported for the window".format(theory_los))
+        if ellsin is not None and np.ndim(ellsin) == 0:
+            ellsin = (ellsin,)
+        if ellsin is not None:
+            ellsin = [e if isinstance(e, tuple) else (int(e), 0) for e in ellsin]
+            if any(wa != 0 for _, wa in ellsin):
+                raise NotImplementedError('wide-angle orders > 0 are not supported')
+            ellsin = [e for e, _ in ellsin]
+        edgesin, ellsin = _window_edges(edgesin, ellsin)
+        wmat = _firstpoint_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm, batch_size)
+        return _window_matrix(bin, norm, edgesin, ellsin, wmat)
     edgesin, ellsin = _window_edges(edgesin, ellsin)
     nin = len(edgesin)
     klo, khi = edgesin[:, 0].astype('f4'), edgesin[:, -1].astype('f4')
@@ -833,15 +848,104 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     else:
         wmat = [spectra[iin].reshape(nin, -1) for iin in range(len(ellsin))]
     wmat = np.concatenate(wmat, axis=0).T
+    return _window_matrix(bin, norm, edgesin, ellsin, wmat)
 
+
+def _window_matrix(bin, norm, edgesin, ellsin, wmat):
+    """The ``WindowMatrix`` of ``mesh2.py:1462-1482``: output multipoles on ``bin`` with
+    ``norm`` per ell, theory multipoles on the input edges (``k`` their mid-points)."""
+    from .types import WindowMatrix
+    nbins, nin = bin.nbins, len(edgesin)
     observable = Mesh2SpectrumPoles([Mesh2SpectrumPole(k=bin.xavg, k_edges=bin.edges, nmodes=bin.nmodes,
                                                        num_raw=np.zeros(nbins), num_shotnoise=np.zeros(nbins),
                                                        norm=np.ones(nbins) * norm[ill], ell=ell)
-                                     for ill, ell in enumerate(ells)])
+                                     for ill, ell in enumerate(bin.ells)])
     kin = np.mean(edgesin, axis=-1)
     theory = Mesh2SpectrumPoles([Mesh2SpectrumPole(k=kin, k_edges=edgesin, nmodes=np.ones(nin), num_raw=np.zeros(nin),
                                                    ell=ellin) for ellin in ellsin])
     return WindowMatrix(observable=observable, theory=theory, value=wmat)
+
+
+def _firstpoint_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm, batch_size=None):
+    """First-point window matrix, input power on the mesh, wide-angle order 0
+    (``mesh2.py:1264-1304``, ``1462-1470``).  For each input ell_in:
+
+        Q_{ell m m1} = 4 pi / (2 ell_in + 1) c2r(conj(r2c(W1 Y_lm(xhat) Y_{ell_in m1}(xhat))) A0),
+
+    kept for every output (ell, m); then per input bin [k_lo, k_hi] (both ends included),
+    ``xi_m1 = c2r(1{k_lo <= |k| <= k_hi} Y_{ell_in m1}(khat))``,
+    ``A_ell = sum_m r2c(sum_m1 xi_m1 Q_{ell m m1}) Y_lm(khat)`` and the column is
+    ``4 pi rnorm bin(A_ell)`` with k = 0 dropped for ell = 0 only (``remove_zero=ell == 0``).
+    The real part is kept, but the first multipole's rows take the imaginary part when that
+    multipole is odd (``mesh2.py:1464-1469`` advances only over the first multipole)."""
+    meshsize = mattrs.meshsize
+    stream = _lib.stream_handle()
+    if swap:
+        meshes = meshes[::-1]
+    if periodic:
+        rmesh1 = torch.ones(tuple(int(n) for n in meshsize), dtype=torch.float32, device=_device())
+        A0 = _r2c(rmesh1, meshsize)
+    else:
+        rmesh1 = _2r(meshes[0]).value.contiguous()
+        A0 = _2c(meshes[0] if fields[1] == fields[0] else meshes[1]).value.contiguous()
+    offset = (mattrs.boxcenter - (mattrs.boxsize / np.float32(2.)).astype('f4')).astype('f4')
+    geo = (_lib.i32(meshsize), _lib.f32(mattrs.cellsize), _lib.f32(offset))
+    kf = _lib.f32(mattrs.kfun)
+    cshape = tuple(int(n) for n in meshsize[:2]) + (int(meshsize[2]) // 2 + 1,)
+    rshape = tuple(int(n) for n in meshsize)
+    nreal = int(np.prod(rshape))
+    ells = bin.ells
+    out_terms = [(ell, m) for ell in ells for m in range(-ell, ell + 1)]
+    kvec = mattrs.kcoords(sparse=True)
+    knorm = torch.sqrt(kvec[0] ** 2 + kvec[1] ** 2 + kvec[2] ** 2)
+    r1 = torch.empty((1,) + rshape, dtype=torch.float32, device=_device())
+    blocks = []
+    for ellin in ellsin:
+        n1 = 2 * ellin + 1
+        if n1 > 32:
+            raise NotImplementedError('ell_in <= 15')
+        in_ell, in_m = _lib.i32([ellin] * n1), _lib.i32(list(range(-ellin, ellin + 1)))
+        # Q[t] for output term t: (n1, N) real meshes
+        Q = torch.empty((len(out_terms), n1) + rshape, dtype=torch.float32, device=_device())
+        R = torch.empty((n1,) + rshape, dtype=torch.float32, device=_device())
+        for t, (ell, m) in enumerate(out_terms):
+            _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rmesh1), *geo, 1, _lib.i32([ell]), _lib.i32([m]),
+                      _lib.ptr(r1))
+            _lib.call('pk_ylm_premultiply', stream, _lib.ptr(r1), *geo, n1, in_ell, in_m, _lib.ptr(R))
+            F = _r2c(R, meshsize)
+            _lib.call('pk_conj_multiply', stream, _lib.ptr(F), _lib.ptr(A0), n1, A0.numel(), _lib.ptr(F))
+            Q[t] = _c2r(F, meshsize, destroy_input=True)
+            del F
+        coef = np.full(n1, 4. * np.pi / (2 * ellin + 1), dtype='f4')
+        rows = []
+        tmp = torch.empty(rshape, dtype=torch.float32, device=_device())
+        for lo, hi in edgesin.astype('f4'):
+            tophat = ((knorm >= float(lo)) & (knorm <= float(hi))).to(torch.complex64)
+            xi_c = torch.empty((n1,) + cshape, dtype=torch.complex64, device=_device())
+            _lib.call('pk_ylm_kgrid_multiply', stream, _lib.ptr(tophat), _lib.i32(meshsize), kf, n1, in_ell, in_m, 1.,
+                      0, _lib.ptr(xi_c))
+            xi = _c2r(xi_c, meshsize, destroy_input=True)
+            del xi_c
+            spectrum = []
+            for ill, ell in enumerate(ells):
+                Aell = torch.zeros(cshape, dtype=torch.complex64, device=_device())
+                for m in range(-ell, ell + 1):
+                    t = out_terms.index((ell, m))
+                    _lib.call('pk_sum_products', stream, _lib.ptr(tmp), _lib.ptr(xi), _lib.ptr(Q[t]), n1,
+                              _lib.f32(coef), nreal, 0)
+                    Ft = _r2c(tmp, meshsize)
+                    _lib.call('pk_ylm_kgrid_multiply', stream, _lib.ptr(Ft), _lib.i32(meshsize), kf, 1,
+                              _lib.i32([ell]), _lib.i32([m]), 1., 1, _lib.ptr(Aell))
+                spectrum.append(4. * np.pi * bin(Aell, remove_zero=ell == 0) * float(rnorm[ill]))
+            rows.append(np.concatenate(spectrum))
+        blocks.append(np.array(rows))
+        del Q, R
+    wmat = np.concatenate(blocks, axis=0).T
+    nb = bin.nbins
+    first = wmat[:nb].imag if ells[0] % 2 else wmat[:nb].real
+    wmat = wmat.real.copy()
+    wmat[:nb] = first
+    return wmat
 
 
 _LEGENDRE_COEFS = {0: (1.,), 1: (0., 1.), 2: (-1. / 2., 0., 3. / 2.), 3: (0., -3. / 2., 0., 5. / 2.),

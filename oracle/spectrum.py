@@ -375,6 +375,61 @@ def compute_mesh2_spectrum_mean_firstpoint(bins, theory, meshes=None, swap=False
         out.append(np.real(value) if ell % 2 == 0 else np.imag(value))
     return np.array(out)
 
+
+def compute_mesh2_spectrum_window_firstpoint(bins, edgesin, ellsin, meshes=None, swap=False, norm=None):
+    """``compute_mesh2_spectrum_window(..., los='firstpoint' / 'endpoint')``, input power on the
+    mesh, wide-angle order 0 (``mesh2.py:1135-1304``, ``1462-1470``).  ``meshes``: None
+    (periodic box) or one / two real selection meshes.  Returns the window matrix
+    (len(ells) nbins, len(ellsin) len(edgesin))."""
+    geom = bins.geom
+    dt = geom.dtype
+    t = dt.type
+    ells = bins.ells
+    N = t(np.prod(geom.meshsize.astype(dt)))
+    _norm = t(N / t(np.prod(geom.cellsize.astype(dt))))
+    norm = np.asarray(_norm if norm is None else norm, dtype=dt)
+    if norm.ndim <= 1:
+        norm = norm * np.ones(len(ells), dtype=dt)
+    rnorm = (_norm / norm / N).astype(dt)
+    edgesin = np.asarray(edgesin, dtype='f8')
+    if edgesin.ndim != 2:
+        edgesin = np.column_stack([edgesin[:-1], edgesin[1:]])
+    meshes = [np.ones(geom.rshape, dtype=dt)] if meshes is None else list(meshes)
+    if swap:
+        meshes = meshes[::-1]
+    rmesh1 = _to_real(geom, meshes[0])
+    A0 = _to_complex(geom, meshes[0] if len(meshes) == 1 else meshes[1])
+    xvec = rcoords(geom)
+    kvec = kcoords(geom)
+    knorm = bins.knorm()
+    blocks = []
+    for ellin in ellsin:
+        Qs = {}
+        for ell in ells:
+            for m in range(-ell, ell + 1):
+                for m1 in range(-ellin, ellin + 1):
+                    F = r2c(geom, ((rmesh1 * get_ylm(ell, m)(*xvec)).astype(dt) * get_ylm(ellin, m1)(*xvec)).astype(dt))
+                    Qs[ell, m, m1] = (t(4. * np.pi / (2 * ellin + 1)) * c2r(geom, (np.conj(F) * A0).astype(np.complex64))).astype(dt)
+        rows = []
+        for lo, hi in edgesin.astype(dt):
+            xi = {m1: c2r(geom, (((knorm >= lo) & (knorm <= hi)) * get_ylm(ellin, m1)(*kvec)).astype(np.complex64))
+                  for m1 in range(-ellin, ellin + 1)}
+            spectrum = []
+            for ill, ell in enumerate(ells):
+                Aell = np.zeros(geom.cshape, dtype=np.complex64)
+                for m in range(-ell, ell + 1):
+                    tmp = sum(xi[m1] * Qs[ell, m, m1] for m1 in xi).astype(dt)
+                    Aell = (Aell + r2c(geom, tmp) * get_ylm(ell, m)(*kvec)).astype(np.complex64)
+                spectrum.append(4. * np.pi * bins(Aell, remove_zero=ell == 0) * rnorm[ill])
+            rows.append(np.concatenate(spectrum))
+        blocks.append(np.array(rows))
+    wmat = np.concatenate(blocks, axis=0).T
+    nb = bins.nbins
+    first = wmat[:nb].imag if ells[0] % 2 else wmat[:nb].real
+    wmat = wmat.real.copy()
+    wmat[:nb] = first
+    return wmat
+
 # --------------------------------------------------------------------------- FKP
 
 def next_fft_size(n, primes=(2, 3, 5, 7), divisors=()):

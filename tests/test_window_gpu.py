@@ -214,3 +214,29 @@ def test_local_theory_mean_spectrum_matches_oracle(selection):
         got = jp.compute_mesh2_spectrum_mean(*meshes, theory=(theory, 'local'), bin=b, los='firstpoint')
         ref = omean_fp(ob, theory, meshes=use, theory_los='local')
     _check(np.array([p.num_raw for p in got]), ref)
+
+
+@pytest.mark.parametrize('selection', [None, 'auto', 'cross'])
+@pytest.mark.parametrize('los', ['firstpoint', 'endpoint'])
+def test_firstpoint_window_matches_oracle(selection, los):
+    """First-point / end-point window matrix (input power on the mesh) against the oracle."""
+    import jaxpower_b200 as jp
+    from oracle.spectrum import compute_mesh2_spectrum_window_firstpoint as owin_fp
+    meshsize, boxsize, center = (12, 10, 8), np.array([500., 400., 300.]), (900., -200., 300.)
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=center)
+    ells = (0, 2) if selection != 'cross' else (1, 2)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.02}, ells=ells)
+    ob = Bins(Geometry(meshsize, boxsize, center), step=0.02, ells=ells)
+    rng = np.random.default_rng(13)
+    sel = [rng.uniform(0.5, 1.5, meshsize).astype('f4') for _ in range(2)]
+    edgesin = np.arange(0., 0.06, 0.015)
+    if selection is None:
+        w = jp.compute_mesh2_spectrum_window(attrs, edgesin=edgesin, ellsin=((0, 2), 'firstpoint'), bin=b, los=los)
+        ref = owin_fp(ob, edgesin, (0, 2), swap=los == 'endpoint')
+    else:
+        use = sel if selection == 'cross' else sel[:1]
+        meshes = [attrs.create(kind='real', fill=torch.as_tensor(s)) for s in use]
+        w = jp.compute_mesh2_spectrum_window(*meshes, edgesin=edgesin, ellsin=(0, 2), bin=b, los=los)
+        ref = owin_fp(ob, edgesin, (0, 2), meshes=use, swap=los == 'endpoint')
+    _check(w.value, ref)
+    assert w.theory.ells == (0, 2)
