@@ -722,8 +722,9 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     (len(ells) nbins, len(ellsin) len(edgesin)).  ``buffer`` and ``pbar`` are accepted and
     have no effect; ``batch_size`` caps the columns per FFT batch.  The first-point /
     end-point line of sight (theory line of sight 'firstpoint', wide-angle order 0) goes
-    through ``_firstpoint_window``.  The 'local' theory line of sight, the 'smooth' /
-    'infinite' flags and the 'jaxdecomp' backend raise ``NotImplementedError``.
+    through ``_firstpoint_window``, the 'local' theory line of sight (``ellsin=(ells, 'local')``)
+    through ``_local_window``.  The 'smooth' / 'infinite' flags and the 'jaxdecomp' backend
+    raise ``NotImplementedError``.
     """
     from .types import WindowMatrix
     flags = tuple(flags)
@@ -753,7 +754,7 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
         theory_los = 'firstpoint'
         if isinstance(ellsin, (tuple, list)) and len(ellsin) == 2 and isinstance(ellsin[1], str):
             ellsin, theory_los = ellsin
-        if theory_los != 'firstpoint':
+        if theory_los not in ('firstpoint', 'local'):
             raise NotImplementedError("theory line of sight '{}' is not supported for the window".format(theory_los))
         if ellsin is not None and np.ndim(ellsin) == 0:
             ellsin = (ellsin,)
@@ -763,7 +764,10 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
                 raise NotImplementedError('wide-angle orders > 0 are not supported')
             ellsin = [e for e, _ in ellsin]
         edgesin, ellsin = _window_edges(edgesin, ellsin)
-        wmat = _firstpoint_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm, batch_size)
+        if theory_los == 'local':
+            wmat = _local_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm)
+        else:
+            wmat = _firstpoint_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm, batch_size)
         return _window_matrix(bin, norm, edgesin, ellsin, wmat)
     edgesin, ellsin = _window_edges(edgesin, ellsin)
     nin = len(edgesin)
@@ -864,6 +868,106 @@ def _window_matrix(bin, norm, edgesin, ellsin, wmat):
     theory = Mesh2SpectrumPoles([Mesh2SpectrumPole(k=kin, k_edges=edgesin, nmodes=np.ones(nin), num_raw=np.zeros(nin),
                                                    ell=ellin) for ellin in ellsin])
     return WindowMatrix(observable=observable, theory=theory, value=wmat)
+
+
+def _local_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm):
+    """Window matrix with the 'local' theory line of sight (``mesh2.py:1398-1455``).  For each
+    (ell1, ell2) in {2, 0}^2 and output (ell, m), the (m1, m2) pairs give
+    ``Q = (4 pi)^2 / ((2 ell1 + 1) (2 ell2 + 1)) c2r(conj(r2c(W1 Y_lm Y_l1m1)) r2c(W2 Y_l2m2))``;
+    each input bin [k_lo, k_hi] (ends included) gives
+    ``xi = c2r(1{shell} Y_l1m1(khat) Y_l2m2(-khat))`` per pair and the block column
+    ``4 pi rnorm bin(sum_m r2c(sum_pairs xi Q) Y_lm(khat))`` (k = 0 dropped for ell = 0).  The
+    blocks combine into the input multipoles 0, 2, 4 with the coefficients of L_ell1 L_ell2 on
+    L_0, L_2, L_4."""
+    if any(ell not in (0, 2, 4) for ell in ellsin):
+        raise ValueError("the 'local' theory line of sight takes input multipoles among (0, 2, 4)")
+    meshsize = mattrs.meshsize
+    stream = _lib.stream_handle()
+    if swap:
+        meshes = meshes[::-1]
+    if periodic:
+        rmesh1 = torch.ones(tuple(int(n) for n in meshsize), dtype=torch.float32, device=_device())
+        rmesh2 = rmesh1
+    else:
+        rmesh1 = _2r(meshes[0]).value.contiguous()
+        rmesh2 = rmesh1 if fields[1] == fields[0] else _2r(meshes[1]).value.contiguous()
+    offset = (mattrs.boxcenter - (mattrs.boxsize / np.float32(2.)).astype('f4')).astype('f4')
+    geo = (_lib.i32(meshsize), _lib.f32(mattrs.cellsize), _lib.f32(offset))
+    kf = _lib.f32(mattrs.kfun)
+    cshape = tuple(int(n) for n in meshsize[:2]) + (int(meshsize[2]) // 2 + 1,)
+    rshape = tuple(int(n) for n in meshsize)
+    nreal = int(np.prod(rshape))
+    ells = bin.ells
+    out_terms = [(ell, m) for ell in ells for m in range(-ell, ell + 1)]
+    kvec = mattrs.kcoords(sparse=True)
+    knorm = torch.sqrt(kvec[0] ** 2 + kvec[1] ** 2 + kvec[2] ** 2)
+    # B_{l2 m2} = r2c(W2 Y_l2m2(xhat)), l2 in (0, 2)
+    t2 = [(0, 0)] + [(2, m) for m in range(-2, 3)]
+    R2 = torch.empty((len(t2),) + rshape, dtype=torch.float32, device=_device())
+    _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rmesh2), *geo, len(t2), _lib.i32([t[0] for t in t2]),
+              _lib.i32([t[1] for t in t2]), _lib.ptr(R2))
+    B = _r2c(R2, meshsize)
+    del R2
+    index2 = {t: i for i, t in enumerate(t2)}
+    coeff2 = {(0, 0): [(0, 1.), (4, -7. / 18.)], (0, 2): [(2, 1. / 2.), (4, -5. / 18.)], (2, 2): [(4, 35. / 18.)]}
+    coeff2[2, 0] = coeff2[0, 2]
+    r1 = torch.empty((1,) + rshape, dtype=torch.float32, device=_device())
+    tmp = torch.empty(rshape, dtype=torch.float32, device=_device())
+    one = torch.empty((1,) + cshape, dtype=torch.complex64, device=_device())
+    nin, nb = len(edgesin), bin.nbins
+    wmat = np.zeros((len(ellsin), nin, len(ells) * nb), dtype='c16')
+    for ell1 in (2, 0):
+        for ell2 in (2, 0):
+            pairs = [((ell1, m1), (ell2, m2)) for m1 in range(-ell1, ell1 + 1) for m2 in range(-ell2, ell2 + 1)]
+            npair = len(pairs)
+            weight = np.full(npair, (4. * np.pi) ** 2 / ((2 * ell1 + 1) * (2 * ell2 + 1)), dtype='f4')
+            n1 = 2 * ell1 + 1
+            in_ell, in_m = _lib.i32([ell1] * n1), _lib.i32(list(range(-ell1, ell1 + 1)))
+            R = torch.empty((n1,) + rshape, dtype=torch.float32, device=_device())
+            Q = torch.empty((len(out_terms), npair) + rshape, dtype=torch.float32, device=_device())
+            P = torch.empty((npair,) + cshape, dtype=torch.complex64, device=_device())
+            for t, (ell, m) in enumerate(out_terms):
+                _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rmesh1), *geo, 1, _lib.i32([ell]), _lib.i32([m]),
+                          _lib.ptr(r1))
+                _lib.call('pk_ylm_premultiply', stream, _lib.ptr(r1), *geo, n1, in_ell, in_m, _lib.ptr(R))
+                F = _r2c(R, meshsize)
+                for p, ((_, m1), t2p) in enumerate(pairs):
+                    _lib.call('pk_conj_multiply', stream, _lib.ptr(F[m1 + ell1]), _lib.ptr(B[index2[t2p]]), 1,
+                              B[0].numel(), _lib.ptr(P[p]))
+                Q[t] = _c2r(P, meshsize, destroy_input=True)
+                del F
+            block = np.zeros((nin, len(ells) * nb), dtype='c16')
+            for e, (lo, hi) in enumerate(edgesin.astype('f4')):
+                tophat = ((knorm >= float(lo)) & (knorm <= float(hi))).to(torch.complex64)
+                xi_c = torch.empty((npair,) + cshape, dtype=torch.complex64, device=_device())
+                for p, ((l1, m1), (l2, m2)) in enumerate(pairs):
+                    _lib.call('pk_ylm_kgrid_multiply', stream, _lib.ptr(tophat), _lib.i32(meshsize), kf, 1,
+                              _lib.i32([l1]), _lib.i32([m1]), 1., 0, _lib.ptr(one))
+                    _lib.call('pk_ylm_kgrid_multiply', stream, _lib.ptr(one), _lib.i32(meshsize), kf, 1,
+                              _lib.i32([l2]), _lib.i32([m2]), 1., 0, _lib.ptr(xi_c[p]))
+                xi = _c2r(xi_c, meshsize, destroy_input=True)
+                del xi_c
+                spectrum = []
+                for ill, ell in enumerate(ells):
+                    Aell = torch.zeros(cshape, dtype=torch.complex64, device=_device())
+                    for m in range(-ell, ell + 1):
+                        t = out_terms.index((ell, m))
+                        _lib.call('pk_sum_products', stream, _lib.ptr(tmp), _lib.ptr(xi), _lib.ptr(Q[t]), npair,
+                                  _lib.f32(weight), nreal, 0)
+                        Ft = _r2c(tmp, meshsize)
+                        _lib.call('pk_ylm_kgrid_multiply', stream, _lib.ptr(Ft), _lib.i32(meshsize), kf, 1,
+                                  _lib.i32([ell]), _lib.i32([m]), 1., 1, _lib.ptr(Aell))
+                    spectrum.append(4. * np.pi * bin(Aell, remove_zero=ell == 0) * float(rnorm[ill]))
+                block[e] = np.concatenate(spectrum)
+            del Q, R, P
+            for illin, ellin in enumerate(ellsin):
+                coeff = sum(c * (ell == ellin) for ell, c in coeff2[ell1, ell2])
+                wmat[illin] += coeff * block
+    wmat = wmat.reshape(-1, wmat.shape[-1]).T
+    first = wmat[:nb].imag if ells[0] % 2 else wmat[:nb].real
+    wmat = wmat.real.copy()
+    wmat[:nb] = first
+    return wmat
 
 
 def _firstpoint_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm, batch_size=None):

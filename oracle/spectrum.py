@@ -376,7 +376,8 @@ def compute_mesh2_spectrum_mean_firstpoint(bins, theory, meshes=None, swap=False
     return np.array(out)
 
 
-def compute_mesh2_spectrum_window_firstpoint(bins, edgesin, ellsin, meshes=None, swap=False, norm=None):
+def compute_mesh2_spectrum_window_firstpoint(bins, edgesin, ellsin, meshes=None, swap=False, norm=None,
+                                             theory_los='firstpoint'):
     """``compute_mesh2_spectrum_window(..., los='firstpoint' / 'endpoint')``, input power on the
     mesh, wide-angle order 0 (``mesh2.py:1135-1304``, ``1462-1470``).  ``meshes``: None
     (periodic box) or one / two real selection meshes.  Returns the window matrix
@@ -402,6 +403,44 @@ def compute_mesh2_spectrum_window_firstpoint(bins, edgesin, ellsin, meshes=None,
     xvec = rcoords(geom)
     kvec = kcoords(geom)
     knorm = bins.knorm()
+    if theory_los == 'local':  # mesh2.py:1398-1455
+        rmesh2 = rmesh1 if len(meshes) == 1 else _to_real(geom, meshes[1])
+        coeff2 = {(0, 0): [(0, 1.), (4, -7. / 18.)], (0, 2): [(2, 1. / 2.), (4, -5. / 18.)], (2, 2): [(4, 35. / 18.)]}
+        coeff2[2, 0] = coeff2[0, 2]
+        wmat = np.zeros((len(ellsin), len(edgesin), len(ells) * bins.nbins), dtype='c16')
+        for ell1 in (2, 0):
+            for ell2 in (2, 0):
+                pairs = [(m1, m2) for m1 in range(-ell1, ell1 + 1) for m2 in range(-ell2, ell2 + 1)]
+                w = t((4. * np.pi) ** 2 / ((2 * ell1 + 1) * (2 * ell2 + 1)))
+                Qs = {}
+                for ell in ells:
+                    for m in range(-ell, ell + 1):
+                        for m1, m2 in pairs:
+                            F = r2c(geom, ((rmesh1 * get_ylm(ell, m)(*xvec)).astype(dt) * get_ylm(ell1, m1)(*xvec)).astype(dt))
+                            B = r2c(geom, (rmesh2 * get_ylm(ell2, m2)(*xvec)).astype(dt))
+                            Qs[ell, m, m1, m2] = (w * c2r(geom, (np.conj(F) * B).astype(np.complex64))).astype(dt)
+                block = []
+                for lo, hi in edgesin.astype(dt):
+                    shell = ((knorm >= lo) & (knorm <= hi))
+                    xi = {(m1, m2): c2r(geom, ((shell * get_ylm(ell1, m1)(*kvec)).astype(dt)
+                                               * get_ylm(ell2, m2)(*[-kk for kk in kvec])).astype(np.complex64))
+                          for m1, m2 in pairs}
+                    spectrum = []
+                    for ill, ell in enumerate(ells):
+                        Aell = np.zeros(geom.cshape, dtype=np.complex64)
+                        for m in range(-ell, ell + 1):
+                            tmp = sum(xi[pr] * Qs[(ell, m) + pr] for pr in pairs).astype(dt)
+                            Aell = (Aell + r2c(geom, tmp) * get_ylm(ell, m)(*kvec)).astype(np.complex64)
+                        spectrum.append(4. * np.pi * bins(Aell, remove_zero=ell == 0) * rnorm[ill])
+                    block.append(np.concatenate(spectrum))
+                for illin, ellin in enumerate(ellsin):
+                    wmat[illin] += sum(c * (ell == ellin) for ell, c in coeff2[ell1, ell2]) * np.array(block)
+        wmat = wmat.reshape(-1, wmat.shape[-1]).T
+        nb = bins.nbins
+        first = wmat[:nb].imag if ells[0] % 2 else wmat[:nb].real
+        wmat = wmat.real.copy()
+        wmat[:nb] = first
+        return wmat
     blocks = []
     for ellin in ellsin:
         Qs = {}
