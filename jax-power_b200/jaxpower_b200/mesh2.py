@@ -723,13 +723,14 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     have no effect; ``batch_size`` caps the columns per FFT batch.  The first-point /
     end-point line of sight (theory line of sight 'firstpoint', wide-angle order 0) goes
     through ``_firstpoint_window``, the 'local' theory line of sight (``ellsin=(ells, 'local')``)
-    through ``_local_window``.  The 'smooth' / 'infinite' flags and the 'jaxdecomp' backend
-    raise ``NotImplementedError``.
+    through ``_local_window``.  ``flags=('smooth',)`` with a global line of sight goes through
+    ``_smooth_window``.  The 'infinite' flag, 'smooth' with the first-point line of sight and
+    the 'jaxdecomp' backend raise ``NotImplementedError``.
     """
     from .types import WindowMatrix
     flags = tuple(flags)
-    if 'smooth' in flags or 'infinite' in flags:
-        raise NotImplementedError("the 'smooth' and 'infinite' window flags are not supported on the GPU path")
+    if 'infinite' in flags:
+        raise NotImplementedError("the 'infinite' window flag is not supported on the GPU path")
     meshes, fields = _format_meshes(*meshes)
     periodic = isinstance(meshes[0], MeshAttrs)
     if periodic:
@@ -750,6 +751,13 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     if norm.ndim <= 1:
         norm = norm * np.ones(nells, dtype='f4')
     rnorm = (_norm / norm / N).astype('f4')
+    if 'smooth' in flags:
+        if vlos is None:
+            raise NotImplementedError("the 'smooth' window flag takes a global line of sight on the GPU path")
+        edgesin, ellsin = _window_edges(edgesin, ellsin)
+        Q = None if periodic else _selection_q(meshes, fields, mattrs, N)
+        wmat = _smooth_window(mattrs, bin, Q, vlos, ellsin, edgesin, rnorm)
+        return _window_matrix(bin, norm, edgesin, ellsin, wmat)
     if vlos is None:
         theory_los = 'firstpoint'
         if isinstance(ellsin, (tuple, list)) and len(ellsin) == 2 and isinstance(ellsin[1], str):
@@ -868,6 +876,101 @@ def _window_matrix(bin, norm, edgesin, ellsin, wmat):
     theory = Mesh2SpectrumPoles([Mesh2SpectrumPole(k=kin, k_edges=edgesin, nmodes=np.ones(nin), num_raw=np.zeros(nin),
                                                    ell=ellin) for ellin in ellsin])
     return WindowMatrix(observable=observable, theory=theory, value=wmat)
+
+
+def _selection_q(meshes, fields, mattrs, N):
+    """``Q = c2r(W1 W2*) / N`` (``mesh2.py:1019-1026``), a real device mesh."""
+    A1 = _2c(meshes[0]).value.contiguous()
+    A2 = A1 if fields[1] == fields[0] else _2c(meshes[1]).value.contiguous()
+    prod = torch.empty_like(A1)
+    _lib.call('pk_conj_multiply', _lib.stream_handle(), _lib.ptr(A2), _lib.ptr(A1), 1, A1.numel(), _lib.ptr(prod))
+    Q = _c2r(prod, mattrs.meshsize, destroy_input=True)
+    _lib.call('pk_scale_real', _lib.stream_handle(), _lib.ptr(Q), Q.numel(), float(np.float32(1.) / N))
+    return Q
+
+
+def _bessel_primitive(ell, x, h=0.05):
+    """``F(x) = int_0^x t^2 j_ell(t) dt`` (float64) for x >= 0: 8-point Gauss-Legendre panels
+    of width h summed cumulatively, plus one 8-point panel from the last node to x."""
+    from scipy.special import spherical_jn
+    x = np.asarray(x, dtype='f8')
+    xg, wg = np.polynomial.legendre.leggauss(8)
+    n = int(np.ceil(float(x.max(initial=0.)) / h)) + 1
+    nodes = np.arange(n + 1) * h
+    t = ((nodes[1:] + nodes[:-1]) / 2.)[:, None] + (h / 2.) * xg
+    Fn = np.concatenate([[0.], np.cumsum((h / 2.) * np.sum(wg * t ** 2 * spherical_jn(ell, t), axis=-1))])
+    i = np.minimum((x / h).astype(np.int64), n)
+    a = nodes[i]
+    half = (x - a) / 2.
+    t = ((x + a) / 2.)[..., None] + half[..., None] * xg
+    return Fn[i] + half * np.sum(wg * t ** 2 * spherical_jn(ell, t), axis=-1)
+
+
+def _bessel_shell(ell, lo, hi, s):
+    """``4 pi int_lo^hi k^2 j_ell(k s) dk`` for separations s: ``4 pi (F(hi s) - F(lo s)) / s^3``;
+    at s = 0, ``4 pi (hi^3 - lo^3) / 3`` for ell = 0, else 0 (the tophat integral of
+    ``utils.py:453-462``)."""
+    s = np.asarray(s, dtype='f8')
+    out = np.zeros_like(s)
+    nz = s > 0
+    if nz.any():
+        sz = s[nz]
+        out[nz] = 4. * np.pi * (_bessel_primitive(ell, hi * sz) - _bessel_primitive(ell, lo * sz)) / sz ** 3
+    if ell == 0:
+        out[~nz] = 4. * np.pi * (hi ** 3 - lo ** 3) / 3.
+    return out
+
+
+def _smooth_window(mattrs, bin, Q, vlos, ellsin, edgesin, rnorm):
+    """'smooth' window of the global line of sight (``mesh2.py:1061-1093``): the mesh enters only
+    through the correlation-space multipoles ``Qs = sbin(Q L_ell(mu_s) L_ell_in(mu_s))`` on the
+    separation grid with default (unique |s|) bins, one binning pass per 3 Legendre orders: the
+    product ``L_ell L_ell_in`` is expanded on ``L_p`` and each ``sbin(Q L_p)`` comes from
+    ``pk_bin_separation_global`` (the s = 0 cell, which that pass drops for p > 0, is added back:
+    the reference's bin keeps it).  Each column is then a 1D transform on the host:
+    ``(2 ell + 1) rnorm (-1)^(ell / 2) sum_s n_s j_ell(k s) W_in(s) V Qs`` with
+    ``W_in = (-1)^(ell_in / 2) / (2 pi)^3 4 pi int k^2 j_ell_in(k s) dk`` over the input bin."""
+    from numpy.polynomial import legendre as npleg
+    from scipy.special import spherical_jn
+    sbin = BinMesh2CorrelationPoles(mattrs, edges=None)
+    value = Q if Q is not None else torch.ones(tuple(int(n) for n in mattrs.meshsize), dtype=torch.float32,
+                                               device=_device())
+    q0 = float(value.reshape(-1)[0])
+    ells = bin.ells
+
+    def product(a, b):
+        return npleg.legmul([0.] * a + [1.], [0.] * b + [1.])
+
+    orders = sorted({p for ell in ells for ellin in ellsin for p, c in enumerate(product(ell, ellin)) if c != 0})
+    sums = {}
+    for p0 in range(0, len(orders), 3):
+        chunk = orders[p0:p0 + 3]
+        got = sbin._sums(value, chunk, los=vlos).cpu().numpy()
+        for i, p in enumerate(chunk):
+            sums[p] = got[i].copy()
+            if p > 0:  # the s = 0 cell, mu = 0
+                sums[p][0] += q0 * npleg.legval(0., [0.] * p + [1.])
+    snmodes = sbin.nmodes
+    with np.errstate(invalid='ignore', divide='ignore'):
+        savg = np.where(snmodes == 0, 0., sbin.xavg)
+    kout = np.where(bin.nmodes == 0, 0., bin.xavg)
+    volume = float(np.prod(mattrs.boxsize.astype('f8')))
+    wmat = []
+    for ellin in ellsin:
+        shells = [_bessel_shell(ellin, float(lo), float(hi), savg) * (-1) ** (ellin // 2) / (2. * np.pi) ** 3
+                  for lo, hi in edgesin]
+        blocks = []
+        for ill, ell in enumerate(ells):
+            with np.errstate(invalid='ignore', divide='ignore'):
+                Qs = sum(c * sums[p] for p, c in enumerate(product(ell, ellin)) if c != 0) / snmodes
+            if ell != 0:
+                Qs[0] = 0.
+            Qs = np.where(snmodes == 0, 0., Qs)
+            jk = spherical_jn(ell, kout[:, None] * savg[None, :]) * snmodes[None, :]
+            cols = [(2 * ell + 1) * float(rnorm[ill]) * (-1) ** (ell // 2) * jk.dot(w * volume * Qs) for w in shells]
+            blocks.append(np.array(cols))
+        wmat.append(np.concatenate(blocks, axis=-1))
+    return np.concatenate(wmat, axis=0).T
 
 
 def _local_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm):

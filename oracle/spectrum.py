@@ -469,6 +469,74 @@ def compute_mesh2_spectrum_window_firstpoint(bins, edgesin, ellsin, meshes=None,
     wmat[:nb] = first
     return wmat
 
+
+def compute_mesh2_spectrum_window_smooth(bins, sedges, edgesin, ellsin, los='z', meshes=None, norm=None):
+    """``compute_mesh2_spectrum_window(..., flags=('smooth',))``, global line of sight
+    (``mesh2.py:1061-1093``): ``Qs = sbin(Q L_ell(mu_s) L_ell_in(mu_s))`` on the separation grid
+    (bins ``sedges``; first bin 0 for ell > 0), then per input bin
+    ``(2 ell + 1) rnorm (-1)^(ell/2) sum_s n_s j_ell(k s) W(s) V Qs`` with
+    ``W = (-1)^(ell_in/2) / (2 pi)^3 4 pi int_lo^hi k^2 j_ell_in(k s) dk`` (``utils.py:470-504``,
+    integrated here by adaptive quadrature)."""
+    from scipy.integrate import quad
+    from scipy.special import spherical_jn
+    geom = bins.geom
+    dt = geom.dtype
+    t = dt.type
+    ells = bins.ells
+    N = t(np.prod(geom.meshsize.astype(dt)))
+    _norm = t(N / t(np.prod(geom.cellsize.astype(dt))))
+    norm = np.asarray(_norm if norm is None else norm, dtype=dt)
+    if norm.ndim <= 1:
+        norm = norm * np.ones(len(ells), dtype=dt)
+    rnorm = (_norm / norm / N).astype(dt)
+    vlos = np.zeros(3)
+    if isinstance(los, str):
+        vlos['xyz'.index(los)] = 1.
+    else:
+        vlos = np.asarray(los, dtype='f8')
+    edgesin = np.asarray(edgesin, dtype='f8')
+    if edgesin.ndim != 2:
+        edgesin = np.column_stack([edgesin[:-1], edgesin[1:]])
+    if meshes is None:
+        Q = np.ones(geom.rshape, dtype=dt)
+    else:
+        W = [_to_complex(geom, m) for m in meshes]
+        W2 = W[0] if len(W) == 1 else W[1]
+        Q = (c2r(geom, (W[0] * np.conj(W2)).astype(W[0].dtype)) / N).astype(dt)
+    sbin = CorrelationBins(geom, edges=sedges)
+    svec = separation_coords(geom)
+    snorm = sbin.snorm.astype('f8')
+    smu = sum(xx.astype('f8') * ll for xx, ll in zip(svec, vlos)) / np.where(snorm == 0., 1., snorm)
+    snmodes = sbin.nmodes
+    with np.errstate(invalid='ignore', divide='ignore'):
+        savg = np.where(snmodes == 0, 0., sbin.xavg)
+    kout = np.where(bins.nmodes == 0, 0., bins.xavg)
+    volume = float(np.prod(geom.boxsize.astype('f8')))
+
+    def shell(ell, lo, hi, s):
+        if s == 0.:
+            return 4. * np.pi * (hi ** 3 - lo ** 3) / 3. if ell == 0 else 0.
+        return 4. * np.pi * quad(lambda k: k * k * spherical_jn(ell, k * s), lo, hi, limit=500, epsabs=0.,
+                                 epsrel=1e-9)[0]
+
+    wmat = []
+    for ellin in ellsin:
+        blocks = []
+        for ill, ell in enumerate(ells):
+            Qs = sbin(Q.astype('f8') * legendre(ell, smu) * legendre(ellin, smu))
+            if ell != 0:
+                Qs[0] = 0.
+            Qs = np.where(snmodes == 0, 0., Qs)
+            cols = []
+            for lo, hi in edgesin:
+                w = np.array([shell(ellin, lo, hi, s) for s in savg]) * (-1) ** (ellin // 2) / (2. * np.pi) ** 3
+                tq = w * volume * Qs
+                cols.append((2 * ell + 1) * rnorm[ill] * (-1) ** (ell // 2)
+                            * np.sum(snmodes[None, :] * spherical_jn(ell, kout[:, None] * savg[None, :]) * tq[None, :], axis=-1))
+            blocks.append(np.array(cols))
+        wmat.append(np.concatenate(blocks, axis=-1))
+    return np.concatenate(wmat, axis=0).T
+
 # --------------------------------------------------------------------------- FKP
 
 def next_fft_size(n, primes=(2, 3, 5, 7), divisors=()):

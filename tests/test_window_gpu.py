@@ -264,3 +264,29 @@ def test_local_theory_window_matches_oracle(selection):
                                              los='firstpoint')
         ref = owin_fp(ob, edgesin, (0, 2, 4), meshes=sel, theory_los='local')
     _check(w.value, ref)
+
+
+@pytest.mark.parametrize('selection', [None, 'auto'])
+@pytest.mark.parametrize('los', ['z', [0.6, 0., 0.8]])
+def test_smooth_window_matches_oracle(selection, los):
+    """'smooth' window (global line of sight): correlation-space Legendre products binned on the
+    GPU, Bessel transforms on the host, against the oracle (direct products, adaptive
+    quadrature)."""
+    import jaxpower_b200 as jp
+    from oracle.spectrum import compute_mesh2_spectrum_window_smooth as owin_smooth
+    meshsize, boxsize = (12, 10, 8), np.array([500., 400., 300.])
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.02}, ells=(0, 2, 4))
+    ob = Bins(Geometry(meshsize, boxsize), step=0.02, ells=(0, 2, 4))
+    sedges = jp.BinMesh2CorrelationPoles(attrs)._edges1d
+    rng = np.random.default_rng(19)
+    sel = rng.uniform(0.5, 1.5, meshsize).astype('f4')
+    edgesin = np.arange(0., 0.08, 0.02)
+    if selection is None:
+        w = jp.compute_mesh2_spectrum_window(attrs, edgesin=edgesin, ellsin=(0, 2), bin=b, los=los, flags=('smooth',))
+        ref = owin_smooth(ob, sedges, edgesin, (0, 2), los=los)
+    else:
+        mesh = attrs.create(kind='real', fill=torch.as_tensor(sel))
+        w = jp.compute_mesh2_spectrum_window(mesh, edgesin=edgesin, ellsin=(0, 2), bin=b, los=los, flags=('smooth',))
+        ref = owin_smooth(ob, sedges, edgesin, (0, 2), los=los, meshes=[sel])
+    _check(w.value, ref)
