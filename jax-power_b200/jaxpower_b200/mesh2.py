@@ -724,13 +724,12 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     end-point line of sight (theory line of sight 'firstpoint', wide-angle order 0) goes
     through ``_firstpoint_window``, the 'local' theory line of sight (``ellsin=(ells, 'local')``)
     through ``_local_window``.  ``flags=('smooth',)`` with a global line of sight goes through
-    ``_smooth_window``.  The 'infinite' flag, 'smooth' with the first-point line of sight and
-    the 'jaxdecomp' backend raise ``NotImplementedError``.
+    ``_smooth_window``, ``flags=('infinite',)`` through ``_infinite_window``.  Either flag
+    with the first-point line of sight and the 'jaxdecomp' backend raise
+    ``NotImplementedError``.
     """
     from .types import WindowMatrix
     flags = tuple(flags)
-    if 'infinite' in flags:
-        raise NotImplementedError("the 'infinite' window flag is not supported on the GPU path")
     meshes, fields = _format_meshes(*meshes)
     periodic = isinstance(meshes[0], MeshAttrs)
     if periodic:
@@ -751,6 +750,13 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     if norm.ndim <= 1:
         norm = norm * np.ones(nells, dtype='f4')
     rnorm = (_norm / norm / N).astype('f4')
+    if 'infinite' in flags and 'smooth' not in flags:
+        if vlos is None:
+            raise NotImplementedError("the 'infinite' window flag takes a global line of sight on the GPU path")
+        edgesin, ellsin = _window_edges(edgesin, ellsin)
+        Q = None if periodic else _selection_q(meshes, fields, mattrs, N)
+        wmat = _infinite_window(mattrs, bin, Q, vlos, ellsin, edgesin, rnorm, batch_size)
+        return _window_matrix(bin, norm, edgesin, ellsin, wmat)
     if 'smooth' in flags:
         if vlos is None:
             raise NotImplementedError("the 'smooth' window flag takes a global line of sight on the GPU path")
@@ -971,6 +977,62 @@ def _smooth_window(mattrs, bin, Q, vlos, ellsin, edgesin, rnorm):
             blocks.append(np.array(cols))
         wmat.append(np.concatenate(blocks, axis=-1))
     return np.concatenate(wmat, axis=0).T
+
+
+def _infinite_window(mattrs, bin, Q, vlos, ellsin, edgesin, rnorm, batch_size=None):
+    """'infinite' window of the global line of sight (``mesh2.py:1095-1107``): column
+    (ell_in, [k_lo, k_hi]) is the estimator applied to ``r2c(Q V W_in(|s|) L_ell_in(mu_s))``,
+    ``W_in = (-1)^(ell_in / 2) / (2 pi)^3 4 pi int k^2 j_ell_in(k s) dk`` (the theory correlation
+    function of a tophat power spectrum, no mesh resolution limit).  The radial profile is
+    tabulated on the host on the distinct |s| of the separation grid and gathered onto the
+    mesh with torch; the columns then go through one batched cuFFT R2C and the fused binning
+    pass linear in the mesh (``pk_bin_window_batch``, k = 0 dropped)."""
+    stream = _lib.stream_handle()
+    meshsize = mattrs.meshsize
+    sx, sy, sz = mattrs.rcoords(kind='separation', sparse=True)
+    s2 = (sx * sx + sy * sy) + sz * sz
+    snorm = torch.sqrt(s2)
+    smu = (sx * float(vlos[0]) + sy * float(vlos[1]) + sz * float(vlos[2])) / \
+        torch.where(snorm == 0., torch.ones_like(snorm), snorm)
+    uniq, inverse = torch.unique(snorm.reshape(-1), return_inverse=True)
+    uniq_h = uniq.cpu().numpy().astype('f8')
+    volume = float(np.prod(mattrs.boxsize.astype('f8')))
+    ells = bin.ells
+    even = [ill for ill, ell in enumerate(ells) if ell % 2 == 0]
+    nin, nb = len(edgesin), bin.nbins
+    rshape = tuple(int(n) for n in meshsize)
+    B = _window_batch(mattrs, batch_size)
+    sums = np.zeros((len(ellsin), nin, len(ells), nb))
+    if even:
+        nbytes = _lib.c_size_t()
+        _lib.call('pk_bin_batch_workspace_size', _lib.i32(meshsize), len(bin._edges1d), len(even), B,
+                  _lib.ctypes.byref(nbytes))
+        ws = _workspace(nbytes.value)
+        raw = torch.empty((B, len(even), nb), dtype=torch.float64, device=_device())
+    for iin, ellin in enumerate(ellsin):
+        legin = _legendre(ellin, smu).reshape(-1) * volume
+        if Q is not None:
+            legin = legin * Q.reshape(-1)
+        for e0 in range(0, nin if even else 0, B):
+            n = min(B, nin - e0)
+            cols = torch.empty((n,) + rshape, dtype=torch.float32, device=_device())
+            for c in range(n):
+                lo, hi = edgesin[e0 + c]
+                prof = _bessel_shell(ellin, float(np.float32(lo)), float(np.float32(hi)), uniq_h)
+                prof = prof * (-1) ** (ellin // 2) / (2. * np.pi) ** 3
+                table = torch.as_tensor(prof.astype('f4'), device=_device())
+                cols[c].view(-1).copy_(table[inverse] * legin)
+            A = _r2c(cols, meshsize)
+            del cols
+            _lib.call('pk_bin_window_batch', stream, _lib.ptr(A), n, _lib.i32(meshsize), _lib.f32(mattrs.kfun),
+                      _lib.f32(vlos), _lib.ptr(bin.d_edges), len(bin._edges1d), bin._step, mattrs.backend_code,
+                      len(even), _lib.i32([ells[ill] for ill in even]), 1, _lib.ptr(raw), _lib.ptr(ws), ws.numel())
+            sums[iin, e0:e0 + n][:, even] = raw[:n].cpu().numpy()
+            del A
+    with np.errstate(invalid='ignore', divide='ignore'):
+        factor = np.array([(2 * ell + 1) / (1 + ell % 2) * float(rnorm[ill]) for ill, ell in enumerate(ells)])
+        spectra = sums / bin.nmodes * factor[:, None]
+    return np.concatenate([spectra[iin].reshape(nin, -1) for iin in range(len(ellsin))], axis=0).T
 
 
 def _local_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm):

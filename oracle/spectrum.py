@@ -537,6 +537,75 @@ def compute_mesh2_spectrum_window_smooth(bins, sedges, edgesin, ellsin, los='z',
         wmat.append(np.concatenate(blocks, axis=-1))
     return np.concatenate(wmat, axis=0).T
 
+
+def compute_mesh2_spectrum_window_infinite(bins, edgesin, ellsin, los='z', meshes=None, norm=None):
+    """``compute_mesh2_spectrum_window(..., flags=('infinite',))``, global line of sight
+    (``mesh2.py:1095-1107``): column (ell_in, edge) is the estimator applied to
+    ``r2c(Q V W(|s|) L_ell_in(mu_s))``, ``W = (-1)^(ell_in/2) / (2 pi)^3 4 pi int k^2 j_ell_in(k s) dk``
+    (adaptive quadrature here)."""
+    from scipy.integrate import quad
+    from scipy.special import spherical_jn
+    geom = bins.geom
+    dt = geom.dtype
+    t = dt.type
+    ells = bins.ells
+    N = t(np.prod(geom.meshsize.astype(dt)))
+    _norm = t(N / t(np.prod(geom.cellsize.astype(dt))))
+    norm = np.asarray(_norm if norm is None else norm, dtype=dt)
+    if norm.ndim <= 1:
+        norm = norm * np.ones(len(ells), dtype=dt)
+    rnorm = (_norm / norm / N).astype(dt)
+    vlos = np.zeros(3)
+    if isinstance(los, str):
+        vlos['xyz'.index(los)] = 1.
+    else:
+        vlos = np.asarray(los, dtype='f8')
+    edgesin = np.asarray(edgesin, dtype='f8')
+    if edgesin.ndim != 2:
+        edgesin = np.column_stack([edgesin[:-1], edgesin[1:]])
+    Q = None
+    if meshes is not None:
+        W = [_to_complex(geom, m) for m in meshes]
+        W2 = W[0] if len(W) == 1 else W[1]
+        Q = (c2r(geom, (W[0] * np.conj(W2)).astype(W[0].dtype)) / N).astype(dt)
+    svec = separation_coords(geom)
+    s2 = (((t(0.) + svec[0] * svec[0]).astype(dt) + svec[1] * svec[1]).astype(dt) + svec[2] * svec[2]).astype(dt)
+    snorm = np.sqrt(s2).astype('f8')
+    smu = sum(xx.astype('f8') * ll for xx, ll in zip(svec, vlos)) / np.where(snorm == 0., 1., snorm)
+    uniq, inverse = np.unique(snorm.ravel(), return_inverse=True)
+    kvec = kcoords(geom)
+    kl = [(kk * t(ll)).astype(dt) for kk, ll in zip(kvec, vlos)]
+    num = (((t(0.) + kl[0]).astype(dt) + kl[1]).astype(dt) + kl[2]).astype(dt)
+    knorm = bins.knorm()
+    mu = (num / np.where(knorm == 0., t(1.), knorm)).astype(dt)
+    volume = float(np.prod(geom.boxsize.astype('f8')))
+
+    def shell(ell, lo, hi, s):
+        if s == 0.:
+            return 4. * np.pi * (hi ** 3 - lo ** 3) / 3. if ell == 0 else 0.
+        return 4. * np.pi * quad(lambda k: k * k * spherical_jn(ell, k * s), lo, hi, limit=500, epsabs=0.,
+                                 epsrel=1e-9)[0]
+
+    wmat = []
+    for ellin in ellsin:
+        rows = []
+        for lo, hi in edgesin.astype(dt):
+            prof = np.array([shell(ellin, float(lo), float(hi), s) for s in uniq]) * (-1) ** (ellin // 2) / (2. * np.pi) ** 3
+            A = (prof[inverse].reshape(snorm.shape) * legendre(ellin, smu) * volume)
+            if Q is not None:
+                A = A * Q
+            A = r2c(geom, A.astype(dt))
+            spectrum = []
+            for ill, ell in enumerate(ells):
+                odd = ell % 2
+                leg = legendre(ell, mu)
+                if odd:
+                    leg = (leg + legendre(ell, (-mu).astype(dt))).astype(dt)
+                spectrum.append((2 * ell + 1) / (1 + odd) * bins((A * leg).astype(A.dtype), remove_zero=True) * rnorm[ill])
+            rows.append(np.concatenate(spectrum))
+        wmat.append(np.array(rows))
+    return np.real(np.concatenate(wmat, axis=0).T)
+
 # --------------------------------------------------------------------------- FKP
 
 def next_fft_size(n, primes=(2, 3, 5, 7), divisors=()):

@@ -290,3 +290,28 @@ def test_smooth_window_matches_oracle(selection, los):
         w = jp.compute_mesh2_spectrum_window(mesh, edgesin=edgesin, ellsin=(0, 2), bin=b, los=los, flags=('smooth',))
         ref = owin_smooth(ob, sedges, edgesin, (0, 2), los=los, meshes=[sel])
     _check(w.value, ref)
+
+
+@pytest.mark.parametrize('selection', [None, 'auto'])
+def test_infinite_window_matches_oracle(selection):
+    """'infinite' window (global line of sight): tophat theory correlation function on the
+    separation grid, batched R2C and the fused linear binning pass, against the oracle."""
+    import jaxpower_b200 as jp
+    from oracle.spectrum import compute_mesh2_spectrum_window_infinite as owin_inf
+    meshsize, boxsize = (12, 10, 8), np.array([500., 400., 300.])
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.02}, ells=(0, 1, 2))
+    ob = Bins(Geometry(meshsize, boxsize), step=0.02, ells=(0, 1, 2))
+    rng = np.random.default_rng(23)
+    sel = rng.uniform(0.5, 1.5, meshsize).astype('f4')
+    edgesin = np.arange(0.01, 0.08, 0.02)
+    if selection is None:
+        w = jp.compute_mesh2_spectrum_window(attrs, edgesin=edgesin, ellsin=(0, 2), bin=b, los='y',
+                                             flags=('infinite',), batch_size=2)
+        ref = owin_inf(ob, edgesin, (0, 2), los='y')
+    else:
+        mesh = attrs.create(kind='real', fill=torch.as_tensor(sel))
+        w = jp.compute_mesh2_spectrum_window(mesh, edgesin=edgesin, ellsin=(0, 2), bin=b, los='y',
+                                             flags=('infinite',), batch_size=2)
+        ref = owin_inf(ob, edgesin, (0, 2), los='y', meshes=[sel])
+    _check(w.value, ref)
