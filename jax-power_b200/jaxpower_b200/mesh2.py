@@ -724,9 +724,9 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     end-point line of sight (theory line of sight 'firstpoint', wide-angle order 0) goes
     through ``_firstpoint_window``, the 'local' theory line of sight (``ellsin=(ells, 'local')``)
     through ``_local_window``.  ``flags=('smooth',)`` with a global line of sight goes through
-    ``_smooth_window``, ``flags=('infinite',)`` through ``_infinite_window``.  Either flag
-    with the first-point line of sight and the 'jaxdecomp' backend raise
-    ``NotImplementedError``.
+    ``_smooth_window`` (first point: ``_firstpoint_smooth_window``), ``flags=('infinite',)``
+    with a global line of sight through ``_infinite_window``.  The first-point 'infinite'
+    window and the 'jaxdecomp' backend raise ``NotImplementedError``.
     """
     from .types import WindowMatrix
     flags = tuple(flags)
@@ -757,9 +757,22 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
         Q = None if periodic else _selection_q(meshes, fields, mattrs, N)
         wmat = _infinite_window(mattrs, bin, Q, vlos, ellsin, edgesin, rnorm, batch_size)
         return _window_matrix(bin, norm, edgesin, ellsin, wmat)
+    if 'smooth' in flags and vlos is None:
+        if isinstance(ellsin, (tuple, list)) and len(ellsin) == 2 and isinstance(ellsin[1], str):
+            ellsin, theory_los = ellsin
+            if theory_los != 'firstpoint':
+                raise NotImplementedError("the 'smooth' window takes the 'firstpoint' theory line of sight")
+        if ellsin is not None and np.ndim(ellsin) == 0:
+            ellsin = (ellsin,)
+        if ellsin is not None:
+            ellsin = [e if isinstance(e, tuple) else (int(e), 0) for e in ellsin]
+            if any(wa != 0 for _, wa in ellsin):
+                raise NotImplementedError('wide-angle orders > 0 are not supported')
+            ellsin = [e for e, _ in ellsin]
+        edgesin, ellsin = _window_edges(edgesin, ellsin)
+        wmat = _firstpoint_smooth_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm)
+        return _window_matrix(bin, norm, edgesin, ellsin, wmat)
     if 'smooth' in flags:
-        if vlos is None:
-            raise NotImplementedError("the 'smooth' window flag takes a global line of sight on the GPU path")
         edgesin, ellsin = _window_edges(edgesin, ellsin)
         Q = None if periodic else _selection_q(meshes, fields, mattrs, N)
         wmat = _smooth_window(mattrs, bin, Q, vlos, ellsin, edgesin, rnorm)
@@ -977,6 +990,77 @@ def _smooth_window(mattrs, bin, Q, vlos, ellsin, edgesin, rnorm):
             blocks.append(np.array(cols))
         wmat.append(np.concatenate(blocks, axis=-1))
     return np.concatenate(wmat, axis=0).T
+
+
+def _firstpoint_smooth_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm):
+    """'smooth' window of the first-point line of sight, wide-angle order 0
+    (``mesh2.py:1196-1238``): for each ell_in and output ell,
+    ``Qs = 4 pi V_cell sbin(sum_{m, m1} Q_{ell m m1} Y_lm(shat) Y_{ell_in m1}(shat))`` with
+    ``Q_{ell m m1} = 4 pi / (2 ell_in + 1) c2r(conj(r2c(W1 Y_lm Y_{ell_in m1})) A0)`` (first bin 0
+    for ell > 0), then ``rnorm (-1)^(ell/2) sum_s n_s j_ell(k s) W_in(s) Qs`` per input bin (no
+    2 ell + 1 factor on this path).  The Y_lm(shat) weights go through
+    ``pk_ylm_separation_accumulate`` (twice: the m1 sum, then the Y_lm factor)."""
+    from scipy.special import spherical_jn
+    meshsize = mattrs.meshsize
+    stream = _lib.stream_handle()
+    if swap:
+        meshes = meshes[::-1]
+    if periodic:
+        rmesh1 = torch.ones(tuple(int(n) for n in meshsize), dtype=torch.float32, device=_device())
+        A0 = _r2c(rmesh1, meshsize)
+    else:
+        rmesh1 = _2r(meshes[0]).value.contiguous()
+        A0 = _2c(meshes[0] if fields[1] == fields[0] else meshes[1]).value.contiguous()
+    offset = (mattrs.boxcenter - (mattrs.boxsize / np.float32(2.)).astype('f4')).astype('f4')
+    geo = (_lib.i32(meshsize), _lib.f32(mattrs.cellsize), _lib.f32(offset))
+    rshape = tuple(int(n) for n in meshsize)
+    sbin = BinMesh2CorrelationPoles(mattrs, edges=None)
+    snmodes = sbin.nmodes
+    with np.errstate(invalid='ignore', divide='ignore'):
+        savg = np.where(snmodes == 0, 0., sbin.xavg)
+    kout = np.where(bin.nmodes == 0, 0., bin.xavg)
+    cellvol = float(np.prod(mattrs.cellsize.astype('f8')))
+    ells = bin.ells
+    nb = bin.nbins
+    r1 = torch.empty((1,) + rshape, dtype=torch.float32, device=_device())
+    blocks = []
+    for ellin in ellsin:
+        n1 = 2 * ellin + 1
+        in_ell, in_m = _lib.i32([ellin] * n1), _lib.i32(list(range(-ellin, ellin + 1)))
+        R = torch.empty((n1,) + rshape, dtype=torch.float32, device=_device())
+        block = np.zeros((len(edgesin), len(ells) * nb))
+        shells = [_bessel_shell(ellin, float(lo), float(hi), savg) * (-1) ** (ellin // 2) / (2. * np.pi) ** 3
+                  for lo, hi in edgesin.astype('f4')]
+        for ill, ell in enumerate(ells):
+            carry2 = torch.zeros(rshape, dtype=torch.float32, device=_device())
+            for m in range(-ell, ell + 1):
+                _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rmesh1), *geo, 1, _lib.i32([ell]), _lib.i32([m]),
+                          _lib.ptr(r1))
+                _lib.call('pk_ylm_premultiply', stream, _lib.ptr(r1), *geo, n1, in_ell, in_m, _lib.ptr(R))
+                F = _r2c(R, meshsize)
+                _lib.call('pk_conj_multiply', stream, _lib.ptr(F), _lib.ptr(A0), n1, A0.numel(), _lib.ptr(F))
+                G = _c2r(F, meshsize, destroy_input=True)
+                del F
+                _lib.call('pk_scale_real', stream, _lib.ptr(G), G.numel(), float(4. * np.pi / (2 * ellin + 1)))
+                carry1 = torch.zeros(rshape, dtype=torch.float32, device=_device())
+                _lib.call('pk_ylm_separation_accumulate', stream, _lib.ptr(G), _lib.i32(meshsize),
+                          _lib.f32(mattrs.cellsize), n1, in_ell, in_m, _lib.ptr(carry1))
+                _lib.call('pk_ylm_separation_accumulate', stream, _lib.ptr(carry1), _lib.i32(meshsize),
+                          _lib.f32(mattrs.cellsize), 1, _lib.i32([ell]), _lib.i32([m]), _lib.ptr(carry2))
+                del G, carry1
+            Qs = 4. * np.pi * sbin(carry2) * cellvol
+            if ell != 0:
+                Qs[0] = 0.
+            Qs = np.where(snmodes == 0, 0., Qs)
+            jk = spherical_jn(ell, kout[:, None] * savg[None, :]) * snmodes[None, :]
+            for e, w in enumerate(shells):
+                block[e, ill * nb:(ill + 1) * nb] = (-1) ** (ell // 2) * jk.dot(w * Qs) * float(rnorm[ill])
+        blocks.append(block)
+        del R
+    wmat = np.concatenate(blocks, axis=0).T
+    if ells[0] % 2:  # the reference keeps the imaginary part of the first multipole's rows: 0 here
+        wmat[:nb] = 0.
+    return wmat
 
 
 def _infinite_window(mattrs, bin, Q, vlos, ellsin, edgesin, rnorm, batch_size=None):

@@ -606,6 +606,68 @@ def compute_mesh2_spectrum_window_infinite(bins, edgesin, ellsin, los='z', meshe
         wmat.append(np.array(rows))
     return np.real(np.concatenate(wmat, axis=0).T)
 
+
+def compute_mesh2_spectrum_window_firstpoint_smooth(bins, sedges, edgesin, ellsin, meshes=None, swap=False):
+    """``compute_mesh2_spectrum_window(..., los='firstpoint', flags=('smooth',))``, wide-angle
+    order 0 (``mesh2.py:1196-1238``): ``Qs = 4 pi V_cell sum_{m, m1} sbin(Q Y_lm(shat) Y_l1m1(shat))``,
+    ``Q = 4 pi / (2 ell_in + 1) c2r(conj(r2c(W1 Y_lm(xhat) Y_l1m1(xhat))) A0)``, then
+    ``rnorm (-1)^(ell/2) sum_s n_s j_ell(k s) W(s) Qs`` (adaptive quadrature for W)."""
+    from scipy.integrate import quad
+    from scipy.special import spherical_jn
+    geom = bins.geom
+    dt = geom.dtype
+    t = dt.type
+    ells = bins.ells
+    N = t(np.prod(geom.meshsize.astype(dt)))
+    rnorm = np.full(len(ells), t(1.) / N, dtype=dt)
+    edgesin = np.asarray(edgesin, dtype='f8')
+    if edgesin.ndim != 2:
+        edgesin = np.column_stack([edgesin[:-1], edgesin[1:]])
+    meshes = [np.ones(geom.rshape, dtype=dt)] if meshes is None else list(meshes)
+    if swap:
+        meshes = meshes[::-1]
+    rmesh1 = _to_real(geom, meshes[0])
+    A0 = _to_complex(geom, meshes[0] if len(meshes) == 1 else meshes[1])
+    xvec = rcoords(geom)
+    svec = separation_coords(geom)
+    sbin = CorrelationBins(geom, edges=sedges)
+    snmodes = sbin.nmodes
+    with np.errstate(invalid='ignore', divide='ignore'):
+        savg = np.where(snmodes == 0, 0., sbin.xavg)
+    kout = np.where(bins.nmodes == 0, 0., bins.xavg)
+    cellvol = float(np.prod(geom.cellsize.astype('f8')))
+
+    def shell(ell, lo, hi, s):
+        if s == 0.:
+            return 4. * np.pi * (hi ** 3 - lo ** 3) / 3. if ell == 0 else 0.
+        return 4. * np.pi * quad(lambda k: k * k * spherical_jn(ell, k * s), lo, hi, limit=500, epsabs=0.,
+                                 epsrel=1e-9)[0]
+
+    blocks = []
+    for ellin in ellsin:
+        block = np.zeros((len(edgesin), len(ells) * bins.nbins))
+        for ill, ell in enumerate(ells):
+            Qs = 0.
+            for m1 in range(-ellin, ellin + 1):
+                Y1 = get_ylm(ellin, m1)
+                for m in range(-ell, ell + 1):
+                    Y = get_ylm(ell, m)
+                    F = r2c(geom, ((rmesh1 * Y(*xvec)).astype(dt) * Y1(*xvec)).astype(dt))
+                    Q = (t(4. * np.pi / (2 * ellin + 1)) * c2r(geom, (np.conj(F) * A0).astype(np.complex64))).astype(dt)
+                    Qs = Qs + 4. * np.pi * sbin(Q.astype('f8') * Y(*svec) * Y1(*svec)) * cellvol
+            if ell != 0:
+                Qs[0] = 0.
+            Qs = np.where(snmodes == 0, 0., Qs)
+            for e, (lo, hi) in enumerate(edgesin.astype(dt)):
+                w = np.array([shell(ellin, float(lo), float(hi), s) for s in savg]) * (-1) ** (ellin // 2) / (2. * np.pi) ** 3
+                block[e, ill * bins.nbins:(ill + 1) * bins.nbins] = (-1) ** (ell // 2) * np.sum(
+                    snmodes[None, :] * spherical_jn(ell, kout[:, None] * savg[None, :]) * (w * Qs)[None, :], axis=-1) * rnorm[ill]
+        blocks.append(block)
+    wmat = np.concatenate(blocks, axis=0).T
+    if ells[0] % 2:
+        wmat[:bins.nbins] = 0.
+    return wmat
+
 # --------------------------------------------------------------------------- FKP
 
 def next_fft_size(n, primes=(2, 3, 5, 7), divisors=()):

@@ -315,3 +315,29 @@ def test_infinite_window_matches_oracle(selection):
                                              flags=('infinite',), batch_size=2)
         ref = owin_inf(ob, edgesin, (0, 2), los='y', meshes=[sel])
     _check(w.value, ref)
+
+
+@pytest.mark.parametrize('selection', [None, 'cross'])
+@pytest.mark.parametrize('los', ['firstpoint', 'endpoint'])
+def test_firstpoint_smooth_window_matches_oracle(selection, los):
+    """'smooth' window with the first-point / end-point line of sight against the oracle."""
+    import jaxpower_b200 as jp
+    from oracle.spectrum import compute_mesh2_spectrum_window_firstpoint_smooth as owin
+    meshsize, boxsize, center = (10, 8, 8), np.array([500., 400., 400.]), (900., -200., 300.)
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=center)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.02}, ells=(0, 2))
+    ob = Bins(Geometry(meshsize, boxsize, center), step=0.02, ells=(0, 2))
+    sedges = jp.BinMesh2CorrelationPoles(attrs)._edges1d
+    rng = np.random.default_rng(29)
+    sel = [rng.uniform(0.5, 1.5, meshsize).astype('f4') for _ in range(2)]
+    edgesin = np.arange(0.005, 0.06, 0.02)
+    if selection is None:
+        w = jp.compute_mesh2_spectrum_window(attrs, edgesin=edgesin, ellsin=((0, 2), 'firstpoint'), bin=b, los=los,
+                                             flags=('smooth',))
+        ref = owin(ob, sedges, edgesin, (0, 2), swap=los == 'endpoint')
+    else:
+        meshes = [attrs.create(kind='real', fill=torch.as_tensor(s)) for s in sel]
+        w = jp.compute_mesh2_spectrum_window(*meshes, edgesin=edgesin, ellsin=(0, 2), bin=b, los=los,
+                                             flags=('smooth',))
+        ref = owin(ob, sedges, edgesin, (0, 2), meshes=sel, swap=los == 'endpoint')
+    _check(w.value, ref)
