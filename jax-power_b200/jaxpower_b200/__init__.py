@@ -16,7 +16,7 @@ from .mesh2 import (BinMesh2SpectrumPoles, BinMesh2CorrelationPoles, compute_mes
                     compute_mesh2_correlation, compute_mesh2, compute_fkp2_normalization,
                     compute_fkp2_shotnoise, compute_box2_normalization, compute_normalization,
                     compute_box_normalization, compute_mesh2_spectrum_window,
-                    compute_mesh2_spectrum_mean)
+                    compute_mesh2_spectrum_mean, compute_smooth2_spectrum_window)
 from .types import (Mesh2SpectrumPole, Mesh2SpectrumPoles, Mesh2CorrelationPole, Mesh2CorrelationPoles, WindowMatrix,
                     read, write)
 from ._lib import load as load_library, LIBRARY_PATH

@@ -24,7 +24,8 @@ from .types import Mesh2SpectrumPole, Mesh2SpectrumPoles, Mesh2CorrelationPole, 
 
 __all__ = ['BinMesh2SpectrumPoles', 'compute_mesh2_spectrum', 'compute_mesh2', 'compute_fkp2_normalization',
            'compute_fkp2_shotnoise', 'compute_box2_normalization', 'compute_normalization',
-           'compute_box_normalization', 'compute_mesh2_spectrum_window', 'compute_mesh2_spectrum_mean']
+           'compute_box_normalization', 'compute_mesh2_spectrum_window', 'compute_mesh2_spectrum_mean',
+           'compute_smooth2_spectrum_window']
 
 
 def _format_ells(ells):
@@ -1615,3 +1616,75 @@ def compute_mesh2_spectrum_mean(*meshes, theory, bin=None, los='z'):
                                                  norm=np.ones(bin.nbins) * norm, volume=volume, ell=ell,
                                                  attrs=dict(los=np.asarray(vlos).tolist()))
                                for ill, ell in enumerate(ells)])
+
+
+def _window_coeffs(ell, ellin):
+    """``get_window_coeffs`` (``mesh2.py:759-765``): (q, (2 ell + 1) (ell ellin q; 0 0 0)^2) with the
+    Wigner 3j squares read off the Legendre expansion ``L_ell L_ellin = sum_q (2 q + 1) (3j)^2 L_q``."""
+    from numpy.polynomial import legendre as npleg
+    c = npleg.legmul([0.] * ell + [1.], [0.] * ellin + [1.])
+    out = []
+    for q in range(abs(ell - ellin), ell + ellin + 1):
+        coeff = (2 * ell + 1) * (c[q] / (2 * q + 1) if q < len(c) else 0.)
+        if abs(coeff) >= 1e-7:
+            out.append((q, coeff))
+    return out
+
+
+def compute_smooth2_spectrum_window(window, edgesin, ellsin=None, bin=None, flags=('rect',), batch_size=None):
+    """'Smooth' (no binning effect) window matrix from configuration-space window multipoles
+    (``mesh2.py:803-918``), 'rect' integration.
+
+    ``window``: a ``Mesh2CorrelationPoles`` (e.g. from ``compute_mesh2_correlation`` of the
+    selection function).  For each input ell_in and output ell, ``Qs = sum_q c_q W_q(s)``
+    (``_window_coeffs``), then per input bin (mid-point k_in) and output k
+    ``(-1)^(ell/2) sum_s j_ell(k s) n_s (-1)^(ell_in/2) / (2 pi)^3 j_ell_in(k_in s) V_in Qs(s)``,
+    ``n_s`` the window's ``volume`` (ones if absent), ``V_in = 4 pi / 3 (k_hi^3 - k_lo^3)``.  These
+    are 1D host sums over the window's separations (no mesh work).  The 'fftlog' integration
+    (any flag set without 'rect') and wide-angle orders > 0 raise ``NotImplementedError``.
+    """
+    from scipy.special import spherical_jn
+    if 'rect' not in flags:
+        raise NotImplementedError("only the 'rect' integration of the smooth window is supported")
+    ells = bin.ells
+    if hasattr(edgesin, 'ells') and hasattr(edgesin, 'poles'):
+        ellsin = edgesin.ells
+        edgesin = next(iter(edgesin)).k_edges
+    edgesin = np.asarray(edgesin, dtype='f8')
+    if edgesin.ndim != 2:
+        edgesin = np.column_stack([edgesin[:-1], edgesin[1:]])
+    ellsin = [e if isinstance(e, tuple) else (int(e), 0) for e in ((ellsin,) if np.ndim(ellsin) == 0 else ellsin)]
+    if any(wa != 0 for _, wa in ellsin):
+        raise ValueError('wa_orders must be provided in input window')
+    kout = np.asarray(bin.xavg, dtype='f8')
+    first = next(iter(window))
+    s = np.asarray(first.coords('s'), dtype='f8')
+    snmodes = np.ones_like(s) if first.volume is None else np.asarray(first.volume, dtype='f8')
+    savg = np.where(snmodes == 0, 0., s)
+    kin = np.mean(edgesin, axis=-1)
+    vin = 4. / 3. * np.pi * (edgesin[:, 1] ** 3 - edgesin[:, 0] ** 3)
+
+    def get_w(q):
+        if q in window.ells:
+            return np.real(np.asarray(window.get(q).value(), dtype='c16'))
+        return 0.
+
+    blocks = []
+    for ellin, _ in ellsin:
+        col = []
+        for ell in ells:
+            Qs = sum(coeff * get_w(q) for q, coeff in _window_coeffs(ell, ellin))
+            Qs = np.where(snmodes == 0, 0., Qs)
+            tophat = ((-1) ** (ellin // 2) / (2. * np.pi) ** 3 * spherical_jn(ellin, savg[None, :] * kin[:, None])
+                      * vin[:, None] * Qs)  # (nin, ns)
+            jk = (-1) ** (ell // 2) * spherical_jn(ell, kout[:, None] * savg[None, :])  # (nbins, ns)
+            col.append(jk.dot((snmodes * tophat).T))  # (nbins, nin)
+        blocks.append(np.concatenate(col, axis=0))
+    wmat = np.concatenate(blocks, axis=1)
+    observable = Mesh2SpectrumPoles([Mesh2SpectrumPole(k=bin.xavg, k_edges=bin.edges, nmodes=bin.nmodes,
+                                                       num_raw=np.zeros(len(kout)), num_shotnoise=np.zeros(len(kout)),
+                                                       norm=np.ones(len(kout)), ell=ell) for ell in ells])
+    theory = Mesh2SpectrumPoles([Mesh2SpectrumPole(k=kin, k_edges=edgesin, nmodes=np.ones(len(kin)),
+                                                   num_raw=np.zeros(len(kin)), ell=ellin) for ellin, _ in ellsin])
+    from .types import WindowMatrix
+    return WindowMatrix(observable=observable, theory=theory, value=wmat)

@@ -668,6 +668,34 @@ def compute_mesh2_spectrum_window_firstpoint_smooth(bins, sedges, edgesin, ellsi
         wmat[:bins.nbins] = 0.
     return wmat
 
+
+def compute_smooth2_spectrum_window(s, windows, snmodes, edgesin, ellsin, ells, kout):
+    """``compute_smooth2_spectrum_window(window, edgesin, ellsin, bin, flags=('rect',))``
+    (``mesh2.py:803-918``) as plain loops: ``windows`` {q: W_q(s)}, coefficients
+    ``(2 ell + 1) (ell ellin q; 0 0 0)^2`` from sympy's Wigner 3j symbols."""
+    from scipy.special import spherical_jn
+    from sympy.physics.wigner import wigner_3j
+    edgesin = np.asarray(edgesin, dtype='f8')
+    if edgesin.ndim != 2:
+        edgesin = np.column_stack([edgesin[:-1], edgesin[1:]])
+    savg = np.where(snmodes == 0, 0., s)
+    wmat = np.zeros((len(ells) * len(kout), len(ellsin) * len(edgesin)))
+    for iin, ellin in enumerate(ellsin):
+        for ill, ell in enumerate(ells):
+            Qs = np.zeros_like(s)
+            for q in range(abs(ell - ellin), ell + ellin + 1):
+                c = (2 * ell + 1) * float(wigner_3j(ell, ellin, q, 0, 0, 0)) ** 2
+                if abs(c) >= 1e-7 and q in windows:
+                    Qs = Qs + c * windows[q]
+            Qs = np.where(snmodes == 0, 0., Qs)
+            for e, (lo, hi) in enumerate(edgesin):
+                kin = (lo + hi) / 2.
+                tophat = (-1) ** (ellin // 2) / (2. * np.pi) ** 3 * spherical_jn(ellin, savg * kin) * 4. / 3. * np.pi * (hi ** 3 - lo ** 3) * Qs
+                for b, k in enumerate(kout):
+                    wmat[ill * len(kout) + b, iin * len(edgesin) + e] = (-1) ** (ell // 2) * np.sum(
+                        spherical_jn(ell, k * savg) * snmodes * tophat)
+    return wmat
+
 # --------------------------------------------------------------------------- FKP
 
 def next_fft_size(n, primes=(2, 3, 5, 7), divisors=()):

@@ -48,3 +48,28 @@ def test_window_theory_vector_of_a_constant_power():
     expect[0] = (bins.nmodes[0] - 1.) / bins.nmodes[0]
     assert np.allclose(got[:nb], expect, rtol=1e-6)
     assert np.allclose(got[nb:], 0., atol=1e-6)  # isotropic input: no quadrupole
+
+
+def test_smooth2_window_from_correlation_multipoles():
+    """compute_smooth2_spectrum_window ('rect'): host sums over the window's separations, against
+    plain loops with sympy's Wigner 3j coefficients (no GPU: the output binning is given by its
+    attributes)."""
+    from types import SimpleNamespace
+    import jaxpower_b200 as jp
+    from oracle.spectrum import compute_smooth2_spectrum_window as osmooth2
+    rng = np.random.default_rng(3)
+    s = np.linspace(2.5, 200., 80)
+    nmodes = rng.integers(0, 50, s.size).astype('f8')
+    windows = {0: np.exp(-s / 80.), 2: 0.3 * np.exp(-s / 60.), 4: 0.1 * np.exp(-s / 40.)}
+    poles = jp.Mesh2CorrelationPoles([jp.Mesh2CorrelationPole(s=s, s_edges=np.column_stack([s - 1.25, s + 1.25]),
+                                                               nmodes=nmodes, num_raw=windows[q], volume=nmodes, ell=q)
+                                      for q in (0, 2, 4)])
+    kedges = np.arange(0.01, 0.2, 0.02)
+    bin = SimpleNamespace(ells=(0, 2, 4), xavg=(kedges[:-1] + kedges[1:]) / 2.,
+                          edges=np.column_stack([kedges[:-1], kedges[1:]]), nmodes=np.ones(kedges.size - 1))
+    edgesin = np.arange(0., 0.25, 0.025)
+    w = jp.compute_smooth2_spectrum_window(poles, edgesin=edgesin, ellsin=(0, 2, 4), bin=bin)
+    ref = osmooth2(s, windows, nmodes, edgesin, (0, 2, 4), (0, 2, 4), bin.xavg)
+    assert w.value.shape == ref.shape == (3 * bin.xavg.size, 3 * (edgesin.size - 1))
+    assert np.allclose(w.value, ref, rtol=1e-10, atol=1e-12 * np.abs(ref).max())
+    assert w.theory.ells == (0, 2, 4)
