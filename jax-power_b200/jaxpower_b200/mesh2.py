@@ -726,8 +726,9 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     through ``_firstpoint_window``, the 'local' theory line of sight (``ellsin=(ells, 'local')``)
     through ``_local_window``.  ``flags=('smooth',)`` with a global line of sight goes through
     ``_smooth_window`` (first point: ``_firstpoint_smooth_window``), ``flags=('infinite',)``
-    with a global line of sight through ``_infinite_window``.  The first-point 'infinite'
-    window and the 'jaxdecomp' backend raise ``NotImplementedError``.
+    through ``_infinite_window`` (first point: ``_firstpoint_infinite_window``).  Those flags
+    with the 'local' theory line of sight and the 'jaxdecomp' backend raise
+    ``NotImplementedError``.
     """
     from .types import WindowMatrix
     flags = tuple(flags)
@@ -751,18 +752,11 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     if norm.ndim <= 1:
         norm = norm * np.ones(nells, dtype='f4')
     rnorm = (_norm / norm / N).astype('f4')
-    if 'infinite' in flags and 'smooth' not in flags:
-        if vlos is None:
-            raise NotImplementedError("the 'infinite' window flag takes a global line of sight on the GPU path")
-        edgesin, ellsin = _window_edges(edgesin, ellsin)
-        Q = None if periodic else _selection_q(meshes, fields, mattrs, N)
-        wmat = _infinite_window(mattrs, bin, Q, vlos, ellsin, edgesin, rnorm, batch_size)
-        return _window_matrix(bin, norm, edgesin, ellsin, wmat)
-    if 'smooth' in flags and vlos is None:
+    if ('smooth' in flags or 'infinite' in flags) and vlos is None:
         if isinstance(ellsin, (tuple, list)) and len(ellsin) == 2 and isinstance(ellsin[1], str):
             ellsin, theory_los = ellsin
             if theory_los != 'firstpoint':
-                raise NotImplementedError("the 'smooth' window takes the 'firstpoint' theory line of sight")
+                raise NotImplementedError("the 'smooth' / 'infinite' windows take the 'firstpoint' theory line of sight")
         if ellsin is not None and np.ndim(ellsin) == 0:
             ellsin = (ellsin,)
         if ellsin is not None:
@@ -771,7 +765,15 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
                 raise NotImplementedError('wide-angle orders > 0 are not supported')
             ellsin = [e for e, _ in ellsin]
         edgesin, ellsin = _window_edges(edgesin, ellsin)
-        wmat = _firstpoint_smooth_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm)
+        if 'smooth' in flags:
+            wmat = _firstpoint_smooth_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm)
+        else:
+            wmat = _firstpoint_infinite_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm)
+        return _window_matrix(bin, norm, edgesin, ellsin, wmat)
+    if 'infinite' in flags and 'smooth' not in flags:
+        edgesin, ellsin = _window_edges(edgesin, ellsin)
+        Q = None if periodic else _selection_q(meshes, fields, mattrs, N)
+        wmat = _infinite_window(mattrs, bin, Q, vlos, ellsin, edgesin, rnorm, batch_size)
         return _window_matrix(bin, norm, edgesin, ellsin, wmat)
     if 'smooth' in flags:
         edgesin, ellsin = _window_edges(edgesin, ellsin)
@@ -1062,6 +1064,73 @@ def _firstpoint_smooth_window(meshes, fields, periodic, mattrs, bin, edgesin, el
     if ells[0] % 2:  # the reference keeps the imaginary part of the first multipole's rows: 0 here
         wmat[:nb] = 0.
     return wmat
+
+
+def _firstpoint_infinite_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm):
+    """'infinite' window of the first-point line of sight, wide-angle order 0
+    (``mesh2.py:1240-1262``): for each ell_in and output (ell, m),
+    ``C_{ell m} = V_cell sum_m1 Y_{ell_in m1}(shat) Q_{ell m m1}`` (``pk_ylm_separation_accumulate``),
+    then per input bin ``4 pi rnorm bin(sum_m r2c(W_in(|s|) C_{ell m}) Y_lm(khat))`` with k = 0
+    dropped for ell = 0 only, ``W_in`` the tophat Bessel profile tabulated on the distinct |s|."""
+    meshsize = mattrs.meshsize
+    stream = _lib.stream_handle()
+    if swap:
+        meshes = meshes[::-1]
+    if periodic:
+        rmesh1 = torch.ones(tuple(int(n) for n in meshsize), dtype=torch.float32, device=_device())
+        A0 = _r2c(rmesh1, meshsize)
+    else:
+        rmesh1 = _2r(meshes[0]).value.contiguous()
+        A0 = _2c(meshes[0] if fields[1] == fields[0] else meshes[1]).value.contiguous()
+    offset = (mattrs.boxcenter - (mattrs.boxsize / np.float32(2.)).astype('f4')).astype('f4')
+    geo = (_lib.i32(meshsize), _lib.f32(mattrs.cellsize), _lib.f32(offset))
+    kf = _lib.f32(mattrs.kfun)
+    rshape = tuple(int(n) for n in meshsize)
+    cshape = rshape[:2] + (rshape[2] // 2 + 1,)
+    sx, sy, sz = mattrs.rcoords(kind='separation', sparse=True)
+    snorm = torch.sqrt((sx * sx + sy * sy) + sz * sz)
+    uniq, inverse = torch.unique(snorm.reshape(-1), return_inverse=True)
+    uniq_h = uniq.cpu().numpy().astype('f8')
+    cellvol = float(np.prod(mattrs.cellsize.astype('f8')))
+    ells = bin.ells
+    nb = bin.nbins
+    out_terms = [(ell, m) for ell in ells for m in range(-ell, ell + 1)]
+    r1 = torch.empty((1,) + rshape, dtype=torch.float32, device=_device())
+    col = torch.empty(rshape, dtype=torch.float32, device=_device())
+    blocks = []
+    for ellin in ellsin:
+        n1 = 2 * ellin + 1
+        in_ell, in_m = _lib.i32([ellin] * n1), _lib.i32(list(range(-ellin, ellin + 1)))
+        R = torch.empty((n1,) + rshape, dtype=torch.float32, device=_device())
+        C = torch.zeros((len(out_terms),) + rshape, dtype=torch.float32, device=_device())
+        for t, (ell, m) in enumerate(out_terms):
+            _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rmesh1), *geo, 1, _lib.i32([ell]), _lib.i32([m]),
+                      _lib.ptr(r1))
+            _lib.call('pk_ylm_premultiply', stream, _lib.ptr(r1), *geo, n1, in_ell, in_m, _lib.ptr(R))
+            F = _r2c(R, meshsize)
+            _lib.call('pk_conj_multiply', stream, _lib.ptr(F), _lib.ptr(A0), n1, A0.numel(), _lib.ptr(F))
+            G = _c2r(F, meshsize, destroy_input=True)
+            del F
+            _lib.call('pk_scale_real', stream, _lib.ptr(G), G.numel(), float(4. * np.pi / (2 * ellin + 1) * cellvol))
+            _lib.call('pk_ylm_separation_accumulate', stream, _lib.ptr(G), _lib.i32(meshsize),
+                      _lib.f32(mattrs.cellsize), n1, in_ell, in_m, _lib.ptr(C[t]))
+            del G
+        block = np.zeros((len(edgesin), len(ells) * nb))
+        for e, (lo, hi) in enumerate(edgesin.astype('f4')):
+            prof = _bessel_shell(ellin, float(lo), float(hi), uniq_h) * (-1) ** (ellin // 2) / (2. * np.pi) ** 3
+            profile = torch.as_tensor(prof.astype('f4'), device=_device())[inverse].reshape(rshape)
+            for ill, ell in enumerate(ells):
+                Aell = torch.zeros(cshape, dtype=torch.complex64, device=_device())
+                for m in range(-ell, ell + 1):
+                    torch.mul(profile, C[out_terms.index((ell, m))], out=col)
+                    Ft = _r2c(col, meshsize)
+                    _lib.call('pk_ylm_kgrid_multiply', stream, _lib.ptr(Ft), _lib.i32(meshsize), kf, 1,
+                              _lib.i32([ell]), _lib.i32([m]), 1., 1, _lib.ptr(Aell))
+                value = 4. * np.pi * bin(Aell, remove_zero=ell == 0) * float(rnorm[ill])
+                block[e, ill * nb:(ill + 1) * nb] = value.imag if (ill == 0 and ell % 2) else value.real
+        blocks.append(block)
+        del C, R
+    return np.concatenate(blocks, axis=0).T
 
 
 def _infinite_window(mattrs, bin, Q, vlos, ellsin, edgesin, rnorm, batch_size=None):

@@ -696,6 +696,66 @@ def compute_smooth2_spectrum_window(s, windows, snmodes, edgesin, ellsin, ells, 
                         spherical_jn(ell, k * savg) * snmodes * tophat)
     return wmat
 
+
+def compute_mesh2_spectrum_window_firstpoint_infinite(bins, edgesin, ellsin, meshes=None, swap=False):
+    """``compute_mesh2_spectrum_window(..., los='firstpoint', flags=('infinite',))``, wide-angle
+    order 0 (``mesh2.py:1240-1262``): ``Qs = V_cell sum_m1 Y_l1m1(shat) Q``, then per input bin
+    ``4 pi rnorm sum_m bin(Y_lm(khat) r2c(W(|s|) Qs))`` (adaptive quadrature for W)."""
+    from scipy.integrate import quad
+    from scipy.special import spherical_jn
+    geom = bins.geom
+    dt = geom.dtype
+    t = dt.type
+    ells = bins.ells
+    N = t(np.prod(geom.meshsize.astype(dt)))
+    rnorm = t(1.) / N
+    edgesin = np.asarray(edgesin, dtype='f8')
+    if edgesin.ndim != 2:
+        edgesin = np.column_stack([edgesin[:-1], edgesin[1:]])
+    meshes = [np.ones(geom.rshape, dtype=dt)] if meshes is None else list(meshes)
+    if swap:
+        meshes = meshes[::-1]
+    rmesh1 = _to_real(geom, meshes[0])
+    A0 = _to_complex(geom, meshes[0] if len(meshes) == 1 else meshes[1])
+    xvec, kvec, svec = rcoords(geom), kcoords(geom), separation_coords(geom)
+    s2 = (((t(0.) + svec[0] * svec[0]).astype(dt) + svec[1] * svec[1]).astype(dt) + svec[2] * svec[2]).astype(dt)
+    snorm = np.sqrt(s2).astype('f8')
+    uniq, inverse = np.unique(snorm.ravel(), return_inverse=True)
+    cellvol = float(np.prod(geom.cellsize.astype('f8')))
+
+    def shell(ell, lo, hi, s):
+        if s == 0.:
+            return 4. * np.pi * (hi ** 3 - lo ** 3) / 3. if ell == 0 else 0.
+        return 4. * np.pi * quad(lambda k: k * k * spherical_jn(ell, k * s), lo, hi, limit=500, epsabs=0.,
+                                 epsrel=1e-9)[0]
+
+    blocks = []
+    for ellin in ellsin:
+        profiles = []
+        for lo, hi in edgesin.astype(dt):
+            prof = np.array([shell(ellin, float(lo), float(hi), x) for x in uniq]) * (-1) ** (ellin // 2) / (2. * np.pi) ** 3
+            profiles.append(prof[inverse].reshape(snorm.shape))
+        block = np.zeros((len(edgesin), len(ells) * bins.nbins), dtype='c16')
+        for ill, ell in enumerate(ells):
+            for m in range(-ell, ell + 1):
+                Y = get_ylm(ell, m)
+                Qs = 0.
+                for m1 in range(-ellin, ellin + 1):
+                    Y1 = get_ylm(ellin, m1)
+                    F = r2c(geom, ((rmesh1 * Y(*xvec)).astype(dt) * Y1(*xvec)).astype(dt))
+                    Q = (t(4. * np.pi / (2 * ellin + 1)) * c2r(geom, (np.conj(F) * A0).astype(np.complex64))).astype(dt)
+                    Qs = Qs + Y1(*svec).astype('f8') * Q * cellvol
+                for e, prof in enumerate(profiles):
+                    A = (Y(*kvec) * r2c(geom, (prof * Qs).astype(dt))).astype(np.complex64)
+                    block[e, ill * bins.nbins:(ill + 1) * bins.nbins] += 4. * np.pi * bins(A, remove_zero=ell == 0) * rnorm
+        blocks.append(block)
+    wmat = np.concatenate(blocks, axis=0).T
+    nb = bins.nbins
+    first = wmat[:nb].imag if ells[0] % 2 else wmat[:nb].real
+    wmat = wmat.real.copy()
+    wmat[:nb] = first
+    return wmat
+
 # --------------------------------------------------------------------------- FKP
 
 def next_fft_size(n, primes=(2, 3, 5, 7), divisors=()):

@@ -341,3 +341,28 @@ def test_firstpoint_smooth_window_matches_oracle(selection, los):
                                              flags=('smooth',))
         ref = owin(ob, sedges, edgesin, (0, 2), meshes=sel, swap=los == 'endpoint')
     _check(w.value, ref)
+
+
+@pytest.mark.parametrize('selection', [None, 'cross'])
+def test_firstpoint_infinite_window_matches_oracle(selection):
+    """'infinite' window with the first-point line of sight against the oracle."""
+    import jaxpower_b200 as jp
+    from oracle.spectrum import compute_mesh2_spectrum_window_firstpoint_infinite as owin
+    meshsize, boxsize, center = (10, 8, 8), np.array([500., 400., 400.]), (900., -200., 300.)
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=center)
+    ells = (0, 2) if selection is None else (1, 2)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.02}, ells=ells)
+    ob = Bins(Geometry(meshsize, boxsize, center), step=0.02, ells=ells)
+    rng = np.random.default_rng(31)
+    sel = [rng.uniform(0.5, 1.5, meshsize).astype('f4') for _ in range(2)]
+    edgesin = np.arange(0.005, 0.06, 0.02)
+    if selection is None:
+        w = jp.compute_mesh2_spectrum_window(attrs, edgesin=edgesin, ellsin=(0, 2), bin=b, los='firstpoint',
+                                             flags=('infinite',))
+        ref = owin(ob, edgesin, (0, 2))
+    else:
+        meshes = [attrs.create(kind='real', fill=torch.as_tensor(s)) for s in sel]
+        w = jp.compute_mesh2_spectrum_window(*meshes, edgesin=edgesin, ellsin=(0, 2), bin=b, los='endpoint',
+                                             flags=('infinite',))
+        ref = owin(ob, edgesin, (0, 2), meshes=sel, swap=True)
+    _check(w.value, ref)
