@@ -12,6 +12,7 @@ Mirrors ``jaxpower/mesh2.py``:
 - ``compute_fkp2_normalization`` / ``compute_fkp2_shotnoise`` /
   ``compute_box2_normalization`` (``mesh2.py:508-621``).
 """
+import functools
 import math
 
 import numpy as np
@@ -726,9 +727,9 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     through ``_firstpoint_window``, the 'local' theory line of sight (``ellsin=(ells, 'local')``)
     through ``_local_window``.  ``flags=('smooth',)`` with a global line of sight goes through
     ``_smooth_window`` (first point: ``_firstpoint_smooth_window``), ``flags=('infinite',)``
-    through ``_infinite_window`` (first point: ``_firstpoint_infinite_window``).  Those flags
-    with the 'local' theory line of sight and the 'jaxdecomp' backend raise
-    ``NotImplementedError``.
+    through ``_infinite_window`` (first point: ``_firstpoint_infinite_window``); 'smooth' with
+    the 'local' theory line of sight through ``_local_smooth_window``.  'infinite' with the
+    'local' theory line of sight and the 'jaxdecomp' backend raise ``NotImplementedError``.
     """
     from .types import WindowMatrix
     flags = tuple(flags)
@@ -755,8 +756,10 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     if ('smooth' in flags or 'infinite' in flags) and vlos is None:
         if isinstance(ellsin, (tuple, list)) and len(ellsin) == 2 and isinstance(ellsin[1], str):
             ellsin, theory_los = ellsin
-            if theory_los != 'firstpoint':
-                raise NotImplementedError("the 'smooth' / 'infinite' windows take the 'firstpoint' theory line of sight")
+            if theory_los not in ('firstpoint', 'local') or (theory_los == 'local' and 'smooth' not in flags):
+                raise NotImplementedError("theory line of sight '{}' with these flags is not supported".format(theory_los))
+        else:
+            theory_los = 'firstpoint'
         if ellsin is not None and np.ndim(ellsin) == 0:
             ellsin = (ellsin,)
         if ellsin is not None:
@@ -765,7 +768,9 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
                 raise NotImplementedError('wide-angle orders > 0 are not supported')
             ellsin = [e for e, _ in ellsin]
         edgesin, ellsin = _window_edges(edgesin, ellsin)
-        if 'smooth' in flags:
+        if 'smooth' in flags and theory_los == 'local':
+            wmat = _local_smooth_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm)
+        elif 'smooth' in flags:
             wmat = _firstpoint_smooth_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm)
         else:
             wmat = _firstpoint_infinite_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm)
@@ -1062,6 +1067,122 @@ def _firstpoint_smooth_window(meshes, fields, periodic, mattrs, bin, edgesin, el
         del R
     wmat = np.concatenate(blocks, axis=0).T
     if ells[0] % 2:  # the reference keeps the imaginary part of the first multipole's rows: 0 here
+        wmat[:nb] = 0.
+    return wmat
+
+
+@functools.lru_cache(maxsize=None)
+def _real_gaunt(lm1, lm2, lm3):
+    """Integral over the sphere of three real spherical harmonics (the ``real_gaunt`` table of
+    ``utils.py:540-622``), by Gauss-Legendre quadrature in cos(theta) and a uniform phi grid
+    (exact for these polynomial degrees).  The harmonics follow the library's definition
+    (associated Legendre functions with the Condon-Shortley phase, cos(m phi) / sin(|m| phi));
+    a (-1)^m convention change leaves every nonzero coefficient unchanged."""
+    from scipy.special import lpmv
+    x, wx = np.polynomial.legendre.leggauss(16)
+    phi = 2. * np.pi * np.arange(48) / 48.
+
+    def Y(ell, m):
+        amp = np.sqrt((2 * ell + 1) / (4. * np.pi))
+        if m != 0:
+            amp *= np.sqrt(2. * math.factorial(ell - abs(m)) / math.factorial(ell + abs(m))) * (-1) ** m
+        trig = np.cos(m * phi) if m > 0 else (np.sin(-m * phi) if m < 0 else np.ones_like(phi))
+        return amp * lpmv(abs(m), ell, x)[:, None] * trig[None, :]
+
+    return float(np.sum(wx[:, None] * (2. * np.pi / 48.) * Y(*lm1) * Y(*lm2) * Y(*lm3)))
+
+
+def _local_smooth_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm):
+    """'smooth' window with the 'local' theory line of sight (``mesh2.py:1319-1361``, combined into
+    the input multipoles as ``:1447-1455``).  For each (ell1, ell2) in {2, 0}^2, output ell and
+    p in (0, 2, 4) with a nonzero Gaunt (p 0, ell1 0, ell2 0):
+    ``Qs_p = 4 pi V_cell sbin(sum_{m, m1, m2, mp} G(p mp, l1 m1, l2 m2) Y_lm(shat) Y_p mp(shat) Q)``,
+    ``Q = (4 pi)^2 / ((2 l1 + 1)(2 l2 + 1)) c2r(conj(r2c(W1 Y_lm Y_l1m1)) r2c(W2 Y_l2m2))``.  The
+    Gaunt sums are one small matrix product over the pair meshes (torch); the Y(shat) weights go
+    through ``pk_ylm_separation_accumulate``; then host Bessel transforms with the tophat of
+    order p."""
+    from scipy.special import spherical_jn
+    meshsize = mattrs.meshsize
+    stream = _lib.stream_handle()
+    if any(ell not in (0, 2, 4) for ell in ellsin):
+        raise ValueError("the 'local' theory line of sight takes input multipoles among (0, 2, 4)")
+    if swap:
+        meshes = meshes[::-1]
+    if periodic:
+        rmesh1 = torch.ones(tuple(int(n) for n in meshsize), dtype=torch.float32, device=_device())
+        rmesh2 = rmesh1
+    else:
+        rmesh1 = _2r(meshes[0]).value.contiguous()
+        rmesh2 = rmesh1 if fields[1] == fields[0] else _2r(meshes[1]).value.contiguous()
+    offset = (mattrs.boxcenter - (mattrs.boxsize / np.float32(2.)).astype('f4')).astype('f4')
+    geo = (_lib.i32(meshsize), _lib.f32(mattrs.cellsize), _lib.f32(offset))
+    cs = _lib.f32(mattrs.cellsize)
+    rshape = tuple(int(n) for n in meshsize)
+    cshape = rshape[:2] + (rshape[2] // 2 + 1,)
+    nreal = int(np.prod(rshape))
+    t2 = [(0, 0)] + [(2, m) for m in range(-2, 3)]
+    R2 = torch.empty((len(t2),) + rshape, dtype=torch.float32, device=_device())
+    _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rmesh2), *geo, len(t2), _lib.i32([t[0] for t in t2]),
+              _lib.i32([t[1] for t in t2]), _lib.ptr(R2))
+    B = _r2c(R2, meshsize)
+    del R2
+    index2 = {t: i for i, t in enumerate(t2)}
+    sbin = BinMesh2CorrelationPoles(mattrs, edges=None)
+    snmodes = sbin.nmodes
+    with np.errstate(invalid='ignore', divide='ignore'):
+        savg = np.where(snmodes == 0, 0., sbin.xavg)
+    kout = np.where(bin.nmodes == 0, 0., bin.xavg)
+    cellvol = float(np.prod(mattrs.cellsize.astype('f8')))
+    ells, nb, nin = bin.ells, bin.nbins, len(edgesin)
+    coeff2 = {(0, 0): [(0, 1.), (4, -7. / 18.)], (0, 2): [(2, 1. / 2.), (4, -5. / 18.)], (2, 2): [(4, 35. / 18.)]}
+    coeff2[2, 0] = coeff2[0, 2]
+    r1 = torch.empty((1,) + rshape, dtype=torch.float32, device=_device())
+    wmat = np.zeros((len(ellsin), nin, len(ells) * nb))
+    for ell1 in (2, 0):
+        for ell2 in (2, 0):
+            pairs = [(m1, m2) for m1 in range(-ell1, ell1 + 1) for m2 in range(-ell2, ell2 + 1)]
+            weight = (4. * np.pi) ** 2 / ((2 * ell1 + 1) * (2 * ell2 + 1))
+            n1 = 2 * ell1 + 1
+            in_ell, in_m = _lib.i32([ell1] * n1), _lib.i32(list(range(-ell1, ell1 + 1)))
+            R = torch.empty((n1,) + rshape, dtype=torch.float32, device=_device())
+            P = torch.empty((len(pairs),) + cshape, dtype=torch.complex64, device=_device())
+            ps = [p for p in (0, 2, 4) if abs(_real_gaunt((p, 0), (ell1, 0), (ell2, 0))) > 1e-10]
+            gaunt = {p: torch.as_tensor(np.array([[_real_gaunt((p, mp), (ell1, m1), (ell2, m2)) for m1, m2 in pairs]
+                                                   for mp in range(-p, p + 1)], dtype='f4'), device=_device())
+                     for p in ps}
+            block = np.zeros((nin, len(ells) * nb))
+            for ill, ell in enumerate(ells):
+                carry3 = {p: torch.zeros(rshape, dtype=torch.float32, device=_device()) for p in ps}
+                for m in range(-ell, ell + 1):
+                    _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rmesh1), *geo, 1, _lib.i32([ell]), _lib.i32([m]),
+                              _lib.ptr(r1))
+                    _lib.call('pk_ylm_premultiply', stream, _lib.ptr(r1), *geo, n1, in_ell, in_m, _lib.ptr(R))
+                    F = _r2c(R, meshsize)
+                    for q, (m1, m2) in enumerate(pairs):
+                        _lib.call('pk_conj_multiply', stream, _lib.ptr(F[m1 + ell1]), _lib.ptr(B[index2[ell2, m2]]), 1,
+                                  B[0].numel(), _lib.ptr(P[q]))
+                    G = _c2r(P, meshsize) * weight
+                    for p in ps:
+                        H = torch.tensordot(gaunt[p], G.reshape(len(pairs), nreal), dims=1).contiguous()
+                        carry = torch.zeros(rshape, dtype=torch.float32, device=_device())
+                        _lib.call('pk_ylm_separation_accumulate', stream, _lib.ptr(H), _lib.i32(meshsize), cs, 2 * p + 1,
+                                  _lib.i32([p] * (2 * p + 1)), _lib.i32(list(range(-p, p + 1))), _lib.ptr(carry))
+                        _lib.call('pk_ylm_separation_accumulate', stream, _lib.ptr(carry), _lib.i32(meshsize), cs, 1,
+                                  _lib.i32([ell]), _lib.i32([m]), _lib.ptr(carry3[p]))
+                    del F, G
+                jk = (-1) ** (ell // 2) * spherical_jn(ell, kout[:, None] * savg[None, :]) * snmodes[None, :]
+                for p in ps:
+                    Qp = 4. * np.pi * sbin(carry3[p]) * cellvol
+                    if ell != 0:
+                        Qp[0] = 0.
+                    Qp = np.where(snmodes == 0, 0., Qp)
+                    for e, (lo, hi) in enumerate(edgesin.astype('f4')):
+                        w = _bessel_shell(p, float(lo), float(hi), savg) * (-1) ** (p // 2) / (2. * np.pi) ** 3
+                        block[e, ill * nb:(ill + 1) * nb] += jk.dot(w * Qp) * float(rnorm[ill])
+            for illin, ellin in enumerate(ellsin):
+                wmat[illin] += sum(c * (ell == ellin) for ell, c in coeff2[ell1, ell2]) * block
+    wmat = wmat.reshape(-1, wmat.shape[-1]).T
+    if ells[0] % 2:
         wmat[:nb] = 0.
     return wmat
 

@@ -756,6 +756,94 @@ def compute_mesh2_spectrum_window_firstpoint_infinite(bins, edgesin, ellsin, mes
     wmat[:nb] = first
     return wmat
 
+
+def real_gaunt(lm1, lm2, lm3):
+    """Integral over the sphere of three real Y_lm (``utils.py:540-622``), by quadrature of the
+    oracle's own Y_lm (``get_ylm``) on a Gauss-Legendre x uniform-phi grid."""
+    x, wx = np.polynomial.legendre.leggauss(16)
+    phi = 2. * np.pi * np.arange(48) / 48.
+    st = np.sqrt(1. - x ** 2)[:, None]
+    X, Y, Z = st * np.cos(phi)[None, :], st * np.sin(phi)[None, :], np.broadcast_to(x[:, None], (16, 48))
+    prod = 1.
+    for ell, m in (lm1, lm2, lm3):
+        prod = prod * get_ylm(ell, m)(X, Y, Z)
+    return float(np.sum(wx[:, None] * (2. * np.pi / 48.) * prod))
+
+
+def compute_mesh2_spectrum_window_local_smooth(bins, sedges, edgesin, ellsin, meshes=None, swap=False):
+    """``compute_mesh2_spectrum_window(..., ellsin=(ellsin, 'local'), los='firstpoint',
+    flags=('smooth',))`` (``mesh2.py:1319-1361``, ``1447-1455``), as direct sums over every
+    (m, m1, m2, mp) term."""
+    from scipy.integrate import quad
+    from scipy.special import spherical_jn
+    geom = bins.geom
+    dt = geom.dtype
+    t = dt.type
+    ells = bins.ells
+    N = t(np.prod(geom.meshsize.astype(dt)))
+    rnorm = t(1.) / N
+    edgesin = np.asarray(edgesin, dtype='f8')
+    if edgesin.ndim != 2:
+        edgesin = np.column_stack([edgesin[:-1], edgesin[1:]])
+    meshes = [np.ones(geom.rshape, dtype=dt)] if meshes is None else list(meshes)
+    if swap:
+        meshes = meshes[::-1]
+    rmesh1 = _to_real(geom, meshes[0])
+    rmesh2 = rmesh1 if len(meshes) == 1 else _to_real(geom, meshes[1])
+    xvec, svec = rcoords(geom), separation_coords(geom)
+    sbin = CorrelationBins(geom, edges=sedges)
+    snmodes = sbin.nmodes
+    with np.errstate(invalid='ignore', divide='ignore'):
+        savg = np.where(snmodes == 0, 0., sbin.xavg)
+    kout = np.where(bins.nmodes == 0, 0., bins.xavg)
+    cellvol = float(np.prod(geom.cellsize.astype('f8')))
+
+    def shell(ell, lo, hi, s):
+        if s == 0.:
+            return 4. * np.pi * (hi ** 3 - lo ** 3) / 3. if ell == 0 else 0.
+        return 4. * np.pi * quad(lambda k: k * k * spherical_jn(ell, k * s), lo, hi, limit=500, epsabs=0.,
+                                 epsrel=1e-9)[0]
+
+    coeff2 = {(0, 0): [(0, 1.), (4, -7. / 18.)], (0, 2): [(2, 1. / 2.), (4, -5. / 18.)], (2, 2): [(4, 35. / 18.)]}
+    coeff2[2, 0] = coeff2[0, 2]
+    wmat = np.zeros((len(ellsin), len(edgesin), len(ells) * bins.nbins))
+    for ell1 in (2, 0):
+        for ell2 in (2, 0):
+            ps = [p for p in (0, 2, 4) if abs(real_gaunt((p, 0), (ell1, 0), (ell2, 0))) > 1e-10]
+            block = np.zeros((len(edgesin), len(ells) * bins.nbins))
+            for ill, ell in enumerate(ells):
+                Qs = {p: 0. for p in ps}
+                for m1 in range(-ell1, ell1 + 1):
+                    for m2 in range(-ell2, ell2 + 1):
+                        for m in range(-ell, ell + 1):
+                            Yl = get_ylm(ell, m)
+                            F = r2c(geom, ((rmesh1 * Yl(*xvec)).astype(dt) * get_ylm(ell1, m1)(*xvec)).astype(dt))
+                            B = r2c(geom, (rmesh2 * get_ylm(ell2, m2)(*xvec)).astype(dt))
+                            Q = t((4. * np.pi) ** 2 / ((2 * ell1 + 1) * (2 * ell2 + 1))) * c2r(geom, (np.conj(F) * B).astype(np.complex64))
+                            for p in ps:
+                                tmp = 0.
+                                for mp in range(-p, p + 1):
+                                    rg = real_gaunt((p, mp), (ell1, m1), (ell2, m2))
+                                    if abs(rg) > 1e-12:
+                                        tmp = tmp + rg * Yl(*svec) * get_ylm(p, mp)(*svec) * Q.astype('f8')
+                                if not np.isscalar(tmp):
+                                    Qs[p] = Qs[p] + 4. * np.pi * sbin(tmp) * cellvol
+                for p in ps:
+                    Qp = np.broadcast_to(np.asarray(Qs[p], dtype='f8'), savg.shape).copy()
+                    if ell != 0:
+                        Qp[0] = 0.
+                    Qp = np.where(snmodes == 0, 0., Qp)
+                    for e, (lo, hi) in enumerate(edgesin.astype(dt)):
+                        w = np.array([shell(p, float(lo), float(hi), s) for s in savg]) * (-1) ** (p // 2) / (2. * np.pi) ** 3
+                        block[e, ill * bins.nbins:(ill + 1) * bins.nbins] += (-1) ** (ell // 2) * np.sum(
+                            snmodes[None, :] * spherical_jn(ell, kout[:, None] * savg[None, :]) * (w * Qp)[None, :], axis=-1) * rnorm
+            for illin, ellin in enumerate(ellsin):
+                wmat[illin] += sum(c * (ell == ellin) for ell, c in coeff2[ell1, ell2]) * block
+    wmat = wmat.reshape(-1, wmat.shape[-1]).T
+    if ells[0] % 2:
+        wmat[:bins.nbins] = 0.
+    return wmat
+
 # --------------------------------------------------------------------------- FKP
 
 def next_fft_size(n, primes=(2, 3, 5, 7), divisors=()):
