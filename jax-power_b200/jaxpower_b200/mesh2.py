@@ -728,8 +728,8 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     through ``_local_window``.  ``flags=('smooth',)`` with a global line of sight goes through
     ``_smooth_window`` (first point: ``_firstpoint_smooth_window``), ``flags=('infinite',)``
     through ``_infinite_window`` (first point: ``_firstpoint_infinite_window``); 'smooth' with
-    the 'local' theory line of sight through ``_local_smooth_window``.  'infinite' with the
-    'local' theory line of sight and the 'jaxdecomp' backend raise ``NotImplementedError``.
+    the 'local' theory line of sight through ``_local_smooth_window``, 'infinite' through
+    ``_local_infinite_window``.  The 'jaxdecomp' backend raises ``NotImplementedError``.
     """
     from .types import WindowMatrix
     flags = tuple(flags)
@@ -756,7 +756,7 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     if ('smooth' in flags or 'infinite' in flags) and vlos is None:
         if isinstance(ellsin, (tuple, list)) and len(ellsin) == 2 and isinstance(ellsin[1], str):
             ellsin, theory_los = ellsin
-            if theory_los not in ('firstpoint', 'local') or (theory_los == 'local' and 'smooth' not in flags):
+            if theory_los not in ('firstpoint', 'local'):
                 raise NotImplementedError("theory line of sight '{}' with these flags is not supported".format(theory_los))
         else:
             theory_los = 'firstpoint'
@@ -772,6 +772,8 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
             wmat = _local_smooth_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm)
         elif 'smooth' in flags:
             wmat = _firstpoint_smooth_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm)
+        elif theory_los == 'local':
+            wmat = _local_infinite_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm)
         else:
             wmat = _firstpoint_infinite_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm)
         return _window_matrix(bin, norm, edgesin, ellsin, wmat)
@@ -1184,6 +1186,102 @@ def _local_smooth_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin,
     wmat = wmat.reshape(-1, wmat.shape[-1]).T
     if ells[0] % 2:
         wmat[:nb] = 0.
+    return wmat
+
+
+def _local_infinite_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm):
+    """'infinite' window with the 'local' theory line of sight (``mesh2.py:1363-1396``, combined
+    into the input multipoles as ``:1447-1455``).  For each (ell1, ell2) in {2, 0}^2 and output
+    (ell, m): ``C_p = V_cell sum_{m1, m2, mp} G(p mp, l1 m1, l2 m2) Y_p mp(shat) Q`` (the pair
+    meshes of the 'local' window, Gaunt sums by one matrix product, ``pk_ylm_separation_accumulate``),
+    then per input bin ``4 pi rnorm bin(Y_lm(khat) r2c(sum_p W_p(|s|) C_p))`` with k = 0 dropped
+    for ell = 0 only, ``W_p`` the tophat Bessel profile of order p tabulated on the distinct |s|."""
+    meshsize = mattrs.meshsize
+    stream = _lib.stream_handle()
+    if any(ell not in (0, 2, 4) for ell in ellsin):
+        raise ValueError("the 'local' theory line of sight takes input multipoles among (0, 2, 4)")
+    if swap:
+        meshes = meshes[::-1]
+    if periodic:
+        rmesh1 = torch.ones(tuple(int(n) for n in meshsize), dtype=torch.float32, device=_device())
+        rmesh2 = rmesh1
+    else:
+        rmesh1 = _2r(meshes[0]).value.contiguous()
+        rmesh2 = rmesh1 if fields[1] == fields[0] else _2r(meshes[1]).value.contiguous()
+    offset = (mattrs.boxcenter - (mattrs.boxsize / np.float32(2.)).astype('f4')).astype('f4')
+    geo = (_lib.i32(meshsize), _lib.f32(mattrs.cellsize), _lib.f32(offset))
+    cs, kf = _lib.f32(mattrs.cellsize), _lib.f32(mattrs.kfun)
+    rshape = tuple(int(n) for n in meshsize)
+    cshape = rshape[:2] + (rshape[2] // 2 + 1,)
+    nreal = int(np.prod(rshape))
+    t2 = [(0, 0)] + [(2, m) for m in range(-2, 3)]
+    R2 = torch.empty((len(t2),) + rshape, dtype=torch.float32, device=_device())
+    _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rmesh2), *geo, len(t2), _lib.i32([t[0] for t in t2]),
+              _lib.i32([t[1] for t in t2]), _lib.ptr(R2))
+    B = _r2c(R2, meshsize)
+    del R2
+    index2 = {t: i for i, t in enumerate(t2)}
+    sx, sy, sz = mattrs.rcoords(kind='separation', sparse=True)
+    snorm = torch.sqrt((sx * sx + sy * sy) + sz * sz)
+    uniq, inverse = torch.unique(snorm.reshape(-1), return_inverse=True)
+    uniq_h = uniq.cpu().numpy().astype('f8')
+    profiles = {}
+    for p in (0, 2, 4):
+        profiles[p] = [torch.as_tensor((_bessel_shell(p, float(lo), float(hi), uniq_h) * (-1) ** (p // 2)
+                                        / (2. * np.pi) ** 3).astype('f4'), device=_device())[inverse].reshape(rshape)
+                       for lo, hi in edgesin.astype('f4')]
+    cellvol = float(np.prod(mattrs.cellsize.astype('f8')))
+    ells, nb, nin = bin.ells, bin.nbins, len(edgesin)
+    coeff2 = {(0, 0): [(0, 1.), (4, -7. / 18.)], (0, 2): [(2, 1. / 2.), (4, -5. / 18.)], (2, 2): [(4, 35. / 18.)]}
+    coeff2[2, 0] = coeff2[0, 2]
+    r1 = torch.empty((1,) + rshape, dtype=torch.float32, device=_device())
+    xi = torch.empty(rshape, dtype=torch.float32, device=_device())
+    wmat = np.zeros((len(ellsin), nin, len(ells) * nb), dtype='c16')
+    for ell1 in (2, 0):
+        for ell2 in (2, 0):
+            pairs = [(m1, m2) for m1 in range(-ell1, ell1 + 1) for m2 in range(-ell2, ell2 + 1)]
+            weight = (4. * np.pi) ** 2 / ((2 * ell1 + 1) * (2 * ell2 + 1))
+            n1 = 2 * ell1 + 1
+            in_ell, in_m = _lib.i32([ell1] * n1), _lib.i32(list(range(-ell1, ell1 + 1)))
+            R = torch.empty((n1,) + rshape, dtype=torch.float32, device=_device())
+            P = torch.empty((len(pairs),) + cshape, dtype=torch.complex64, device=_device())
+            ps = [p for p in (0, 2, 4) if abs(_real_gaunt((p, 0), (ell1, 0), (ell2, 0))) > 1e-10]
+            gaunt = {p: torch.as_tensor(np.array([[_real_gaunt((p, mp), (ell1, m1), (ell2, m2)) for m1, m2 in pairs]
+                                                   for mp in range(-p, p + 1)], dtype='f4'), device=_device())
+                     for p in ps}
+            block = np.zeros((nin, len(ells) * nb), dtype='c16')
+            for ill, ell in enumerate(ells):
+                for m in range(-ell, ell + 1):
+                    _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rmesh1), *geo, 1, _lib.i32([ell]), _lib.i32([m]),
+                              _lib.ptr(r1))
+                    _lib.call('pk_ylm_premultiply', stream, _lib.ptr(r1), *geo, n1, in_ell, in_m, _lib.ptr(R))
+                    F = _r2c(R, meshsize)
+                    for q, (m1, m2) in enumerate(pairs):
+                        _lib.call('pk_conj_multiply', stream, _lib.ptr(F[m1 + ell1]), _lib.ptr(B[index2[ell2, m2]]), 1,
+                                  B[0].numel(), _lib.ptr(P[q]))
+                    G = _c2r(P, meshsize) * (weight * cellvol)
+                    C = {}
+                    for p in ps:
+                        H = torch.tensordot(gaunt[p], G.reshape(len(pairs), nreal), dims=1).contiguous()
+                        C[p] = torch.zeros(rshape, dtype=torch.float32, device=_device())
+                        _lib.call('pk_ylm_separation_accumulate', stream, _lib.ptr(H), _lib.i32(meshsize), cs, 2 * p + 1,
+                                  _lib.i32([p] * (2 * p + 1)), _lib.i32(list(range(-p, p + 1))), _lib.ptr(C[p]))
+                    del F, G
+                    for e in range(nin):
+                        xi.zero_()
+                        for p in ps:
+                            xi.add_(profiles[p][e] * C[p])
+                        A = _r2c(xi, meshsize)
+                        Aell = torch.zeros(cshape, dtype=torch.complex64, device=_device())
+                        _lib.call('pk_ylm_kgrid_multiply', stream, _lib.ptr(A), _lib.i32(meshsize), kf, 1,
+                                  _lib.i32([ell]), _lib.i32([m]), 1., 0, _lib.ptr(Aell))
+                        block[e, ill * nb:(ill + 1) * nb] += 4. * np.pi * bin(Aell, remove_zero=ell == 0) * float(rnorm[ill])
+            for illin, ellin in enumerate(ellsin):
+                wmat[illin] += sum(c * (ell == ellin) for ell, c in coeff2[ell1, ell2]) * block
+    wmat = wmat.reshape(-1, wmat.shape[-1]).T
+    first = wmat[:nb].imag if ells[0] % 2 else wmat[:nb].real
+    wmat = wmat.real.copy()
+    wmat[:nb] = first
     return wmat
 
 

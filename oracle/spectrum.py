@@ -844,6 +844,74 @@ def compute_mesh2_spectrum_window_local_smooth(bins, sedges, edgesin, ellsin, me
         wmat[:bins.nbins] = 0.
     return wmat
 
+
+def compute_mesh2_spectrum_window_local_infinite(bins, edgesin, ellsin, meshes=None, swap=False):
+    """``compute_mesh2_spectrum_window(..., ellsin=(ellsin, 'local'), los='firstpoint',
+    flags=('infinite',))`` (``mesh2.py:1363-1396``, ``1447-1455``), as direct sums."""
+    from scipy.integrate import quad
+    from scipy.special import spherical_jn
+    geom = bins.geom
+    dt = geom.dtype
+    t = dt.type
+    ells = bins.ells
+    N = t(np.prod(geom.meshsize.astype(dt)))
+    rnorm = t(1.) / N
+    edgesin = np.asarray(edgesin, dtype='f8')
+    if edgesin.ndim != 2:
+        edgesin = np.column_stack([edgesin[:-1], edgesin[1:]])
+    meshes = [np.ones(geom.rshape, dtype=dt)] if meshes is None else list(meshes)
+    if swap:
+        meshes = meshes[::-1]
+    rmesh1 = _to_real(geom, meshes[0])
+    rmesh2 = rmesh1 if len(meshes) == 1 else _to_real(geom, meshes[1])
+    xvec, kvec, svec = rcoords(geom), kcoords(geom), separation_coords(geom)
+    s2 = (((t(0.) + svec[0] * svec[0]).astype(dt) + svec[1] * svec[1]).astype(dt) + svec[2] * svec[2]).astype(dt)
+    snorm = np.sqrt(s2).astype('f8')
+    uniq, inverse = np.unique(snorm.ravel(), return_inverse=True)
+    cellvol = float(np.prod(geom.cellsize.astype('f8')))
+
+    def shell(ell, lo, hi, s):
+        if s == 0.:
+            return 4. * np.pi * (hi ** 3 - lo ** 3) / 3. if ell == 0 else 0.
+        return 4. * np.pi * quad(lambda k: k * k * spherical_jn(ell, k * s), lo, hi, limit=500, epsabs=0.,
+                                 epsrel=1e-9)[0]
+
+    prof = {p: [(np.array([shell(p, float(lo), float(hi), x) for x in uniq]) * (-1) ** (p // 2)
+                 / (2. * np.pi) ** 3)[inverse].reshape(snorm.shape) for lo, hi in edgesin.astype(dt)] for p in (0, 2, 4)}
+    coeff2 = {(0, 0): [(0, 1.), (4, -7. / 18.)], (0, 2): [(2, 1. / 2.), (4, -5. / 18.)], (2, 2): [(4, 35. / 18.)]}
+    coeff2[2, 0] = coeff2[0, 2]
+    wmat = np.zeros((len(ellsin), len(edgesin), len(ells) * bins.nbins), dtype='c16')
+    for ell1 in (2, 0):
+        for ell2 in (2, 0):
+            ps = [p for p in (0, 2, 4) if abs(real_gaunt((p, 0), (ell1, 0), (ell2, 0))) > 1e-10]
+            block = np.zeros((len(edgesin), len(ells) * bins.nbins), dtype='c16')
+            for ill, ell in enumerate(ells):
+                for m in range(-ell, ell + 1):
+                    Yl = get_ylm(ell, m)
+                    Qs = {p: 0. for p in ps}
+                    for m1 in range(-ell1, ell1 + 1):
+                        for m2 in range(-ell2, ell2 + 1):
+                            F = r2c(geom, ((rmesh1 * Yl(*xvec)).astype(dt) * get_ylm(ell1, m1)(*xvec)).astype(dt))
+                            B = r2c(geom, (rmesh2 * get_ylm(ell2, m2)(*xvec)).astype(dt))
+                            Q = t((4. * np.pi) ** 2 / ((2 * ell1 + 1) * (2 * ell2 + 1))) * c2r(geom, (np.conj(F) * B).astype(np.complex64))
+                            for p in ps:
+                                for mp in range(-p, p + 1):
+                                    rg = real_gaunt((p, mp), (ell1, m1), (ell2, m2))
+                                    if abs(rg) > 1e-12:
+                                        Qs[p] = Qs[p] + rg * get_ylm(p, mp)(*svec) * Q.astype('f8')
+                    for e in range(len(edgesin)):
+                        xi = sum(prof[p][e] * Qs[p] * cellvol for p in ps)
+                        A = (Yl(*kvec) * r2c(geom, np.asarray(xi, dtype=dt))).astype(np.complex64)
+                        block[e, ill * bins.nbins:(ill + 1) * bins.nbins] += 4. * np.pi * bins(A, remove_zero=ell == 0) * rnorm
+            for illin, ellin in enumerate(ellsin):
+                wmat[illin] += sum(c * (ell == ellin) for ell, c in coeff2[ell1, ell2]) * block
+    wmat = wmat.reshape(-1, wmat.shape[-1]).T
+    nb = bins.nbins
+    first = wmat[:nb].imag if ells[0] % 2 else wmat[:nb].real
+    wmat = wmat.real.copy()
+    wmat[:nb] = first
+    return wmat
+
 # --------------------------------------------------------------------------- FKP
 
 def next_fft_size(n, primes=(2, 3, 5, 7), divisors=()):

@@ -392,3 +392,27 @@ def test_local_smooth_window_matches_oracle(selection):
                                              los='firstpoint', flags=('smooth',))
         ref = owin(ob, sedges, edgesin, (0, 2, 4), meshes=sel)
     _check(w.value, ref)
+
+
+@pytest.mark.parametrize('selection', [None, 'cross'])
+def test_local_infinite_window_matches_oracle(selection):
+    """'infinite' window with the 'local' theory line of sight against the oracle."""
+    import jaxpower_b200 as jp
+    from oracle.spectrum import compute_mesh2_spectrum_window_local_infinite as owin
+    meshsize, boxsize, center = (8, 8, 6), np.array([500., 400., 400.]), (900., -200., 300.)
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=center)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.02}, ells=(0, 2))
+    ob = Bins(Geometry(meshsize, boxsize, center), step=0.02, ells=(0, 2))
+    rng = np.random.default_rng(41)
+    sel = [rng.uniform(0.5, 1.5, meshsize).astype('f4') for _ in range(2)]
+    edgesin = np.arange(0.005, 0.05, 0.02)
+    if selection is None:
+        w = jp.compute_mesh2_spectrum_window(attrs, edgesin=edgesin, ellsin=((0, 2, 4), 'local'), bin=b,
+                                             los='firstpoint', flags=('infinite',))
+        ref = owin(ob, edgesin, (0, 2, 4))
+    else:
+        meshes = [attrs.create(kind='real', fill=torch.as_tensor(s)) for s in sel]
+        w = jp.compute_mesh2_spectrum_window(*meshes, edgesin=edgesin, ellsin=((0, 2, 4), 'local'), bin=b,
+                                             los='firstpoint', flags=('infinite',))
+        ref = owin(ob, edgesin, (0, 2, 4), meshes=sel)
+    _check(w.value, ref)
