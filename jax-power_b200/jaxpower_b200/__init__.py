@@ -6,7 +6,8 @@ Public API mirrors ``jaxpower`` for the single-GPU power-spectrum estimator:
 ``compute_fkp2_normalization``, ``compute_fkp2_shotnoise``, ``compute_box2_normalization``,
 ``BinMesh2CorrelationPoles``, ``compute_mesh2_correlation``,
 ``compute_mesh2_spectrum_window`` / ``compute_mesh2_spectrum_mean`` (``WindowMatrix``; global,
-first-point and end-point lines of sight) and the ``resamplers`` namespaces.  All computation runs in the CUDA library
+first-point and end-point lines of sight, 'firstpoint' and 'local' theory, 'smooth' and
+'infinite' flags), ``compute_smooth2_spectrum_window`` and the ``resamplers`` namespaces.  All computation runs in the CUDA library
 ``libjaxpower_b200.so`` through its C ABI (``include/jaxpower_b200.h``).
 """
 from . import resamplers
