@@ -1658,8 +1658,8 @@ def _firstpoint_mean(meshes, fields, periodic, mattrs, bin, poles, get_theory, s
     if not isinstance(poles, dict):
         raise NotImplementedError('the first-point mean spectrum takes theory multipoles, not a callable of k')
     poles = {(ell if isinstance(ell, tuple) else (ell, 0)): pole for ell, pole in poles.items()}
-    if any(wa != 0 for _, wa in poles):
-        raise NotImplementedError('wide-angle orders > 0 are not supported')
+    if theory_los == 'local' and any(wa != 0 for _, wa in poles):
+        raise NotImplementedError("wide-angle orders > 0 with the 'local' theory line of sight are not supported")
     meshsize = mattrs.meshsize
     stream = _lib.stream_handle()
     if swap:
@@ -1678,40 +1678,57 @@ def _firstpoint_mean(meshes, fields, periodic, mattrs, bin, poles, get_theory, s
     if theory_los == 'local':
         return _local_mean(rmesh1, A0, meshes, fields, periodic, mattrs, bin, poles, get_theory, swap, norm, rnorm,
                            geo)
-    # xi_{ell1 m1}, every theory term, kept for all output terms
-    terms1 = [(ell1, m1) for (ell1, _) in poles for m1 in range(-ell1, ell1 + 1)]
-    if len(terms1) > 32:
-        raise NotImplementedError('at most 32 theory (ell, m) terms')
-    coef = np.array([4. * np.pi / (2 * ell1 + 1) for ell1, _ in terms1], dtype='f4')
-    xi_c = torch.empty((len(terms1),) + cshape, dtype=torch.complex64, device=_device())
-    t0 = 0
-    for (ell1, wa), pole in poles.items():
-        kernel = torch.zeros(cshape, dtype=torch.complex64, device=_device())
-        kernel.real.copy_((get_theory(pole) * rnorm).to(torch.float32).expand(cshape))
-        n1 = 2 * ell1 + 1
-        _lib.call('pk_ylm_kgrid_multiply', stream, _lib.ptr(kernel), _lib.i32(meshsize), _lib.f32(mattrs.kfun), n1,
-                  _lib.i32([ell1] * n1), _lib.i32(list(range(-ell1, ell1 + 1))), 1., 0, _lib.ptr(xi_c[t0:t0 + n1]))
-        t0 += n1
-    xi = _c2r(xi_c, meshsize, destroy_input=True)
-    del xi_c
-    t_ell, t_m = _lib.i32([t[0] for t in terms1]), _lib.i32([t[1] for t in terms1])
+    # per wide-angle order wa: the theory terms, their xi_{ell1 m1} = c2r(P rnorm Y(khat)) s^wa, and
+    # the mesh W1 |x|^-wa that the Y_lm(xhat) products start from (mesh2.py:1641-1645)
+    was = sorted({wa for _, wa in poles})
+    if any(wa != 0 for wa in was):
+        px, py, pz = mattrs.rcoords(kind='position', sparse=True)
+        xnorm = torch.sqrt((px * px + py * py) + pz * pz)
+        sx, sy, sz = mattrs.rcoords(kind='separation', sparse=True)
+        snorm = torch.sqrt((sx * sx + sy * sy) + sz * sz)
+    groups = []
+    for wa in was:
+        terms1 = [(ell1, m1) for (ell1, w) in poles if w == wa for m1 in range(-ell1, ell1 + 1)]
+        if len(terms1) > 32:
+            raise NotImplementedError('at most 32 theory (ell, m) terms per wide-angle order')
+        coef = np.array([4. * np.pi / (2 * ell1 + 1) for ell1, _ in terms1], dtype='f4')
+        xi_c = torch.empty((len(terms1),) + cshape, dtype=torch.complex64, device=_device())
+        t0 = 0
+        for (ell1, w), pole in poles.items():
+            if w != wa:
+                continue
+            kernel = torch.zeros(cshape, dtype=torch.complex64, device=_device())
+            kernel.real.copy_((get_theory(pole) * rnorm).to(torch.float32).expand(cshape))
+            n1 = 2 * ell1 + 1
+            _lib.call('pk_ylm_kgrid_multiply', stream, _lib.ptr(kernel), _lib.i32(meshsize), _lib.f32(mattrs.kfun), n1,
+                      _lib.i32([ell1] * n1), _lib.i32(list(range(-ell1, ell1 + 1))), 1., 0, _lib.ptr(xi_c[t0:t0 + n1]))
+            t0 += n1
+        xi = _c2r(xi_c, meshsize, destroy_input=True)
+        del xi_c
+        rho = rmesh1
+        if wa != 0:
+            xi = (xi * snorm ** wa).contiguous()
+            rho = (rmesh1 * xnorm ** (-wa)).contiguous()
+        groups.append((rho, terms1, coef, xi,
+                       torch.empty((len(terms1),) + rshape, dtype=torch.float32, device=_device())))
     num = []
     r1 = torch.empty((1,) + rshape, dtype=torch.float32, device=_device())
-    R = torch.empty((len(terms1),) + rshape, dtype=torch.float32, device=_device())
     Q = torch.empty(rshape, dtype=torch.float32, device=_device())
     for ell in bin.ells:
         Aell = torch.zeros(cshape, dtype=torch.complex64, device=_device())
         for m in range(-ell, ell + 1):
-            _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rmesh1), *geo, 1, _lib.i32([ell]), _lib.i32([m]),
-                      _lib.ptr(r1))
-            _lib.call('pk_ylm_premultiply', stream, _lib.ptr(r1), *geo, len(terms1), t_ell, t_m, _lib.ptr(R))
-            F = _r2c(R, meshsize)
-            _lib.call('pk_conj_multiply', stream, _lib.ptr(F), _lib.ptr(A0), len(terms1), A0.numel(), _lib.ptr(F))
-            G = _c2r(F, meshsize, destroy_input=True)
-            del F
-            _lib.call('pk_sum_products', stream, _lib.ptr(Q), _lib.ptr(xi), _lib.ptr(G), len(terms1), _lib.f32(coef),
-                      nreal, 0)
-            del G
+            for gi, (rho, terms1, coef, xi, R) in enumerate(groups):
+                _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rho), *geo, 1, _lib.i32([ell]), _lib.i32([m]),
+                          _lib.ptr(r1))
+                _lib.call('pk_ylm_premultiply', stream, _lib.ptr(r1), *geo, len(terms1),
+                          _lib.i32([t[0] for t in terms1]), _lib.i32([t[1] for t in terms1]), _lib.ptr(R))
+                F = _r2c(R, meshsize)
+                _lib.call('pk_conj_multiply', stream, _lib.ptr(F), _lib.ptr(A0), len(terms1), A0.numel(), _lib.ptr(F))
+                G = _c2r(F, meshsize, destroy_input=True)
+                del F
+                _lib.call('pk_sum_products', stream, _lib.ptr(Q), _lib.ptr(xi), _lib.ptr(G), len(terms1),
+                          _lib.f32(coef), nreal, int(gi > 0))
+                del G
             FQ = _r2c(Q, meshsize)
             _lib.call('pk_ylm_kgrid_multiply', stream, _lib.ptr(FQ), _lib.i32(meshsize), _lib.f32(mattrs.kfun), 1,
                       _lib.i32([ell]), _lib.i32([m]), 1., 1, _lib.ptr(Aell))

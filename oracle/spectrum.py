@@ -351,23 +351,28 @@ def compute_mesh2_spectrum_mean_firstpoint(bins, theory, meshes=None, swap=False
                 value = np.conj(value)
             out.append(np.real(value) if ell % 2 == 0 else np.imag(value))
         return np.array(out)
+    # theory keys: ell or (ell, wide-angle order wa): xi * |s|^wa, W1 * |x|^-wa (mesh2.py:1641-1645)
+    theory = {(k if isinstance(k, tuple) else (k, 0)): v for k, v in theory.items()}
+    sv = separation_coords(geom)
+    snorm = np.sqrt(((sv[0] * sv[0] + sv[1] * sv[1]) + sv[2] * sv[2]).astype(dt)).astype(dt)
+    xnorm = np.sqrt(((xvec[0] * xvec[0] + xvec[1] * xvec[1]) + xvec[2] * xvec[2]).astype(dt)).astype(dt)
     xi = {}
-    for ell1, pole in theory.items():
+    for (ell1, wa), pole in theory.items():
         kernel = (np.asarray(pole(knorm)) * rnorm).astype(dt)
         for m1 in range(-ell1, ell1 + 1):
-            xi[ell1, m1] = c2r(geom, (kernel * get_ylm(ell1, m1)(*kvec)).astype(np.complex64))
+            xi[ell1, wa, m1] = (c2r(geom, (kernel * get_ylm(ell1, m1)(*kvec)).astype(np.complex64)) * snorm ** wa).astype(dt)
     out = []
     for ell in bins.ells:
         Aell = np.zeros(geom.cshape, dtype=np.complex64)
         for m in range(-ell, ell + 1):
             Ylm = get_ylm(ell, m)
             Q = np.zeros(geom.rshape, dtype=dt)
-            for ell1 in theory:
+            for ell1, wa in theory:
                 for m1 in range(-ell1, ell1 + 1):
                     Y1 = get_ylm(ell1, m1)
-                    F = r2c(geom, ((rmesh1 * Ylm(*xvec)).astype(dt) * Y1(*xvec)).astype(dt))
+                    F = r2c(geom, (((rmesh1 * xnorm ** (-wa)).astype(dt) * Ylm(*xvec)).astype(dt) * Y1(*xvec)).astype(dt))
                     G = c2r(geom, (np.conj(F) * A0).astype(np.complex64))
-                    Q = (Q + t(4. * np.pi / (2 * ell1 + 1)) * xi[ell1, m1] * G).astype(dt)
+                    Q = (Q + t(4. * np.pi / (2 * ell1 + 1)) * xi[ell1, wa, m1] * G).astype(dt)
             Aell = (Aell + r2c(geom, Q) * Ylm(*kvec)).astype(np.complex64)
         value = 4. * np.pi * bins(Aell)
         if swap:

@@ -416,3 +416,26 @@ def test_local_infinite_window_matches_oracle(selection):
                                              los='firstpoint', flags=('infinite',))
         ref = owin(ob, edgesin, (0, 2, 4), meshes=sel)
     _check(w.value, ref)
+
+
+@pytest.mark.parametrize('selection', [None, 'auto'])
+def test_wide_angle_mean_spectrum_matches_oracle(selection):
+    """First-point mean spectrum with a wide-angle order 1 theory term ((ell, 1) keys):
+    xi |s|, W1 |x|^-1 (mesh2.py:1641-1645)."""
+    import jaxpower_b200 as jp
+    from oracle.spectrum import compute_mesh2_spectrum_mean_firstpoint as omean_fp
+    meshsize, boxsize, center = (12, 10, 8), np.array([500., 400., 300.]), (900., -200., 300.)
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=center)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.02}, ells=(0, 1, 2))
+    ob = Bins(Geometry(meshsize, boxsize, center), step=0.02, ells=(0, 1, 2))
+    rng = np.random.default_rng(43)
+    sel = rng.uniform(0.5, 1.5, meshsize).astype('f4')
+    theory = {(0, 0): _pk0, (2, 0): _pk2, (1, 1): lambda k: 50. * (k + 0.05) ** -1.}
+    if selection is None:
+        got = jp.compute_mesh2_spectrum_mean(attrs, theory=theory, bin=b, los='firstpoint')
+        ref = omean_fp(ob, theory)
+    else:
+        got = jp.compute_mesh2_spectrum_mean(attrs.create(kind='real', fill=torch.as_tensor(sel)), theory=theory, bin=b,
+                                             los='firstpoint')
+        ref = omean_fp(ob, theory, meshes=[sel])
+    _check(np.array([p.num_raw for p in got]), ref)
