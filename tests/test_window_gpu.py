@@ -1,7 +1,8 @@
-"""Window matrix of the power-spectrum multipoles (compute_mesh2_spectrum_window, global line
-of sight, input power on the mesh) against the CPU oracle: periodic box with common and other
-input edges, selection functions (auto and cross) through the batched c2r -> Q -> r2c path.
-Float32 modes and FFTs, float64 bin sums: 2e-5 of the largest entry."""
+"""Window matrices (compute_mesh2_spectrum_window) and mean spectra (compute_mesh2_spectrum_mean)
+against the CPU oracle: global, first-point and end-point lines of sight; input power on the mesh
+and the 'smooth' / 'infinite' flags; 'firstpoint' and 'local' theory lines of sight; wide-angle
+theory orders; periodic boxes and auto / cross selection functions.  Float32 modes and FFTs,
+float64 bin sums: 2e-5 of the largest entry."""
 import numpy as np
 import pytest
 import torch
