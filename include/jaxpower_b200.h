@@ -293,8 +293,9 @@ pk_status pk_bin_global_interlaced(void *stream, const void *shifted, int nbatch
  * foreign runtime that owns the allocator): its scratch is a fixed 16 MiB static device
  * array, held by every GPU that loads the library until exit.  Returns PK_ERR_RANGE when
  * the bins x multipoles need more scratch than that.  The first call on a device looks
- * the array's address up (make it before any stream capture); calls that overlap on the
- * GPU share the array and race. */
+ * the array's address up (make it before any stream capture); later calls on a stream
+ * that is not capturing look it up again, so a recreated context (cudaDeviceReset) is
+ * picked up.  Calls that overlap on the GPU share the array and race. */
 pk_status pk_bin_global_noalloc(void *stream, const void *delta1, const void *delta2,
                                 const int32_t meshsize[3], const float kfun[3],
                                 const float los[3], const float *d_edges, int nedges, float step,

@@ -1775,23 +1775,31 @@ extern "C" pk_status pk_bin_firstpoint(void *stream, const void *a0, const void 
 //
 // - The array is NOALLOC_SCRATCH_BYTES = 16 MiB; every GPU that loads the library holds
 //   it until the process exits.
-// - Host code cannot use the symbol as a device address; the address is looked up once
-//   per device, with that device current, by cudaGetSymbolAddress.  The first call on a
-//   device does this set-up, so make that first call before any stream capture.
+// - Host code cannot use the symbol as a device address; the address is looked up per
+//   device, with that device current, by cudaGetSymbolAddress.  The first call on a device
+//   does this set-up, so make that first call before any stream capture.  Later calls on a
+//   stream that is not capturing look the address up again (it is cheap), so a context
+//   that was destroyed and recreated (cudaDeviceReset) never leaves a stale address behind;
+//   a call on a capturing stream reuses the address of the last call on that device.
 // - Every call shares the array.  Each call overwrites all the partial rows it reads, so
 //   nothing needs clearing between calls, but calls that overlap on the GPU (different
 //   streams, or several host threads) race on it.
 constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)16 << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
-static pk_status noalloc_scratch(void **out) {
+static pk_status noalloc_scratch(cudaStream_t stream, void **out) {
   static std::mutex lock;
   static void *address[256] = {};
   int dev = 0;
   PK_CUDA(cudaGetDevice(&dev));
   PK_REQUIRE(dev >= 0 && dev < 256, PK_ERR_RANGE, "device index %d out of range", dev);
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &capture) != cudaSuccess) {
+    (void)cudaGetLastError();  // e.g. the legacy stream while another stream captures
+    capture = cudaStreamCaptureStatusActive;
+  }
   std::lock_guard<std::mutex> guard(lock);
-  if (!address[dev]) {
+  if (!address[dev] || capture == cudaStreamCaptureStatusNone) {
     void *p = nullptr;
     PK_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
     address[dev] = p;
@@ -1817,7 +1825,7 @@ extern "C" pk_status pk_bin_global_noalloc(void *stream, const void *delta1, con
              "the fixed %zu; use pk_bin_global with a workspace",
              nedges - 1, nells, L.partial_bytes, NOALLOC_SCRATCH_BYTES);
   void *scratch = nullptr;
-  pk_status st = noalloc_scratch(&scratch);
+  pk_status st = noalloc_scratch((cudaStream_t)stream, &scratch);
   if (st) return st;
   return pk_bin_global(stream, delta1, delta2, meshsize, kfun, los, d_edges, nedges, step, backend,
                        nells, ells, d_out, scratch, NOALLOC_SCRATCH_BYTES);

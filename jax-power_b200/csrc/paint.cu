@@ -290,13 +290,23 @@ __global__ void bucket_kernel(PaintGeom g, const float *__restrict__ pos,
 // Fixed-point exponent e such that count * max|w| * 2^e < 2^62, count = the particles of the
 // catalog: every partial sum of a cell fits in a signed 64-bit integer (each particle adds
 // at most |w| to a cell).  It depends on the catalog only, not on the tiling, so every tile
-// configuration rounds each contribution identically and paints the same bits.
+// configuration rounds each contribution identically and paints the same bits.  For tiny
+// weights e exceeds float32's largest power of two (127; max|w| subnormal gives up to 187),
+// so the scale is applied as two exact factors (fixed_scales).
 __device__ __forceinline__ int fixed_exponent(unsigned wmax_bits, long long count) {
   const float wmax = __uint_as_float(wmax_bits);
   if (!(wmax > 0.f) || !isfinite(wmax)) return 40;
-  const int ew = (int)((wmax_bits >> 23) & 0xff) - 126;  // wmax < 2^ew
+  const int ew = (int)((wmax_bits >> 23) & 0xff) - 126;  // wmax < 2^ew (subnormals: 2^-126)
   const int en = 64 - __clzll(count > 0 ? count : 1);     // count < 2^en
-  return 62 - ew - en;
+  return 62 - ew - en;                                    // in [-129, 187]
+}
+
+// 2^e as two float32 factors, each a power of two within float32's normal range or (e < -126)
+// an exact subnormal: (w * s0) * s1 is w 2^e exactly whenever that is a normal float.
+__device__ __forceinline__ void fixed_scales(int e, float *s0, float *s1) {
+  const int e0 = e > 120 ? 120 : e;
+  *s0 = ldexpf(1.f, e0);
+  *s1 = ldexpf(1.f, e - e0);
 }
 
 // Shared-memory atomics on 32-bit shared-window addresses.
@@ -385,7 +395,8 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
     __syncthreads();
     const long long ncat = g.offsets ? (long long)(g.offsets[mock + 1] - g.offsets[mock]) : (long long)g.n;
     const int fexp = fixed_exponent(*wmax_bits, ncat);
-    const float fscale = ldexpf(1.f, fexp);  // exact power-of-two scaling of each contribution
+    float fscale0, fscale1;  // exact power-of-two scaling of each contribution, 2^fexp
+    fixed_scales(fexp, &fscale0, &fscale1);
     const int ns[3] = {g.d.n0, g.d.n1, g.d.n2};
     const int tl[3] = {T0, T1, T2};
     constexpr int OLO = -((ORDER - 1) / 2);
@@ -410,7 +421,7 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
       const float uq[3] = {q.x, q.y, q.z};
       // w 2^fexp is exact, so (w 2^fexp) * ker rounds like the reference's w * ker, scaled;
       // lanes past the end of the bucket add zeros (to their scratch words)
-      const float wq = has ? q.w * fscale : 0.f;
+      const float wq = has ? __fmul_rn(__fmul_rn(q.w, fscale0), fscale1) : 0.f;
       for (int s = s_begin; s < s_end; ++s) {
         float k[3][ORDER];
         int l[3][ORDER];

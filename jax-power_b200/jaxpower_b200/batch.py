@@ -67,7 +67,7 @@ class BatchedSpectra:
                                                          device=dev)
         self.nells, self.nbins = len(bin.ells), bin.nbins
         self.raw = torch.zeros(M * self.nells * self.nbins, dtype=torch.float64, device=dev)
-        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.status_flag = torch.zeros(1, dtype=torch.int32, device=dev)
         nbytes = _lib.c_size_t()
         _lib.call('pk_bin_batch_workspace_size', _lib.i32(shape), len(bin._edges1d), self.nells, M,
                   _lib.ctypes.byref(nbytes))
@@ -111,11 +111,12 @@ class BatchedSpectra:
         _lib.call('pk_paint_batch', _lib.stream_handle(), _lib.ptr(self.positions), _lib.ptr(self.weights),
                   _lib.ptr(self.offsets), self.n, self.nmocks, _lib.i32(a.meshsize), _lib.f32(a.boxsize),
                   _lib.f32(a.boxcenter), _lib.f32(a.cellsize), self.order, self.interlacing, 0, self.interlacing,
-                  config, _lib.ptr(self.real), _lib.ptr(ws), ws.numel(), _lib.ptr(self.status))
+                  config, _lib.ptr(self.real), _lib.ptr(ws), ws.numel(), _lib.ptr(self.status_flag))
 
     def _enqueue(self):
         a, b = self.attrs, self.bin
         stream = _lib.stream_handle()
+        self.status_flag.zero_()  # inside the graph: every replay reports its own inputs
         self._paint_with(self.tile_config, self.paint_ws)
         _lib.call('pk_fft_exec', self.plan, stream, _lib.ptr(self.real), _lib.ptr(self.cplx))
         if self.fused:
@@ -132,10 +133,14 @@ class BatchedSpectra:
                   a.backend_code, self.nells, _lib.i32(b.ells), _lib.ptr(self.raw), _lib.ptr(self.bin_ws),
                   self.bin_ws.numel())
 
-    def __call__(self, positions=None, weights=None):
+    def __call__(self, positions=None, weights=None, check=True):
         """Multipoles ``num_raw`` of every catalog: (nmocks, nells, nbins) float64 on the device.
 
         ``positions`` (concatenated, (n, 3)) are copied into the static input buffer first.
+        ``check``: raise ``ValueError`` if a particle was dropped (non-finite position or
+        weight, or a position far outside the box), as ``ParticleField.paint`` does; this waits
+        for the batch.  With ``check=False`` the call stays asynchronous and ``status()`` reads
+        the flag later.
         """
         if positions is not None:
             self.positions.copy_(positions)
@@ -149,4 +154,11 @@ class BatchedSpectra:
             self.graph.replay()
         else:
             self._enqueue()
+        if check and self.status():
+            raise ValueError('non-finite or out-of-range particle positions / weights in the batch '
+                             '(those particles were not painted)')
         return self.raw.view(self.nmocks, self.nells, self.nbins) * self.scale
+
+    def status(self):
+        """Nonzero if the last batch dropped a particle (waits for that batch)."""
+        return int(self.status_flag.item())

@@ -70,7 +70,28 @@ def _workspace(nbytes):
 
 # ---------------------------------------------------------------------- FFT plans
 
+class _Plan(_lib.c_void_p):
+    """A cuFFT plan handle (``pk_fft_plan``) destroyed, with its work area, when the last
+    reference goes: the plan cache below and any holder that outlives it (a captured CUDA
+    graph's owner such as ``BatchedSpectra``) keep it alive."""
+
+    nbytes = 0
+
+    def __del__(self):
+        if self.value:
+            try:
+                _lib.load().pk_fft_plan_destroy(self)
+            except Exception:  # interpreter shutdown
+                pass
+            self.value = None
+
+
+# Least-recently-used plan cache.  Each plan holds its own work area (about the size of its
+# complex batch), which the torch caching allocator cannot see, so the cache is bounded by
+# count and by those bytes; an evicted plan is destroyed once nothing else refers to it.
 _PLANS = {}
+_PLAN_CACHE_MAX = 16
+_PLAN_CACHE_BYTES_FRACTION = 0.125
 
 
 def _plan(meshsize, batch, direction):
@@ -78,12 +99,18 @@ def _plan(meshsize, batch, direction):
     # streams (which may run concurrently) must not share a plan
     key = (torch.cuda.current_device(), tuple(int(n) for n in meshsize), int(batch), int(direction),
            torch.cuda.current_stream().cuda_stream)
-    plan = _PLANS.get(key)
+    plan = _PLANS.pop(key, None)
     if plan is None:
-        handle = _lib.c_void_p()
+        plan = _Plan()
         _lib.call('pk_fft_plan_create', _lib.i32(meshsize), int(batch), int(direction),
-                  _lib.ctypes.byref(handle))
-        plan = _PLANS[key] = handle
+                  _lib.ctypes.byref(plan))
+        n0, n1, n2 = key[1]
+        plan.nbytes = 8 * int(batch) * n0 * n1 * (n2 // 2 + 1)
+        limit = _PLAN_CACHE_BYTES_FRACTION * torch.cuda.get_device_properties(key[0]).total_memory
+        while _PLANS and (len(_PLANS) >= _PLAN_CACHE_MAX
+                          or sum(p.nbytes for p in _PLANS.values()) + plan.nbytes > limit):
+            _PLANS.pop(next(iter(_PLANS)))  # oldest use first
+    _PLANS[key] = plan  # most recent last
     return plan
 
 

@@ -56,3 +56,25 @@ def test_batched_vs_oracle_float64():
         ref = ospectrum(opaint.paint(geom, pos.astype('f8'), None, 'tsc', 2, True, 'complex'), ob, los='z')['num_raw']
         scale = np.abs(ref[0]).max()
         assert np.allclose(out[m], ref, rtol=0, atol=1e-5 * scale)
+
+
+def test_batched_reports_dropped_particles():
+    """A non-finite position in one mock raises, like ParticleField.paint; each replay reports its
+    own inputs (the flag is cleared inside the graph), so a clean batch afterwards passes."""
+    import jaxpower_b200 as jp
+    from jaxpower_b200.batch import BatchedSpectra
+    counts = [500, 700]
+    boxsize = 300.
+    attrs = jp.MeshAttrs(meshsize=24, boxsize=boxsize)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.05}, ells=(0, 2))
+    clean = torch.as_tensor(np.concatenate(_mocks(counts, boxsize, seed=4))).cuda()
+    bad = clean.clone()
+    bad[600, 1] = float('nan')
+    bs = BatchedSpectra(attrs, b, counts, resampler='cic', interlacing=2)
+    ref = bs(clean).cpu().numpy()
+    with pytest.raises(ValueError):
+        bs(bad)
+    assert bs(bad, check=False) is not None and bs.status() != 0
+    again = bs(clean).cpu().numpy()
+    assert bs.status() == 0
+    assert np.array_equal(ref, again)

@@ -238,3 +238,26 @@ def test_paint_empty_and_status():
     with pytest.raises(ValueError):
         from jaxpower_b200.mesh import _paint
         _paint(attrs, pos, None, resampler='cic', check=True)
+
+
+@pytest.mark.parametrize('wscale', [1e-20, 1e-38, 1e30])
+def test_paint_tiny_and_huge_weights(wscale):
+    """The 64-bit fixed-point scale 2^e (e = 62 - log2 max|w| - log2 n) leaves float32's range
+    for tiny weights (e up to 187): it is applied as two exact power-of-two factors, so the
+    mesh still equals the float64-accumulated oracle to one ulp (plus the fixed-point step)."""
+    jp = _jp()
+    from jaxpower_b200.mesh import _paint_shifts
+    meshsize, boxsize = 16, 100.
+    pos, w = _catalog(3000, boxsize, 0., seed=9)
+    w = (w.astype('f8') * wscale).astype('f4')
+    assert np.all(np.isfinite(w)) and np.all(w != 0.)
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize)
+    meshes, status = _paint_shifts(attrs, torch.as_tensor(pos).cuda(), torch.as_tensor(w).cuda(), 3, 1)
+    assert int(status.item()) == 0
+    got = meshes[0].cpu().numpy()
+    assert np.all(np.isfinite(got))
+    geom = Geometry(meshsize, boxsize, 0.)
+    exact = opaint.paint_mesh(geom.rshape, opaint.normalize_positions(geom, pos), w, 3, accum='f64')
+    fixed = 3000 * np.abs(w).max(initial=0.).astype('f8') * 2.**-62 * 64
+    tiny = np.finfo(np.float32).smallest_subnormal * 64  # products below the normal range round differently
+    assert np.all(np.abs(got - exact) <= np.spacing(np.abs(exact)) + fixed + tiny)
