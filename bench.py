@@ -10,8 +10,9 @@ global line of sight 'z', ells (0, 2, 4), k edges step 0.005 up to k_Nyq.
 Prints one JSON line (rank 0).  ``value``: spectra/s with positions resident in HBM;
 ``e2e``: the same through the public API with positions copied from pinned host
 memory every step and the multipoles read back.  ``--impl reference`` times the
-CPU oracle (a NumPy/SciPy restatement of the reference's JAX code, which cannot run
-here: no jax) on a bounded sample of the same workload.  Multi-GPU runs are
+CPU oracle (a NumPy/SciPy/C restatement of the reference's JAX code, which cannot run
+here: no jax) on whole 512^3 spectra of the same catalog (the catalog is made on the
+host with NumPy, so both arms read the same positions).  Multi-GPU runs are
 replicas (weak scaling): each rank computes its own spectra, no collective on the
 data path.
 """
@@ -99,8 +100,14 @@ def run_c0(reps=50):
                     Bins(geom, step=c['k_step'], ells=(0, 2, 4)), los='z')['num_raw']
     t_cpu = time.perf_counter() - t
     got = np.array([p.num_raw for p in res])
-    return dict(c, gpu_spectra_per_s=1. / t_gpu, cpu_oracle_spectra_per_s=1. / t_cpu, cpu_cores=os.cpu_count(),
+    geom64 = Geometry(c['meshsize'], c['boxsize'], c['boxsize'] / 2., dtype=np.float64)
+    ref64 = ospectrum(opaint.paint(geom64, pos.astype('f8'), None, c['resampler'], c['interlacing'], c['compensate'],
+                                   'complex'), Bins(geom64, step=c['k_step'], ells=(0, 2, 4)), los='z')
+    same = np.asarray(b.nmodes) == ref64['nmodes']
+    return dict(c, gpu_spectra_per_s=1. / t_gpu, cpu_oracle_spectra_per_s=1. / t_cpu, cpu_cores=cpu_cores(),
                 max_rel_diff_vs_oracle=float(np.abs(got - ref).max() / np.abs(ref[0]).max()),
+                max_rel_diff_vs_fp64_oracle=float(np.abs(got[:, same] - ref64['num_raw'][:, same]).max()
+                                                  / np.abs(ref64['num_raw'][0][same]).max()),
                 timing='GPU: wall clock per spectrum through the public API with host read-back (positions '
                        'resident); CPU: the oracle float32 pipeline, one run')
 
@@ -177,51 +184,112 @@ class ClockSampler:
                 'samples': len(rows), 'reasons': reasons}
 
 
+# ----------------------------------------------------------------------------- benchmark catalog
+
+def lognormal_catalog(meshsize=512, boxsize=1000., nbar=5e-3, seed=42, amplitude=2e4, k0=0.1, index=-1.5,
+                      kcut=0.5):
+    """The benchmark catalog, made on the host with NumPy/SciPy so that both arms (GPU and CPU)
+    read the same float32 positions: a Gaussian field with P(k) = A (k/k0)^index exp(-(k/kcut)^2)
+    (white noise, r2c, times sqrt(P / V_cell), c2r with 1/N^3), the lognormal transform
+    1 + delta_LN = exp(delta - sigma^2 / 2), Poisson counts of mean nbar V_cell (1 + delta_LN)
+    per cell and positions uniform within each cell (the recipe of ``jaxpower_b200.mock``)."""
+    import scipy.fft
+    rng = np.random.default_rng(seed)
+    n = int(meshsize)
+    cell = boxsize / n
+    vcell = cell**3
+    noise = rng.standard_normal((n, n, n), dtype=np.float32)
+    c = scipy.fft.rfftn(noise, workers=-1)
+    del noise
+    kf = 2. * np.pi / boxsize
+    kx = (np.fft.fftfreq(n, 1. / n) * kf).astype('f4')
+    kz = (np.fft.rfftfreq(n, 1. / n) * kf).astype('f4')
+    for i in range(n):  # plane by plane: small temporaries
+        k = np.sqrt(kx[i]**2 + kx[:, None]**2 + kz[None, :]**2)
+        safe = np.where(k > 0, k, 1.)
+        p = np.where(k > 0, amplitude * (safe / k0)**index * np.exp(-(safe / kcut)**2), 0.)
+        c[i] *= np.sqrt(p / vcell).astype('f4')
+    delta = scipy.fft.irfftn(c, s=(n, n, n), workers=-1).astype('f4')
+    del c
+    sigma2 = float(np.mean(delta.astype('f8')**2))
+    lam = np.exp(delta - np.float32(0.5 * sigma2), dtype=np.float32)
+    del delta
+    lam *= np.float32(nbar * vcell)
+    counts = rng.poisson(lam.ravel())
+    del lam
+    cells = np.repeat(np.arange(n**3, dtype=np.int64), counts)
+    ijk = np.stack([cells // (n * n), (cells // n) % n, cells % n], axis=1).astype('f4')
+    del cells
+    u = rng.random(ijk.shape, dtype=np.float32)
+    return ((ijk + u) * np.float32(cell) - np.float32(boxsize / 2.)).astype('f4')
+
+
+def benchmark_catalog(seed=None, meshsize=None):
+    W = WORKLOAD
+    return lognormal_catalog(meshsize=meshsize or W['meshsize'], boxsize=W['boxsize'], nbar=W['nbar'],
+                             seed=W['seed'] if seed is None else seed)
+
+
 # ----------------------------------------------------------------------------- CPU arm
 
-def cpu_sample(meshsize=256, seed=0):
-    """Time the oracle's float32 pipeline on a scaled sample of the workload; return
-    (seconds extrapolated to one full 512^3 spectrum, description, threads)."""
+def oracle_pipeline(meshsize=None, catalog=None, dtype=np.float32):
+    """The oracle's pipeline for the benchmark workload on the host: (one-spectrum callable,
+    positions).  float32: the reference's operation order (serial float32 scatter in C,
+    scipy.fft with all host cores, float64 bin sums); float64: the same in float64."""
     from oracle.coords import Geometry
     from oracle import paint as opaint
     from oracle.spectrum import Bins, compute_mesh2_spectrum
-    full = WORKLOAD['meshsize']
-    scale_n = (full / meshsize)**3
-    npart = int(round(5.0e6 / scale_n))
-    rng = np.random.default_rng(seed)
-    box = WORKLOAD['boxsize']
-    pos = (rng.uniform(-0.5, 0.5, (npart, 3)) * box).astype('f4')
-    geom = Geometry(meshsize, box, 0.)
-    t0 = time.perf_counter()
-    mesh = opaint.paint(geom, pos, None, 'tsc', 3, True, 'complex')
-    t1 = time.perf_counter()
-    bins = Bins(geom, step=WORKLOAD['k_step'], ells=(0, 2, 4))
-    t2 = time.perf_counter()
-    compute_mesh2_spectrum(mesh, bins, los='z', accum='f64')
-    t3 = time.perf_counter()
-    # paint+FFT scale with N_p and N log N, binning with the number of modes
-    fft_factor = scale_n * np.log(full**3) / np.log(meshsize**3)
-    seconds = (t1 - t0) * fft_factor + (t3 - t2) * scale_n
-    desc = ('oracle float32 pipeline (numpy serial paint, scipy.fft workers=all) on a {m}^3 mesh with {n} '
-            'uniform particles ({f:.0f}x fewer cells/particles), per-stage times scaled to 512^3 / 5e6 '
-            '(paint+FFT by N log N, binning by modes); bin setup excluded').format(m=meshsize, n=npart, f=scale_n)
-    return seconds, desc, os.cpu_count()
+    W = WORKLOAD
+    n = meshsize or W['meshsize']
+    pos = benchmark_catalog(meshsize=n) if catalog is None else catalog
+    geom = Geometry(n, W['boxsize'], 0., dtype=dtype)
+    bins = Bins(geom, step=W['k_step'], ells=tuple(W['ells']))  # bin setup, once (as the reference's)
+    x = pos.astype(dtype)
+
+    def spectrum():
+        mesh = opaint.paint(geom, x, None, W['resampler'], W['interlacing'], W['compensate'], 'complex')
+        return compute_mesh2_spectrum(mesh, bins, los=W['los'], accum='f64')
+
+    return spectrum, pos
+
+
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count()
+
+
+ORACLE_SAMPLE = ('oracle float32 pipeline on the benchmark catalog itself, 512^3 (C scatter in the reference\'s '
+                 'serial order, scipy.fft on all host cores, bin sums in float64), measured whole spectra, no scaling')
 
 
 def run_reference(args):
+    """The CPU arm: the oracle's restatement of the reference's JAX CPU path (the reference itself
+    needs jax, absent here), timed on whole 512^3 spectra of the benchmark catalog.  A spectrum
+    takes tens of seconds, so one warm-up step is run and the timed steps stop at ``--ref-budget``
+    seconds (at least one); the line reports the steps actually run."""
     rank = int(os.environ.get('RANK', 0))
     if rank != 0:
         return
+    spectrum, pos = oracle_pipeline()
+    warmup = min(args.warmup, 1)
+    for _ in range(warmup):
+        spectrum()
     times = []
-    for step in range(args.warmup + args.steps):
-        seconds, desc, cores = cpu_sample(meshsize=args.cpu_meshsize, seed=step)
-        if step >= args.warmup:
-            times.append(seconds)
-    value = 1. / float(np.mean(times))
+    t_all = time.perf_counter()
+    while len(times) < args.steps and (not times or time.perf_counter() - t_all < args.ref_budget):
+        t0 = time.perf_counter()
+        spectrum()
+        times.append(time.perf_counter() - t0)
+    value = len(times) / float(np.sum(times))
+    cores = cpu_cores()
     line = {'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': 'spectra/s', 'n_gpus': args.gpus,
-            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 / value, 'higher_is_better': True,
-            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic', 'config': WORKLOAD,
-            'cpu_baseline': {'value': value, 'unit': 'spectra/s', 'cores': cores, 'kind': 'port', 'sample': desc},
+            'steps': len(times), 'warmup': warmup, 'steps_requested': args.steps, 'warmup_requested': args.warmup,
+            'ms_per_step': 1e3 / value, 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'f32', 'data': 'synthetic', 'config': dict(WORKLOAD, nparticles=int(pos.shape[0])),
+            'cpu_baseline': {'value': value, 'unit': 'spectra/s', 'cores': cores, 'kind': 'port',
+                             'sample': ORACLE_SAMPLE + '; {} timed spectra'.format(len(times))},
             'e2e': {'value': value, 'unit': 'spectra/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
     print(json.dumps(line), flush=True)
 
@@ -688,7 +756,8 @@ def run_ours(args):
     if args.meshsize:  # smaller case of the same workload (profiling): same nbar and box
         W['meshsize'] = args.meshsize
     attrs = jp.MeshAttrs(meshsize=W['meshsize'], boxsize=W['boxsize'], boxcenter=0.)
-    positions = lognormal_particles(attrs, power_law_pk(), W['nbar'], seed=W['seed'] + rank)
+    catalog = benchmark_catalog(seed=W['seed'] + rank, meshsize=W['meshsize'])
+    positions = torch.as_tensor(catalog).cuda()
     npart = positions.shape[0]
     bins = jp.BinMesh2SpectrumPoles(attrs, edges={'step': W['k_step']}, ells=tuple(W['ells']))
     torch.cuda.synchronize()
@@ -780,24 +849,112 @@ def run_ours(args):
             'e2e': {'value': e2e_value, 'unit': 'spectra/s', 'h2d_bytes_per_step': int(npart * 12),
                     'd2h_bytes_per_step': int(len(W['ells']) * nbins * 8)},
             'gpu_launches': int(launches), 'stages': stage_report, 'clocks': clocks.summary()}
+    details = {}
     if rank == 0 and world == 1 and not args.no_batched:
-        line['batched'] = run_batched()
-    if rank == 0 and world == 1 and not args.no_cpu:
-        line['c0'] = run_c0()
+        details['batched'] = run_batched()
+        line['batched'] = summary(details['batched'], ('plain_spectra_per_s', 'batched_spectra_per_s', 'speedup',
+                                                       'covariance_max_rel_vs_plain', 'fp64_max_rel'))
     if rank == 0 and world == 1 and not args.no_cutsky:
-        line['cutsky'] = run_cutsky()
+        details['cutsky'] = run_cutsky()
+        line['cutsky'] = summary(details['cutsky'], ('spectra_per_s', 'seconds_forward', 'seconds_forward_backward'))
+        line['cutsky']['gradient_rel_err'] = details['cutsky']['gradient_check']['rel_err']
     if rank == 0 and world == 1 and not args.no_learned:
-        line['learned'] = run_learned()
-        line['learned']['mlp_forward'] = run_mlp_forward()
+        details['learned'] = run_learned()
+        details['learned']['mlp_forward'] = run_mlp_forward()
+        line['learned'] = learned_summary(details['learned'])
     if rank == 0 and world == 1 and not args.no_cpu:
-        seconds, desc, cores = cpu_sample(meshsize=args.cpu_meshsize)
-        line['cpu_baseline'] = {'value': 1. / seconds, 'unit': 'spectra/s', 'cores': cores, 'kind': 'port',
-                                'sample': desc}
+        # the CPU oracle on the same catalog: one whole 512^3 spectrum, timed (no scaling)
+        spectrum, _ = oracle_pipeline(meshsize=W['meshsize'], catalog=catalog)
+        t0 = time.perf_counter()
+        ref32 = spectrum()
+        seconds = time.perf_counter() - t0
+        line['cpu_baseline'] = {'value': 1. / seconds, 'unit': 'spectra/s', 'cores': cpu_cores(), 'kind': 'port',
+                                'sample': ORACLE_SAMPLE + '; 1 timed spectrum'}
+        got = np.array([p.num_raw for p in result])
+        scale = np.abs(ref32['num_raw'][0]).max()
+        parity = {'c1_max_rel_vs_fp32_oracle': float(np.abs(got - ref32['num_raw']).max() / scale),
+                  'c1_nmodes_exact': bool(np.array_equal(np.asarray(bins.nmodes), ref32['nmodes']))}
+        if not args.no_fp64:
+            parity.update(fp64_errors(W, catalog, got, bins))
+        details['c0'] = run_c0()
+        parity['c0_max_rel_vs_fp32_oracle'] = details['c0']['max_rel_diff_vs_oracle']
+        parity['c0_max_rel_vs_fp64_oracle'] = details['c0']['max_rel_diff_vs_fp64_oracle']
+        line['c0'] = summary(details['c0'], ('gpu_spectra_per_s', 'cpu_oracle_spectra_per_s'))
+        line['parity'] = parity
     if rank == 0:
+        if args.details:
+            with open(args.details, 'w') as f:
+                json.dump(details, f, indent=1)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def summary(report, keys):
+    return {k: report[k] for k in keys if k in report}
+
+
+def learned_summary(r):
+    """Scalar figures of the learned-correction report (the full report goes to --details)."""
+    out = {'heldout_bias_max_learned': r['heldout_bias_max']['learned'],
+           'heldout_bias_max_table': r['heldout_bias_max']['mean_table_128'],
+           'heldout_bias_max_plain_128': r['heldout_bias_max']['plain_128'],
+           'heldout_bias_sigma_learned': r['heldout_bias_in_standard_errors']['learned'],
+           'heldout_bias_sigma_table': r['heldout_bias_in_standard_errors']['mean_table_128'],
+           'per_mock_max_rel_err_median_learned': r['heldout_max_rel_err']['learned']['median'],
+           'per_mock_max_rel_err_median_table': r['heldout_max_rel_err']['mean_table_128']['median'],
+           'frac_heldout_within_0p5pct': r['frac_heldout_within_0p5pct'],
+           'per_mock_target_0p5pct_met': r['frac_heldout_within_0p5pct'] >= 0.5,
+           'batched_speedup_learned_vs_plain_512': r['batched_speedup_learned_vs_plain_512'],
+           'seconds_training': r['seconds_training'],
+           'mlp_forward_tflops': r['mlp_forward']['tflops']}
+    for k in ('training_step_ms', 'heldout_rms_gain_vs_table_sigma'):
+        if k in r:
+            out[k] = r[k]
+    return out
+
+
+def fp64_errors(W, catalog, got, bins):
+    """Error of the GPU multipoles against the oracle's float64 pipeline: the benchmark catalog
+    (512^3), and the cut-sky first-point configuration at 256^3 (its full catalog), as
+    max |P_gpu - P_fp64| / max |P_0 fp64| over the bins whose float32 and float64 mode counts agree."""
+    spectrum64, _ = oracle_pipeline(meshsize=W['meshsize'], catalog=catalog, dtype=np.float64)
+    ref = spectrum64()
+    same = np.asarray(bins.nmodes) == ref['nmodes']
+    out = {'c1_max_rel_vs_fp64_oracle': float(np.abs(got[:, same] - ref['num_raw'][:, same]).max()
+                                              / np.abs(ref['num_raw'][0][same]).max()),
+           'c1_bins_with_other_fp64_nmodes': int((~same).sum())}
+    out.update(cutsky_fp64_error(meshsize=256))
+    return out
+
+
+def cutsky_fp64_error(meshsize=256):
+    import torch
+    import jaxpower_b200 as jp
+    from jaxpower_b200.mock import cutsky_particles
+    from oracle.coords import Geometry
+    from oracle import paint as opaint
+    from oracle.spectrum import Bins, compute_mesh2_spectrum, fkp_particles
+    C = CUTSKY
+    data, randoms, wd, wr = cutsky_particles(ndata=C['ndata'], nrandoms=C['nrandoms'], seed=C['seed'])
+    attrs = jp.get_mesh_attrs(data, randoms, meshsize=meshsize, boxpad=C['boxpad'])
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': C['k_step']}, ells=C['ells'])
+    fkp = jp.FKPField(jp.ParticleField(data, wd, attrs=attrs), jp.ParticleField(randoms, wr, attrs=attrs))
+    mesh = fkp.paint(resampler=C['resampler'], interlacing=C['interlacing'], compensate=True, out='real')
+    got = np.array([p.num_raw for p in jp.compute_mesh2_spectrum(mesh, bin=b, los='firstpoint')])
+    host = [t.cpu().numpy() for t in (data, randoms, wd, wr)]
+    del mesh, fkp, data, randoms
+    torch.cuda.empty_cache()
+    geom = Geometry(attrs.meshsize, attrs.boxsize, attrs.boxcenter, dtype=np.float64)
+    pos, w, _ = fkp_particles(*host, dtype=np.float64)
+    ref = compute_mesh2_spectrum(opaint.paint(geom, pos, w, C['resampler'], C['interlacing'], True, 'real'),
+                                 Bins(geom, step=C['k_step'], ells=C['ells']), los='firstpoint')
+    same = np.asarray(b.nmodes) == ref['nmodes']
+    return {'c2_meshsize': meshsize,
+            'c2_max_rel_vs_fp64_oracle': float(np.abs(got[:, same] - ref['num_raw'][:, same]).max()
+                                               / np.abs(ref['num_raw'][0][same]).max()),
+            'c2_bins_with_other_fp64_nmodes': int((~same).sum())}
 
 
 def main():
@@ -806,8 +963,11 @@ def main():
     parser.add_argument('--steps', type=int, default=20)
     parser.add_argument('--warmup', type=int, default=5)
     parser.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    parser.add_argument('--cpu-meshsize', type=int, default=256)
-    parser.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline sample')
+    parser.add_argument('--ref-budget', type=float, default=240.,
+                        help='--impl reference: stop the timed oracle spectra after this many seconds (>= 1 step)')
+    parser.add_argument('--no-cpu', action='store_true', help='skip the CPU baseline and parity against the oracle')
+    parser.add_argument('--no-fp64', action='store_true', help='skip the float64-oracle errors')
+    parser.add_argument('--details', default='', help='write the full sub-reports (JSON) to this file')
     parser.add_argument('--no-e2e', action='store_true', help='skip the end-to-end (host buffers) measurement')
     parser.add_argument('--meshsize', type=int, default=0, help='smaller mesh of the same workload (profiling)')
     parser.add_argument('--no-batched', action='store_true', help='skip the batched-mocks measurement')

@@ -138,6 +138,15 @@ pk_status pk_interlace_compensate_batch(void *stream, const void *in, int nbatch
 /* Multiply a real array by scale (e.g. the C2R normalisation). */
 pk_status pk_scale_real(void *stream, float *mesh, int64_t size, float scale);
 
+/* One uniform [0, 1) float64 variate per particle id, d_out[i] = jax.random.uniform(
+ * fold_in(fold_in(key(seed), lo32(ids[i])), hi32(ids[i])), ()) with jax_enable_x64
+ * (Threefry-2x32, 20 rounds): the per-id draw of create_sharded_random((seed, ids))
+ * (mesh.py:237-329, _fold_in mesh.py:215-233) that split_particles (mesh.py:3160-3204)
+ * uses for disjoint random subsamples of the randoms in compute_fkp2_normalization(split=)
+ * (mesh2.py:543).  d_ids NULL: jax.random.uniform(key(seed), (n,)) over the whole array
+ * (partitionable Threefry layout, one device), the draw for an integer seed. */
+pk_status pk_uniform_ids(void *stream, uint64_t seed, const int64_t *d_ids, int64_t n, double *d_out);
+
 /* --------------------------------------------------------------- binning
  * Bins are the reference's BinMesh2SpectrumPoles (mesh2.py:25-119):
  * k edges edges[0..nedges-1] (float32-rounded, as jnp.digitize compares them),

@@ -12,7 +12,7 @@ first-point and end-point lines of sight, 'firstpoint' and 'local' theory, 'smoo
 """
 from . import resamplers
 from .mesh import (MeshAttrs, BaseMeshField, RealMeshField, ComplexMeshField, ParticleField, FKPField,
-                   get_mesh_attrs, next_fft_size, r2c, c2r, apply, read, paint)
+                   get_mesh_attrs, next_fft_size, r2c, c2r, apply, read, paint, split_particles)
 from .mesh2 import (BinMesh2SpectrumPoles, BinMesh2CorrelationPoles, compute_mesh2_spectrum,
                     compute_mesh2_correlation, compute_mesh2, compute_fkp2_normalization,
                     compute_fkp2_shotnoise, compute_box2_normalization, compute_normalization,

@@ -48,6 +48,7 @@ SIGNATURES = {
     'pk_interlace_compensate': [c_void_p, c_void_p, c_int, c_int32_p, c_int, c_int, c_int, c_float,
                                 c_void_p],
     'pk_scale_real': [c_void_p, c_void_p, c_int64, c_float],
+    'pk_uniform_ids': [c_void_p, ctypes.c_uint64, c_void_p, c_int64, c_void_p],
     'pk_bin_workspace_size': [c_int32_p, c_int, c_int, ctypes.POINTER(c_size_t)],
     'pk_bin_modes': [c_void_p, c_int32_p, c_float_p, c_void_p, c_int, c_float, c_int, c_void_p,
                      c_void_p, c_void_p, c_size_t],

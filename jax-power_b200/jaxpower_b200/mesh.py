@@ -27,7 +27,7 @@ import torch
 from . import _lib
 from . import resamplers
 
-__all__ = ['MeshAttrs', 'RealMeshField', 'ComplexMeshField', 'ParticleField', 'FKPField',
+__all__ = ['MeshAttrs', 'RealMeshField', 'ComplexMeshField', 'ParticleField', 'FKPField', 'split_particles',
            'get_mesh_attrs', 'next_fft_size', 'r2c', 'c2r', 'paint', 'read']
 
 
@@ -526,6 +526,71 @@ def paint(particles, *args, **kwargs):
 
 # ---------------------------------------------------------------------- particles
 
+def _same_order(value, *args, **kwargs):
+    return value
+
+
+def _uniform_per_particle(seed, size, device):
+    """Uniform [0, 1) float64 per particle for ``seed`` = int, (key, ids) or (key, 'index'), as
+    ``create_sharded_random(jax.random.uniform, seed, size)`` draws them with x64 on
+    (``mesh.py:237-329``), through ``pk_uniform_ids``."""
+    key, ids = seed if isinstance(seed, tuple) else (seed, None)
+    if key is None or not isinstance(key, (int, np.integer)):
+        raise NotImplementedError('split seeds must be an integer key, optionally with ids')
+    if isinstance(ids, str):
+        if ids != 'index':
+            raise ValueError('ids must be an array or \'index\'')
+        ids = torch.arange(size, dtype=torch.int64, device=device)
+    elif ids is not None:
+        ids = ids if isinstance(ids, torch.Tensor) else torch.as_tensor(np.asarray(ids))
+        ids = ids.to(device=device, dtype=torch.int64).reshape(-1).contiguous()
+        if ids.numel() != size:
+            raise ValueError('expected {} ids, got {}'.format(size, ids.numel()))
+    out = torch.empty(size, dtype=torch.float64, device=device)
+    _lib.call('pk_uniform_ids', _lib.stream_handle(), int(key) & 0xFFFFFFFFFFFFFFFF, _lib.ptr(ids), int(size),
+              _lib.ptr(out))
+    return out
+
+
+def split_particles(*particles, seed=0, fields=None, return_masks=False):
+    """Disjoint random subsamples for the normalisation (``split_particles``, ``mesh.py:3160-3204``).
+
+    Particles sharing a field id (``fields``; a ``None`` entry repeats the previous particles)
+    are split by one uniform draw per particle: subsample ``i`` of ``n`` keeps
+    ``i / n <= x < (i + 1) / n`` (its weights multiplied by the mask).  ``seed``: one per unique
+    field, each an integer or ``(integer, ids)`` with per-particle ids or ``'index'``.
+    """
+    if len(particles) == 1 and isinstance(particles[0], (tuple, list)):
+        particles = tuple(particles[0])
+    particles = list(particles)
+    fields = [0] if fields is None else list(fields)
+    for p in particles[len(fields):]:
+        fields.append(fields[-1] if p is None else fields[-1] + 1)
+    for i, (p, f) in enumerate(zip(particles, fields)):
+        if p is None:
+            particles[i] = particles[fields.index(f)]
+    unique = []
+    for f in fields:
+        if f not in unique:
+            unique.append(f)
+    seeds = seed if isinstance(seed, list) else [seed]
+    if len(seeds) != len(unique):
+        raise ValueError('provide as many seeds as unique fields')
+    out = [None] * len(particles) if return_masks else list(particles)
+    for f, sd in zip(unique, seeds):
+        idx = [i for i, ff in enumerate(fields) if ff == f]
+        first = particles[idx[0]]
+        x = _uniform_per_particle(sd, first.size, first.positions.device)
+        nsplits = len(idx)
+        for isplit, i in enumerate(idx):
+            mask = (x >= isplit * 1. / nsplits) & (x < (isplit + 1) * 1. / nsplits)
+            if return_masks:
+                out[i] = mask
+            else:
+                out[i] = particles[i].clone(weights=(particles[i].weights * mask).to(torch.float32))
+    return out
+
+
 class ParticleField:
     """Particles with weights (``mesh.py:2398-2670``).
 
@@ -545,7 +610,8 @@ class ParticleField:
         self.attrs = attrs
         self.extra = {k: torch.as_tensor(np.asarray(v) if not isinstance(v, torch.Tensor) else v).to(_device())
                       for k, v in (extra or {}).items()}
-        self.exchange_direct = self.exchange_inverse = None
+        # one GPU holds the whole catalog: particle-ordered arrays need no exchange
+        self.exchange_direct = self.exchange_inverse = _same_order
 
     @property
     def weights(self):

@@ -20,7 +20,7 @@ import torch
 
 from . import _lib
 from .mesh import (MeshAttrs, BaseMeshField, RealMeshField, ComplexMeshField, ParticleField, FKPField,
-                   _r2c, _c2r, _workspace, _device, _paint, get_mesh_attrs)
+                   _r2c, _c2r, _workspace, _device, _paint, get_mesh_attrs, split_particles)
 from .types import Mesh2SpectrumPole, Mesh2SpectrumPoles, Mesh2CorrelationPole, Mesh2CorrelationPoles, DeferredRows
 
 __all__ = ['BinMesh2SpectrumPoles', 'compute_mesh2_spectrum', 'compute_mesh2', 'compute_fkp2_normalization',
@@ -608,10 +608,33 @@ def compute_box2_normalization(*inputs, bin=None):
 
 
 def compute_fkp2_normalization(*fkps, bin=None, cellsize=10., split=None, fields=None, **kwargs):
-    """FKP normalisation (``mesh2.py:516-574``): alpha * sum(rho_d rho_r) / V_cell, CIC at ``cellsize``."""
-    if split is not None:
-        raise NotImplementedError('split normalisation (random subsampling) is not supported')
+    """FKP normalisation (``mesh2.py:516-574``): alpha * sum(rho_d rho_r) / V_cell, CIC at ``cellsize``.
+
+    With ``split`` (a seed as ``split_particles`` takes it), the two randoms fields are
+    disjoint random subsamples of the randoms instead (``mesh2.py:543-553``), alpha rescaled
+    by each subsample's share of the weights.
+    """
     kwargs.update(cellsize=cellsize)
+    if split is not None:
+
+        def randoms_of(f):
+            return f.randoms if isinstance(f, FKPField) else f
+
+        fkps, fields = _format_meshes(*fkps, fields=fields)
+        def wsum(p):
+            return float(p.weights.double().sum())
+
+        alpha = 1.
+        for f in fkps:
+            if isinstance(f, FKPField):
+                alpha *= wsum(f.data) / wsum(f.randoms)
+        randoms = split_particles(*[randoms_of(f) for f in fkps], seed=split, fields=fields)
+        for f, r in zip(fkps, randoms):
+            alpha *= wsum(randoms_of(f)) / wsum(r)
+        norm = alpha * compute_normalization(*randoms, **kwargs)
+        if bin is not None:
+            return [norm] * len(bin.ells)
+        return norm
     fkps, fields = _format_meshes(*fkps)
     if fields[1] == fields[0]:
         fkp = fkps[0]

@@ -20,6 +20,7 @@ from itertools import product
 
 import numpy as np
 
+from . import _native
 from .coords import Geometry, kcoords, r2c, c2r
 
 
@@ -76,7 +77,22 @@ def cell_index(u, order, shape):
     return base_index(u, order) % np.asarray(shape, dtype='i8')
 
 
-def paint_mesh(shape, u, weights, order, dtype=np.float32, accum=None):
+_NATIVE = None
+
+
+def _native_ok():
+    """True when the C restatement (``paint_c.c``) builds; the NumPy loops are the fallback."""
+    global _NATIVE
+    if _NATIVE is None:
+        try:
+            _native.load()
+            _NATIVE = True
+        except Exception:
+            _NATIVE = False
+    return _NATIVE
+
+
+def paint_mesh(shape, u, weights, order, dtype=np.float32, accum=None, native=True):
     """``resamplers.paint`` (``resamplers.py:66-97``) onto a zero mesh of ``shape``.
 
     ``u``: (N, 3) positions in cell units (already normalised), ``weights``: (N,).
@@ -85,6 +101,13 @@ def paint_mesh(shape, u, weights, order, dtype=np.float32, accum=None):
     ``accum='f64'`` with float32: the reference's float32 contributions ``w * ker``
     summed in float64 and rounded once to float32 (an order-independent sum).
     """
+    if native and np.dtype(dtype) == np.float64 and _native_ok():
+        return _native.paint(shape, u, weights, order, 'double')
+    if native and np.dtype(dtype) == np.float32 and _native_ok():
+        # the C restatement of the loops below (paint_c.c): same float32 arithmetic
+        if accum == 'f64':
+            return _native.paint(shape, u, weights, order, 'f64').astype(np.float32)
+        return _native.paint(shape, u, weights, order, 'serial')
     if accum == 'f64' and np.dtype(dtype) == np.float32:
         shape = tuple(int(s) for s in shape)
         u = np.asarray(u, dtype=np.float32)
@@ -231,10 +254,12 @@ def _sym(out, planes):
 
 
 def paint(geom, positions, weights=None, resampler='cic', interlacing=0, compensate=False,
-          out='real', shifts_only=False):
+          out='real', shifts_only=False, accum=None):
     """``ParticleField.paint`` → ``_paint`` (``mesh.py:2604-2754``).
 
     Returns a real mesh (out='real') or the Hermitian complex mesh (out='complex').
+    ``accum='f64'`` (float32 geometry): each shifted mesh is the float32 contributions
+    summed in float64 and rounded once, instead of the serial float32 scatter.
     """
     order = {'ngp': 1, 'cic': 2, 'tsc': 3, 'pcs': 4}[resampler] if isinstance(resampler, str) else int(resampler)
     dt = geom.dtype
@@ -247,7 +272,7 @@ def paint(geom, positions, weights=None, resampler='cic', interlacing=0, compens
     shape = geom.rshape
     interlacing = max(int(interlacing), 1)
     if interlacing == 1:
-        mesh = paint_mesh(shape, u, weights, order, dtype=dt)
+        mesh = paint_mesh(shape, u, weights, order, dtype=dt, accum=accum)
         if compensate:
             c = (r2c(geom, mesh) * compensation_kernel(geom, order)).astype(cdt)
             if out == 'real':
@@ -259,7 +284,7 @@ def paint(geom, positions, weights=None, resampler='cic', interlacing=0, compens
     acc = np.zeros(geom.cshape, dtype=cdt)
     for shift in interlacing_shifts(interlacing, dt):
         us = (u + dt.type(shift)).astype(dt)
-        mesh = paint_mesh(shape, us, weights, order, dtype=dt)
+        mesh = paint_mesh(shape, us, weights, order, dtype=dt, accum=accum)
         c = r2c(geom, mesh)
         ph = interlacing_phase(geom, shift, interlacing)
         acc = (acc + ((c * ph).astype(cdt) / dt.type(interlacing)).astype(cdt)).astype(cdt)

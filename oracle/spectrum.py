@@ -981,19 +981,45 @@ def fkp2_shotnoise(weights):
     return float(np.sum(w * w))
 
 
-def fkp2_normalization(geom, data_pos, data_w, rand_pos, rand_w, cellsize=10.):
+def fkp2_normalization(geom, data_pos, data_w, rand_pos, rand_w, cellsize=10., split=None):
     """``compute_fkp2_normalization`` auto case (``mesh2.py:516-574``, ``mesh.py:3002-3118``).
 
-    alpha * sum(rho_d * rho_r) / V_cell with CIC meshes at the given cellsize.
+    alpha * sum(rho_d * rho_r) / V_cell with CIC meshes at the given cellsize (None: the
+    geometry's own mesh).  ``split=(seed, ids)``: the randoms split in two disjoint halves by
+    one uniform per id (``split_particles``, ``mesh.py:3160-3204``), alpha^2 rescaled by
+    each half's weight share (``mesh2.py:543-553``), sum(rho_r0 * rho_r1) / V_cell.
     """
     dt = geom.dtype
     data_w = np.ones(len(data_pos), dt) if data_w is None else np.asarray(data_w, dt)
     rand_w = np.ones(len(rand_pos), dt) if rand_w is None else np.asarray(rand_w, dt)
     alpha = np.sum(data_w.astype('f8')) / np.sum(rand_w.astype('f8'))
-    g2 = norm_geometry(geom, cellsize)
-    rd = paint_field(g2, data_pos, data_w, resampler='cic', interlacing=0, compensate=False)
-    rr = paint_field(g2, rand_pos, rand_w, resampler='cic', interlacing=0, compensate=False)
-    return float(alpha * np.sum(rd.astype('f8') * rr.astype('f8')) / np.prod(g2.cellsize.astype('f8')))
+    g2 = geom if cellsize is None else norm_geometry(geom, cellsize)
+
+    def cic(pos, w):
+        return paint_field(g2, pos, w, resampler='cic', interlacing=0, compensate=False).astype('f8')
+
+    if split is not None:
+        m0, m1 = split_masks(split, len(rand_pos), nsplits=2)
+        w0, w1 = (rand_w * m0).astype(dt), (rand_w * m1).astype(dt)
+        total = np.sum(rand_w.astype('f8'))
+        alpha = alpha**2 * (total / np.sum(w0.astype('f8'))) * (total / np.sum(w1.astype('f8')))
+        return float(alpha * np.sum(cic(rand_pos, w0) * cic(rand_pos, w1)) / np.prod(g2.cellsize.astype('f8')))
+    return float(alpha * np.sum(cic(data_pos, data_w) * cic(rand_pos, rand_w)) / np.prod(g2.cellsize.astype('f8')))
+
+
+def split_masks(seed, size, nsplits=2):
+    """Masks of ``split_particles`` (``mesh.py:3160-3204``) for one field split ``nsplits`` ways:
+    x = jax.random.uniform per particle (``create_sharded_random``, ``mesh.py:237-329``, x64),
+    subsample i keeps i / n <= x < (i + 1) / n."""
+    from .threefry import seed_key, fold_in_index, uniform_per_key, uniform
+    key, ids = seed if isinstance(seed, tuple) else (seed, None)
+    if isinstance(ids, str) and ids == 'index':
+        ids = np.arange(size)
+    if ids is None:
+        x = uniform(seed_key(key), (size,), np.float64, partitionable=True)
+    else:
+        x = uniform_per_key(fold_in_index(seed_key(key), np.asarray(ids, dtype='i8')), 1, np.float64)[:, 0]
+    return [(x >= i * 1. / nsplits) & (x < (i + 1) * 1. / nsplits) for i in range(nsplits)]
 
 
 def norm_geometry(geom, cellsize=10.):

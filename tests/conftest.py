@@ -12,3 +12,5 @@ for path in (ROOT, os.path.join(ROOT, 'jax-power_b200')):
 def pytest_configure(config):
     config.addinivalue_line('markers', 'gpu: needs a CUDA device (B200) and the built library')
     config.addinivalue_line('markers', 'slow: CPU test that takes tens of seconds')
+    config.addinivalue_line('markers', 'fullsize: GPU parity test on a benchmark configuration at its full '
+                                       'size (512^3), with a CPU oracle run of a minute or two')

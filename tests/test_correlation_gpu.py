@@ -86,3 +86,27 @@ def test_firstpoint_correlation_matches_oracle(los, cross):
     scale = np.abs(ref['num_raw'][0]).max()
     for i, ell in enumerate((0, 2, 4)):
         assert np.allclose(got.get(ell).num_raw, ref['num_raw'][i], rtol=0, atol=2e-5 * scale), ell
+
+
+def test_correlation_ref_golden_gpu():
+    """tests/test_mesh2.py:1042-1046: value().std() of the correlation multipoles of the test_ref FKP
+    mesh (CIC, interlacing 3, compensate, 128^3, jaxdecomp layout), s step 4 cells, ells (0, 2, 4),
+    for los 'x', 'firstpoint' and 'endpoint'.  The goldens are x64; the GPU path is float32."""
+    import json
+    import os
+    import jaxpower_b200 as jp
+    from tests.golden.catalogs import uniform_particles
+    golden = json.load(open(os.path.join(os.path.dirname(__file__), 'golden', 'reference_goldens.json')))
+    g, gc = golden['spectrum_ref'], golden['correlation_ref']
+    attrs = jp.MeshAttrs(meshsize=g['meshsize'], boxsize=g['boxsize'], boxcenter=g['boxcenter'], fft_backend='jaxdecomp')
+    data = jp.ParticleField(uniform_particles(g['data_seed'], g['size'], g['boxsize'], g['boxcenter']).astype('f4'),
+                            attrs=attrs)
+    randoms = jp.ParticleField(uniform_particles(g['randoms_seed'], g['randoms_size'], g['boxsize'],
+                                                 g['boxcenter']).astype('f4'), attrs=attrs)
+    mesh = jp.FKPField(data, randoms).paint(resampler=g['resampler'], interlacing=g['interlacing'],
+                                            compensate=g['compensate'])
+    b = jp.BinMesh2CorrelationPoles(attrs, edges={'step': gc['edges_step_in_cellsize'] * float(attrs.cellsize.min())},
+                                    ells=tuple(gc['ells']))
+    for los, expected in gc['value_std'].items():
+        value = jp.compute_mesh2_correlation(mesh, bin=b, los=los).value()
+        assert np.isclose(value.std(), expected, rtol=3e-5, atol=0.), (los, value.std(), expected)

@@ -219,3 +219,43 @@ def test_fused_interlaced_binning_matches_stored_mesh(resampler, interlacing, co
     for ell in (0, 2, 4):
         scale = np.abs(stored.get(0).num_raw).max()
         assert np.allclose(fused.get(ell).num_raw, stored.get(ell).num_raw, rtol=0, atol=1e-6 * scale), ell
+
+
+def test_uniform_ids_match_oracle():
+    """pk_uniform_ids: the per-id uniforms of create_sharded_random((seed, ids)) (x64), and the
+    whole-array draw of an integer seed, bit for bit against the oracle's Threefry."""
+    from jaxpower_b200 import _lib
+    from oracle.threefry import seed_key, fold_in_index, uniform_per_key, uniform
+    ids = np.concatenate([np.arange(1000), [2**32 - 1, 2**32, 2**40 + 7, 2**62 + 3]]).astype('i8')
+    d_ids = torch.as_tensor(ids).cuda()
+    for seed in (42, 0, 2**33 + 5):
+        out = torch.empty(len(ids), dtype=torch.float64, device='cuda')
+        _lib.call('pk_uniform_ids', _lib.stream_handle(), seed, _lib.ptr(d_ids), len(ids), _lib.ptr(out))
+        ref = uniform_per_key(fold_in_index(seed_key(seed), ids), 1, np.float64)[:, 0]
+        assert np.array_equal(out.cpu().numpy(), ref), seed
+        _lib.call('pk_uniform_ids', _lib.stream_handle(), seed, None, len(ids), _lib.ptr(out))
+        assert np.array_equal(out.cpu().numpy(), uniform(seed_key(seed), (len(ids),), np.float64)), seed
+
+
+def test_fkp2_normalization_goldens_gpu():
+    """tests/test_mesh.py:278-281 on the GPU path: cellsize None, cellsize 10, split=(42, index)."""
+    jp = _jp()
+    g = GOLDEN['fkp2_normalization']
+    attrs = jp.MeshAttrs(meshsize=g['meshsize'], boxsize=g['boxsize'], boxcenter=g['boxcenter'])
+    data = jp.ParticleField(uniform_particles(g['data_seed'], g['size'], g['boxsize'], g['boxcenter']).astype('f4'),
+                            attrs=attrs)
+    randoms = jp.ParticleField(uniform_particles(g['randoms_seed'], g['size'], g['boxsize'],
+                                                 g['boxcenter']).astype('f4'), attrs=attrs)
+    fkp = jp.FKPField(data, randoms)
+    index = torch.arange(g['size'], device='cuda')
+    got = {'cellsize_none': jp.compute_fkp2_normalization(fkp, cellsize=None),
+           'cellsize_10': jp.compute_fkp2_normalization(fkp, cellsize=10.),
+           'cellsize_10_split': jp.compute_fkp2_normalization(fkp, cellsize=10., split=(g['split_seed'], index))}
+    for name, value in got.items():
+        # float32 positions and meshes against the x64 golden
+        assert np.isclose(value, g['norm'][name], rtol=1e-5, atol=0.), (name, value, g['norm'][name])
+    # the split halves are disjoint and cover the randoms
+    m0, m1 = jp.split_particles(randoms, None, seed=(g['split_seed'], index), return_masks=True)
+    assert not bool((m0 & m1).any()) and bool((m0 | m1).all())
+    halves = jp.split_particles(randoms, None, seed=(g['split_seed'], 'index'))
+    assert np.isclose(float(halves[0].sum() + halves[1].sum()), g['size'])
