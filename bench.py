@@ -943,7 +943,7 @@ def cutsky_fp64_error(meshsize=256):
     fkp = jp.FKPField(jp.ParticleField(data, wd, attrs=attrs), jp.ParticleField(randoms, wr, attrs=attrs))
     mesh = fkp.paint(resampler=C['resampler'], interlacing=C['interlacing'], compensate=True, out='real')
     got = np.array([p.num_raw for p in jp.compute_mesh2_spectrum(mesh, bin=b, los='firstpoint')])
-    host = [t.cpu().numpy() for t in (data, randoms, wd, wr)]
+    host = [t.cpu().numpy() for t in (data, wd, randoms, wr)]
     del mesh, fkp, data, randoms
     torch.cuda.empty_cache()
     geom = Geometry(attrs.meshsize, attrs.boxsize, attrs.boxcenter, dtype=np.float64)

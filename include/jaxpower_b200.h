@@ -297,6 +297,31 @@ pk_status pk_bin_global_interlaced(void *stream, const void *shifted, int nbatch
                                    int backend, int nells, const int32_t *ells, double *d_out,
                                    void *workspace, size_t workspace_bytes);
 
+/* Mode oversampling of BinMesh2SpectrumPoles (mode_oversampling = s > 0, mesh2.py:48-61,
+ * _bincount mesh.py:2876-2910): the reference bins the modes once per integer shift in
+ * [-s, s]^3 by |k + shift| (the shift added to each k coordinate in float32; Hermitian
+ * weights and the binned values of k unchanged) and averages the per-shift sums.  Each call
+ * below is one shift (kshift = the shift as float32), the counterpart of pk_bin_modes /
+ * pk_bin_mesh / pk_bin_global / pk_bin_firstpoint with the bin of |k + kshift|; with
+ * `accumulate` it adds into the outputs, so the caller sums the (2s+1)^3 calls and divides.
+ * Same workspaces as the unshifted entry points. */
+pk_status pk_bin_modes_shifted(void *stream, const int32_t meshsize[3], const float kfun[3], const float kshift[3],
+                               const float *d_edges, int nedges, float step, int backend, int accumulate,
+                               double *d_nmodes, double *d_ksum, void *workspace, size_t workspace_bytes);
+pk_status pk_bin_mesh_shifted(void *stream, const void *value, const int32_t meshsize[3], const float kfun[3],
+                              const float kshift[3], const float *d_edges, int nedges, float step, int backend,
+                              int remove_zero, int accumulate, double *d_out, void *workspace,
+                              size_t workspace_bytes);
+pk_status pk_bin_global_shifted(void *stream, const void *delta1, const void *delta2, const int32_t meshsize[3],
+                                const float kfun[3], const float kshift[3], const float los[3], const float *d_edges,
+                                int nedges, float step, int backend, int nells, const int32_t *ells, int accumulate,
+                                double *d_out, void *workspace, size_t workspace_bytes);
+pk_status pk_bin_firstpoint_shifted(void *stream, const void *a0, const void *b0, const void *f, int nterms,
+                                    const int32_t *term_ell, const int32_t *term_m, const int32_t meshsize[3],
+                                    const float kfun[3], const float kshift[3], const float *d_edges, int nedges,
+                                    float step, int backend, int nells, const int32_t *ells, int include_ell0,
+                                    int accumulate, double *d_out, void *workspace, size_t workspace_bytes);
+
 /* No counterpart in the reference.  pk_bin_global without a workspace argument, for
  * callers that cannot allocate device memory when they call (a host callback, or a
  * foreign runtime that owns the allocator): its scratch is a fixed 16 MiB static device

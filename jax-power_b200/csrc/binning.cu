@@ -35,7 +35,18 @@ struct BinGeom {
   float step;  // > 0: uniform edges
   int backend;
   int sep;     // 1: real-space separation grid (fftfreq * cellsize * n, unit weights)
+  // mode oversampling (mesh2.py:48-61): the bin of a mode is that of |k + kshift|, the
+  // shift added to each coordinate in float32 as the reference adds it; its value (mu,
+  // khat) still comes from k.  Only the chunk walk (bin_chunks_kernel) takes a shift.
+  int shifted;
+  float kshift[3];
 };
+
+// |k + kshift|^2 = ((0 + (kx + sx)^2) + (ky + sy)^2) + (kz + sz)^2 in float32 (mesh2.py:50).
+__device__ __forceinline__ float shifted_k2(const BinGeom &g, float kx, float ky, float kz) {
+  const float a = __fadd_rn(kx, g.kshift[0]), b = __fadd_rn(ky, g.kshift[1]), c = __fadd_rn(kz, g.kshift[2]);
+  return __fadd_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)), __fmul_rn(c, c));
+}
 
 // Hermitian weight of stored mode z: 'jax' 1 + (kz > 0); 'jaxdecomp' counts the
 // mirrored half of a full complex grid (self-conjugate planes once).
@@ -109,8 +120,14 @@ __device__ __forceinline__ int bin_from_k2(const float *__restrict__ thr, int ne
 // op(idx, i, j, z, kx, ky, kz, k2, w, v): values of stored mode (i, j, z), weight w.
 struct ModesOp {  // nmodes and sum of w |k| (|k| = sqrt_rn(k2), as the reference's float32 knorm)
   static constexpr int NV = 2;
-  __device__ void operator()(int64_t, int, int, int, float, float, float, float k2, float w,
+  int shifted = 0;  // mode oversampling: |k + kshift| instead
+  float kshift[3] = {0.f, 0.f, 0.f};
+  __device__ void operator()(int64_t, int, int, int, float kx, float ky, float kz, float k2, float w,
                              float v[NV]) const {
+    if (shifted) {
+      const float a = __fadd_rn(kx, kshift[0]), b = __fadd_rn(ky, kshift[1]), c = __fadd_rn(kz, kshift[2]);
+      k2 = __fadd_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)), __fmul_rn(c, c));
+    }
     v[0] = w;
     v[1] = __fmul_rn(__fsqrt_rn(k2), w);
   }
@@ -439,7 +456,7 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_chunks_kernel(BinGeom g, Op o
           kz2 = __fmul_rn(kz, kz);
         }
         const float k2 = __fadd_rn(kxy, kz2);
-        key = bin_from_k2(s.thr, g.nedges, e0, inv_step, k2);
+        key = bin_from_k2(s.thr, g.nedges, e0, inv_step, g.shifted ? shifted_k2(g, kx, ky, kz) : k2);
         op(row * g.d.nz + z, i, j, z, kx, ky, kz, k2, mode_weight(g, z), v);
       } else {
 #pragma unroll
@@ -1281,6 +1298,21 @@ static pk_status make_geom(const int32_t meshsize[3], const float kfun[3], int n
   g->step = step;
   g->backend = backend;
   g->sep = 0;
+  g->shifted = 0;
+  g->kshift[0] = g->kshift[1] = g->kshift[2] = 0.f;
+  return PK_OK;
+}
+
+static pk_status make_shifted_geom(const int32_t meshsize[3], const float kfun[3], const float kshift[3], int nedges,
+                                   float step, int backend, BinGeom *g) {
+  pk_status st = make_geom(meshsize, kfun, nedges, step, backend, g);
+  if (st) return st;
+  PK_REQUIRE(kshift, PK_ERR_INVALID, "kshift is NULL");
+  for (int a = 0; a < 3; ++a) {
+    PK_REQUIRE(isfinite(kshift[a]), PK_ERR_INVALID, "kshift must be finite");
+    g->kshift[a] = kshift[a];
+  }
+  g->shifted = 1;
   return PK_OK;
 }
 
@@ -1356,6 +1388,65 @@ extern "C" pk_status pk_bin_global_batch(void *stream, const void *delta1, const
                                          const float los[3], const float *d_edges, int nedges,
                                          float step, int backend, int nells, const int32_t *ells,
                                          double *d_out, void *workspace, size_t workspace_bytes);
+
+// ------------------------------------------------------------ mode oversampling
+// BinMesh2SpectrumPoles(mode_oversampling=s) (mesh2.py:48-61): every integer shift in
+// [-s, s]^3 bins the modes by |k + shift| (Hermitian weights and the binned values of k
+// itself unchanged); the operator averages the per-shift sums (mesh.py:2894-2895).  One call
+// per shift, each accumulating into d_out when `accumulate`; bins are found per mode (the
+// chunk walk), since |k + shift| is not monotone along a row.
+
+extern "C" pk_status pk_bin_modes_shifted(void *stream, const int32_t meshsize[3], const float kfun[3],
+                                          const float kshift[3], const float *d_edges, int nedges, float step,
+                                          int backend, int accumulate, double *d_nmodes, double *d_ksum,
+                                          void *workspace, size_t workspace_bytes) {
+  BinGeom g;
+  pk_status st = make_shifted_geom(meshsize, kfun, kshift, nedges, step, backend, &g);
+  if (st) return st;
+  PK_REQUIRE(d_edges && d_nmodes && d_ksum, PK_ERR_INVALID, "null pointer");
+  ModesOp op;
+  op.shifted = 1;
+  for (int a = 0; a < 3; ++a) op.kshift[a] = kshift[a];
+  return launch_bins<2>((cudaStream_t)stream, g, op, d_edges, false, accumulate, d_nmodes, d_ksum, workspace,
+                        workspace_bytes);
+}
+
+extern "C" pk_status pk_bin_mesh_shifted(void *stream, const void *value, const int32_t meshsize[3],
+                                         const float kfun[3], const float kshift[3], const float *d_edges,
+                                         int nedges, float step, int backend, int remove_zero, int accumulate,
+                                         double *d_out, void *workspace, size_t workspace_bytes) {
+  BinGeom g;
+  pk_status st = make_shifted_geom(meshsize, kfun, kshift, nedges, step, backend, &g);
+  if (st) return st;
+  PK_REQUIRE(value && d_edges && d_out, PK_ERR_INVALID, "null pointer");
+  MeshOp op;
+  op.v = (const float2 *)value;
+  op.remove_zero = remove_zero;
+  return launch_bins<2>((cudaStream_t)stream, g, op, d_edges, false, accumulate, d_out, nullptr, workspace,
+                        workspace_bytes);
+}
+
+extern "C" pk_status pk_bin_global_shifted(void *stream, const void *delta1, const void *delta2,
+                                           const int32_t meshsize[3], const float kfun[3], const float kshift[3],
+                                           const float los[3], const float *d_edges, int nedges, float step,
+                                           int backend, int nells, const int32_t *ells, int accumulate,
+                                           double *d_out, void *workspace, size_t workspace_bytes) {
+  BinGeom g;
+  pk_status st = make_shifted_geom(meshsize, kfun, kshift, nedges, step, backend, &g);
+  if (st) return st;
+  PK_REQUIRE(delta1 && d_edges && d_out && los && ells, PK_ERR_INVALID, "null pointer");
+  PK_REQUIRE(nells >= 1 && nells <= MAX_ELLS, PK_ERR_INVALID, "nells must be in 1..%d", MAX_ELLS);
+  for (int l = 0; l < nells; ++l)
+    PK_REQUIRE(ells[l] >= 0 && ells[l] <= 8, PK_ERR_INVALID, "ell must be in 0..8");
+  auto fill = [&](auto &op) {
+    op.d1 = (const float2 *)delta1;
+    op.d2 = (const float2 *)delta2;
+    for (int a = 0; a < 3; ++a) op.los[a] = los[a];
+    for (int l = 0; l < MAX_ELLS; ++l) op.ells[l] = l < nells ? ells[l] : 0;
+  };
+  return dispatch_nv<GlobalOp>(nells, fill, (cudaStream_t)stream, g, d_edges, false, accumulate, d_out,
+                               workspace, workspace_bytes);
+}
 
 extern "C" pk_status pk_bin_global(void *stream, const void *delta1, const void *delta2,
                                    const int32_t meshsize[3], const float kfun[3],
@@ -1764,6 +1855,43 @@ extern "C" pk_status pk_bin_firstpoint(void *stream, const void *a0, const void 
   };
   return dispatch_nv<FirstPointOp>(nells, fill, (cudaStream_t)stream, g, d_edges, false,
                                    accumulate, d_out, workspace, workspace_bytes);
+}
+
+extern "C" pk_status pk_bin_firstpoint_shifted(void *stream, const void *a0, const void *b0, const void *f,
+                                               int nterms, const int32_t *term_ell, const int32_t *term_m,
+                                               const int32_t meshsize[3], const float kfun[3],
+                                               const float kshift[3], const float *d_edges, int nedges, float step,
+                                               int backend, int nells, const int32_t *ells, int include_ell0,
+                                               int accumulate, double *d_out, void *workspace,
+                                               size_t workspace_bytes) {
+  BinGeom g;
+  pk_status st = make_shifted_geom(meshsize, kfun, kshift, nedges, step, backend, &g);
+  if (st) return st;
+  PK_REQUIRE(a0 && d_edges && d_out && ells, PK_ERR_INVALID, "null pointer");
+  PK_REQUIRE(nterms >= 0 && nterms <= MAX_FP_TERMS, PK_ERR_INVALID, "nterms must be in 0..%d",
+             MAX_FP_TERMS);
+  PK_REQUIRE(nterms == 0 || (f && term_ell && term_m), PK_ERR_INVALID, "null term arrays");
+  PK_REQUIRE(nells >= 1 && nells <= MAX_ELLS, PK_ERR_INVALID, "nells must be in 1..%d", MAX_ELLS);
+  for (int t = 0; t < nterms; ++t)
+    PK_REQUIRE(term_ell[t] >= 0 && term_ell[t] <= YLM_LMAX && term_m[t] >= -term_ell[t] &&
+                   term_m[t] <= term_ell[t],
+               PK_ERR_INVALID, "invalid (ell, m)");
+  const int64_t stride = g.d.ncomplex();
+  auto fill = [&](auto &op) {
+    op.a0 = (const float2 *)a0;
+    op.b0 = (const float2 *)b0;
+    op.f = (const float2 *)f;
+    op.fstride = stride;
+    op.nterms = nterms;
+    for (int t = 0; t < MAX_FP_TERMS; ++t) {
+      op.term_ell[t] = t < nterms ? term_ell[t] : -1;
+      op.term_m[t] = t < nterms ? term_m[t] : 0;
+    }
+    for (int l = 0; l < MAX_ELLS; ++l) op.ells[l] = l < nells ? ells[l] : 0;
+    op.include_ell0 = include_ell0;
+  };
+  return dispatch_nv<FirstPointOp>(nells, fill, (cudaStream_t)stream, g, d_edges, false, accumulate, d_out,
+                                   workspace, workspace_bytes);
 }
 
 // ------------------------------------------------------------ allocation-free variant

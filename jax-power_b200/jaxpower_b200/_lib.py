@@ -54,6 +54,15 @@ SIGNATURES = {
                      c_void_p, c_void_p, c_size_t],
     'pk_bin_mesh': [c_void_p, c_void_p, c_int32_p, c_float_p, c_void_p, c_int, c_float, c_int, c_int,
                     c_void_p, c_void_p, c_size_t],
+    'pk_bin_modes_shifted': [c_void_p, c_int32_p, c_float_p, c_float_p, c_void_p, c_int, c_float, c_int, c_int,
+                             c_void_p, c_void_p, c_void_p, c_size_t],
+    'pk_bin_mesh_shifted': [c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_void_p, c_int, c_float, c_int,
+                            c_int, c_int, c_void_p, c_void_p, c_size_t],
+    'pk_bin_global_shifted': [c_void_p, c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_float_p, c_void_p,
+                              c_int, c_float, c_int, c_int, c_int32_p, c_int, c_void_p, c_void_p, c_size_t],
+    'pk_bin_firstpoint_shifted': [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int32_p, c_int32_p, c_int32_p,
+                                  c_float_p, c_float_p, c_void_p, c_int, c_float, c_int, c_int, c_int32_p, c_int,
+                                  c_int, c_void_p, c_void_p, c_size_t],
     'pk_bin_global': [c_void_p, c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_void_p,
                       c_int, c_float, c_int, c_int, c_int32_p, c_void_p, c_void_p, c_size_t],
     'pk_bin_separation_workspace_size': [c_int32_p, c_int, c_int, ctypes.POINTER(c_size_t)],

@@ -177,6 +177,8 @@ class _Spectrum(torch.autograd.Function):
 
 def spectrum_value(mesh, attrs=None, bin=None, los='z'):
     """Differentiable multipoles ``num_raw`` (nells, nbins) float64 of ``compute_mesh2_spectrum``."""
+    from .mesh2 import _plain_bins
+    _plain_bins(bin, 'the differentiable spectrum')
     value = mesh.value if hasattr(mesh, 'value') else mesh
     attrs = attrs if attrs is not None else mesh.attrs
     return _Spectrum.apply(value, attrs, bin, los)

@@ -19,7 +19,7 @@ from . import _lib
 from . import resamplers
 from .autotune import best_tile_config, make_key
 from .mesh import _plan, _device, _workspace
-from .mesh2 import _los, _ell_factors, _fusable
+from .mesh2 import _los, _ell_factors, _fusable, _plain_bins
 
 __all__ = ['BatchedSpectra']
 
@@ -39,6 +39,7 @@ class BatchedSpectra:
 
     def __init__(self, attrs, bin, counts, resampler='tsc', interlacing=2, compensate=True, los='z',
                  tile_config=None, graph=True, weights=False):
+        _plain_bins(bin, 'BatchedSpectra')
         self.attrs, self.bin = attrs, bin
         self.order = resamplers.get_resampler(resampler).order
         self.interlacing = max(int(interlacing), 1)

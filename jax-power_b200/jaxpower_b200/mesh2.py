@@ -13,6 +13,7 @@ Mirrors ``jaxpower/mesh2.py``:
   ``compute_box2_normalization`` (``mesh2.py:508-621``).
 """
 import functools
+import itertools
 import math
 
 import numpy as np
@@ -27,6 +28,12 @@ __all__ = ['BinMesh2SpectrumPoles', 'compute_mesh2_spectrum', 'compute_mesh2', '
            'compute_fkp2_shotnoise', 'compute_box2_normalization', 'compute_normalization',
            'compute_box_normalization', 'compute_mesh2_spectrum_window', 'compute_mesh2_spectrum_mean',
            'compute_smooth2_spectrum_window']
+
+
+def _plain_bins(bin, what):
+    """Window, mean-spectrum, batched and adjoint paths bin each mode once: no mode oversampling."""
+    if getattr(bin, '_kshifts', None):
+        raise NotImplementedError('{} does not support mode_oversampling > 0'.format(what))
 
 
 def _format_ells(ells):
@@ -52,14 +59,22 @@ class BinMesh2SpectrumPoles:
     mattrs : MeshAttrs or mesh field
     edges : array, dict ('min', 'max', 'step') or None
     ells : int or tuple
-    mode_oversampling : only 0 is supported
+    mode_oversampling : int s >= 0; s > 0 bins the modes once per integer shift in [-s, s]^3
+        by |k + shift| (the shift added to each k coordinate as the reference adds it,
+        ``mesh2.py:48-61``) and averages: nmodes is the mean over the shifts, xavg the sum of
+        the per-shift sums of |k + shift| divided by that mean (the reference's expression),
+        and binned values the mean of the per-shift sums over nmodes (``mesh.py:2876-2910``).
     """
 
     def __init__(self, mattrs, edges=None, ells=0, mode_oversampling=0):
         if not isinstance(mattrs, MeshAttrs):
             mattrs = mattrs.attrs
-        if mode_oversampling:
-            raise NotImplementedError('mode_oversampling > 0 is not supported on the GPU path')
+        mode_oversampling = int(mode_oversampling)
+        if mode_oversampling < 0:
+            raise ValueError('mode_oversampling must be >= 0')
+        self.mode_oversampling = mode_oversampling
+        r = range(-mode_oversampling, mode_oversampling + 1)
+        self._kshifts = [tuple(float(v) for v in sh) for sh in itertools.product(r, r, r)] if mode_oversampling else []
         self.mattrs = mattrs
         self.ells = _format_ells(ells)
         vec0 = np.float32(mattrs.kfun.min())
@@ -83,9 +98,17 @@ class BinMesh2SpectrumPoles:
         nmodes = torch.empty(nbins, dtype=torch.float64, device=_device())
         ksum = torch.empty(nbins, dtype=torch.float64, device=_device())
         ws = self._workspace()
-        _lib.call('pk_bin_modes', _lib.stream_handle(), _lib.i32(mattrs.meshsize), _lib.f32(mattrs.kfun),
-                  _lib.ptr(self.d_edges), len(edges), self._step, mattrs.backend_code, _lib.ptr(nmodes),
-                  _lib.ptr(ksum), _lib.ptr(ws), ws.numel())
+        if self._kshifts:
+            for ish, sh in enumerate(self._kshifts):
+                _lib.call('pk_bin_modes_shifted', _lib.stream_handle(), _lib.i32(mattrs.meshsize),
+                          _lib.f32(mattrs.kfun), _lib.f32(sh), _lib.ptr(self.d_edges), len(edges), self._step,
+                          mattrs.backend_code, int(ish > 0), _lib.ptr(nmodes), _lib.ptr(ksum), _lib.ptr(ws),
+                          ws.numel())
+            nmodes /= len(self._kshifts)
+        else:
+            _lib.call('pk_bin_modes', _lib.stream_handle(), _lib.i32(mattrs.meshsize), _lib.f32(mattrs.kfun),
+                      _lib.ptr(self.d_edges), len(edges), self._step, mattrs.backend_code, _lib.ptr(nmodes),
+                      _lib.ptr(ksum), _lib.ptr(ws), ws.numel())
         self.nmodes = nmodes.cpu().numpy()
         with np.errstate(invalid='ignore', divide='ignore'):
             self.xavg = ksum.cpu().numpy() / self.nmodes
@@ -132,9 +155,17 @@ class BinMesh2SpectrumPoles:
         value = value.to(device=_device(), dtype=torch.complex64).contiguous()
         out = torch.empty(2 * self.nbins, dtype=torch.float64, device=value.device)
         ws = self._workspace()
-        _lib.call('pk_bin_mesh', _lib.stream_handle(), _lib.ptr(value), _lib.i32(self.mattrs.meshsize),
-                  _lib.f32(self.mattrs.kfun), _lib.ptr(self.d_edges), len(self._edges1d), self._step,
-                  self.mattrs.backend_code, int(bool(remove_zero)), _lib.ptr(out), _lib.ptr(ws), ws.numel())
+        if self._kshifts:
+            for ish, sh in enumerate(self._kshifts):
+                _lib.call('pk_bin_mesh_shifted', _lib.stream_handle(), _lib.ptr(value), _lib.i32(self.mattrs.meshsize),
+                          _lib.f32(self.mattrs.kfun), _lib.f32(sh), _lib.ptr(self.d_edges), len(self._edges1d),
+                          self._step, self.mattrs.backend_code, int(bool(remove_zero)), int(ish > 0), _lib.ptr(out),
+                          _lib.ptr(ws), ws.numel())
+            out /= len(self._kshifts)
+        else:
+            _lib.call('pk_bin_mesh', _lib.stream_handle(), _lib.ptr(value), _lib.i32(self.mattrs.meshsize),
+                      _lib.f32(self.mattrs.kfun), _lib.ptr(self.d_edges), len(self._edges1d), self._step,
+                      self.mattrs.backend_code, int(bool(remove_zero)), _lib.ptr(out), _lib.ptr(ws), ws.numel())
         out = out.cpu().numpy()
         return (out[:self.nbins] + 1j * out[self.nbins:]) / self.nmodes
 
@@ -440,11 +471,23 @@ def _spectrum_sums(mattrs, bin, los, rmesh=None, cmesh=None, cmesh2=None, rmesh2
             B0 = None
         A0 = A0.contiguous()
         terms = _firstpoint_terms(ells)
+        kshifts = getattr(bin, '_kshifts', [])
+
+        def bin_firstpoint(F, nt, t_ell, t_m, include_ell0):
+            if not kshifts:
+                _lib.call('pk_bin_firstpoint', stream, _lib.ptr(A0), _lib.ptr(B0), _lib.ptr(F), nt, t_ell, t_m,
+                          _lib.i32(meshsize), _lib.f32(mattrs.kfun), _lib.ptr(bin.d_edges), len(bin._edges1d),
+                          bin._step, mattrs.backend_code, len(ells), _lib.i32(ells), include_ell0, 1, _lib.ptr(raw),
+                          _lib.ptr(ws), ws.numel())
+                return
+            for sh in kshifts:  # mode oversampling: the per-shift sums, averaged below
+                _lib.call('pk_bin_firstpoint_shifted', stream, _lib.ptr(A0), _lib.ptr(B0), _lib.ptr(F), nt, t_ell, t_m,
+                          _lib.i32(meshsize), _lib.f32(mattrs.kfun), _lib.f32(sh), _lib.ptr(bin.d_edges),
+                          len(bin._edges1d), bin._step, mattrs.backend_code, len(ells), _lib.i32(ells), include_ell0,
+                          1, _lib.ptr(raw), _lib.ptr(ws), ws.numel())
+
         if not terms:
-            _lib.call('pk_bin_firstpoint', stream, _lib.ptr(A0), _lib.ptr(B0), None, 0, None, None,
-                      _lib.i32(meshsize), _lib.f32(mattrs.kfun), _lib.ptr(bin.d_edges), len(bin._edges1d),
-                      bin._step, mattrs.backend_code, len(ells), _lib.i32(ells), 1, 1, _lib.ptr(raw),
-                      _lib.ptr(ws), ws.numel())
+            bin_firstpoint(None, 0, None, None, 1)
         else:
             rho = rmesh.contiguous()
             offset = (mattrs.boxcenter - (mattrs.boxsize / np.float32(2.)).astype('f4')).astype('f4')
@@ -464,14 +507,13 @@ def _spectrum_sums(mattrs, bin, los, rmesh=None, cmesh=None, cmesh2=None, rmesh2
                           _lib.f32(offset), nt, _lib.i32(t_ell), _lib.i32(t_m), _lib.ptr(real))
                 F = _r2c(real[:nt], meshsize)
                 include_ell0 = int(ib == 0 and 0 in ells)  # ell = 0 rides on the first batch
-                _lib.call('pk_bin_firstpoint', stream, _lib.ptr(A0), _lib.ptr(B0), _lib.ptr(F), nt, _lib.i32(t_ell),
-                          _lib.i32(t_m), _lib.i32(meshsize), _lib.f32(mattrs.kfun), _lib.ptr(bin.d_edges),
-                          len(bin._edges1d), bin._step, mattrs.backend_code, len(ells), _lib.i32(ells),
-                          include_ell0, 1, _lib.ptr(raw), _lib.ptr(ws), ws.numel())
+                bin_firstpoint(F, nt, _lib.i32(t_ell), _lib.i32(t_m), include_ell0)
                 if keep is not None:
                     keep['F'].append((chunk, F))
                 del F
         raw = raw.reshape(len(ells), nbins)
+        if kshifts:
+            raw = raw / len(kshifts)
         if swap:  # conj: odd multipoles (imaginary parts) change sign
             sign = torch.tensor([-1. if ell % 2 else 1. for ell in ells], dtype=raw.dtype, device=raw.device)
             raw = raw * sign[:, None]
@@ -480,6 +522,14 @@ def _spectrum_sums(mattrs, bin, los, rmesh=None, cmesh=None, cmesh2=None, rmesh2
     d2 = None
     if cross:
         d2 = (cmesh2 if cmesh2 is not None else _r2c(rmesh2, meshsize)).contiguous()
+    kshifts = getattr(bin, '_kshifts', [])
+    if kshifts:  # mode oversampling: mean of the per-shift sums
+        for ish, sh in enumerate(kshifts):
+            _lib.call('pk_bin_global_shifted', stream, _lib.ptr(d1), _lib.ptr(d2), _lib.i32(meshsize),
+                      _lib.f32(mattrs.kfun), _lib.f32(sh), _lib.f32(vlos), _lib.ptr(bin.d_edges), len(bin._edges1d),
+                      bin._step, mattrs.backend_code, len(ells), _lib.i32(ells), int(ish > 0), _lib.ptr(raw),
+                      _lib.ptr(ws), ws.numel())
+        return raw.reshape(len(ells), nbins) / len(kshifts)
     _lib.call('pk_bin_global', stream, _lib.ptr(d1), _lib.ptr(d2), _lib.i32(meshsize), _lib.f32(mattrs.kfun),
               _lib.f32(vlos), _lib.ptr(bin.d_edges), len(bin._edges1d), bin._step, mattrs.backend_code,
               len(ells), _lib.i32(ells), _lib.ptr(raw), _lib.ptr(ws), ws.numel())
@@ -525,7 +575,7 @@ def compute_mesh2_spectrum(*meshes, bin=None, los='z'):
     ells = bin.ells
     nbins = bin.nbins
     lazy = getattr(meshes[0], 'lazy', None) if fields[1] == fields[0] else None
-    if lazy is not None and vlos is not None and _fusable(ells):
+    if lazy is not None and vlos is not None and _fusable(ells) and not getattr(bin, '_kshifts', []):
         raw = _interlaced_sums(mattrs, bin, vlos, *lazy)
     else:
         r1, c1 = _split(meshes[0])
@@ -754,6 +804,7 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     the 'local' theory line of sight through ``_local_smooth_window``, 'infinite' through
     ``_local_infinite_window``.  The 'jaxdecomp' backend raises ``NotImplementedError``.
     """
+    _plain_bins(bin, 'compute_mesh2_spectrum_window')
     from .types import WindowMatrix
     flags = tuple(flags)
     meshes, fields = _format_meshes(*meshes)
@@ -1854,6 +1905,7 @@ def compute_mesh2_spectrum_mean(*meshes, theory, bin=None, los='z'):
     line of sight takes theory multipoles (wide-angle order 0) through ``_firstpoint_mean``.
     The 'jaxdecomp' layout raises ``NotImplementedError``.
     """
+    _plain_bins(bin, 'compute_mesh2_spectrum_mean')
     meshes, fields = _format_meshes(*meshes)
     periodic = isinstance(meshes[0], MeshAttrs)
     if periodic:

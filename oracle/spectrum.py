@@ -19,6 +19,7 @@ reference's CPU bincount order); ``accum='f64'`` accumulates the same float32
 per-mode products in float64 (the accuracy the CUDA kernels are held to).
 """
 import math
+from itertools import product
 
 import numpy as np
 
@@ -30,7 +31,7 @@ from .ylm import get_ylm, legendre
 class Bins:
     """``BinMesh2SpectrumPoles(mattrs, edges={'step': step}, ells)`` restated."""
 
-    def __init__(self, geom, step=None, edges=None, ells=(0, 2, 4), kmin=0., kmax=None):
+    def __init__(self, geom, step=None, edges=None, ells=(0, 2, 4), kmin=0., kmax=None, mode_oversampling=0):
         dt = geom.dtype
         self.geom = geom
         self.ells = tuple(sorted((ells,) if np.ndim(ells) == 0 else ells))
@@ -42,12 +43,21 @@ class Bins:
         self.edges = np.asarray(edges, dtype='f8')
         self.edges_dtype = self.edges.astype(dt)
         self.wmodes = hermitian_weights(geom)
-        knorm = self.knorm()
-        self.ibin = np.searchsorted(self.edges_dtype, knorm.ravel(), side='right').reshape(knorm.shape)
         nb = len(self.edges) + 1
         w = self.wmodes.ravel()
-        self.nmodes = np.bincount(self.ibin.ravel(), weights=w, minlength=nb)[1:-1]
-        ksum = np.bincount(self.ibin.ravel(), weights=(knorm.ravel().astype('f8') * w), minlength=nb)[1:-1]
+        # mode oversampling (mesh2.py:48-61): one bin index per integer shift in [-s, s]^3 of the
+        # k coordinates, nmodes averaged over the shifts, xavg = summed sum(|k + shift| w) / nmodes
+        r = range(-int(mode_oversampling), int(mode_oversampling) + 1)
+        shifts = list(product(r, r, r)) if mode_oversampling else [(0, 0, 0)]
+        self.ibins, nmodes, ksum = [], 0., 0.
+        for shift in shifts:
+            knorm = self.knorm(shift if mode_oversampling else None)
+            ibin = np.searchsorted(self.edges_dtype, knorm.ravel(), side='right').reshape(knorm.shape)
+            self.ibins.append(ibin)
+            nmodes = nmodes + np.bincount(ibin.ravel(), weights=w, minlength=nb)[1:-1]
+            ksum = ksum + np.bincount(ibin.ravel(), weights=(knorm.ravel().astype('f8') * w), minlength=nb)[1:-1]
+        self.ibin = self.ibins[0]
+        self.nmodes = nmodes / len(shifts) if mode_oversampling else nmodes
         with np.errstate(invalid='ignore', divide='ignore'):
             self.xavg = ksum / self.nmodes
 
@@ -55,9 +65,11 @@ class Bins:
     def nbins(self):
         return len(self.edges) - 1
 
-    def knorm(self):
+    def knorm(self, shift=None):
         dt = self.geom.dtype
         kx, ky, kz = kcoords(self.geom)
+        if shift is not None:  # xx + ss in the mesh dtype (mesh2.py:50)
+            kx, ky, kz = [(kk + dt.type(ss)).astype(dt) for kk, ss in zip((kx, ky, kz), shift)]
         k2 = (((dt.type(0.) + kx * kx).astype(dt) + ky * ky).astype(dt) + kz * kz).astype(dt)
         return np.sqrt(k2).astype(dt)
 
@@ -70,11 +82,17 @@ class Bins:
         ib = self.ibin.ravel()
         if accum == 'f64':
             wv = value.ravel() * self.wmodes.ravel().astype(value.real.dtype)
-            if np.iscomplexobj(wv):
-                s = np.bincount(ib, weights=wv.real, minlength=nb) + 1j * np.bincount(ib, weights=wv.imag, minlength=nb)
-            else:
-                s = np.bincount(ib, weights=wv, minlength=nb)
-            return s[1:-1] / self.nmodes
+            s = 0.
+            for ibin in self.ibins:  # the mean over the oversampling shifts (mesh.py:2894-2895)
+                ib = ibin.ravel()
+                if np.iscomplexobj(wv):
+                    s = s + np.bincount(ib, weights=wv.real, minlength=nb) + 1j * np.bincount(ib, weights=wv.imag,
+                                                                                              minlength=nb)
+                else:
+                    s = s + np.bincount(ib, weights=wv, minlength=nb)
+            return s[1:-1] / len(self.ibins) / self.nmodes
+        if len(self.ibins) > 1:
+            raise NotImplementedError('float32 serial accumulation without mode oversampling only')
         dt = value.real.dtype
         wv = (value.ravel() * self.wmodes.ravel().astype(dt))
         if np.iscomplexobj(wv):

@@ -259,3 +259,32 @@ def test_fkp2_normalization_goldens_gpu():
     assert not bool((m0 & m1).any()) and bool((m0 | m1).all())
     halves = jp.split_particles(randoms, None, seed=(g['split_seed'], 'index'))
     assert np.isclose(float(halves[0].sum() + halves[1].sum()), g['size'])
+
+
+@pytest.mark.parametrize('los', ['z', (0.2, 0.3, 0.9327379053088815), 'firstpoint', 'endpoint'])
+def test_mode_oversampling_matches_oracle(los):
+    """BinMesh2SpectrumPoles(mode_oversampling=1) (mesh2.py:48-61): the modes binned once per
+    integer shift of the k coordinates in [-1, 1]^3 and averaged.  The box is small (10 Mpc/h)
+    so that unit shifts of k (in h/Mpc, as the reference adds them) keep modes in range."""
+    jp = _jp()
+    meshsize, boxsize, boxcenter = (16, 12, 20), np.array([10., 8., 12.]), (0. if los in ('z',) else 30.)
+    rng = np.random.default_rng(12)
+    value = rng.normal(size=meshsize).astype('f4')
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=boxcenter)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.4}, ells=(0, 2, 4), mode_oversampling=1)
+    geom = Geometry(meshsize, boxsize, boxcenter)
+    ob = Bins(geom, step=0.4, ells=(0, 2, 4), mode_oversampling=1)
+    assert np.allclose(b.nmodes, ob.nmodes, rtol=1e-12, atol=0.)
+    assert np.allclose(b.xavg, ob.xavg, rtol=1e-6, equal_nan=True)
+    mesh = jp.RealMeshField(torch.as_tensor(value).cuda(), attrs=attrs)
+    res = jp.compute_mesh2_spectrum(mesh, bin=b, los=los)
+    ref = ospectrum(value, ob, los=los)
+    scale = np.abs(ref['num_raw'][0]).max()
+    for i, ell in enumerate(ob.ells):
+        got = res.get(ell).num_raw
+        assert np.allclose(got, ref['num_raw'][i], rtol=0, atol=RTOL * scale), (ell, np.abs(got - ref['num_raw'][i]).max() / scale)
+    # the binning operator itself on a complex mesh
+    cvalue = np.fft.rfftn(value).astype('c8')
+    assert np.allclose(b(torch.as_tensor(cvalue)), ob(cvalue), rtol=1e-5, atol=1e-5 * np.abs(ob(cvalue)).max())
+    plain = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.4}, ells=(0, 2, 4))
+    assert plain.mode_oversampling == 0 and not np.allclose(plain.nmodes, b.nmodes)
