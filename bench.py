@@ -465,7 +465,7 @@ def run_cutsky(reps=3):
 
 
 def run_paint_only(meshsize=None, reps=3, config=4):
-    """Profiling aid: the benchmark catalog (generated at 512^3) painted with TSC and 3
+    """Profiling aid: the benchmark catalog (made at 512^3) painted with TSC and 3
     interlacing shifts at ``meshsize`` through pk_paint_batch with tile configuration ``config``,
     one warm-up and ``reps`` timed calls; nothing else is on the device meanwhile."""
     import torch
@@ -473,10 +473,7 @@ def run_paint_only(meshsize=None, reps=3, config=4):
     from jaxpower_b200.mesh import _paint_call
     from jaxpower_b200.mock import lognormal_particles, power_law_pk
     W = WORKLOAD
-    pos = lognormal_particles(jp.MeshAttrs(meshsize=W['meshsize'], boxsize=W['boxsize'], boxcenter=0.),
-                              power_law_pk(), W['nbar'], seed=W['seed']).contiguous()
-    torch.cuda.synchronize()
-    torch.cuda.empty_cache()
+    pos = torch.as_tensor(benchmark_catalog()).cuda()
     n = meshsize or W['meshsize']
     attrs = jp.MeshAttrs(meshsize=n, boxsize=W['boxsize'], boxcenter=0.)
     out = torch.empty((W['interlacing'], n, n, n), dtype=torch.float32, device='cuda')
@@ -977,6 +974,7 @@ def main():
                         help='only time the correction network forward pass (profiling aid)')
     parser.add_argument('--paint-only', action='store_true',
                         help='only paint the benchmark catalog (at --meshsize if given; profiling aid)')
+    parser.add_argument('--paint-config', type=int, default=4, help='tile configuration of --paint-only')
     parser.add_argument('--window-only', action='store_true',
                         help='only time window matrices (at --meshsize if given; profiling aid)')
     parser.add_argument('--cutsky-forward-only', action='store_true',
@@ -986,7 +984,7 @@ def main():
         print(json.dumps({'mlp_forward': run_mlp_forward()}), flush=True)
         return
     if args.paint_only:
-        print(json.dumps({'paint': run_paint_only(args.meshsize or None)}), flush=True)
+        print(json.dumps({'paint': run_paint_only(args.meshsize or None, config=args.paint_config)}), flush=True)
         return
     if args.window_only:
         print(json.dumps({'window': run_window_only(args.meshsize or None)}), flush=True)

@@ -463,10 +463,16 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_chunks_kernel(BinGeom g, Op o
         for (int c = 0; c < NV; ++c) v[c] = 0.f;
       }
       const int prev = __shfl_up_sync(0xffffffffu, key, 1);
-      if (!__all_sync(0xffffffffu, lane == 0 || prev != key)) {
+      const bool head = lane == 0 || prev != key;
+      if (!__all_sync(0xffffffffu, head)) {
+        // segmented inclusive scan over runs of equal keys: a lane adds only lanes of its own
+        // run (for monotone keys this is the same as comparing keys; with a k shift equal keys
+        // may recur after another run)
+        const unsigned heads = __ballot_sync(0xffffffffu, head);
+        const int first = 31 - __clz(heads & (lane == 31 ? 0xffffffffu : ((2u << lane) - 1u)));
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1) {
-          const bool ok = __shfl_up_sync(0xffffffffu, key, d) == key && lane >= d;
+          const bool ok = lane - d >= first;
 #pragma unroll
           for (int c = 0; c < NV; ++c) {
             const float t = __shfl_up_sync(0xffffffffu, v[c], d);
@@ -475,9 +481,20 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_chunks_kernel(BinGeom g, Op o
         }
       }
       const int next = __shfl_down_sync(0xffffffffu, key, 1);
-      if (valid && (lane == 31 || next != key) && key >= 1 && key <= nbins) {
+      const bool tail = valid && (lane == 31 || next != key) && key >= 1 && key <= nbins;
+      if (!g.shifted) {  // keys are non-decreasing along a row: the run tails have distinct bins
+        if (tail) {
 #pragma unroll
-        for (int c = 0; c < NV; ++c) my[(size_t)(key - 1) * NV + c] += (double)v[c];
+          for (int c = 0; c < NV; ++c) my[(size_t)(key - 1) * NV + c] += (double)v[c];
+        }
+      } else {  // |k + shift| is not monotone: two runs may share a bin, add them one at a time
+        for (unsigned tails = __ballot_sync(0xffffffffu, tail); tails; tails &= tails - 1) {
+          if (lane == __ffs(tails) - 1) {
+#pragma unroll
+            for (int c = 0; c < NV; ++c) my[(size_t)(key - 1) * NV + c] += (double)v[c];
+          }
+          __syncwarp();
+        }
       }
       __syncwarp();
     }

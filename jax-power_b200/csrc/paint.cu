@@ -18,6 +18,8 @@
 //      Each output cell is written exactly once; the mesh is never memset.
 // Tile shapes / CTA sizes are compile-time configurations chosen by the caller's
 // autotuner (pk_paint uses configuration 0).
+#include <algorithm>
+
 #include <cub/device/device_scan.cuh>
 #include <math.h>
 
@@ -28,22 +30,33 @@ namespace pk {
 constexpr int MAX_SHIFTS = 4;
 constexpr int MAX_ORDER = 4;
 constexpr float MAX_CELL_COORD = 4194304.f;  // 2^22 cells
-constexpr int NUM_TILE_CONFIGS = 8;
+constexpr int NUM_TILE_CONFIGS = 11;
 
 // Tile configurations: (cells along axes 0, 1, 2; threads per CTA; SWZ: shared-memory rows
-// swizzled, see paint_swizzle).  Configurations 4..7 are 0..3 with the swizzle.
+// swizzled, see paint_swizzle; ROWS36: the per-shift kernel paint_shift_tile_kernel, see
+// there).  Configurations 4..7 are 0..3 with the swizzle; 8 to 10 take the per-shift
+// kernel where the mesh allows it (last axis a multiple of 32, at least 64; the others a
+// multiple of 8), else the all-shifts kernel with the same tile.
 template <int C>
 struct TileConfig;
-template <>
-struct TileConfig<0> { static constexpr int T0 = 8, T1 = 16, T2 = 32, THREADS = 512; static constexpr bool SWZ = false; };
-template <>
-struct TileConfig<1> { static constexpr int T0 = 8, T1 = 16, T2 = 32, THREADS = 256; static constexpr bool SWZ = false; };
-template <>
-struct TileConfig<2> { static constexpr int T0 = 8, T1 = 8, T2 = 32, THREADS = 256; static constexpr bool SWZ = false; };
-template <>
-struct TileConfig<3> { static constexpr int T0 = 4, T1 = 16, T2 = 32, THREADS = 256; static constexpr bool SWZ = false; };
-template <int C>
-struct TileConfig : TileConfig<C - 4> { static constexpr bool SWZ = true; };
+#define PK_TILE_CONFIG(C, A, B, TH, S, R)                                                         \
+  template <>                                                                                     \
+  struct TileConfig<C> {                                                                          \
+    static constexpr int T0 = A, T1 = B, T2 = 32, THREADS = TH;                                   \
+    static constexpr bool SWZ = S, ROWS36 = R;                                                    \
+  };
+PK_TILE_CONFIG(0, 8, 16, 512, false, false)
+PK_TILE_CONFIG(1, 8, 16, 256, false, false)
+PK_TILE_CONFIG(2, 8, 8, 256, false, false)
+PK_TILE_CONFIG(3, 4, 16, 256, false, false)
+PK_TILE_CONFIG(4, 8, 16, 512, true, false)
+PK_TILE_CONFIG(5, 8, 16, 256, true, false)
+PK_TILE_CONFIG(6, 8, 8, 256, true, false)
+PK_TILE_CONFIG(7, 4, 16, 256, true, false)
+PK_TILE_CONFIG(8, 8, 16, 256, false, true)
+PK_TILE_CONFIG(9, 16, 16, 256, false, true)
+PK_TILE_CONFIG(10, 16, 16, 512, false, true)
+#undef PK_TILE_CONFIG
 
 static void tile_dims(int config, int t[3], int *threads) {
   switch (config) {
@@ -54,7 +67,7 @@ static void tile_dims(int config, int t[3], int *threads) {
     t[2] = TileConfig<C>::T2;          \
     *threads = TileConfig<C>::THREADS; \
     return;
-    PK_TC(0) PK_TC(1) PK_TC(2) PK_TC(3) PK_TC(4) PK_TC(5) PK_TC(6) PK_TC(7)
+    PK_TC(0) PK_TC(1) PK_TC(2) PK_TC(3) PK_TC(4) PK_TC(5) PK_TC(6) PK_TC(7) PK_TC(8) PK_TC(9) PK_TC(10)
 #undef PK_TC
   }
 }
@@ -209,82 +222,188 @@ __device__ __forceinline__ int warp_mock_of(const PaintGeom &g, int64_t base, in
   return base + lane < n ? mock_of(g, base + lane) : m0;
 }
 
-// Warp-aggregated tile counting / filling: a run of consecutive lanes that reach the same
-// tile makes one global atomic (catalogs are often sorted by cell, so neighbouring
-// particles usually share tiles); the lanes of a run then fill consecutive bucket slots.
+// The tiles reached by a warp's particles base .. base + 31 (those below `end`), every
+// interlacing shift at once: per axis the base cell c (floor for even orders, round-half-even
+// for odd ones, as the shift-0 stencil) and the reach [c - reach_lo, c + reach_hi] over all
+// shifts.  Each reached tile goes to `sink` as a run of consecutive lanes with the same tile
+// (catalogs are often sorted by cell, so neighbouring particles usually share tiles); the
+// run leader makes one atomic for the whole run and its lanes take consecutive slots.
+//   sink.particle(ok, wp)                  once per lane (validity, weight)
+//   sink.run(act, lead, leads, runlen, tile, u, wp)   once per candidate copy (warp-uniform)
+template <class Sink>
+__device__ __forceinline__ void warp_tile_runs(const PaintGeom &g, const float *__restrict__ pos,
+                                               const float *__restrict__ w, int64_t n, int64_t end,
+                                               int64_t base, Sink &sink) {
+  const int ns[3] = {g.d.n0, g.d.n1, g.d.n2};
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int64_t p = base + lane;
+  float u[3] = {0.f, 0.f, 0.f}, wp = 0.f;
+  bool ok = false;
+  const int mock = warp_mock_of(g, base, n);
+  if (p < end) ok = load_particle(g, pos, w, p, u, &wp) && isfinite(wp);
+  sink.particle(p < end, ok, wp);
+  int t[3][3], nt[3] = {0, 0, 0};
+  if (ok) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      nt[d] = span_tiles(base_index(g.order, u[d]), g.reach_lo, g.reach_hi, ns[d], g.tshift[d], g.nt[d], t[d]);
+  }
+  const int m0 = __reduce_max_sync(FULL, nt[0]), m1 = __reduce_max_sync(FULL, nt[1]),
+            m2 = __reduce_max_sync(FULL, nt[2]);
+  const int64_t mbase = (int64_t)mock * g.tiles_per_mock;
+  // the copies in (axis 0, 1, 2) order; loop bounds are warp-uniform
+#pragma unroll
+  for (int c0 = 0; c0 < 3; ++c0) {
+    if (c0 >= m0) break;
+#pragma unroll
+    for (int c1 = 0; c1 < 3; ++c1) {
+      if (c1 >= m1) break;
+#pragma unroll
+      for (int c2 = 0; c2 < 3; ++c2) {
+        if (c2 >= m2) break;
+        const bool act = c0 < nt[0] && c1 < nt[1] && c2 < nt[2];
+        int tile = -1;
+        if (act) tile = (int)(mbase + ((int64_t)t[0][c0] * g.nt[1] + t[1][c1]) * g.nt[2] + t[2][c2]);
+        // a run ends at the next leader or inactive lane
+        const int prev = __shfl_up_sync(FULL, tile, 1);
+        const bool lead = act && (lane == 0 || prev != tile);
+        const unsigned leads = __ballot_sync(FULL, lead);
+        const unsigned ends = leads | ~__ballot_sync(FULL, act);
+        const unsigned above = lane == 31 ? 0u : (ends & (0xffffffffu << (lane + 1)));
+        const unsigned runlen = (unsigned)((above ? __ffs(above) - 1 : 32) - lane);
+        sink.run(act, lead, leads, runlen, tile, u, wp);
+      }
+    }
+  }
+}
+
+// Slot of each lane of a run: the leader's atomic result, shuffled to its run, plus the
+// lane's place in the run.
+__device__ __forceinline__ unsigned run_slot(unsigned leader_base, unsigned leads) {
+  const int lane = threadIdx.x & 31;
+  const unsigned upto = leads & (lane == 31 ? 0xffffffffu : ((2u << lane) - 1u));
+  const int my_lead = upto ? 31 - __clz(upto) : lane;
+  return __shfl_sync(0xffffffffu, leader_base, my_lead) + (unsigned)(lane - my_lead);
+}
+
+// Global-memory counters (any number of tiles): bucket_kernel<false> counts the copies per
+// tile, bucket_kernel<true> fills the bucket from the scanned offsets.
+template <bool FILL>
+struct GlobalSink {
+  unsigned *counts;
+  const int *offsets;
+  unsigned *cursors;
+  float4 *bucket;
+  unsigned *wmax_bits;
+  int *status;
+  __device__ __forceinline__ void particle(bool in, bool ok, float wp) {
+    if (FILL) return;
+    if (in && !ok && status) atomicExch(status, 1);
+    const unsigned wb = __reduce_max_sync(0xffffffffu, ok ? __float_as_uint(fabsf(wp)) : 0u);
+    if ((threadIdx.x & 31) == 0 && wb) atomicMax(wmax_bits, wb);
+  }
+  __device__ __forceinline__ void run(bool act, bool lead, unsigned leads, unsigned runlen, int tile,
+                                      const float u[3], float wp) {
+    if (!FILL) {
+      if (lead) atomicAdd(counts + tile, runlen);
+      return;
+    }
+    unsigned b0 = 0;
+    if (lead) b0 = atomicAdd(cursors + tile, runlen);
+    const unsigned slot = run_slot(b0, leads);
+    if (act) bucket[(int64_t)offsets[tile] + slot] = make_float4(u[0], u[1], u[2], wp);
+  }
+};
+
 template <bool FILL>
 __global__ void bucket_kernel(PaintGeom g, const float *__restrict__ pos,
                               const float *__restrict__ w, int64_t n,
                               unsigned *__restrict__ counts, const int *__restrict__ offsets,
                               unsigned *__restrict__ cursors, float4 *__restrict__ bucket,
                               unsigned *__restrict__ wmax_bits, int *__restrict__ status) {
-  const int ns[3] = {g.d.n0, g.d.n1, g.d.n2};
-  const unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
+  GlobalSink<FILL> sink{counts, offsets, cursors, bucket, wmax_bits, status};
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t base = warp * 32; base < n; base += nwarps * 32) {
-    const int64_t p = base + lane;
-    float u[3] = {0.f, 0.f, 0.f}, wp = 0.f;
-    bool ok = false;
-    int mock = 0;
-    mock = warp_mock_of(g, base, n);
-    if (p < n) {
-      ok = load_particle(g, pos, w, p, u, &wp) && isfinite(wp);
-      if (!ok && !FILL && status) atomicExch(status, 1);
-    }
-    if (!FILL) {
-      const unsigned wb = __reduce_max_sync(FULL, ok ? __float_as_uint(fabsf(wp)) : 0u);
-      if (lane == 0 && wb) atomicMax(wmax_bits, wb);
-    }
-    int t[3][3], nt[3] = {0, 0, 0};
-    if (ok) {
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const int c = (int)floorf(u[d]);
-        nt[d] = span_tiles(c, g.reach_lo, g.reach_hi, ns[d], g.tshift[d], g.nt[d], t[d]);
-      }
-    }
-    const int m0 = __reduce_max_sync(FULL, nt[0]), m1 = __reduce_max_sync(FULL, nt[1]),
-              m2 = __reduce_max_sync(FULL, nt[2]);
-    const int64_t mbase = (int64_t)mock * g.tiles_per_mock;
-    // the copies in (axis 0, 1, 2) order; loop bounds are warp-uniform
-#pragma unroll
-    for (int c0 = 0; c0 < 3; ++c0) {
-      if (c0 >= m0) break;
-#pragma unroll
-      for (int c1 = 0; c1 < 3; ++c1) {
-        if (c1 >= m1) break;
-#pragma unroll
-        for (int c2 = 0; c2 < 3; ++c2) {
-          if (c2 >= m2) break;
-          const bool act = c0 < nt[0] && c1 < nt[1] && c2 < nt[2];
-          int tile = -1;
-          if (act) tile = (int)(mbase + ((int64_t)t[0][c0] * g.nt[1] + t[1][c1]) * g.nt[2] + t[2][c2]);
-          // runs of consecutive lanes with the same tile (catalogs sorted by cell give long
-          // runs) share one global atomic; a run ends at the next leader or inactive lane
-          const int prev = __shfl_up_sync(FULL, tile, 1);
-          const bool lead = act && (lane == 0 || prev != tile);
-          const unsigned leads = __ballot_sync(FULL, lead);
-          const unsigned ends = leads | ~__ballot_sync(FULL, act);
-          const unsigned above = lane == 31 ? 0u : (ends & (0xffffffffu << (lane + 1)));
-          const unsigned runlen = (unsigned)((above ? __ffs(above) - 1 : 32) - lane);
-          if (!FILL) {
-            if (lead) atomicAdd(counts + tile, runlen);
-          } else {
-            unsigned base0 = 0;
-            if (lead) base0 = atomicAdd(cursors + tile, runlen);
-            const unsigned upto = leads & (lane == 31 ? 0xffffffffu : ((2u << lane) - 1u));
-            const int my_lead = upto ? 31 - __clz(upto) : lane;
-            const unsigned base1 = __shfl_sync(FULL, base0, my_lead);
-            if (act)
-              bucket[(int64_t)offsets[tile] + base1 + (unsigned)(lane - my_lead)] =
-                  make_float4(u[0], u[1], u[2], wp);
-          }
-        }
-      }
-    }
+  for (int64_t base = warp * 32; base < n; base += nwarps * 32) warp_tile_runs(g, pos, w, n, n, base, sink);
+}
+
+// Shared-memory counters (tile index spaces up to HIST_MAX_TILES): each CTA takes a
+// contiguous range of particles and counts its copies per tile in shared memory; the
+// counts form a (CTA, tile) matrix whose column scan gives each CTA its own slots in every
+// tile.  The fill pass then assigns slots with shared-memory atomics only.  Versus global
+// counters this removes the global atomics (and their latency) from both passes.
+constexpr int HIST_THREADS = 1024;
+constexpr int HIST_MAX_TILES = 48 * 1024;  // 192 KB of counters per CTA
+
+template <bool PLACE>
+struct SharedSink {
+  unsigned *hist;  // shared counters (count) or cursors (place)
+  float4 *bucket;
+  unsigned wmax;   // per-lane max |w| bits (count)
+  int bad;
+  __device__ __forceinline__ void particle(bool in, bool ok, float wp) {
+    if (PLACE) return;
+    bad |= in && !ok;
+    if (ok) wmax = max(wmax, __float_as_uint(fabsf(wp)));
   }
+  __device__ __forceinline__ void run(bool act, bool lead, unsigned leads, unsigned runlen, int tile,
+                                      const float u[3], float wp) {
+    if (!PLACE) {
+      if (lead) atomicAdd(hist + tile, runlen);
+      return;
+    }
+    unsigned b0 = 0;
+    if (lead) b0 = atomicAdd(hist + tile, runlen);
+    const unsigned slot = run_slot(b0, leads);
+    if (act) bucket[slot] = make_float4(u[0], u[1], u[2], wp);
+  }
+};
+
+// colmat[c * ntiles + t]: the copies CTA c makes in tile t (count); after
+// bucket_colscan_kernel the first of them within tile t, to which PLACE adds tile_start[t].
+template <bool PLACE>
+__global__ void __launch_bounds__(HIST_THREADS) bucket_hist_kernel(
+    PaintGeom g, const float *__restrict__ pos, const float *__restrict__ w, int64_t n, int64_t chunk,
+    int ntiles, unsigned *__restrict__ colmat, const int *__restrict__ tile_start, float4 *__restrict__ bucket,
+    unsigned *__restrict__ wmax_bits, int *__restrict__ status) {
+  extern __shared__ unsigned hist[];
+  unsigned *row = colmat + (size_t)blockIdx.x * ntiles;
+  for (int t = threadIdx.x; t < ntiles; t += blockDim.x) hist[t] = PLACE ? (unsigned)tile_start[t] + row[t] : 0u;
+  __syncthreads();
+  SharedSink<PLACE> sink{hist, bucket, 0u, 0};
+  const int64_t begin = (int64_t)blockIdx.x * chunk;
+  const int64_t end = min(n, begin + chunk);
+  const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  for (int64_t base = begin + (int64_t)warp * 32; base < end; base += (int64_t)nwarps * 32)
+    warp_tile_runs(g, pos, w, n, end, base, sink);
+  if (!PLACE) {
+    const unsigned wb = __reduce_max_sync(0xffffffffu, sink.wmax);
+    if ((threadIdx.x & 31) == 0 && wb) atomicMax(wmax_bits, wb);
+    if (__any_sync(0xffffffffu, sink.bad) && (threadIdx.x & 31) == 0 && status) atomicExch(status, 1);
+  }
+  __syncthreads();
+  if (!PLACE)
+    for (int t = threadIdx.x; t < ntiles; t += blockDim.x) row[t] = hist[t];
+}
+
+// Exclusive scan of every tile's column of the (CTA, tile) count matrix, in place, and the
+// tile totals (totals[ntiles] = 0, so that the scan of totals ends on the bucket size).
+__global__ void bucket_colscan_kernel(unsigned *__restrict__ colmat, int nctas, int ntiles,
+                                      unsigned *__restrict__ totals) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t > ntiles) return;
+  if (t == ntiles) {
+    totals[t] = 0u;
+    return;
+  }
+  unsigned acc = 0u;
+  for (int c = 0; c < nctas; ++c) {
+    const unsigned v = colmat[(size_t)c * ntiles + t];
+    colmat[(size_t)c * ntiles + t] = acc;
+    acc += v;
+  }
+  totals[t] = acc;
 }
 
 // Fixed-point exponent e such that count * max|w| * 2^e < 2^62, count = the particles of the
@@ -307,6 +426,20 @@ __device__ __forceinline__ void fixed_scales(int e, float *s0, float *s1) {
   const int e0 = e > 120 ? 120 : e;
   *s0 = ldexpf(1.f, e0);
   *s1 = ldexpf(1.f, e - e0);
+}
+
+// A cell's 64-bit fixed-point sum (units 2^-e) to float32: one correctly rounded int64 ->
+// float32 conversion, then the exact power-of-two scaling 2^-e in two factors (inv from
+// fixed_inverse); only a result below float32's normal range rounds again.
+__device__ __forceinline__ void fixed_inverse(int e, float *inv0, float *inv1) {
+  const int e0 = e > 120 ? 120 : (e < -120 ? -120 : e);
+  *inv0 = ldexpf(1.f, -e0);
+  *inv1 = ldexpf(1.f, e0 - e);
+}
+
+__device__ __forceinline__ float fixed_to_float(unsigned lo, unsigned hi, float inv0, float inv1) {
+  const long long fx = (long long)(((unsigned long long)hi << 32) | lo);
+  return __fmul_rn(__fmul_rn(__ll2float_rn(fx), inv0), inv1);
 }
 
 // Shared-memory atomics on 32-bit shared-window addresses.
@@ -486,7 +619,8 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
       }
     }
     __syncthreads();
-    const double inv = ldexp(1.0, -fexp);
+    float inv0, inv1;
+    fixed_inverse(fexp, &inv0, &inv1);
     for (int s = 0; s < g.nshifts; ++s) {
       float *mesh = mock_out + (int64_t)s * g.d.nreal();
       const unsigned *alo = acc32 + s * CELLS;
@@ -502,10 +636,7 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
         const unsigned los4[4] = {lo4.x, lo4.y, lo4.z, lo4.w}, his4[4] = {hi4.x, hi4.y, hi4.z, hi4.w};
         float v[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {  // exact integer -> double, one rounding to float
-          const long long fx = (long long)(((unsigned long long)his4[j] << 32) | los4[j]);
-          v[j] = __double2float_rn((double)fx * inv);
-        }
+        for (int j = 0; j < 4; ++j) v[j] = fixed_to_float(los4[j], his4[j], inv0, inv1);
         if (vec) {
           if (x2 < g.d.n2) *reinterpret_cast<float4 *>(mesh + base) = make_float4(v[0], v[1], v[2], v[3]);
         } else {
@@ -532,6 +663,156 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
         }
       }
     }
+  }
+}
+
+// ------------------------------------------------------------ per-shift tile kernel
+// One CTA per (tile, interlacing shift), tiles T0 x T1 x 32, on meshes whose last axis is a
+// multiple of 4 and at least 64 cells (paint_run falls back to paint_tiles_kernel otherwise).
+//
+// Shared memory holds the low and the high words of the tile's 64-bit fixed-point cells in
+// rows of ROW_WORDS = 37 words: tile row (x, y) starts at word (x T1 + y) 37 and cell z sits
+// at + z + 4, so cells z in [-4, 33) are in the row and z in [33, 36) fall on the next row's
+// first words, which hold cells z < 0 of that row: cells outside the tile, never written out.
+// The odd row length spreads the cells of neighbouring rows over the banks.
+// A particle's ORDER stencil cells along z are therefore immediate offsets from one address,
+// with no per-cell test.  Stencil rows outside the tile go to a dummy row.
+//
+// Lane l of a warp takes entry l S + j of slot j (S = ceil(count / 32)): the lanes of one
+// atomic instruction sit S entries apart in the bucket, which keeps the catalog's order (often
+// spatial), so they rarely paint the same cell.  The three shifts of a tile are consecutive
+// CTAs (blockIdx.x = tile * nshifts + shift), so they read the tile's bucket from L2.  The
+// contributions, their fixed-point rounding and the write-out are those of
+// paint_tiles_kernel, so every configuration paints the same bits.
+constexpr int ROW_WORDS = 37;  // odd: the bank of a cell mixes its row (x, y) and z
+constexpr int ROW_ZOFF = 4;
+
+template <int T0, int T1>
+struct ShiftTileLayout {
+  static constexpr int ROWS = T0 * T1;
+  static constexpr int DUMMY_ROW = ROWS;  // stencil rows outside the tile
+  static constexpr int IDLE = (ROWS + 1) * ROW_WORDS + 4;  // 32 words: one per lane without a contribution
+  // low words rounded to 32 words so that a high word shares its low word's bank
+  static constexpr int LO_WORDS = (IDLE + 32 + 31) / 32 * 32;
+  static constexpr int ACC_WORDS = 2 * LO_WORDS;
+  static constexpr size_t BYTES = (size_t)ACC_WORDS * 4;
+};
+
+// First stencil cell of shift value `shift` along one axis (global index) and its kernel weights.
+template <int ORDER>
+__device__ __forceinline__ int stencil_axis(float u, float shift, float k[ORDER]) {
+  constexpr int OLO = -((ORDER - 1) / 2);
+  const float us = __fadd_rn(u, shift);
+  const float fi0 = (ORDER & 1) ? rintf(us) : floorf(us);
+  k[0] = bspline_at<ORDER, 0>(fabsf(__fsub_rn(__fadd_rn(fi0, (float)OLO), us)));
+  if (ORDER > 1) k[ORDER > 1 ? 1 : 0] = bspline_at<ORDER, 1>(fabsf(__fsub_rn(__fadd_rn(fi0, (float)(OLO + 1)), us)));
+  if (ORDER > 2) k[ORDER > 2 ? 2 : 0] = bspline_at<ORDER, 2>(fabsf(__fsub_rn(__fadd_rn(fi0, (float)(OLO + 2)), us)));
+  if (ORDER > 3) k[ORDER > 3 ? 3 : 0] = bspline_at<ORDER, 3>(fabsf(__fsub_rn(__fadd_rn(fi0, (float)(OLO + 3)), us)));
+  return (int)fi0 + OLO;
+}
+
+// First stencil cell along the last axis relative to the tile origin z0, as the representative
+// of (first - z0) mod n in [-8, n - 8) (n >= 64): for every bucket copy of the tile it lies in
+// [-4, 32], the periodic wrap included.
+__device__ __forceinline__ int tile_z(int first, int z0, int n) {
+  int r = wrapi(first - z0, n);
+  return r >= n - 8 ? r - n : r;
+}
+
+template <int ORDER, int T0, int T1, int SHIFT_TILE_THREADS>
+__global__ void __launch_bounds__(SHIFT_TILE_THREADS) paint_shift_tile_kernel(
+    PaintGeom g, const float4 *__restrict__ bucket, const int *__restrict__ offsets,
+    const unsigned *__restrict__ wmax_bits, float *__restrict__ out) {
+  using L = ShiftTileLayout<T0, T1>;
+  constexpr int T2 = 32;
+  constexpr int NWARPS = SHIFT_TILE_THREADS / 32;
+  constexpr int GROUPS = T0 * T1 * (T2 / 4);  // float4 groups of the write-out
+  extern __shared__ __align__(16) unsigned acc[];  // lo [LO_WORDS], hi [LO_WORDS]
+  const int64_t gtile = blockIdx.x / g.nshifts;
+  const int s = (int)(blockIdx.x % g.nshifts);
+  const int mock = (int)(gtile / g.tiles_per_mock);
+  const int tile = (int)(gtile % g.tiles_per_mock);
+  const int t2i = tile % g.nt[2];
+  const int t1i = (tile / g.nt[2]) % g.nt[1];
+  const int t0i = tile / (g.nt[2] * g.nt[1]);
+  const int x0 = t0i * T0, y0 = t1i * T1, z0 = t2i * T2;
+  const int begin = offsets[gtile];
+  const int count = offsets[gtile + 1] - begin;
+  float *mesh = out + ((int64_t)mock * g.nshifts + s) * g.d.nreal();
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+  if (count == 0) {
+    for (int i = tid; i < GROUPS; i += SHIFT_TILE_THREADS) {
+      const int row = i / (T2 / 4), z = (i % (T2 / 4)) * 4;
+      const int x = x0 + row / T1, y = y0 + row % T1;
+      if (x < g.d.n0 && y < g.d.n1 && z0 + z < g.d.n2)
+        *reinterpret_cast<float4 *>(mesh + ((int64_t)x * g.d.n1 + y) * g.d.n2 + z0 + z) = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    return;
+  }
+  {
+    uint4 *z4 = reinterpret_cast<uint4 *>(acc);
+    for (int i = tid; i < L::ACC_WORDS / 4; i += SHIFT_TILE_THREADS) z4[i] = make_uint4(0u, 0u, 0u, 0u);
+  }
+  __syncthreads();
+  const long long ncat = g.offsets ? (long long)(g.offsets[mock + 1] - g.offsets[mock]) : (long long)g.n;
+  const int fexp = fixed_exponent(*wmax_bits, ncat);
+  float fscale0, fscale1;
+  fixed_scales(fexp, &fscale0, &fscale1);
+  const float shift = g.shifts[s];
+  const unsigned acc_base = (unsigned)__cvta_generic_to_shared(acc);
+  constexpr unsigned HI = 4u * L::LO_WORDS;  // byte distance from a low word to its high word
+  const unsigned idle_addr = acc_base + 4u * (unsigned)(L::IDLE + lane);
+  const float4 *entries = bucket + begin;
+
+  const int S = (count + 31) >> 5;
+  for (int j = warp; j < S; j += NWARPS) {
+    const int e = lane * S + j;
+    const bool has = e < count;
+    const float4 q = entries[has ? e : 0];
+    const float wq = has ? __fmul_rn(__fmul_rn(q.w, fscale0), fscale1) : 0.f;
+    float kx[ORDER], ky[ORDER], kz[ORDER];
+    const int fx = stencil_axis<ORDER>(q.x, shift, kx);
+    const int fy = stencil_axis<ORDER>(q.y, shift, ky);
+    const int fz = stencil_axis<ORDER>(q.z, shift, kz);
+    const unsigned zbyte = 4u * (unsigned)(tile_z(fz, z0, g.d.n2) + ROW_ZOFF);
+    int xr[ORDER], yr[ORDER];
+#pragma unroll
+    for (int o = 0; o < ORDER; ++o) {
+      xr[o] = wrapi(fx + o, g.d.n0) - x0;
+      yr[o] = wrapi(fy + o, g.d.n1) - y0;
+    }
+#pragma unroll
+    for (int a = 0; a < ORDER; ++a) {
+#pragma unroll
+      for (int b = 0; b < ORDER; ++b) {
+        const float kab = __fmul_rn(kx[a], ky[b]);
+        const bool in = (unsigned)xr[a] < (unsigned)T0 && (unsigned)yr[b] < (unsigned)T1;
+        const int row = in ? xr[a] * T1 + yr[b] : L::DUMMY_ROW;
+        // a lane without an entry adds its zeros to its own idle word
+        const unsigned addr = has ? acc_base + 4u * (unsigned)(row * ROW_WORDS) + zbyte : idle_addr;
+        const unsigned step = has ? 4u : 0u;
+#pragma unroll
+        for (int c = 0; c < ORDER; ++c) {
+          const long long v = __float2ll_rn(__fmul_rn(wq, __fmul_rn(kab, kz[c])));  // (w * ker) 2^fexp
+          const unsigned lo = (unsigned)v;
+          const unsigned old = atom_add_shared(addr + step * c, lo);
+          red_add_shared(addr + step * c + HI, add_carry_hi(old, lo, (unsigned)(v >> 32)));
+        }
+      }
+    }
+  }
+  __syncthreads();
+  float inv0, inv1;
+  fixed_inverse(fexp, &inv0, &inv1);
+  for (int i = tid; i < GROUPS; i += SHIFT_TILE_THREADS) {
+    const int row = i / (T2 / 4), z = (i % (T2 / 4)) * 4;
+    const int x = x0 + row / T1, y = y0 + row % T1;
+    if (x >= g.d.n0 || y >= g.d.n1 || z0 + z >= g.d.n2) continue;
+    const unsigned *lo = acc + row * ROW_WORDS + ROW_ZOFF + z, *hi = lo + L::LO_WORDS;  // rows are not 16 B aligned
+    *reinterpret_cast<float4 *>(mesh + ((int64_t)x * g.d.n1 + y) * g.d.n2 + z0 + z) =
+        make_float4(fixed_to_float(lo[0], hi[0], inv0, inv1), fixed_to_float(lo[1], hi[1], inv0, inv1),
+                    fixed_to_float(lo[2], hi[2], inv0, inv1), fixed_to_float(lo[3], hi[3], inv0, inv1));
   }
 }
 
@@ -642,9 +923,11 @@ static bool fill_geom(const int32_t meshsize[3], const float boxsize[3], const f
     g->shifts[s] = s < nshifts ? shifts[s] : 0.f;
     shifted |= (s < nshifts && shifts[s] != 0.f);
   }
+  // stencil of shift s: base_index(u + s) + [-lo, hi], and base_index(u + s) is base_index(u)
+  // or base_index(u) + 1 for 0 <= s < 1: the bucket key is base_index(u), reach [-lo, hi + 1]
   const int hi = order - 1 - (order - 1) / 2;
   g->reach_lo = (order - 1) / 2;
-  g->reach_hi = hi + (order & 1 ? 1 : 0) + (shifted ? 1 : 0);
+  g->reach_hi = hi + (shifted ? 1 : 0);
   int threads;
   tile_dims(config, g->tile, &threads);
   for (int d = 0; d < 3; ++d) {
@@ -674,6 +957,11 @@ struct PaintLayout {
   size_t total;
 };
 
+constexpr int HIST_MAX_CTAS = 256;
+
+// The shared-histogram bucket passes serve tile index spaces that fit in shared memory.
+static bool hist_bucket(const PaintLayout &L) { return L.ntiles <= HIST_MAX_TILES; }
+
 static pk_status paint_layout(int64_t n, const PaintGeom &g, PaintLayout *L) {
   L->ntiles = g.tiles_per_mock * g.nmocks;
   PK_REQUIRE(L->ntiles < (int64_t)INT32_MAX / 2, PK_ERR_RANGE, "too many tiles (%lld)",
@@ -696,8 +984,54 @@ static pk_status paint_layout(int64_t n, const PaintGeom &g, PaintLayout *L) {
   c.take<unsigned>(4);              // wmax bits
   c.take<char>(L->scan_bytes);
   c.take<float4>(L->max_entries);
+  if (hist_bucket(*L)) c.take<unsigned>((size_t)HIST_MAX_CTAS * L->ntiles);  // (CTA, tile) counts
   L->total = align_up(c.used);
   return PK_OK;
+}
+
+// Configurations 8 to 10 take the per-shift tile kernel when the last axis is a multiple of 4
+// (float4 rows) and has at least 64 cells (unambiguous tile-relative z, see tile_z); on other
+// meshes they stand for configuration 4 (effective_config).
+static bool shift_tile_mesh(const int32_t meshsize[3]) { return meshsize[2] % 4 == 0 && meshsize[2] >= 64; }
+
+static bool shift_tile_config(int config) { return config >= 8 && config < NUM_TILE_CONFIGS; }
+
+static int effective_config(int config, const int32_t meshsize[3]) {
+  return (shift_tile_config(config) && meshsize && !shift_tile_mesh(meshsize)) ? 4 : config;
+}
+
+static bool shift_tile_eligible(int config, const PaintGeom &g) {
+  const int32_t ms[3] = {g.d.n0, g.d.n1, g.d.n2};
+  return shift_tile_config(config) && shift_tile_mesh(ms);
+}
+
+template <int ORDER, int C>
+static pk_status launch_shift_tile(cudaStream_t s, const PaintGeom &g, const float4 *bucket, const int *offsets,
+                                   const unsigned *wmax, float *out, int64_t ntiles) {
+  using TC = TileConfig<C>;
+  const size_t smem = ShiftTileLayout<TC::T0, TC::T1>::BYTES;
+  PK_REQUIRE(ntiles * g.nshifts < (int64_t)INT32_MAX, PK_ERR_RANGE, "too many tiles x shifts (%lld)",
+             (long long)(ntiles * g.nshifts));
+  auto kernel = paint_shift_tile_kernel<ORDER, TC::T0, TC::T1, TC::THREADS>;
+  PK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kernel<<<(unsigned)(ntiles * g.nshifts), TC::THREADS, smem, s>>>(g, bucket, offsets, wmax, out);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+static pk_status launch_shift_tiles(cudaStream_t s, const PaintGeom &g, int config, const float4 *bucket,
+                                    const int *offsets, const unsigned *wmax, float *out, int64_t ntiles) {
+  switch (config * 8 + g.order) {
+#define PK_ST_CASE(C, O) \
+  case C * 8 + O:        \
+    return launch_shift_tile<O, C>(s, g, bucket, offsets, wmax, out, ntiles);
+#define PK_ST_CFG(C) PK_ST_CASE(C, 1) PK_ST_CASE(C, 2) PK_ST_CASE(C, 3) PK_ST_CASE(C, 4)
+    PK_ST_CFG(8) PK_ST_CFG(9) PK_ST_CFG(10)
+#undef PK_ST_CFG
+#undef PK_ST_CASE
+  }
+  set_error("no per-shift tile kernel for order %d", g.order);
+  return PK_ERR_INVALID;
 }
 
 static pk_status paint_run(cudaStream_t s, const float *positions, const float *weights,
@@ -717,30 +1051,53 @@ static pk_status paint_run(cudaStream_t s, const float *positions, const float *
   void *scan_tmp = c.take<char>(L.scan_bytes);
   float4 *bucket = c.take<float4>(L.max_entries);
 
-  PK_CUDA(cudaMemsetAsync(counts, 0, (L.ntiles + 1) * sizeof(unsigned), s));
-  PK_CUDA(cudaMemsetAsync(cursors, 0, L.ntiles * sizeof(unsigned), s));
   PK_CUDA(cudaMemsetAsync(wmax, 0, 4 * sizeof(unsigned), s));
-  const int threads = 256;
-  const int64_t want = (n + threads - 1) / threads;
-  const int blocks = (int)(want < 64LL * sm_count() ? (want > 0 ? want : 1) : 64LL * sm_count());
-  if (n > 0) {
-    bucket_kernel<false><<<blocks, threads, 0, s>>>(g, positions, weights, n, counts, nullptr,
-                                                    nullptr, nullptr, wmax, d_status);
-    PK_LAUNCH_CHECK();
-  }
   size_t scan_bytes = L.scan_bytes;
-  PK_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, counts, offsets,
-                                        (int)(L.ntiles + 1), s));
-  if (n > 0) {
-    bucket_kernel<true><<<blocks, threads, 0, s>>>(g, positions, weights, n, nullptr, offsets,
-                                                   cursors, bucket, nullptr, nullptr);
+  if (hist_bucket(L)) {
+    // per-CTA shared counters over contiguous particle ranges, a column scan of the
+    // (CTA, tile) counts, the tile offsets, then the placement (shared-memory atomics only)
+    unsigned *colmat = c.take<unsigned>((size_t)HIST_MAX_CTAS * L.ntiles);
+    const int ntiles = (int)L.ntiles;
+    const int64_t want = (n + HIST_THREADS - 1) / HIST_THREADS;
+    const int nctas = (int)std::max<int64_t>(1, std::min<int64_t>(want, std::min(sm_count(), HIST_MAX_CTAS)));
+    const int64_t chunk = (n + nctas - 1) / nctas;
+    const size_t hsmem = (size_t)ntiles * sizeof(unsigned);
+    PK_CUDA(cudaFuncSetAttribute(bucket_hist_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
+    PK_CUDA(cudaFuncSetAttribute(bucket_hist_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hsmem));
+    bucket_hist_kernel<false><<<nctas, HIST_THREADS, hsmem, s>>>(g, positions, weights, n, chunk, ntiles, colmat,
+                                                                 nullptr, nullptr, wmax, d_status);
     PK_LAUNCH_CHECK();
+    bucket_colscan_kernel<<<(ntiles + 1 + 255) / 256, 256, 0, s>>>(colmat, nctas, ntiles, counts);
+    PK_LAUNCH_CHECK();
+    PK_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, counts, offsets, ntiles + 1, s));
+    bucket_hist_kernel<true><<<nctas, HIST_THREADS, hsmem, s>>>(g, positions, weights, n, chunk, ntiles, colmat,
+                                                                offsets, bucket, nullptr, nullptr);
+    PK_LAUNCH_CHECK();
+  } else {
+    PK_CUDA(cudaMemsetAsync(counts, 0, (L.ntiles + 1) * sizeof(unsigned), s));
+    PK_CUDA(cudaMemsetAsync(cursors, 0, L.ntiles * sizeof(unsigned), s));
+    const int threads = 256;
+    const int64_t want = (n + threads - 1) / threads;
+    const int blocks = (int)(want < 64LL * sm_count() ? (want > 0 ? want : 1) : 64LL * sm_count());
+    if (n > 0) {
+      bucket_kernel<false><<<blocks, threads, 0, s>>>(g, positions, weights, n, counts, nullptr,
+                                                      nullptr, nullptr, wmax, d_status);
+      PK_LAUNCH_CHECK();
+    }
+    PK_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, counts, offsets,
+                                          (int)(L.ntiles + 1), s));
+    if (n > 0) {
+      bucket_kernel<true><<<blocks, threads, 0, s>>>(g, positions, weights, n, nullptr, offsets,
+                                                     cursors, bucket, nullptr, nullptr);
+      PK_LAUNCH_CHECK();
+    }
   }
   int tdims[3], tthreads;
   tile_dims(config, tdims, &tthreads);
+  if (shift_tile_eligible(config, g)) return launch_shift_tiles(s, g, config, bucket, offsets, wmax, out, L.ntiles);
   // accumulators (lo, hi words per shift and cell) + 64 scratch words for masked-off lanes
   const size_t smem = ((size_t)g.nshifts * tdims[0] * tdims[1] * tdims[2] * 2 + 64) * sizeof(unsigned);
-  switch (config * 8 + g.order) {
+  switch (config * 8 + g.order) {  // all-shifts tile kernel
 #define PK_PAINT_CASE(C, O)                                                                    \
   case C * 8 + O:                                                                              \
     PK_CUDA(cudaFuncSetAttribute(paint_tiles_kernel<O, C>,                                     \
@@ -751,6 +1108,9 @@ static pk_status paint_run(cudaStream_t s, const float *positions, const float *
 #define PK_PAINT_CFG(C) PK_PAINT_CASE(C, 1) PK_PAINT_CASE(C, 2) PK_PAINT_CASE(C, 3) PK_PAINT_CASE(C, 4)
     PK_PAINT_CFG(0) PK_PAINT_CFG(1) PK_PAINT_CFG(2) PK_PAINT_CFG(3) PK_PAINT_CFG(4) PK_PAINT_CFG(5)
     PK_PAINT_CFG(6) PK_PAINT_CFG(7)
+    default:  // 8 to 10 took the per-shift kernel above or were mapped to 4 (effective_config)
+      set_error("no tile kernel for configuration %d", config);
+      return PK_ERR_INVALID;
 #undef PK_PAINT_CFG
 #undef PK_PAINT_CASE
   }
@@ -781,6 +1141,7 @@ extern "C" pk_status pk_paint_batch_workspace_size(int64_t n, int nmocks, const 
   // worst-case reach: any nonzero shift
   float shifts[MAX_SHIFTS] = {0.f, 0.5f, 0.5f, 0.5f};
   if (nshifts > MAX_SHIFTS) nshifts = MAX_SHIFTS;
+  if (meshsize) tile_config = effective_config(tile_config, meshsize);
   PaintGeom g;
   PK_REQUIRE(fill_geom(meshsize, box, cen, cell, order, nshifts, shifts, tile_config, nmocks, &g),
              PK_ERR_INVALID,
@@ -794,7 +1155,15 @@ extern "C" pk_status pk_paint_batch_workspace_size(int64_t n, int nmocks, const 
 
 extern "C" pk_status pk_paint_workspace_size(int64_t n, const int32_t meshsize[3], int order,
                                              int nshifts, size_t *bytes) {
-  return pk_paint_batch_workspace_size(n, 1, meshsize, order, nshifts, 0, bytes);
+  // the larger workspace of the two configurations pk_paint may pick
+  PK_REQUIRE(bytes, PK_ERR_INVALID, "bytes is NULL");
+  size_t a = 0, b = 0;
+  pk_status st = pk_paint_batch_workspace_size(n, 1, meshsize, order, nshifts, 4, &a);
+  if (st) return st;
+  st = pk_paint_batch_workspace_size(n, 1, meshsize, order, nshifts, 9, &b);
+  if (st) return st;
+  *bytes = a > b ? a : b;
+  return PK_OK;
 }
 
 extern "C" pk_status pk_paint_batch(void *stream, const float *positions, const float *weights,
@@ -811,6 +1180,7 @@ extern "C" pk_status pk_paint_batch(void *stream, const float *positions, const 
   float shifts[MAX_SHIFTS];
   pk_status st = make_shifts(interlacing, shift_begin, nshifts, shifts);
   if (st) return st;
+  if (meshsize) tile_config = effective_config(tile_config, meshsize);
   PaintGeom g;
   PK_REQUIRE(fill_geom(meshsize, boxsize, boxcenter, cellsize, order, nshifts, shifts, tile_config,
                        nmocks, &g),
@@ -827,8 +1197,11 @@ extern "C" pk_status pk_paint(void *stream, const float *positions, const float 
                               const float boxcenter[3], const float cellsize[3], int order,
                               int interlacing, int shift_begin, int nshifts, float *out,
                               void *workspace, size_t workspace_bytes, int *d_status) {
+  // the per-shift tile kernel (16 x 16 x 32 tiles) where the mesh allows it, else the swizzled
+  // all-shifts kernel
+  const int config = (meshsize && shift_tile_mesh(meshsize)) ? 9 : 4;
   return pk_paint_batch(stream, positions, weights, nullptr, n, 1, meshsize, boxsize, boxcenter,
-                        cellsize, order, interlacing, shift_begin, nshifts, 4, out, workspace,
+                        cellsize, order, interlacing, shift_begin, nshifts, config, out, workspace,
                         workspace_bytes, d_status);
 }
 

@@ -13,7 +13,7 @@ import threading
 
 import torch
 
-NUM_TILE_CONFIGS = 8
+NUM_TILE_CONFIGS = 11
 _cache = {}
 _lock = threading.Lock()
 

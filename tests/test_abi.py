@@ -58,9 +58,9 @@ def test_argument_errors_of_later_entries_without_gpu(lib):
     fake = ctypes.c_void_p(4096)
     nbytes = ctypes.c_size_t()
     ms = _lib.i32([32, 32, 32])
-    # paint tile configurations 0..7 (4..7 swizzled); 8 is out of range
-    assert lib.pk_paint_batch_workspace_size(1000, 1, ms, 3, 3, 7, ctypes.byref(nbytes)) == 0
-    assert lib.pk_paint_batch_workspace_size(1000, 1, ms, 3, 3, 8, ctypes.byref(nbytes)) == 1
+    # paint tile configurations 0..10 (4..7 swizzled, 8..10 the per-shift kernel); 11 is out of range
+    assert lib.pk_paint_batch_workspace_size(1000, 1, ms, 3, 3, 10, ctypes.byref(nbytes)) == 0
+    assert lib.pk_paint_batch_workspace_size(1000, 1, ms, 3, 3, 11, ctypes.byref(nbytes)) == 1
     geo = (ms, _lib.f32([100.] * 3), _lib.f32([0.] * 3), _lib.f32([100. / 32] * 3), 3)
     # interlaced read: interlacing out of range, NULL meshes
     assert lib.pk_read_interlaced(None, fake, 0, fake, None, 10, *geo, 1., fake, fake, 0) == 1

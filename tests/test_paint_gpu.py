@@ -28,7 +28,7 @@ def _catalog(n, boxsize, boxcenter, seed=0):
     return pos, w
 
 
-@pytest.mark.parametrize('meshsize', [(16, 16, 16), (17, 12, 10), (4, 4, 4), (32, 40, 36)])
+@pytest.mark.parametrize('meshsize', [(16, 16, 16), (17, 12, 10), (4, 4, 4), (32, 40, 36), (12, 20, 68)])
 @pytest.mark.parametrize('resampler', list(RESAMPLERS))
 def test_paint_shifts_match_oracle(meshsize, resampler):
     jp = _jp()
@@ -189,23 +189,30 @@ def test_read_interlaced_equals_per_shift_reads(order, interlacing):
     assert torch.equal(grad_a, grad_b)
 
 
-@pytest.mark.parametrize('resampler', ['cic', 'tsc', 'pcs'])
-def test_paint_same_bits_for_every_tile_config(resampler):
+# (64, 48, 32): last axis below 64, every configuration takes the all-shifts kernel;
+# (40, 36, 100) and (16, 24, 64): configurations 8 to 10 take the per-shift kernel (partial
+# tiles along every axis, an axis that is not a multiple of 8, dense tiles)
+@pytest.mark.parametrize('meshsize', [(64, 48, 32), (40, 36, 100), (16, 24, 64)])
+@pytest.mark.parametrize('resampler', ['ngp', 'cic', 'tsc', 'pcs'])
+def test_paint_same_bits_for_every_tile_config(resampler, meshsize):
     """The fixed-point scale depends on the catalog only: all tile configurations (and so the
     autotuner's choice) paint identical meshes."""
     from jaxpower_b200 import _lib as L
     from jaxpower_b200.mesh import _paint_call
+    from jaxpower_b200.autotune import NUM_TILE_CONFIGS
     jp = _jp()
     pos, w = _catalog(300000, [500.] * 3, [0.] * 3, seed=12)
     pos[:1000] = pos[0]  # a dense clump (many particles on a few cells)
+    pos[1000:1100] = [249.99998, -250., 0.5]  # on the box faces: periodic wrap of the stencil
     w[::7] *= -0.5
-    attrs = jp.MeshAttrs(meshsize=(64, 48, 32), boxsize=500.)
-    order = {'cic': 2, 'tsc': 3, 'pcs': 4}[resampler]
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=500.)
+    order = RESAMPLERS[resampler]
     pos = torch.as_tensor(pos).cuda()
     w = torch.as_tensor(w).cuda()
     status = torch.zeros(1, dtype=torch.int32, device='cuda')
     outs = []
-    for config in range(8):
+    assert NUM_TILE_CONFIGS == 11
+    for config in range(NUM_TILE_CONFIGS):
         out = torch.empty((3,) + tuple(attrs.meshsize), dtype=torch.float32, device='cuda')
         _paint_call(attrs, pos, w, order, 3, 0, 3, out, status, config)
         outs.append(out)
