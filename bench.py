@@ -49,16 +49,16 @@ CUTSKY = dict(workload='cut-sky FKP, first-point los, with adjoint: ~2e6 cluster
               k_step=0.005, ell_weights=(1., 0.5, 0.25), fd_step=0.25, seed=11)
 
 # kernel launches issued by each C-ABI entry point (ours, including CUB's scan kernels)
-LAUNCHES = {'pk_paint': 5, 'pk_paint_batch': 5, 'pk_interlace_compensate': 1, 'pk_interlace_compensate_batch': 1,
+LAUNCHES = {'pk_paint': 6, 'pk_paint_batch': 6, 'pk_interlace_compensate': 1, 'pk_interlace_compensate_batch': 1,
             'pk_bin_global': 2, 'pk_bin_global_batch': 2, 'pk_bin_global_interlaced': 2, 'pk_bin_firstpoint': 2,
             'pk_bin_modes': 2, 'pk_bin_mesh': 2, 'pk_scale_real': 1, 'pk_ylm_premultiply': 1, 'pk_read': 1,
             'pk_read_interlaced': 3}
 
 
-# ncu DRAM read + write of one pk_paint call of the 512^3 workload above (its count and fill
-# bucket passes and the tile pass, one-pass metrics on the full-size workload); the event
-# timing supplies the duration
-PAINT_TRAFFIC_512 = 59693824 + 15360 + 59910400 + 107581184 + 168319488 + 1547460096
+# ncu DRAM read + write of one pk_paint call of the 512^3 workload above (its counting, column
+# scan, placement and per-shift tile kernels, one-pass metrics on the full-size workload); the
+# event timing supplies the duration
+PAINT_TRAFFIC_512 = (60061696 + 256768) + (9705984 + 0) + (73378304 + 70682368) + (123594240 + 1547215360)
 
 C0 = dict(workload='uniform catalog 1e5 particles in a 1000 Mpc/h cube (seed 0), meshsize 64, CIC, no interlacing, '
                    'compensate, los z, ells (0,2,4), k step 0.01', nparticles=100000, meshsize=64, boxsize=1000.,
@@ -392,6 +392,57 @@ def run_batched(nmocks=256, fp64_subset=3, group=32):
                 tile_configs=sorted({bs.tile_config for _, bs in runners}), graphs=len(runners),
                 timing='plain: wall clock of the per-mock public-API loop (host-synchronous per mock); '
                        'batched: CUDA events around the graph replays (inputs resident)')
+
+
+def run_sharded_mocks(world, rank, barrier, max_over_ranks, group=32):
+    """The batched-mocks workload (256 lognormal mocks, mesh sizes 128 / 192 / 256) shared out over
+    the ranks: each rank measures its cost-balanced share (``sharding.ShardedMocks``: one
+    BatchedSpectra graph per mesh size and group) and one NCCL all_reduce assembles every mock's
+    multipoles on every rank.  Timed with CUDA events, max over ranks, the gather included; rank 0
+    checks two of its mocks against the plain public API."""
+    import torch
+    import jaxpower_b200 as jp
+    from jaxpower_b200.mock import lognormal_particles, power_law_pk
+    from jaxpower_b200.sharding import ShardedMocks, covariance
+    B = BATCHED
+    nmocks = B['nmocks']
+    rng = np.random.default_rng(B['seed'])
+    lo, hi = np.log(B['np_range'][0]), np.log(B['np_range'][1])
+    targets = np.exp(rng.uniform(lo, hi, nmocks))
+    sizes = rng.choice(B['meshsizes'], nmocks)
+    kmax = float(np.pi * min(B['meshsizes']) / B['boxsize'])
+    edges = np.arange(0., kmax, 0.005)
+    attrs_of = {n: jp.MeshAttrs(meshsize=n, boxsize=B['boxsize']) for n in B['meshsizes']}
+    bins = {n: jp.BinMesh2SpectrumPoles(attrs_of[n], edges=edges, ells=(0, 2, 4)) for n in B['meshsizes']}
+    sharded = ShardedMocks([(int(m), float(t)) for m, t in zip(sizes, targets)], bins, resampler='tsc',
+                           interlacing=B['interlacing'], group=group)
+    cats = {i: lognormal_particles(attrs_of[int(sizes[i])], power_law_pk(), targets[i] / B['boxsize']**3,
+                                   seed=1000 + i) for i in sharded.mine}  # this rank's mocks only
+    sharded(cats.__getitem__)  # warm-up: autotuning, graph capture
+    barrier()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    full = sharded(cats.__getitem__)
+    end.record()
+    torch.cuda.synchronize()
+    seconds = max_over_ranks(start.elapsed_time(end) / 1e3)
+    check = None
+    if rank == 0:
+        errs = []
+        for i in sharded.mine[:2]:
+            n = int(sizes[i])
+            mesh = jp.ParticleField(cats[i], attrs=attrs_of[n]).paint(resampler='tsc', interlacing=B['interlacing'],
+                                                                      compensate=True, out='complex')
+            ref = np.array([p.num_raw for p in jp.compute_mesh2_spectrum(mesh, bin=bins[n], los='z')])
+            got = full[i].cpu().numpy()
+            errs.append(float(np.abs(got - ref).max() / np.abs(ref[0]).max()))
+        check = max(errs) if errs else None
+    cov = covariance(full.cpu())
+    return dict(workload=B['workload'], nmocks=nmocks, ranks=world, mocks_per_s=nmocks / seconds, seconds=seconds,
+                mocks_on_rank0=len(sharded.mine), batches_on_rank0=len(sharded.batches),
+                max_rel_vs_public_api=check, covariance_shape=list(cov.shape),
+                timing='CUDA events around this rank\'s batched graphs and the NCCL all_reduce of all multipoles, '
+                       'max over ranks; catalogs resident')
 
 
 def run_cutsky(reps=3):
@@ -842,11 +893,14 @@ def run_ours(args):
                          'algorithmic_bytes': abytes,
                          'traffic': float(PAINT_TRAFFIC_512) if (dominant in ('pk_paint', 'pk_paint_batch')
                                                                  and W['meshsize'] == 512) else None,
-                         'traffic_source': 'ncu dram read+write of the pk_paint kernels, this workload at 512^3'},
+                         'traffic_source': 'ncu dram read+write of the pk_paint kernels (bucket count, column scan, '
+                                           'placement, per-shift tiles), this workload at 512^3'},
             'e2e': {'value': e2e_value, 'unit': 'spectra/s', 'h2d_bytes_per_step': int(npart * 12),
                     'd2h_bytes_per_step': int(len(W['ells']) * nbins * 8)},
             'gpu_launches': int(launches), 'stages': stage_report, 'clocks': clocks.summary()}
     details = {}
+    if (world > 1 or args.sharded_mocks) and not args.no_batched:  # every rank: mocks shared out, one gather
+        line['sharded_mocks'] = run_sharded_mocks(world, rank, barrier, max_over_ranks)
     if rank == 0 and world == 1 and not args.no_batched:
         details['batched'] = run_batched()
         line['batched'] = summary(details['batched'], ('plain_spectra_per_s', 'batched_spectra_per_s', 'speedup',
@@ -968,6 +1022,8 @@ def main():
     parser.add_argument('--no-e2e', action='store_true', help='skip the end-to-end (host buffers) measurement')
     parser.add_argument('--meshsize', type=int, default=0, help='smaller mesh of the same workload (profiling)')
     parser.add_argument('--no-batched', action='store_true', help='skip the batched-mocks measurement')
+    parser.add_argument('--sharded-mocks', action='store_true',
+                        help='run the sharded-mocks measurement (every N > 1 run does) also with one GPU')
     parser.add_argument('--no-learned', action='store_true', help='skip training / evaluating the learned correction')
     parser.add_argument('--no-cutsky', action='store_true', help='skip the cut-sky FKP first-point measurement')
     parser.add_argument('--mlp-forward-only', action='store_true',

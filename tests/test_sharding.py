@@ -63,3 +63,54 @@ def test_gather_two_ranks_gloo():
         assert np.array_equal(out[rank][1], expected)
         cov = np.cov(expected.reshape(len(costs), -1).T)
         assert np.allclose(out[rank][2], cov, rtol=1e-12, atol=1e-14)
+
+
+class _StubSpectra:
+    """Stands in for BatchedSpectra on CPU: multipoles made from each catalog's positions."""
+
+    def __init__(self, attrs, bin, counts, **kwargs):
+        self.counts, self.shape = counts, (len(bin.ells), bin.nbins)
+
+    def __call__(self, positions):
+        out, start = [], 0
+        for n in self.counts:
+            x = positions[start:start + n].double()
+            start += n
+            out.append(torch.full(self.shape, float(x.sum()) + n, dtype=torch.float64))
+        return torch.stack(out)
+
+
+class _StubBins:
+    ells, nbins, mattrs = (0, 2, 4), 5, None
+
+
+def _catalog(i):
+    return torch.as_tensor(np.random.default_rng(i).uniform(0., 1., (100 + 37 * i, 3)).astype('f4'))
+
+
+def _runner_worker(rank, world, port, specs, out):
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        from jaxpower_b200.sharding import measure_mocks
+        full, mine = measure_mocks(specs, _catalog, {128: _StubBins(), 192: _StubBins()}, group=3,
+                                   runner=_StubSpectra)
+        out[rank] = (mine, full.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_measure_mocks_two_ranks_gloo():
+    """The sharded mock runner's host path (partition, per-mesh-size batches of at most `group`
+    mocks, gather) with the batched spectra stubbed: every rank ends with every mock's row."""
+    specs = [(128 if i % 3 else 192, 100 + 37 * i) for i in range(11)]
+    with mp.Manager() as manager:
+        out = manager.dict()
+        mp.start_processes(_runner_worker, args=(2, _free_port(), specs, out), nprocs=2, join=True,
+                           start_method='spawn')
+        out = dict(out)
+    expected = np.stack([np.full((3, 5), float(_catalog(i).double().sum()) + specs[i][1]) for i in range(11)])
+    assert sorted(out[0][0] + out[1][0]) == list(range(11))
+    for rank in (0, 1):
+        assert np.array_equal(out[rank][1], expected)
