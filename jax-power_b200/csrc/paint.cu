@@ -683,7 +683,7 @@ __global__ void __launch_bounds__(TileConfig<CFG>::THREADS) paint_tiles_kernel(
 // first words, which hold cells z < 0 of that row: cells outside the tile, never written out.
 // The odd row length spreads the cells of neighbouring rows over the banks.
 // A particle's ORDER stencil cells along z are therefore immediate offsets from one address,
-// with no per-cell test.  Stencil rows outside the tile go to a dummy row.
+// with no per-cell test.
 //
 // Lane l of a warp takes entry l S + j of slot j (S = ceil(count / 32)): the lanes of one
 // atomic instruction sit S entries apart in the bucket, which keeps the catalog's order (often
@@ -697,8 +697,9 @@ constexpr int ROW_ZOFF = 4;
 template <int T0, int T1>
 struct ShiftTileLayout {
   static constexpr int ROWS = T0 * T1;
-  static constexpr int DUMMY_ROW = ROWS;  // stencil rows outside the tile
-  static constexpr int IDLE = (ROWS + 1) * ROW_WORDS + 4;  // 32 words: one per lane without a contribution
+  // 32 words after the rows (and the 3 words the last row's z >= 33 cells spill into): one per
+  // lane that adds nothing to the tile
+  static constexpr int IDLE = ROWS * ROW_WORDS + 4;
   // low words rounded to 32 words so that a high word shares its low word's bank
   static constexpr int LO_WORDS = (IDLE + 32 + 31) / 32 * 32;
   static constexpr int ACC_WORDS = 2 * LO_WORDS;
@@ -794,11 +795,11 @@ __global__ void __launch_bounds__(SHIFT_TILE_THREADS) paint_shift_tile_kernel(
 #pragma unroll
       for (int b = 0; b < ORDER; ++b) {
         const float kab = __fmul_rn(kx[a], ky[b]);
-        const bool in = (unsigned)xr[a] < (unsigned)T0 && (unsigned)yr[b] < (unsigned)T1;
-        const int row = in ? xr[a] * T1 + yr[b] : L::DUMMY_ROW;
-        // a lane without an entry adds its zeros to its own idle word
-        const unsigned addr = has ? acc_base + 4u * (unsigned)(row * ROW_WORDS) + zbyte : idle_addr;
-        const unsigned step = has ? 4u : 0u;
+        // a lane without an entry, or whose stencil row is outside the tile, adds to its own
+        // idle word (lanes of one instruction then never share a word there)
+        const bool in = has && (unsigned)xr[a] < (unsigned)T0 && (unsigned)yr[b] < (unsigned)T1;
+        const unsigned addr = in ? acc_base + 4u * (unsigned)((xr[a] * T1 + yr[b]) * ROW_WORDS) + zbyte : idle_addr;
+        const unsigned step = in ? 4u : 0u;
 #pragma unroll
         for (int c = 0; c < ORDER; ++c) {
           const long long v = __float2ll_rn(__fmul_rn(wq, __fmul_rn(kab, kz[c])));  // (w * ker) 2^fexp
