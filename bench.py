@@ -771,6 +771,63 @@ def run_learned(ntrain=None, nheld=None, steps=None):
                        'replays of 16 resident catalogs (+ the on-device correction), per spectrum')
 
 
+def run_mlp_training(batch=4096, rows=1 << 20, reps=20):
+    """The correction network's backward pass (tcgen05, and the mma.sync formulation beside it)
+    on ``rows`` random feature rows, and one whole training step (tcgen05 forward with stored
+    activations, loss, tcgen05 backward, CTA-order reduction, AdamW) at the training batch,
+    replayed from a CUDA graph.  Backward dense FLOPs per row: 2 x 128 x (16 + 2 x 128) for the
+    weight gradients and 2 x 128 x 2 x 128 for the activation gradients."""
+    import torch
+    from jaxpower_b200 import _lib
+    from jaxpower_b200.learned import MLP
+    mlp = MLP(seed=5)
+    gen = torch.Generator(device='cuda').manual_seed(6)
+    stream = _lib.stream_handle()
+
+    def events(fn, n):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(n):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / 1e3 / n
+
+    x = torch.randn((rows, 16), generator=gen, device='cuda')
+    dy = torch.randn(rows, generator=gen, device='cuda') / rows
+    y = torch.empty(rows, device='cuda')
+    z = torch.empty((3, rows, 128), device='cuda')
+    h = torch.empty_like(z)
+    grad = torch.empty(mlp.nparams, device='cuda')
+    nbytes = _lib.c_size_t()
+    _lib.call('pk_mlp_backward_workspace_size', rows, _lib.ctypes.byref(nbytes))
+    ws = torch.empty(nbytes.value, dtype=torch.uint8, device='cuda')
+    _lib.call('pk_mlp_forward_tc', stream, _lib.ptr(x), None, rows, _lib.ptr(mlp.wb), _lib.ptr(mlp.w), _lib.ptr(y),
+              _lib.ptr(z), _lib.ptr(h), _lib.ptr(mlp.status))
+    common = (_lib.ptr(x), None, rows, _lib.ptr(mlp.wb), _lib.ptr(z), _lib.ptr(h), _lib.ptr(dy), _lib.ptr(grad),
+              _lib.ptr(ws), ws.numel())
+    t_tc = events(lambda: _lib.call('pk_mlp_backward_tc', stream, *common, _lib.ptr(mlp.status)), reps)
+    t_mma = events(lambda: _lib.call('pk_mlp_backward', stream, *common), reps)
+    flops = 2. * 128 * (16 + 2 * 128) * rows + 2. * 128 * 2 * 128 * rows
+    del z, h, y, ws
+    # one training step at the training batch, as a graph of `reps` steps
+    n = 16 * batch
+    xt = torch.randn((n, 16), generator=gen, device='cuda')
+    target = torch.randn(n, generator=gen, device='cuda')
+    mlp.fit(xt, target, steps=16, batch=batch, graph=False)  # warm-up, kernel attributes
+    torch.cuda.synchronize()
+    step_s = mlp.fit_step_seconds(xt, target, batch=batch, steps=reps)
+    mlp.check()
+    return dict(backward_rows=rows, backward_seconds_tc=t_tc, backward_seconds_mma_sync=t_mma,
+                backward_tflops_tc=flops / t_tc / 1e12, backward_tflops_mma_sync=flops / t_mma / 1e12,
+                training_batch=batch, training_step_ms=step_s * 1e3,
+                timing='CUDA events; backward: %d calls on resident rows and stored activations; training step: '
+                       'a CUDA graph of %d steps (forward, loss, backward, reduction, AdamW) replayed' % (reps, reps))
+
+
 # ----------------------------------------------------------------------------- GPU arm
 
 def run_ours(args):
@@ -912,6 +969,7 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_learned:
         details['learned'] = run_learned()
         details['learned']['mlp_forward'] = run_mlp_forward()
+        details['learned']['mlp_training'] = run_mlp_training()
         line['learned'] = learned_summary(details['learned'])
     if rank == 0 and world == 1 and not args.no_cpu:
         # the CPU oracle on the same catalog: one whole 512^3 spectrum, timed (no scaling)
@@ -960,7 +1018,11 @@ def learned_summary(r):
            'batched_speedup_learned_vs_plain_512': r['batched_speedup_learned_vs_plain_512'],
            'seconds_training': r['seconds_training'],
            'mlp_forward_tflops': r['mlp_forward']['tflops']}
-    for k in ('training_step_ms', 'heldout_rms_gain_vs_table_sigma'):
+    if 'mlp_training' in r:
+        t = r['mlp_training']
+        out.update(mlp_backward_tflops_tc=t['backward_tflops_tc'], mlp_backward_tflops_mma_sync=t['backward_tflops_mma_sync'],
+                   training_step_ms=t['training_step_ms'])
+    for k in ('heldout_rms_gain_vs_table_sigma',):
         if k in r:
             out[k] = r[k]
     return out
@@ -1028,6 +1090,8 @@ def main():
     parser.add_argument('--no-cutsky', action='store_true', help='skip the cut-sky FKP first-point measurement')
     parser.add_argument('--mlp-forward-only', action='store_true',
                         help='only time the correction network forward pass (profiling aid)')
+    parser.add_argument('--mlp-training-only', action='store_true',
+                        help='only time the correction network backward pass and training step (profiling aid)')
     parser.add_argument('--paint-only', action='store_true',
                         help='only paint the benchmark catalog (at --meshsize if given; profiling aid)')
     parser.add_argument('--paint-config', type=int, default=4, help='tile configuration of --paint-only')
@@ -1038,6 +1102,9 @@ def main():
     args = parser.parse_args()
     if args.mlp_forward_only:
         print(json.dumps({'mlp_forward': run_mlp_forward()}), flush=True)
+        return
+    if args.mlp_training_only:
+        print(json.dumps({'mlp_training': run_mlp_training()}), flush=True)
         return
     if args.paint_only:
         print(json.dumps({'paint': run_paint_only(args.meshsize or None, config=args.paint_config)}), flush=True)

@@ -432,6 +432,17 @@ pk_status pk_mlp_backward(void *stream, const float *x, const int32_t *idx, int 
                           const float *z, const float *h, const float *dy, float *grad,
                           void *workspace, size_t workspace_bytes);
 
+/* pk_mlp_backward on the 5th-generation tensor cores: dW_l += bf16(dZ_l)^T bf16(A_l) and
+ * dH_{l-1} = bf16(dZ_l) bf16(W_l) as tcgen05.mma with float32 accumulators in tensor memory
+ * (the weight gradients accumulate there over a persistent CTA's 128-sample tiles), bias and
+ * output-layer gradients as fixed-order float32 column sums; one partial row per CTA (at most
+ * one CTA per SM), added in CTA order.  The same workspace as pk_mlp_backward suffices; wb, z
+ * and h 16-byte aligned.  d_status (device int, may be NULL) is set to 1 if a tensor-core step
+ * did not complete within its bounded wait. */
+pk_status pk_mlp_backward_tc(void *stream, const float *x, const int32_t *idx, int batch, const void *wb,
+                             const float *z, const float *h, const float *dy, float *grad,
+                             void *workspace, size_t workspace_bytes, int32_t *d_status);
+
 /* AdamW step on w (and its bf16 copy wb): t = *step (device int, steps taken so far),
  * learning rate lr_table[min(t, ntable - 1)] (device), bias corrections 1 - beta^(t + 1),
  * then *step = t + 1.  Everything the step depends on lives on the device, so a captured

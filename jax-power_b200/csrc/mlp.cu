@@ -6,9 +6,12 @@
 //     optionally keeps pre-activations Z and activations H for the backward pass;
 //   - mlp_mse_kernel: weighted mean-squared-error loss and its gradient dL/dy (one CTA,
 //     fixed-order reduction);
+//   - mlp_forward_tc_kernel: the forward pass on the tcgen05 tensor cores;
 //   - mlp_backward_kernel: per CTA (64 samples) the weight and bias gradients of its
 //     samples, written as one partial row; mlp_reduce_kernel adds the rows in CTA order,
 //     so the gradient is deterministic;
+//   - mlp_backward_tc_kernel: the backward pass on the tcgen05 tensor cores (weight gradients
+//     accumulated in tensor memory over a persistent CTA's tiles, one partial row per CTA);
 //   - mlp_adam_kernel: AdamW update of the FP32 master weights and their BF16 copies.
 // Samples can be gathered through an index array (minibatches of a resident training set).
 // There is no counterpart in the reference: the learned correction is a new method.
@@ -511,6 +514,235 @@ __global__ void __launch_bounds__(MLP_WARPS * 32) mlp_backward_kernel(
   }
 }
 
+// ------------------------------------------------------------- tcgen05 backward pass
+// The gradient on the 5th-generation tensor cores.  Per 128-sample tile, for l = 2, 1, 0:
+//   dZ_l = dH_l silu'(Z_l)            float, per thread: its sample and 32 columns
+//   dW_l += bf16(dZ_l)^T bf16(A_l)    M = 128 outputs, N = K_l inputs, reduction over samples
+//   dH_{l-1} = bf16(dZ_l) bf16(W_l)   M = 128 samples, N = 128 inputs, reduction over outputs
+// with dH_2 = dy W3[0].  The operands stay in the layouts of the forward pass: the sample-major
+// tiles (dZ, A_l: element (r, c) at canon_off(r, c, K)) and the weights (W_l[n][k] at
+// canon_off(n, k, 128)).  Where the contiguous index is the reduction index they are K-major
+// operands; where it is the output index they are MN-major operands (instruction descriptor
+// bits 15 / 16).  A no-swizzle MN-major core matrix is 8 contiguous MN elements x 8 K rows of
+// 16 bytes, with SBO the byte step between MN groups and LBO the step between K groups, so
+// the same bytes serve both ways and no transposed copy is made.  The dW_l accumulate in
+// tensor memory over all of the CTA's tiles (columns 128, 256, 384); dH_{l-1} goes to
+// columns 0-127.  The bias and W3 gradients are float column sums over the samples (the
+// oracle's float dZ), read from a float copy in shared memory in a fixed order while the MMAs
+// run.  One CTA per SM (all 512 tensor-memory columns, ~200 KB of shared memory), persistent;
+// each CTA writes one partial row, added in CTA order by mlp_reduce_kernel.  With every index
+// bound, a descriptor read with LBO and SBO exchanged would still stay inside the CTA's shared
+// memory (largest reach: 59.6 KB past the start of a 32 KB operand tile).
+constexpr int BT_THREADS = 512;  // 4 warpgroups; warpgroup q takes columns [32 q, 32 q + 32)
+constexpr int BT_TMEM_COLS = 512;
+constexpr uint32_t BT_DH = 0, BT_DW2 = 128, BT_DW1 = 256, BT_DW0 = 384;  // tensor-memory columns
+constexpr int BT_LDF = MLP_H + 1;  // float staging row: conflict-free column writes and reads
+constexpr int BT_DZ = 0;                              // bf16 dZ tile (128 x 128)
+constexpr int BT_A = BT_DZ + 32768;                   // bf16 A_l tile, l = 1, 2 (128 x 128)
+constexpr int BT_A0 = BT_A + 32768;                   // bf16 input features (128 x 16)
+constexpr int BT_W1 = BT_A0 + 4096;                   // bf16 W1 (128 x 128)
+constexpr int BT_W2 = BT_W1 + 32768;                  // bf16 W2
+constexpr int BT_F = BT_W2 + 32768;                   // float [128][129] staging
+constexpr int BT_PART = BT_F + TC_ROWS * BT_LDF * 4;  // float [4][128] partial column sums
+constexpr int BT_ACC = BT_PART + 4 * MLP_H * 4;       // float [4][128]: db0, db1, db2, dW3 row 0
+constexpr int BT_W3 = BT_ACC + 4 * MLP_H * 4;         // float [128]: bf16 W3 row 0
+constexpr int BT_DY = BT_W3 + MLP_H * 4;              // float [128]: the tile's dy
+constexpr int BT_BAR = BT_DY + TC_ROWS * 4;           // mbarrier, tensor-memory slot
+constexpr size_t BT_SMEM = BT_BAR + 16;
+static_assert(BT_SMEM <= 227 * 1024, "backward tile exceeds the shared memory of one CTA");
+static_assert(BT_BAR % 8 == 0, "mbarrier alignment");
+
+// sums[c] += the column sum of sF over the tile's 128 rows, in a fixed order (four sums of 32
+// rows, then theirs).  Every thread calls it; threads < 128 write sums after a barrier.
+__device__ __forceinline__ void bt_column_sums(const float (*sF)[BT_LDF], float (*sPart)[MLP_H], float *sums) {
+  const int c = threadIdx.x & (MLP_H - 1), rq = threadIdx.x >> 7;
+  float s = 0.f;
+#pragma unroll 8
+  for (int i = 0; i < 32; ++i) s += sF[rq * 32 + i][c];
+  sPart[rq][c] = s;
+  __syncthreads();
+  if (threadIdx.x < MLP_H) sums[c] += (sPart[0][c] + sPart[1][c]) + (sPart[2][c] + sPart[3][c]);
+}
+
+__global__ void __launch_bounds__(BT_THREADS, 1) mlp_backward_tc_kernel(
+    const float *__restrict__ X, const int *__restrict__ idx, int batch, const __nv_bfloat16 *__restrict__ Wb,
+    const float *__restrict__ Z, const float *__restrict__ H, const float *__restrict__ dy,
+    float *__restrict__ partial, int *__restrict__ status) {
+  extern __shared__ __align__(1024) unsigned char btsm[];
+  unsigned char *sDZ = btsm + BT_DZ, *sA = btsm + BT_A, *sA0 = btsm + BT_A0, *sW1 = btsm + BT_W1,
+                *sW2 = btsm + BT_W2;
+  float(*sF)[BT_LDF] = reinterpret_cast<float(*)[BT_LDF]>(btsm + BT_F);
+  float(*sPart)[MLP_H] = reinterpret_cast<float(*)[MLP_H]>(btsm + BT_PART);
+  float(*sAcc)[MLP_H] = reinterpret_cast<float(*)[MLP_H]>(btsm + BT_ACC);
+  float *sW3 = reinterpret_cast<float *>(btsm + BT_W3);
+  float *sDY = reinterpret_cast<float *>(btsm + BT_DY);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(btsm + BT_BAR);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(btsm + BT_BAR + 8);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int r = tid & (TC_ROWS - 1), q = tid >> 7, c0 = 32 * q;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(BT_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  load_canon(sW1, Wb + OFF_W1, MLP_H, MLP_H, MLP_H);
+  load_canon(sW2, Wb + OFF_W2, MLP_H, MLP_H, MLP_H);
+  for (int i = tid; i < MLP_H; i += BT_THREADS) sW3[i] = __bfloat162float(Wb[OFF_W3 + i]);
+  for (int i = tid; i < 4 * MLP_H; i += BT_THREADS) (&sAcc[0][0])[i] = 0.f;
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+  const int ntiles = (batch + TC_ROWS - 1) / TC_ROWS;
+  float db3 = 0.f;  // thread 0
+  bool ok = true, first = true;
+  uint32_t phase = 0;
+  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const int row = tile * TC_ROWS + r;
+    const bool in = row < batch;
+    const int64_t rowc = in ? row : 0;
+    const float g = in ? dy[row] : 0.f;
+    if (q == 0) sDY[r] = g;
+    float dh[32];
+    {  // output layer: dH_2 = dy W3[0]; dW3[0] from the column sums of dy bf16(H_2)
+      const float *hr = H + ((int64_t)2 * batch + rowc) * MLP_H + c0;
+#pragma unroll
+      for (int c = 0; c < 32; c += 4) {
+        const float4 hv = in ? *reinterpret_cast<const float4 *>(hr + c) : make_float4(0.f, 0.f, 0.f, 0.f);
+        sF[r][c0 + c] = g * __bfloat162float(__float2bfloat16_rn(hv.x));
+        sF[r][c0 + c + 1] = g * __bfloat162float(__float2bfloat16_rn(hv.y));
+        sF[r][c0 + c + 2] = g * __bfloat162float(__float2bfloat16_rn(hv.z));
+        sF[r][c0 + c + 3] = g * __bfloat162float(__float2bfloat16_rn(hv.w));
+      }
+#pragma unroll
+      for (int c = 0; c < 32; ++c) dh[c] = g * sW3[c0 + c];
+    }
+    __syncthreads();
+    bt_column_sums(sF, sPart, sAcc[3]);
+    if (tid == 0)
+      for (int i = 0; i < TC_ROWS; ++i) db3 += sDY[i];
+    __syncthreads();
+    for (int l = 2; l >= 0 && ok; --l) {
+      if (l < 2) {
+        uint32_t v[32];
+        tmem_ld32(lane_addr + BT_DH + (uint32_t)c0, v);
+#pragma unroll
+        for (int c = 0; c < 32; ++c) dh[c] = __uint_as_float(v[c]);
+      }
+      {  // dZ_l: float copy for the bias sums, bf16 tile for the MMAs
+        const float *zr = Z + ((int64_t)l * batch + rowc) * MLP_H + c0;
+#pragma unroll
+        for (int c = 0; c < 32; c += 8) {
+          unsigned pk[4];
+#pragma unroll
+          for (int u = 0; u < 8; u += 4) {
+            const float4 zv = in ? *reinterpret_cast<const float4 *>(zr + c + u) : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float zz[4] = {zv.x, zv.y, zv.z, zv.w};
+            float d[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const float s = sigmoid(zz[e]);
+              d[e] = in ? dh[c + u + e] * (s * (1.f + zz[e] * (1.f - s))) : 0.f;
+              sF[r][c0 + c + u + e] = d[e];
+            }
+            pk[u / 2] = pack_raw(__float2bfloat16_rn(d[0]), __float2bfloat16_rn(d[1]));
+            pk[u / 2 + 1] = pack_raw(__float2bfloat16_rn(d[2]), __float2bfloat16_rn(d[3]));
+          }
+          *reinterpret_cast<uint4 *>(sDZ + canon_off(r, c0 + c, MLP_H)) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        }
+      }
+      if (l > 0) {  // A_l = bf16(H_{l-1})
+        const float *ar = H + ((int64_t)(l - 1) * batch + rowc) * MLP_H + c0;
+#pragma unroll
+        for (int c = 0; c < 32; c += 8) {
+          const float4 a = in ? *reinterpret_cast<const float4 *>(ar + c) : make_float4(0.f, 0.f, 0.f, 0.f);
+          const float4 b = in ? *reinterpret_cast<const float4 *>(ar + c + 4) : make_float4(0.f, 0.f, 0.f, 0.f);
+          *reinterpret_cast<uint4 *>(sA + canon_off(r, c0 + c, MLP_H)) =
+              make_uint4(pack_raw(__float2bfloat16_rn(a.x), __float2bfloat16_rn(a.y)),
+                         pack_raw(__float2bfloat16_rn(a.z), __float2bfloat16_rn(a.w)),
+                         pack_raw(__float2bfloat16_rn(b.x), __float2bfloat16_rn(b.y)),
+                         pack_raw(__float2bfloat16_rn(b.z), __float2bfloat16_rn(b.w)));
+        }
+      } else {  // A_0 = bf16(X): 4 of the 16 features per warpgroup
+        const float *xr = X + (int64_t)(in ? sample_of(idx, row) : 0) * MLP_IN + 4 * q;
+        const float x0 = in ? xr[0] : 0.f, x1 = in ? xr[1] : 0.f, x2 = in ? xr[2] : 0.f, x3 = in ? xr[3] : 0.f;
+        *reinterpret_cast<uint2 *>(sA0 + canon_off(r, 4 * q, MLP_IN)) =
+            make_uint2(pack_raw(__float2bfloat16_rn(x0), __float2bfloat16_rn(x1)),
+                       pack_raw(__float2bfloat16_rn(x2), __float2bfloat16_rn(x3)));
+      }
+      async_proxy_fence();
+      tc_fence_before();
+      __syncthreads();
+      tc_fence_after();
+      if (tid == 0) {
+        const int K = l == 0 ? MLP_IN : MLP_H;
+        const unsigned char *A = l == 0 ? sA0 : sA;
+        const uint32_t dw = tmem + (l == 2 ? BT_DW2 : (l == 1 ? BT_DW1 : BT_DW0));
+        // dW_l += dZ^T A_l: A = dZ tile MN-major (MN groups of 8 outputs 128 B apart, K groups
+        // of 8 samples 2048 B apart), B = A_l tile MN-major (input groups 128 B apart, sample
+        // groups 16 K B apart); 16 samples per instruction
+        const uint32_t idw = umma_idesc_bf16(K) | (1u << 15) | (1u << 16);
+        for (int j = 0; j < TC_ROWS / 16; ++j)
+          tc_mma(dw, umma_desc(smem_u32(sDZ) + 4096u * j, 2048u, 128u),
+                 umma_desc(smem_u32(A) + (uint32_t)(32 * K) * j, (uint32_t)(16 * K), 128u), idw,
+                 (first && j == 0) ? 0u : 1u);
+        if (l > 0) {
+          // dH_{l-1} = dZ W_l: A = dZ tile K-major (as in the forward pass), B = W_l MN-major
+          // (input groups 128 B apart, output groups 2048 B apart); 16 outputs per instruction
+          const unsigned char *W = l == 2 ? sW2 : sW1;
+          const uint32_t idh = umma_idesc_bf16(MLP_H) | (1u << 16);
+          for (int j = 0; j < MLP_H / 16; ++j)
+            tc_mma(tmem + BT_DH, umma_desc(smem_u32(sDZ) + 256u * j, 128u, 2048u),
+                   umma_desc(smem_u32(W) + 4096u * j, 2048u, 128u), idh, j > 0 ? 1u : 0u);
+        }
+        tc_commit(smem_u32(bar));
+      }
+      bt_column_sums(sF, sPart, sAcc[l]);  // while the MMAs run
+      ok = __syncthreads_and(mbar_wait(smem_u32(bar), phase & 1u) ? 1 : 0) != 0;
+      ++phase;
+      tc_fence_after();
+    }
+    first = false;
+  }
+  if (ok) {
+    float *out = partial + (size_t)blockIdx.x * MLP_NPARAMS;
+    uint32_t v[32];
+    tmem_ld32(lane_addr + BT_DW2 + (uint32_t)c0, v);  // lane = output r, columns = inputs
+#pragma unroll
+    for (int c = 0; c < 32; ++c) out[OFF_W2 + r * MLP_H + c0 + c] = __uint_as_float(v[c]);
+    tmem_ld32(lane_addr + BT_DW1 + (uint32_t)c0, v);
+#pragma unroll
+    for (int c = 0; c < 32; ++c) out[OFF_W1 + r * MLP_H + c0 + c] = __uint_as_float(v[c]);
+    if (q == 0) {  // warp-uniform; columns 400-415 are read but not used
+      tmem_ld32(lane_addr + BT_DW0, v);
+#pragma unroll
+      for (int c = 0; c < MLP_IN; ++c) out[OFF_W0 + r * MLP_IN + c] = __uint_as_float(v[c]);
+    }
+    for (int i = tid; i < MLP_H; i += BT_THREADS) {
+      out[OFF_B0 + i] = sAcc[0][i];
+      out[OFF_B1 + i] = sAcc[1][i];
+      out[OFF_B2 + i] = sAcc[2][i];
+      out[OFF_W3 + i] = sAcc[3][i];
+    }
+    for (int i = MLP_H + tid; i < MLP_OUT * MLP_H + MLP_OUT; i += BT_THREADS)
+      if (i != MLP_OUT * MLP_H) out[OFF_W3 + i] = 0.f;  // unused output rows and biases
+    if (tid == 0) out[OFF_B3] = db3;
+  } else if (tid == 0 && status) {
+    atomicExch(status, 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BT_TMEM_COLS)
+                 : "memory");
+}
+
 // grad[p] = sum over the CTA partial rows, in CTA order.
 __global__ void mlp_reduce_kernel(const float *__restrict__ partial, int nblocks, float *__restrict__ grad) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < MLP_NPARAMS; p += gridDim.x * blockDim.x) {
@@ -619,6 +851,27 @@ extern "C" pk_status pk_mlp_backward(void *stream, const float *x, const int *id
   float *partial = static_cast<float *>(workspace);
   mlp_backward_kernel<<<blocks, MLP_WARPS * 32, smem, s>>>(x, idx, batch, (const __nv_bfloat16 *)wb, z, h, dy,
                                                            partial);
+  PK_LAUNCH_CHECK();
+  mlp_reduce_kernel<<<(MLP_NPARAMS + 255) / 256, 256, 0, s>>>(partial, blocks, grad);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+extern "C" pk_status pk_mlp_backward_tc(void *stream, const float *x, const int *idx, int batch, const void *wb,
+                                        const float *z, const float *h, const float *dy, float *grad,
+                                        void *workspace, size_t workspace_bytes, int *d_status) {
+  PK_REQUIRE(x && wb && z && h && dy && grad && batch > 0, PK_ERR_INVALID, "mlp_backward_tc: invalid arguments");
+  PK_REQUIRE((((uintptr_t)wb | (uintptr_t)z | (uintptr_t)h) & 15u) == 0, PK_ERR_INVALID,
+             "mlp_backward_tc: wb, z and h must be 16-byte aligned");
+  const int ntiles = (batch + TC_ROWS - 1) / TC_ROWS;
+  const int blocks = ntiles < sm_count() ? ntiles : sm_count();  // persistent, one CTA per SM
+  PK_REQUIRE(workspace && workspace_bytes >= (size_t)blocks * MLP_NPARAMS * sizeof(float), PK_ERR_WORKSPACE,
+             "mlp_backward_tc: workspace too small");
+  cudaStream_t s = (cudaStream_t)stream;
+  PK_CUDA(cudaFuncSetAttribute(mlp_backward_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BT_SMEM));
+  float *partial = static_cast<float *>(workspace);
+  mlp_backward_tc_kernel<<<blocks, BT_THREADS, BT_SMEM, s>>>(x, idx, batch, (const __nv_bfloat16 *)wb, z, h, dy,
+                                                             partial, d_status);
   PK_LAUNCH_CHECK();
   mlp_reduce_kernel<<<(MLP_NPARAMS + 255) / 256, 256, 0, s>>>(partial, blocks, grad);
   PK_LAUNCH_CHECK();

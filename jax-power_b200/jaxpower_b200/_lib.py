@@ -112,6 +112,8 @@ SIGNATURES = {
     'pk_mlp_backward_workspace_size': [c_int, ctypes.POINTER(c_size_t)],
     'pk_mlp_backward': [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                         c_void_p, c_size_t],
+    'pk_mlp_backward_tc': [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                           c_void_p, c_size_t, c_void_p],
     'pk_mlp_adam': [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p,
                     c_float, c_float, c_float, c_float],
 }

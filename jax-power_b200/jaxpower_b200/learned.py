@@ -113,9 +113,10 @@ class MLP:
         return (y, (z, h)) if cache else y
 
     def check(self):
-        """Raise if a tensor-core step of an earlier forward pass did not complete (synchronises)."""
+        """Raise if a tensor-core step of an earlier forward or backward pass did not complete
+        (synchronises)."""
         if int(self.status.item()):
-            raise RuntimeError('MLP forward: a tensor-core step did not complete within its wait limit')
+            raise RuntimeError('MLP: a tensor-core step did not complete within its wait limit')
 
     __call__ = forward
 
@@ -131,17 +132,51 @@ class MLP:
         nbytes = _lib.c_size_t()
         _lib.call('pk_mlp_backward_workspace_size', b, _lib.ctypes.byref(nbytes))
         ws = _workspace(nbytes.value)
-        _lib.call('pk_mlp_backward', _lib.stream_handle(), _lib.ptr(x), None, b, _lib.ptr(self.wb), _lib.ptr(z),
-                  _lib.ptr(h), _lib.ptr(dy), _lib.ptr(grad), _lib.ptr(ws), ws.numel())
+        _lib.call('pk_mlp_backward_tc', _lib.stream_handle(), _lib.ptr(x), None, b, _lib.ptr(self.wb),
+                  _lib.ptr(z), _lib.ptr(h), _lib.ptr(dy), _lib.ptr(grad), _lib.ptr(ws), ws.numel(),
+                  _lib.ptr(self.status))
         return grad
+
+    def _trainer(self, x, target, weight, batch, nsteps_table, lr_table, weight_decay):
+        """Buffers and an enqueuer of one training step (forward with stored activations, loss,
+        backward, reduction, AdamW: 5 kernels) on the samples perm[s * batch:(s + 1) * batch]."""
+        dev = x.device
+        n = x.shape[0]
+        nb = n // batch
+        perm = torch.zeros(nb * batch, dtype=torch.int32, device=dev)
+        y = torch.empty(batch, dtype=torch.float32, device=dev)
+        dy = torch.empty_like(y)
+        z = torch.empty((3, batch, HIDDEN), dtype=torch.float32, device=dev)
+        h = torch.empty_like(z)
+        grad = torch.empty(self.nparams, dtype=torch.float32, device=dev)
+        losses = torch.zeros(nb, dtype=torch.float32, device=dev)
+        nbytes = _lib.c_size_t()
+        _lib.call('pk_mlp_backward_workspace_size', batch, _lib.ctypes.byref(nbytes))
+        ws = _workspace(nbytes.value)
+
+        def step(s):
+            stream = _lib.stream_handle()
+            idx = _lib.ctypes.c_void_p(perm.data_ptr() + 4 * s * batch)
+            _lib.call('pk_mlp_forward_tc', stream, _lib.ptr(x), idx, batch, _lib.ptr(self.wb), _lib.ptr(self.w),
+                      _lib.ptr(y), _lib.ptr(z), _lib.ptr(h), _lib.ptr(self.status))
+            _lib.call('pk_mlp_mse', stream, _lib.ptr(y), _lib.ptr(target), _lib.ptr(weight), idx, batch,
+                      _lib.ptr(dy), _lib.ctypes.c_void_p(losses.data_ptr() + 4 * s))
+            _lib.call('pk_mlp_backward_tc', stream, _lib.ptr(x), idx, batch, _lib.ptr(self.wb), _lib.ptr(z),
+                      _lib.ptr(h), _lib.ptr(dy), _lib.ptr(grad), _lib.ptr(ws), ws.numel(), _lib.ptr(self.status))
+            _lib.call('pk_mlp_adam', stream, _lib.ptr(self.w), _lib.ptr(self.wb), _lib.ptr(self.m),
+                      _lib.ptr(self.v), _lib.ptr(grad), _lib.ptr(lr_table), nsteps_table, _lib.ptr(self.step),
+                      0.9, 0.999, 1e-8, float(weight_decay))
+
+        return step, perm, losses, nb
 
     def fit(self, x, target, weight=None, steps=2000, batch=4096, lr=2e-3, lr_final=2e-5, weight_decay=0.,
             seed=0, graph=True):
         """Minimise the (weighted) MSE with AdamW on the device; returns the mean loss per epoch.
 
         Each epoch draws a permutation of the samples; its steps (forward, loss, backward,
-        reduction, AdamW: 5 kernels each) are captured once in a CUDA graph and replayed.
-        The learning rate follows a cosine from ``lr`` to ``lr_final`` over ``steps``.
+        reduction, AdamW: 5 kernels each, on the tcgen05 tensor cores for the forward and
+        backward passes) are captured once in a CUDA graph and replayed.  The learning rate
+        follows a cosine from ``lr`` to ``lr_final`` over ``steps``.
         """
         x = self._x(x)
         dev = x.device
@@ -155,33 +190,14 @@ class MLP:
         t = np.arange(total)
         lrs = lr_final + 0.5 * (lr - lr_final) * (1. + np.cos(np.pi * t / max(total - 1, 1)))
         lr_table = torch.as_tensor(lrs, dtype=torch.float32, device=dev)
-        perm = torch.zeros(nb * batch, dtype=torch.int32, device=dev)
-        y = torch.empty(batch, dtype=torch.float32, device=dev)
-        dy = torch.empty_like(y)
-        z = torch.empty((3, batch, HIDDEN), dtype=torch.float32, device=dev)
-        h = torch.empty_like(z)
-        grad = torch.empty(self.nparams, dtype=torch.float32, device=dev)
-        losses = torch.zeros(nb, dtype=torch.float32, device=dev)
-        nbytes = _lib.c_size_t()
-        _lib.call('pk_mlp_backward_workspace_size', batch, _lib.ctypes.byref(nbytes))
-        ws = _workspace(nbytes.value)
+        step, perm, losses, nb = self._trainer(x, target, weight, batch, total, lr_table, weight_decay)
         self.step.zero_()
         self.m.zero_()
         self.v.zero_()
 
         def epoch():
-            stream = _lib.stream_handle()
             for s in range(nb):
-                idx = _lib.ctypes.c_void_p(perm.data_ptr() + 4 * s * batch)
-                _lib.call('pk_mlp_forward_tc', stream, _lib.ptr(x), idx, batch, _lib.ptr(self.wb), _lib.ptr(self.w),
-                          _lib.ptr(y), _lib.ptr(z), _lib.ptr(h), _lib.ptr(self.status))
-                _lib.call('pk_mlp_mse', stream, _lib.ptr(y), _lib.ptr(target), _lib.ptr(weight), idx, batch,
-                          _lib.ptr(dy), _lib.ctypes.c_void_p(losses.data_ptr() + 4 * s))
-                _lib.call('pk_mlp_backward', stream, _lib.ptr(x), idx, batch, _lib.ptr(self.wb), _lib.ptr(z),
-                          _lib.ptr(h), _lib.ptr(dy), _lib.ptr(grad), _lib.ptr(ws), ws.numel())
-                _lib.call('pk_mlp_adam', stream, _lib.ptr(self.w), _lib.ptr(self.wb), _lib.ptr(self.m),
-                          _lib.ptr(self.v), _lib.ptr(grad), _lib.ptr(lr_table), total, _lib.ptr(self.step),
-                          0.9, 0.999, 1e-8, float(weight_decay))
+                step(s)
 
         gen = torch.Generator(device=dev)
         gen.manual_seed(int(seed))
@@ -203,6 +219,35 @@ class MLP:
         out = torch.stack(history).cpu().numpy()
         self.check()
         return out
+
+    def fit_step_seconds(self, x, target, batch=4096, steps=20, lr=1e-4, seed=0):
+        """Device time of one training step at ``batch`` (CUDA events around a replay of a CUDA
+        graph of ``steps`` steps over the first samples of a random permutation; the weights are
+        updated, with a small constant learning rate)."""
+        x = self._x(x)
+        dev = x.device
+        batch = int(min(batch, x.shape[0]))
+        target = torch.as_tensor(target, dtype=torch.float32, device=dev).contiguous()
+        lr_table = torch.full((1,), float(lr), dtype=torch.float32, device=dev)
+        step, perm, _, nb = self._trainer(x, target, None, batch, 1, lr_table, 0.)
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(int(seed))
+        perm.copy_(torch.randperm(x.shape[0], generator=gen, device=dev)[:perm.numel()].to(torch.int32))
+        for s in range(min(steps, nb)):
+            step(s)  # warm-up
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            for s in range(steps):
+                step(s % nb)
+        g.replay()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        g.replay()
+        b.record()
+        torch.cuda.synchronize()
+        self.check()
+        return a.elapsed_time(b) / 1e3 / steps
 
     def state(self):
         return self.w.detach().cpu().numpy().copy()

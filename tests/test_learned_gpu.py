@@ -85,6 +85,65 @@ def test_gradient_matches_oracle():
         assert np.allclose(g, r, rtol=0, atol=5e-3 * np.abs(r).max()), name
 
 
+@pytest.mark.parametrize('batch', [1, 127, 128, 129, 3000, 40000])
+def test_tcgen05_backward_matches_mma_backward(batch):
+    """The tcgen05 backward (weight gradients accumulated in tensor memory over a persistent
+    CTA's tiles; 40000 samples give several tiles per CTA) against the mma.sync backward and
+    the oracle, through a sample gather."""
+    from jaxpower_b200 import _lib
+    flat = _flat(9)
+    mlp = _mlp(flat)
+    rng = np.random.default_rng(10)
+    n = batch + 17
+    x = torch.as_tensor(rng.normal(size=(n, omlp.IN)).astype('f4')).cuda()
+    idx = torch.as_tensor(rng.permutation(n)[:batch].astype('i4')).cuda()
+    dy = torch.as_tensor(rng.normal(size=batch).astype('f4')).cuda()
+    y = torch.empty(batch, device='cuda')
+    z = torch.empty((3, batch, omlp.H), device='cuda')
+    h = torch.empty_like(z)
+    _lib.call('pk_mlp_forward_tc', _lib.stream_handle(), _lib.ptr(x), _lib.ptr(idx), batch, _lib.ptr(mlp.wb),
+              _lib.ptr(mlp.w), _lib.ptr(y), _lib.ptr(z), _lib.ptr(h), _lib.ptr(mlp.status))
+    nbytes = _lib.c_size_t()
+    _lib.call('pk_mlp_backward_workspace_size', batch, _lib.ctypes.byref(nbytes))
+    ws = torch.empty(nbytes.value, dtype=torch.uint8, device='cuda')
+    grads = []
+    for name in ('pk_mlp_backward', 'pk_mlp_backward_tc'):
+        grad = torch.full((mlp.nparams,), float('nan'), device='cuda')
+        extra = (_lib.ptr(mlp.status),) if name.endswith('_tc') else ()
+        _lib.call(name, _lib.stream_handle(), _lib.ptr(x), _lib.ptr(idx), batch, _lib.ptr(mlp.wb), _lib.ptr(z),
+                  _lib.ptr(h), _lib.ptr(dy), _lib.ptr(grad), _lib.ptr(ws), ws.numel(), *extra)
+        grads.append(grad.cpu().numpy())
+    mlp.check()
+    g0, g1 = grads
+    assert np.all(np.isfinite(g1))
+    xs = x.cpu().numpy()[idx.cpu().numpy()]
+    _, cache = omlp.forward(flat.astype('f8'), xs)
+    ref = omlp.backward(flat.astype('f8'), cache, dy.cpu().numpy().astype('f8'))
+    off = 0
+    for name, shape in omlp.LAYOUT:
+        size = int(np.prod(shape))
+        a, b, r = g0[off:off + size], g1[off:off + size], ref[off:off + size]
+        off += size
+        if not np.any(r):
+            assert np.all(b == 0.), name
+            continue
+        # both kernels round the same operands to bf16 and sum in float32 in different orders
+        # (a dZ on a bf16 rounding boundary can round either way)
+        assert np.linalg.norm(b - a) <= 2e-4 * np.linalg.norm(a), name
+        assert np.linalg.norm(b - r) <= 2e-3 * np.linalg.norm(r), name
+
+
+def test_tcgen05_backward_is_deterministic():
+    from jaxpower_b200 import _lib
+    flat = _flat(11)
+    mlp = _mlp(flat)
+    x = torch.randn(70000, omlp.IN, generator=torch.Generator().manual_seed(0)).cuda()
+    dy = torch.randn(70000, generator=torch.Generator().manual_seed(1)).cuda()
+    _, cache = mlp.forward(x, cache=True)
+    assert torch.equal(mlp.gradient(x, dy, cache), mlp.gradient(x, dy, cache))
+    mlp.check()
+
+
 def test_gradient_is_deterministic():
     flat = _flat(4)
     x = torch.randn(5000, omlp.IN, generator=torch.Generator().manual_seed(0))
