@@ -633,7 +633,7 @@ def run_learned(ntrain=None, nheld=None, steps=None):
     import torch
     import jaxpower_b200 as jp
     from jaxpower_b200.learned import (LearnedCorrection, mock_spectra, spectrum_errors, ensemble_bias,
-                                      ensemble_bias_significance)
+                                      ensemble_bias_significance, ensemble_bias_chi2)
     L = dict(LEARNED)
     ntrain = ntrain or L['ntrain']
     nheld = nheld or L['nheld']
@@ -749,6 +749,10 @@ def run_learned(ntrain=None, nheld=None, steps=None):
                     'plain_128': ensemble_bias_significance(low, high, data['k'], kmax),
                     'mean_table_128': ensemble_bias_significance(low + table[None] * low[:, :1], high, data['k'],
                                                                  kmax)},
+                heldout_bias_chi2_per_bin={
+                    'learned': ensemble_bias_chi2(fixed, high, data['k'], kmax),
+                    'plain_128': ensemble_bias_chi2(low, high, data['k'], kmax),
+                    'mean_table_128': ensemble_bias_chi2(low + table[None] * low[:, :1], high, data['k'], kmax)},
                 heldout_rms_rel_err_per_ell={'learned': [float(v) for v in np.sqrt((bin_corr**2).mean(axis=(0, 2)))],
                                              'plain_128': [float(v) for v in np.sqrt((bin_plain**2).mean(axis=(0, 2)))],
                                              'mean_table_128': [float(v) for v in
@@ -1011,6 +1015,8 @@ def learned_summary(r):
            'heldout_bias_max_plain_128': r['heldout_bias_max']['plain_128'],
            'heldout_bias_sigma_learned': r['heldout_bias_in_standard_errors']['learned'],
            'heldout_bias_sigma_table': r['heldout_bias_in_standard_errors']['mean_table_128'],
+           'heldout_bias_chi2_per_bin_learned': r['heldout_bias_chi2_per_bin']['learned'],
+           'heldout_bias_chi2_per_bin_table': r['heldout_bias_chi2_per_bin']['mean_table_128'],
            'per_mock_max_rel_err_median_learned': r['heldout_max_rel_err']['learned']['median'],
            'per_mock_max_rel_err_median_table': r['heldout_max_rel_err']['mean_table_128']['median'],
            'frac_heldout_within_0p5pct': r['frac_heldout_within_0p5pct'],
