@@ -790,6 +790,77 @@ __host__ inline void legendre_coefs(int ell, float c[5], int *odd) {
   *odd = ell & 1;
 }
 
+// End of a row walk (bin_global_kernel, bin_interlaced_staged_kernel): join the lanes' lead and
+// trail runs with a segmented scan over the lanes and add each bin's sum to the warp histogram
+// once.  cur: the lane's last bin (-1: no mode), nseg: its finished runs, lead / facc: the first
+// run (when nseg > 0), acc: the open run.
+template <int NV>
+__device__ __forceinline__ void finish_row_runs(int cur, int nseg, int lead, const float facc_in[NV],
+                                                const float acc[NV], float *my, int nbins, int lane) {
+  constexpr int NONE = 0x7fffffff;
+  int trail;
+  float facc[NV], tacc[NV];
+  if (cur < 0) {
+    lead = trail = NONE;
+#pragma unroll
+    for (int c = 0; c < NV; ++c) tacc[c] = facc[c] = 0.f;
+  } else if (nseg == 0) {
+    lead = trail = cur;
+#pragma unroll
+    for (int c = 0; c < NV; ++c) {
+      tacc[c] = acc[c];
+      facc[c] = 0.f;
+    }
+  } else {
+    trail = cur;
+#pragma unroll
+    for (int c = 0; c < NV; ++c) {
+      tacc[c] = acc[c];
+      facc[c] = facc_in[c];
+    }
+  }
+  float S[NV];
+#pragma unroll
+  for (int c = 0; c < NV; ++c) S[c] = tacc[c];
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int k = __shfl_up_sync(0xffffffffu, trail, d);
+    const bool ok = lane >= d && k == trail;
+#pragma unroll
+    for (int c = 0; c < NV; ++c) {
+      const float t = __shfl_up_sync(0xffffffffu, S[c], d);
+      if (ok) S[c] += t;
+    }
+  }
+  const int prev_trail = __shfl_up_sync(0xffffffffu, trail, 1);
+  float carry[NV];
+#pragma unroll
+  for (int c = 0; c < NV; ++c) {
+    const float t = __shfl_up_sync(0xffffffffu, S[c], 1);
+    carry[c] = (lane > 0 && prev_trail == lead) ? t : 0.f;
+  }
+  const int next_lead = __shfl_down_sync(0xffffffffu, lead, 1);
+  const int next_trail = __shfl_down_sync(0xffffffffu, trail, 1);
+  if (cur >= 0 && nseg > 0 && lead >= 1 && lead <= nbins) {
+#pragma unroll
+    for (int c = 0; c < NV; ++c) my[(size_t)(lead - 1) * NV + c] += facc[c] + carry[c];
+  }
+  const bool next_takes = lane < 31 && next_lead == trail;
+  const bool next_continues = lane < 31 && next_trail == trail;
+  if (cur >= 0 && !next_takes && !next_continues && trail >= 1 && trail <= nbins) {
+#pragma unroll
+    for (int c = 0; c < NV; ++c) my[(size_t)(trail - 1) * NV + c] += S[c];
+  }
+  __syncwarp();
+}
+
+template <int NV>
+__device__ __forceinline__ void moments_to_poles(const LegendreCoefs &lc, float m0, float m1, float m2,
+                                                 float out[NV]) {
+#pragma unroll
+  for (int l = 0; l < NV; ++l) out[l] = __fmaf_rn(lc.c[l][2], m2, __fmaf_rn(lc.c[l][1], m1, lc.c[l][0] * m0));
+}
+
 // Shared layout of the fused kernel: float32 warp histograms [nwarps][nbins][NV] (warp
 // partials), thresholds, kz tables.
 struct GlobalSmem {
@@ -868,7 +939,7 @@ __global__ void __launch_bounds__(BIN_THREADS, MINB) bin_global_kernel(
     const float kl = kx * lx + ky * ly;
     RowFactor<NSR> rf;
     if (NS > 0) row_factor<NSR, FULL, XYM != XY_NONE>(fp, zt, i, j, rf);
-    int cur = -1, lead = NONE, trail = NONE, nseg = 0;
+    int cur = -1, lead = NONE, nseg = 0;
     float acc[NV], facc[NV];
 #pragma unroll
     for (int c = 0; c < NV; ++c) acc[c] = facc[c] = 0.f;
@@ -965,62 +1036,226 @@ __global__ void __launch_bounds__(BIN_THREADS, MINB) bin_global_kernel(
         }
       }
     }
-    float tacc[NV];
-    if (cur < 0) {
-      lead = trail = NONE;
-#pragma unroll
-      for (int c = 0; c < NV; ++c) tacc[c] = 0.f;
-    } else if (nseg == 0) {
-      lead = trail = cur;
-#pragma unroll
-      for (int c = 0; c < NV; ++c) {
-        tacc[c] = acc[c];
-        facc[c] = 0.f;
-      }
-    } else {
-      trail = cur;
-#pragma unroll
-      for (int c = 0; c < NV; ++c) tacc[c] = acc[c];
-    }
-    float S[NV];
-#pragma unroll
-    for (int c = 0; c < NV; ++c) S[c] = tacc[c];
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const int k = __shfl_up_sync(0xffffffffu, trail, d);
-      const bool ok = lane >= d && k == trail;
-#pragma unroll
-      for (int c = 0; c < NV; ++c) {
-        const float t = __shfl_up_sync(0xffffffffu, S[c], d);
-        if (ok) S[c] += t;
-      }
-    }
-    const int prev_trail = __shfl_up_sync(0xffffffffu, trail, 1);
-    float carry[NV];
-#pragma unroll
-    for (int c = 0; c < NV; ++c) {
-      const float t = __shfl_up_sync(0xffffffffu, S[c], 1);
-      carry[c] = (lane > 0 && prev_trail == lead) ? t : 0.f;
-    }
-    const int next_lead = __shfl_down_sync(0xffffffffu, lead, 1);
-    const int next_trail = __shfl_down_sync(0xffffffffu, trail, 1);
-    if (cur >= 0 && nseg > 0 && lead >= 1 && lead <= nbins) {
-#pragma unroll
-      for (int c = 0; c < NV; ++c) my[(size_t)(lead - 1) * NV + c] += facc[c] + carry[c];
-    }
-    const bool next_takes = lane < 31 && next_lead == trail;
-    const bool next_continues = lane < 31 && next_trail == trail;
-    if (cur >= 0 && !next_takes && !next_continues && trail >= 1 && trail <= nbins) {
-#pragma unroll
-      for (int c = 0; c < NV; ++c) my[(size_t)(trail - 1) * NV + c] += S[c];
-    }
-    __syncwarp();
+    finish_row_runs<NV>(cur, nseg, lead, facc, acc, my, nbins, lane);
   }
   __syncthreads();  // warp partials (float32) finished in float64, in warp order
   double *outp = partials + (size_t)blockIdx.x * hist_len;
   for (int q = threadIdx.x; q < hist_len; q += blockDim.x) {
     double a = 0.;
     for (int w = 0; w < nwarps; ++w) a += (double)s.hist[(size_t)w * hist_len + q];
+    outp[q] = a;
+  }
+}
+
+// ------------------------------------------------- fused interlaced binning, staged rows
+// The interlaced + compensated global-los pass for even multipoles (ell <= 4) of 'jax'
+// half-complex meshes (a single mesh or a batch).  A prologue (staged_rows_kernel) tabulates
+// per (i, j) row |k_xy|^2, k_xy . los, the window scale, the interlacing phases and the row's
+// cut: |k|^2 increases along kz, so the modes at or beyond the last edge form the row's tail,
+// cut at the first such kz (rows whose first mode is already beyond it are skipped, meshes
+// unread: with edges up to k_Nyq that is 48 % of the stored modes, the corners of the k cube;
+// they would fall in no bin, so the sums do not change).  Then per row and warp:
+//  1. lanes on consecutive kz form each mode's weighted power w |combine_mode(...)|^2 from
+//     coalesced loads of the NS shifted meshes (one 128-byte line per 16 lanes and mesh) and
+//     its mu^2, into the warp's row buffers in shared memory;
+//  2. each lane walks a contiguous run of the row, following the bin by comparing |k|^2 with
+//     the next exact threshold (the bin is non-decreasing along kz), and accumulates per bin
+//     run the moments M_p = sum P mu^(2p), p = 0, 1, 2, in registers; a finished run becomes
+//     its multipoles sum_p c_{ell,p} M_p once, and runs continuing across lanes are joined by
+//     the segmented scan of bin_global_kernel.
+// The k = 0 mode (row 0, kz 0) enters the monopole only (when ell = 0 is asked), added by lane 0
+// on its own.  Mode values, row factors and bins are bit-identical to bin_global_kernel's (the
+// same combine_mode, row_factor and exact thresholds); the multipoles differ by float32
+// rounding in the run sums.
+#ifndef PK_FUSED_STAGED
+#define PK_FUSED_STAGED 1
+#endif
+#ifndef PK_STAGED_MIN_CTAS
+#define PK_STAGED_MIN_CTAS 3
+#endif
+constexpr int STAGED_MAX_SHIFTS = 4;
+// shared-memory bytes of one warp's row buffers (power and mu^2, float) for nz modes
+__host__ __device__ inline size_t staged_row_bytes(int nz) { return (size_t)32 * ((nz + 31) / 32) * 8; }
+// global bytes of the row table: (|k_xy|^2, k_xy . los, scale, cut) per row, then the phases of
+// shifts 1..NS-1 per row
+inline size_t staged_table_bytes(const Dims &d, int nshifts) {
+  return (size_t)d.n0 * d.n1 * (sizeof(float4) + (size_t)(nshifts - 1) * sizeof(float2));
+}
+
+template <int NS>
+__global__ void staged_rows_kernel(BinGeom g, FourierParams fp, float lx, float ly, const float *__restrict__ edges,
+                                   float4 *__restrict__ rowa, float2 *__restrict__ rowph) {
+  const float thr_last = sqrt_threshold(edges[g.nedges - 1]);
+  const ZTable zt = ztable_at<XY_GLOBAL>(nullptr, fp, false);  // the per-axis tables of fp.gxy
+  const int64_t nrows = (int64_t)g.d.n0 * g.d.n1;
+  for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < nrows;
+       row += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(row / g.d.n1), j = (int)(row % g.d.n1);
+    const float kx = kcoord(i, g.d.n0, g.kfun[0], false);
+    const float ky = kcoord(j, g.d.n1, g.kfun[1], false);
+    const float kxy = __fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky));
+    int zhi = 0;  // the first kz whose |k|^2 reaches the last threshold (0: none below it)
+    if (kxy < thr_last) {
+      int lim = g.d.nz;
+      while (zhi < lim) {
+        const int mid = (zhi + lim) >> 1;
+        const float kz = kz_coord(g, mid);
+        if (__fadd_rn(kxy, __fmul_rn(kz, kz)) >= thr_last) lim = mid;
+        else zhi = mid + 1;
+      }
+    }
+    RowFactor<NS> rf;
+    row_factor<NS, false, true>(fp, zt, i, j, rf);
+    rowa[row] = make_float4(kxy, kx * lx + ky * ly, rf.scale, __int_as_float(zhi));
+#pragma unroll
+    for (int s = 1; s < NS; ++s) rowph[row * (NS - 1) + s - 1] = rf.ph[s];
+  }
+}
+
+template <int NV, int NS, int MINB>
+__global__ void __launch_bounds__(BIN_THREADS, MINB) bin_interlaced_staged_kernel(
+    BinGeom g, const float2 *__restrict__ d1, float lz, LegendreCoefs lc, int zero_l0,
+    const float *__restrict__ edges, int nwarps_hist, double *__restrict__ partials, FourierParams fp,
+    const float4 *__restrict__ rowa, const float2 *__restrict__ rowph) {
+  const int nbins = g.nedges - 1;
+  const int hist_len = nbins * NV;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  const int nz = g.d.nz;
+  const int S = 32 * ((nz + 31) / 32);  // row buffer slots
+  extern __shared__ double smem[];
+  float *hist = reinterpret_cast<float *>(smem);
+  float *thr = hist + (((size_t)nwarps_hist * hist_len + 3) & ~(size_t)3);
+  float *skz = thr + ((g.nedges + 3) & ~3);
+  float *skz2 = skz + ((nz + 3) & ~3);
+  float *pbuf_all = skz2 + ((nz + 3) & ~3);         // [nwarps][S] powers
+  float *mbuf_all = pbuf_all + (size_t)nwarps * S;  // [nwarps][S] mu^2
+  ZTable zt = ztable_at<XY_NONE>(mbuf_all + (size_t)nwarps * S, fp, false);
+  fill_ztable<false, XY_NONE>(fp, zt);
+  for (int q = threadIdx.x; q < nwarps_hist * hist_len; q += blockDim.x) hist[q] = 0.f;
+  for (int q = threadIdx.x; q < g.nedges; q += blockDim.x) thr[q] = sqrt_threshold(edges[q]);
+  for (int z = threadIdx.x; z < nz; z += blockDim.x) {
+    const float kzz = kz_coord(g, z);
+    skz[z] = kzz;
+    skz2[z] = __fmul_rn(kzz, kzz);
+  }
+  __syncthreads();
+  float *my = hist + (size_t)warp * hist_len;
+  float *pbuf = pbuf_all + (size_t)warp * S, *mbuf = mbuf_all + (size_t)warp * S;
+  const float e0 = edges[0];
+  const float inv_step = g.step > 0.f ? 1.f / g.step : 0.f;
+  d1 += (int64_t)blockIdx.y * NS * g.d.ncomplex();
+  partials += (size_t)blockIdx.y * gridDim.x * hist_len;
+  RowWalker rw((int64_t)blockIdx.x * nwarps + warp, (int64_t)gridDim.x * nwarps, g.d.n1);
+  // the row table entries of the warp's next row are loaded one row ahead
+  float4 ra = make_float4(0.f, 0.f, 0.f, 0.f);
+  float2 rp[NS > 1 ? NS - 1 : 1];
+  if (rw.i < g.d.n0) {
+    const int64_t r0 = (int64_t)rw.i * g.d.n1 + rw.j;
+    ra = rowa[r0];
+#pragma unroll
+    for (int s = 1; s < NS; ++s) rp[s - 1] = rowph[r0 * (NS - 1) + s - 1];
+  }
+  for (; rw.i < g.d.n0;) {
+    const int64_t row = (int64_t)rw.i * g.d.n1 + rw.j;
+    const float4 rcur = ra;
+    RowFactor<NS> rf;
+#pragma unroll
+    for (int s = 1; s < NS; ++s) rf.ph[s] = rp[s - 1];
+    rw.next();
+    if (rw.i < g.d.n0) {
+      const int64_t rn = (int64_t)rw.i * g.d.n1 + rw.j;
+      ra = rowa[rn];
+#pragma unroll
+      for (int s = 1; s < NS; ++s) rp[s - 1] = rowph[rn * (NS - 1) + s - 1];
+    }
+    const int zhi = __float_as_int(rcur.w);
+    if (zhi == 0) continue;  // every mode of the row is beyond the last edge (warp-uniform)
+    const float kxy = rcur.x, kl = rcur.y;
+    rf.scale = rcur.z;
+    const int Rz = (zhi + 31) >> 5;  // modes per lane
+    // phase 1: lanes on consecutive kz: weighted power and mu^2 of each mode
+    for (int t0 = 0; t0 < Rz; t0 += 3) {
+      float p[3], m[3];
+#pragma unroll
+      for (int u = 0; u < 3; ++u) {
+        const int z = lane + 32 * (t0 + u);
+        p[u] = m[u] = 0.f;
+        if (t0 + u < Rz && z < zhi) {
+          const float2 v = combine_mode<NS, false>(fp, rf, zt, d1, row * nz + z, z);
+          p[u] = (v.x * v.x + v.y * v.y) * (z > 0 ? 2.f : 1.f);
+          const float k2 = __fadd_rn(kxy, skz2[z]);
+          const float num = kl + skz[z] * lz;
+          m[u] = k2 > 0.f ? num * num * __fdividef(1.f, k2) : 0.f;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 3; ++u)
+        if (t0 + u < Rz) {
+          pbuf[lane + 32 * (t0 + u)] = p[u];
+          mbuf[lane + 32 * (t0 + u)] = m[u];
+        }
+    }
+    __syncwarp();
+    // phase 2: contiguous runs per lane, the bin followed by threshold compares
+    const int z0 = lane * Rz, z1 = min(zhi, z0 + Rz);
+    int zs = z0;
+    if (row == 0) {
+      if (lane == 0) {  // the k = 0 mode: the monopole only
+        const int gb = bin_from_k2(thr, g.nedges, e0, inv_step, 0.f);
+        if (gb >= 1 && gb <= nbins)
+#pragma unroll
+          for (int l = 0; l < NV; ++l)
+            if (zero_l0 & (1 << l)) my[(size_t)(gb - 1) * NV + l] += pbuf[0] * lc.c[l][0];
+        zs = 1;
+      }
+      __syncwarp();
+    }
+    int cur = -1, lead = 0, nseg = 0;
+    float thr_next = INFINITY;
+    if (zs < z1) {
+      cur = bin_from_k2(thr, g.nedges, e0, inv_step, __fadd_rn(kxy, skz2[zs]));  // < nedges: zs < zhi
+      thr_next = thr[cur];
+    }
+    float m0 = 0.f, m1 = 0.f, m2 = 0.f;
+    float facc[NV];
+#pragma unroll
+    for (int c = 0; c < NV; ++c) facc[c] = 0.f;
+    for (int z = zs; z < z1; ++z) {
+      const float pz = pbuf[z], mu2 = mbuf[z];
+      const float k2 = __fadd_rn(kxy, skz2[z]);
+      if (k2 >= thr_next) {  // the run of bin cur ends before z
+        float Sv[NV];
+        moments_to_poles<NV>(lc, m0, m1, m2, Sv);
+        const bool first = nseg == 0;
+        lead = first ? cur : lead;
+#pragma unroll
+        for (int c = 0; c < NV; ++c) facc[c] = first ? Sv[c] : facc[c];
+        if (!first && cur >= 1 && cur <= nbins) {
+          float *h = my + (cur - 1) * NV;
+#pragma unroll
+          for (int c = 0; c < NV; ++c) h[c] += Sv[c];
+        }
+        ++nseg;
+        do ++cur;
+        while (cur < g.nedges - 1 && k2 >= thr[cur]);  // k2 < thr[nedges - 1]: z < zhi
+        thr_next = thr[cur];
+        m0 = m1 = m2 = 0.f;
+      }
+      const float pm = pz * mu2;
+      m0 += pz;
+      m1 += pm;
+      m2 = __fmaf_rn(pm, mu2, m2);
+    }
+    float acc[NV];
+    moments_to_poles<NV>(lc, m0, m1, m2, acc);
+    finish_row_runs<NV>(cur, nseg, lead, facc, acc, my, nbins, lane);
+  }
+  __syncthreads();  // warp partials (float32) finished in float64, in warp order
+  double *outp = partials + (size_t)blockIdx.x * hist_len;
+  for (int q = threadIdx.x; q < hist_len; q += blockDim.x) {
+    double a = 0.;
+    for (int w = 0; w < nwarps; ++w) a += (double)hist[(size_t)w * hist_len + q];
     outp[q] = a;
   }
 }
@@ -1243,6 +1478,48 @@ static pk_status launch_global(cudaStream_t st, const BinGeom &g, const float2 *
   }
   const int hist_len = (g.nedges - 1) * NV;
   int blocks = L.blocks;
+#if PK_FUSED_STAGED
+  if constexpr (NS > 0 && NS <= STAGED_MAX_SHIFTS && !CROSS && EVEN && !FULL && NV <= 3) {
+    if (g.d.nz >= PK_GLOBAL_FLAT_NZ) {
+      // workspace: partial rows, the per-axis tables, the row table
+      const size_t xy_off = align_up(L.partial_bytes * nbatch);
+      const size_t rows_off = align_up(xy_off + xy_table_bytes(g.d, NS));
+      PK_REQUIRE(workspace_bytes >= rows_off + staged_table_bytes(g.d, NS), PK_ERR_WORKSPACE,
+                 "binning workspace too small: need %zu bytes, got %zu", rows_off + staged_table_bytes(g.d, NS),
+                 workspace_bytes);
+      fpv.gxy = reinterpret_cast<float2 *>(static_cast<char *>(workspace) + xy_off);
+      if (xy_smem) {  // the row-run kernels keep these tables in shared memory; the prologue reads them here
+        fill_xy_tables_kernel<<<(g.d.n0 + g.d.n1 + 127) / 128, 128, 0, st>>>(fpv);
+        PK_LAUNCH_CHECK();
+      }
+      float4 *rowa = reinterpret_cast<float4 *>(static_cast<char *>(workspace) + rows_off);
+      float2 *rowph = reinterpret_cast<float2 *>(rowa + (size_t)g.d.n0 * g.d.n1);
+      const int64_t nrows = (int64_t)g.d.n0 * g.d.n1;
+      staged_rows_kernel<NS><<<(int)std::min<int64_t>((nrows + 255) / 256, 4 * sm_count()), 256, 0, st>>>(
+          g, fpv, los[0], los[1], edges, rowa, rowph);
+      PK_LAUNCH_CHECK();
+      // shared memory: histograms, thresholds, kz tables, row buffers, the kz phase / window tables
+      const size_t smem = align_up((size_t)L.nwarps * (g.nedges - 1) * NV * sizeof(float), 16) +
+                          (size_t)((g.nedges + 3) & ~3) * sizeof(float) +
+                          2 * (size_t)((g.d.nz + 3) & ~3) * sizeof(float) +
+                          (size_t)L.nwarps * staged_row_bytes(g.d.nz) + ztable_bytes(g.d, NS, false, false);
+      PK_REQUIRE(smem <= 227 * 1024, PK_ERR_RANGE, "mesh too large along the last axis for the fused pass");
+      auto kernel = bin_interlaced_staged_kernel<NV, NS, PK_STAGED_MIN_CTAS>;
+      PK_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      int per_sm = 0;
+      PK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, L.nwarps * 32, smem));
+      if (per_sm < 1) per_sm = 1;
+      // one wave of resident CTAs (at most the planned partial rows)
+      blocks = (int)std::min<int64_t>(L.blocks, std::max<int64_t>(1, (int64_t)per_sm * sm_count() / nbatch));
+      kernel<<<dim3(blocks, nbatch), L.nwarps * 32, smem, st>>>(g, d1, los[2], lc, zero_l0, edges, L.nwarps, partials,
+                                                                fpv, rowa, rowph);
+      PK_LAUNCH_CHECK();
+      launch_finalize(st, partials, blocks, hist_len, NV, g.nedges - 1, 0, out, nullptr, nbatch);
+      PK_LAUNCH_CHECK();
+      return PK_OK;
+    }
+  }
+#endif
   if (g.d.nz < PK_GLOBAL_FLAT_NZ) {
     if (NS <= 0 && !L.tab) {  // the flat kernel always tabulates kz
       L.smem += 2 * (size_t)((g.d.nz + 3) & ~3) * sizeof(float);
@@ -1367,8 +1644,8 @@ extern "C" pk_status pk_bin_workspace_size(const int32_t meshsize[3], int nedges
       if (L.partial_bytes > most) most = L.partial_bytes;
     }
   }
-  // plus the per-axis tables of the fused interlacing pass (up to 4 shifts)
-  most = align_up(most) + xy_table_bytes(d, 4);
+  // plus the per-axis tables and the row table of the fused interlacing pass (up to 4 shifts)
+  most = align_up(align_up(most) + xy_table_bytes(d, 4)) + staged_table_bytes(d, STAGED_MAX_SHIFTS);
   *bytes = most;
   return PK_OK;
 }

@@ -58,6 +58,30 @@ def test_batched_vs_oracle_float64():
         assert np.allclose(out[m], ref, rtol=0, atol=1e-5 * scale)
 
 
+def test_batched_long_rows_vs_oracle_float64():
+    """A batch of meshes with long stored rows (97 modes: the staged row kernel of the fused
+    interlaced binning, one grid row of CTAs per mesh) against the float64 oracle."""
+    import jaxpower_b200 as jp
+    from jaxpower_b200.batch import BatchedSpectra
+    counts = [15000, 0, 6000]
+    boxsize, meshsize = np.array([300., 300., 1200.]), np.array([24, 24, 192])
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.03}, ells=(0, 2, 4))
+    rng = np.random.default_rng(5)
+    mocks = [(rng.uniform(-0.5, 0.5, (c, 3)) * boxsize).astype('f4') for c in counts]
+    out = BatchedSpectra(attrs, b, counts, resampler='tsc', interlacing=3)(
+        torch.as_tensor(np.concatenate(mocks)).cuda()).cpu().numpy()
+    geom = Geometry(meshsize, boxsize, 0., dtype=np.float64)
+    ob = Bins(geom, step=0.03, ells=(0, 2, 4))
+    for m, pos in enumerate(mocks):
+        if len(pos) == 0:
+            assert np.all(out[m] == 0.)
+            continue
+        ref = ospectrum(opaint.paint(geom, pos.astype('f8'), None, 'tsc', 3, True, 'complex'), ob, los='z')['num_raw']
+        scale = np.abs(ref[0]).max()
+        assert np.allclose(out[m], ref, rtol=0, atol=1e-5 * scale)
+
+
 def test_batched_reports_dropped_particles():
     """A non-finite position in one mock raises, like ParticleField.paint; each replay reports its
     own inputs (the flag is cleared inside the graph), so a clean batch afterwards passes."""

@@ -200,12 +200,15 @@ def test_spectrum_deterministic():
 @pytest.mark.parametrize('resampler,interlacing,compensate', [('cic', 0, True), ('tsc', 2, False), ('tsc', 3, True),
                                                             ('pcs', 4, True)])
 @pytest.mark.parametrize('backend', ['jax', 'jaxdecomp'])
-def test_fused_interlaced_binning_matches_stored_mesh(resampler, interlacing, compensate, backend):
+@pytest.mark.parametrize('meshsize', [(32, 40, 36), (24, 20, 200), (264, 256, 180)])
+def test_fused_interlaced_binning_matches_stored_mesh(resampler, interlacing, compensate, backend, meshsize):
     """paint(out='complex') keeps the shifted meshes; its spectrum is binned as the combined
-    mesh is formed (pk_bin_global_interlaced) and must equal binning the stored mesh."""
+    mesh is formed (pk_bin_global_interlaced) and must equal binning the stored mesh.  Meshes:
+    short rows (the flat chunk walk), long rows with per-axis tables in shared memory and in
+    global memory (the staged row kernel for 'jax', the row-run kernel for 'jaxdecomp')."""
     import jaxpower_b200 as jp
     rng = np.random.default_rng(21)
-    meshsize, boxsize = (32, 40, 36), np.array([400., 500., 450.])
+    boxsize = np.array([400., 500., 450.])
     pos = (rng.uniform(-0.5, 0.5, (30000, 3)) * boxsize).astype('f4')
     attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, fft_backend=backend)
     mesh = jp.ParticleField(pos, attrs=attrs).paint(resampler=resampler, interlacing=interlacing,
