@@ -590,13 +590,15 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_firstpoint_kernel(
         const float k2 = __fadd_rn(kxy, kz2);
         bin = bin_from_k2(s.thr, g.nedges, e0, inv_step, k2);
         key = bin | ((int)((i * n1 + j) & 31) << 16);
+        // modes outside the bins (beyond the last edge: the corners of the k cube) are not read
+        const bool inr = bin >= 1 && bin <= nbins;
         float2 F[NT];
 #pragma unroll
-        for (int t = 0; t < NT; ++t) F[t] = __ldcs(f + (int64_t)t * fstride + m);
-        const float2 A = a0[m];
+        for (int t = 0; t < NT; ++t) F[t] = inr ? __ldcs(f + (int64_t)t * fstride + m) : make_float2(0.f, 0.f);
+        const float2 A = inr ? a0[m] : make_float2(0.f, 0.f);
         const float w = mode_weight(g, z);
         if (CROSS) {
-          const float2 B = b0[m];
+          const float2 B = inr ? b0[m] : make_float2(0.f, 0.f);
           v[0] = (B.x * A.x + B.y * A.y) * w;
         } else {
           v[0] = (A.x * A.x + A.y * A.y) * w;
@@ -921,8 +923,9 @@ __global__ void __launch_bounds__(BIN_THREADS, MINB) bin_global_kernel(
   const float e0 = edges[0];
   const float inv_step = g.step > 0.f ? 1.f / g.step : 0.f;
   const int R = (g.d.nz + 31) / 32;
-  const int z0 = lane * R, z1 = min(g.d.nz, z0 + R);
+  const int z0 = lane * R, z1r = min(g.d.nz, z0 + R);
   const bool jaxw = g.backend == PK_BACKEND_JAX;
+  const float thr_last = s.thr[g.nedges - 1];
   // batch of meshes along y: mesh blockIdx.y, its own partial rows
   d1 += (int64_t)blockIdx.y * (NS > 0 ? NS : 1) * g.d.ncomplex();
   if (CROSS) d2 += (int64_t)blockIdx.y * g.d.ncomplex();
@@ -936,6 +939,25 @@ __global__ void __launch_bounds__(BIN_THREADS, MINB) bin_global_kernel(
     const float kx = kcoord(i, g.d.n0, g.kfun[0], false);
     const float ky = kcoord(j, g.d.n1, g.kfun[1], false);
     const float kxy = __fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky));
+    // |k|^2 grows along the stored kz: the modes at or beyond the last edge (no bin) are the
+    // row's tail, cut at the first one; rows beyond it entirely are skipped (warp-uniform)
+    if (!(kxy < thr_last)) continue;
+    int zcut = 0;
+    {
+      int lim = g.d.nz;
+      while (zcut < lim) {
+        const int mid = (zcut + lim) >> 1;
+        float kz2m;
+        if (tab) kz2m = s.kz2[mid];
+        else {
+          const float kzm = kz_coord(g, mid);
+          kz2m = __fmul_rn(kzm, kzm);
+        }
+        if (__fadd_rn(kxy, kz2m) >= thr_last) lim = mid;
+        else zcut = mid + 1;
+      }
+    }
+    const int z1 = min(z1r, zcut);
     const float kl = kx * lx + ky * ly;
     RowFactor<NSR> rf;
     if (NS > 0) row_factor<NSR, FULL, XYM != XY_NONE>(fp, zt, i, j, rf);
@@ -1072,6 +1094,9 @@ __global__ void __launch_bounds__(BIN_THREADS, MINB) bin_global_kernel(
 #endif
 #ifndef PK_STAGED_MIN_CTAS
 #define PK_STAGED_MIN_CTAS 3
+#endif
+#ifndef PK_STAGED_MIN_NZ
+#define PK_STAGED_MIN_NZ 90  // shorter stored rows take bin_global_flat_kernel
 #endif
 constexpr int STAGED_MAX_SHIFTS = 4;
 // shared-memory bytes of one warp's row buffers (power and mu^2, float) for nz modes
@@ -1334,10 +1359,13 @@ __global__ void __launch_bounds__(BIN_THREADS, NS > 0 ? PK_FUSED_MIN_CTAS : 4) b
         const float k2 = __fadd_rn(kxy, s.kz2[z]);
         bin = bin_from_k2(s.thr, g.nedges, e0, inv_step, k2);
         key = bin | ((int)((i * n1 + j) & 31) << 16);
-        const float2 a = NS > 0 ? combine_mode<NSR, FULL>(fp, rf, zt, d1, m, z) : d1[m];
+        // modes outside the bins (beyond the last edge: the corners of the k cube) are not read
+        const bool inr = bin >= 1 && bin <= nbins;
+        const float2 a = !inr ? make_float2(0.f, 0.f)
+                              : (NS > 0 ? combine_mode<NSR, FULL>(fp, rf, zt, d1, m, z) : d1[m]);
         float re, im = 0.f;
         if (CROSS) {
-          const float2 b = d2[m];
+          const float2 b = inr ? d2[m] : make_float2(0.f, 0.f);
           re = a.x * b.x + a.y * b.y;
           im = a.x * b.y - a.y * b.x;
         } else {
@@ -1480,7 +1508,7 @@ static pk_status launch_global(cudaStream_t st, const BinGeom &g, const float2 *
   int blocks = L.blocks;
 #if PK_FUSED_STAGED
   if constexpr (NS > 0 && NS <= STAGED_MAX_SHIFTS && !CROSS && EVEN && !FULL && NV <= 3) {
-    if (g.d.nz >= PK_GLOBAL_FLAT_NZ) {
+    if (g.d.nz >= PK_STAGED_MIN_NZ) {
       // workspace: partial rows, the per-axis tables, the row table
       const size_t xy_off = align_up(L.partial_bytes * nbatch);
       const size_t rows_off = align_up(xy_off + xy_table_bytes(g.d, NS));
