@@ -567,10 +567,22 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_firstpoint_kernel(
     int i = (int)(m / ((int64_t)nz * n1));
     int ic = -1, jc = -1;
     float kx = 0.f, ky = 0.f, kxy = 0.f;
+    const float thr_last = s.thr[g.nedges - 1];
+    auto advance = [&]() {
+      z += 32;
+      while (z >= nz) {
+        z -= nz;
+        if (++j == n1) {
+          j = 0;
+          ++i;
+        }
+      }
+    };
     for (int64_t c = c0; c < c1; ++c, m += 32) {
       const bool valid = m < total;
       float v[NV];
       int key = 0x7fffffff, bin = 0;
+      float kz = 0.f, k2 = INFINITY;
       if (valid) {
         if (i != ic || j != jc) {
           kx = kcoord(i, g.d.n0, g.kfun[0], false);
@@ -579,7 +591,7 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_firstpoint_kernel(
           ic = i;
           jc = j;
         }
-        float kz, kz2;
+        float kz2;
         if (tab) {
           kz = s.kz[z];
           kz2 = s.kz2[z];
@@ -587,18 +599,29 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_firstpoint_kernel(
           kz = kz_coord(g, z);
           kz2 = __fmul_rn(kz, kz);
         }
-        const float k2 = __fadd_rn(kxy, kz2);
+        k2 = __fadd_rn(kxy, kz2);
+      }
+      // a chunk whose modes all lie beyond the last edge adds nothing (warp-uniform skip)
+      if (!__any_sync(0xffffffffu, k2 < thr_last)) {
+        advance();
+        continue;
+      }
+      if (valid) {
         bin = bin_from_k2(s.thr, g.nedges, e0, inv_step, k2);
         key = bin | ((int)((i * n1 + j) & 31) << 16);
         // modes outside the bins (beyond the last edge: the corners of the k cube) are not read
         const bool inr = bin >= 1 && bin <= nbins;
-        float2 F[NT];
+        float2 F[NT], A = make_float2(0.f, 0.f), B = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int t = 0; t < NT; ++t) F[t] = inr ? __ldcs(f + (int64_t)t * fstride + m) : make_float2(0.f, 0.f);
-        const float2 A = inr ? a0[m] : make_float2(0.f, 0.f);
+        for (int t = 0; t < NT; ++t) F[t] = make_float2(0.f, 0.f);
+        if (inr) {
+#pragma unroll
+          for (int t = 0; t < NT; ++t) F[t] = __ldcs(f + (int64_t)t * fstride + m);
+          A = a0[m];
+          if (CROSS) B = b0[m];
+        }
         const float w = mode_weight(g, z);
         if (CROSS) {
-          const float2 B = inr ? b0[m] : make_float2(0.f, 0.f);
           v[0] = (B.x * A.x + B.y * A.y) * w;
         } else {
           v[0] = (A.x * A.x + A.y * A.y) * w;
@@ -635,14 +658,7 @@ __global__ void __launch_bounds__(BIN_THREADS) bin_firstpoint_kernel(
         }
         __syncwarp();
       }
-      z += 32;
-      while (z >= nz) {
-        z -= nz;
-        if (++j == n1) {
-          j = 0;
-          ++i;
-        }
-      }
+      advance();
     }
   }
   bin_smem_flush(s, hist_len, nwarps, partials);
@@ -1341,10 +1357,22 @@ __global__ void __launch_bounds__(BIN_THREADS, NS > 0 ? PK_FUSED_MIN_CTAS : 4) b
     int ic = -1, jc = -1;
     float kxy = 0.f, kl = 0.f;
     RowFactor<NSR> rf;
+    const float thr_last = s.thr[g.nedges - 1];
+    auto advance = [&]() {
+      z += 32;
+      while (z >= nz) {
+        z -= nz;
+        if (++j == n1) {
+          j = 0;
+          ++i;
+        }
+      }
+    };
     for (int64_t c = c0; c < c1; ++c, m += 32) {
       const bool valid = m < total;
       float v[NV];
       int key = 0x7fffffff, bin = 0;
+      float kz = 0.f, k2 = INFINITY;
       if (valid) {
         if (i != ic || j != jc) {
           const float kx = kcoord(i, g.d.n0, g.kfun[0], false);
@@ -1355,17 +1383,26 @@ __global__ void __launch_bounds__(BIN_THREADS, NS > 0 ? PK_FUSED_MIN_CTAS : 4) b
           ic = i;
           jc = j;
         }
-        const float kz = s.kz[z];
-        const float k2 = __fadd_rn(kxy, s.kz2[z]);
+        kz = s.kz[z];
+        k2 = __fadd_rn(kxy, s.kz2[z]);
+      }
+      // a chunk whose modes all lie beyond the last edge adds nothing (warp-uniform skip)
+      if (!__any_sync(0xffffffffu, k2 < thr_last)) {
+        advance();
+        continue;
+      }
+      if (valid) {
         bin = bin_from_k2(s.thr, g.nedges, e0, inv_step, k2);
         key = bin | ((int)((i * n1 + j) & 31) << 16);
         // modes outside the bins (beyond the last edge: the corners of the k cube) are not read
         const bool inr = bin >= 1 && bin <= nbins;
-        const float2 a = !inr ? make_float2(0.f, 0.f)
-                              : (NS > 0 ? combine_mode<NSR, FULL>(fp, rf, zt, d1, m, z) : d1[m]);
+        float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
+        if (inr) {
+          a = NS > 0 ? combine_mode<NSR, FULL>(fp, rf, zt, d1, m, z) : d1[m];
+          if (CROSS) b = d2[m];
+        }
         float re, im = 0.f;
         if (CROSS) {
-          const float2 b = inr ? d2[m] : make_float2(0.f, 0.f);
           re = a.x * b.x + a.y * b.y;
           im = a.x * b.y - a.y * b.x;
         } else {
@@ -1429,14 +1466,7 @@ __global__ void __launch_bounds__(BIN_THREADS, NS > 0 ? PK_FUSED_MIN_CTAS : 4) b
         }
         __syncwarp();
       }
-      z += 32;
-      while (z >= nz) {
-        z -= nz;
-        if (++j == n1) {
-          j = 0;
-          ++i;
-        }
-      }
+      advance();
     }
   }
   __syncthreads();  // warp partials (float32) finished in float64, in warp order
