@@ -224,6 +224,32 @@ def test_fused_interlaced_binning_matches_stored_mesh(resampler, interlacing, co
         assert np.allclose(fused.get(ell).num_raw, stored.get(ell).num_raw, rtol=0, atol=1e-6 * scale), ell
 
 
+@pytest.mark.parametrize('ells', [(0,), (2,), (0, 4), (4, 2, 0)])
+@pytest.mark.parametrize('edges', ['step', 'irregular'])
+def test_fused_staged_binning_ells_and_edges(ells, edges):
+    """The staged fused pass (long stored rows, 'jax' layout) for other even multipole sets
+    (no monopole: the k = 0 mode adds nothing) and non-uniform edges that stop below k_Nyq
+    (rows cut early), against binning the stored combined mesh."""
+    import jaxpower_b200 as jp
+    rng = np.random.default_rng(23)
+    meshsize, boxsize = (40, 36, 192), np.array([400., 360., 960.])
+    pos = (rng.uniform(-0.5, 0.5, (60000, 3)) * boxsize).astype('f4')
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize)
+    mesh = jp.ParticleField(pos, attrs=attrs).paint(resampler='tsc', interlacing=3, compensate=True, out='complex')
+    if edges == 'step':
+        e = {'step': 0.015}
+    else:
+        e = np.concatenate([[0.], np.cumsum(rng.uniform(0.01, 0.03, 20))])
+        e = e[e < 0.45]
+    b = jp.BinMesh2SpectrumPoles(attrs, edges=e, ells=ells)
+    fused = jp.compute_mesh2_spectrum(mesh, bin=b, los='z')
+    assert mesh.lazy is not None
+    stored = jp.compute_mesh2_spectrum(jp.ComplexMeshField(mesh.value, attrs=attrs), bin=b, los='z')
+    scale = max(np.abs(stored.get(ell).num_raw).max() for ell in ells)
+    for ell in ells:
+        assert np.allclose(fused.get(ell).num_raw, stored.get(ell).num_raw, rtol=0, atol=1e-6 * scale), ell
+
+
 def test_uniform_ids_match_oracle():
     """pk_uniform_ids: the per-id uniforms of create_sharded_random((seed, ids)) (x64), and the
     whole-array draw of an integer seed, bit for bit against the oracle's Threefry."""
