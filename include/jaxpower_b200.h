@@ -217,6 +217,24 @@ pk_status pk_bin_separation_global(void *stream, const float *value, const int32
                                    int nedges, float step, int nells, const int32_t *ells,
                                    double *d_out, void *workspace, size_t workspace_bytes);
 
+/* Spherical-Bessel basis of BinMesh2CorrelationPoles (basis='bessel', mesh2.py:169-181),
+ * for the estimators of compute_mesh2_correlation (mesh2.py:414-500): per separation bin b
+ * (s_b = d_sep[b], float64, the bins' xavg) and multipole ells[l] the float64 sum over the
+ * stored modes (each once, no Hermitian weight) of Re(A_l(k)) j_ell(|k| s_b), |k| and
+ * |k| s_b in float32, j_ell in float64.  A_l is |d1|^2 or conj(d1) d2 times L_ell(mu)
+ * (los given, ell <= 4), or, with los NULL (first point), |A0|^2 / conj(B0) A0 for ell 0
+ * (d1 = A0, d2 = B0 or NULL; when include_ell0) and conj(sum_t F_t Y_t(khat)) A0 over this
+ * call's terms (f: nterms half-complex meshes) for ell > 0; k = 0 is dropped for ell > 0.
+ * klimit (NULL: none): only klimit[0] <= |k| < klimit[1].  d_out: (nells, nbins), written or,
+ * with accumulate, added to; multiply by (-1)^(ell/2) / N and the estimator's factor.
+ * nbins <= 1024, nells <= 5.  Workspace from pk_bin_bessel_workspace_size. */
+pk_status pk_bin_bessel_workspace_size(const int32_t meshsize[3], int nbins, int nells, size_t *bytes);
+pk_status pk_bin_bessel(void *stream, const void *d1, const void *d2, const void *f, int nterms,
+                        const int32_t *term_ell, const int32_t *term_m, const int32_t meshsize[3],
+                        const float kfun[3], int backend, const float *los, const double *d_sep, int nbins,
+                        const float *klimit, int nells, const int32_t *ells, int include_ell0,
+                        int accumulate, double *d_out, void *workspace, size_t workspace_bytes);
+
 /* Window matrix of the global line-of-sight power spectrum, mesh input power
  * (compute_mesh2_spectrum_window, mesh2.py:1013-1133).  'jax' (rfftn) layout only.
  *
@@ -373,7 +391,9 @@ pk_status pk_bin_global_adjoint(void *stream, const void *delta, const int32_t m
                                 void *workspace, size_t workspace_bytes);
 
 /* Backward of pk_bin_firstpoint (auto): cotangents of A0 (written or accumulated) and
- * of each F_j of the batch (out_f[j]). */
+ * of each F_j of the batch (out_f[j]).  Even ells bin Re(conj(S) A0), odd ells
+ * Im(conj(S) A0) (mesh2.py:334).  for_c2r = 2 converts the F_j cotangents for C2R but
+ * leaves the A0 cotangent as the conjugate cotangent of a complex input mesh. */
 pk_status pk_bin_firstpoint_adjoint(void *stream, const void *a0, const void *f, int nterms,
                                     const int32_t *term_ell, const int32_t *term_m,
                                     const int32_t meshsize[3], const float kfun[3],
@@ -389,6 +409,13 @@ pk_status pk_bin_firstpoint_adjoint(void *stream, const void *a0, const void *f,
  * are the cotangents of the painted shifted meshes. */
 pk_status pk_interlace_adjoint(void *stream, const void *in, int from_real, int nshifts,
                                const int32_t meshsize[3], int comp_order, int backend, void *out);
+
+/* Backward of the normalised C2R (jnp.fft.irfftn, mesh.py:1699-1719) of a Hermitian
+ * half-mesh: out (+)= R w_z / (N0 N1 N2), R = rfftn(rho_bar), w_z = 2 off the kz = 0 and
+ * kz = N2/2 planes, 1 on them: the conjugate cotangent of the complex mesh.  No
+ * reference counterpart (JAX transposes its FFTs itself). */
+pk_status pk_c2r_adjoint(void *stream, const void *r, const int32_t meshsize[3], int accumulate,
+                         void *out);
 
 /* Backward of pk_ylm_premultiply: rho_bar += sum_j r_j Y_j(xhat). */
 pk_status pk_ylm_accumulate(void *stream, const float *r, const int32_t meshsize[3],

@@ -2443,9 +2443,16 @@ __device__ __forceinline__ void fp_adj_mode(const AdjGeom &a, const FPAdj &t, co
       const float G = w * coef[(size_t)l * a.nbins + (b - 1)];
       const float y = ylm_eval(t.term_ell[q], t.term_m[q], xh, yh, zh);
       const float2 F = f[(int64_t)q * stride + idx];
-      acc.x += G * y * F.x;  // d/dA0 of G Re(conj(S) A0) = G S
-      acc.y += G * y * F.y;
-      gf[q] = make_float2(G * y * A.x, G * y * A.y);  // d/dF of G Re(S conj(A0)) = G Y A0
+      const float gy = G * y;
+      if (t.term_ell[q] & 1) {  // odd ell bins Im(conj(S) A0) = Re(conj(i S) A0) = Re(S conj(-i A0))
+        acc.x -= gy * F.y;      // d/dA0 = G i S
+        acc.y += gy * F.x;
+        gf[q] = make_float2(gy * A.y, -gy * A.x);  // d/dF = G Y (-i A0)
+      } else {
+        acc.x += gy * F.x;  // d/dA0 of G Re(conj(S) A0) = G S
+        acc.y += gy * F.y;
+        gf[q] = make_float2(gy * A.x, gy * A.y);  // d/dF of G Re(S conj(A0)) = G Y A0
+      }
     }
   *ga0 = acc;
 }
@@ -2472,11 +2479,11 @@ __global__ void firstpoint_adjoint_kernel(AdjGeom a, FPAdj t, const float *__res
         float2 ga0m;
         fp_adj_mode(a, t, thr, coef, a0, f, (g.d.n0 - i) % g.d.n0, (g.d.n1 - j) % g.d.n1, z,
                     &ga0m, gfm);
-        ga0 = make_float2(0.5f * (ga0.x + ga0m.x), 0.5f * (ga0.y - ga0m.y));
+        if (a.for_c2r == 1) ga0 = make_float2(0.5f * (ga0.x + ga0m.x), 0.5f * (ga0.y - ga0m.y));
         for (int q = 0; q < t.nterms; ++q)
           gf[q] = make_float2(0.5f * (gf[q].x + gfm[q].x), 0.5f * (gf[q].y - gfm[q].y));
       } else {
-        ga0 = make_float2(0.5f * ga0.x, 0.5f * ga0.y);
+        if (a.for_c2r == 1) ga0 = make_float2(0.5f * ga0.x, 0.5f * ga0.y);
         for (int q = 0; q < t.nterms; ++q) gf[q] = make_float2(0.5f * gf[q].x, 0.5f * gf[q].y);
       }
     }
@@ -2502,11 +2509,17 @@ template <int ELL, int M, int T, int NT>
 __device__ __forceinline__ void fp_adj_terms(float G, float x, float y, float z, float2 A,
                                              const float2 *__restrict__ f, int64_t stride, int64_t idx,
                                              float2 &acc, float2 (&gf)[NT]) {
-  const float yv = ylm_eval(ELL, M, x, y, z);
+  const float gy = G * ylm_eval(ELL, M, x, y, z);
   const float2 F = f[(int64_t)T * stride + idx];
-  acc.x += G * yv * F.x;  // d/dA0 of G Re(conj(S) A0) = G S
-  acc.y += G * yv * F.y;
-  gf[T] = make_float2(G * yv * A.x, G * yv * A.y);  // d/dF of G Re(S conj(A0)) = G Y A0
+  if constexpr (ELL & 1) {  // odd ell: Im(conj(S) A0); d/dA0 = G i S, d/dF = G Y (-i A0)
+    acc.x -= gy * F.y;
+    acc.y += gy * F.x;
+    gf[T] = make_float2(gy * A.y, -gy * A.x);
+  } else {
+    acc.x += gy * F.x;  // d/dA0 of G Re(conj(S) A0) = G S
+    acc.y += gy * F.y;
+    gf[T] = make_float2(gy * A.x, gy * A.y);  // d/dF of G Re(S conj(A0)) = G Y A0
+  }
   if constexpr (M < ELL) fp_adj_terms<ELL, M + 1, T + 1>(G, x, y, z, A, f, stride, idx, acc, gf);
 }
 
@@ -2578,11 +2591,11 @@ __global__ void __launch_bounds__(256) firstpoint_adjoint_block_kernel(
         float2 ga0m, gfm[NT];
         fp_adj_block_mode<MASK>(a, r, thr, coef, a0, f, (g.d.n0 - i) % g.d.n0, (g.d.n1 - j) % g.d.n1, z, ga0m,
                                 gfm);
-        ga0 = make_float2(0.5f * (ga0.x + ga0m.x), 0.5f * (ga0.y - ga0m.y));
+        if (a.for_c2r == 1) ga0 = make_float2(0.5f * (ga0.x + ga0m.x), 0.5f * (ga0.y - ga0m.y));
 #pragma unroll
         for (int q = 0; q < NT; ++q) gf[q] = make_float2(0.5f * (gf[q].x + gfm[q].x), 0.5f * (gf[q].y - gfm[q].y));
       } else {
-        ga0 = make_float2(0.5f * ga0.x, 0.5f * ga0.y);
+        if (a.for_c2r == 1) ga0 = make_float2(0.5f * ga0.x, 0.5f * ga0.y);
 #pragma unroll
         for (int q = 0; q < NT; ++q) gf[q] = make_float2(0.5f * gf[q].x, 0.5f * gf[q].y);
       }

@@ -76,6 +76,26 @@ __global__ void scale_kernel(float *__restrict__ x, int64_t n, float s) {
     x[i] *= s;
 }
 
+// Transpose of the normalised C2R: out (+)= r w_z / N, w_z = 2 off the self-conjugate kz planes.
+__global__ void c2r_adjoint_kernel(Dims d, const float2 *__restrict__ r, int accumulate, float inv_n,
+                                   float2 *__restrict__ out) {
+  const int64_t total = d.ncomplex();
+  const bool even = (d.n2 % 2) == 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int z = (int)(i % d.nz);
+    const float s = (z == 0 || (even && z == d.nz - 1)) ? inv_n : 2.f * inv_n;
+    float2 v = r[i];
+    v.x *= s;
+    v.y *= s;
+    if (accumulate) {
+      const float2 o = out[i];
+      v.x += o.x;
+      v.y += o.y;
+    }
+    out[i] = v;
+  }
+}
+
 struct YlmTerms {
   int n;
   int ell[32];
@@ -334,6 +354,18 @@ extern "C" pk_status pk_scale_real(void *stream, float *mesh, int64_t size, floa
   PK_REQUIRE(mesh || size == 0, PK_ERR_INVALID, "null mesh");
   if (size == 0) return PK_OK;
   scale_kernel<<<grid_for(size, 256), 256, 0, (cudaStream_t)stream>>>(mesh, size, scale);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+extern "C" pk_status pk_c2r_adjoint(void *stream, const void *r, const int32_t meshsize[3], int accumulate,
+                                    void *out) {
+  PK_REQUIRE(r && out, PK_ERR_INVALID, "null pointer");
+  Dims d;
+  PK_REQUIRE(make_dims(meshsize, &d), PK_ERR_INVALID, "invalid meshsize");
+  const int64_t total = d.ncomplex();
+  c2r_adjoint_kernel<<<grid_for(total, 256), 256, 0, (cudaStream_t)stream>>>(
+      d, (const float2 *)r, accumulate, (float)(1.0 / (double)d.nreal()), (float2 *)out);
   PK_LAUNCH_CHECK();
   return PK_OK;
 }

@@ -99,6 +99,11 @@ SIGNATURES = {
                                   c_float_p, c_void_p, c_int, c_float, c_float, c_int, c_int, c_int32_p,
                                   c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_size_t],
     'pk_interlace_adjoint': [c_void_p, c_void_p, c_int, c_int, c_int32_p, c_int, c_int, c_void_p],
+    'pk_c2r_adjoint': [c_void_p, c_void_p, c_int32_p, c_int, c_void_p],
+    'pk_bin_bessel_workspace_size': [c_int32_p, c_int, c_int, ctypes.POINTER(c_size_t)],
+    'pk_bin_bessel': [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int32_p, c_int32_p, c_int32_p, c_float_p,
+                      c_int, c_float_p, c_void_p, c_int, c_float_p, c_int, c_int32_p, c_int, c_int, c_void_p,
+                      c_void_p, c_size_t],
     'pk_ylm_accumulate': [c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_int, c_int32_p, c_int32_p,
                           c_void_p],
     'pk_ylm_premultiply': [c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_int, c_int32_p,

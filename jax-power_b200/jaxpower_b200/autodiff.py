@@ -94,7 +94,7 @@ class _Spectrum(torch.autograd.Function):
         is_complex = value.is_complex()
         _, vlos, _ = _los(los)
         # first point: A0 and the transformed Y_lm-weighted meshes stay resident for backward
-        keep = {} if (vlos is None and not is_complex and ctx.needs_input_grad[0]) else None
+        keep = {} if (vlos is None and ctx.needs_input_grad[0]) else None
         raw = _spectrum_sums(attrs, bin, los, rmesh=None if is_complex else value.detach(),
                              cmesh=value.detach() if is_complex else None, keep=keep)
         ctx.keep = keep
@@ -110,10 +110,12 @@ class _Spectrum(torch.autograd.Function):
         attrs, bin, los, factors, nmodes = ctx.cfg
         meshsize = attrs.meshsize
         ells = bin.ells
-        if any(ell % 2 for ell in ells):
-            raise NotImplementedError('gradients of odd multipoles are not implemented')
-        coef = (grad * factors[:, None] / nmodes).to(torch.float32).contiguous()
         _, vlos, swap = _los(los)
+        coef = grad * factors[:, None] / nmodes
+        if swap:  # the end-point estimator conjugates: odd multipoles (imaginary parts) change sign
+            sign = torch.tensor([-1. if ell % 2 else 1. for ell in ells], dtype=coef.dtype, device=coef.device)
+            coef = coef * sign[:, None]
+        coef = coef.to(torch.float32).contiguous()
         is_complex = value.is_complex()
         nbytes = _lib.c_size_t()
         _lib.call('pk_adjoint_workspace_size', len(bin._edges1d), _lib.ctypes.byref(nbytes))
@@ -130,12 +132,15 @@ class _Spectrum(torch.autograd.Function):
             if is_complex:
                 return out, None, None, None
             return _c2r_unnormalised(out, meshsize), None, None, None
-        if is_complex:
-            raise NotImplementedError('first-point gradients are implemented for real meshes')
-        rho = value.detach().contiguous()
+        # a complex input V enters twice: as A0 itself and through rho = irfftn(V) in the Y_lm products
+        rho = (_c2r(value.detach(), meshsize) if is_complex else value.detach()).contiguous()
         keep = ctx.keep if ctx.keep else {}
         ctx.keep = None
-        A0 = keep['A0'] if 'A0' in keep else _r2c(rho, meshsize).contiguous()
+        if 'A0' in keep:
+            A0 = keep['A0']
+        else:
+            A0 = value.detach().contiguous() if is_complex else _r2c(rho, meshsize).contiguous()
+        a0_mode = 2 if is_complex else 1  # 2: the A0 cotangent stays the complex mesh's own
         ga0 = torch.zeros_like(A0)
         rho_bar = torch.zeros_like(rho)
         terms = _firstpoint_terms(ells)
@@ -143,7 +148,7 @@ class _Spectrum(torch.autograd.Function):
         if not terms:
             _lib.call('pk_bin_firstpoint_adjoint', stream, _lib.ptr(A0), None, 0, None, None, *common,
                       _lib.ptr(bin.d_edges), len(bin._edges1d), bin._step, edge0, attrs.backend_code, len(ells),
-                      _lib.i32(ells), _lib.ptr(coef), 1, _lib.ptr(ga0), 0, None, _lib.ptr(ws), ws.numel())
+                      _lib.i32(ells), _lib.ptr(coef), a0_mode, _lib.ptr(ga0), 0, None, _lib.ptr(ws), ws.numel())
         coef_rest = coef.clone()  # ell = 0 enters the A0 cotangent once, with the first batch
         for l, ell in enumerate(ells):
             if ell == 0:
@@ -165,12 +170,16 @@ class _Spectrum(torch.autograd.Function):
             gf = torch.empty_like(F)
             _lib.call('pk_bin_firstpoint_adjoint', stream, _lib.ptr(A0), _lib.ptr(F), nt, _lib.i32(t_ell),
                       _lib.i32(t_m), *common, _lib.ptr(bin.d_edges), len(bin._edges1d), bin._step, edge0,
-                      attrs.backend_code, len(ells), _lib.i32(ells), _lib.ptr(coef if ib == 0 else coef_rest), 1,
+                      attrs.backend_code, len(ells), _lib.i32(ells), _lib.ptr(coef if ib == 0 else coef_rest), a0_mode,
                       _lib.ptr(ga0), 1, _lib.ptr(gf), _lib.ptr(ws), ws.numel())
             del F
             r = _c2r_unnormalised(gf, meshsize)
             _lib.call('pk_ylm_accumulate', stream, _lib.ptr(r), _lib.i32(meshsize), _lib.f32(attrs.cellsize),
                       _lib.f32(offset), nt, _lib.i32(t_ell), _lib.i32(t_m), _lib.ptr(rho_bar))
+        if is_complex:  # dL/dV = dL/dA0 + irfftn^T(rho_bar)
+            _lib.call('pk_c2r_adjoint', stream, _lib.ptr(_r2c(rho_bar, meshsize)), _lib.i32(meshsize), 1,
+                      _lib.ptr(ga0))
+            return ga0, None, None, None
         rho_bar += _c2r_unnormalised(ga0, meshsize)
         return rho_bar, None, None, None
 

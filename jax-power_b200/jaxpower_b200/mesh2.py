@@ -182,7 +182,12 @@ class BinMesh2CorrelationPoles:
     mattrs : MeshAttrs or mesh field
     edges : array, dict ('min', 'max' (default cellsize * min(meshsize) / 2), 'step') or None
     ells : int or tuple
-    mode_oversampling : only 0; basis : only the default (configuration-space) binning
+    mode_oversampling : only 0
+    basis : None (bins of |s| on the separation grid) or 'bessel': the estimator's Fourier-space
+        mode values projected on j_ell(|k| s) at each bin's mean separation (``mesh2.py:169-181``;
+        ``pk_bin_bessel``)
+    klimit : None, True ((0, k_Nyq)) or (kmin, kmax): modes kept in the Bessel projection
+    batch_size : accepted for the reference's signature (its ``lax.map`` batching); unused
     """
 
     def __init__(self, mattrs, edges=None, ells=0, mode_oversampling=0, basis=None, klimit=None, batch_size=None):
@@ -190,11 +195,15 @@ class BinMesh2CorrelationPoles:
             mattrs = mattrs.attrs
         if mode_oversampling:
             raise NotImplementedError('mode_oversampling > 0 is not supported on the GPU path')
-        if basis == 'bessel':
-            raise NotImplementedError("basis='bessel' is not supported on the GPU path")
+        if basis not in (None, 'bessel'):
+            raise ValueError('unknown basis {}'.format(basis))
         self.mattrs = mattrs
         self.ells = _format_ells(ells)
         self.basis = basis
+        if isinstance(klimit, bool):
+            klimit = (0., float(np.min(mattrs.knyq))) if klimit else None
+        self.klimit = None if klimit is None else tuple(float(k) for k in klimit)
+        self.batch_size = batch_size
         vec0 = np.float32(mattrs.cellsize.min())
         if edges is None:
             edges = {}
@@ -288,6 +297,9 @@ def compute_mesh2_correlation(*meshes, bin=None, los='z'):
     def _r(mesh):
         return mesh.value if isinstance(mesh, RealMeshField) else _c2r(mesh.value, meshsize)
 
+    if bin.basis == 'bessel':
+        return _bessel_correlation(meshes, auto, bin, los_name, vlos, swap, norm_value)
+
     if vlos is None:  # first point (end point: the meshes swapped), mesh2.py:414-463
         if swap and not auto:
             meshes = meshes[::-1]
@@ -346,6 +358,85 @@ def compute_mesh2_correlation(*meshes, bin=None, los='z'):
     poles = []
     for i, ell in enumerate(ells):
         num = raw[i] / bin.nmodes * factors[i]
+        poles.append(Mesh2CorrelationPole(s=bin.xavg, s_edges=bin.edges, nmodes=bin.nmodes, num_raw=num / cellvol,
+                                          norm=norm, volume=cellvol * bin.nmodes, ell=ell, attrs=attrs))
+    return Mesh2CorrelationPoles(poles)
+
+
+def _bessel_correlation(meshes, auto, bin, los_name, vlos, swap, norm_value):
+    """compute_mesh2_correlation with ``bin.basis == 'bessel'`` (``mesh2.py:414-500``).
+
+    The estimator's mode values stay in Fourier space: |delta|^2 (or conj(delta1) delta2)
+    times L_ell(mu_k) for a fixed line of sight, |A0|^2 and conj(sum_m F_lm Y_lm(khat)) A0
+    for the first point; ``pk_bin_bessel`` projects their real parts on j_ell(|k| s) at
+    each bin's ``xavg`` (``mesh2.py:169-177``).  num_raw = factor (-1)^(ell/2) sums / N / V_cell,
+    factor 1 for ell = 0, 2 ell + 1 (fixed los) or 4 pi (first point) otherwise; no division
+    by the bin counts.
+    """
+    mattrs = bin.mattrs
+    meshsize = mattrs.meshsize
+    ells = bin.ells
+    stream = _lib.stream_handle()
+
+    def _c(mesh):
+        return mesh.value if isinstance(mesh, ComplexMeshField) else _r2c(mesh.value, meshsize)
+
+    def _r(mesh):
+        return mesh.value if isinstance(mesh, RealMeshField) else _c2r(mesh.value, meshsize)
+
+    nbins = bin.nbins
+    sep = torch.as_tensor(np.asarray(bin.xavg, dtype="f8"), device=_device())
+    nbytes = _lib.c_size_t()
+    _lib.call('pk_bin_bessel_workspace_size', _lib.i32(meshsize), nbins, len(ells), _lib.ctypes.byref(nbytes))
+    ws = _workspace(nbytes.value)
+    out = torch.zeros(len(ells) * nbins, dtype=torch.float64, device=_device())
+    klimit = None if bin.klimit is None else _lib.f32(bin.klimit)
+    common = (_lib.i32(meshsize), _lib.f32(mattrs.kfun), mattrs.backend_code)
+
+    def project(d1, d2, F, terms, los, include_ell0, accumulate):
+        t_ell = _lib.i32([t[0] for t in terms]) if terms else None
+        t_m = _lib.i32([t[1] for t in terms]) if terms else None
+        _lib.call('pk_bin_bessel', stream, _lib.ptr(d1), _lib.ptr(d2), _lib.ptr(F), len(terms), t_ell, t_m, *common,
+                  None if los is None else _lib.f32(los), _lib.ptr(sep), nbins, klimit, len(ells), _lib.i32(ells),
+                  int(include_ell0), int(accumulate), _lib.ptr(out), _lib.ptr(ws), ws.numel())
+
+    if vlos is None:
+        if swap and not auto:
+            meshes = meshes[::-1]
+        A0 = _c(meshes[0] if auto else meshes[1]).contiguous()
+        B0 = None if auto else _c(meshes[0]).contiguous()
+        project(A0, B0, None, [], None, 0 in ells, False)
+        terms = _firstpoint_terms(ells)
+        if terms:
+            rho = _r(meshes[0]).contiguous()
+            offset = (mattrs.boxcenter - (mattrs.boxsize / np.float32(2.)).astype('f4')).astype('f4')
+            batch = _term_batch(mattrs, len(terms))
+            for start in range(0, len(terms), batch):
+                chunk = terms[start:start + batch]
+                nt = len(chunk)
+                real = torch.empty((nt,) + tuple(int(n) for n in meshsize), dtype=torch.float32, device=rho.device)
+                _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rho), _lib.i32(meshsize), _lib.f32(mattrs.cellsize),
+                          _lib.f32(offset), nt, _lib.i32([t[0] for t in chunk]), _lib.i32([t[1] for t in chunk]),
+                          _lib.ptr(real))
+                F = _r2c(real, meshsize)
+                del real
+                project(A0, None, F, chunk, None, False, True)
+                del F
+        factors = [1. if ell == 0 else 4. * np.pi for ell in ells]
+        attrs = dict(los=los_name)
+    else:
+        d1 = _c(meshes[0]).contiguous()
+        d2 = None if auto else _c(meshes[1]).contiguous()
+        project(d1, d2, None, [], vlos, True, False)
+        factors = [1. if ell == 0 else 2. * ell + 1. for ell in ells]
+        attrs = dict(los=vlos)
+    raw = out.reshape(len(ells), nbins).cpu().numpy()
+    cellvol = float(np.prod(mattrs.cellsize.astype('f8')))
+    nmesh = float(np.prod(meshsize.astype('f8')))
+    norm = np.full(nbins, norm_value, dtype='f8')
+    poles = []
+    for i, ell in enumerate(ells):
+        num = raw[i] * factors[i] * (-1.) ** (ell // 2) / nmesh
         poles.append(Mesh2CorrelationPole(s=bin.xavg, s_edges=bin.edges, nmodes=bin.nmodes, num_raw=num / cellvol,
                                           norm=norm, volume=cellvol * bin.nmodes, ell=ell, attrs=attrs))
     return Mesh2CorrelationPoles(poles)

@@ -1158,3 +1158,94 @@ def compute_mesh2_correlation_firstpoint(mesh, bins, mesh2=None, swap=False):
             carry = (carry + c2r(geom, np.conj(F) * A0) * Y(*svec)).astype(dt)
         out.append(4. * np.pi * bins(carry, remove_zero=True) / cellvol)
     return {'num_raw': np.array(out), 'nmodes': bins.nmodes, 'xavg': bins.xavg}
+
+
+def spherical_jn(ell, x):
+    """``get_spherical_jn(ell)`` (``utils.py:443-450``) in float64: the closed form for x > 0.1
+    (``utils.py:419-440``; evaluated by scipy's spherical Bessel function, the same function)
+    and, for x <= 0.1, its Taylor series x^l / (2l+1)!! sum_k (-x^2/2)^k / (k! (2l+3)...(2l+2k+1))
+    through x^(l+10), the terms the reference keeps."""
+    from scipy import special
+    x = np.asarray(x, dtype='f8')
+    out = np.empty_like(x)
+    hi = x > 0.1
+    out[hi] = special.spherical_jn(ell, x[hi])
+    xl = x[~hi]
+    lead = xl**ell / np.prod(np.arange(1, 2 * ell + 2, 2, dtype='f8'))
+    term, total = lead.copy(), lead.copy()
+    for k in range(5):
+        term = term * (-0.5 * xl * xl) / ((k + 1) * (2 * ell + 2 * k + 3))
+        total = total + term
+    out[~hi] = total
+    return out
+
+
+def compute_mesh2_correlation_bessel(mesh, bins, los='z', mesh2=None, klimit=None):
+    """``compute_mesh2_correlation`` with ``BinMesh2CorrelationPoles(basis='bessel')``
+    (``mesh2.py:169-177`` and the 'bessel' branches of ``mesh2.py:414-500``).
+
+    The estimator's Fourier-space mode values A_ell (fixed los: |d1|^2 or conj(d1) d2 times
+    L_ell(mu); first point: |A0|^2 and conj(sum_m r2c(rho Y_lm(xhat)) Y_lm(khat)) A0), k = 0
+    dropped for ell > 0, projected as (-1)^(ell//2) sum_k Re(A_ell) j_ell(|k| s_b) / N over
+    the stored half-complex modes (no Hermitian weight), s_b = xavg; |k| and |k| s_b in the
+    geometry's dtype, j_ell in float64; times 1, 2 ell + 1 or 4 pi; num_raw = / V_cell.
+    """
+    geom = bins.geom
+    dt = geom.dtype
+    t = dt.type
+    kx, ky, kz = kcoords(geom)
+    k2 = (((t(0.) + kx * kx).astype(dt) + ky * ky).astype(dt) + kz * kz).astype(dt)
+    knorm = np.sqrt(k2).astype(dt)
+    sep = np.asarray(bins.xavg).astype(dt)
+    mask = 1.
+    if klimit is not None:
+        mask = ((knorm >= t(klimit[0])) & (knorm < t(klimit[1]))).astype('f8')
+    nmesh = float(np.prod(geom.meshsize.astype('f8')))
+    cellvol = float(np.prod(geom.cellsize.astype('f8')))
+
+    def project(value, ell):
+        value = np.real(value).astype('f8') * mask
+        out = np.empty(len(sep))
+        for b, s in enumerate(sep):
+            x = (knorm * s).astype(dt)
+            out[b] = np.sum(value * spherical_jn(ell, x))
+        return (-1.)**(ell // 2) * out / nmesh
+
+    out = []
+    if isinstance(los, str) and los in ('firstpoint', 'local', 'endpoint'):
+        swap = los == 'endpoint'
+        m1, m2 = (mesh2, mesh) if (swap and mesh2 is not None) else (mesh, mesh2)
+        A0 = _to_complex(geom, m1 if m2 is None else m2)
+        rho = _to_real(geom, m1)
+        xvec = rcoords(geom)
+        kvec = (kx, ky, kz)
+        for ell in bins.ells:
+            if ell == 0:
+                A = (A0.real**2 + A0.imag**2).astype(dt) if m2 is None else np.conj(_to_complex(geom, m1)) * A0
+                out.append(project(A, 0))
+                continue
+            carry = np.zeros(geom.cshape, dtype=A0.dtype)
+            for m in range(-ell, ell + 1):
+                Y = get_ylm(ell, m)
+                F = r2c(geom, (rho * Y(*xvec)).astype(dt))
+                carry = (carry + F * Y(*kvec)).astype(A0.dtype)
+            A = np.conj(carry) * A0
+            A[0, 0, 0] = 0.
+            out.append(4. * np.pi * project(A, ell))
+    else:
+        vlos = {'x': (1., 0., 0.), 'y': (0., 1., 0.), 'z': (0., 0., 1.)}[los] if isinstance(los, str) else los
+        d1 = _to_complex(geom, mesh)
+        A = (d1.real**2 + d1.imag**2).astype(dt) if mesh2 is None else np.conj(d1) * _to_complex(geom, mesh2)
+        kl = [(kk * t(ll)).astype(dt) for kk, ll in zip((kx, ky, kz), vlos)]
+        mu_num = (((t(0.) + kl[0]).astype(dt) + kl[1]).astype(dt) + kl[2]).astype(dt)
+        kn = knorm.copy()
+        kn[0, 0, 0] = 1.
+        mu = (mu_num / kn).astype(dt)
+        for ell in bins.ells:
+            if ell == 0:
+                out.append(project(A, 0))
+                continue
+            value = A * legendre(ell, mu)
+            value[0, 0, 0] = 0.
+            out.append((2 * ell + 1) * project(value, ell))
+    return {'num_raw': np.array(out) / cellvol, 'nmodes': bins.nmodes, 'xavg': bins.xavg}

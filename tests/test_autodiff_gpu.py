@@ -31,17 +31,26 @@ def _oracle_loss(pos, w, meshsize, boxsize, boxcenter, resampler, interlacing, c
     return float(np.sum(coef * r['num_raw']))
 
 
-@pytest.mark.parametrize('resampler,interlacing,compensate,out,los', [
-    ('tsc', 3, True, 'real', 'z'),
-    ('tsc', 2, False, 'complex', 'x'),
-    ('pcs', 1, True, 'real', 'z'),
-    ('cic', 0, False, 'real', 'z'),
-    ('tsc', 3, True, 'real', 'firstpoint'),
+@pytest.mark.parametrize('resampler,interlacing,compensate,out,los,ells', [
+    ('tsc', 3, True, 'real', 'z', (0, 2, 4)),
+    ('tsc', 2, False, 'complex', 'x', (0, 2, 4)),
+    ('pcs', 1, True, 'real', 'z', (0, 2, 4)),
+    ('cic', 0, False, 'real', 'z', (0, 2, 4)),
+    ('tsc', 3, True, 'real', 'firstpoint', (0, 2, 4)),
+    # odd multipoles: zero for a global line of sight (auto spectrum), imaginary parts for a
+    # local one, with the sign of the end-point conjugation
+    ('cic', 2, True, 'real', 'z', (0, 1, 2, 3)),
+    ('tsc', 2, True, 'real', 'firstpoint', (0, 1, 2, 3)),
+    ('tsc', 2, False, 'real', 'endpoint', (1, 3)),
+    # a complex input mesh to the first-point estimator: A0 itself and irfftn of it
+    ('tsc', 2, True, 'complex', 'firstpoint', (0, 2, 4)),
+    ('cic', 3, False, 'complex', 'endpoint', (0, 1, 2)),
 ])
-def test_position_gradient_vs_finite_differences(resampler, interlacing, compensate, out, los):
+def test_position_gradient_vs_finite_differences(resampler, interlacing, compensate, out, los, ells):
     import jaxpower_b200 as jp
     from jaxpower_b200.autodiff import paint_value, spectrum_value
-    meshsize, boxsize, boxcenter, step, ells = 16, 200., (0. if los != 'firstpoint' else 300.), 0.05, (0, 2, 4)
+    local = los in ('firstpoint', 'endpoint')
+    meshsize, boxsize, boxcenter, step = 16, 200., (300. if local else 0.), 0.05
     pos, w = _setup(meshsize=meshsize, boxsize=boxsize, boxcenter=boxcenter)
     attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=boxcenter)
     bins = jp.BinMesh2SpectrumPoles(attrs, edges={'step': step}, ells=ells)
@@ -60,6 +69,7 @@ def test_position_gradient_vs_finite_differences(resampler, interlacing, compens
     assert np.isclose(float(loss), ref, rtol=1e-4)
     h = 1e-3 * boxsize / meshsize
     scale = np.abs(gpos).max()
+    assert scale > 0.
     for p in (0, 7, 123, 311):
         for d in range(3):
             pp, pm = pos.astype('f8').copy(), pos.astype('f8').copy()

@@ -110,3 +110,41 @@ def test_correlation_ref_golden_gpu():
     for los, expected in gc['value_std'].items():
         value = jp.compute_mesh2_correlation(mesh, bin=b, los=los).value()
         assert np.isclose(value.std(), expected, rtol=3e-5, atol=0.), (los, value.std(), expected)
+
+
+@pytest.mark.parametrize('los,cross,klimit', [
+    ('z', False, None), ('x', True, None), ([0.6, 0., 0.8], False, (0.02, 0.2)),
+    ('firstpoint', False, None), ('firstpoint', True, True), ('endpoint', True, None)])
+def test_bessel_basis_matches_oracle(los, cross, klimit):
+    """basis='bessel' (mesh2.py:169-177): Fourier-space mode values projected on j_ell(|k| s)."""
+    import jaxpower_b200 as jp
+    from oracle.spectrum import compute_mesh2_correlation_bessel as obessel
+    local = los in ('firstpoint', 'endpoint')
+    meshsize, boxsize = (24, 20, 16), np.array([480., 400., 320.])
+    boxcenter = np.array([700., -100., 600.]) if local else np.zeros(3)
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=boxcenter)
+    geom = Geometry(meshsize, boxsize, boxcenter)
+    pos1 = _catalog(20000, boxsize, 7) + boxcenter.astype('f4')
+    pos2 = _catalog(15000, boxsize, 8) + boxcenter.astype('f4')
+    m1 = jp.ParticleField(pos1, attrs=attrs).paint(resampler='tsc', interlacing=2, compensate=True, out='real')
+    o1 = opaint.paint(geom, pos1, None, 'tsc', 2, True, 'real')
+    ells = (0, 1, 2, 3, 4) if local else (0, 2, 4)
+    b = jp.BinMesh2CorrelationPoles(attrs, edges={'step': 20.}, ells=ells, basis='bessel', klimit=klimit)
+    ob = CorrelationBins(geom, step=20., ells=ells)
+    ok = None if klimit is None else b.klimit
+    if cross:
+        m2 = jp.ParticleField(pos2, attrs=attrs).paint(resampler='cic', out='complex')
+        o2 = opaint.paint(geom, pos2, None, 'cic', 0, False, 'complex')
+        got = jp.compute_mesh2_correlation(m1, m2, bin=b, los=los)
+        ref = obessel(o1, ob, los=los, mesh2=o2, klimit=ok)
+    else:
+        got = jp.compute_mesh2_correlation(m1, bin=b, los=los)
+        ref = obessel(o1, ob, los=los, klimit=ok)
+    # float32 mode values and |k| s, float64 j_ell and sums on both sides: the sums agree to
+    # float32 rounding of the per-mode products
+    scale = np.abs(ref['num_raw'][0]).max()
+    assert scale > 0.
+    for i, ell in enumerate(ells):
+        assert np.allclose(got.get(ell).num_raw, ref['num_raw'][i], rtol=0, atol=2e-5 * scale), ell
+    # the plain separation binning of the same estimator differs (another basis)
+    assert got.get(0).s.shape == ob.xavg.shape
