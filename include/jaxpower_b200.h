@@ -403,7 +403,7 @@ pk_status pk_bin_firstpoint_adjoint(void *stream, const void *a0, const void *f,
                                     int accumulate_a0, void *out_f, void *workspace,
                                     size_t workspace_bytes);
 
-/* Backward of pk_interlace_compensate (mesh.py:2737-2752), 'jax' semantics: from the
+/* Backward of pk_interlace_compensate (mesh.py:2737-2752), either backend's phases: from the
  * cotangent of the combined mesh (R = rfftn(rho_bar) if from_real, else the conjugate
  * cotangent of the complex mesh) to nshifts Hermitian half-meshes whose unnormalised C2R
  * are the cotangents of the painted shifted meshes. */

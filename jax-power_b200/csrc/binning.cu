@@ -1111,6 +1111,9 @@ __global__ void __launch_bounds__(BIN_THREADS, MINB) bin_global_kernel(
 #ifndef PK_STAGED_MIN_CTAS
 #define PK_STAGED_MIN_CTAS 3
 #endif
+#ifndef PK_STAGED_UNROLL
+#define PK_STAGED_UNROLL 3
+#endif
 #ifndef PK_STAGED_MIN_NZ
 #define PK_STAGED_MIN_NZ 90  // shorter stored rows take bin_global_flat_kernel
 #endif
@@ -1215,11 +1218,13 @@ __global__ void __launch_bounds__(BIN_THREADS, MINB) bin_interlaced_staged_kerne
     const float kxy = rcur.x, kl = rcur.y;
     rf.scale = rcur.z;
     const int Rz = (zhi + 31) >> 5;  // modes per lane
-    // phase 1: lanes on consecutive kz: weighted power and mu^2 of each mode
-    for (int t0 = 0; t0 < Rz; t0 += 3) {
-      float p[3], m[3];
+    // phase 1: lanes on consecutive kz: weighted power and mu^2 of each mode, PK_STAGED_UNROLL
+    // modes (3 PK_STAGED_UNROLL mesh loads) in flight per lane
+    constexpr int U = PK_STAGED_UNROLL;
+    for (int t0 = 0; t0 < Rz; t0 += U) {
+      float p[U], m[U];
 #pragma unroll
-      for (int u = 0; u < 3; ++u) {
+      for (int u = 0; u < U; ++u) {
         const int z = lane + 32 * (t0 + u);
         p[u] = m[u] = 0.f;
         if (t0 + u < Rz && z < zhi) {
@@ -1231,7 +1236,7 @@ __global__ void __launch_bounds__(BIN_THREADS, MINB) bin_interlaced_staged_kerne
         }
       }
 #pragma unroll
-      for (int u = 0; u < 3; ++u)
+      for (int u = 0; u < U; ++u)
         if (t0 + u < Rz) {
           pbuf[lane + 32 * (t0 + u)] = p[u];
           mbuf[lane + 32 * (t0 + u)] = m[u];

@@ -420,7 +420,7 @@ extern "C" pk_status pk_ylm_premultiply(void *stream, const float *rho, const in
 // is the transpose of interlace_kernel's arithmetic: e^{-i theta_s} = conj of the forward
 // phase, C / I = the same row scale times the kz window.  One warp per (i, j) row, four kz
 // per lane.
-template <int NS>
+template <int NS, bool FULL>
 __global__ void __launch_bounds__(IL_THREADS) interlace_adjoint_kernel(FourierParams p,
                                                                        const float2 *__restrict__ in,
                                                                        int from_real,
@@ -428,9 +428,9 @@ __global__ void __launch_bounds__(IL_THREADS) interlace_adjoint_kernel(FourierPa
   extern __shared__ float4 ilsmem[];
   const Dims d = p.d;
   const bool xy = use_xy_tables(d);
-  ZTable t = xy ? ztable_at<XY_SMEM>(ilsmem, p, false) : ztable_at<XY_NONE>(ilsmem, p, false);
-  if (xy) fill_ztable<false, XY_SMEM>(p, t);
-  else fill_ztable<false, XY_NONE>(p, t);
+  ZTable t = xy ? ztable_at<XY_SMEM>(ilsmem, p, FULL) : ztable_at<XY_NONE>(ilsmem, p, FULL);
+  if (xy) fill_ztable<FULL, XY_SMEM>(p, t);
+  else fill_ztable<FULL, XY_NONE>(p, t);
   __syncthreads();
   const int64_t total = d.ncomplex();
   const bool even = (d.n2 % 2) == 0;
@@ -442,8 +442,8 @@ __global__ void __launch_bounds__(IL_THREADS) interlace_adjoint_kernel(FourierPa
     const int i = rw.i, j = rw.j;
     const int im = (d.n0 - i) % d.n0, jm = (d.n1 - j) % d.n1;
     RowFactor<NS> rf, rm;
-    row_factor_rt<NS, false>(p, t, i, j, rf);
-    row_factor_rt<NS, false>(p, t, im, jm, rm);
+    row_factor_rt<NS, FULL>(p, t, i, j, rf);
+    row_factor_rt<NS, FULL>(p, t, im, jm, rm);
     const int64_t rbase = ((int64_t)i * d.n1 + j) * d.nz;
     const int64_t mbase = ((int64_t)im * d.n1 + jm) * d.nz;
     for (int zb = lane; zb < d.nz; zb += 128) {
@@ -468,11 +468,11 @@ __global__ void __launch_bounds__(IL_THREADS) interlace_adjoint_kernel(FourierPa
         }
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
-          const float2 ph = cmul(rf.ph[s], t.ph[s * d.nz + z]);
+          const float2 ph = mode_phase<NS, FULL>(p, rf, t, s, z);  // the forward's phase (combine_mode)
           float2 v = cmul(x[u], make_float2(ph.x, -ph.y));
           v = make_float2(v.x * c, v.y * c);
           if (plane) {
-            const float2 phm = cmul(rm.ph[s], t.ph[s * d.nz + z]);
+            const float2 phm = mode_phase<NS, FULL>(p, rm, t, s, z);
             float2 m = cmul(xm, make_float2(phm.x, -phm.y));
             m = make_float2(m.x * cm, m.y * cm);
             v = make_float2(0.5f * (v.x + m.x), 0.5f * (v.y - m.y));
@@ -556,8 +556,9 @@ extern "C" pk_status pk_interlace_adjoint(void *stream, const void *in, int from
   PK_REQUIRE(make_dims(meshsize, &p.d), PK_ERR_INVALID, "invalid meshsize");
   PK_REQUIRE(nshifts >= 1 && nshifts <= IL_MAX_SHIFTS, PK_ERR_INVALID, "nshifts must be in 1..8");
   PK_REQUIRE(comp_order >= 0 && comp_order <= 4, PK_ERR_INVALID, "comp_order must be in 0..4");
-  PK_REQUIRE(backend == PK_BACKEND_JAX, PK_ERR_INVALID,
-             "the paint adjoint implements the 'jax' FFT semantics only");
+  PK_REQUIRE(backend == PK_BACKEND_JAX || backend == PK_BACKEND_JAXDECOMP, PK_ERR_INVALID, "unknown backend %d",
+             backend);
+  const bool full = backend == PK_BACKEND_JAXDECOMP;
   const int ns[3] = {p.d.n0, p.d.n1, p.d.n2};
   for (int a = 0; a < 3; ++a) p.cspacing[a] = (float)(2. * M_PI / ns[a]);
   p.nshifts = nshifts;
@@ -568,7 +569,7 @@ extern "C" pk_status pk_interlace_adjoint(void *stream, const void *in, int from
   p.for_c2r = 1;
   p.scale = 1.f;
   p.gxy = nullptr;
-  const size_t smem = ztable_bytes(p.d, nshifts, false, use_xy_tables(p.d));
+  const size_t smem = ztable_bytes(p.d, nshifts, full, use_xy_tables(p.d));
   PK_REQUIRE(smem <= 200 * 1024, PK_ERR_RANGE, "mesh too large for the per-axis tables");
   const int64_t nrows = (int64_t)p.d.n0 * p.d.n1;
   const int64_t want = (nrows + IL_THREADS / 32 - 1) / (IL_THREADS / 32);
@@ -576,16 +577,23 @@ extern "C" pk_status pk_interlace_adjoint(void *stream, const void *in, int from
   const int blocks = (int)(want < cap ? want : cap);
   cudaStream_t st = (cudaStream_t)stream;
   switch (nshifts) {
+#define PK_ILA_LAUNCH(N, F)                                                                            \
+  PK_CUDA(cudaFuncSetAttribute(interlace_adjoint_kernel<N, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                               (int)smem));                                                            \
+  interlace_adjoint_kernel<N, F><<<blocks, IL_THREADS, smem, st>>>(p, (const float2 *)in, from_real,     \
+                                                                   (float2 *)out);
 #define PK_ILA_CASE(N)                                                                                 \
   case N:                                                                                              \
-    PK_CUDA(cudaFuncSetAttribute(interlace_adjoint_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                 (int)smem));                                                          \
-    interlace_adjoint_kernel<N><<<blocks, IL_THREADS, smem, st>>>(p, (const float2 *)in, from_real,      \
-                                                                  (float2 *)out);                      \
+    if (full) {                                                                                        \
+      PK_ILA_LAUNCH(N, true)                                                                           \
+    } else {                                                                                           \
+      PK_ILA_LAUNCH(N, false)                                                                          \
+    }                                                                                                  \
     break;
     PK_ILA_CASE(1) PK_ILA_CASE(2) PK_ILA_CASE(3) PK_ILA_CASE(4) PK_ILA_CASE(5) PK_ILA_CASE(6)
     PK_ILA_CASE(7) PK_ILA_CASE(8)
 #undef PK_ILA_CASE
+#undef PK_ILA_LAUNCH
   }
   PK_LAUNCH_CHECK();
   return PK_OK;

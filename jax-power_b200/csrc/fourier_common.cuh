@@ -136,6 +136,20 @@ __device__ __forceinline__ void row_factor_rt(const FourierParams &p, const ZTab
   else row_factor<NS, FULL, false>(p, t, i, j, r);
 }
 
+// Phase of shift s at stored mode (row factor r, z) in the interlaced sum: e^{i s/I (kx + ky + kz)}
+// ('jax'), or FULL ('jaxdecomp', full-grid circular coordinates) the Hermitian part
+// (e^{i t(k)} + e^{-i t(-k)}) / 2, which differs from e^{i t(k)} on the Nyquist planes only.
+template <int NS, bool FULL>
+__device__ __forceinline__ float2 mode_phase(const FourierParams &p, const RowFactor<NS> &r, const ZTable &t,
+                                             int s, int z) {
+  float2 ph = cmul(r.ph[s], t.ph[s * p.d.nz + z]);
+  if (FULL) {
+    const float2 m = cmul(r.phm[s], t.phm[s * p.d.nz + z]);
+    ph = make_float2(0.5f * (ph.x + m.x), 0.5f * (ph.y + m.y));
+  }
+  return ph;
+}
+
 // Interlaced + compensated value of stored mode (row r, z): shift 0 has phase 1, so its
 // value enters as is; the others are rotated by their phase; the sum is scaled once by the
 // window and 1 / I.

@@ -16,7 +16,10 @@ XLA).  Here each stage has an explicit adjoint in the CUDA library, wired into
   keeps A0 and the transformed Y_lm-weighted meshes resident (when they fit in a third of
   the free memory), so the backward pass does not transform them again.
 
-Gradients follow the 'jax' FFT semantics and even multipoles (odd auto multipoles are 0).
+Gradients follow either FFT backend's semantics ('jax', or 'jaxdecomp' with its full-grid
+interlacing phases) and cover every multipole: odd ones are imaginary parts, identically zero
+for an auto spectrum with a fixed line of sight.  A complex input mesh to the spectrum gets its
+own cotangent (torch's dL/dRe + i dL/dIm convention).
 """
 import numpy as np
 import torch
@@ -78,8 +81,6 @@ class _Paint(torch.autograd.Function):
 def paint_value(positions, weights=None, attrs=None, resampler='cic', interlacing=0, compensate=False,
                 out='real'):
     """Differentiable ``ParticleField(positions, weights, attrs).paint(...)``: returns the mesh tensor."""
-    if attrs.fft_backend != 'jax' and (interlacing > 1 or compensate):
-        raise NotImplementedError("the paint adjoint implements fft_backend='jax'")
     positions = positions if positions.is_cuda and positions.dtype == torch.float32 else _as_positions(positions)
     if weights is not None and not (weights.is_cuda and weights.dtype == torch.float32):
         weights = _as_weights(weights, positions.shape[0])
