@@ -403,6 +403,25 @@ pk_status pk_bin_firstpoint_adjoint(void *stream, const void *a0, const void *f,
                                     int accumulate_a0, void *out_f, void *workspace,
                                     size_t workspace_bytes);
 
+/* pk_bin_global_adjoint / pk_bin_firstpoint_adjoint for mode oversampling (mesh2.py:48-61,
+ * the forward through the *_shifted binning calls): nkshift (<= 125) k shifts, kshifts
+ * (host, 3 floats each, as given to those calls); each mode's coefficient is the mean over the
+ * shifts of coef[l][bin of |k + shift|]. */
+pk_status pk_bin_global_adjoint_shifted(void *stream, const void *delta, const int32_t meshsize[3],
+                                        const float kfun[3], const float los[3], const float *d_edges,
+                                        int nedges, float step, float edge0, int backend, int nells,
+                                        const int32_t *ells, const float *d_coef, int for_c2r, int nkshift,
+                                        const float *kshifts, void *out, void *workspace,
+                                        size_t workspace_bytes);
+pk_status pk_bin_firstpoint_adjoint_shifted(void *stream, const void *a0, const void *f, int nterms,
+                                            const int32_t *term_ell, const int32_t *term_m,
+                                            const int32_t meshsize[3], const float kfun[3],
+                                            const float *d_edges, int nedges, float step, float edge0,
+                                            int backend, int nells, const int32_t *ells, const float *d_coef,
+                                            int for_c2r, int nkshift, const float *kshifts, void *out_a0,
+                                            int accumulate_a0, void *out_f, void *workspace,
+                                            size_t workspace_bytes);
+
 /* Backward of pk_interlace_compensate (mesh.py:2737-2752), either backend's phases: from the
  * cotangent of the combined mesh (R = rfftn(rho_bar) if from_real, else the conjugate
  * cotangent of the complex mesh) to nshifts Hermitian half-meshes whose unnormalised C2R

@@ -2325,6 +2325,8 @@ extern "C" pk_status pk_bin_global_noalloc(void *stream, const void *delta1, con
 // planes) and Hermitian-symmetrised on the kz = 0 / N/2 planes, so that an unnormalised
 // C2R of it is the cotangent of the real mesh the modes were transformed from.
 
+constexpr int ADJ_MAX_KSHIFTS = 125;  // mode_oversampling <= 2: (2 s + 1)^3 shifts
+
 struct AdjGeom {
   BinGeom g;
   int nbins;
@@ -2334,11 +2336,38 @@ struct AdjGeom {
   float los[3];
   float e0, inv_step;
   int for_c2r;
+  int nkshift;  // mode oversampling: the k shifts of the forward's bins (0: none)
+  float kshift[ADJ_MAX_KSHIFTS][3];
 };
 
 // Bin index of a stored mode (thresholds in a global table).
 __device__ __forceinline__ int adj_bin(const AdjGeom &a, const float *thr, float k2) {
   return bin_from_k2(thr, a.g.nedges, a.e0, a.inv_step, k2);
+}
+
+// Mode oversampling (mesh2.py:48-61): the forward averages the sums of the shifted binnings
+// (the bin of |k + shift|, shifted_k2's float32 expression), so a mode's cotangent coefficient
+// for multipole row l is the mean over the shifts of coef[l][b_s - 1]; false when no shift puts
+// the mode in a bin.
+__device__ __forceinline__ bool adj_shifted_coefs(const AdjGeom &a, const float *thr, const float *coef, float kx,
+                                                  float ky, float kz, float (&csum)[MAX_ELLS]) {
+#pragma unroll
+  for (int l = 0; l < MAX_ELLS; ++l) csum[l] = 0.f;
+  bool any = false;
+  for (int q = 0; q < a.nkshift; ++q) {
+    const float x = __fadd_rn(kx, a.kshift[q][0]), y = __fadd_rn(ky, a.kshift[q][1]), z = __fadd_rn(kz, a.kshift[q][2]);
+    const float k2s = __fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z));
+    const int b = adj_bin(a, thr, k2s);
+    if (b < 1 || b > a.nbins) continue;
+    any = true;
+#pragma unroll
+    for (int l = 0; l < MAX_ELLS; ++l)
+      if (l < a.nells) csum[l] += coef[(size_t)l * a.nbins + (b - 1)];
+  }
+  const float inv = 1.f / (float)a.nkshift;
+#pragma unroll
+  for (int l = 0; l < MAX_ELLS; ++l) csum[l] *= inv;
+  return any;
 }
 
 __device__ __forceinline__ float c2r_weight(const BinGeom &g, int z) {
@@ -2352,6 +2381,7 @@ __global__ void thresholds_kernel(const float *__restrict__ edges, int nedges,
 }
 
 // global line of sight: gbar_k = 2 G_k delta_k, G_k = w_k sum_l coef_l[b] L_l(mu)
+template <bool SHIFTED>
 __device__ __forceinline__ float2 global_adj_mode(const AdjGeom &a, const float *thr,
                                                   const float *coef, const float2 *delta, int i,
                                                   int j, int z) {
@@ -2360,8 +2390,14 @@ __device__ __forceinline__ float2 global_adj_mode(const AdjGeom &a, const float 
   const float ky = kcoord(j, g.d.n1, g.kfun[1], false);
   const float kz = kz_coord(g, z);
   const float k2 = __fadd_rn(__fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky)), __fmul_rn(kz, kz));
-  const int b = adj_bin(a, thr, k2);
-  if (b < 1 || b > a.nbins) return make_float2(0.f, 0.f);
+  int b = 1;
+  float csum[MAX_ELLS];
+  if (SHIFTED) {
+    if (!adj_shifted_coefs(a, thr, coef, kx, ky, kz, csum)) return make_float2(0.f, 0.f);
+  } else {
+    b = adj_bin(a, thr, k2);
+    if (b < 1 || b > a.nbins) return make_float2(0.f, 0.f);
+  }
   const float num = (kx * a.los[0] + ky * a.los[1]) + kz * a.los[2];
   const float rk2 = k2 > 0.f ? 1.f / k2 : 0.f;
   const float mu2 = num * num * rk2;
@@ -2376,13 +2412,14 @@ __device__ __forceinline__ float2 global_adj_mode(const AdjGeom &a, const float 
     L = L * mu2 + a.lc.c[l][1];
     L = L * mu2 + a.lc.c[l][0];
     if (a.lc.odd[l]) L *= mu;  // odd multipoles bin Im(A): handled by the caller's coef sign
-    G += coef[(size_t)l * a.nbins + (b - 1)] * L;
+    G += (SHIFTED ? csum[l] : coef[(size_t)l * a.nbins + (b - 1)]) * L;
   }
   G *= mode_weight(g, z);
   const float2 d = delta[((int64_t)i * g.d.n1 + j) * g.d.nz + z];
   return make_float2(2.f * G * d.x, 2.f * G * d.y);
 }
 
+template <bool SHIFTED>
 __global__ void global_adjoint_kernel(AdjGeom a, const float *__restrict__ thr,
                                       const float *__restrict__ coef,
                                       const float2 *__restrict__ delta,
@@ -2394,11 +2431,11 @@ __global__ void global_adjoint_kernel(AdjGeom a, const float *__restrict__ thr,
   IndexWalker3 w(start, stride, g.d.n1, g.d.nz);
   for (int64_t idx = start; idx < total; idx += stride, w.next()) {
     const int i = w.i, j = w.j, z = w.k;
-    float2 v = global_adj_mode(a, thr, coef, delta, i, j, z);
+    float2 v = global_adj_mode<SHIFTED>(a, thr, coef, delta, i, j, z);
     if (a.for_c2r) {
       if (z == 0 || (even && z == g.d.nz - 1)) {
-        const float2 m = global_adj_mode(a, thr, coef, delta, (g.d.n0 - i) % g.d.n0,
-                                         (g.d.n1 - j) % g.d.n1, z);
+        const float2 m = global_adj_mode<SHIFTED>(a, thr, coef, delta, (g.d.n0 - i) % g.d.n0,
+                                                  (g.d.n1 - j) % g.d.n1, z);
         v = make_float2(0.5f * (v.x + m.x), 0.5f * (v.y - m.y));
       } else {
         v = make_float2(0.5f * v.x, 0.5f * v.y);
@@ -2416,6 +2453,7 @@ struct FPAdj {
   int term_l[MAX_FP_TERMS];  // index of the term's ell in ells
 };
 
+template <bool SHIFTED>
 __device__ __forceinline__ void fp_adj_mode(const AdjGeom &a, const FPAdj &t, const float *thr,
                                             const float *coef, const float2 *a0, const float2 *f,
                                             int i, int j, int z, float2 *ga0, float2 *gf) {
@@ -2424,12 +2462,18 @@ __device__ __forceinline__ void fp_adj_mode(const AdjGeom &a, const FPAdj &t, co
   const float ky = kcoord(j, g.d.n1, g.kfun[1], false);
   const float kz = kz_coord(g, z);
   const float k2 = __fadd_rn(__fadd_rn(__fmul_rn(kx, kx), __fmul_rn(ky, ky)), __fmul_rn(kz, kz));
-  const int b = adj_bin(a, thr, k2);
   const int64_t idx = ((int64_t)i * g.d.n1 + j) * g.d.nz + z;
   const int64_t stride = g.d.ncomplex();
   *ga0 = make_float2(0.f, 0.f);
   for (int q = 0; q < t.nterms; ++q) gf[q] = make_float2(0.f, 0.f);
-  if (b < 1 || b > a.nbins) return;
+  int b = 1;
+  float csum[MAX_ELLS];
+  if (SHIFTED) {
+    if (!adj_shifted_coefs(a, thr, coef, kx, ky, kz, csum)) return;
+  } else {
+    b = adj_bin(a, thr, k2);
+    if (b < 1 || b > a.nbins) return;
+  }
   const bool zero = (i == 0 && j == 0 && z == 0);
   const float w = mode_weight(g, z);
   const float rn = k2 > 0.f ? rsqrtf(k2) : 0.f;
@@ -2438,14 +2482,14 @@ __device__ __forceinline__ void fp_adj_mode(const AdjGeom &a, const FPAdj &t, co
   float2 acc = make_float2(0.f, 0.f);
   for (int l = 0; l < a.nells; ++l)
     if (a.ells[l] == 0) {  // ell = 0: |A0|^2 -> 2 G0 A0
-      const float G0 = w * coef[(size_t)l * a.nbins + (b - 1)];
+      const float G0 = w * (SHIFTED ? csum[l] : coef[(size_t)l * a.nbins + (b - 1)]);
       acc.x += 2.f * G0 * A.x;
       acc.y += 2.f * G0 * A.y;
     }
   if (!zero)
     for (int q = 0; q < t.nterms; ++q) {
       const int l = t.term_l[q];
-      const float G = w * coef[(size_t)l * a.nbins + (b - 1)];
+      const float G = w * (SHIFTED ? csum[l] : coef[(size_t)l * a.nbins + (b - 1)]);
       const float y = ylm_eval(t.term_ell[q], t.term_m[q], xh, yh, zh);
       const float2 F = f[(int64_t)q * stride + idx];
       const float gy = G * y;
@@ -2462,6 +2506,7 @@ __device__ __forceinline__ void fp_adj_mode(const AdjGeom &a, const FPAdj &t, co
   *ga0 = acc;
 }
 
+template <bool SHIFTED>
 __global__ void firstpoint_adjoint_kernel(AdjGeom a, FPAdj t, const float *__restrict__ thr,
                                           const float *__restrict__ coef,
                                           const float2 *__restrict__ a0,
@@ -2477,13 +2522,13 @@ __global__ void firstpoint_adjoint_kernel(AdjGeom a, FPAdj t, const float *__res
   for (int64_t idx = start; idx < total; idx += stride, w.next()) {
     const int i = w.i, j = w.j, z = w.k;
     float2 ga0;
-    fp_adj_mode(a, t, thr, coef, a0, f, i, j, z, &ga0, gf);
+    fp_adj_mode<SHIFTED>(a, t, thr, coef, a0, f, i, j, z, &ga0, gf);
     const bool plane = z == 0 || (even && z == g.d.nz - 1);
     if (a.for_c2r) {
       if (plane) {
         float2 ga0m;
-        fp_adj_mode(a, t, thr, coef, a0, f, (g.d.n0 - i) % g.d.n0, (g.d.n1 - j) % g.d.n1, z,
-                    &ga0m, gfm);
+        fp_adj_mode<SHIFTED>(a, t, thr, coef, a0, f, (g.d.n0 - i) % g.d.n0, (g.d.n1 - j) % g.d.n1, z,
+                             &ga0m, gfm);
         if (a.for_c2r == 1) ga0 = make_float2(0.5f * (ga0.x + ga0m.x), 0.5f * (ga0.y - ga0m.y));
         for (int q = 0; q < t.nterms; ++q)
           gf[q] = make_float2(0.5f * (gf[q].x + gfm[q].x), 0.5f * (gf[q].y - gfm[q].y));
@@ -2636,6 +2681,16 @@ static pk_status make_adj(const int32_t meshsize[3], const float kfun[3], int ne
   a->e0 = 0.f;  // refined on the device from edges[0]
   a->inv_step = step > 0.f ? 1.f / step : 0.f;
   a->for_c2r = for_c2r;
+  a->nkshift = 0;
+  return PK_OK;
+}
+
+static pk_status set_adj_kshifts(AdjGeom *a, int nkshift, const float *kshifts) {
+  PK_REQUIRE(nkshift >= 0 && nkshift <= ADJ_MAX_KSHIFTS, PK_ERR_RANGE, "nkshift must be in 0..%d", ADJ_MAX_KSHIFTS);
+  PK_REQUIRE(nkshift == 0 || kshifts, PK_ERR_INVALID, "null kshifts");
+  a->nkshift = nkshift;
+  for (int q = 0; q < nkshift; ++q)
+    for (int c = 0; c < 3; ++c) a->kshift[q][c] = kshifts[3 * q + c];
   return PK_OK;
 }
 
@@ -2645,14 +2700,15 @@ extern "C" pk_status pk_adjoint_workspace_size(int nedges, size_t *bytes) {
   return PK_OK;
 }
 
-extern "C" pk_status pk_bin_global_adjoint(void *stream, const void *delta,
-                                           const int32_t meshsize[3], const float kfun[3],
-                                           const float los[3], const float *d_edges, int nedges,
-                                           float step, float edge0, int backend, int nells,
-                                           const int32_t *ells, const float *d_coef, int for_c2r,
-                                           void *out, void *workspace, size_t workspace_bytes) {
+static pk_status bin_global_adjoint(void *stream, const void *delta, const int32_t meshsize[3], const float kfun[3],
+                                    const float los[3], const float *d_edges, int nedges, float step, float edge0,
+                                    int backend, int nells, const int32_t *ells, const float *d_coef, int for_c2r,
+                                    int nkshift, const float *kshifts, void *out, void *workspace,
+                                    size_t workspace_bytes) {
   AdjGeom a;
   pk_status st = make_adj(meshsize, kfun, nedges, step, backend, nells, ells, d_edges, for_c2r, &a);
+  if (st) return st;
+  st = set_adj_kshifts(&a, nkshift, kshifts);
   if (st) return st;
   PK_REQUIRE(delta && d_coef && out && los, PK_ERR_INVALID, "null pointer");
   PK_REQUIRE(delta != out, PK_ERR_INVALID, "out must not alias delta");
@@ -2666,23 +2722,47 @@ extern "C" pk_status pk_bin_global_adjoint(void *stream, const void *delta,
   PK_LAUNCH_CHECK();
   const int64_t total = a.g.d.ncomplex();
   const int64_t want = (total + 255) / 256, cap = 32LL * sm_count();
-  global_adjoint_kernel<<<(int)(want < cap ? want : cap), 256, 0, s>>>(
-      a, thr, d_coef, (const float2 *)delta, (float2 *)out);
+  if (a.nkshift)
+    global_adjoint_kernel<true><<<(int)(want < cap ? want : cap), 256, 0, s>>>(
+        a, thr, d_coef, (const float2 *)delta, (float2 *)out);
+  else
+    global_adjoint_kernel<false><<<(int)(want < cap ? want : cap), 256, 0, s>>>(
+        a, thr, d_coef, (const float2 *)delta, (float2 *)out);
   PK_LAUNCH_CHECK();
   return PK_OK;
 }
 
-extern "C" pk_status pk_bin_firstpoint_adjoint(void *stream, const void *a0, const void *f,
-                                               int nterms, const int32_t *term_ell,
-                                               const int32_t *term_m, const int32_t meshsize[3],
-                                               const float kfun[3], const float *d_edges,
-                                               int nedges, float step, float edge0, int backend,
-                                               int nells, const int32_t *ells,
-                                               const float *d_coef, int for_c2r, void *out_a0,
-                                               int accumulate_a0, void *out_f, void *workspace,
-                                               size_t workspace_bytes) {
+extern "C" pk_status pk_bin_global_adjoint(void *stream, const void *delta,
+                                           const int32_t meshsize[3], const float kfun[3],
+                                           const float los[3], const float *d_edges, int nedges,
+                                           float step, float edge0, int backend, int nells,
+                                           const int32_t *ells, const float *d_coef, int for_c2r,
+                                           void *out, void *workspace, size_t workspace_bytes) {
+  return bin_global_adjoint(stream, delta, meshsize, kfun, los, d_edges, nedges, step, edge0, backend, nells, ells,
+                            d_coef, for_c2r, 0, nullptr, out, workspace, workspace_bytes);
+}
+
+extern "C" pk_status pk_bin_global_adjoint_shifted(void *stream, const void *delta, const int32_t meshsize[3],
+                                                   const float kfun[3], const float los[3], const float *d_edges,
+                                                   int nedges, float step, float edge0, int backend, int nells,
+                                                   const int32_t *ells, const float *d_coef, int for_c2r,
+                                                   int nkshift, const float *kshifts, void *out, void *workspace,
+                                                   size_t workspace_bytes) {
+  return bin_global_adjoint(stream, delta, meshsize, kfun, los, d_edges, nedges, step, edge0, backend, nells, ells,
+                            d_coef, for_c2r, nkshift, kshifts, out, workspace, workspace_bytes);
+}
+
+static pk_status bin_firstpoint_adjoint(void *stream, const void *a0, const void *f, int nterms,
+                                        const int32_t *term_ell, const int32_t *term_m, const int32_t meshsize[3],
+                                        const float kfun[3], const float *d_edges, int nedges, float step,
+                                        float edge0, int backend, int nells, const int32_t *ells,
+                                        const float *d_coef, int for_c2r, int nkshift, const float *kshifts,
+                                        void *out_a0, int accumulate_a0, void *out_f, void *workspace,
+                                        size_t workspace_bytes) {
   AdjGeom a;
   pk_status st = make_adj(meshsize, kfun, nedges, step, backend, nells, ells, d_edges, for_c2r, &a);
+  if (st) return st;
+  st = set_adj_kshifts(&a, nkshift, kshifts);
   if (st) return st;
   PK_REQUIRE(a0 && d_coef, PK_ERR_INVALID, "null pointer");
   PK_REQUIRE(nterms >= 0 && nterms <= MAX_FP_TERMS, PK_ERR_INVALID, "nterms must be in 0..%d",
@@ -2711,6 +2791,13 @@ extern "C" pk_status pk_bin_firstpoint_adjoint(void *stream, const void *a0, con
   const int64_t total = a.g.d.ncomplex();
   const int64_t want = (total + 255) / 256, cap = 32LL * sm_count();
   const int mask = ylm_terms_mask(nterms, term_ell, term_m);
+  if (a.nkshift) {  // mode oversampling: the general kernel with shift-averaged coefficients
+    firstpoint_adjoint_kernel<true><<<(int)(want < cap ? want : cap), 256, 0, s>>>(
+        a, t, thr, d_coef, (const float2 *)a0, (const float2 *)f, (float2 *)out_a0, accumulate_a0,
+        (float2 *)out_f);
+    PK_LAUNCH_CHECK();
+    return PK_OK;
+  }
   if (nterms > 0 && mask && ylm_mask_compiled(mask)) {
     FPAdjRows r{};
     for (int q = 0; q < nterms; ++q) r.row[term_ell[q]] = t.term_l[q];
@@ -2725,11 +2812,38 @@ extern "C" pk_status pk_bin_firstpoint_adjoint(void *stream, const void *a0, con
     PK_YLM_MASKS(PK_FP_ADJ_CASE)
 #undef PK_FP_ADJ_CASE
   }
-  firstpoint_adjoint_kernel<<<(int)(want < cap ? want : cap), 256, 0, s>>>(
+  firstpoint_adjoint_kernel<false><<<(int)(want < cap ? want : cap), 256, 0, s>>>(
       a, t, thr, d_coef, (const float2 *)a0, (const float2 *)f, (float2 *)out_a0, accumulate_a0,
       (float2 *)out_f);
   PK_LAUNCH_CHECK();
   return PK_OK;
+}
+
+extern "C" pk_status pk_bin_firstpoint_adjoint(void *stream, const void *a0, const void *f,
+                                               int nterms, const int32_t *term_ell,
+                                               const int32_t *term_m, const int32_t meshsize[3],
+                                               const float kfun[3], const float *d_edges,
+                                               int nedges, float step, float edge0, int backend,
+                                               int nells, const int32_t *ells,
+                                               const float *d_coef, int for_c2r, void *out_a0,
+                                               int accumulate_a0, void *out_f, void *workspace,
+                                               size_t workspace_bytes) {
+  return bin_firstpoint_adjoint(stream, a0, f, nterms, term_ell, term_m, meshsize, kfun, d_edges, nedges, step,
+                                edge0, backend, nells, ells, d_coef, for_c2r, 0, nullptr, out_a0, accumulate_a0,
+                                out_f, workspace, workspace_bytes);
+}
+
+extern "C" pk_status pk_bin_firstpoint_adjoint_shifted(void *stream, const void *a0, const void *f, int nterms,
+                                                       const int32_t *term_ell, const int32_t *term_m,
+                                                       const int32_t meshsize[3], const float kfun[3],
+                                                       const float *d_edges, int nedges, float step, float edge0,
+                                                       int backend, int nells, const int32_t *ells,
+                                                       const float *d_coef, int for_c2r, int nkshift,
+                                                       const float *kshifts, void *out_a0, int accumulate_a0,
+                                                       void *out_f, void *workspace, size_t workspace_bytes) {
+  return bin_firstpoint_adjoint(stream, a0, f, nterms, term_ell, term_m, meshsize, kfun, d_edges, nedges, step,
+                                edge0, backend, nells, ells, d_coef, for_c2r, nkshift, kshifts, out_a0,
+                                accumulate_a0, out_f, workspace, workspace_bytes);
 }
 
 extern "C" pk_status pk_window_fill(void *stream, const int32_t meshsize[3], const float kfun[3], int backend,

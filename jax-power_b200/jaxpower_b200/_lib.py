@@ -98,6 +98,13 @@ SIGNATURES = {
     'pk_bin_firstpoint_adjoint': [c_void_p, c_void_p, c_void_p, c_int, c_int32_p, c_int32_p, c_int32_p,
                                   c_float_p, c_void_p, c_int, c_float, c_float, c_int, c_int, c_int32_p,
                                   c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_size_t],
+    'pk_bin_global_adjoint_shifted': [c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_void_p, c_int, c_float,
+                                      c_float, c_int, c_int, c_int32_p, c_void_p, c_int, c_int, c_float_p, c_void_p,
+                                      c_void_p, c_size_t],
+    'pk_bin_firstpoint_adjoint_shifted': [c_void_p, c_void_p, c_void_p, c_int, c_int32_p, c_int32_p, c_int32_p,
+                                          c_float_p, c_void_p, c_int, c_float, c_float, c_int, c_int, c_int32_p,
+                                          c_void_p, c_int, c_int, c_float_p, c_void_p, c_int, c_void_p, c_void_p,
+                                          c_size_t],
     'pk_interlace_adjoint': [c_void_p, c_void_p, c_int, c_int, c_int32_p, c_int, c_int, c_void_p],
     'pk_c2r_adjoint': [c_void_p, c_void_p, c_int32_p, c_int, c_void_p],
     'pk_bin_bessel_workspace_size': [c_int32_p, c_int, c_int, ctypes.POINTER(c_size_t)],

@@ -124,12 +124,17 @@ class _Spectrum(torch.autograd.Function):
         stream = _lib.stream_handle()
         edge0 = float(np.float32(bin._edges1d[0]))
         common = (_lib.i32(meshsize), _lib.f32(attrs.kfun))
+        kshifts = list(getattr(bin, '_kshifts', []))
+        # mode oversampling: the *_shifted adjoints average each mode's coefficient over the shifts
+        shifted = (len(kshifts), _lib.f32([v for sh in kshifts for v in sh])) if kshifts else ()
+        suffix = '_shifted' if kshifts else ''
         if vlos is not None:
             delta = (value.detach() if is_complex else _r2c(value.detach(), meshsize)).contiguous()
             out = torch.empty_like(delta)
-            _lib.call('pk_bin_global_adjoint', stream, _lib.ptr(delta), *common, _lib.f32(vlos), _lib.ptr(bin.d_edges),
-                      len(bin._edges1d), bin._step, edge0, attrs.backend_code, len(ells), _lib.i32(ells),
-                      _lib.ptr(coef), int(not is_complex), _lib.ptr(out), _lib.ptr(ws), ws.numel())
+            _lib.call('pk_bin_global_adjoint' + suffix, stream, _lib.ptr(delta), *common, _lib.f32(vlos),
+                      _lib.ptr(bin.d_edges), len(bin._edges1d), bin._step, edge0, attrs.backend_code, len(ells),
+                      _lib.i32(ells), _lib.ptr(coef), int(not is_complex), *shifted, _lib.ptr(out), _lib.ptr(ws),
+                      ws.numel())
             if is_complex:
                 return out, None, None, None
             return _c2r_unnormalised(out, meshsize), None, None, None
@@ -147,9 +152,10 @@ class _Spectrum(torch.autograd.Function):
         terms = _firstpoint_terms(ells)
         offset = (attrs.boxcenter - (attrs.boxsize / np.float32(2.)).astype('f4')).astype('f4')
         if not terms:
-            _lib.call('pk_bin_firstpoint_adjoint', stream, _lib.ptr(A0), None, 0, None, None, *common,
+            _lib.call('pk_bin_firstpoint_adjoint' + suffix, stream, _lib.ptr(A0), None, 0, None, None, *common,
                       _lib.ptr(bin.d_edges), len(bin._edges1d), bin._step, edge0, attrs.backend_code, len(ells),
-                      _lib.i32(ells), _lib.ptr(coef), a0_mode, _lib.ptr(ga0), 0, None, _lib.ptr(ws), ws.numel())
+                      _lib.i32(ells), _lib.ptr(coef), a0_mode, *shifted, _lib.ptr(ga0), 0, None, _lib.ptr(ws),
+                      ws.numel())
         coef_rest = coef.clone()  # ell = 0 enters the A0 cotangent once, with the first batch
         for l, ell in enumerate(ells):
             if ell == 0:
@@ -169,10 +175,10 @@ class _Spectrum(torch.autograd.Function):
                 F = _r2c(real, meshsize)
                 del real
             gf = torch.empty_like(F)
-            _lib.call('pk_bin_firstpoint_adjoint', stream, _lib.ptr(A0), _lib.ptr(F), nt, _lib.i32(t_ell),
+            _lib.call('pk_bin_firstpoint_adjoint' + suffix, stream, _lib.ptr(A0), _lib.ptr(F), nt, _lib.i32(t_ell),
                       _lib.i32(t_m), *common, _lib.ptr(bin.d_edges), len(bin._edges1d), bin._step, edge0,
                       attrs.backend_code, len(ells), _lib.i32(ells), _lib.ptr(coef if ib == 0 else coef_rest), a0_mode,
-                      _lib.ptr(ga0), 1, _lib.ptr(gf), _lib.ptr(ws), ws.numel())
+                      *shifted, _lib.ptr(ga0), 1, _lib.ptr(gf), _lib.ptr(ws), ws.numel())
             del F
             r = _c2r_unnormalised(gf, meshsize)
             _lib.call('pk_ylm_accumulate', stream, _lib.ptr(r), _lib.i32(meshsize), _lib.f32(attrs.cellsize),
@@ -187,8 +193,6 @@ class _Spectrum(torch.autograd.Function):
 
 def spectrum_value(mesh, attrs=None, bin=None, los='z'):
     """Differentiable multipoles ``num_raw`` (nells, nbins) float64 of ``compute_mesh2_spectrum``."""
-    from .mesh2 import _plain_bins
-    _plain_bins(bin, 'the differentiable spectrum')
     value = mesh.value if hasattr(mesh, 'value') else mesh
     attrs = attrs if attrs is not None else mesh.attrs
     return _Spectrum.apply(value, attrs, bin, los)
