@@ -135,6 +135,28 @@ def algorithmic_bytes(name, npart, meshsize, interlacing, nells):
     return None
 
 
+def binning_roofline(stages, bins, W, peak):
+    """The fused interlace + compensate + binning pass against the HBM peak: on the whole shifted
+    meshes (8 N_c I bytes, the algorithmic figure) and on the stored modes below the last edge,
+    the only ones it reads (8 I bytes each)."""
+    st = stages.get('pk_bin_global_interlaced')
+    if not st:
+        return None
+    n = int(W['meshsize'])
+    kf = 2. * np.pi / float(W['boxsize'])
+    k = np.fft.fftfreq(n, 1. / n) * kf
+    kz2 = (np.arange(n // 2 + 1) * kf) ** 2
+    klast2 = float(bins._edges1d[-1]) ** 2
+    kxy = (k[:, None] ** 2 + k[None, :] ** 2).ravel()
+    in_range = int(np.searchsorted(kz2, klast2 - kxy, side='left').sum())
+    t = st['mean_ms'] * 1e-3
+    whole = 8. * n * n * (n // 2 + 1) * W['interlacing']
+    needed = 8. * W['interlacing'] * in_range
+    return {'kernel': 'pk_bin_global_interlaced', 'bound': 'hbm', 'unit': 'GB/s', 'peak': peak,
+            'algorithmic_bytes': whole, 'achieved': whole / t / 1e9, 'frac': whole / t / 1e9 / peak,
+            'in_range_bytes': needed, 'achieved_in_range': needed / t / 1e9, 'frac_in_range': needed / t / 1e9 / peak}
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled during the timed region."""
 
@@ -956,6 +978,7 @@ def run_ours(args):
                                                                  and W['meshsize'] == 512) else None,
                          'traffic_source': 'ncu dram read+write of the pk_paint kernels (bucket count, column scan, '
                                            'placement, per-shift tiles), this workload at 512^3'},
+            'roofline_binning': binning_roofline(stages, bins, W, peak),
             'e2e': {'value': e2e_value, 'unit': 'spectra/s', 'h2d_bytes_per_step': int(npart * 12),
                     'd2h_bytes_per_step': int(len(W['ells']) * nbins * 8)},
             'gpu_launches': int(launches), 'stages': stage_report, 'clocks': clocks.summary()}

@@ -301,6 +301,14 @@ pk_status pk_ylm_separation_accumulate(void *stream, const float *r, const int32
  * (the conj(F) A0 products of the first-point estimators). */
 pk_status pk_conj_multiply(void *stream, const void *f, const void *a, int nterms, int64_t n, void *out);
 
+/* Wide-angle orders of the first-point window matrix (mesh2.py:1214, 1249, 1273) and mean
+ * spectrum (mesh2.py:1644-1645): mesh_b *= |x|^power (separation = 0: x the cell-corner
+ * position offset + i cellsize, as in pk_ylm_premultiply) or |s|^power (separation = 1: the
+ * separation grid of pk_ylm_separation_accumulate), for nmeshes consecutive real meshes;
+ * |power| <= 8, negative powers as 1 / |x|^-power. */
+pk_status pk_radial_power(void *stream, float *mesh, int nmeshes, const int32_t meshsize[3],
+                          const float cellsize[3], const float offset[3], int separation, int power);
+
 /* pk_bin_global_batch of the meshes that pk_interlace_compensate(_batch) would form
  * (for_c2r = 0, scale 1), without storing them: each mode is combined on the fly from
  * the nshifts interlaced, uncompensated R2C meshes (shifted: nbatch x nshifts Hermitian

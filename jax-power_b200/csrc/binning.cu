@@ -671,9 +671,11 @@ struct RowMap {
 };
 
 // out[e] (+)= sum over CTAs, transposed to [value][bin].  Deterministic two-level sum:
-// 8 threads per entry each add a fixed contiguous range of CTA rows (4 independent loads
-// in flight), then the 8 partials are added in a fixed order.
-constexpr int FIN_ENTRIES = 32, FIN_SPLIT = 8;
+// 32 threads per entry each add a fixed contiguous range of CTA rows (4 independent loads
+// in flight), then the 32 partials are added in a fixed order.  8 entries per CTA: a few
+// hundred entries (bins x multipoles) still make a grid of ~100 CTAs, so the partial rows
+// (one per binning CTA) are read with many loads in flight.
+constexpr int FIN_ENTRIES = 8, FIN_SPLIT = 32;
 __global__ void __launch_bounds__(FIN_ENTRIES * FIN_SPLIT) bin_finalize_kernel(
     const double *__restrict__ partials, int nblocks, int hist_len, int nv, int nbins,
     int accumulate, double *__restrict__ out0, double *__restrict__ out1, RowMap map) {

@@ -536,6 +536,35 @@ __global__ void ylm_separation_accumulate_kernel(Dims d, float c0, float c1, flo
   }
 }
 
+// mesh_b(r) *= |r|^power for nmeshes real meshes: r the cell-corner position o + i cellsize (the
+// x of the Y_lm(xhat) premultiply) or, separation != 0, the separation fftfreq(n)[i] cellsize n
+// (the s of the Y_lm(shat) accumulation), |r| = sqrt((x^2 + y^2) + z^2) in float32; a positive
+// power by repeated products, a negative one as 1 / (|r|^-power) (as JAX's integer powers).
+__global__ void radial_power_kernel(Dims d, float c0, float c1, float c2, float o0, float o1, float o2,
+                                    int separation, int power, int nmeshes, float *__restrict__ mesh) {
+  const int64_t total = d.nreal();
+  const int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  IndexWalker3 w(start, stride, d.n1, d.n2);
+  for (int64_t idx = start; idx < total; idx += stride, w.next()) {
+    float x, y, z;
+    if (separation) {
+      x = kcoord(w.i, d.n0, c0, false);
+      y = kcoord(w.j, d.n1, c1, false);
+      z = kcoord(w.k, d.n2, c2, false);
+    } else {
+      x = __fadd_rn(__fmul_rn((float)w.i, c0), o0);
+      y = __fadd_rn(__fmul_rn((float)w.j, c1), o1);
+      z = __fadd_rn(__fmul_rn((float)w.k, c2), o2);
+    }
+    const float rn = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z)));
+    const int ap = power < 0 ? -power : power;
+    float f = 1.f;
+    for (int q = 0; q < ap; ++q) f = __fmul_rn(f, rn);
+    if (power < 0) f = __fdiv_rn(1.f, f);
+    for (int b = 0; b < nmeshes; ++b) mesh[(int64_t)b * total + idx] = __fmul_rn(mesh[(int64_t)b * total + idx], f);
+  }
+}
+
 // out_t = conj(f_t) * a for nterms complex meshes f_t of n modes each.
 __global__ void conj_multiply_kernel(const float2 *__restrict__ f, const float2 *__restrict__ a, int nterms,
                                      int64_t n, float2 *__restrict__ out) {
@@ -655,6 +684,19 @@ extern "C" pk_status pk_ylm_separation_accumulate(void *stream, const float *r, 
   }
   ylm_separation_accumulate_kernel<<<grid_for(d.nreal(), 256), 256, 0, (cudaStream_t)stream>>>(
       d, cellsize[0], cellsize[1], cellsize[2], t, r, carry);
+  PK_LAUNCH_CHECK();
+  return PK_OK;
+}
+
+extern "C" pk_status pk_radial_power(void *stream, float *mesh, int nmeshes, const int32_t meshsize[3],
+                                     const float cellsize[3], const float offset[3], int separation, int power) {
+  PK_REQUIRE(mesh && cellsize && (separation || offset), PK_ERR_INVALID, "null pointer");
+  PK_REQUIRE(nmeshes >= 1 && power >= -8 && power <= 8, PK_ERR_INVALID, "invalid nmeshes or power");
+  Dims d;
+  PK_REQUIRE(make_dims(meshsize, &d), PK_ERR_INVALID, "invalid meshsize");
+  radial_power_kernel<<<grid_for(d.nreal(), 256), 256, 0, (cudaStream_t)stream>>>(
+      d, cellsize[0], cellsize[1], cellsize[2], separation ? 0.f : offset[0], separation ? 0.f : offset[1],
+      separation ? 0.f : offset[2], separation, power, nmeshes, mesh);
   PK_LAUNCH_CHECK();
   return PK_OK;
 }

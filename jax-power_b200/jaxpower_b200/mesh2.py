@@ -810,15 +810,56 @@ def compute_fkp2_shotnoise(*fkps, bin=None, fields=None):
 
 
 def _window_edges(edgesin, ellsin):
+    """Input k edges as (n, 2) and input multipoles: ints, or (ell, wide-angle order) pairs when
+    any is given as a pair or the container carries wide-angle orders (``mesh2.py:826-836``)."""
     if hasattr(edgesin, 'ells') and hasattr(edgesin, 'poles'):  # a multipole container: its ells and k edges
-        ellsin = edgesin.ells
+        ellsin = list(zip(edgesin.ells, edgesin.wa_orders)) if any(edgesin.wa_orders) else edgesin.ells
         edgesin = next(iter(edgesin)).k_edges
     edgesin = np.asarray(edgesin, dtype='f8')
     if edgesin.ndim != 2:
         edgesin = np.column_stack([edgesin[:-1], edgesin[1:]])
     if np.ndim(ellsin) == 0:
         ellsin = (ellsin,)
+    if any(isinstance(e, tuple) for e in ellsin):
+        return edgesin, [(int(e[0]), int(e[1])) if isinstance(e, tuple) else (int(e), 0) for e in ellsin]
     return edgesin, [int(ell) for ell in ellsin]
+
+
+def _no_wide_angle(ellsin):
+    """Wide-angle orders > 0 are built for the 'firstpoint' theory line of sight only."""
+    if any(isinstance(e, tuple) and e[1] != 0 for e in ellsin):
+        raise NotImplementedError("wide-angle orders > 0 with the 'local' theory line of sight are not supported")
+
+
+def _plain_ells(ellsin):
+    """Input multipoles of a fixed line of sight: wide-angle order 0 only (``mesh2.py:850-851``)."""
+    if any(isinstance(e, tuple) and e[1] != 0 for e in ellsin):
+        raise ValueError('wide-angle orders > 0 need a local (first-point) line of sight')
+    return [e[0] if isinstance(e, tuple) else e for e in ellsin]
+
+
+def _wide_angle_terms(ellsin):
+    """Input multipoles as (ell, wide-angle order) pairs."""
+    return [e if isinstance(e, tuple) else (int(e), 0) for e in ellsin]
+
+
+def _wide_angle_rho(rmesh1, wa, mattrs, offset, cache):
+    """W1 |x|^-wa (``mesh2.py:1214``), W1 itself for wa = 0; cached per order."""
+    if wa == 0:
+        return rmesh1
+    if wa not in cache:
+        rho = rmesh1.clone()
+        _lib.call('pk_radial_power', _lib.stream_handle(), _lib.ptr(rho), 1, _lib.i32(mattrs.meshsize),
+                  _lib.f32(mattrs.cellsize), _lib.f32(offset), 0, -int(wa))
+        cache[wa] = rho
+    return cache[wa]
+
+
+def _wide_angle_s(meshes, nmeshes, wa, mattrs):
+    """meshes *= |s|^wa on the separation grid (``mesh2.py:1214``: Q s^wa), in place."""
+    if wa != 0:
+        _lib.call('pk_radial_power', _lib.stream_handle(), _lib.ptr(meshes), nmeshes, _lib.i32(mattrs.meshsize),
+                  _lib.f32(mattrs.cellsize), None, 1, int(wa))
 
 
 def _window_batch(mattrs, batch_size):
@@ -887,8 +928,8 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     reference's Legendre sum vanishes for odd ell).  Returns a ``WindowMatrix`` of shape
     (len(ells) nbins, len(ellsin) len(edgesin)).  ``buffer`` and ``pbar`` are accepted and
     have no effect; ``batch_size`` caps the columns per FFT batch.  The first-point /
-    end-point line of sight (theory line of sight 'firstpoint', wide-angle order 0) goes
-    through ``_firstpoint_window``, the 'local' theory line of sight (``ellsin=(ells, 'local')``)
+    end-point line of sight (theory line of sight 'firstpoint', inputs ell_in or (ell_in,
+    wide-angle order)) goes through ``_firstpoint_window``, the 'local' theory line of sight (``ellsin=(ells, 'local')``)
     through ``_local_window``.  ``flags=('smooth',)`` with a global line of sight goes through
     ``_smooth_window`` (first point: ``_firstpoint_smooth_window``), ``flags=('infinite',)``
     through ``_infinite_window`` (first point: ``_firstpoint_infinite_window``); 'smooth' with
@@ -927,12 +968,10 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
             theory_los = 'firstpoint'
         if ellsin is not None and np.ndim(ellsin) == 0:
             ellsin = (ellsin,)
-        if ellsin is not None:
-            ellsin = [e if isinstance(e, tuple) else (int(e), 0) for e in ellsin]
-            if any(wa != 0 for _, wa in ellsin):
-                raise NotImplementedError('wide-angle orders > 0 are not supported')
-            ellsin = [e for e, _ in ellsin]
         edgesin, ellsin = _window_edges(edgesin, ellsin)
+        if theory_los == 'local':
+            _no_wide_angle(ellsin)
+            ellsin = _plain_ells(ellsin)
         if 'smooth' in flags and theory_los == 'local':
             wmat = _local_smooth_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm)
         elif 'smooth' in flags:
@@ -944,11 +983,13 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
         return _window_matrix(bin, norm, edgesin, ellsin, wmat)
     if 'infinite' in flags and 'smooth' not in flags:
         edgesin, ellsin = _window_edges(edgesin, ellsin)
+        ellsin = _plain_ells(ellsin)
         Q = None if periodic else _selection_q(meshes, fields, mattrs, N)
         wmat = _infinite_window(mattrs, bin, Q, vlos, ellsin, edgesin, rnorm, batch_size)
         return _window_matrix(bin, norm, edgesin, ellsin, wmat)
     if 'smooth' in flags:
         edgesin, ellsin = _window_edges(edgesin, ellsin)
+        ellsin = _plain_ells(ellsin)
         Q = None if periodic else _selection_q(meshes, fields, mattrs, N)
         wmat = _smooth_window(mattrs, bin, Q, vlos, ellsin, edgesin, rnorm)
         return _window_matrix(bin, norm, edgesin, ellsin, wmat)
@@ -960,18 +1001,16 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
             raise NotImplementedError("theory line of sight '{}' is not supported for the window".format(theory_los))
         if ellsin is not None and np.ndim(ellsin) == 0:
             ellsin = (ellsin,)
-        if ellsin is not None:
-            ellsin = [e if isinstance(e, tuple) else (int(e), 0) for e in ellsin]
-            if any(wa != 0 for _, wa in ellsin):
-                raise NotImplementedError('wide-angle orders > 0 are not supported')
-            ellsin = [e for e, _ in ellsin]
         edgesin, ellsin = _window_edges(edgesin, ellsin)
         if theory_los == 'local':
+            _no_wide_angle(ellsin)
+            ellsin = _plain_ells(ellsin)
             wmat = _local_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm)
         else:
             wmat = _firstpoint_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm, batch_size)
         return _window_matrix(bin, norm, edgesin, ellsin, wmat)
     edgesin, ellsin = _window_edges(edgesin, ellsin)
+    ellsin = _plain_ells(ellsin)
     nin = len(edgesin)
     klo, khi = edgesin[:, 0].astype('f4'), edgesin[:, -1].astype('f4')
 
@@ -1067,8 +1106,10 @@ def _window_matrix(bin, norm, edgesin, ellsin, wmat):
                                                        norm=np.ones(nbins) * norm[ill], ell=ell)
                                      for ill, ell in enumerate(bin.ells)])
     kin = np.mean(edgesin, axis=-1)
+    terms = _wide_angle_terms(ellsin)
     theory = Mesh2SpectrumPoles([Mesh2SpectrumPole(k=kin, k_edges=edgesin, nmodes=np.ones(nin), num_raw=np.zeros(nin),
-                                                   ell=ellin) for ellin in ellsin])
+                                                   ell=ellin, attrs=dict(wa_order=wa) if wa else None)
+                                 for ellin, wa in terms])
     return WindowMatrix(observable=observable, theory=theory, value=wmat)
 
 
@@ -1168,8 +1209,8 @@ def _smooth_window(mattrs, bin, Q, vlos, ellsin, edgesin, rnorm):
 
 
 def _firstpoint_smooth_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm):
-    """'smooth' window of the first-point line of sight, wide-angle order 0
-    (``mesh2.py:1196-1238``): for each ell_in and output ell,
+    """'smooth' window of the first-point line of sight (``mesh2.py:1196-1238``; a wide-angle
+    order n > 0 takes W1 |x|^-n and Q |s|^n, ``mesh2.py:1214``): for each ell_in and output ell,
     ``Qs = 4 pi V_cell sbin(sum_{m, m1} Q_{ell m m1} Y_lm(shat) Y_{ell_in m1}(shat))`` with
     ``Q_{ell m m1} = 4 pi / (2 ell_in + 1) c2r(conj(r2c(W1 Y_lm Y_{ell_in m1})) A0)`` (first bin 0
     for ell > 0), then ``rnorm (-1)^(ell/2) sum_s n_s j_ell(k s) W_in(s) Qs`` per input bin (no
@@ -1199,9 +1240,11 @@ def _firstpoint_smooth_window(meshes, fields, periodic, mattrs, bin, edgesin, el
     nb = bin.nbins
     r1 = torch.empty((1,) + rshape, dtype=torch.float32, device=_device())
     blocks = []
-    for ellin in ellsin:
+    rhos = {}
+    for ellin, wa in _wide_angle_terms(ellsin):
         n1 = 2 * ellin + 1
         in_ell, in_m = _lib.i32([ellin] * n1), _lib.i32(list(range(-ellin, ellin + 1)))
+        rho = _wide_angle_rho(rmesh1, wa, mattrs, offset, rhos)
         R = torch.empty((n1,) + rshape, dtype=torch.float32, device=_device())
         block = np.zeros((len(edgesin), len(ells) * nb))
         shells = [_bessel_shell(ellin, float(lo), float(hi), savg) * (-1) ** (ellin // 2) / (2. * np.pi) ** 3
@@ -1209,7 +1252,7 @@ def _firstpoint_smooth_window(meshes, fields, periodic, mattrs, bin, edgesin, el
         for ill, ell in enumerate(ells):
             carry2 = torch.zeros(rshape, dtype=torch.float32, device=_device())
             for m in range(-ell, ell + 1):
-                _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rmesh1), *geo, 1, _lib.i32([ell]), _lib.i32([m]),
+                _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rho), *geo, 1, _lib.i32([ell]), _lib.i32([m]),
                           _lib.ptr(r1))
                 _lib.call('pk_ylm_premultiply', stream, _lib.ptr(r1), *geo, n1, in_ell, in_m, _lib.ptr(R))
                 F = _r2c(R, meshsize)
@@ -1217,6 +1260,7 @@ def _firstpoint_smooth_window(meshes, fields, periodic, mattrs, bin, edgesin, el
                 G = _c2r(F, meshsize, destroy_input=True)
                 del F
                 _lib.call('pk_scale_real', stream, _lib.ptr(G), G.numel(), float(4. * np.pi / (2 * ellin + 1)))
+                _wide_angle_s(G, n1, wa, mattrs)
                 carry1 = torch.zeros(rshape, dtype=torch.float32, device=_device())
                 _lib.call('pk_ylm_separation_accumulate', stream, _lib.ptr(G), _lib.i32(meshsize),
                           _lib.f32(mattrs.cellsize), n1, in_ell, in_m, _lib.ptr(carry1))
@@ -1451,8 +1495,8 @@ def _local_infinite_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsi
 
 
 def _firstpoint_infinite_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm):
-    """'infinite' window of the first-point line of sight, wide-angle order 0
-    (``mesh2.py:1240-1262``): for each ell_in and output (ell, m),
+    """'infinite' window of the first-point line of sight (``mesh2.py:1240-1262``; a wide-angle
+    order n > 0 takes W1 |x|^-n and Q |s|^n, ``mesh2.py:1249``): for each ell_in and output (ell, m),
     ``C_{ell m} = V_cell sum_m1 Y_{ell_in m1}(shat) Q_{ell m m1}`` (``pk_ylm_separation_accumulate``),
     then per input bin ``4 pi rnorm bin(sum_m r2c(W_in(|s|) C_{ell m}) Y_lm(khat))`` with k = 0
     dropped for ell = 0 only, ``W_in`` the tophat Bessel profile tabulated on the distinct |s|."""
@@ -1482,13 +1526,15 @@ def _firstpoint_infinite_window(meshes, fields, periodic, mattrs, bin, edgesin, 
     r1 = torch.empty((1,) + rshape, dtype=torch.float32, device=_device())
     col = torch.empty(rshape, dtype=torch.float32, device=_device())
     blocks = []
-    for ellin in ellsin:
+    rhos = {}
+    for ellin, wa in _wide_angle_terms(ellsin):
         n1 = 2 * ellin + 1
         in_ell, in_m = _lib.i32([ellin] * n1), _lib.i32(list(range(-ellin, ellin + 1)))
+        rho = _wide_angle_rho(rmesh1, wa, mattrs, offset, rhos)
         R = torch.empty((n1,) + rshape, dtype=torch.float32, device=_device())
         C = torch.zeros((len(out_terms),) + rshape, dtype=torch.float32, device=_device())
         for t, (ell, m) in enumerate(out_terms):
-            _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rmesh1), *geo, 1, _lib.i32([ell]), _lib.i32([m]),
+            _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rho), *geo, 1, _lib.i32([ell]), _lib.i32([m]),
                       _lib.ptr(r1))
             _lib.call('pk_ylm_premultiply', stream, _lib.ptr(r1), *geo, n1, in_ell, in_m, _lib.ptr(R))
             F = _r2c(R, meshsize)
@@ -1496,6 +1542,7 @@ def _firstpoint_infinite_window(meshes, fields, periodic, mattrs, bin, edgesin, 
             G = _c2r(F, meshsize, destroy_input=True)
             del F
             _lib.call('pk_scale_real', stream, _lib.ptr(G), G.numel(), float(4. * np.pi / (2 * ellin + 1) * cellvol))
+            _wide_angle_s(G, n1, wa, mattrs)
             _lib.call('pk_ylm_separation_accumulate', stream, _lib.ptr(G), _lib.i32(meshsize),
                       _lib.f32(mattrs.cellsize), n1, in_ell, in_m, _lib.ptr(C[t]))
             del G
@@ -1674,8 +1721,9 @@ def _local_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, 
 
 
 def _firstpoint_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm, batch_size=None):
-    """First-point window matrix, input power on the mesh, wide-angle order 0
-    (``mesh2.py:1264-1304``, ``1462-1470``).  For each input ell_in:
+    """First-point window matrix, input power on the mesh (``mesh2.py:1264-1304``,
+    ``1462-1470``).  For each input (ell_in, wide-angle order n) (n = 0 for a plain ell_in; for
+    n > 0 W1 is W1 |x|^-n and each Q is multiplied by |s|^n, ``mesh2.py:1273``):
 
         Q_{ell m m1} = 4 pi / (2 ell_in + 1) c2r(conj(r2c(W1 Y_lm(xhat) Y_{ell_in m1}(xhat))) A0),
 
@@ -1707,21 +1755,24 @@ def _firstpoint_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, s
     knorm = torch.sqrt(kvec[0] ** 2 + kvec[1] ** 2 + kvec[2] ** 2)
     r1 = torch.empty((1,) + rshape, dtype=torch.float32, device=_device())
     blocks = []
-    for ellin in ellsin:
+    rhos = {}
+    for ellin, wa in _wide_angle_terms(ellsin):
         n1 = 2 * ellin + 1
         if n1 > 32:
             raise NotImplementedError('ell_in <= 15')
         in_ell, in_m = _lib.i32([ellin] * n1), _lib.i32(list(range(-ellin, ellin + 1)))
+        rho = _wide_angle_rho(rmesh1, wa, mattrs, offset, rhos)
         # Q[t] for output term t: (n1, N) real meshes
         Q = torch.empty((len(out_terms), n1) + rshape, dtype=torch.float32, device=_device())
         R = torch.empty((n1,) + rshape, dtype=torch.float32, device=_device())
         for t, (ell, m) in enumerate(out_terms):
-            _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rmesh1), *geo, 1, _lib.i32([ell]), _lib.i32([m]),
+            _lib.call('pk_ylm_premultiply', stream, _lib.ptr(rho), *geo, 1, _lib.i32([ell]), _lib.i32([m]),
                       _lib.ptr(r1))
             _lib.call('pk_ylm_premultiply', stream, _lib.ptr(r1), *geo, n1, in_ell, in_m, _lib.ptr(R))
             F = _r2c(R, meshsize)
             _lib.call('pk_conj_multiply', stream, _lib.ptr(F), _lib.ptr(A0), n1, A0.numel(), _lib.ptr(F))
             Q[t] = _c2r(F, meshsize, destroy_input=True)
+            _wide_angle_s(Q[t], n1, wa, mattrs)
             del F
         coef = np.full(n1, 4. * np.pi / (2 * ellin + 1), dtype='f4')
         rows = []
@@ -1809,7 +1860,7 @@ def _local_theory_pairs(poles, get_theory, rnorm):
 def _firstpoint_mean(meshes, fields, periodic, mattrs, bin, poles, get_theory, swap, N, norm, rnorm,
                      theory_los='firstpoint'):
     """First-point branch of compute_mesh2_spectrum_mean (``mesh2.py:1607-1669``, theory line of
-    sight 'firstpoint', wide-angle order 0).  For each output (ell, m):
+    sight 'firstpoint'; theory keys ell or (ell, wide-angle order)).  For each output (ell, m):
 
         Q = sum over theory (ell1, m1) of 4 pi / (2 ell1 + 1) xi_{ell1 m1} G,
         xi_{ell1 m1} = c2r(P_ell1(k) rnorm Y_{ell1 m1}(khat)),
@@ -1846,11 +1897,7 @@ def _firstpoint_mean(meshes, fields, periodic, mattrs, bin, poles, get_theory, s
     # per wide-angle order wa: the theory terms, their xi_{ell1 m1} = c2r(P rnorm Y(khat)) s^wa, and
     # the mesh W1 |x|^-wa that the Y_lm(xhat) products start from (mesh2.py:1641-1645)
     was = sorted({wa for _, wa in poles})
-    if any(wa != 0 for wa in was):
-        px, py, pz = mattrs.rcoords(kind='position', sparse=True)
-        xnorm = torch.sqrt((px * px + py * py) + pz * pz)
-        sx, sy, sz = mattrs.rcoords(kind='separation', sparse=True)
-        snorm = torch.sqrt((sx * sx + sy * sy) + sz * sz)
+    rhos = {}
     groups = []
     for wa in was:
         terms1 = [(ell1, m1) for (ell1, w) in poles if w == wa for m1 in range(-ell1, ell1 + 1)]
@@ -1870,10 +1917,8 @@ def _firstpoint_mean(meshes, fields, periodic, mattrs, bin, poles, get_theory, s
             t0 += n1
         xi = _c2r(xi_c, meshsize, destroy_input=True)
         del xi_c
-        rho = rmesh1
-        if wa != 0:
-            xi = (xi * snorm ** wa).contiguous()
-            rho = (rmesh1 * xnorm ** (-wa)).contiguous()
+        _wide_angle_s(xi, len(terms1), wa, mattrs)
+        rho = _wide_angle_rho(rmesh1, wa, mattrs, offset, rhos)
         groups.append((rho, terms1, coef, xi,
                        torch.empty((len(terms1),) + rshape, dtype=torch.float32, device=_device())))
     num = []
@@ -1993,7 +2038,7 @@ def compute_mesh2_spectrum_mean(*meshes, theory, bin=None, los='z'):
     code), then ``A <- r2c(Q c2r(A))`` with ``Q = c2r(W1 W2*)`` for a selection function, else
     ``A <- N A``; each even ell is ``(2 ell + 1) bin(A L_ell(mu))`` with k = 0 kept, in one
     fused binning pass (``pk_bin_window_batch``); odd ell is 0.  The first-point / end-point
-    line of sight takes theory multipoles (wide-angle order 0) through ``_firstpoint_mean``.
+    line of sight takes theory multipoles (keys ell or (ell, wide-angle order)) through ``_firstpoint_mean``.
     The 'jaxdecomp' layout raises ``NotImplementedError``.
     """
     _plain_bins(bin, 'compute_mesh2_spectrum_mean')
@@ -2111,8 +2156,11 @@ def compute_smooth2_spectrum_window(window, edgesin, ellsin=None, bin=None, flag
     (``_window_coeffs``), then per input bin (mid-point k_in) and output k
     ``(-1)^(ell/2) sum_s j_ell(k s) n_s (-1)^(ell_in/2) / (2 pi)^3 j_ell_in(k_in s) V_in Qs(s)``,
     ``n_s`` the window's ``volume`` (ones if absent), ``V_in = 4 pi / 3 (k_hi^3 - k_lo^3)``.  These
-    are 1D host sums over the window's separations (no mesh work).  The 'fftlog' integration
-    (any flag set without 'rect') and wide-angle orders > 0 raise ``NotImplementedError``.
+    are 1D host sums over the window's separations (no mesh work).  Wide-angle inputs
+    (ell_in, n) take the window multipoles labelled with order n (``window.wa_orders``) and an
+    extra s^n (``mesh2.py:845-851, 869``); an order n > 0 needs a window carrying wide-angle
+    labels (``ValueError`` otherwise, as the reference).  The 'fftlog' integration (any flag
+    set without 'rect') raises ``NotImplementedError``.
     """
     from scipy.special import spherical_jn
     if 'rect' not in flags:
@@ -2125,7 +2173,8 @@ def compute_smooth2_spectrum_window(window, edgesin, ellsin=None, bin=None, flag
     if edgesin.ndim != 2:
         edgesin = np.column_stack([edgesin[:-1], edgesin[1:]])
     ellsin = [e if isinstance(e, tuple) else (int(e), 0) for e in ((ellsin,) if np.ndim(ellsin) == 0 else ellsin)]
-    if any(wa != 0 for _, wa in ellsin):
+    labelled = any(getattr(window, 'wa_orders', ()))
+    if any(wa != 0 for _, wa in ellsin) and not labelled:
         raise ValueError('wa_orders must be provided in input window')
     kout = np.asarray(bin.xavg, dtype='f8')
     first = next(iter(window))
@@ -2135,19 +2184,20 @@ def compute_smooth2_spectrum_window(window, edgesin, ellsin=None, bin=None, flag
     kin = np.mean(edgesin, axis=-1)
     vin = 4. / 3. * np.pi * (edgesin[:, 1] ** 3 - edgesin[:, 0] ** 3)
 
-    def get_w(q):
-        if q in window.ells:
-            return np.real(np.asarray(window.get(q).value(), dtype='c16'))
+    def get_w(q, wa):
+        keys = list(zip(window.ells, window.wa_orders)) if labelled else [(e, 0) for e in window.ells]
+        if (q, wa) in keys:
+            return np.real(np.asarray(window.get(q, wa_orders=wa if labelled else None).value(), dtype='c16'))
         return 0.
 
     blocks = []
-    for ellin, _ in ellsin:
+    for ellin, wa in ellsin:
         col = []
         for ell in ells:
-            Qs = sum(coeff * get_w(q) for q, coeff in _window_coeffs(ell, ellin))
+            Qs = sum(coeff * get_w(q, wa) for q, coeff in _window_coeffs(ell, ellin))
             Qs = np.where(snmodes == 0, 0., Qs)
             tophat = ((-1) ** (ellin // 2) / (2. * np.pi) ** 3 * spherical_jn(ellin, savg[None, :] * kin[:, None])
-                      * vin[:, None] * Qs)  # (nin, ns)
+                      * vin[:, None] * Qs * savg[None, :] ** wa)  # (nin, ns)
             jk = (-1) ** (ell // 2) * spherical_jn(ell, kout[:, None] * savg[None, :])  # (nbins, ns)
             col.append(jk.dot((snmodes * tophat).T))  # (nbins, nin)
         blocks.append(np.concatenate(col, axis=0))
@@ -2156,6 +2206,7 @@ def compute_smooth2_spectrum_window(window, edgesin, ellsin=None, bin=None, flag
                                                        num_raw=np.zeros(len(kout)), num_shotnoise=np.zeros(len(kout)),
                                                        norm=np.ones(len(kout)), ell=ell) for ell in ells])
     theory = Mesh2SpectrumPoles([Mesh2SpectrumPole(k=kin, k_edges=edgesin, nmodes=np.ones(len(kin)),
-                                                   num_raw=np.zeros(len(kin)), ell=ellin) for ellin, _ in ellsin])
+                                                   num_raw=np.zeros(len(kin)), ell=ellin,
+                                                   attrs=dict(wa_order=wa) if wa else None) for ellin, wa in ellsin])
     from .types import WindowMatrix
     return WindowMatrix(observable=observable, theory=theory, value=wmat)

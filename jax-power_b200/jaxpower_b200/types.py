@@ -140,20 +140,34 @@ class Mesh2SpectrumPoles:
     def ells(self):
         return tuple(p.ell for p in self.poles)
 
+    @property
+    def wa_orders(self):
+        """Wide-angle order of each pole (``attrs['wa_order']``, 0 when absent): the theory side
+        of a first-point window matrix (the reference's ``wa_orders`` label)."""
+        return tuple(int(p.attrs.get('wa_order', 0)) for p in self.poles)
+
     def __iter__(self):
         return iter(self.poles)
 
     def __len__(self):
         return len(self.poles)
 
-    def get(self, ells=None, ell=None):
+    def _index(self, ell, wa_order):
+        keys = list(zip(self.ells, self.wa_orders))
+        if wa_order is None:
+            return self.ells.index(int(ell))
+        return keys.index((int(ell), int(wa_order)))
+
+    def get(self, ells=None, ell=None, wa_orders=None):
         if ells is None:
             ells = ell
         if ells is None:
             return self
         if np.ndim(ells) == 0:
-            return self.poles[self.ells.index(int(ells))]
-        return self.__class__([self.poles[self.ells.index(int(e))] for e in ells])
+            return self.poles[self._index(ells, wa_orders)]
+        was = [None] * len(ells) if wa_orders is None else (list(wa_orders) if np.ndim(wa_orders) else
+                                                            [wa_orders] * len(ells))
+        return self.__class__([self.poles[self._index(e, w)] for e, w in zip(ells, was)])
 
     def value(self):
         return np.concatenate([p.value() for p in self.poles])

@@ -399,10 +399,28 @@ def compute_mesh2_spectrum_mean_firstpoint(bins, theory, meshes=None, swap=False
     return np.array(out)
 
 
+def _wide_angle_factors(geom, wa):
+    """``xnorm**(-wain)`` and ``snorm**wain`` of the first-point window (``mesh2.py:1212-1214``):
+    |x| of the cell-corner positions and |s| of the separation grid, in the geometry's dtype
+    (negative powers as 1 / |x|^-wa)."""
+    dt = geom.dtype
+    t = dt.type
+    x = rcoords(geom)
+    s = separation_coords(geom)
+    xn = np.sqrt((((t(0.) + x[0] * x[0]).astype(dt) + x[1] * x[1]).astype(dt) + x[2] * x[2]).astype(dt)).astype(dt)
+    sn = np.sqrt((((t(0.) + s[0] * s[0]).astype(dt) + s[1] * s[1]).astype(dt) + s[2] * s[2]).astype(dt)).astype(dt)
+    with np.errstate(divide='ignore'):
+        return (t(1.) / xn ** wa).astype(dt), (sn ** wa).astype(dt)
+
+
+def _wa_terms(ellsin):
+    return [e if isinstance(e, tuple) else (int(e), 0) for e in ellsin]
+
+
 def compute_mesh2_spectrum_window_firstpoint(bins, edgesin, ellsin, meshes=None, swap=False, norm=None,
                                              theory_los='firstpoint'):
     """``compute_mesh2_spectrum_window(..., los='firstpoint' / 'endpoint')``, input power on the
-    mesh, wide-angle order 0 (``mesh2.py:1135-1304``, ``1462-1470``).  ``meshes``: None
+    mesh (``mesh2.py:1135-1304``, ``1462-1470``); inputs ell_in or (ell_in, wide-angle order).  ``meshes``: None
     (periodic box) or one / two real selection meshes.  Returns the window matrix
     (len(ells) nbins, len(ellsin) len(edgesin))."""
     geom = bins.geom
@@ -465,13 +483,17 @@ def compute_mesh2_spectrum_window_firstpoint(bins, edgesin, ellsin, meshes=None,
         wmat[:nb] = first
         return wmat
     blocks = []
-    for ellin in ellsin:
+    for ellin, wa in _wa_terms(ellsin):  # wide-angle order wa: W1 |x|^-wa, Q |s|^wa (mesh2.py:1273)
+        xf, sf = _wide_angle_factors(geom, wa)
+        rho = (rmesh1 * xf).astype(dt) if wa else rmesh1
         Qs = {}
         for ell in ells:
             for m in range(-ell, ell + 1):
                 for m1 in range(-ellin, ellin + 1):
-                    F = r2c(geom, ((rmesh1 * get_ylm(ell, m)(*xvec)).astype(dt) * get_ylm(ellin, m1)(*xvec)).astype(dt))
+                    F = r2c(geom, ((rho * get_ylm(ell, m)(*xvec)).astype(dt) * get_ylm(ellin, m1)(*xvec)).astype(dt))
                     Qs[ell, m, m1] = (t(4. * np.pi / (2 * ellin + 1)) * c2r(geom, (np.conj(F) * A0).astype(np.complex64))).astype(dt)
+                    if wa:
+                        Qs[ell, m, m1] = (Qs[ell, m, m1] * sf).astype(dt)
         rows = []
         for lo, hi in edgesin.astype(dt):
             xi = {m1: c2r(geom, (((knorm >= lo) & (knorm <= hi)) * get_ylm(ellin, m1)(*kvec)).astype(np.complex64))
@@ -631,8 +653,8 @@ def compute_mesh2_spectrum_window_infinite(bins, edgesin, ellsin, los='z', meshe
 
 
 def compute_mesh2_spectrum_window_firstpoint_smooth(bins, sedges, edgesin, ellsin, meshes=None, swap=False):
-    """``compute_mesh2_spectrum_window(..., los='firstpoint', flags=('smooth',))``, wide-angle
-    order 0 (``mesh2.py:1196-1238``): ``Qs = 4 pi V_cell sum_{m, m1} sbin(Q Y_lm(shat) Y_l1m1(shat))``,
+    """``compute_mesh2_spectrum_window(..., los='firstpoint', flags=('smooth',))``, inputs ell_in
+    or (ell_in, wide-angle order) (``mesh2.py:1196-1238``): ``Qs = 4 pi V_cell sum_{m, m1} sbin(Q Y_lm(shat) Y_l1m1(shat))``,
     ``Q = 4 pi / (2 ell_in + 1) c2r(conj(r2c(W1 Y_lm(xhat) Y_l1m1(xhat))) A0)``, then
     ``rnorm (-1)^(ell/2) sum_s n_s j_ell(k s) W(s) Qs`` (adaptive quadrature for W)."""
     from scipy.integrate import quad
@@ -667,7 +689,9 @@ def compute_mesh2_spectrum_window_firstpoint_smooth(bins, sedges, edgesin, ellsi
                                  epsrel=1e-9)[0]
 
     blocks = []
-    for ellin in ellsin:
+    for ellin, wa in _wa_terms(ellsin):  # wide-angle order wa: W1 |x|^-wa, Q |s|^wa (mesh2.py:1214)
+        xf, sf = _wide_angle_factors(geom, wa)
+        rho = (rmesh1 * xf).astype(dt) if wa else rmesh1
         block = np.zeros((len(edgesin), len(ells) * bins.nbins))
         for ill, ell in enumerate(ells):
             Qs = 0.
@@ -675,8 +699,10 @@ def compute_mesh2_spectrum_window_firstpoint_smooth(bins, sedges, edgesin, ellsi
                 Y1 = get_ylm(ellin, m1)
                 for m in range(-ell, ell + 1):
                     Y = get_ylm(ell, m)
-                    F = r2c(geom, ((rmesh1 * Y(*xvec)).astype(dt) * Y1(*xvec)).astype(dt))
+                    F = r2c(geom, ((rho * Y(*xvec)).astype(dt) * Y1(*xvec)).astype(dt))
                     Q = (t(4. * np.pi / (2 * ellin + 1)) * c2r(geom, (np.conj(F) * A0).astype(np.complex64))).astype(dt)
+                    if wa:
+                        Q = (Q * sf).astype(dt)
                     Qs = Qs + 4. * np.pi * sbin(Q.astype('f8') * Y(*svec) * Y1(*svec)) * cellvol
             if ell != 0:
                 Qs[0] = 0.
@@ -694,7 +720,8 @@ def compute_mesh2_spectrum_window_firstpoint_smooth(bins, sedges, edgesin, ellsi
 
 def compute_smooth2_spectrum_window(s, windows, snmodes, edgesin, ellsin, ells, kout):
     """``compute_smooth2_spectrum_window(window, edgesin, ellsin, bin, flags=('rect',))``
-    (``mesh2.py:803-918``) as plain loops: ``windows`` {q: W_q(s)}, coefficients
+    (``mesh2.py:803-918``) as plain loops: ``windows`` {q: W_q(s)} or, with wide-angle inputs
+    (ell_in, n), {(q, n): W_q,n(s)} with the extra s^n of ``mesh2.py:869``; coefficients
     ``(2 ell + 1) (ell ellin q; 0 0 0)^2`` from sympy's Wigner 3j symbols."""
     from scipy.special import spherical_jn
     from sympy.physics.wigner import wigner_3j
@@ -704,13 +731,15 @@ def compute_smooth2_spectrum_window(s, windows, snmodes, edgesin, ellsin, ells, 
     savg = np.where(snmodes == 0, 0., s)
     wmat = np.zeros((len(ells) * len(kout), len(ellsin) * len(edgesin)))
     for iin, ellin in enumerate(ellsin):
+        ellin, wa = ellin if isinstance(ellin, tuple) else (ellin, None)
         for ill, ell in enumerate(ells):
             Qs = np.zeros_like(s)
             for q in range(abs(ell - ellin), ell + ellin + 1):
                 c = (2 * ell + 1) * float(wigner_3j(ell, ellin, q, 0, 0, 0)) ** 2
-                if abs(c) >= 1e-7 and q in windows:
-                    Qs = Qs + c * windows[q]
-            Qs = np.where(snmodes == 0, 0., Qs)
+                key = q if wa is None else (q, wa)
+                if abs(c) >= 1e-7 and key in windows:
+                    Qs = Qs + c * windows[key]
+            Qs = np.where(snmodes == 0, 0., Qs) * savg ** (wa or 0)
             for e, (lo, hi) in enumerate(edgesin):
                 kin = (lo + hi) / 2.
                 tophat = (-1) ** (ellin // 2) / (2. * np.pi) ** 3 * spherical_jn(ellin, savg * kin) * 4. / 3. * np.pi * (hi ** 3 - lo ** 3) * Qs
@@ -721,8 +750,8 @@ def compute_smooth2_spectrum_window(s, windows, snmodes, edgesin, ellsin, ells, 
 
 
 def compute_mesh2_spectrum_window_firstpoint_infinite(bins, edgesin, ellsin, meshes=None, swap=False):
-    """``compute_mesh2_spectrum_window(..., los='firstpoint', flags=('infinite',))``, wide-angle
-    order 0 (``mesh2.py:1240-1262``): ``Qs = V_cell sum_m1 Y_l1m1(shat) Q``, then per input bin
+    """``compute_mesh2_spectrum_window(..., los='firstpoint', flags=('infinite',))``, inputs
+    ell_in or (ell_in, wide-angle order) (``mesh2.py:1240-1262``): ``Qs = V_cell sum_m1 Y_l1m1(shat) Q``, then per input bin
     ``4 pi rnorm sum_m bin(Y_lm(khat) r2c(W(|s|) Qs))`` (adaptive quadrature for W)."""
     from scipy.integrate import quad
     from scipy.special import spherical_jn
@@ -753,7 +782,9 @@ def compute_mesh2_spectrum_window_firstpoint_infinite(bins, edgesin, ellsin, mes
                                  epsrel=1e-9)[0]
 
     blocks = []
-    for ellin in ellsin:
+    for ellin, wa in _wa_terms(ellsin):  # wide-angle order wa: W1 |x|^-wa, Q |s|^wa (mesh2.py:1249)
+        xf, sf = _wide_angle_factors(geom, wa)
+        rho = (rmesh1 * xf).astype(dt) if wa else rmesh1
         profiles = []
         for lo, hi in edgesin.astype(dt):
             prof = np.array([shell(ellin, float(lo), float(hi), x) for x in uniq]) * (-1) ** (ellin // 2) / (2. * np.pi) ** 3
@@ -765,8 +796,10 @@ def compute_mesh2_spectrum_window_firstpoint_infinite(bins, edgesin, ellsin, mes
                 Qs = 0.
                 for m1 in range(-ellin, ellin + 1):
                     Y1 = get_ylm(ellin, m1)
-                    F = r2c(geom, ((rmesh1 * Y(*xvec)).astype(dt) * Y1(*xvec)).astype(dt))
+                    F = r2c(geom, ((rho * Y(*xvec)).astype(dt) * Y1(*xvec)).astype(dt))
                     Q = (t(4. * np.pi / (2 * ellin + 1)) * c2r(geom, (np.conj(F) * A0).astype(np.complex64))).astype(dt)
+                    if wa:
+                        Q = (Q * sf).astype(dt)
                     Qs = Qs + Y1(*svec).astype('f8') * Q * cellvol
                 for e, prof in enumerate(profiles):
                     A = (Y(*kvec) * r2c(geom, (prof * Qs).astype(dt))).astype(np.complex64)

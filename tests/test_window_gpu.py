@@ -440,3 +440,48 @@ def test_wide_angle_mean_spectrum_matches_oracle(selection):
                                              los='firstpoint')
         ref = omean_fp(ob, theory, meshes=[sel])
     _check(np.array([p.num_raw for p in got]), ref)
+
+
+@pytest.mark.parametrize('flag', [None, 'smooth', 'infinite'])
+@pytest.mark.parametrize('los', ['firstpoint', 'endpoint'])
+def test_firstpoint_window_wide_angle_matches_oracle(flag, los):
+    """First-point window matrices with wide-angle theory orders (ell_in, wa): the selection
+    mesh times |x|^-wa and the real-space products times |s|^wa (mesh2.py:1214, 1249, 1273)."""
+    import jaxpower_b200 as jp
+    from oracle import spectrum as ospec
+    meshsize, boxsize, center = (10, 8, 8), np.array([500., 400., 400.]), (900., -200., 300.)
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=center)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.02}, ells=(0, 2))
+    ob = Bins(Geometry(meshsize, boxsize, center), step=0.02, ells=(0, 2))
+    sel = np.random.default_rng(37).uniform(0.5, 1.5, meshsize).astype('f4')
+    mesh = attrs.create(kind='real', fill=torch.as_tensor(sel))
+    ellsin = [(0, 0), (0, 1), (2, 1), (1, 2)]
+    edgesin = np.arange(0.005, 0.06, 0.02)
+    w = jp.compute_mesh2_spectrum_window(mesh, edgesin=edgesin, ellsin=(ellsin, 'firstpoint'), bin=b, los=los,
+                                         flags=(flag,) if flag else ())
+    swap = los == 'endpoint'
+    if flag is None:
+        ref = ospec.compute_mesh2_spectrum_window_firstpoint(ob, edgesin, ellsin, meshes=[sel], swap=swap)
+    elif flag == 'smooth':
+        sedges = jp.BinMesh2CorrelationPoles(attrs)._edges1d
+        ref = ospec.compute_mesh2_spectrum_window_firstpoint_smooth(ob, sedges, edgesin, ellsin, meshes=[sel],
+                                                                    swap=swap)
+    else:
+        ref = ospec.compute_mesh2_spectrum_window_firstpoint_infinite(ob, edgesin, ellsin, meshes=[sel], swap=swap)
+    _check(w.value, ref)
+    assert w.theory.ells == (0, 0, 2, 1) and w.theory.wa_orders == (0, 1, 1, 2)
+    assert w.theory.get(0, wa_orders=1) is w.theory.poles[1]
+    # the wide-angle columns differ from the order-0 ones (the |x|^-wa |s|^wa factors act)
+    n = len(edgesin)
+    assert not np.allclose(w.value[:, :n], w.value[:, n:2 * n])
+
+
+def test_wide_angle_needs_local_line_of_sight():
+    import jaxpower_b200 as jp
+    attrs = jp.MeshAttrs(meshsize=8, boxsize=400.)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.05}, ells=(0,))
+    with pytest.raises(ValueError):
+        jp.compute_mesh2_spectrum_window(attrs, edgesin=np.array([0., 0.1]), ellsin=[(0, 1)], bin=b, los='z')
+    with pytest.raises(NotImplementedError):
+        jp.compute_mesh2_spectrum_window(attrs, edgesin=np.array([0., 0.1]), ellsin=([(0, 1)], 'local'), bin=b,
+                                         los='firstpoint')

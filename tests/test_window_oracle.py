@@ -73,3 +73,35 @@ def test_smooth2_window_from_correlation_multipoles():
     assert w.value.shape == ref.shape == (3 * bin.xavg.size, 3 * (edgesin.size - 1))
     assert np.allclose(w.value, ref, rtol=1e-10, atol=1e-12 * np.abs(ref).max())
     assert w.theory.ells == (0, 2, 4)
+
+
+def test_smooth2_window_wide_angle_orders():
+    """compute_smooth2_spectrum_window with wide-angle inputs (ell_in, n): the window multipoles
+    labelled with order n times s^n (mesh2.py:845-851, 869); an order n > 0 without labelled
+    window multipoles raises ValueError (mesh2.py:850-851)."""
+    from types import SimpleNamespace
+    import jaxpower_b200 as jp
+    from oracle.spectrum import compute_smooth2_spectrum_window as osmooth2
+    s = np.linspace(2.5, 200., 60)
+    nmodes = np.full(s.size, 3.)
+    windows = {(0, 0): np.exp(-s / 80.), (2, 0): 0.3 * np.exp(-s / 60.), (0, 1): 0.01 * np.exp(-s / 50.),
+               (2, 1): 0.004 * np.exp(-s / 70.), (1, 1): 0.02 * np.exp(-s / 90.)}
+    poles = jp.Mesh2CorrelationPoles([jp.Mesh2CorrelationPole(s=s, s_edges=np.column_stack([s - 1.25, s + 1.25]),
+                                                               nmodes=nmodes, num_raw=w, volume=nmodes, ell=q,
+                                                               attrs=dict(wa_order=n))
+                                      for (q, n), w in windows.items()])
+    assert poles.wa_orders == (0, 0, 1, 1, 1)
+    kedges = np.arange(0.01, 0.2, 0.02)
+    bin = SimpleNamespace(ells=(0, 1, 2), xavg=(kedges[:-1] + kedges[1:]) / 2.,
+                          edges=np.column_stack([kedges[:-1], kedges[1:]]), nmodes=np.ones(kedges.size - 1))
+    edgesin = np.arange(0., 0.25, 0.025)
+    ellsin = [(0, 0), (2, 0), (1, 1), (0, 1)]
+    w = jp.compute_smooth2_spectrum_window(poles, edgesin=edgesin, ellsin=ellsin, bin=bin)
+    ref = osmooth2(s, windows, nmodes, edgesin, ellsin, (0, 1, 2), bin.xavg)
+    assert np.allclose(w.value, ref, rtol=1e-10, atol=1e-12 * np.abs(ref).max())
+    assert w.theory.wa_orders == (0, 0, 1, 1)
+    plain = jp.Mesh2CorrelationPoles([jp.Mesh2CorrelationPole(s=s, s_edges=np.column_stack([s - 1.25, s + 1.25]),
+                                                               nmodes=nmodes, num_raw=windows[q, 0], volume=nmodes,
+                                                               ell=q) for q in (0, 2)])
+    with pytest.raises(ValueError):
+        jp.compute_smooth2_spectrum_window(plain, edgesin=edgesin, ellsin=[(0, 1)], bin=bin)
