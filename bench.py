@@ -918,7 +918,10 @@ def run_ours(args):
     if not args.no_e2e:
         # every step copies its positions from pinned host memory and reads its multipoles
         # back to the host; the copy of step k + 1 runs on a copy stream while step k computes
-        # (two device buffers, events order the copy after the step that last used the buffer)
+        # (two device buffers, events order the copy after the step that last used the buffer),
+        # and step k's multipoles are read back (prefetch: a side-stream copy) while step k + 1
+        # runs: the host waits for them after enqueuing step k + 1, the last one before the
+        # timing event
         host = torch.empty(positions.shape, dtype=torch.float32, pin_memory=True)
         host.copy_(positions)
         bufs = [torch.empty_like(positions) for _ in range(2)]
@@ -936,13 +939,19 @@ def run_ours(args):
         def run_steps(n):
             copy_stream.wait_stream(compute)  # the first copy starts after the timing event
             issue_copy(0)
+            prev = None
             for k in range(n):
                 if k + 1 < n:
                     issue_copy(k + 1)
                 compute.wait_event(copied[k % 2])
                 res = step(bufs[k % 2])
                 used[k % 2].record(compute)
-                _ = res.value()
+                res.prefetch()
+                if prev is not None:
+                    _ = prev.value()
+                prev = res
+            if prev is not None:
+                _ = prev.value()
 
         for e in used:
             e.record(compute)

@@ -10,7 +10,9 @@ normalisation that reproduces the reference's golden ``value().std()``),
 ``coords('k')``, ``ells``.  Arrays are NumPy float64 on the host.  ``num_raw`` may be given
 as a deferred value (``DeferredRows``): the estimator's per-bin sums stay on the device and
 are read back, once for all multipoles, when ``num_raw`` is first used, so that computing a
-spectrum does not wait for the GPU (as JAX arrays do not).
+spectrum does not wait for the GPU (as JAX arrays do not).  ``Mesh2SpectrumPoles.prefetch()``
+starts that read-back on a side stream, so that reading a spectrum after enqueuing the next
+one waits only for the first.
 
 On disk (``write`` / ``read``, the names lsstypes exports and ``types.py:5-7`` re-exports):
 lsstypes' own HDF5 layout is not available here (neither lsstypes nor h5py is installed),
@@ -36,18 +38,55 @@ class DeferredRows:
     def __init__(self, sums, divisor, scales):
         self._sums = sums
         self._host = None
+        self._pending = None
         self._divisor = np.asarray(divisor, dtype='f8')
         self._scales = list(scales)
         self.shape = tuple(sums.shape[1:])
 
+    def prefetch(self):
+        """Start the read-back now: a copy into pinned host memory on a side stream that waits
+        only for the sums, so that a later read waits for that copy, not for the work the caller
+        has enqueued since (e.g. the next spectrum)."""
+        if self._host is not None or self._pending is not None or not getattr(self._sums, 'is_cuda', False):
+            return
+        import torch
+        ready = torch.cuda.Event()
+        ready.record()
+        stream = _readback_stream(self._sums.device)
+        host = torch.empty(self._sums.shape, dtype=self._sums.dtype, pin_memory=True)
+        with torch.cuda.stream(stream):
+            stream.wait_event(ready)
+            host.copy_(self._sums, non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(stream)
+        self._sums.record_stream(stream)
+        self._pending = (host, done)
+
     def _read(self):
         if self._host is None:
-            self._host = self._sums.cpu().numpy()
+            if self._pending is not None:
+                host, done = self._pending
+                done.synchronize()
+                self._host = host.numpy()
+                self._pending = None
+            else:
+                self._host = self._sums.cpu().numpy()
             self._sums = None
         return self._host
 
     def row(self, i):
         return _DeferredRow(self, i)
+
+
+_READBACK_STREAMS = {}
+
+
+def _readback_stream(device):
+    import torch
+    key = torch.device(device).index
+    if key not in _READBACK_STREAMS:
+        _READBACK_STREAMS[key] = torch.cuda.Stream(device=device)
+    return _READBACK_STREAMS[key]
 
 
 class _DeferredRow:
@@ -171,6 +210,15 @@ class Mesh2SpectrumPoles:
 
     def value(self):
         return np.concatenate([p.value() for p in self.poles])
+
+    def prefetch(self):
+        """Start reading back the multipoles still on the device (see ``DeferredRows.prefetch``);
+        returns self."""
+        for p in self.poles:
+            deferred = getattr(p, '_deferred', None)
+            if deferred is not None:
+                deferred.rows.prefetch()
+        return self
 
     def clone(self, **kwargs):
         """Per-pole update; list values (one per ell) are dispatched, scalars broadcast."""
