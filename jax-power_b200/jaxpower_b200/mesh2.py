@@ -936,7 +936,6 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
     the 'local' theory line of sight through ``_local_smooth_window``, 'infinite' through
     ``_local_infinite_window``.  The 'jaxdecomp' backend raises ``NotImplementedError``.
     """
-    _plain_bins(bin, 'compute_mesh2_spectrum_window')
     from .types import WindowMatrix
     flags = tuple(flags)
     meshes, fields = _format_meshes(*meshes)
@@ -981,6 +980,10 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
         else:
             wmat = _firstpoint_infinite_window(meshes, fields, periodic, mattrs, bin, edgesin, ellsin, swap, rnorm)
         return _window_matrix(bin, norm, edgesin, ellsin, wmat)
+    # a fixed line of sight bins with the fused window kernels, which take each mode once; the
+    # local lines of sight bin through bin(...), which takes mode oversampling
+    if vlos is not None:
+        _plain_bins(bin, 'compute_mesh2_spectrum_window with a fixed line of sight')
     if 'infinite' in flags and 'smooth' not in flags:
         edgesin, ellsin = _window_edges(edgesin, ellsin)
         ellsin = _plain_ells(ellsin)
@@ -2041,7 +2044,6 @@ def compute_mesh2_spectrum_mean(*meshes, theory, bin=None, los='z'):
     line of sight takes theory multipoles (keys ell or (ell, wide-angle order)) through ``_firstpoint_mean``.
     The 'jaxdecomp' layout raises ``NotImplementedError``.
     """
-    _plain_bins(bin, 'compute_mesh2_spectrum_mean')
     meshes, fields = _format_meshes(*meshes)
     periodic = isinstance(meshes[0], MeshAttrs)
     if periodic:
@@ -2081,9 +2083,10 @@ def compute_mesh2_spectrum_mean(*meshes, theory, bin=None, los='z'):
         table = torch.as_tensor(pole.astype('f4'), device=knorm.device)
         return torch.where(inside, table[idx.clamp(0, len(pole) - 1)], torch.zeros_like(knorm))
 
-    if vlos is None:
+    if vlos is None:  # binned through bin(...): mode oversampling is taken
         return _firstpoint_mean(meshes, fields, periodic, mattrs, bin, poles, get_theory, swap, N, norm, rnorm,
                                 theory_los=theory_los)
+    _plain_bins(bin, 'compute_mesh2_spectrum_mean with a fixed line of sight')
     mu = (kvec[0] * float(vlos[0]) + kvec[1] * float(vlos[1]) + kvec[2] * float(vlos[2])) / \
         torch.where(knorm == 0., torch.ones_like(knorm), knorm)
     if callable(poles):

@@ -485,3 +485,28 @@ def test_wide_angle_needs_local_line_of_sight():
     with pytest.raises(NotImplementedError):
         jp.compute_mesh2_spectrum_window(attrs, edgesin=np.array([0., 0.1]), ellsin=([(0, 1)], 'local'), bin=b,
                                          los='firstpoint')
+
+
+@pytest.mark.parametrize('flag', [None, 'infinite'])
+def test_firstpoint_window_mode_oversampling_matches_oracle(flag):
+    """First-point window and mean spectrum with mode_oversampling = 1: the output bins average
+    the shifted binnings (mesh2.py:48-61) through bin(...), as the reference's."""
+    import jaxpower_b200 as jp
+    from oracle import spectrum as ospec
+    meshsize, boxsize, center = (10, 8, 8), np.array([500., 400., 400.]), (900., -200., 300.)
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=center)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.02}, ells=(0, 2), mode_oversampling=1)
+    ob = Bins(Geometry(meshsize, boxsize, center), step=0.02, ells=(0, 2), mode_oversampling=1)
+    assert np.allclose(b.nmodes, ob.nmodes)
+    sel = np.random.default_rng(41).uniform(0.5, 1.5, meshsize).astype('f4')
+    mesh = attrs.create(kind='real', fill=torch.as_tensor(sel))
+    edgesin = np.arange(0.005, 0.06, 0.02)
+    w = jp.compute_mesh2_spectrum_window(mesh, edgesin=edgesin, ellsin=(0, 2), bin=b, los='firstpoint',
+                                         flags=(flag,) if flag else ())
+    if flag is None:
+        ref = ospec.compute_mesh2_spectrum_window_firstpoint(ob, edgesin, (0, 2), meshes=[sel])
+    else:
+        ref = ospec.compute_mesh2_spectrum_window_firstpoint_infinite(ob, edgesin, (0, 2), meshes=[sel])
+    _check(w.value, ref)
+    with pytest.raises(NotImplementedError):
+        jp.compute_mesh2_spectrum_window(mesh, edgesin=edgesin, ellsin=(0, 2), bin=b, los='z')
