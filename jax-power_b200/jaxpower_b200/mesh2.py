@@ -818,7 +818,7 @@ def _window_edges(edgesin, ellsin):
     edgesin = np.asarray(edgesin, dtype='f8')
     if edgesin.ndim != 2:
         edgesin = np.column_stack([edgesin[:-1], edgesin[1:]])
-    if np.ndim(ellsin) == 0:
+    if isinstance(ellsin, (int, np.integer)):
         ellsin = (ellsin,)
     if any(isinstance(e, tuple) for e in ellsin):
         return edgesin, [(int(e[0]), int(e[1])) if isinstance(e, tuple) else (int(e), 0) for e in ellsin]
@@ -965,7 +965,7 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
                 raise NotImplementedError("theory line of sight '{}' with these flags is not supported".format(theory_los))
         else:
             theory_los = 'firstpoint'
-        if ellsin is not None and np.ndim(ellsin) == 0:
+        if isinstance(ellsin, (int, np.integer)):
             ellsin = (ellsin,)
         edgesin, ellsin = _window_edges(edgesin, ellsin)
         if theory_los == 'local':
@@ -1002,7 +1002,7 @@ def compute_mesh2_spectrum_window(*meshes, edgesin, ellsin=None, bin=None, los='
             ellsin, theory_los = ellsin
         if theory_los not in ('firstpoint', 'local'):
             raise NotImplementedError("theory line of sight '{}' is not supported for the window".format(theory_los))
-        if ellsin is not None and np.ndim(ellsin) == 0:
+        if isinstance(ellsin, (int, np.integer)):
             ellsin = (ellsin,)
         edgesin, ellsin = _window_edges(edgesin, ellsin)
         if theory_los == 'local':
@@ -2175,7 +2175,7 @@ def compute_smooth2_spectrum_window(window, edgesin, ellsin=None, bin=None, flag
     edgesin = np.asarray(edgesin, dtype='f8')
     if edgesin.ndim != 2:
         edgesin = np.column_stack([edgesin[:-1], edgesin[1:]])
-    ellsin = [e if isinstance(e, tuple) else (int(e), 0) for e in ((ellsin,) if np.ndim(ellsin) == 0 else ellsin)]
+    ellsin = [e if isinstance(e, tuple) else (int(e), 0) for e in ((ellsin,) if isinstance(ellsin, (int, np.integer)) else ellsin)]
     labelled = any(getattr(window, 'wa_orders', ()))
     if any(wa != 0 for _, wa in ellsin) and not labelled:
         raise ValueError('wa_orders must be provided in input window')

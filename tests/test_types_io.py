@@ -80,3 +80,39 @@ def test_deferred_rows_read_once_and_match(tmp_path):
     fn = str(tmp_path / 'lazy.npz')
     lazy.write(fn)
     _same(eager, read(fn))
+
+
+def test_wide_angle_labels_round_trip(tmp_path):
+    """Theory multipoles labelled with wide-angle orders (attrs['wa_order']): wa_orders, get by
+    (ell, order), and the labels survive write / read."""
+    edges = np.linspace(0., 0.1, 6)
+    k = 0.5 * (edges[:-1] + edges[1:])
+    pairs = [(0, 0), (2, 0), (0, 1), (2, 1)]
+    poles = Mesh2SpectrumPoles([Mesh2SpectrumPole(k, np.column_stack([edges[:-1], edges[1:]]), np.ones(5),
+                                                  np.full(5, 10. * ell + wa), ell=ell,
+                                                  attrs=dict(wa_order=wa) if wa else None) for ell, wa in pairs])
+    assert poles.ells == (0, 2, 0, 2) and poles.wa_orders == (0, 0, 1, 1)
+    assert poles.get(0).num_raw[0] == 0. and poles.get(0, wa_orders=1).num_raw[0] == 1.
+    sub = poles.get([2, 2], wa_orders=[1, 0])
+    assert [p.num_raw[0] for p in sub] == [21., 20.]
+    fn = str(tmp_path / 'wa.npz')
+    poles.write(fn)
+    back = read(fn)
+    assert back.wa_orders == (0, 0, 1, 1)
+    _same(poles, back)
+
+
+def test_window_input_multipoles_parsing():
+    """Input multipoles of a window matrix: ints stay ints, (ell, order) pairs become pairs, and a
+    fixed line of sight rejects orders > 0."""
+    import pytest
+    from jaxpower_b200.mesh2 import _window_edges, _plain_ells, _no_wide_angle
+    e, ells = _window_edges(np.array([0., 0.1, 0.2]), (0, 2))
+    assert e.shape == (2, 2) and ells == [0, 2]
+    _, ells = _window_edges(np.array([0., 0.1]), [(0, 0), 2, (4, 1)])
+    assert ells == [(0, 0), (2, 0), (4, 1)]
+    assert _plain_ells([(0, 0), 2]) == [0, 2]
+    with pytest.raises(ValueError):
+        _plain_ells([(0, 1)])
+    with pytest.raises(NotImplementedError):
+        _no_wide_angle([(2, 2)])
