@@ -230,10 +230,39 @@ __device__ __forceinline__ int warp_mock_of(const PaintGeom &g, int64_t base, in
 // run leader makes one atomic for the whole run and its lanes take consecutive slots.
 //   sink.particle(ok, wp)                  once per lane (validity, weight)
 //   sink.run(act, lead, leads, runlen, tile, u, wp)   once per candidate copy (warp-uniform)
+// A lane's raw position and weight (0 beyond `end`): loaded one warp iteration ahead by the
+// shared-histogram passes, so that the next loads are in flight while a warp works on its runs.
+struct RawParticle {
+  float x, y, z, w;
+};
+
+__device__ __forceinline__ RawParticle load_raw(const float *__restrict__ pos, const float *__restrict__ w,
+                                                int64_t p, int64_t end) {
+  RawParticle r{0.f, 0.f, 0.f, 0.f};
+  if (p < end) {
+    const float *q = pos + 3 * p;
+    r.x = q[0];
+    r.y = q[1];
+    r.z = q[2];
+    r.w = w ? w[p] : 1.f;
+  }
+  return r;
+}
+
+template <class Sink>
+__device__ __forceinline__ void warp_tile_runs_raw(const PaintGeom &g, int64_t n, int64_t end, int64_t base,
+                                                   const RawParticle &raw, Sink &sink);
+
 template <class Sink>
 __device__ __forceinline__ void warp_tile_runs(const PaintGeom &g, const float *__restrict__ pos,
                                                const float *__restrict__ w, int64_t n, int64_t end,
                                                int64_t base, Sink &sink) {
+  warp_tile_runs_raw(g, n, end, base, load_raw(pos, w, base + (threadIdx.x & 31), end), sink);
+}
+
+template <class Sink>
+__device__ __forceinline__ void warp_tile_runs_raw(const PaintGeom &g, int64_t n, int64_t end, int64_t base,
+                                                   const RawParticle &raw, Sink &sink) {
   const int ns[3] = {g.d.n0, g.d.n1, g.d.n2};
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -241,7 +270,17 @@ __device__ __forceinline__ void warp_tile_runs(const PaintGeom &g, const float *
   float u[3] = {0.f, 0.f, 0.f}, wp = 0.f;
   bool ok = false;
   const int mock = warp_mock_of(g, base, n);
-  if (p < end) ok = load_particle(g, pos, w, p, u, &wp) && isfinite(wp);
+  if (p < end) {
+    const float q[3] = {raw.x, raw.y, raw.z};
+    ok = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      u[d] = normalise(q[d], g.half[d], g.center[d], g.cell[d]);
+      ok &= isfinite(u[d]) && fabsf(u[d]) < MAX_CELL_COORD;
+    }
+    wp = raw.w;
+    ok = ok && isfinite(wp);
+  }
   sink.particle(p < end, ok, wp);
   int t[3][3], nt[3] = {0, 0, 0};
   if (ok) {
@@ -375,8 +414,15 @@ __global__ void __launch_bounds__(HIST_THREADS) bucket_hist_kernel(
   const int64_t begin = (int64_t)blockIdx.x * chunk;
   const int64_t end = min(n, begin + chunk);
   const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  for (int64_t base = begin + (int64_t)warp * 32; base < end; base += (int64_t)nwarps * 32)
-    warp_tile_runs(g, pos, w, n, end, base, sink);
+  const int lane = threadIdx.x & 31;
+  const int64_t wstride = (int64_t)nwarps * 32;
+  int64_t base = begin + (int64_t)warp * 32;
+  RawParticle cur = load_raw(pos, w, base + lane, end);
+  for (; base < end; base += wstride) {
+    const RawParticle next = load_raw(pos, w, base + wstride + lane, end);  // one iteration ahead
+    warp_tile_runs_raw(g, n, end, base, cur, sink);
+    cur = next;
+  }
   if (!PLACE) {
     const unsigned wb = __reduce_max_sync(0xffffffffu, sink.wmax);
     if ((threadIdx.x & 31) == 0 && wb) atomicMax(wmax_bits, wb);
