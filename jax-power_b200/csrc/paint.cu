@@ -820,10 +820,14 @@ __global__ void __launch_bounds__(SHIFT_TILE_THREADS) paint_shift_tile_kernel(
   const float4 *entries = bucket + begin;
 
   const int S = (count + 31) >> 5;
+  // each lane's entry of the warp's next slot is loaded one slot ahead (L2 latency behind the atomics)
+  float4 qn = warp < S && lane * S + warp < count ? entries[lane * S + warp] : make_float4(0.f, 0.f, 0.f, 0.f);
   for (int j = warp; j < S; j += NWARPS) {
     const int e = lane * S + j;
     const bool has = e < count;
-    const float4 q = entries[has ? e : 0];
+    const float4 q = qn;
+    const int en = e + NWARPS;
+    if (j + NWARPS < S && en < count) qn = entries[en];
     const float wq = has ? __fmul_rn(__fmul_rn(q.w, fscale0), fscale1) : 0.f;
     float kx[ORDER], ky[ORDER], kz[ORDER];
     const int fx = stencil_axis<ORDER>(q.x, shift, kx);

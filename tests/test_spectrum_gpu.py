@@ -186,6 +186,27 @@ def test_fkp_normalization_shotnoise():
     assert np.isclose(sn, np.sum(w.astype('f8')**2), rtol=1e-5)
 
 
+def test_fkp2_shotnoise_identities():
+    """The reference's shot-noise identities (tests/test_mesh2.py:75-91): two different fields
+    have none; the same positions with two weightings give sum w1 w2 in the monopole only; an
+    FKP field gives the sum of its signed squared weights."""
+    jp = _jp()
+    attrs = jp.MeshAttrs(boxsize=1000., meshsize=128)
+    rng = np.random.default_rng(11)
+    pos = rng.uniform(-500., 500., (100000, 3)).astype('f4')
+    w1, w2 = rng.uniform(0., 1., 100000).astype('f4'), rng.uniform(0., 1., 100000).astype('f4')
+    data1, data2 = jp.ParticleField(pos, w1, attrs=attrs), jp.ParticleField(pos, w2, attrs=attrs)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.005}, ells=(0, 2))
+    sn = jp.compute_fkp2_shotnoise([data1, data2], bin=b)
+    assert np.allclose(sn[0], 0.)
+    sn = jp.compute_fkp2_shotnoise([data1, data2], bin=b, fields=[0, 0])
+    assert np.allclose(sn[0], np.sum(w1.astype('f8') * w2.astype('f8'))) and np.allclose(sn[1], 0.)
+    fkp = jp.FKPField(data1, data2)
+    sn = jp.compute_fkp2_shotnoise(fkp, bin=b)
+    w = fkp.particles.weights.double().cpu().numpy()
+    assert np.allclose(sn[0], np.sum(w ** 2))
+
+
 def test_spectrum_deterministic():
     jp = _jp()
     pos = _random_field((64,) * 3, [1000.] * 3, seed=3, n=300000)
@@ -195,6 +216,24 @@ def test_spectrum_deterministic():
     a = jp.compute_mesh2_spectrum(mesh, bin=b, los='firstpoint').value()
     c = jp.compute_mesh2_spectrum(mesh, bin=b, los='firstpoint').value()
     assert np.array_equal(a, c)
+
+
+@pytest.mark.parametrize('meshsize', [128, (128, 124, 122)])
+@pytest.mark.parametrize('los', ['x', 'endpoint'])
+def test_gaussian_mesh_recovers_power(meshsize, los):
+    """The reference's own check of the estimator's normalisation (tests/test_mesh2.py:23-61):
+    a unitary-amplitude Gaussian mesh of P(k) = 1e4 (k / 0.03)^3 exp(-k / 0.03) gives back P(k)
+    within 1 % in the monopole, past the first two bins."""
+    jp = _jp()
+    from jaxpower_b200.mock import generate_gaussian_mesh
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=1000.)
+    b = jp.BinMesh2SpectrumPoles(attrs, edges={'step': 0.01}, ells=(0, 2, 4))
+    mesh = generate_gaussian_mesh(attrs, lambda k: 1e4 * (k / 0.03) ** 3 * torch.exp(-k / 0.03), seed=43,
+                                  unitary_amplitude=True)
+    spectrum = jp.compute_mesh2_spectrum(mesh, bin=b, los=los)
+    k = spectrum.get(0).coords('k')
+    assert np.allclose(spectrum.get(0).value()[2:], (1e4 * (k / 0.03) ** 3 * np.exp(-k / 0.03))[2:], rtol=1e-2)
+    assert tuple(spectrum.ells) == (0, 2, 4)
 
 
 def test_prefetched_readback_matches():
