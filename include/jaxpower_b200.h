@@ -217,6 +217,20 @@ pk_status pk_bin_separation_global(void *stream, const float *value, const int32
                                    int nedges, float step, int nells, const int32_t *ells,
                                    double *d_out, void *workspace, size_t workspace_bytes);
 
+/* Mode oversampling of BinMesh2CorrelationPoles (mode_oversampling > 0, _make_edges2('real'),
+ * mesh2.py:48-61): the separations binned by |s + sshift| (sshift added to each coordinate in
+ * float32, as the reference adds its integer shifts), their values and mu from s; one call per
+ * shift, written or added (accumulate) into the outputs, the caller averaging over the shifts. */
+pk_status pk_bin_separation_modes_shifted(void *stream, const int32_t meshsize[3], const float cellsize[3],
+                                          const float sshift[3], const float *d_edges, int nedges, float step,
+                                          int accumulate, double *d_nmodes, double *d_ssum, void *workspace,
+                                          size_t workspace_bytes);
+pk_status pk_bin_separation_global_shifted(void *stream, const float *value, const int32_t meshsize[3],
+                                           const float cellsize[3], const float sshift[3], const float los[3],
+                                           const float *d_edges, int nedges, float step, int nells,
+                                           const int32_t *ells, int accumulate, double *d_out, void *workspace,
+                                           size_t workspace_bytes);
+
 /* Spherical-Bessel basis of BinMesh2CorrelationPoles (basis='bessel', mesh2.py:169-181),
  * for the estimators of compute_mesh2_correlation (mesh2.py:414-500): per separation bin b
  * (s_b = d_sep[b], float64, the bins' xavg) and multipole ells[l] the float64 sum over the

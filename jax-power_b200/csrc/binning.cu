@@ -1945,6 +1945,63 @@ extern "C" pk_status pk_bin_separation_modes(void *stream, const int32_t meshsiz
                                        workspace, workspace_bytes);
 }
 
+// Mode oversampling of BinMesh2CorrelationPoles (_make_edges2('real'), mesh2.py:48-61): the
+// separations binned by |s + shift| (the chunk walk, which takes a shift), their values (and
+// mu) from s; one call per shift, added (accumulate) and averaged by the caller.
+static pk_status make_sep_shifted_geom(const int32_t meshsize[3], const float cellsize[3], const float sshift[3],
+                                       int nedges, float step, BinGeom *g) {
+  pk_status st = make_sep_geom(meshsize, cellsize, nedges, step, g);
+  if (st) return st;
+  PK_REQUIRE(sshift, PK_ERR_INVALID, "sshift is NULL");
+  for (int a = 0; a < 3; ++a) {
+    PK_REQUIRE(isfinite(sshift[a]), PK_ERR_INVALID, "sshift must be finite");
+    g->kshift[a] = sshift[a];
+  }
+  g->shifted = 1;
+  return PK_OK;
+}
+
+extern "C" pk_status pk_bin_separation_modes_shifted(void *stream, const int32_t meshsize[3],
+                                                     const float cellsize[3], const float sshift[3],
+                                                     const float *d_edges, int nedges, float step, int accumulate,
+                                                     double *d_nmodes, double *d_ssum, void *workspace,
+                                                     size_t workspace_bytes) {
+  BinGeom g;
+  pk_status st = make_sep_shifted_geom(meshsize, cellsize, sshift, nedges, step, &g);
+  if (st) return st;
+  PK_REQUIRE(d_edges && d_nmodes && d_ssum, PK_ERR_INVALID, "null pointer");
+  ModesOp op;
+  op.shifted = 1;
+  for (int a = 0; a < 3; ++a) op.kshift[a] = sshift[a];
+  return launch_bins<2>((cudaStream_t)stream, g, op, d_edges, false, accumulate, d_nmodes, d_ssum, workspace,
+                        workspace_bytes);
+}
+
+extern "C" pk_status pk_bin_separation_global_shifted(void *stream, const float *value, const int32_t meshsize[3],
+                                                      const float cellsize[3], const float sshift[3],
+                                                      const float los[3], const float *d_edges, int nedges,
+                                                      float step, int nells, const int32_t *ells, int accumulate,
+                                                      double *d_out, void *workspace, size_t workspace_bytes) {
+  BinGeom g;
+  pk_status st = make_sep_shifted_geom(meshsize, cellsize, sshift, nedges, step, &g);
+  if (st) return st;
+  PK_REQUIRE(value && d_edges && d_out && los && ells, PK_ERR_INVALID, "null pointer");
+  PK_REQUIRE(nells >= 1 && nells <= 3, PK_ERR_INVALID, "nells must be in 1..3");
+  for (int l = 0; l < nells; ++l) PK_REQUIRE(ells[l] >= 0 && ells[l] <= 8, PK_ERR_INVALID, "ell must be in 0..8");
+  cudaStream_t cs = (cudaStream_t)stream;
+#define PK_SEPS_CASE(N)                                                                            \
+  if (nells == N) {                                                                                \
+    SepLegendreOp<N> op;                                                                           \
+    op.v = value;                                                                                  \
+    for (int a = 0; a < 3; ++a) op.los[a] = los[a];                                                \
+    for (int l = 0; l < MAX_ELLS; ++l) op.ells[l] = l < nells ? ells[l] : 0;                       \
+    return launch_bins<N>(cs, g, op, d_edges, false, accumulate, d_out, nullptr, workspace, workspace_bytes); \
+  }
+  PK_SEPS_CASE(1) PK_SEPS_CASE(2) PK_SEPS_CASE(3)
+#undef PK_SEPS_CASE
+  return PK_ERR_INVALID;
+}
+
 extern "C" pk_status pk_bin_separation_global(void *stream, const float *value, const int32_t meshsize[3],
                                               const float cellsize[3], const float los[3], const float *d_edges,
                                               int nedges, float step, int nells, const int32_t *ells,

@@ -112,6 +112,10 @@ SIGNATURES = {
                       c_int, c_float_p, c_void_p, c_int, c_float_p, c_int, c_int32_p, c_int, c_int, c_void_p,
                       c_void_p, c_size_t],
     'pk_radial_power': [c_void_p, c_void_p, c_int, c_int32_p, c_float_p, c_float_p, c_int, c_int],
+    'pk_bin_separation_modes_shifted': [c_void_p, c_int32_p, c_float_p, c_float_p, c_void_p, c_int, c_float, c_int,
+                                        c_void_p, c_void_p, c_void_p, c_size_t],
+    'pk_bin_separation_global_shifted': [c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_float_p, c_void_p,
+                                         c_int, c_float, c_int, c_int32_p, c_int, c_void_p, c_void_p, c_size_t],
     'pk_ylm_accumulate': [c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_int, c_int32_p, c_int32_p,
                           c_void_p],
     'pk_ylm_premultiply': [c_void_p, c_void_p, c_int32_p, c_float_p, c_float_p, c_int, c_int32_p,

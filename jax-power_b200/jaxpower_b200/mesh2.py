@@ -182,7 +182,8 @@ class BinMesh2CorrelationPoles:
     mattrs : MeshAttrs or mesh field
     edges : array, dict ('min', 'max' (default cellsize * min(meshsize) / 2), 'step') or None
     ells : int or tuple
-    mode_oversampling : only 0
+    mode_oversampling : int s >= 0; s > 0 bins the separations once per integer shift in
+        [-s, s]^3 by |s + shift| and averages, as ``BinMesh2SpectrumPoles`` does for k
     basis : None (bins of |s| on the separation grid) or 'bessel': the estimator's Fourier-space
         mode values projected on j_ell(|k| s) at each bin's mean separation (``mesh2.py:169-181``;
         ``pk_bin_bessel``)
@@ -193,8 +194,13 @@ class BinMesh2CorrelationPoles:
     def __init__(self, mattrs, edges=None, ells=0, mode_oversampling=0, basis=None, klimit=None, batch_size=None):
         if not isinstance(mattrs, MeshAttrs):
             mattrs = mattrs.attrs
-        if mode_oversampling:
-            raise NotImplementedError('mode_oversampling > 0 is not supported on the GPU path')
+        mode_oversampling = int(mode_oversampling)
+        if mode_oversampling < 0:
+            raise ValueError('mode_oversampling must be >= 0')
+        r = range(-mode_oversampling, mode_oversampling + 1)
+        self._sshifts = [tuple(float(v) for v in sh) for sh in itertools.product(r, r, r)] if mode_oversampling else []
+        if self._sshifts and basis == 'bessel':
+            raise NotImplementedError("mode_oversampling > 0 with basis='bessel' is not supported")
         if basis not in (None, 'bessel'):
             raise ValueError('unknown basis {}'.format(basis))
         self.mattrs = mattrs
@@ -225,9 +231,16 @@ class BinMesh2CorrelationPoles:
         nmodes = torch.empty(nbins, dtype=torch.float64, device=_device())
         ssum = torch.empty(nbins, dtype=torch.float64, device=_device())
         ws = self._workspace()
-        _lib.call('pk_bin_separation_modes', _lib.stream_handle(), _lib.i32(mattrs.meshsize), _lib.f32(mattrs.cellsize),
-                  _lib.ptr(self.d_edges), len(edges), self._step, _lib.ptr(nmodes), _lib.ptr(ssum), _lib.ptr(ws),
-                  ws.numel())
+        if self._sshifts:  # mesh2.py:48-61: nmodes averaged over the shifts, xavg the summed |s + shift| over it
+            for ish, sh in enumerate(self._sshifts):
+                _lib.call('pk_bin_separation_modes_shifted', _lib.stream_handle(), _lib.i32(mattrs.meshsize),
+                          _lib.f32(mattrs.cellsize), _lib.f32(sh), _lib.ptr(self.d_edges), len(edges), self._step,
+                          int(ish > 0), _lib.ptr(nmodes), _lib.ptr(ssum), _lib.ptr(ws), ws.numel())
+            nmodes /= len(self._sshifts)
+        else:
+            _lib.call('pk_bin_separation_modes', _lib.stream_handle(), _lib.i32(mattrs.meshsize),
+                      _lib.f32(mattrs.cellsize), _lib.ptr(self.d_edges), len(edges), self._step, _lib.ptr(nmodes),
+                      _lib.ptr(ssum), _lib.ptr(ws), ws.numel())
         self.nmodes = nmodes.cpu().numpy()
         with np.errstate(invalid='ignore', divide='ignore'):
             self.xavg = ssum.cpu().numpy() / self.nmodes
@@ -259,6 +272,13 @@ class BinMesh2CorrelationPoles:
         value = value.to(device=_device(), dtype=torch.float32).contiguous()
         out = torch.empty(len(ells) * self.nbins, dtype=torch.float64, device=value.device)
         ws = self._workspace()
+        if self._sshifts:  # the mean over the shifted binnings (mesh.py:2894-2895)
+            for ish, sh in enumerate(self._sshifts):
+                _lib.call('pk_bin_separation_global_shifted', _lib.stream_handle(), _lib.ptr(value),
+                          _lib.i32(self.mattrs.meshsize), _lib.f32(self.mattrs.cellsize), _lib.f32(sh), _lib.f32(los),
+                          _lib.ptr(self.d_edges), len(self._edges1d), self._step, len(ells), _lib.i32(ells),
+                          int(ish > 0), _lib.ptr(out), _lib.ptr(ws), ws.numel())
+            return out.reshape(len(ells), self.nbins) / len(self._sshifts)
         _lib.call('pk_bin_separation_global', _lib.stream_handle(), _lib.ptr(value), _lib.i32(self.mattrs.meshsize),
                   _lib.f32(self.mattrs.cellsize), _lib.f32(los), _lib.ptr(self.d_edges), len(self._edges1d),
                   self._step, len(ells), _lib.i32(ells), _lib.ptr(out), _lib.ptr(ws), ws.numel())

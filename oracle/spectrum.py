@@ -1107,7 +1107,7 @@ class CorrelationBins:
     (``mesh2.py:124-192``, ``_make_edges2('real')`` ``mesh2.py:25-62``): |s| of the separation
     grid binned by ``digitize``; unit weights."""
 
-    def __init__(self, geom, step=None, edges=None, ells=(0, 2, 4)):
+    def __init__(self, geom, step=None, edges=None, ells=(0, 2, 4), mode_oversampling=0):
         dt = geom.dtype
         self.geom = geom
         self.ells = tuple(sorted((ells,) if np.ndim(ells) == 0 else ells))
@@ -1119,10 +1119,25 @@ class CorrelationBins:
         sx, sy, sz = separation_coords(geom)
         s2 = (((dt.type(0.) + sx * sx).astype(dt) + sy * sy).astype(dt) + sz * sz).astype(dt)
         self.snorm = np.sqrt(s2).astype(dt)
-        self.ibin = np.searchsorted(self.edges.astype(dt), self.snorm.ravel(), side='right').reshape(self.snorm.shape)
         nb = len(self.edges) + 1
-        self.nmodes = np.bincount(self.ibin.ravel(), minlength=nb)[1:-1].astype('f8')
-        ssum = np.bincount(self.ibin.ravel(), weights=self.snorm.ravel().astype('f8'), minlength=nb)[1:-1]
+        # mode oversampling (mesh2.py:48-61): one binning per integer shift of the separations,
+        # |s + shift| in the geometry's dtype; nmodes their mean, xavg the summed |s + shift| over it
+        r = range(-int(mode_oversampling), int(mode_oversampling) + 1)
+        shifts = list(product(r, r, r)) if mode_oversampling else [(0, 0, 0)]
+        self.ibins, nmodes, ssum = [], 0., 0.
+        for sh in shifts:
+            if mode_oversampling:
+                a, b, c = [(x + dt.type(v)).astype(dt) for x, v in zip((sx, sy, sz), sh)]
+                norm = np.sqrt((((dt.type(0.) + a * a).astype(dt) + b * b).astype(dt) + c * c).astype(dt)).astype(dt)
+                norm = np.broadcast_to(norm, self.snorm.shape)
+            else:
+                norm = self.snorm
+            ib = np.searchsorted(self.edges.astype(dt), norm.ravel(), side='right')
+            self.ibins.append(ib)
+            nmodes = nmodes + np.bincount(ib, minlength=nb)[1:-1].astype('f8')
+            ssum = ssum + np.bincount(ib, weights=norm.ravel().astype('f8'), minlength=nb)[1:-1]
+        self.ibin = self.ibins[0].reshape(self.snorm.shape)
+        self.nmodes = nmodes / len(shifts)
         with np.errstate(invalid='ignore', divide='ignore'):
             self.xavg = ssum / self.nmodes
 
@@ -1135,7 +1150,8 @@ class CorrelationBins:
         if remove_zero:
             value[0, 0, 0] = 0.
         nb = len(self.edges) + 1
-        return np.bincount(self.ibin.ravel(), weights=value.ravel(), minlength=nb)[1:-1] / self.nmodes
+        total = sum(np.bincount(ib, weights=value.ravel(), minlength=nb)[1:-1] for ib in self.ibins)
+        return total / len(self.ibins) / self.nmodes
 
 
 def compute_mesh2_correlation(mesh, bins, los='z', mesh2=None):

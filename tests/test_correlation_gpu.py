@@ -148,3 +148,28 @@ def test_bessel_basis_matches_oracle(los, cross, klimit):
         assert np.allclose(got.get(ell).num_raw, ref['num_raw'][i], rtol=0, atol=2e-5 * scale), ell
     # the plain separation binning of the same estimator differs (another basis)
     assert got.get(0).s.shape == ob.xavg.shape
+
+
+@pytest.mark.parametrize('los', ['z', 'firstpoint'])
+def test_correlation_mode_oversampling_matches_oracle(los):
+    """BinMesh2CorrelationPoles(mode_oversampling=1): separations binned by |s + shift| for the
+    27 integer shifts and averaged (mesh2.py:48-61, as for k); nmodes, xavg and the multipoles
+    against the oracle."""
+    import jaxpower_b200 as jp
+    from oracle.spectrum import compute_mesh2_correlation_firstpoint as ofp
+    meshsize, boxsize = (20, 16, 12), np.array([400., 320., 240.])
+    center = np.array([600., -100., 500.]) if los == 'firstpoint' else np.zeros(3)
+    attrs = jp.MeshAttrs(meshsize=meshsize, boxsize=boxsize, boxcenter=center)
+    geom = Geometry(meshsize, boxsize, center)
+    pos = _catalog(20000, boxsize, 9) + center.astype('f4')
+    m = jp.ParticleField(pos, attrs=attrs).paint(resampler='tsc', interlacing=2, compensate=True, out='real')
+    o = opaint.paint(geom, pos, None, 'tsc', 2, True, 'real')
+    b = jp.BinMesh2CorrelationPoles(attrs, edges={'step': 25.}, ells=(0, 2), mode_oversampling=1)
+    ob = CorrelationBins(geom, step=25., ells=(0, 2), mode_oversampling=1)
+    assert np.array_equal(b.nmodes, ob.nmodes)
+    assert np.allclose(b.xavg, ob.xavg, rtol=1e-6, equal_nan=True)
+    got = jp.compute_mesh2_correlation(m, bin=b, los=los)
+    ref = ofp(o, ob) if los == 'firstpoint' else ocorr(o, ob, los=los)
+    scale = np.abs(ref['num_raw'][0]).max()
+    for i, ell in enumerate((0, 2)):
+        assert np.allclose(got.get(ell).num_raw, ref['num_raw'][i], rtol=0, atol=1e-5 * scale), ell
