@@ -104,12 +104,11 @@ class BinMesh2SpectrumPoles:
                           _lib.f32(mattrs.kfun), _lib.f32(sh), _lib.ptr(self.d_edges), len(edges), self._step,
                           mattrs.backend_code, int(ish > 0), _lib.ptr(nmodes), _lib.ptr(ksum), _lib.ptr(ws),
                           ws.numel())
-            nmodes /= len(self._kshifts)
         else:
             _lib.call('pk_bin_modes', _lib.stream_handle(), _lib.i32(mattrs.meshsize), _lib.f32(mattrs.kfun),
                       _lib.ptr(self.d_edges), len(edges), self._step, mattrs.backend_code, _lib.ptr(nmodes),
                       _lib.ptr(ksum), _lib.ptr(ws), ws.numel())
-        self.nmodes = nmodes.cpu().numpy()
+        self.nmodes = nmodes.cpu().numpy() / max(len(self._kshifts), 1)  # mean over the shifts, an IEEE division
         with np.errstate(invalid='ignore', divide='ignore'):
             self.xavg = ksum.cpu().numpy() / self.nmodes
 
@@ -236,12 +235,11 @@ class BinMesh2CorrelationPoles:
                 _lib.call('pk_bin_separation_modes_shifted', _lib.stream_handle(), _lib.i32(mattrs.meshsize),
                           _lib.f32(mattrs.cellsize), _lib.f32(sh), _lib.ptr(self.d_edges), len(edges), self._step,
                           int(ish > 0), _lib.ptr(nmodes), _lib.ptr(ssum), _lib.ptr(ws), ws.numel())
-            nmodes /= len(self._sshifts)
         else:
             _lib.call('pk_bin_separation_modes', _lib.stream_handle(), _lib.i32(mattrs.meshsize),
                       _lib.f32(mattrs.cellsize), _lib.ptr(self.d_edges), len(edges), self._step, _lib.ptr(nmodes),
                       _lib.ptr(ssum), _lib.ptr(ws), ws.numel())
-        self.nmodes = nmodes.cpu().numpy()
+        self.nmodes = nmodes.cpu().numpy() / max(len(self._sshifts), 1)  # mean over the shifts, an IEEE division
         with np.errstate(invalid='ignore', divide='ignore'):
             self.xavg = ssum.cpu().numpy() / self.nmodes
 
