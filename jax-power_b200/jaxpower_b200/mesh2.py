@@ -403,7 +403,7 @@ def _bessel_correlation(meshes, auto, bin, los_name, vlos, swap, norm_value):
         return mesh.value if isinstance(mesh, RealMeshField) else _c2r(mesh.value, meshsize)
 
     nbins = bin.nbins
-    sep = torch.as_tensor(np.asarray(bin.xavg, dtype="f8"), device=_device())
+    sep = torch.as_tensor(np.asarray(bin.xavg, dtype='f8'), device=_device())
     nbytes = _lib.c_size_t()
     _lib.call('pk_bin_bessel_workspace_size', _lib.i32(meshsize), nbins, len(ells), _lib.ctypes.byref(nbytes))
     ws = _workspace(nbytes.value)
