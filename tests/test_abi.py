@@ -110,3 +110,38 @@ def test_window_argument_errors_without_gpu(lib):
                                    1 << 20) == 1
     assert lib.pk_bin_window_batch(None, fake, 0, ms, kf, los, fake, 10, 0.01, 0, 2, ev, 1, fake, fake, 1 << 20) == 1
     assert lib.pk_bin_window_batch(None, None, 1, ms, kf, los, fake, 10, 0.01, 0, 2, ev, 1, fake, fake, 1 << 20) == 1
+
+
+def test_argument_errors_of_bessel_adjoint_and_shift_entries_without_gpu(lib):
+    """The Bessel projection, wide-angle factor, C2R adjoint and shifted (mode oversampling)
+    entry points reject bad arguments before any launch."""
+    from jaxpower_b200 import _lib
+    fake = ctypes.c_void_p(4096)
+    nbytes = ctypes.c_size_t()
+    ms, kf, cs, off = _lib.i32([32, 32, 32]), _lib.f32([0.01] * 3), _lib.f32([1.] * 3), _lib.f32([0.] * 3)
+    los, ells = _lib.f32([0., 0., 1.]), _lib.i32([0, 2, 4])
+    # Bessel basis: at most 1024 separation bins and 5 multipoles; terms are first-point inputs
+    assert lib.pk_bin_bessel_workspace_size(ms, 2000, 3, ctypes.byref(nbytes)) == 4
+    assert lib.pk_bin_bessel_workspace_size(ms, 10, 6, ctypes.byref(nbytes)) == 4
+    assert lib.pk_bin_bessel(None, fake, None, None, 0, None, None, ms, kf, 0, los, fake, 2000, None, 3, ells, 1, 0,
+                             fake, fake, 1 << 20) == 4
+    assert lib.pk_bin_bessel(None, fake, None, fake, 1, _lib.i32([2]), _lib.i32([0]), ms, kf, 0, los, fake, 10, None,
+                             3, ells, 1, 0, fake, fake, 1 << 20) == 1
+    assert lib.pk_bin_bessel(None, fake, None, None, 0, None, None, ms, kf, 0, los, fake, 10, None, 1,
+                             _lib.i32([6]), 1, 0, fake, fake, 1 << 20) == 4
+    # wide-angle factors: |power| <= 8, an offset for positions
+    assert lib.pk_radial_power(None, fake, 1, ms, cs, off, 0, 9) == 1
+    assert lib.pk_radial_power(None, fake, 1, ms, cs, None, 0, 1) == 1
+    assert lib.pk_radial_power(None, fake, 0, ms, cs, off, 1, 1) == 1
+    # C2R adjoint: NULL buffers
+    assert lib.pk_c2r_adjoint(None, None, ms, 0, fake) == 1
+    # shifted adjoints: at most 125 shifts, a shift array
+    many = _lib.f32([0.] * (3 * 126))
+    assert lib.pk_bin_global_adjoint_shifted(None, fake, ms, kf, los, fake, 10, 0.01, 0., 0, 3, ells, fake, 1, 126,
+                                             many, fake, fake, 1 << 20) == 4
+    assert lib.pk_bin_firstpoint_adjoint_shifted(None, fake, None, 0, None, None, ms, kf, fake, 10, 0.01, 0., 0, 3,
+                                                 ells, fake, 1, 27, None, fake, 0, None, fake, 1 << 20) == 1
+    # shifted separation bins: a shift vector
+    assert lib.pk_bin_separation_modes_shifted(None, ms, cs, None, fake, 10, 10., 0, fake, fake, fake, 1 << 20) == 1
+    assert lib.pk_bin_separation_global_shifted(None, fake, ms, cs, None, los, fake, 10, 10., 3, ells, 0, fake, fake,
+                                                1 << 20) == 1
