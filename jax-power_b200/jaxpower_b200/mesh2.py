@@ -31,7 +31,8 @@ __all__ = ['BinMesh2SpectrumPoles', 'compute_mesh2_spectrum', 'compute_mesh2', '
 
 
 def _plain_bins(bin, what):
-    """Window, mean-spectrum, batched and adjoint paths bin each mode once: no mode oversampling."""
+    """Paths whose fused kernels bin each mode once (the fixed line-of-sight window and mean
+    spectrum, the batched runner) reject mode oversampling."""
     if getattr(bin, '_kshifts', None):
         raise NotImplementedError('{} does not support mode_oversampling > 0'.format(what))
 
