@@ -4,10 +4,12 @@ Public API mirrors ``jaxpower`` for the single-GPU power-spectrum estimator:
 ``MeshAttrs``, ``RealMeshField``, ``ComplexMeshField``, ``ParticleField``, ``FKPField``,
 ``get_mesh_attrs``, ``BinMesh2SpectrumPoles``, ``compute_mesh2_spectrum``,
 ``compute_fkp2_normalization``, ``compute_fkp2_shotnoise``, ``compute_box2_normalization``,
-``BinMesh2CorrelationPoles``, ``compute_mesh2_correlation``,
-``compute_mesh2_spectrum_window`` / ``compute_mesh2_spectrum_mean`` (``WindowMatrix``; global,
-first-point and end-point lines of sight, 'firstpoint' and 'local' theory, 'smooth' and
-'infinite' flags), ``compute_smooth2_spectrum_window`` and the ``resamplers`` namespaces.  All computation runs in the CUDA library
+``BinMesh2CorrelationPoles`` (separation bins with mode oversampling, or the spherical-Bessel
+basis), ``compute_mesh2_correlation``, ``compute_mesh2_spectrum_window`` /
+``compute_mesh2_spectrum_mean`` (``WindowMatrix``; global, first-point and end-point lines of
+sight, 'firstpoint' and 'local' theory, wide-angle orders, 'smooth' and 'infinite' flags),
+``compute_smooth2_spectrum_window`` and the ``resamplers`` namespaces; differentiable paint and
+spectrum in ``jaxpower_b200.autodiff``.  All computation runs in the CUDA library
 ``libjaxpower_b200.so`` through its C ABI (``include/jaxpower_b200.h``).
 """
 from . import resamplers
