@@ -21,8 +21,8 @@
 
 namespace pk {
 
-constexpr int BES_THREADS = 256;        // = modes per staged chunk
-constexpr int BES_BINS_PER_THREAD = 4;  // separation bins <= 1024
+constexpr int BES_THREADS = 512;        // = modes per staged chunk
+constexpr int BES_BINS_PER_THREAD = 2;  // separation bins <= 1024
 constexpr int BES_MAX_ELLS = 5;
 constexpr int BES_MAX_TERMS = 32;
 constexpr int BES_MAX_ORDER = 8;
@@ -39,32 +39,32 @@ __device__ __forceinline__ float bessel_legendre(int ell, float x) {
   }
 }
 
-// j_0 .. j_lmax at x (float64): x > 0.1 upward recurrence from sin and cos; x <= 0.1 the
+// j_0 .. j_LMAX at x (float64): x > 0.1 upward recurrence from sin and cos; x <= 0.1 the
 // Taylor series x^l / (2l+1)!! sum_k (-x^2/2)^k / (k! (2l+3)(2l+5)...(2l+2k+1)), 6 terms
-// (the reference truncates at x^10).  Loops are unrolled to BES_MAX_ORDER so that j stays
-// in registers.
-__device__ __forceinline__ void spherical_jn(double x, int lmax, double (&j)[BES_MAX_ORDER + 1]) {
+// (the reference truncates at x^10).  LMAX is a compile-time bound, so j stays in registers.
+template <int LMAX>
+__device__ __forceinline__ void spherical_jn(double x, double (&j)[LMAX + 1]) {
   if (x > 0.1) {
     double s, c;
     sincos(x, &s, &c);
     const double inv = 1.0 / x;
     j[0] = s * inv;
-    j[1] = (s * inv - c) * inv;
+    if constexpr (LMAX >= 1) j[1] = (s * inv - c) * inv;
 #pragma unroll
-    for (int l = 1; l < BES_MAX_ORDER; ++l) j[l + 1] = l < lmax ? (2 * l + 1) * inv * j[l] - j[l - 1] : 0.;
+    for (int l = 1; l < LMAX; ++l) j[l + 1] = (2 * l + 1) * inv * j[l] - j[l - 1];
     return;
   }
   const double h = -0.5 * x * x;
   double lead = 1.0;  // x^l / (2l+1)!!
 #pragma unroll
-  for (int l = 0; l <= BES_MAX_ORDER; ++l) {
+  for (int l = 0; l <= LMAX; ++l) {
     double term = lead, sum = lead;
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
       term *= h / ((k + 1) * (double)(2 * l + 2 * k + 3));
       sum += term;
     }
-    j[l] = l <= lmax ? sum : 0.;
+    j[l] = sum;
     lead *= x / (double)(2 * l + 3);
   }
 }
@@ -131,18 +131,16 @@ struct BesselGeom {
   float klimit[2];
 };
 
+template <int LMAX>
 __global__ void __launch_bounds__(BES_THREADS, 1) bessel_project_kernel(BesselGeom g, BesselOp op,
                                                                      const double *__restrict__ sep,
                                                                      double *__restrict__ partials) {
   __shared__ float skn[BES_THREADS];
   __shared__ float sv[BES_MAX_ELLS][BES_THREADS];
   const int tid = threadIdx.x;
-  int lmax = 0, ells[BES_MAX_ELLS];
+  int ells[BES_MAX_ELLS];
 #pragma unroll
-  for (int l = 0; l < BES_MAX_ELLS; ++l) {
-    ells[l] = l < op.nells ? op.ells[l] : -1;  // -1: no multipole, adds 0
-    lmax = max(lmax, ells[l]);
-  }
+  for (int l = 0; l < BES_MAX_ELLS; ++l) ells[l] = l < op.nells ? op.ells[l] : -1;  // -1: no multipole, adds 0
   float s[BES_BINS_PER_THREAD];
   double acc[BES_BINS_PER_THREAD][BES_MAX_ELLS];
 #pragma unroll
@@ -190,13 +188,13 @@ __global__ void __launch_bounds__(BES_THREADS, 1) bessel_project_kernel(BesselGe
 #pragma unroll
       for (int q = 0; q < BES_BINS_PER_THREAD; ++q) {
         if (tid + q * BES_THREADS >= g.nbins) break;
-        double jn[BES_MAX_ORDER + 1];
-        spherical_jn((double)__fmul_rn(knm, s[q]), lmax, jn);
+        double jn[LMAX + 1];
+        spherical_jn<LMAX>((double)__fmul_rn(knm, s[q]), jn);
 #pragma unroll
         for (int l = 0; l < BES_MAX_ELLS; ++l) {
           double jv = 0.;
 #pragma unroll
-          for (int o = 0; o <= BES_MAX_ORDER; ++o) jv = o == ells[l] ? jn[o] : jv;
+          for (int o = 0; o <= LMAX; ++o) jv = o == ells[l] ? jn[o] : jv;
           acc[q][l] += vm[l] * jv;
         }
       }
@@ -292,7 +290,17 @@ extern "C" pk_status pk_bin_bessel(void *stream, const void *d1, const void *d2,
              "Bessel workspace too small");
   cudaStream_t s = (cudaStream_t)stream;
   double *partials = static_cast<double *>(workspace);
-  bessel_project_kernel<<<nctas, BES_THREADS, 0, s>>>(g, op, d_sep, partials);
+  int lmax = 0;
+  for (int l = 0; l < nells; ++l) lmax = ells[l] > lmax ? ells[l] : lmax;
+  switch (lmax) {
+#define PK_BES_CASE(L)                                                          \
+  case L:                                                                       \
+    bessel_project_kernel<L><<<nctas, BES_THREADS, 0, s>>>(g, op, d_sep, partials); \
+    break;
+    PK_BES_CASE(0) PK_BES_CASE(1) PK_BES_CASE(2) PK_BES_CASE(3) PK_BES_CASE(4) PK_BES_CASE(5) PK_BES_CASE(6)
+    PK_BES_CASE(7) PK_BES_CASE(8)
+#undef PK_BES_CASE
+  }
   PK_LAUNCH_CHECK();
   const int n = nells * nbins;
   bessel_finalize_kernel<<<(n + 255) / 256, 256, 0, s>>>(partials, nctas, n, accumulate, d_out);
