@@ -64,3 +64,31 @@ def test_theory_and_edges_parsing():
                                                         num_raw=np.zeros(4), ell=ell) for ell in (0, 2)])
     edges, ells = _window_edges(poles, None)
     assert np.array_equal(edges, k_edges) and ells == [0, 2]
+
+
+def test_wide_angle_edges_parsing():
+    """Input multipoles given as (ell, wide-angle order) pairs (``mesh2.py:826-836``): pairs
+    anywhere turn every input into a pair, a container's ``wa_order`` labels are read back, and
+    the fixed-line-of-sight and 'local' paths refuse orders > 0."""
+    import jaxpower_b200 as jp
+    from jaxpower_b200.mesh2 import _no_wide_angle, _plain_ells, _wide_angle_terms, _window_edges
+    edges = np.arange(0., 0.1, 0.02)
+    _, ells = _window_edges(edges, [(0, 0), 2, (2, 1)])
+    assert ells == [(0, 0), (2, 0), (2, 1)]
+    _, ells = _window_edges(edges, (0, 2))
+    assert ells == [0, 2]
+    assert _wide_angle_terms([0, (2, 1)]) == [(0, 0), (2, 1)]
+    assert _plain_ells([(0, 0), 2]) == [0, 2]
+    with pytest.raises(ValueError):
+        _plain_ells([(0, 0), (2, 1)])
+    _no_wide_angle([(0, 0), 2])
+    with pytest.raises(NotImplementedError):
+        _no_wide_angle([(1, 1)])
+    k_edges = np.column_stack([edges[:-1], edges[1:]])
+    poles = jp.Mesh2SpectrumPoles([jp.Mesh2SpectrumPole(k=k_edges.mean(-1), k_edges=k_edges, nmodes=np.ones(4),
+                                                        num_raw=np.zeros(4), ell=ell, attrs={'wa_order': wa})
+                                   for ell, wa in ((0, 0), (2, 0), (1, 1))])
+    assert poles.wa_orders == (0, 0, 1)
+    got, ells = _window_edges(poles, None)
+    assert np.array_equal(got, k_edges) and ells == [(0, 0), (2, 0), (1, 1)]
+    assert poles.get(ells=1, wa_orders=1).ell == 1
