@@ -51,7 +51,7 @@ class DeferredRows:
             return
         import torch
         ready = torch.cuda.Event()
-        ready.record()
+        ready.record(torch.cuda.current_stream(self._sums.device))  # the sums' device, whichever is current
         stream = _readback_stream(self._sums.device)
         host = torch.empty(self._sums.shape, dtype=self._sums.dtype, pin_memory=True)
         with torch.cuda.stream(stream):
